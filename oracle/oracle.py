@@ -1,0 +1,133 @@
+"""ctypes wrapper of the oracle restatement oracle/libp2oracle.so (built from
+oracle/p2oracle.c by oracle/Makefile).
+
+TEST INFRASTRUCTURE ONLY: tests/, __graft_entry__.smoke() and bench.py's
+CPU-baseline leg use it as the checker; nothing in pardiso2_b200 imports it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libp2oracle.so")
+
+_dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_fp = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
+_ip = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+_bp = np.ctypeslib.ndpointer(dtype=np.int8, flags="C_CONTIGUOUS")
+_lib: Optional[C.CDLL] = None
+
+
+def available() -> bool:
+    return os.path.exists(LIB_PATH)
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        L = C.CDLL(LIB_PATH)
+        L.p2o_create.argtypes = [C.c_int, C.c_int, C.c_int, _dp, _dp, _dp, C.c_int, _ip, _fp, _ip]
+        L.p2o_create.restype = C.c_void_p
+        L.p2o_destroy.argtypes = [C.c_void_p]
+        L.p2o_set_params.argtypes = [C.c_void_p, _dp, C.c_int, _ip, _ip]
+        L.p2o_set_fields.argtypes = [C.c_void_p] + [_fp] * 6
+        L.p2o_set_fields.restype = C.c_int
+        L.p2o_solve.argtypes = [C.c_void_p, C.c_double, C.c_int, C.c_int, _dp]
+        L.p2o_solve.restype = C.c_int
+        L.p2o_get_solution.argtypes = [C.c_void_p] + [_dp] * 4
+        L.p2o_set_solution.argtypes = [C.c_void_p] + [_dp] * 4
+        L.p2o_apply.argtypes = [C.c_void_p, C.c_int, _dp, _dp]
+        L.p2o_rhs.argtypes = [C.c_void_p, _dp]
+        L.p2o_level_fields.argtypes = [C.c_void_p, C.c_int, _fp, _fp, _dp]
+        L.p2o_rel_residual.argtypes = [C.c_void_p]
+        L.p2o_rel_residual.restype = C.c_double
+        L.p2o_ronurecalc.argtypes = [C.c_int, C.c_int, C.c_int, _dp, _dp, _dp, C.c_long, _fp, _fp, _fp, _bp,
+                                     _dp, _dp, C.c_double, C.c_double, C.c_double, C.c_int] + [_fp] * 6
+        _lib = L
+    return _lib
+
+
+def ronurecalc(model, init=None):
+    """Marker -> node fields (dict of float32 arrays) computed by the oracle."""
+    L = lib()
+    n = model.nodenum
+    keys = ("nu", "ro", "nxx", "nxy", "nxz", "nyz")
+    out = {k: (np.array(init[k], np.float32) if init is not None else np.zeros(n, np.float32)) for k in keys}
+    p = model.params
+    nx, ny, nz = model.shape
+    L.p2o_ronurecalc(nx, ny, nz, model.gx, model.gy, model.gz, model.markx.size, model.markx, model.marky,
+                     model.markz, np.ascontiguousarray(model.markt, np.int8),
+                     np.ascontiguousarray(model.rocks.n0, np.float64), np.ascontiguousarray(model.rocks.ro, np.float64),
+                     p.nubeg, p.nuend, p.nukoef, p.viscmod, *[out[k] for k in keys])
+    return out
+
+
+class OracleSolver:
+    """FP64 CPU multigrid on the reference's discrete Stokes problem."""
+
+    def __init__(self, model, npre=None, npost=None):
+        L = lib()
+        self.L = L
+        self.m = model
+        nx, ny, nz = model.shape
+        bc = model.bc
+        # keep the tables alive: the C side stores the pointers
+        self._bondm = np.ascontiguousarray(bc.bondm, np.int32)
+        self._bondv1 = np.ascontiguousarray(bc.bondv1.reshape(-1), np.float32)
+        self._bondn1 = np.ascontiguousarray(bc.bondn1, np.int32)
+        self.h = L.p2o_create(nx, ny, nz, model.gx, model.gy, model.gz, model.multinum,
+                              self._bondm, self._bondv1, self._bondn1)
+        if not self.h:
+            raise RuntimeError("oracle create failed")
+        nlev = model.multinum + 1
+        p = model.params
+        if p.p2koef != 0:
+            raise ValueError("the oracle restates p2koef == 0 only")
+        dpar = np.array([p.p0koef, p.p1koef, p.v0koef, p.v1koef, p.nubeg, p.nuend, p.gx, p.gy, p.gz], np.float64)
+        self.npre = np.array(npre if npre is not None else [2] * nlev, np.int32)
+        self.npost = np.array(npost if npost is not None else [2] * nlev, np.int32)
+        L.p2o_set_params(self.h, dpar, p.viscmod, self.npre, self.npost)
+
+    def close(self):
+        if self.h:
+            self.L.p2o_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def set_fields(self, f):
+        st = self.L.p2o_set_fields(self.h, *[np.ascontiguousarray(f[k], np.float32)
+                                             for k in ("nu", "ro", "nxx", "nxy", "nxz", "nyz")])
+        if st != 0:
+            raise RuntimeError("coarsest LU failed (status %d)" % st)
+
+    def solve(self, tol=1e-8, max_cycles=100, restart=8):
+        hist = np.zeros(max_cycles + 1, np.float64)
+        it = self.L.p2o_solve(self.h, tol, max_cycles, restart, hist)
+        return hist[: it + 1]
+
+    def solution(self):
+        n = self.m.nodenum
+        out = [np.zeros(n, np.float64) for _ in range(4)]
+        self.L.p2o_get_solution(self.h, *out)
+        return dict(zip(("pr", "vx", "vy", "vz"), out))
+
+    def set_solution(self, s):
+        self.L.p2o_set_solution(self.h, *[np.ascontiguousarray(s[k], np.float64) for k in ("pr", "vx", "vy", "vz")])
+
+    def apply(self, lev, x):
+        y = np.zeros_like(x)
+        self.L.p2o_apply(self.h, lev, np.ascontiguousarray(x, np.float64), y)
+        return y
+
+    def rhs(self):
+        b = np.zeros(self.m.nodenum * 4, np.float64)
+        self.L.p2o_rhs(self.h, b)
+        return b
+
+    def rel_residual(self):
+        return self.L.p2o_rel_residual(self.h)

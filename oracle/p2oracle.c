@@ -1,0 +1,1220 @@
+/*
+ * CPU oracle: a plain-C restatement of the reference's Stokes multigrid path
+ * (TEST INFRASTRUCTURE ONLY — tests, smoke() and bench.py's CPU-baseline leg
+ * use it as the checker; the product never links it).
+ *
+ * What is restated, with the reference lines each part follows
+ * (paths relative to the reference project):
+ *   level tables / coarse gridlines ...... pardiso/load3mg.c:2056-2194
+ *   viscosity per stencil (nxx/nxy/nxz/nyz on level 0, 8- or 2-node averages
+ *     of nu on coarse levels, clamp [nubeg,nuend]) ...
+ *                                          pardiso/move3mgNew.c:36-49, 431-444,
+ *                                          563-577, 701-714, 1506-1523
+ *   deviatoric stresses sxx..syz ......... pardiso/move3mgNew.c:3-130, 132-257,
+ *                                          259-386, 388-518, 520-657, 659-794
+ *   x/y/z-Stokes rows, right-hand sides ... pardiso/move3mgNew.c:796-1008,
+ *                                          1011-1228, 1231-1450
+ *   continuity row ....................... pardiso/move3mgNew.c:1455-1576
+ *   boundary rows x_i = c + k x_j ........ pardiso/move3mgNew.c:1682-1729
+ *   damped Gauss-Seidel / Uzawa smoother . pardiso/move3mgNew.c:3854-3959
+ *   residual restriction ................. pardiso/move3mgNew.c:3965-4353
+ *   correction prolongation .............. pardiso/move3mgNew.c:3534-3849
+ *   nu/ro restriction .................... pardiso/move3mgNew.c:3386-3527
+ *   pressure reset to pinit .............. pardiso/move3mgNew.c:2834-2855
+ *   marker -> node interpolation ......... pardiso/mark3mg.c:630-1133
+ *     (cell search m1serch..m3serch 1138-1204, constant rock viscosity
+ *      viscalc 1481-1482, constant density dencalc1 1429)
+ *   coarsest direct solve (MKL PARDISO) .. banded pivoted LU (banded_lu.h)
+ *
+ * Two deliberate solver-level differences from vpiterate() (the discrete
+ * problem is unchanged, so the converged solution is the reference's):
+ *   - a classic V-cycle with a direct coarsest correction on every cycle
+ *     (the reference solves the coarsest level only on its first outer
+ *     iteration, move3mgNew.c:2741-2768);
+ *   - the pressure cell pinned by a pure constant boundary row is smoothed
+ *     as a continuity row and the pressure is shifted afterwards so that
+ *     the pinned value holds; restricted continuity right-hand sides on
+ *     coarse levels get a volume-weighted compatibility shift.  With sealed
+ *     edges the pinned cell's continuity row is implied by the others, so
+ *     the pinned system and this formulation have the same solution.
+ * Periodic boundaries (x/y/zperiodic) and the grad-div term (p2koef != 0)
+ * are not restated: the oracle rejects them.
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "banded_lu.h"
+
+#define MAXLEV 12
+
+typedef struct {
+    int nx, ny, nz;
+    long n;           /* nodes */
+    long off;         /* node offset of the level in the reference layout (mgp) */
+    double *gx, *gy, *gz;
+    /* inverse spacings, see p2o_spacings() */
+    double *ihx, *ihy, *ihz;       /* 1/(g[i]-g[i-1])      (i>=1) */
+    double *ihxc, *ihyc, *ihzc;    /* 2/(g[i+1]-g[i-1])    (1<=i<=n-2) */
+    double *ihxe, *ihye, *ihze;    /* 1/(g[i+1]-g[i-1])    (1<=i<=n-2) */
+    double *ihxv, *ihyv, *ihzv;    /* 1/(g[i+1]-g[i])      (i<=n-2) */
+    float *nu, *ro;
+    double *ec, *exy, *exz, *eyz;  /* clamped viscosities per stencil */
+    double *x[4], *b[4], *r[4];
+    unsigned char *bcmask;         /* bit c set: unknown (node,c) is a boundary row */
+    int pin;                       /* node index of the pinned pressure cell, -1 none */
+    double pinval;
+} p2o_level;
+
+typedef struct {
+    int nlev;                      /* levels 0..nlev-1 (multinum = nlev-1) */
+    p2o_level L[MAXLEV];
+    /* boundary tables, reference layout */
+    const int *bondm;
+    const float *bondv1;
+    const int *bondn1;
+    /* parameters */
+    double p0koef, p1koef, v0koef, v1koef, nubeg, nuend;
+    double GX, GY, GZ;
+    int viscmod;
+    int npre[MAXLEV], npost[MAXLEV];
+    /* coarsest factorisation */
+    p2_band_lu lu;
+    int lu_ready;
+} p2o_ctx;
+
+#define IDX(l, i, j, k) ((long)(k) * (l)->nx * (l)->ny + (long)(i) * (l)->ny + (j))
+
+static double clampd(const p2o_ctx *c, double v)
+{
+    if (v > c->nuend) v = c->nuend;
+    if (v < c->nubeg) v = c->nubeg;
+    return v;
+}
+
+static double vavg(int viscmod, const double *v, int n)
+{
+    double s = 0;
+    int i;
+    if (viscmod == 0) { for (i = 0; i < n; i++) s += v[i]; return s / n; }
+    if (viscmod == 1) { for (i = 0; i < n; i++) s += log(v[i]); return exp(s / n); }
+    for (i = 0; i < n; i++) s += 1.0 / v[i];
+    return 1.0 / (s / n);
+}
+
+static void spacings(double *g, int n, double **ih, double **ihc, double **ihe, double **ihv)
+{
+    int i;
+    *ih = calloc(n, sizeof(double));
+    *ihc = calloc(n, sizeof(double));
+    *ihe = calloc(n, sizeof(double));
+    *ihv = calloc(n, sizeof(double));
+    for (i = 1; i < n; i++) (*ih)[i] = 1.0 / (g[i] - g[i - 1]);
+    for (i = 1; i < n - 1; i++) {
+        (*ihc)[i] = 2.0 / (g[i + 1] - g[i - 1]);
+        (*ihe)[i] = 1.0 / (g[i + 1] - g[i - 1]);
+    }
+    for (i = 0; i < n - 1; i++) (*ihv)[i] = 1.0 / (g[i + 1] - g[i]);
+}
+
+/* ---------------------------------------------------------------------- */
+/* Stencil building blocks (level-generic).                               */
+#define VX(i, j, k) (l->x[1][IDX(l, i, j, k)])
+#define VY(i, j, k) (l->x[2][IDX(l, i, j, k)])
+#define VZ(i, j, k) (l->x[3][IDX(l, i, j, k)])
+#define PR(i, j, k) (l->x[0][IDX(l, i, j, k)])
+
+/* normal strain-rate parts in cell (a,b,c) */
+static void cell_rates(const p2o_level *l, int a, int b, int c, double *dxx, double *dyy, double *dzz)
+{
+    *dxx = (VX(a, b - 1, c - 1) - VX(a - 1, b - 1, c - 1)) * l->ihx[a];
+    *dyy = (VY(a - 1, b, c - 1) - VY(a - 1, b - 1, c - 1)) * l->ihy[b];
+    *dzz = (VZ(a - 1, b - 1, c) - VZ(a - 1, b - 1, c - 1)) * l->ihz[c];
+}
+static double sxx(const p2o_level *l, int a, int b, int c)
+{
+    double dxx, dyy, dzz;
+    cell_rates(l, a, b, c, &dxx, &dyy, &dzz);
+    return 2.0 * l->ec[IDX(l, a, b, c)] * (dxx - (dxx + dyy + dzz) / 3.0);
+}
+static double syy(const p2o_level *l, int a, int b, int c)
+{
+    double dxx, dyy, dzz;
+    cell_rates(l, a, b, c, &dxx, &dyy, &dzz);
+    return 2.0 * l->ec[IDX(l, a, b, c)] * (dyy - (dxx + dyy + dzz) / 3.0);
+}
+static double szz(const p2o_level *l, int a, int b, int c)
+{
+    double dxx, dyy, dzz;
+    cell_rates(l, a, b, c, &dxx, &dyy, &dzz);
+    return 2.0 * l->ec[IDX(l, a, b, c)] * (dzz - (dxx + dyy + dzz) / 3.0);
+}
+static double sxy(const p2o_level *l, int a, int b, int c)
+{
+    return 2.0 * l->exy[IDX(l, a, b, c)] *
+           ((VX(a, b, c) - VX(a, b - 1, c)) * l->ihye[b] + (VY(a, b, c) - VY(a - 1, b, c)) * l->ihxe[a]);
+}
+static double sxz(const p2o_level *l, int a, int b, int c)
+{
+    return 2.0 * l->exz[IDX(l, a, b, c)] *
+           ((VX(a, b, c) - VX(a, b, c - 1)) * l->ihze[c] + (VZ(a, b, c) - VZ(a - 1, b, c)) * l->ihxe[a]);
+}
+static double syz(const p2o_level *l, int a, int b, int c)
+{
+    return 2.0 * l->eyz[IDX(l, a, b, c)] *
+           ((VY(a, b, c) - VY(a, b, c - 1)) * l->ihze[c] + (VZ(a, b, c) - VZ(a, b - 1, c)) * l->ihye[b]);
+}
+
+/* Rows: (A x) and the diagonal coefficient. */
+static double row_vx(const p2o_level *l, int i, int j, int k, double *diag)
+{
+    double v = (sxx(l, i + 1, j + 1, k + 1) - sxx(l, i, j + 1, k + 1)) * l->ihxc[i] +
+               (sxy(l, i, j + 1, k) - sxy(l, i, j, k)) * l->ihyv[j] +
+               (sxz(l, i, j, k + 1) - sxz(l, i, j, k)) * l->ihzv[k] -
+               (PR(i + 1, j + 1, k + 1) - PR(i, j + 1, k + 1)) * l->ihxc[i];
+    if (diag)
+        *diag = -(l->ihxc[i] * (4.0 / 3.0) *
+                      (l->ec[IDX(l, i + 1, j + 1, k + 1)] * l->ihx[i + 1] + l->ec[IDX(l, i, j + 1, k + 1)] * l->ihx[i]) +
+                  l->ihyv[j] * 2.0 * (l->exy[IDX(l, i, j + 1, k)] * l->ihye[j + 1] + l->exy[IDX(l, i, j, k)] * l->ihye[j]) +
+                  l->ihzv[k] * 2.0 * (l->exz[IDX(l, i, j, k + 1)] * l->ihze[k + 1] + l->exz[IDX(l, i, j, k)] * l->ihze[k]));
+    return v;
+}
+static double row_vy(const p2o_level *l, int i, int j, int k, double *diag)
+{
+    double v = (syy(l, i + 1, j + 1, k + 1) - syy(l, i + 1, j, k + 1)) * l->ihyc[j] +
+               (sxy(l, i + 1, j, k) - sxy(l, i, j, k)) * l->ihxv[i] +
+               (syz(l, i, j, k + 1) - syz(l, i, j, k)) * l->ihzv[k] -
+               (PR(i + 1, j + 1, k + 1) - PR(i + 1, j, k + 1)) * l->ihyc[j];
+    if (diag)
+        *diag = -(l->ihyc[j] * (4.0 / 3.0) *
+                      (l->ec[IDX(l, i + 1, j + 1, k + 1)] * l->ihy[j + 1] + l->ec[IDX(l, i + 1, j, k + 1)] * l->ihy[j]) +
+                  l->ihxv[i] * 2.0 * (l->exy[IDX(l, i + 1, j, k)] * l->ihxe[i + 1] + l->exy[IDX(l, i, j, k)] * l->ihxe[i]) +
+                  l->ihzv[k] * 2.0 * (l->eyz[IDX(l, i, j, k + 1)] * l->ihze[k + 1] + l->eyz[IDX(l, i, j, k)] * l->ihze[k]));
+    return v;
+}
+static double row_vz(const p2o_level *l, int i, int j, int k, double *diag)
+{
+    double v = (szz(l, i + 1, j + 1, k + 1) - szz(l, i + 1, j + 1, k)) * l->ihzc[k] +
+               (sxz(l, i + 1, j, k) - sxz(l, i, j, k)) * l->ihxv[i] +
+               (syz(l, i, j + 1, k) - syz(l, i, j, k)) * l->ihyv[j] -
+               (PR(i + 1, j + 1, k + 1) - PR(i + 1, j + 1, k)) * l->ihzc[k];
+    if (diag)
+        *diag = -(l->ihzc[k] * (4.0 / 3.0) *
+                      (l->ec[IDX(l, i + 1, j + 1, k + 1)] * l->ihz[k + 1] + l->ec[IDX(l, i + 1, j + 1, k)] * l->ihz[k]) +
+                  l->ihxv[i] * 2.0 * (l->exz[IDX(l, i + 1, j, k)] * l->ihxe[i + 1] + l->exz[IDX(l, i, j, k)] * l->ihxe[i]) +
+                  l->ihyv[j] * 2.0 * (l->eyz[IDX(l, i, j + 1, k)] * l->ihye[j + 1] + l->eyz[IDX(l, i, j, k)] * l->ihye[j]));
+    return v;
+}
+static double row_p(const p2o_level *l, int i, int j, int k)
+{
+    return (VX(i, j - 1, k - 1) - VX(i - 1, j - 1, k - 1)) * l->ihx[i] +
+           (VY(i - 1, j, k - 1) - VY(i - 1, j - 1, k - 1)) * l->ihy[j] +
+           (VZ(i - 1, j - 1, k) - VZ(i - 1, j - 1, k - 1)) * l->ihz[k];
+}
+
+static int valid(const p2o_level *l, int c, int i, int j, int k)
+{
+    if (c == 0) return i > 0 && j > 0 && k > 0;
+    if (c == 1) return j < l->ny - 1 && k < l->nz - 1;
+    if (c == 2) return i < l->nx - 1 && k < l->nz - 1;
+    return i < l->nx - 1 && j < l->ny - 1;
+}
+
+/* Boundary row of unknown (node u, comp c) on level li: x = cst + koef * x[target]. */
+static void bc_of(const p2o_ctx *C, int li, long u, int c, double *cst, double *koef, long *tnode, int *tcomp)
+{
+    const p2o_level *l = &C->L[li];
+    long g = (l->off + u) * 4 + c;
+    int bi = C->bondm[g];
+    long t = C->bondn1[bi];
+    *cst = C->bondv1[2 * bi];
+    *koef = 0;
+    *tnode = -1;
+    *tcomp = 0;
+    if (t) {
+        t -= 1;
+        *koef = C->bondv1[2 * bi + 1];
+        *tnode = t / 4 - l->off;
+        *tcomp = (int)(t % 4);
+    }
+}
+
+/* Is unknown (u,c) a boundary row that is NOT the pressure pin? */
+static int is_bc(const p2o_level *l, long u, int c)
+{
+    if (!(l->bcmask[u] & (1 << c))) return 0;
+    if (c == 0 && u == l->pin) return 0;
+    return 1;
+}
+
+/* r = b - A x on all rows of level li (BC rows: r = cst*(li==0) + koef*x_t - x). */
+static void residual(p2o_ctx *C, int li)
+{
+    p2o_level *l = &C->L[li];
+    int i, j, k, c;
+    for (k = 0; k < l->nz; k++)
+        for (i = 0; i < l->nx; i++)
+            for (j = 0; j < l->ny; j++) {
+                long u = IDX(l, i, j, k);
+                for (c = 0; c < 4; c++) {
+                    double ax;
+                    if (!valid(l, c, i, j, k)) { l->r[c][u] = 0; continue; }
+                    if (is_bc(l, u, c)) {
+                        double cst, koef; long tn; int tc;
+                        bc_of(C, li, u, c, &cst, &koef, &tn, &tc);
+                        l->r[c][u] = l->b[c][u] + (tn >= 0 ? koef * l->x[tc][tn] : 0.0) - l->x[c][u];
+                        continue;
+                    }
+                    if (c == 0) ax = row_p(l, i, j, k);
+                    else if (c == 1) ax = row_vx(l, i, j, k, NULL);
+                    else if (c == 2) ax = row_vy(l, i, j, k, NULL);
+                    else ax = row_vz(l, i, j, k, NULL);
+                    l->r[c][u] = l->b[c][u] - ax;
+                }
+            }
+}
+
+/* Level-0 relative residual of the pinned system: every row except the pinned
+ * cell's continuity row (whose pin row is exact after the pressure shift). */
+static double rel_residual(p2o_ctx *C, double *rnorm, double *bnorm)
+{
+    p2o_level *l = &C->L[0];
+    long u;
+    int c;
+    double rr = 0, bb = 0;
+    residual(C, 0);
+    for (c = 0; c < 4; c++)
+        for (u = 0; u < l->n; u++) {
+            double bv;
+            if (c == 0 && u == l->pin) continue;
+            rr += l->r[c][u] * l->r[c][u];
+            bv = l->b[c][u];
+            bb += bv * bv;
+        }
+    /* the pin row itself: b = pinval */
+    if (l->pin >= 0) bb += l->pinval * l->pinval;
+    if (rnorm) *rnorm = sqrt(rr);
+    if (bnorm) *bnorm = sqrt(bb);
+    return bb > 0 ? sqrt(rr / bb) : sqrt(rr);
+}
+
+/* Lexicographic damped Gauss-Seidel with Uzawa pressure update, per node
+ * P, Vx, Vy, Vz as gausmat4 does (move3mgNew.c:3880-3924). */
+static void smooth(p2o_ctx *C, int li, int sweeps)
+{
+    p2o_level *l = &C->L[li];
+    int s, i, j, k, c;
+    for (s = 0; s < sweeps; s++)
+        for (k = 0; k < l->nz; k++)
+            for (i = 0; i < l->nx; i++)
+                for (j = 0; j < l->ny; j++) {
+                    long u = IDX(l, i, j, k);
+                    for (c = 0; c < 4; c++) {
+                        double ax, dg;
+                        if (!valid(l, c, i, j, k)) continue;
+                        if (is_bc(l, u, c)) {
+                            double cst, koef; long tn; int tc;
+                            bc_of(C, li, u, c, &cst, &koef, &tn, &tc);
+                            l->x[c][u] = l->b[c][u] + (tn >= 0 ? koef * l->x[tc][tn] : 0.0);
+                            continue;
+                        }
+                        if (c == 0) {
+                            ax = row_p(l, i, j, k);
+                            l->x[0][u] -= (ax - l->b[0][u]) * l->ec[u] * C->p0koef;
+                            continue;
+                        }
+                        if (c == 1) ax = row_vx(l, i, j, k, &dg);
+                        else if (c == 2) ax = row_vy(l, i, j, k, &dg);
+                        else ax = row_vz(l, i, j, k, &dg);
+                        l->x[c][u] -= (ax - l->b[c][u]) / dg * C->v0koef;
+                    }
+                }
+}
+
+/* Coloured cell-block smoother (diagonal Vanka / SCGS): for every cell of one
+ * colour (parity of i+j+k) the six face velocities and the cell pressure are
+ * corrected together, with the velocity block replaced by its diagonal:
+ *   d_v dv_v + g_v dp = r_v,  sum_v c_v dv_v = r_p.
+ * All cells of a colour read the state from before that colour's pass
+ * (Jacobi within a colour, Gauss-Seidel between colours), which is what a
+ * parallel GPU pass does.  Boundary-row faces are excluded from the block and
+ * re-applied after each colour. */
+static double row_any(const p2o_level *l, int c, int i, int j, int k, double *dg)
+{
+    if (c == 1) return row_vx(l, i, j, k, dg);
+    if (c == 2) return row_vy(l, i, j, k, dg);
+    return row_vz(l, i, j, k, dg);
+}
+
+static void apply_bc_rows(p2o_ctx *C, int li)
+{
+    p2o_level *l = &C->L[li];
+    int i, j, k, c, pass;
+    for (pass = 0; pass < 2; pass++) /* two passes resolve copy chains of length 2 */
+        for (k = 0; k < l->nz; k++)
+            for (i = 0; i < l->nx; i++)
+                for (j = 0; j < l->ny; j++) {
+                    long u = IDX(l, i, j, k);
+                    for (c = 0; c < 4; c++) {
+                        double cst, koef; long tn; int tc;
+                        if (!valid(l, c, i, j, k) || !is_bc(l, u, c)) continue;
+                        bc_of(C, li, u, c, &cst, &koef, &tn, &tc);
+                        l->x[c][u] = l->b[c][u] + (tn >= 0 ? koef * l->x[tc][tn] : 0.0);
+                    }
+                }
+}
+
+double p2o_vanka_omega = 1.0;
+
+static void smooth_vanka(p2o_ctx *C, int li, int sweeps)
+{
+    p2o_level *l = &C->L[li];
+    double *dx[4];
+    int s, col, i, j, k, c;
+    for (c = 0; c < 4; c++) dx[c] = calloc(l->n, sizeof(double));
+    apply_bc_rows(C, li);
+    for (s = 0; s < sweeps; s++)
+        for (col = 0; col < 2; col++) {
+            for (c = 0; c < 4; c++) memset(dx[c], 0, sizeof(double) * l->n);
+            for (k = 1; k < l->nz; k++)
+                for (i = 1; i < l->nx; i++)
+                    for (j = 1; j < l->ny; j++) {
+                        long u = IDX(l, i, j, k), vn[6];
+                        int vc[6], vi[6], vj[6], vk[6], q, pbc;
+                        double r[6], d[6], g[6], cc[6], rp, num = 0, den = 0, dp = 0;
+                        if (((i + j + k) & 1) != col) continue;
+                        /* faces: vx left/right, vy front/back, vz bottom/top */
+                        vc[0] = 1; vi[0] = i - 1; vj[0] = j - 1; vk[0] = k - 1; g[0] = -l->ihxc[i - 1]; cc[0] = -l->ihx[i];
+                        vc[1] = 1; vi[1] = i;     vj[1] = j - 1; vk[1] = k - 1; g[1] = +l->ihxc[i];     cc[1] = +l->ihx[i];
+                        vc[2] = 2; vi[2] = i - 1; vj[2] = j - 1; vk[2] = k - 1; g[2] = -l->ihyc[j - 1]; cc[2] = -l->ihy[j];
+                        vc[3] = 2; vi[3] = i - 1; vj[3] = j;     vk[3] = k - 1; g[3] = +l->ihyc[j];     cc[3] = +l->ihy[j];
+                        vc[4] = 3; vi[4] = i - 1; vj[4] = j - 1; vk[4] = k - 1; g[4] = -l->ihzc[k - 1]; cc[4] = -l->ihz[k];
+                        vc[5] = 3; vi[5] = i - 1; vj[5] = j - 1; vk[5] = k;     g[5] = +l->ihzc[k];     cc[5] = +l->ihz[k];
+                        pbc = is_bc(l, u, 0);
+                        for (q = 0; q < 6; q++) {
+                            vn[q] = IDX(l, vi[q], vj[q], vk[q]);
+                            if (is_bc(l, vn[q], vc[q])) { d[q] = 0; r[q] = 0; continue; }
+                            r[q] = l->b[vc[q]][vn[q]] - row_any(l, vc[q], vi[q], vj[q], vk[q], &d[q]);
+                            if (!pbc) { num += cc[q] * r[q] / d[q]; den += cc[q] * g[q] / d[q]; }
+                        }
+                        if (!pbc && den != 0.0) {
+                            rp = l->b[0][u] - row_p(l, i, j, k);
+                            dp = (num - rp) / den;
+                            dx[0][u] = dp;
+                        }
+                        for (q = 0; q < 6; q++)
+                            if (d[q] != 0.0) dx[vc[q]][vn[q]] = (r[q] - (pbc ? 0.0 : g[q] * dp)) / d[q];
+                    }
+            for (c = 0; c < 4; c++) {
+                long u;
+                for (u = 0; u < l->n; u++) l->x[c][u] += p2o_vanka_omega * dx[c][u];
+            }
+            apply_bc_rows(C, li);
+        }
+    for (c = 0; c < 4; c++) free(dx[c]);
+}
+
+int p2o_smoother = 0; /* 0: lexicographic GS + Uzawa (reference scheme), 1: coloured Vanka */
+
+/* ---------------------------------------------------------------------- */
+/* Transfer weights along one axis (vprestrict/vpprolong index rules).     */
+typedef struct { int lo; double w0, w1; } axw;
+
+static int cmin_common(int m, int nf, int nc)
+{
+    int r = (m - 2) / 2 + 2;
+    if (m < 3) r = m;
+    if (m > nf - 4) r = nc - (nf - m);
+    return r;
+}
+
+/* node-located component along its own axis */
+static axw axis_node(const double *gf, int nf, const double *gc, int nc, int m)
+{
+    axw a;
+    double d;
+    int lo = cmin_common(m, nf, nc);
+    if (lo > nc - 2) lo = nc - 2;
+    d = gc[lo + 1] - gc[lo];
+    a.lo = lo;
+    a.w0 = 1.0 + (gc[lo] - gf[m]) / d;
+    a.w1 = 1.0 - (gc[lo + 1] - gf[m]) / d;
+    return a;
+}
+/* mid-located (between lines m and m+1) */
+static axw axis_mid(const double *gf, int nf, const double *gc, int nc, int m)
+{
+    axw a;
+    double d, xf;
+    int lo = cmin_common(m, nf, nc);
+    if (lo > nc - 3) lo = nc - 3;
+    if ((gf[m] + gf[m + 1]) / 2.0 < (gc[lo] + gc[lo + 1]) / 2.0 && lo > 0) lo -= 1;
+    d = (gc[lo + 2] - gc[lo]) / 2.0;
+    xf = gf[m] + gf[m + 1];
+    a.lo = lo;
+    a.w0 = 1.0 + (gc[lo] + gc[lo + 1] - xf) / 2.0 / d;
+    a.w1 = 1.0 - (gc[lo + 1] + gc[lo + 2] - xf) / 2.0 / d;
+    return a;
+}
+/* pressure cell centre (between lines m-1 and m) */
+static axw axis_cell(const double *gf, int nf, const double *gc, int nc, int m)
+{
+    axw a;
+    double d, xf;
+    int lo = cmin_common(m, nf, nc);
+    if (lo > nc - 2) lo = nc - 2;
+    if ((gf[m] + gf[m - 1]) / 2.0 < (gc[lo] + gc[lo - 1]) / 2.0 && lo > 1) lo -= 1;
+    d = (gc[lo + 1] - gc[lo - 1]) / 2.0;
+    xf = gf[m] + gf[m - 1];
+    a.lo = lo;
+    a.w0 = 1.0 + (gc[lo] + gc[lo - 1] - xf) / 2.0 / d;
+    a.w1 = 1.0 - (gc[lo + 1] + gc[lo] - xf) / 2.0 / d;
+    return a;
+}
+
+static void axes_for(const p2o_level *f, const p2o_level *cl, int c, int i, int j, int k, axw *ax, axw *ay, axw *az)
+{
+    if (c == 0) {
+        *ax = axis_cell(f->gx, f->nx, cl->gx, cl->nx, i);
+        *ay = axis_cell(f->gy, f->ny, cl->gy, cl->ny, j);
+        *az = axis_cell(f->gz, f->nz, cl->gz, cl->nz, k);
+    } else if (c == 1) {
+        *ax = axis_node(f->gx, f->nx, cl->gx, cl->nx, i);
+        *ay = axis_mid(f->gy, f->ny, cl->gy, cl->ny, j);
+        *az = axis_mid(f->gz, f->nz, cl->gz, cl->nz, k);
+    } else if (c == 2) {
+        *ax = axis_mid(f->gx, f->nx, cl->gx, cl->nx, i);
+        *ay = axis_node(f->gy, f->ny, cl->gy, cl->ny, j);
+        *az = axis_mid(f->gz, f->nz, cl->gz, cl->nz, k);
+    } else {
+        *ax = axis_mid(f->gx, f->nx, cl->gx, cl->nx, i);
+        *ay = axis_mid(f->gy, f->ny, cl->gy, cl->ny, j);
+        *az = axis_node(f->gz, f->nz, cl->gz, cl->nz, k);
+    }
+}
+
+static double cell_volume(const p2o_level *l, int i, int j, int k)
+{
+    return 1.0 / (l->ihx[i] * l->ihy[j] * l->ihz[k]);
+}
+
+/* Coarse right-hand side from the fine residual (vprestrict), then the
+ * compatibility shift of the continuity rows. */
+int p2o_eta_scale = 1;
+static void restrict_level(p2o_ctx *C, int lc)
+{
+    p2o_level *f = &C->L[lc - 1], *cl = &C->L[lc];
+    double *acc[4], *wsum[4];
+    int c, i, j, k, a, b2, d;
+    for (c = 0; c < 4; c++) {
+        acc[c] = calloc(cl->n, sizeof(double));
+        wsum[c] = calloc(cl->n, sizeof(double));
+    }
+    for (k = 0; k < f->nz; k++)
+        for (i = 0; i < f->nx; i++)
+            for (j = 0; j < f->ny; j++) {
+                long u = IDX(f, i, j, k);
+                for (c = 0; c < 4; c++) {
+                    axw ax, ay, az;
+                    if (!valid(f, c, i, j, k) || is_bc(f, u, c)) continue;
+                    axes_for(f, cl, c, i, j, k, &ax, &ay, &az);
+                    for (d = 0; d < 2; d++)
+                        for (a = 0; a < 2; a++)
+                            for (b2 = 0; b2 < 2; b2++) {
+                                long v = IDX(cl, ax.lo + a, ay.lo + b2, az.lo + d);
+                                double w = (a ? ax.w1 : ax.w0) * (b2 ? ay.w1 : ay.w0) * (d ? az.w1 : az.w0);
+                                double val = f->r[c][u];
+                                if (is_bc(cl, v, c)) continue;
+                                if (c == 0 && p2o_eta_scale) val *= f->ec[u] / cl->ec[v];
+                                acc[c][v] += val * w;
+                                wsum[c][v] += w;
+                            }
+                }
+            }
+    for (c = 0; c < 4; c++) {
+        long v;
+        for (v = 0; v < cl->n; v++) {
+            cl->b[c][v] = wsum[c][v] != 0 ? acc[c][v] / wsum[c][v] : 0.0;
+            cl->x[c][v] = 0;
+        }
+        free(acc[c]);
+        free(wsum[c]);
+    }
+    /* compatibility: sum over continuity rows of volume * rhs must vanish */
+    {
+        double sv = 0, s = 0;
+        for (k = 1; k < cl->nz; k++)
+            for (i = 1; i < cl->nx; i++)
+                for (j = 1; j < cl->ny; j++) {
+                    long v = IDX(cl, i, j, k);
+                    if (is_bc(cl, v, 0)) continue;
+                    s += cell_volume(cl, i, j, k) * cl->b[0][v];
+                    sv += cell_volume(cl, i, j, k);
+                }
+        if (sv > 0) {
+            double sh = s / sv;
+            for (k = 1; k < cl->nz; k++)
+                for (i = 1; i < cl->nx; i++)
+                    for (j = 1; j < cl->ny; j++) {
+                        long v = IDX(cl, i, j, k);
+                        if (!is_bc(cl, v, 0)) cl->b[0][v] -= sh;
+                    }
+        }
+    }
+}
+
+static void prolong_level(p2o_ctx *C, int lc)
+{
+    p2o_level *f = &C->L[lc - 1], *cl = &C->L[lc];
+    int c, i, j, k, a, b2, d;
+    for (k = 0; k < f->nz; k++)
+        for (i = 0; i < f->nx; i++)
+            for (j = 0; j < f->ny; j++) {
+                long u = IDX(f, i, j, k);
+                for (c = 0; c < 4; c++) {
+                    axw ax, ay, az;
+                    double s = 0;
+                    if (!valid(f, c, i, j, k)) continue;
+                    axes_for(f, cl, c, i, j, k, &ax, &ay, &az);
+                    for (d = 0; d < 2; d++)
+                        for (a = 0; a < 2; a++)
+                            for (b2 = 0; b2 < 2; b2++) {
+                                long v = IDX(cl, ax.lo + a, ay.lo + b2, az.lo + d);
+                                double w = (a ? ax.w1 : ax.w0) * (b2 ? ay.w1 : ay.w0) * (d ? az.w1 : az.w0);
+                                s += cl->x[c][v] * w;
+                            }
+                    f->x[c][u] += s * (c == 0 ? C->p1koef : C->v1koef);
+                }
+            }
+}
+
+/* nu, ro of level lc from level lc-1 (ronurestrict). */
+static void ronurestrict_level(p2o_ctx *C, int lc)
+{
+    p2o_level *f = &C->L[lc - 1], *cl = &C->L[lc];
+    double *sn = calloc(cl->n, sizeof(double)), *sr = calloc(cl->n, sizeof(double)), *sw = calloc(cl->n, sizeof(double));
+    int i, j, k, a, b2, d;
+    long v;
+    for (k = 0; k < f->nz; k++)
+        for (i = 0; i < f->nx; i++)
+            for (j = 0; j < f->ny; j++) {
+                long u = IDX(f, i, j, k);
+                int lo[3], m[3], n[3], nf[3], q;
+                const double *gf[3], *gc[3];
+                m[0] = i; m[1] = j; m[2] = k;
+                nf[0] = f->nx; nf[1] = f->ny; nf[2] = f->nz;
+                n[0] = cl->nx; n[1] = cl->ny; n[2] = cl->nz;
+                gf[0] = f->gx; gf[1] = f->gy; gf[2] = f->gz;
+                gc[0] = cl->gx; gc[1] = cl->gy; gc[2] = cl->gz;
+                for (q = 0; q < 3; q++) {
+                    lo[q] = cmin_common(m[q], nf[q], n[q]);
+                    if (lo[q] > n[q] - 2) lo[q] = n[q] - 2;
+                }
+                for (d = 0; d < 2; d++)
+                    for (a = 0; a < 2; a++)
+                        for (b2 = 0; b2 < 2; b2++) {
+                            double wz = 1.0 - fabs((gc[2][lo[2] + d] - gf[2][k]) / (gc[2][lo[2] + 1] - gc[2][lo[2]]));
+                            double wx = 1.0 - fabs((gc[0][lo[0] + a] - gf[0][i]) / (gc[0][lo[0] + 1] - gc[0][lo[0]]));
+                            double wy = 1.0 - fabs((gc[1][lo[1] + b2] - gf[1][j]) / (gc[1][lo[1] + 1] - gc[1][lo[1]]));
+                            double w = wx * wy * wz, fv;
+                            long t = IDX(cl, lo[0] + a, lo[1] + b2, lo[2] + d);
+                            if (C->viscmod == 0) fv = f->nu[u];
+                            else if (C->viscmod == 1) fv = log(f->nu[u]);
+                            else fv = 1.0 / f->nu[u];
+                            sn[t] += fv * w;
+                            sr[t] += f->ro[u] * w;
+                            sw[t] += w;
+                        }
+            }
+    for (v = 0; v < cl->n; v++) {
+        double nv = sn[v] / sw[v];
+        if (C->viscmod == 1) nv = exp(nv);
+        if (C->viscmod == 2) nv = 1.0 / nv;
+        cl->nu[v] = (float)nv;
+        cl->ro[v] = (float)(sr[v] / sw[v]);
+    }
+    free(sn); free(sr); free(sw);
+}
+
+/* Viscosity per stencil on a level (level 0 from nxx..nyz, coarse from nu). */
+static void level_viscosity(p2o_ctx *C, int li, const float *nxx, const float *nxy, const float *nxz, const float *nyz)
+{
+    p2o_level *l = &C->L[li];
+    int i, j, k;
+    for (k = 0; k < l->nz; k++)
+        for (i = 0; i < l->nx; i++)
+            for (j = 0; j < l->ny; j++) {
+                long u = IDX(l, i, j, k);
+                if (li == 0) {
+                    l->ec[u] = clampd(C, nxx[u]);
+                    l->exy[u] = clampd(C, nxy[u]);
+                    l->exz[u] = clampd(C, nxz[u]);
+                    l->eyz[u] = clampd(C, nyz[u]);
+                    continue;
+                }
+                if (i > 0 && j > 0 && k > 0) {
+                    double v[8];
+                    v[0] = l->nu[IDX(l, i - 1, j - 1, k - 1)]; v[1] = l->nu[IDX(l, i - 1, j, k - 1)];
+                    v[2] = l->nu[IDX(l, i, j - 1, k - 1)];     v[3] = l->nu[IDX(l, i, j, k - 1)];
+                    v[4] = l->nu[IDX(l, i - 1, j - 1, k)];     v[5] = l->nu[IDX(l, i - 1, j, k)];
+                    v[6] = l->nu[IDX(l, i, j - 1, k)];         v[7] = l->nu[IDX(l, i, j, k)];
+                    l->ec[u] = clampd(C, vavg(C->viscmod, v, 8));
+                } else {
+                    l->ec[u] = C->nubeg;
+                }
+                {
+                    double v[2];
+                    v[0] = l->nu[u];
+                    v[1] = k + 1 < l->nz ? l->nu[IDX(l, i, j, k + 1)] : l->nu[u];
+                    l->exy[u] = clampd(C, vavg(C->viscmod, v, 2));
+                    v[1] = j + 1 < l->ny ? l->nu[IDX(l, i, j + 1, k)] : l->nu[u];
+                    l->exz[u] = clampd(C, vavg(C->viscmod, v, 2));
+                    v[1] = i + 1 < l->nx ? l->nu[IDX(l, i + 1, j, k)] : l->nu[u];
+                    l->eyz[u] = clampd(C, vavg(C->viscmod, v, 2));
+                }
+            }
+}
+
+/* ---------------------------------------------------------------------- */
+/* Coarsest operator: probe the matrix-free rows (pinned system: the pin row
+ * is x = 0, ghost rows are the identity) and factor as a band. */
+static int coarse_factor(p2o_ctx *C)
+{
+    int li = C->nlev - 1;
+    p2o_level *l = &C->L[li];
+    long N = l->n * 4, kl = 4 * ((long)l->nx * l->ny + l->ny + 1) + 8;
+    int cx, cy, cz, cc, i, j, k, c;
+    double *save[4];
+    if (C->lu_ready) { p2_band_free(&C->lu); C->lu_ready = 0; }
+    if (p2_band_alloc(&C->lu, N, kl, kl)) return -1;
+    for (c = 0; c < 4; c++) { save[c] = l->x[c]; l->x[c] = calloc(l->n, sizeof(double)); }
+    for (cz = 0; cz < 5; cz++)
+        for (cx = 0; cx < 5; cx++)
+            for (cy = 0; cy < 5; cy++)
+                for (cc = 0; cc < 4; cc++) {
+                    for (c = 0; c < 4; c++) memset(l->x[c], 0, sizeof(double) * l->n);
+                    for (k = cz; k < l->nz; k += 5)
+                        for (i = cx; i < l->nx; i += 5)
+                            for (j = cy; j < l->ny; j += 5) l->x[cc][IDX(l, i, j, k)] = 1.0;
+                    for (k = 0; k < l->nz; k++)
+                        for (i = 0; i < l->nx; i++)
+                            for (j = 0; j < l->ny; j++) {
+                                long u = IDX(l, i, j, k);
+                                int ci = i + ((cx - i) % 5 + 5) % 5, cj = j + ((cy - j) % 5 + 5) % 5, ck = k + ((cz - k) % 5 + 5) % 5;
+                                long col;
+                                if (ci > i + 2) ci -= 5;
+                                if (cj > j + 2) cj -= 5;
+                                if (ck > k + 2) ck -= 5;
+                                if (ci < 0 || cj < 0 || ck < 0 || ci >= l->nx || cj >= l->ny || ck >= l->nz) continue;
+                                col = IDX(l, ci, cj, ck) * 4 + cc;
+                                for (c = 0; c < 4; c++) {
+                                    long row = u * 4 + c;
+                                    double a;
+                                    if (!valid(l, c, i, j, k)) {
+                                        a = (row == col) ? 1.0 : 0.0;
+                                    } else if ((l->bcmask[u] & (1 << c))) {
+                                        double cst, koef; long tn; int tc;
+                                        bc_of(C, li, u, c, &cst, &koef, &tn, &tc);
+                                        a = (row == col) ? 1.0 : 0.0;
+                                        if (tn >= 0 && tn * 4 + tc == col) a -= koef;
+                                    } else if (c == 0) {
+                                        a = row_p(l, i, j, k);
+                                    } else if (c == 1) {
+                                        a = row_vx(l, i, j, k, NULL);
+                                    } else if (c == 2) {
+                                        a = row_vy(l, i, j, k, NULL);
+                                    } else {
+                                        a = row_vz(l, i, j, k, NULL);
+                                    }
+                                    if (a != 0.0) {
+                                        if (labs(row - col) > kl) { fprintf(stderr, "coarse band overflow\n"); return -2; }
+                                        *p2_band_at(&C->lu, row, col) = a;
+                                    }
+                                }
+                            }
+                }
+    for (c = 0; c < 4; c++) { free(l->x[c]); l->x[c] = save[c]; }
+    C->lu_ready = 1;
+    return p2_band_factor(&C->lu);
+}
+
+static void coarse_solve(p2o_ctx *C)
+{
+    int li = C->nlev - 1;
+    p2o_level *l = &C->L[li];
+    long N = l->n * 4, u;
+    int c;
+    double *rhs = calloc(N, sizeof(double));
+    for (u = 0; u < l->n; u++)
+        for (c = 0; c < 4; c++) {
+            int ii = (int)((u / l->ny) % l->nx), jj = (int)(u % l->ny), kk = (int)(u / ((long)l->nx * l->ny));
+            if (!valid(l, c, ii, jj, kk) || (l->bcmask[u] & (1 << c))) rhs[u * 4 + c] = 0;
+            else rhs[u * 4 + c] = l->b[c][u];
+        }
+    p2_band_solve(&C->lu, rhs);
+    for (u = 0; u < l->n; u++)
+        for (c = 0; c < 4; c++) l->x[c][u] = rhs[u * 4 + c];
+    free(rhs);
+}
+
+/* Shift the pressure so that the pinned cell holds its value. */
+static void normalize_pressure(p2o_ctx *C, int li)
+{
+    p2o_level *l = &C->L[li];
+    long u;
+    double sh;
+    if (l->pin < 0) return;
+    sh = (li == 0 ? l->pinval : 0.0) - l->x[0][l->pin];
+    for (u = 0; u < l->n; u++) {
+        int i = (int)((u / l->ny) % l->nx), j = (int)(u % l->ny), k = (int)(u / ((long)l->nx * l->ny));
+        if (i > 0 && j > 0 && k > 0) l->x[0][u] += sh;
+    }
+}
+
+static void vcycle(p2o_ctx *C)
+{
+    int li;
+    for (li = 0; li < C->nlev - 1; li++) {
+        if (p2o_smoother) smooth_vanka(C, li, C->npre[li]); else smooth(C, li, C->npre[li]);
+        residual(C, li);
+        restrict_level(C, li + 1);
+    }
+    coarse_solve(C);
+    for (li = C->nlev - 2; li >= 0; li--) {
+        prolong_level(C, li + 1);
+        if (p2o_smoother) smooth_vanka(C, li, C->npost[li]); else smooth(C, li, C->npost[li]);
+    }
+}
+
+/* ---------------------------------------------------------------------- */
+/* Public API (ctypes).                                                    */
+
+void *p2o_create(int nx, int ny, int nz, const double *gx, const double *gy, const double *gz, int multinum,
+                 const int *bondm, const float *bondv1, const int *bondn1)
+{
+    p2o_ctx *C = calloc(1, sizeof(p2o_ctx));
+    int li;
+    long off = 0;
+    if (multinum + 1 > MAXLEV) { free(C); return NULL; }
+    C->nlev = multinum + 1;
+    C->bondm = bondm; C->bondv1 = bondv1; C->bondn1 = bondn1;
+    for (li = 0; li <= multinum; li++) {
+        p2o_level *l = &C->L[li];
+        int q, c, s = 1 << li;
+        if (li == 0) { l->nx = nx; l->ny = ny; l->nz = nz; }
+        else {
+            l->nx = (C->L[li - 1].nx - 5) / 2 + 5;
+            l->ny = (C->L[li - 1].ny - 5) / 2 + 5;
+            l->nz = (C->L[li - 1].nz - 5) / 2 + 5;
+        }
+        l->n = (long)l->nx * l->ny * l->nz;
+        l->off = off;
+        off += l->n;
+        l->gx = malloc(sizeof(double) * l->nx);
+        l->gy = malloc(sizeof(double) * l->ny);
+        l->gz = malloc(sizeof(double) * l->nz);
+        /* load3mg.c:2079-2194: outer three lines copied, interior (n2-2)*s+2 */
+        for (q = 0; q < 3; q++) {
+            int n = q == 0 ? l->nx : q == 1 ? l->ny : l->nz, nf = q == 0 ? nx : q == 1 ? ny : nz, n2;
+            const double *g = q == 0 ? gx : q == 1 ? gy : gz;
+            double *o = q == 0 ? l->gx : q == 1 ? l->gy : l->gz;
+            o[0] = g[0]; o[1] = g[1]; o[2] = g[2];
+            o[n - 1] = g[nf - 1]; o[n - 2] = g[nf - 2]; o[n - 3] = g[nf - 3];
+            for (n2 = 3; n2 < n - 3; n2++) o[n2] = g[(n2 - 2) * s + 2];
+        }
+        spacings(l->gx, l->nx, &l->ihx, &l->ihxc, &l->ihxe, &l->ihxv);
+        spacings(l->gy, l->ny, &l->ihy, &l->ihyc, &l->ihye, &l->ihyv);
+        spacings(l->gz, l->nz, &l->ihz, &l->ihzc, &l->ihze, &l->ihzv);
+        l->nu = calloc(l->n, sizeof(float));
+        l->ro = calloc(l->n, sizeof(float));
+        l->ec = calloc(l->n, sizeof(double));
+        l->exy = calloc(l->n, sizeof(double));
+        l->exz = calloc(l->n, sizeof(double));
+        l->eyz = calloc(l->n, sizeof(double));
+        for (c = 0; c < 4; c++) {
+            l->x[c] = calloc(l->n, sizeof(double));
+            l->b[c] = calloc(l->n, sizeof(double));
+            l->r[c] = calloc(l->n, sizeof(double));
+        }
+        l->bcmask = calloc(l->n, 1);
+        l->pin = -1;
+        {
+            long u;
+            int npin = 0;
+            for (u = 0; u < l->n; u++)
+                for (c = 0; c < 4; c++)
+                    if (bondm[(l->off + u) * 4 + c]) {
+                        l->bcmask[u] |= (unsigned char)(1 << c);
+                        if (c == 0 && bondn1[bondm[(l->off + u) * 4]] == 0) {
+                            npin++;
+                            l->pin = u;
+                            l->pinval = bondv1[2 * bondm[(l->off + u) * 4]];
+                        }
+                    }
+            if (npin != 1) l->pin = -1; /* several pure pins: all stay boundary rows */
+        }
+    }
+    return C;
+}
+
+void p2o_destroy(void *h)
+{
+    p2o_ctx *C = h;
+    int li, c;
+    if (!C) return;
+    for (li = 0; li < C->nlev; li++) {
+        p2o_level *l = &C->L[li];
+        free(l->gx); free(l->gy); free(l->gz);
+        free(l->ihx); free(l->ihxc); free(l->ihxe); free(l->ihxv);
+        free(l->ihy); free(l->ihyc); free(l->ihye); free(l->ihyv);
+        free(l->ihz); free(l->ihzc); free(l->ihze); free(l->ihzv);
+        free(l->nu); free(l->ro); free(l->ec); free(l->exy); free(l->exz); free(l->eyz);
+        for (c = 0; c < 4; c++) { free(l->x[c]); free(l->b[c]); free(l->r[c]); }
+        free(l->bcmask);
+    }
+    if (C->lu_ready) p2_band_free(&C->lu);
+    free(C);
+}
+
+/* dpar: p0koef p1koef v0koef v1koef nubeg nuend GX GY GZ ; viscmod */
+void p2o_set_params(void *h, const double *dpar, int viscmod, const int *npre, const int *npost)
+{
+    p2o_ctx *C = h;
+    int li;
+    C->p0koef = dpar[0]; C->p1koef = dpar[1]; C->v0koef = dpar[2]; C->v1koef = dpar[3];
+    C->nubeg = dpar[4]; C->nuend = dpar[5]; C->GX = dpar[6]; C->GY = dpar[7]; C->GZ = dpar[8];
+    C->viscmod = viscmod;
+    for (li = 0; li < C->nlev; li++) { C->npre[li] = npre[li]; C->npost[li] = npost[li]; }
+}
+
+/* Node fields (level 0) -> coarse nu/ro, stencil viscosities, level-0 rhs,
+ * coarsest factorisation.  Returns 0 or the LU status. */
+int p2o_set_fields(void *h, const float *nu, const float *ro, const float *nxx, const float *nxy,
+                   const float *nxz, const float *nyz)
+{
+    p2o_ctx *C = h;
+    p2o_level *l = &C->L[0];
+    int li, i, j, k;
+    memcpy(l->nu, nu, sizeof(float) * l->n);
+    memcpy(l->ro, ro, sizeof(float) * l->n);
+    for (li = 1; li < C->nlev; li++) ronurestrict_level(C, li);
+    level_viscosity(C, 0, nxx, nxy, nxz, nyz);
+    for (li = 1; li < C->nlev; li++) level_viscosity(C, li, NULL, NULL, NULL, NULL);
+    /* level-0 right-hand sides (xstokserr:845, ystokserr:1060, zstokserr:1279) */
+    for (k = 0; k < l->nz; k++)
+        for (i = 0; i < l->nx; i++)
+            for (j = 0; j < l->ny; j++) {
+                long u = IDX(l, i, j, k);
+                l->b[0][u] = 0;
+                l->b[1][u] = l->b[2][u] = l->b[3][u] = 0;
+                if (valid(l, 1, i, j, k) && i < l->nx - 1 && i > 0)
+                    l->b[1][u] = -C->GX * ((double)ro[u] + ro[IDX(l, i, j + 1, k)] + ro[IDX(l, i, j, k + 1)] + ro[IDX(l, i, j + 1, k + 1)]) / 4.0;
+                if (valid(l, 2, i, j, k) && j < l->ny - 1 && j > 0)
+                    l->b[2][u] = -C->GY * ((double)ro[u] + ro[IDX(l, i + 1, j, k)] + ro[IDX(l, i, j, k + 1)] + ro[IDX(l, i + 1, j, k + 1)]) / 4.0;
+                if (valid(l, 3, i, j, k) && k < l->nz - 1 && k > 0)
+                    l->b[3][u] = -C->GZ * ((double)ro[u] + ro[IDX(l, i, j + 1, k)] + ro[IDX(l, i + 1, j, k)] + ro[IDX(l, i + 1, j + 1, k)]) / 4.0;
+            }
+    for (k = 0; k < l->nz; k++)
+        for (i = 0; i < l->nx; i++)
+            for (j = 0; j < l->ny; j++) {
+                long u = IDX(l, i, j, k);
+                int c;
+                for (c = 0; c < 4; c++)
+                    if (is_bc(l, u, c)) l->b[c][u] = C->bondv1[2 * C->bondm[u * 4 + c]];
+            }
+    return coarse_factor(C);
+}
+
+/* Solve from the current x (zero after create) to rel residual tol.
+ * restart == 0: plain defect correction x += V(b - A x);
+ * restart >= 1: GCR(restart) with the V-cycle as preconditioner.
+ * Returns iterations used; hist[0..it] receives relative residuals. */
+static void vec_zero(double **v, long n) { int c; for (c = 0; c < 4; c++) memset(v[c], 0, sizeof(double) * n); }
+static double vec_dot(double **a, double **b, long n)
+{
+    double s = 0; long u; int c;
+    for (c = 0; c < 4; c++) for (u = 0; u < n; u++) s += a[c][u] * b[c][u];
+    return s;
+}
+static void vec_axpy(double **y, double a, double **x, long n)
+{
+    long u; int c;
+    for (c = 0; c < 4; c++) for (u = 0; u < n; u++) y[c][u] += a * x[c][u];
+}
+static void vec_copy(double **y, double **x, long n) { int c; for (c = 0; c < 4; c++) memcpy(y[c], x[c], sizeof(double) * n); }
+static void zero_pin_row(p2o_level *l, double **v) { if (l->pin >= 0) v[0][l->pin] = 0; }
+
+/* z = V(r): one V-cycle from zero for right-hand side r (level 0). */
+static void precond(p2o_ctx *C, double **r, double **z)
+{
+    p2o_level *l = &C->L[0];
+    double *sb[4], *sx[4];
+    int c;
+    for (c = 0; c < 4; c++) { sb[c] = l->b[c]; sx[c] = l->x[c]; l->b[c] = r[c]; l->x[c] = z[c]; }
+    vec_zero(l->x, l->n);
+    vcycle(C);
+    for (c = 0; c < 4; c++) { l->b[c] = sb[c]; l->x[c] = sx[c]; }
+}
+
+/* q = A z (level 0, BC rows x - koef x_t, pin cell as continuity). */
+static void apply_A(p2o_ctx *C, double **z, double **q)
+{
+    p2o_level *l = &C->L[0];
+    double *sb[4], *sx[4], *sr[4];
+    int c;
+    long u;
+    for (c = 0; c < 4; c++) { sb[c] = l->b[c]; sx[c] = l->x[c]; sr[c] = l->r[c]; l->b[c] = calloc(l->n, sizeof(double)); l->x[c] = z[c]; l->r[c] = q[c]; }
+    residual(C, 0);
+    for (c = 0; c < 4; c++) { for (u = 0; u < l->n; u++) q[c][u] = -q[c][u]; free(l->b[c]); l->b[c] = sb[c]; l->x[c] = sx[c]; l->r[c] = sr[c]; }
+}
+
+int p2o_zero_pin = 0;
+int p2o_solve(void *h, double tol, int maxit, int restart, double *hist)
+{
+    p2o_ctx *C = h;
+    p2o_level *l = &C->L[0];
+    long n = l->n;
+    int it = 0, c, m = restart > 0 ? restart : 1, k, j;
+    double rel, **Z, **Q, *r[4], *qq = calloc(m, sizeof(double));
+    Z = calloc((size_t)m * 4, sizeof(double *));
+    Q = calloc((size_t)m * 4, sizeof(double *));
+    for (k = 0; k < m * 4; k++) { Z[k] = calloc(n, sizeof(double)); Q[k] = calloc(n, sizeof(double)); }
+    for (c = 0; c < 4; c++) r[c] = calloc(n, sizeof(double));
+    rel = rel_residual(C, NULL, NULL);
+    if (hist) hist[0] = rel;
+    k = 0;
+    while (rel > tol && it < maxit) {
+        double **z = &Z[k * 4], **q = &Q[k * 4], alpha;
+        residual(C, 0);
+        vec_copy(r, l->r, n);
+        if (p2o_zero_pin) zero_pin_row(l, r);
+        precond(C, r, z);
+        if (restart == 0) {
+            vec_axpy(l->x, 1.0, z, n);
+        } else {
+            apply_A(C, z, q);
+            if (p2o_zero_pin) zero_pin_row(l, q);
+            for (j = 0; j < k; j++) {
+                double beta = vec_dot(q, &Q[j * 4], n) / qq[j];
+                vec_axpy(q, -beta, &Q[j * 4], n);
+                vec_axpy(z, -beta, &Z[j * 4], n);
+            }
+            qq[k] = vec_dot(q, q, n);
+            alpha = vec_dot(r, q, n) / qq[k];
+            vec_axpy(l->x, alpha, z, n);
+            k = (k + 1) % m;
+        }
+        rel = rel_residual(C, NULL, NULL);
+        it++;
+        if (hist) hist[it] = rel;
+        if (!(rel == rel)) break;
+    }
+    normalize_pressure(C, 0);
+    for (k = 0; k < m * 4; k++) { free(Z[k]); free(Q[k]); }
+    free(Z); free(Q); free(qq);
+    for (c = 0; c < 4; c++) free(r[c]);
+    return it;
+}
+
+/* Level-0 solution in the node layout (entries that are not unknowns are 0). */
+void p2o_get_solution(void *h, double *pr, double *vx, double *vy, double *vz)
+{
+    p2o_ctx *C = h;
+    p2o_level *l = &C->L[0];
+    int i, j, k;
+    for (k = 0; k < l->nz; k++)
+        for (i = 0; i < l->nx; i++)
+            for (j = 0; j < l->ny; j++) {
+                long u = IDX(l, i, j, k);
+                pr[u] = valid(l, 0, i, j, k) ? l->x[0][u] : 0;
+                vx[u] = valid(l, 1, i, j, k) ? l->x[1][u] : 0;
+                vy[u] = valid(l, 2, i, j, k) ? l->x[2][u] : 0;
+                vz[u] = valid(l, 3, i, j, k) ? l->x[3][u] : 0;
+            }
+}
+
+void p2o_set_solution(void *h, const double *pr, const double *vx, const double *vy, const double *vz)
+{
+    p2o_ctx *C = h;
+    p2o_level *l = &C->L[0];
+    memcpy(l->x[0], pr, sizeof(double) * l->n);
+    memcpy(l->x[1], vx, sizeof(double) * l->n);
+    memcpy(l->x[2], vy, sizeof(double) * l->n);
+    memcpy(l->x[3], vz, sizeof(double) * l->n);
+}
+
+/* A x for an arbitrary level-li vector in the interleaved [P,Vx,Vy,Vz] layout
+ * (BC rows: x - koef x_t; ghosts: x) — compared against the reference's row store. */
+void p2o_apply(void *h, int li, const double *xin, double *yout)
+{
+    p2o_ctx *C = h;
+    p2o_level *l = &C->L[li];
+    double *save[4];
+    int c, i, j, k;
+    for (c = 0; c < 4; c++) {
+        long u;
+        save[c] = l->x[c];
+        l->x[c] = malloc(sizeof(double) * l->n);
+        for (u = 0; u < l->n; u++) l->x[c][u] = xin[u * 4 + c];
+    }
+    for (k = 0; k < l->nz; k++)
+        for (i = 0; i < l->nx; i++)
+            for (j = 0; j < l->ny; j++) {
+                long u = IDX(l, i, j, k);
+                for (c = 0; c < 4; c++) {
+                    double a;
+                    if (!valid(l, c, i, j, k)) { a = l->x[c][u]; }
+                    else if (l->bcmask[u] & (1 << c)) {
+                        double cst, koef; long tn; int tc;
+                        bc_of(C, li, u, c, &cst, &koef, &tn, &tc);
+                        a = l->x[c][u] - (tn >= 0 ? koef * l->x[tc][tn] : 0.0);
+                    } else if (c == 0) a = row_p(l, i, j, k);
+                    else if (c == 1) a = row_vx(l, i, j, k, NULL);
+                    else if (c == 2) a = row_vy(l, i, j, k, NULL);
+                    else a = row_vz(l, i, j, k, NULL);
+                    yout[u * 4 + c] = a;
+                }
+            }
+    for (c = 0; c < 4; c++) { free(l->x[c]); l->x[c] = save[c]; }
+}
+
+void p2o_rhs(void *h, double *b)
+{
+    p2o_ctx *C = h;
+    p2o_level *l = &C->L[0];
+    long u;
+    int c;
+    for (u = 0; u < l->n; u++)
+        for (c = 0; c < 4; c++) {
+            int i = (int)((u / l->ny) % l->nx), j = (int)(u % l->ny), k = (int)(u / ((long)l->nx * l->ny));
+            if (!valid(l, c, i, j, k)) b[u * 4 + c] = 0;
+            else if ((l->bcmask[u] & (1 << c)) && !is_bc(l, u, c)) b[u * 4 + c] = l->pinval;
+            else b[u * 4 + c] = l->b[c][u];
+        }
+}
+
+void p2o_level_fields(void *h, int li, float *nu, float *ro, double *ec)
+{
+    p2o_ctx *C = h;
+    p2o_level *l = &C->L[li];
+    memcpy(nu, l->nu, sizeof(float) * l->n);
+    memcpy(ro, l->ro, sizeof(float) * l->n);
+    memcpy(ec, l->ec, sizeof(double) * l->n);
+}
+
+double p2o_rel_residual(void *h)
+{
+    return rel_residual((p2o_ctx *)h, NULL, NULL);
+}
+
+/* ---------------------------------------------------------------------- */
+/* Marker -> node interpolation (ronurecalc, mark3mg.c:630-1133), single   */
+/* thread, with the reference's float accumulators and double weights.     */
+static long serch(const double *g, long n, double x)
+{
+    long m, a = 0, b = n - 1;
+    do {
+        m = (a + b) / 2;
+        if (g[m] > x) b = m; else a = m;
+    } while (b - a > 1);
+    if (a > n - 2) a = n - 2;
+    return a;
+}
+
+/* In/out: nu, ro, nxx, nxy, nxz, nyz (float[nodenum]); nodes without
+ * markers keep their input value (then clamped), as in the reference. */
+void p2o_ronurecalc(int nx, int ny, int nz, const double *gx, const double *gy, const double *gz,
+                    long nmark, const float *mx, const float *my, const float *mz, const signed char *mt,
+                    const double *markn0, const double *markro, double nubeg, double nuend, double nukoef,
+                    int viscmod, float *nu, float *ro, float *nxx, float *nxy, float *nxz, float *nyz)
+{
+    long nn = (long)nx * ny * nz, mm, v;
+    double xsize = gx[nx - 1], ysize = gy[ny - 1], zsize = gz[nz - 1];
+    long xy = (long)nx * ny;
+    float *A[6];
+    double *W[6];
+    int q;
+    for (q = 0; q < 6; q++) { A[q] = calloc(nn, sizeof(float)); W[q] = calloc(nn, sizeof(double)); }
+    /* A/W order: 0 ro, 1 nu, 2 nxx, 3 nxy, 4 nxz, 5 nyz */
+    for (mm = 0; mm < nmark; mm++) {
+        double mnu, mro, dx, dy, dz;
+        long m10, m20, m30, m1, m2, m3;
+        int t = mt[mm];
+        if (!(mx[mm] > 0 && my[mm] > 0 && mz[mm] > 0 && mx[mm] < xsize && my[mm] < ysize && mz[mm] < zsize && t < 50)) continue;
+        mnu = markn0[t];
+        mro = markro[t];
+        if (mnu < nubeg) mnu = nubeg;
+        if (mnu > nuend) mnu = nuend;
+        m10 = serch(gx, nx, (double)mx[mm]);
+        m20 = serch(gy, ny, (double)my[mm]);
+        m30 = serch(gz, nz, (double)mz[mm]);
+        dx = gx[m10 + 1] - gx[m10];
+        dy = gy[m20 + 1] - gy[m20];
+        dz = gz[m30 + 1] - gz[m30];
+        for (m3 = m30; m3 <= m30 + 1; m3++) {
+            double ddz = 1.0 - fabs((gz[m3] - mz[mm]) / dz);
+            for (m1 = m10; m1 <= m10 + 1; m1++) {
+                double ddx = 1.0 - fabs((gx[m1] - mx[mm]) / dx);
+                for (m2 = m20; m2 <= m20 + 1; m2++) {
+                    double ddy = 1.0 - fabs((gy[m2] - my[mm]) / dy);
+                    double swt = ddx * ddy * ddz, f, s1;
+                    long m4 = m3 * xy + m1 * ny + m2;
+                    f = viscmod == 0 ? mnu : viscmod == 1 ? log(mnu) : 1.0 / mnu;
+                    if (ddx > nukoef && ddy > nukoef && ddz > nukoef) { A[1][m4] += f * swt; W[1][m4] += swt; }
+                    if (m1 > m10 && m2 > m20 && m3 > m30) {
+                        s1 = 8.0 * (0.5 - fabs(ddx - 0.5)) * (0.5 - fabs(ddy - 0.5)) * (0.5 - fabs(ddz - 0.5));
+                        A[2][m4] += f * s1; W[2][m4] += s1;
+                    }
+                    if (m3 == m30 && ddx > 0.5 && ddy > 0.5) {
+                        s1 = 8.0 * (ddx - 0.5) * (ddy - 0.5) * (0.5 - fabs(ddz - 0.5));
+                        A[3][m4] += f * s1; W[3][m4] += s1;
+                    }
+                    if (m2 == m20 && ddx > 0.5 && ddz > 0.5) {
+                        s1 = 8.0 * (ddx - 0.5) * (0.5 - fabs(ddy - 0.5)) * (ddz - 0.5);
+                        A[4][m4] += f * s1; W[4][m4] += s1;
+                    }
+                    if (m1 == m10 && ddy > 0.5 && ddz > 0.5) {
+                        s1 = 8.0 * (0.5 - fabs(ddx - 0.5)) * (ddy - 0.5) * (ddz - 0.5);
+                        A[5][m4] += f * s1; W[5][m4] += s1;
+                    }
+                    if (ddx > 0.5 && ddy > 0.5 && ddz > 0.5) {
+                        s1 = 8.0 * (ddx - 0.5) * (ddy - 0.5) * (ddz - 0.5);
+                        A[0][m4] += mro * s1; W[0][m4] += s1;
+                    }
+                }
+            }
+        }
+    }
+    for (v = 0; v < nn; v++) {
+        float *out[6];
+        out[0] = ro; out[1] = nu; out[2] = nxx; out[3] = nxy; out[4] = nxz; out[5] = nyz;
+        for (q = 0; q < 6; q++) {
+            if (W[q][v] > 0) {
+                /* the reference sums per-thread float buffers into a float array first */
+                float s = 0.0f;
+                s += A[q][v];
+                if (q == 0) out[q][v] = (float)(s / W[q][v]);
+                else {
+                    out[q][v] = (float)(s / W[q][v]);
+                    if (viscmod == 1) out[q][v] = (float)exp(out[q][v]);
+                    if (viscmod == 2) out[q][v] = (float)(1.0 / out[q][v]);
+                }
+            }
+            if (q > 0) {
+                if (out[q][v] < nubeg) out[q][v] = (float)nubeg;
+                if (out[q][v] > nuend) out[q][v] = (float)nuend;
+            }
+        }
+    }
+    for (q = 0; q < 6; q++) { free(A[q]); free(W[q]); }
+}
+
+/* Debug/test helpers: sweeps of the level-0 smoother only; two-grid count. */
+double p2o_smooth_only(void *h, int sweeps)
+{
+    p2o_ctx *C = h;
+    smooth(C, 0, sweeps);
+    return rel_residual(C, NULL, NULL);
+}

@@ -1,0 +1,189 @@
+"""ctypes driver for oracle/_ref/libp2ref.so, the reference's own C sources
+compiled by oracle/Makefile (TEST INFRASTRUCTURE ONLY: tests, smoke() and
+bench.py's CPU-baseline leg use it as the checker; the product never does).
+
+Each instance owns the reference's global state, so only one model can be
+live per process (the reference keeps everything in globals, head3mg.c).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_ref", "libp2ref.so")
+
+_dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_fp = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
+_ip = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+_bp = np.ctypeslib.ndpointer(dtype=np.int8, flags="C_CONTIGUOUS")
+
+_lib: Optional[C.CDLL] = None
+_live = False
+
+
+def available() -> bool:
+    return os.path.exists(LIB_PATH)
+
+
+def _load() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        lib = C.CDLL(LIB_PATH)
+        lib.p2ref_init.argtypes = [C.c_long, C.c_long, C.c_long, _dp, _dp, _dp, C.c_int, C.c_long]
+        lib.p2ref_init.restype = C.c_int
+        lib.p2ref_levels.argtypes = [_ip] * 5
+        lib.p2ref_level_coords.argtypes = [C.c_int, _dp, _dp, _dp]
+        lib.p2ref_set_params.argtypes = [_dp, _ip, _ip, _ip]
+        lib.p2ref_set_bc.argtypes = [_ip, C.c_long, _fp, _ip]
+        lib.p2ref_set_bc.restype = C.c_int
+        lib.p2ref_set_rocks.argtypes = [C.c_int, _dp, _dp, _dp]
+        lib.p2ref_set_markers.argtypes = [_fp, _fp, _fp, _bp]
+        lib.p2ref_set_nodes.argtypes = [_fp] * 6
+        lib.p2ref_get_nodes.argtypes = [_fp] * 6
+        lib.p2ref_get_level_fields.argtypes = [_fp] * 3
+        lib.p2ref_ronurecalc.restype = C.c_double
+        lib.p2ref_true_residual.argtypes = [C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        lib.p2ref_true_residual.restype = C.c_double
+        lib.p2ref_vpiterate_first.restype = C.c_double
+        lib.p2ref_vcycle.argtypes = [C.c_int]
+        lib.p2ref_get_solution.argtypes = [_dp] * 4
+        lib.p2ref_get_written.argtypes = [_dp, _fp, _fp, _fp]
+        lib.p2ref_get_vectors.argtypes = [_dp, _dp, _dp]
+        lib.p2ref_set_sol0.argtypes = [_dp]
+        lib.p2ref_rows_nnz.argtypes = [C.c_int]
+        lib.p2ref_rows_nnz.restype = C.c_long
+        lib.p2ref_get_rows.argtypes = [C.c_int, _ip, _ip, _dp, _dp]
+        lib.p2ref_rows_apply.argtypes = [C.c_int, _dp, _dp]
+        lib.p2ref_restrict.argtypes = [C.c_int, _dp, _dp]
+        lib.p2ref_prolong.argtypes = [C.c_int, _dp, _dp]
+        lib.p2ref_set_quiet.argtypes = [C.c_int]
+        lib.p2ref_lu_count.restype = C.c_int
+        lib.p2ref_num_threads.restype = C.c_int
+        _lib = lib
+    return _lib
+
+
+class RefModel:
+    """The reference's global state set up for one Model (pardiso2_b200.model)."""
+
+    def __init__(self, model, npre=None, npost=None):
+        global _live
+        if _live:
+            raise RuntimeError("the reference keeps its state in globals: one RefModel per process")
+        lib = _load()
+        self.lib = lib
+        self.m = model
+        nx, ny, nz = model.shape
+        nlev = lib.p2ref_init(nx, ny, nz, model.gx, model.gy, model.gz, model.multinum, model.markx.size)
+        if nlev != model.multinum:
+            raise RuntimeError("reference init failed")
+        _live = True
+        L = nlev + 1
+        self.mgx = np.zeros(L, np.int32)
+        self.mgy = np.zeros(L, np.int32)
+        self.mgz = np.zeros(L, np.int32)
+        self.mgp = np.zeros(L, np.int32)
+        self.mgn = np.zeros(L, np.int32)
+        lib.p2ref_levels(self.mgx, self.mgy, self.mgz, self.mgp, self.mgn)
+        p = model.params
+        dpar = np.array([p.p0koef, p.p1koef, p.p2koef, p.v0koef, p.v1koef, p.nubeg, p.nuend, p.nukoef,
+                         p.gx, p.gy, p.gz, p.pinit], dtype=np.float64)
+        ipar = np.array([p.viscmod, p.pin[0], p.pin[1], p.pin[2], 1], dtype=np.int32)
+        npre = np.array(npre if npre is not None else [2] * L, dtype=np.int32)
+        npost = np.array(npost if npost is not None else [2] * L, dtype=np.int32)
+        lib.p2ref_set_params(dpar, ipar, npre, npost)
+        bc = model.bc
+        if lib.p2ref_set_bc(np.ascontiguousarray(bc.bondm, np.int32), bc.bondnum,
+                            np.ascontiguousarray(bc.bondv1.reshape(-1), np.float32),
+                            np.ascontiguousarray(bc.bondn1, np.int32)):
+            raise RuntimeError("too many boundary equations for the reference (MAXBON)")
+        r = model.rocks
+        lib.p2ref_set_rocks(len(r.n0), np.ascontiguousarray(r.n0, np.float64),
+                            np.ascontiguousarray(r.n1, np.float64), np.ascontiguousarray(r.ro, np.float64))
+        if model.markx.size:
+            lib.p2ref_set_markers(model.markx, model.marky, model.markz, np.ascontiguousarray(model.markt, np.int8))
+
+    # -- marker -> node ----------------------------------------------------
+    def ronurecalc(self) -> float:
+        return self.lib.p2ref_ronurecalc()
+
+    def nodes(self):
+        n = self.m.nodenum
+        out = [np.zeros(n, np.float32) for _ in range(6)]
+        self.lib.p2ref_get_nodes(*out)
+        return dict(zip(("nu", "ro", "nxx", "nxy", "nxz", "nyz"), out))
+
+    def set_nodes(self, f):
+        self.lib.p2ref_set_nodes(*[np.ascontiguousarray(f[k], np.float32)
+                                   for k in ("nu", "ro", "nxx", "nxy", "nxz", "nyz")])
+
+    def level_fields(self):
+        n = int(self.mgp[-1] + self.mgn[-1])
+        out = [np.zeros(n, np.float32) for _ in range(3)]
+        self.lib.p2ref_get_level_fields(*out)
+        return dict(zip(("nu", "ro", "nd"), out))
+
+    # -- solve -------------------------------------------------------------
+    def residual(self):
+        rn, bn = C.c_double(), C.c_double()
+        rel = self.lib.p2ref_true_residual(C.byref(rn), C.byref(bn))
+        return rel, rn.value, bn.value
+
+    def first_iteration(self) -> float:
+        return self.lib.p2ref_vpiterate_first()
+
+    def vcycle(self, coarse: bool = True):
+        self.lib.p2ref_vcycle(1 if coarse else 0)
+
+    def solve(self, tol=1e-8, max_cycles=200, coarse=True, verbose=False):
+        hist = []
+        self.first_iteration()
+        rel = self.residual()[0]
+        hist.append(rel)
+        it = 0
+        while rel > tol and it < max_cycles:
+            self.vcycle(coarse)
+            rel = self.residual()[0]
+            hist.append(rel)
+            it += 1
+            if verbose:
+                print("ref cycle %d rel %.3e" % (it, rel))
+        return hist
+
+    def solution(self):
+        n = self.m.nodenum
+        out = [np.zeros(n, np.float64) for _ in range(4)]
+        self.lib.p2ref_get_solution(*out)
+        return dict(zip(("pr", "vx", "vy", "vz"), out))
+
+    def rows(self, lev=0):
+        nnz = self.lib.p2ref_rows_nnz(lev)
+        row = np.zeros(nnz, np.int32)
+        col = np.zeros(nnz, np.int32)
+        val = np.zeros(nnz, np.float64)
+        rhs = np.zeros(int(self.mgn[lev]) * 4, np.float64)
+        self.lib.p2ref_get_rows(lev, row, col, val, rhs)
+        return row, col, val, rhs
+
+    def vectors(self):
+        n = int(self.mgp[-1] + self.mgn[-1]) * 4
+        s0, f1, f0 = (np.zeros(n, np.float64) for _ in range(3))
+        self.lib.p2ref_get_vectors(s0, f1, f0)
+        return s0, f1, f0
+
+    def restrict(self, lev_coarse, fine_res):
+        out = np.zeros(int(self.mgn[lev_coarse]) * 4, np.float64)
+        self.lib.p2ref_restrict(lev_coarse, np.ascontiguousarray(fine_res, np.float64), out)
+        return out
+
+    def prolong(self, lev_coarse, coarse_x, fine_x):
+        f = np.ascontiguousarray(fine_x, np.float64).copy()
+        self.lib.p2ref_prolong(lev_coarse, np.ascontiguousarray(coarse_x, np.float64), f)
+        return f
+
+    def num_threads(self):
+        return self.lib.p2ref_num_threads()
