@@ -1,0 +1,348 @@
+"""Benchmark: ms per Stokes solve to relative residual 1e-8 on one B200.
+
+Workload (default): spheres65 — 65^3 nodes, 4 levels (65-35-20-12), 8 random
+spheres with viscosity log-uniform in [1e-3, 1e3] (contrast 1e6), density
+contrast U[-1, 1], 2x2x2 markers per cell, free-slip box, seed 2.  Inputs are
+seeded synthetic data of those shapes (no public dataset exists).
+
+One step = one complete Stokes solve (coarse viscosities, coarsest LU and
+inverse, FP64 outer iterations with FP32 V-cycles) from a zero initial guess
+on node fields resident in HBM, to ||b - Ax|| / ||b|| <= 1e-8 in FP64.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+Under torchrun (N > 1) every rank solves its own replica (the solve does not
+shard); the timed region is bracketed by a barrier and the max over ranks is
+reported.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "ms per Stokes solve to rel.residual 1e-8 (mixed vs FP64, 1 B200); HBM GB/s"
+WORKLOAD = ("spheres65: 65^3 nodes, 4 levels, 8 spheres viscosity 1e-3..1e3 (contrast 1e6), "
+            "2x2x2 markers/cell, free-slip box, seed 2")
+CONFIG_IDX = 2
+# Algorithmic bytes of one FP32 colour pass of the cell-block smoother per
+# node: read 3 velocity fields (12 B), pressure (4 B), 4 right-hand sides
+# (16 B) and 4 viscosity fields (16 B); write 3 velocity fields (12 B) and
+# half of the pressures (2 B).
+SMOOTHER_BYTES_PER_NODE = 62
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", type=int, default=CONFIG_IDX)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--solve-only", action="store_true",
+                    help="warm-up + timed resident solves + smoother timing only (profiling runs)")
+    ap.add_argument("--restart", type=int, default=16, help="GCR restart length")
+    return ap.parse_args()
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profile_traffic():
+    """Per-launch DRAM bytes of the level-0 FP32 smoother pass from the
+    committed ncu summary (None until one is captured)."""
+    p = os.path.join(ROOT, "profiles", "ncu_vanka_f32_level0_spheres65.txt")
+    if not os.path.exists(p):
+        return None
+    m = re.search(r"dram_bytes_per_launch:\s*([0-9.eE+]+)", open(p).read())
+    return float(m.group(1)) if m else None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.th = threading.Thread(target=self._read, daemon=True)
+            self.th.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup(gpus):
+    rank, world = 0, 1
+    if gpus > 1 or "WORLD_SIZE" in os.environ:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        rank = int(os.environ.get("RANK", 0))
+        world = int(os.environ.get("WORLD_SIZE", 1))
+        local = int(os.environ.get("LOCAL_RANK", rank))
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        return rank, world, local, dist
+    return rank, world, 0, None
+
+
+def cpu_solve_ms(model, threads: int, steps: int = 1):
+    """The oracle port (same algorithm, FP64, OpenMP) on the host cores."""
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    from oracle import oracle as O
+    if not O.available():
+        subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "all"], check=True, stdout=subprocess.DEVNULL)
+    times, its = [], []
+    f = O.ronurecalc(model)
+    for _ in range(steps):
+        s = O.OracleSolver(model, npre=[4] * (model.multinum + 1), npost=[4] * (model.multinum + 1))
+        t0 = time.perf_counter()
+        s.set_fields(f)
+        h = s.solve(tol=1e-8, max_cycles=200, restart=16)
+        times.append((time.perf_counter() - t0) * 1e3)
+        its.append(len(h) - 1)
+        s.close()
+    return times, its
+
+
+def reference_own_solver(model, cycles: int = 6):
+    """Bounded run of the reference's own vpiterate() path (oracle/_ref):
+    first iteration (assembly + direct coarsest solve) and further V-cycles,
+    reporting ms per cycle and the true residual reached."""
+    from oracle import refdrv
+    if not refdrv.available():
+        return None
+    r = refdrv.RefModel(model, npre=[4] * (model.multinum + 1), npost=[4] * (model.multinum + 1))
+    t0 = time.perf_counter()
+    r.ronurecalc()
+    t1 = time.perf_counter()
+    r.first_iteration()
+    t2 = time.perf_counter()
+    res = [r.residual()[0]]
+    for _ in range(cycles):
+        r.vcycle(False)
+        res.append(r.residual()[0])
+    t3 = time.perf_counter()
+    return {"threads": r.num_threads(), "ronurecalc_ms": (t1 - t0) * 1e3, "first_iteration_ms": (t2 - t1) * 1e3,
+            "ms_per_vcycle": (t3 - t2) * 1e3 / cycles, "true_rel_residual": res}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", 0))
+    if rank != 0:
+        return
+    from pardiso2_b200 import model as M
+    m = M.config_model(args.config)
+    threads = os.cpu_count() or 1
+    n = args.warmup + args.steps
+    times, its = cpu_solve_ms(m, threads, steps=max(1, n))
+    timed = times[args.warmup:] or times
+    v = statistics.mean(timed)
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "ms", "n_gpus": args.gpus,
+            "steps": len(timed), "warmup": args.warmup, "ms_per_step": v, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "unknowns": m.real_dofs(), "iterations": its[-1]},
+            "cpu_baseline": {"value": v, "unit": "ms", "cores": threads, "kind": "port",
+                             "sample": "full solve of the workload to 1e-8 per step (oracle port: same discretisation"
+                                       " and algorithm in C + OpenMP)"},
+            "e2e": {"value": v, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    try:
+        line["reference_own_solver"] = reference_own_solver(m)
+    except Exception as e:  # the reference's own MG is bounded here, never required
+        line["reference_own_solver"] = {"error": str(e)}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    rank, world, local, dist = dist_setup(args.gpus)
+    import numpy as np
+    import torch
+    import pardiso2_b200 as P
+    from pardiso2_b200 import capi
+    from pardiso2_b200 import model as M
+
+    torch.cuda.set_device(local)
+    m = M.config_model(args.config)
+    n = m.nodenum
+    prob = P.StokesProblem(m, device=local, precision=0, tol=1e-8, restart=args.restart)
+    ronu_ms = [prob.ctx.upload_markers(m.markx, m.marky, m.markz, m.markt, m.rocks.n0, m.rocks.n1, m.rocks.ro)
+               or prob.ctx.ronurecalc_resident() for _ in range(3)]
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def one(p):
+        flush.fill_(1.0)
+        torch.cuda.synchronize()
+        info = p.ctx.solve_resident()
+        return info
+
+    for _ in range(args.warmup):
+        one(prob)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clk = ClockSampler(local)
+    clk.start()
+    infos = [one(prob) for _ in range(args.steps)]
+    torch.cuda.synchronize()
+    clocks = clk.stop()
+    if dist:
+        dist.barrier()
+    dev_ms = sum(i.ms_total for i in infos)
+    launches = sum(i.kernels for i in infos)
+    if dist:
+        t = torch.tensor([dev_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dev_ms = float(t.item())
+    ms_per_step = dev_ms / args.steps
+    value = dev_ms / (args.steps * world)   # ms per solve for the whole job
+
+    # the dominant kernel: level-0 FP32 colour pass of the cell-block smoother
+    H = capi.DebugHooks(prob.ctx)
+    pass_ms = H.time_smoother(0, 40)
+    bytes_per_launch = SMOOTHER_BYTES_PER_NODE * n
+    achieved = bytes_per_launch / (pass_ms * 1e-3) / 1e9
+    peak, peak_kind = measured_peaks()
+    traffic = profile_traffic()
+    if args.solve_only:
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": value, "unit": "ms", "solve_only": True,
+                              "iterations": infos[-1].iterations, "gpu_launches": launches,
+                              "smoother_ms_per_pass": pass_ms, "smoother_GBps": achieved}), flush=True)
+        prob.close()
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+
+    # FP64 V-cycle for comparison
+    p64 = P.StokesProblem(m, device=local, precision=1, tol=1e-8)
+    p64.ctx.upload_markers(m.markx, m.marky, m.markz, m.markt, m.rocks.n0, m.rocks.n1, m.rocks.ro)
+    p64.ctx.ronurecalc_resident()
+    for _ in range(max(1, args.warmup)):
+        one(p64)
+    i64 = [one(p64) for _ in range(args.steps)]
+    fp64_ms = sum(i.ms_total for i in i64) / args.steps
+    p64.close()
+
+    # end to end through the public C ABI with pinned host buffers
+    keys = ("nu", "ro", "nxx", "nxy", "nxz", "nyz")
+    host_nodes = prob.ctx.get_nodes(n)
+    pinned = {k: torch.empty(n, dtype=torch.float32, pin_memory=True).numpy() for k in keys}
+    for k in keys:
+        pinned[k][:] = host_nodes[k]
+    vx = torch.zeros(n, dtype=torch.float32, pin_memory=True).numpy()
+    vy = torch.zeros(n, dtype=torch.float32, pin_memory=True).numpy()
+    vz = torch.zeros(n, dtype=torch.float32, pin_memory=True).numpy()
+    pr = torch.zeros(n, dtype=torch.float64, pin_memory=True).numpy()
+    e2e = []
+    for it in range(args.warmup + args.steps):
+        vx[:] = 0; vy[:] = 0; vz[:] = 0; pr[:] = 0
+        flush.fill_(1.0)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        prob.ctx.set_nodes(pinned)
+        info = prob.ctx.stokes_solve(vx, vy, vz, pr)
+        t1 = time.perf_counter()
+        if it >= args.warmup:
+            e2e.append((t1 - t0) * 1e3)
+    e2e_ms = statistics.mean(e2e)
+    if dist:
+        t = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item()) / world
+    last = infos[-1]
+    line = {
+        "metric": METRIC, "value": value, "unit": "ms", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 V-cycle / f64 outer", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "unknowns": m.real_dofs(), "levels": m.multinum + 1,
+                   "sweeps": "4 pre + 4 post cell-block", "outer": "GCR(16) in FP64",
+                   "l2": "flushed (256 MB write) before every step", "parallelism": "replicas" if world > 1 else "1 GPU"},
+        "iterations": last.iterations, "rel_residual": last.rel_residual,
+        "fp64_ms_per_solve": fp64_ms, "iterations_fp64": i64[-1].iterations,
+        "speedup_mixed_vs_fp64": fp64_ms / ms_per_step,
+        "setup_ms": last.ms_setup, "vcycles_ms": last.ms_vcycles,
+        "ronurecalc_ms": statistics.mean(ronu_ms[1:]),
+        "unknowns_per_s": m.real_dofs() * world / (ms_per_step * 1e-3),
+        "gpu_launches": launches,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic, "kernel": "k_vanka<float> level-0 colour pass",
+                     "bytes_per_launch": bytes_per_launch, "ms_per_launch": pass_ms,
+                     "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs, burst)"},
+        "clocks": clocks,
+        "e2e": {"value": e2e_ms, "unit": "ms", "h2d_bytes_per_step": 24 * n + 32 * n, "d2h_bytes_per_step": 32 * n},
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        times, its = cpu_solve_ms(m, threads, steps=1)
+        line["cpu_baseline"] = {"value": times[0], "unit": "ms", "cores": threads, "kind": "port",
+                                "sample": "one full solve of the workload to 1e-8 (oracle port, %d iterations)" % its[0]}
+    prob.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

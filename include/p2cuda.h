@@ -1,0 +1,156 @@
+/*
+ * p2cuda — B200 (sm_100a) Stokes multigrid behind the Pardiso2 entry points.
+ *
+ * Plain C ABI: host pointers, sizes and a status code; no CUDA or torch
+ * types cross this boundary.  Every array uses the reference's own layout:
+ * node index n = m3*ynumy*xnumx + m1*ynumy + m2 (y fastest, then x, then z),
+ * velocities vx/vy/vz as float, pressure pr as double, node fields
+ * nu/ro/nxx/nxy/nxz/nyz as float, boundary tables bondm/bondv1/bondn1 as in
+ * the reference's head3mg.c.
+ *
+ * Which reference interface each entry point replaces (paths relative to the
+ * reference project):
+ *   p2_set_grid        gridcheck() level tables, pardiso/load3mg.c:2011-2195
+ *   p2_set_bc          bondm/bondv1/bondn1 tables, pardiso/head3mg.c:110-112
+ *                      (filled by pardiso/in3mg.c:304-388)
+ *   p2_set_nodes       the node fields vpiterate() reads, head3mg.c:95-96
+ *   p2_stokes_solve    void vpiterate(int m0, int f0), pardiso/move3mgNew.c:1791
+ *                      (prototype pardiso/head3mg.c:362); the coarsest
+ *                      pardisomat() PARDISO solve, pardiso/gaus3mg_SerieMG.c:64
+ *   p2_ronurecalc      void ronurecalc(void), pardiso/mark3mg.c:630
+ *                      (prototype pardiso/head3mg.c:417)
+ * A C shim with the reference's own signatures on top of these calls is in
+ * pardiso2_b200/csrc/move3mg_cuda.c.
+ */
+#ifndef P2CUDA_H
+#define P2CUDA_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct p2_ctx p2_ctx;
+
+typedef enum {
+    P2_OK = 0,
+    P2_ERR_ARG = 1,            /* bad argument or inconsistent sizes */
+    P2_ERR_CUDA = 2,           /* a CUDA runtime call failed */
+    P2_ERR_NOMEM = 3,          /* device allocation failed */
+    P2_ERR_NOT_CONVERGED = 4,  /* iteration cap reached above the tolerance */
+    P2_ERR_NAN = 5,            /* NaN/Inf in the residual */
+    P2_ERR_SINGULAR = 6,       /* zero pivot in the coarsest LU */
+    P2_ERR_STATE = 7,          /* call out of order (e.g. solve before set_grid) */
+    P2_ERR_UNSUPPORTED = 8     /* periodic boundaries, p2koef != 0, open boundary rows */
+} p2_status;
+
+#define P2_MAX_LEVELS 12
+
+/* The mode.t3c knobs vpiterate() reads (pardiso/mode.t3c:77-97) plus the
+ * solver controls of this library. */
+typedef struct {
+    double p0koef, p1koef, p2koef, v0koef, v1koef; /* smoother / transfer scaling */
+    double nubeg, nuend;                           /* viscosity clamp */
+    double nukoef;                                 /* marker weight threshold (ronurecalc) */
+    double gxkoef, gykoef, gzkoef;                 /* gravity components */
+    double pinit;                                  /* pressure value in the pinned cell */
+    int pxinit, pyinit, pzinit;                    /* pinned pressure cell */
+    int viscmod;                                   /* 0 arithmetic, 1 geometric, 2 harmonic */
+    int multinum;                                  /* coarse levels (levels = multinum + 1) */
+    int npre[P2_MAX_LEVELS];                       /* multinnn[0][level] */
+    int npost[P2_MAX_LEVELS];                      /* multinnn[1][level] */
+    /* library controls */
+    double tol;          /* relative residual target ||b-Ax||/||b|| (default 1e-8) */
+    int max_iter;        /* outer iteration cap (default 200) */
+    int precision;       /* 0: FP32 V-cycle in an FP64 outer loop; 1: FP64 V-cycle */
+    int restart;         /* GCR restart length (default 16, at most 18) */
+    double omega;        /* cell-block smoother damping (default 0.7) */
+    int use_graphs;      /* capture the V-cycle in a CUDA graph (default 1) */
+} p2_params;
+
+typedef struct {
+    int iterations;          /* outer (GCR) iterations */
+    double rel_residual;     /* final ||b-Ax||/||b|| of the level-0 system, FP64 */
+    double rel_residual0;    /* initial */
+    double ms_total;         /* device time of the whole solve (CUDA events) */
+    double ms_setup;         /* coarse viscosity, coarsest LU and inverse */
+    double ms_vcycles;       /* preconditioner V-cycles */
+    int status;
+    long long kernels;       /* kernels this library launched during the solve */
+} p2_solve_info;
+
+/* Fill p with the reference's defaults (mode.t3c) and this library's. */
+void p2_default_params(p2_params *p);
+
+p2_status p2_create(p2_ctx **ctx, int device);
+void p2_destroy(p2_ctx *ctx);
+/* Human-readable text of the last error on this context (never NULL). */
+const char *p2_last_error(const p2_ctx *ctx);
+
+/* Grid: node counts and gridlines; builds the multigrid levels exactly as
+ * gridcheck() does.  Periodic flags must be 0 (P2_ERR_UNSUPPORTED otherwise). */
+p2_status p2_set_grid(p2_ctx *ctx, long xnumx, long ynumy, long znumz, const double *gx, const double *gy,
+                      const double *gz, int xperiodic, int yperiodic, int zperiodic, const p2_params *prm);
+
+/* Boundary tables in the reference layout: bondm has 4*(sum of level nodes)
+ * entries, bondv1 has 2*(bondnum+1) (const, koef), bondn1 has bondnum+1
+ * (1 + coupled unknown index, 0 = none). */
+p2_status p2_set_bc(p2_ctx *ctx, const int *bondm, long bondm_len, const float *bondv1, const int *bondn1,
+                    long bondnum);
+
+/* Level-0 node fields (host arrays of xnumx*ynumy*znumz floats). */
+p2_status p2_set_nodes(p2_ctx *ctx, const float *nu, const float *ro, const float *nxx, const float *nxy,
+                       const float *nxz, const float *nyz);
+
+/* vpiterate(): solve the Stokes system; vx,vy,vz (float) and pr (double)
+ * are the initial guess on entry (NULL = zero) and the solution on return,
+ * with the pressure shifted so that cell (pxinit,pyinit,pzinit) holds pinit. */
+p2_status p2_stokes_solve(p2_ctx *ctx, float *vx, float *vy, float *vz, double *pr, p2_solve_info *info);
+
+/* Same solve on the resident node fields with the solution kept on the
+ * device (no host transfers); read it back with p2_get_solution. */
+p2_status p2_stokes_solve_resident(p2_ctx *ctx, p2_solve_info *info);
+p2_status p2_get_solution(p2_ctx *ctx, double *vx, double *vy, double *vz, double *pr);
+
+/* ronurecalc(): marker -> node viscosity/density interpolation.  Rock
+ * viscosity is the per-type constant markn0 (pardiso/mark3mg.c:1481-1482;
+ * types with markn0 != markn1 are rejected), density markro (densimod 0).
+ * nu..nyz are in/out: nodes that receive no marker keep their input value,
+ * then every viscosity is clamped to [nubeg, nuend], as in the reference.
+ * The fields also become this context's resident node fields. */
+p2_status p2_ronurecalc(p2_ctx *ctx, long nmark, const float *markx, const float *marky, const float *markz,
+                        const signed char *markt, int nrock, const double *markn0, const double *markn1,
+                        const double *markro, float *nu, float *ro, float *nxx, float *nxy, float *nxz,
+                        float *nyz);
+
+/* Same interpolation on markers already resident on the device (see
+ * p2_upload_markers), writing the resident node fields only. */
+p2_status p2_upload_markers(p2_ctx *ctx, long nmark, const float *markx, const float *marky, const float *markz,
+                            const signed char *markt, int nrock, const double *markn0, const double *markn1,
+                            const double *markro);
+p2_status p2_ronurecalc_resident(p2_ctx *ctx, double *ms);
+p2_status p2_get_nodes(p2_ctx *ctx, float *nu, float *ro, float *nxx, float *nxy, float *nxz, float *nyz);
+
+/* Test hooks (no counterpart in the reference; they expose single stages so
+ * parity tests can compare them with the reference's own functions).  Vectors
+ * are FP64, interleaved [P,Vx,Vy,Vz] per node of the given level (the layout
+ * of the reference's sol0/fre0/fre1 slices); the node fields must be set. */
+/* y = A x with the level operator (move3mgNew.c:796-1576 rows, boundary rows
+ * x - koef x_t, identity on non-unknown positions and on the pinned cell). */
+p2_status p2_debug_apply(p2_ctx *ctx, int level, const double *x, double *y);
+/* vprestrict (move3mgNew.c:3965) of a fine residual onto coarse_level;
+ * compat != 0 adds the continuity compatibility shift of the V-cycle. */
+p2_status p2_debug_restrict(p2_ctx *ctx, int coarse_level, const double *fine_res, double *coarse_rhs, int compat);
+/* vpprolong (move3mgNew.c:3534): fine_x += P coarse_x. */
+p2_status p2_debug_prolong(p2_ctx *ctx, int coarse_level, const double *coarse_x, double *fine_x);
+/* nu, ro of all levels after ronurestrict (move3mgNew.c:3386), concatenated
+ * with the level offsets mgp (float[sum of level nodes] each). */
+p2_status p2_debug_level_fields(p2_ctx *ctx, float *nu, float *ro);
+/* Average device time (CUDA events on the library's stream) of one colour
+ * pass of the cell-block smoother on `level` (FP32 when precision is 0),
+ * over `passes` back-to-back passes on the state left by the last solve. */
+p2_status p2_debug_time_smoother(p2_ctx *ctx, int level, int passes, double *ms_per_pass);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

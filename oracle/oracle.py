@@ -131,3 +131,22 @@ class OracleSolver:
 
     def rel_residual(self):
         return self.L.p2o_rel_residual(self.h)
+
+
+def _transfer_sigs():
+    L = lib()
+    L.p2o_restrict.argtypes = [C.c_void_p, C.c_int, _dp, _dp, C.c_int]
+    L.p2o_prolong.argtypes = [C.c_void_p, C.c_int, _dp, _dp]
+    return L
+
+
+def restrict(solver: "OracleSolver", lc: int, fine_res, n_coarse: int, compat: bool = False):
+    out = np.zeros(n_coarse * 4, np.float64)
+    _transfer_sigs().p2o_restrict(solver.h, lc, np.ascontiguousarray(fine_res, np.float64), out, 1 if compat else 0)
+    return out
+
+
+def prolong(solver: "OracleSolver", lc: int, coarse_x, fine_x):
+    f = np.array(fine_x, np.float64)
+    _transfer_sigs().p2o_prolong(solver.h, lc, np.ascontiguousarray(coarse_x, np.float64), f)
+    return f

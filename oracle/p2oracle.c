@@ -254,6 +254,7 @@ static void residual(p2o_ctx *C, int li)
 {
     p2o_level *l = &C->L[li];
     int i, j, k, c;
+#pragma omp parallel for private(i, j, c) schedule(static)
     for (k = 0; k < l->nz; k++)
         for (i = 0; i < l->nx; i++)
             for (j = 0; j < l->ny; j++) {
@@ -366,7 +367,7 @@ static void apply_bc_rows(p2o_ctx *C, int li)
                 }
 }
 
-double p2o_vanka_omega = 1.0;
+double p2o_vanka_omega = 0.7;
 
 static void smooth_vanka(p2o_ctx *C, int li, int sweeps)
 {
@@ -378,6 +379,7 @@ static void smooth_vanka(p2o_ctx *C, int li, int sweeps)
     for (s = 0; s < sweeps; s++)
         for (col = 0; col < 2; col++) {
             for (c = 0; c < 4; c++) memset(dx[c], 0, sizeof(double) * l->n);
+#pragma omp parallel for private(i, j) schedule(static)
             for (k = 1; k < l->nz; k++)
                 for (i = 1; i < l->nx; i++)
                     for (j = 1; j < l->ny; j++) {
@@ -409,6 +411,7 @@ static void smooth_vanka(p2o_ctx *C, int li, int sweeps)
                     }
             for (c = 0; c < 4; c++) {
                 long u;
+#pragma omp parallel for schedule(static)
                 for (u = 0; u < l->n; u++) l->x[c][u] += p2o_vanka_omega * dx[c][u];
             }
             apply_bc_rows(C, li);
@@ -416,7 +419,7 @@ static void smooth_vanka(p2o_ctx *C, int li, int sweeps)
     for (c = 0; c < 4; c++) free(dx[c]);
 }
 
-int p2o_smoother = 0; /* 0: lexicographic GS + Uzawa (reference scheme), 1: coloured Vanka */
+int p2o_smoother = 1; /* 0: lexicographic GS + Uzawa (reference scheme), 1: coloured Vanka */
 
 /* ---------------------------------------------------------------------- */
 /* Transfer weights along one axis (vprestrict/vpprolong index rules).     */
@@ -503,6 +506,7 @@ static double cell_volume(const p2o_level *l, int i, int j, int k)
 /* Coarse right-hand side from the fine residual (vprestrict), then the
  * compatibility shift of the continuity rows. */
 int p2o_eta_scale = 1;
+static int p2o_compat = 1;
 static void restrict_level(p2o_ctx *C, int lc)
 {
     p2o_level *f = &C->L[lc - 1], *cl = &C->L[lc];
@@ -543,7 +547,7 @@ static void restrict_level(p2o_ctx *C, int lc)
         free(wsum[c]);
     }
     /* compatibility: sum over continuity rows of volume * rhs must vanish */
-    {
+    if (p2o_compat) {
         double sv = 0, s = 0;
         for (k = 1; k < cl->nz; k++)
             for (i = 1; i < cl->nx; i++)
@@ -569,6 +573,7 @@ static void prolong_level(p2o_ctx *C, int lc)
 {
     p2o_level *f = &C->L[lc - 1], *cl = &C->L[lc];
     int c, i, j, k, a, b2, d;
+#pragma omp parallel for private(i, j, c, a, b2, d) schedule(static)
     for (k = 0; k < f->nz; k++)
         for (i = 0; i < f->nx; i++)
             for (j = 0; j < f->ny; j++) {
@@ -909,12 +914,19 @@ int p2o_set_fields(void *h, const float *nu, const float *ro, const float *nxx, 
                 long u = IDX(l, i, j, k);
                 l->b[0][u] = 0;
                 l->b[1][u] = l->b[2][u] = l->b[3][u] = 0;
-                if (valid(l, 1, i, j, k) && i < l->nx - 1 && i > 0)
-                    l->b[1][u] = -C->GX * ((double)ro[u] + ro[IDX(l, i, j + 1, k)] + ro[IDX(l, i, j, k + 1)] + ro[IDX(l, i, j + 1, k + 1)]) / 4.0;
-                if (valid(l, 2, i, j, k) && j < l->ny - 1 && j > 0)
-                    l->b[2][u] = -C->GY * ((double)ro[u] + ro[IDX(l, i + 1, j, k)] + ro[IDX(l, i, j, k + 1)] + ro[IDX(l, i + 1, j, k + 1)]) / 4.0;
-                if (valid(l, 3, i, j, k) && k < l->nz - 1 && k > 0)
-                    l->b[3][u] = -C->GZ * ((double)ro[u] + ro[IDX(l, i, j + 1, k)] + ro[IDX(l, i + 1, j, k)] + ro[IDX(l, i + 1, j + 1, k)]) / 4.0;
+                /* the four float densities are summed in float, as the reference does */
+                if (valid(l, 1, i, j, k)) {
+                    float s = ro[u] + ro[IDX(l, i, j + 1, k)] + ro[IDX(l, i, j, k + 1)] + ro[IDX(l, i, j + 1, k + 1)];
+                    l->b[1][u] = -C->GX * s / 4.0;
+                }
+                if (valid(l, 2, i, j, k)) {
+                    float s = ro[u] + ro[IDX(l, i + 1, j, k)] + ro[IDX(l, i, j, k + 1)] + ro[IDX(l, i + 1, j, k + 1)];
+                    l->b[2][u] = -C->GY * s / 4.0;
+                }
+                if (valid(l, 3, i, j, k)) {
+                    float s = ro[u] + ro[IDX(l, i, j + 1, k)] + ro[IDX(l, i + 1, j, k)] + ro[IDX(l, i + 1, j + 1, k)];
+                    l->b[3][u] = -C->GZ * s / 4.0;
+                }
             }
     for (k = 0; k < l->nz; k++)
         for (i = 0; i < l->nx; i++)
@@ -935,13 +947,19 @@ static void vec_zero(double **v, long n) { int c; for (c = 0; c < 4; c++) memset
 static double vec_dot(double **a, double **b, long n)
 {
     double s = 0; long u; int c;
-    for (c = 0; c < 4; c++) for (u = 0; u < n; u++) s += a[c][u] * b[c][u];
+    for (c = 0; c < 4; c++) {
+#pragma omp parallel for reduction(+ : s) schedule(static)
+        for (u = 0; u < n; u++) s += a[c][u] * b[c][u];
+    }
     return s;
 }
 static void vec_axpy(double **y, double a, double **x, long n)
 {
     long u; int c;
-    for (c = 0; c < 4; c++) for (u = 0; u < n; u++) y[c][u] += a * x[c][u];
+    for (c = 0; c < 4; c++) {
+#pragma omp parallel for schedule(static)
+        for (u = 0; u < n; u++) y[c][u] += a * x[c][u];
+    }
 }
 static void vec_copy(double **y, double **x, long n) { int c; for (c = 0; c < 4; c++) memcpy(y[c], x[c], sizeof(double) * n); }
 static void zero_pin_row(p2o_level *l, double **v) { if (l->pin >= 0) v[0][l->pin] = 0; }
@@ -1217,4 +1235,39 @@ double p2o_smooth_only(void *h, int sweeps)
     p2o_ctx *C = h;
     smooth(C, 0, sweeps);
     return rel_residual(C, NULL, NULL);
+}
+
+/* Single transfers on interleaved [P,Vx,Vy,Vz] vectors of one level pair
+ * (for pinning against the reference's vprestrict / vpprolong). */
+void p2o_restrict(void *h, int lc, const double *fine_res, double *coarse_rhs, int compat)
+{
+    p2o_ctx *C = h;
+    p2o_level *f = &C->L[lc - 1], *cl = &C->L[lc];
+    long u;
+    int c;
+    double *sx[4];
+    for (c = 0; c < 4; c++) sx[c] = cl->x[c];
+    for (u = 0; u < f->n; u++)
+        for (c = 0; c < 4; c++) f->r[c][u] = fine_res[u * 4 + c];
+    p2o_compat = compat;
+    restrict_level(C, lc);
+    p2o_compat = 1;
+    for (u = 0; u < cl->n; u++)
+        for (c = 0; c < 4; c++) coarse_rhs[u * 4 + c] = cl->b[c][u];
+    (void)sx;
+}
+
+void p2o_prolong(void *h, int lc, const double *coarse_x, double *fine_x)
+{
+    p2o_ctx *C = h;
+    p2o_level *f = &C->L[lc - 1], *cl = &C->L[lc];
+    long u;
+    int c;
+    for (u = 0; u < cl->n; u++)
+        for (c = 0; c < 4; c++) cl->x[c][u] = coarse_x[u * 4 + c];
+    for (u = 0; u < f->n; u++)
+        for (c = 0; c < 4; c++) f->x[c][u] = fine_x[u * 4 + c];
+    prolong_level(C, lc);
+    for (u = 0; u < f->n; u++)
+        for (c = 0; c < 4; c++) fine_x[u * 4 + c] = f->x[c][u];
 }

@@ -1,0 +1,241 @@
+"""ctypes binding of libp2cuda.so (include/p2cuda.h).
+
+Only plain host pointers and sizes cross this boundary.  There is no CPU
+fallback: if the library or a CUDA device is missing, every call raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Dict, Optional
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libp2cuda.so")
+
+P2_MAX_LEVELS = 12
+STATUS = {0: "P2_OK", 1: "P2_ERR_ARG", 2: "P2_ERR_CUDA", 3: "P2_ERR_NOMEM", 4: "P2_ERR_NOT_CONVERGED",
+          5: "P2_ERR_NAN", 6: "P2_ERR_SINGULAR", 7: "P2_ERR_STATE", 8: "P2_ERR_UNSUPPORTED"}
+EXPORTED = ["p2_default_params", "p2_create", "p2_destroy", "p2_last_error", "p2_set_grid", "p2_set_bc",
+            "p2_set_nodes", "p2_stokes_solve", "p2_stokes_solve_resident", "p2_get_solution", "p2_ronurecalc",
+            "p2_upload_markers", "p2_ronurecalc_resident", "p2_get_nodes", "p2_debug_apply", "p2_debug_restrict",
+            "p2_debug_prolong", "p2_debug_level_fields", "p2_debug_time_smoother"]
+
+
+class Params(C.Structure):
+    _fields_ = [("p0koef", C.c_double), ("p1koef", C.c_double), ("p2koef", C.c_double), ("v0koef", C.c_double),
+                ("v1koef", C.c_double), ("nubeg", C.c_double), ("nuend", C.c_double), ("nukoef", C.c_double),
+                ("gxkoef", C.c_double), ("gykoef", C.c_double), ("gzkoef", C.c_double), ("pinit", C.c_double),
+                ("pxinit", C.c_int), ("pyinit", C.c_int), ("pzinit", C.c_int), ("viscmod", C.c_int),
+                ("multinum", C.c_int), ("npre", C.c_int * P2_MAX_LEVELS), ("npost", C.c_int * P2_MAX_LEVELS),
+                ("tol", C.c_double), ("max_iter", C.c_int), ("precision", C.c_int), ("restart", C.c_int),
+                ("omega", C.c_double), ("use_graphs", C.c_int)]
+
+
+class SolveInfo(C.Structure):
+    _fields_ = [("iterations", C.c_int), ("rel_residual", C.c_double), ("rel_residual0", C.c_double),
+                ("ms_total", C.c_double), ("ms_setup", C.c_double), ("ms_vcycles", C.c_double), ("status", C.c_int),
+                ("kernels", C.c_longlong)]
+
+    def as_dict(self) -> Dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class P2Error(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__("%s: %s" % (STATUS.get(code, code), msg))
+        self.code = code
+
+
+_dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_fp = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
+_ip = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+_bp = np.ctypeslib.ndpointer(dtype=np.int8, flags="C_CONTIGUOUS")
+_lib: Optional[C.CDLL] = None
+
+
+def load() -> C.CDLL:
+    """Load the library (raises if it was not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError("libp2cuda.so is not built (run python -m pardiso2_b200.build)")
+    L = C.CDLL(LIB_PATH)
+    vp = C.c_void_p
+    L.p2_default_params.argtypes = [C.POINTER(Params)]
+    L.p2_create.argtypes = [C.POINTER(vp), C.c_int]
+    L.p2_destroy.argtypes = [vp]
+    L.p2_last_error.argtypes = [vp]
+    L.p2_last_error.restype = C.c_char_p
+    L.p2_set_grid.argtypes = [vp, C.c_long, C.c_long, C.c_long, _dp, _dp, _dp, C.c_int, C.c_int, C.c_int,
+                              C.POINTER(Params)]
+    L.p2_set_bc.argtypes = [vp, _ip, C.c_long, _fp, _ip, C.c_long]
+    L.p2_set_nodes.argtypes = [vp] + [_fp] * 6
+    L.p2_stokes_solve.argtypes = [vp, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(SolveInfo)]
+    L.p2_stokes_solve_resident.argtypes = [vp, C.POINTER(SolveInfo)]
+    L.p2_get_solution.argtypes = [vp, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    L.p2_ronurecalc.argtypes = [vp, C.c_long, _fp, _fp, _fp, _bp, C.c_int, _dp, _dp, _dp] + [_fp] * 6
+    L.p2_upload_markers.argtypes = [vp, C.c_long, _fp, _fp, _fp, _bp, C.c_int, _dp, _dp, _dp]
+    L.p2_ronurecalc_resident.argtypes = [vp, C.POINTER(C.c_double)]
+    L.p2_get_nodes.argtypes = [vp] + [C.c_void_p] * 6
+    for f in ("p2_create", "p2_set_grid", "p2_set_bc", "p2_set_nodes", "p2_stokes_solve", "p2_stokes_solve_resident",
+              "p2_get_solution", "p2_ronurecalc", "p2_upload_markers", "p2_ronurecalc_resident", "p2_get_nodes"):
+        getattr(L, f).restype = C.c_int
+    _lib = L
+    return L
+
+
+def default_params() -> Params:
+    p = Params()
+    load().p2_default_params(C.byref(p))
+    return p
+
+
+def _ptr(a: Optional[np.ndarray]):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+class Context:
+    """One device context (p2_ctx): levels, boundary tables, node fields and
+    solver state stay resident on the GPU across calls."""
+
+    def __init__(self, device: int = 0):
+        self.L = load()
+        h = C.c_void_p()
+        st = self.L.p2_create(C.byref(h), device)
+        if st != 0:
+            raise P2Error(st, "p2_create failed (is a CUDA device visible?)")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.p2_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def _check(self, st: int, what: str):
+        if st != 0:
+            raise P2Error(st, "%s: %s" % (what, self.L.p2_last_error(self.h).decode()))
+
+    def set_grid(self, gx, gy, gz, params: Params, periodic=(0, 0, 0)):
+        gx, gy, gz = (np.ascontiguousarray(a, np.float64) for a in (gx, gy, gz))
+        self._check(self.L.p2_set_grid(self.h, gx.size, gy.size, gz.size, gx, gy, gz, *periodic, C.byref(params)),
+                    "p2_set_grid")
+
+    def set_bc(self, bondm, bondv1, bondn1):
+        bm = np.ascontiguousarray(bondm, np.int32)
+        bv = np.ascontiguousarray(np.asarray(bondv1, np.float32).reshape(-1))
+        bn = np.ascontiguousarray(bondn1, np.int32)
+        self._check(self.L.p2_set_bc(self.h, bm, bm.size, bv, bn, bn.size - 1), "p2_set_bc")
+
+    def set_nodes(self, f: Dict[str, np.ndarray]):
+        self._check(self.L.p2_set_nodes(self.h, *[np.ascontiguousarray(f[k], np.float32)
+                                                   for k in ("nu", "ro", "nxx", "nxy", "nxz", "nyz")]),
+                    "p2_set_nodes")
+
+    def stokes_solve(self, vx=None, vy=None, vz=None, pr=None, check=True):
+        """vpiterate(): in/out arrays (float vx/vy/vz, double pr); returns SolveInfo."""
+        info = SolveInfo()
+        st = self.L.p2_stokes_solve(self.h, _ptr(vx), _ptr(vy), _ptr(vz), _ptr(pr), C.byref(info))
+        if check:
+            self._check(st, "p2_stokes_solve")
+        return info
+
+    def solve_resident(self, check=True) -> SolveInfo:
+        info = SolveInfo()
+        st = self.L.p2_stokes_solve_resident(self.h, C.byref(info))
+        if check:
+            self._check(st, "p2_stokes_solve_resident")
+        return info
+
+    def solution(self, n: int) -> Dict[str, np.ndarray]:
+        out = {k: np.zeros(n, np.float64) for k in ("vx", "vy", "vz", "pr")}
+        self._check(self.L.p2_get_solution(self.h, _ptr(out["vx"]), _ptr(out["vy"]), _ptr(out["vz"]),
+                                           _ptr(out["pr"])), "p2_get_solution")
+        return out
+
+    def upload_markers(self, mx, my, mz, mt, n0, n1, ro):
+        self._check(self.L.p2_upload_markers(self.h, mx.size, np.ascontiguousarray(mx, np.float32),
+                                             np.ascontiguousarray(my, np.float32), np.ascontiguousarray(mz, np.float32),
+                                             np.ascontiguousarray(mt, np.int8), len(n0),
+                                             np.ascontiguousarray(n0, np.float64), np.ascontiguousarray(n1, np.float64),
+                                             np.ascontiguousarray(ro, np.float64)), "p2_upload_markers")
+
+    def ronurecalc_resident(self) -> float:
+        ms = C.c_double()
+        self._check(self.L.p2_ronurecalc_resident(self.h, C.byref(ms)), "p2_ronurecalc_resident")
+        return ms.value
+
+    def get_nodes(self, n: int) -> Dict[str, np.ndarray]:
+        keys = ("nu", "ro", "nxx", "nxy", "nxz", "nyz")
+        out = {k: np.zeros(n, np.float32) for k in keys}
+        self._check(self.L.p2_get_nodes(self.h, *[_ptr(out[k]) for k in keys]), "p2_get_nodes")
+        return out
+
+    def ronurecalc(self, mx, my, mz, mt, n0, n1, ro, fields: Dict[str, np.ndarray]):
+        """ronurecalc(): in/out node fields (dict of float32 arrays, modified in place)."""
+        keys = ("nu", "ro", "nxx", "nxy", "nxz", "nyz")
+        for k in keys:
+            if fields[k].dtype != np.float32 or not fields[k].flags.c_contiguous:
+                raise ValueError("node field %s must be a contiguous float32 array" % k)
+        self._check(self.L.p2_ronurecalc(self.h, mx.size, np.ascontiguousarray(mx, np.float32),
+                                         np.ascontiguousarray(my, np.float32), np.ascontiguousarray(mz, np.float32),
+                                         np.ascontiguousarray(mt, np.int8), len(n0), np.ascontiguousarray(n0, np.float64),
+                                         np.ascontiguousarray(n1, np.float64), np.ascontiguousarray(ro, np.float64),
+                                         *[fields[k] for k in keys]), "p2_ronurecalc")
+        return fields
+
+
+def _debug_sigs(L):
+    _dpp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+    _fpp = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
+    L.p2_debug_apply.argtypes = [C.c_void_p, C.c_int, _dpp, _dpp]
+    L.p2_debug_restrict.argtypes = [C.c_void_p, C.c_int, _dpp, _dpp, C.c_int]
+    L.p2_debug_prolong.argtypes = [C.c_void_p, C.c_int, _dpp, _dpp]
+    L.p2_debug_level_fields.argtypes = [C.c_void_p, _fpp, _fpp]
+    L.p2_debug_time_smoother.argtypes = [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_double)]
+    for f in ("p2_debug_apply", "p2_debug_restrict", "p2_debug_prolong", "p2_debug_level_fields",
+              "p2_debug_time_smoother"):
+        getattr(L, f).restype = C.c_int
+
+
+class DebugHooks:
+    """Single-stage test hooks of the library (FP64, interleaved [P,Vx,Vy,Vz])."""
+
+    def __init__(self, ctx: Context):
+        self.ctx = ctx
+        _debug_sigs(ctx.L)
+
+    def apply(self, level: int, x: np.ndarray) -> np.ndarray:
+        y = np.zeros_like(x, dtype=np.float64)
+        self.ctx._check(self.ctx.L.p2_debug_apply(self.ctx.h, level, np.ascontiguousarray(x, np.float64), y),
+                        "p2_debug_apply")
+        return y
+
+    def restrict(self, coarse_level: int, fine_res: np.ndarray, n_coarse: int, compat: bool = False) -> np.ndarray:
+        out = np.zeros(n_coarse * 4, np.float64)
+        self.ctx._check(self.ctx.L.p2_debug_restrict(self.ctx.h, coarse_level, np.ascontiguousarray(fine_res, np.float64),
+                                                     out, 1 if compat else 0), "p2_debug_restrict")
+        return out
+
+    def prolong(self, coarse_level: int, coarse_x: np.ndarray, fine_x: np.ndarray) -> np.ndarray:
+        f = np.array(fine_x, np.float64)
+        self.ctx._check(self.ctx.L.p2_debug_prolong(self.ctx.h, coarse_level, np.ascontiguousarray(coarse_x, np.float64),
+                                                    f), "p2_debug_prolong")
+        return f
+
+    def time_smoother(self, level: int = 0, passes: int = 20) -> float:
+        ms = C.c_double()
+        self.ctx._check(self.ctx.L.p2_debug_time_smoother(self.ctx.h, level, passes, C.byref(ms)),
+                        "p2_debug_time_smoother")
+        return ms.value
+
+    def level_fields(self, total_nodes: int):
+        nu = np.zeros(total_nodes, np.float32)
+        ro = np.zeros(total_nodes, np.float32)
+        self.ctx._check(self.ctx.L.p2_debug_level_fields(self.ctx.h, nu, ro), "p2_debug_level_fields")
+        return nu, ro

@@ -1,0 +1,294 @@
+// extern "C" entry points of libp2cuda.so (declared in include/p2cuda.h).
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "p2_solver.h"
+
+struct p2_ctx {
+    p2::Solver *s = nullptr;
+    std::string err;
+};
+
+template <typename F>
+static p2_status guard(p2_ctx *ctx, F &&f)
+{
+    if (!ctx) return P2_ERR_ARG;
+    try {
+        f();
+        ctx->err.clear();
+        return P2_OK;
+    } catch (const p2::Error &e) {
+        ctx->err = e.msg;
+        return e.code;
+    } catch (const std::bad_alloc &) {
+        ctx->err = "host allocation failed";
+        return P2_ERR_NOMEM;
+    } catch (...) {
+        ctx->err = "unknown error";
+        return P2_ERR_CUDA;
+    }
+}
+
+extern "C" {
+
+void p2_default_params(p2_params *p)
+{
+    if (!p) return;
+    std::memset(p, 0, sizeof(*p));
+    // pardiso/mode.t3c:83-93
+    p->p0koef = 0.3;
+    p->p1koef = 1.0;
+    p->p2koef = 0.0;
+    p->v0koef = 1.0;
+    p->v1koef = 1.0;
+    p->nubeg = 1.0;
+    p->nuend = 1e4;
+    p->nukoef = 0.0;
+    p->gxkoef = p->gykoef = 0.0;
+    p->gzkoef = 0.0;
+    p->pinit = 0.0;
+    p->pxinit = p->pyinit = p->pzinit = 2;
+    p->viscmod = 0;
+    p->multinum = 2;
+    for (int l = 0; l < P2_MAX_LEVELS; l++) { p->npre[l] = 4; p->npost[l] = 4; }
+    p->tol = 1e-8;
+    p->max_iter = 200;
+    p->precision = 0;
+    p->restart = 16;
+    p->omega = 0.7;
+    p->use_graphs = 1;
+}
+
+p2_status p2_create(p2_ctx **out, int device)
+{
+    if (!out) return P2_ERR_ARG;
+    *out = nullptr;
+    p2_ctx *ctx = new (std::nothrow) p2_ctx;
+    if (!ctx) return P2_ERR_NOMEM;
+    p2_status st = guard(ctx, [&] {
+        int n = 0;
+        P2_CUDA_TRY(cudaGetDeviceCount(&n));
+        if (device < 0 || device >= n) throw p2::Error(P2_ERR_ARG, "no such CUDA device");
+        ctx->s = new p2::Solver(device);
+    });
+    if (st != P2_OK) {
+        delete ctx;
+        return st;
+    }
+    *out = ctx;
+    return P2_OK;
+}
+
+void p2_destroy(p2_ctx *ctx)
+{
+    if (!ctx) return;
+    delete ctx->s;
+    delete ctx;
+}
+
+const char *p2_last_error(const p2_ctx *ctx)
+{
+    if (!ctx) return "null context";
+    return ctx->err.c_str();
+}
+
+p2_status p2_set_grid(p2_ctx *ctx, long xnumx, long ynumy, long znumz, const double *gx, const double *gy,
+                      const double *gz, int xperiodic, int yperiodic, int zperiodic, const p2_params *prm)
+{
+    return guard(ctx, [&] {
+        if (!gx || !gy || !gz || !prm) throw p2::Error(P2_ERR_ARG, "null argument");
+        if (xperiodic || yperiodic || zperiodic)
+            throw p2::Error(P2_ERR_UNSUPPORTED, "periodic boundaries are not supported");
+        if (prm->precision != 0 && prm->precision != 1) throw p2::Error(P2_ERR_ARG, "precision must be 0 or 1");
+        if (!(prm->omega > 0 && prm->omega < 2)) throw p2::Error(P2_ERR_ARG, "omega must be in (0, 2)");
+        if (!(prm->tol > 0)) throw p2::Error(P2_ERR_ARG, "tol must be positive");
+        if (!(prm->nubeg > 0) || !(prm->nuend >= prm->nubeg)) throw p2::Error(P2_ERR_ARG, "bad nubeg/nuend");
+        P2_CUDA_TRY(cudaSetDevice(ctx->s->dev));
+        ctx->s->set_grid(xnumx, ynumy, znumz, gx, gy, gz, *prm);
+    });
+}
+
+p2_status p2_set_bc(p2_ctx *ctx, const int *bondm, long bondm_len, const float *bondv1, const int *bondn1,
+                    long bondnum)
+{
+    return guard(ctx, [&] {
+        if (!bondm || !bondv1 || !bondn1 || bondnum < 0) throw p2::Error(P2_ERR_ARG, "null or negative argument");
+        P2_CUDA_TRY(cudaSetDevice(ctx->s->dev));
+        ctx->s->set_bc(bondm, bondm_len, bondv1, bondn1, bondnum);
+    });
+}
+
+p2_status p2_set_nodes(p2_ctx *ctx, const float *nu, const float *ro, const float *nxx, const float *nxy,
+                       const float *nxz, const float *nyz)
+{
+    return guard(ctx, [&] {
+        P2_CUDA_TRY(cudaSetDevice(ctx->s->dev));
+        ctx->s->upload_nodes(nu, ro, nxx, nxy, nxz, nyz);
+    });
+}
+
+static void finish_info(p2_solve_info *info, const p2_solve_info &r)
+{
+    if (info) *info = r;
+}
+
+p2_status p2_stokes_solve(p2_ctx *ctx, float *vx, float *vy, float *vz, double *pr, p2_solve_info *info)
+{
+    p2_solve_info r{};
+    p2_status st = guard(ctx, [&] {
+        p2::Solver &S = *ctx->s;
+        P2_CUDA_TRY(cudaSetDevice(S.dev));
+        if (!S.bc_ready) throw p2::Error(P2_ERR_STATE, "solve before p2_set_bc");
+        S.set_initial(vx, vy, vz, pr);
+        r = S.solve();
+        long n = S.L[0].n;
+        std::vector<double> hv[3];
+        for (int q = 0; q < 3; q++) hv[q].resize(n);
+        S.get_solution(vx ? hv[0].data() : nullptr, vy ? hv[1].data() : nullptr, vz ? hv[2].data() : nullptr, pr);
+        float *dst[3] = {vx, vy, vz};
+        for (int q = 0; q < 3; q++)
+            if (dst[q])
+                for (long u = 0; u < n; u++) dst[q][u] = (float)hv[q][u];
+    });
+    finish_info(info, r);
+    if (st != P2_OK) return st;
+    return (p2_status)r.status;
+}
+
+p2_status p2_stokes_solve_resident(p2_ctx *ctx, p2_solve_info *info)
+{
+    p2_solve_info r{};
+    p2_status st = guard(ctx, [&] {
+        p2::Solver &S = *ctx->s;
+        P2_CUDA_TRY(cudaSetDevice(S.dev));
+        if (!S.bc_ready) throw p2::Error(P2_ERR_STATE, "solve before p2_set_bc");
+        S.set_initial(nullptr, nullptr, nullptr, nullptr);
+        r = S.solve();
+    });
+    finish_info(info, r);
+    if (st != P2_OK) return st;
+    return (p2_status)r.status;
+}
+
+p2_status p2_get_solution(p2_ctx *ctx, double *vx, double *vy, double *vz, double *pr)
+{
+    return guard(ctx, [&] {
+        P2_CUDA_TRY(cudaSetDevice(ctx->s->dev));
+        if (!ctx->s->bc_ready) throw p2::Error(P2_ERR_STATE, "no solution");
+        ctx->s->get_solution(vx, vy, vz, pr);
+    });
+}
+
+p2_status p2_upload_markers(p2_ctx *ctx, long nmark, const float *markx, const float *marky, const float *markz,
+                            const signed char *markt, int nrock, const double *markn0, const double *markn1,
+                            const double *markro)
+{
+    return guard(ctx, [&] {
+        if (nmark > 0 && (!markx || !marky || !markz || !markt)) throw p2::Error(P2_ERR_ARG, "null marker array");
+        if (!markn0 || !markn1 || !markro) throw p2::Error(P2_ERR_ARG, "null rock table");
+        P2_CUDA_TRY(cudaSetDevice(ctx->s->dev));
+        ctx->s->upload_markers(nmark, markx, marky, markz, markt, nrock, markn0, markn1, markro);
+    });
+}
+
+p2_status p2_ronurecalc_resident(p2_ctx *ctx, double *ms)
+{
+    return guard(ctx, [&] {
+        p2::Solver &S = *ctx->s;
+        P2_CUDA_TRY(cudaSetDevice(S.dev));
+        P2_CUDA_TRY(cudaEventRecord(S.ev[5], S.st));
+        S.ronurecalc_device();
+        P2_CUDA_TRY(cudaEventRecord(S.ev[6], S.st));
+        P2_CUDA_TRY(cudaEventSynchronize(S.ev[6]));
+        float t = 0;
+        P2_CUDA_TRY(cudaEventElapsedTime(&t, S.ev[5], S.ev[6]));
+        if (ms) *ms = t;
+    });
+}
+
+p2_status p2_get_nodes(p2_ctx *ctx, float *nu, float *ro, float *nxx, float *nxy, float *nxz, float *nyz)
+{
+    return guard(ctx, [&] {
+        p2::Solver &S = *ctx->s;
+        P2_CUDA_TRY(cudaSetDevice(S.dev));
+        if (!S.markers_ready) throw p2::Error(P2_ERR_STATE, "no node fields computed");
+        float *dst[6] = {nu, ro, nxx, nxy, nxz, nyz};
+        for (int q = 0; q < 6; q++)
+            if (dst[q])
+                P2_CUDA_TRY(cudaMemcpyAsync(dst[q], S.mk_nodes[q], sizeof(float) * S.L[0].n, cudaMemcpyDeviceToHost,
+                                            S.st));
+        P2_CUDA_TRY(cudaStreamSynchronize(S.st));
+    });
+}
+
+p2_status p2_ronurecalc(p2_ctx *ctx, long nmark, const float *markx, const float *marky, const float *markz,
+                        const signed char *markt, int nrock, const double *markn0, const double *markn1,
+                        const double *markro, float *nu, float *ro, float *nxx, float *nxy, float *nxz, float *nyz)
+{
+    p2_status st = p2_upload_markers(ctx, nmark, markx, marky, markz, markt, nrock, markn0, markn1, markro);
+    if (st != P2_OK) return st;
+    st = guard(ctx, [&] {
+        p2::Solver &S = *ctx->s;
+        float *src[6] = {nu, ro, nxx, nxy, nxz, nyz};
+        for (int q = 0; q < 6; q++) {
+            if (!src[q]) throw p2::Error(P2_ERR_ARG, "null node field");
+            P2_CUDA_TRY(cudaMemcpyAsync(S.mk_nodes[q], src[q], sizeof(float) * S.L[0].n, cudaMemcpyHostToDevice,
+                                        S.st));
+        }
+    });
+    if (st != P2_OK) return st;
+    st = p2_ronurecalc_resident(ctx, nullptr);
+    if (st != P2_OK) return st;
+    return p2_get_nodes(ctx, nu, ro, nxx, nxy, nxz, nyz);
+}
+
+p2_status p2_debug_apply(p2_ctx *ctx, int level, const double *x, double *y)
+{
+    return guard(ctx, [&] {
+        if (!x || !y) throw p2::Error(P2_ERR_ARG, "null argument");
+        P2_CUDA_TRY(cudaSetDevice(ctx->s->dev));
+        ctx->s->debug_apply(level, x, y);
+    });
+}
+
+p2_status p2_debug_restrict(p2_ctx *ctx, int coarse_level, const double *fine_res, double *coarse_rhs, int compat)
+{
+    return guard(ctx, [&] {
+        if (!fine_res || !coarse_rhs) throw p2::Error(P2_ERR_ARG, "null argument");
+        P2_CUDA_TRY(cudaSetDevice(ctx->s->dev));
+        ctx->s->debug_restrict(coarse_level, fine_res, coarse_rhs, compat);
+    });
+}
+
+p2_status p2_debug_prolong(p2_ctx *ctx, int coarse_level, const double *coarse_x, double *fine_x)
+{
+    return guard(ctx, [&] {
+        if (!coarse_x || !fine_x) throw p2::Error(P2_ERR_ARG, "null argument");
+        P2_CUDA_TRY(cudaSetDevice(ctx->s->dev));
+        ctx->s->debug_prolong(coarse_level, coarse_x, fine_x);
+    });
+}
+
+p2_status p2_debug_time_smoother(p2_ctx *ctx, int level, int passes, double *ms_per_pass)
+{
+    return guard(ctx, [&] {
+        if (!ms_per_pass) throw p2::Error(P2_ERR_ARG, "null argument");
+        P2_CUDA_TRY(cudaSetDevice(ctx->s->dev));
+        *ms_per_pass = ctx->s->debug_time_smoother(level, passes);
+    });
+}
+
+p2_status p2_debug_level_fields(p2_ctx *ctx, float *nu, float *ro)
+{
+    return guard(ctx, [&] {
+        if (!nu || !ro) throw p2::Error(P2_ERR_ARG, "null argument");
+        P2_CUDA_TRY(cudaSetDevice(ctx->s->dev));
+        ctx->s->debug_level_fields(nu, ro);
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,455 @@
+// Stencil, transfer and reduction kernels of the p2cuda Stokes multigrid.
+#pragma once
+
+#include "p2_internal.cuh"
+
+namespace p2 {
+
+constexpr int kThreads = 256;
+
+// ---------------------------------------------------------------------------
+// Rows: out = b - A x (mode 0) or out = A x (mode 1) on every non-boundary
+// row; boundary rows and non-unknown positions get 0 here (boundary rows are
+// written by k_bc_rows).  Optionally also writes a float copy (the FP32
+// right-hand side of the mixed-precision V-cycle).
+template <typename T, typename S>
+__global__ void k_rows(LevelView<T> L, Fields<T, S> x, Vec4<T> b, Vec4<T> out, Vec4<float> out32, int mode)
+{
+    int u = blockIdx.x * blockDim.x + threadIdx.x;
+    if (u >= L.n) return;
+    int j = u % L.ny, i = (u / L.ny) % L.nx, k = u / (L.nx * L.ny);
+    uint8_t m = L.bcm[u];
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+        T v = 0;
+        if (valid_pos(c, i, j, k, L.nx, L.ny, L.nz) && !(m & (1 << c))) {
+            T ax;
+            if (c == 0) ax = row_p(L, x, i, j, k);
+            else if (c == 1) ax = row_vx(L, x, i, j, k, (T *)nullptr);
+            else if (c == 2) ax = row_vy(L, x, i, j, k, (T *)nullptr);
+            else ax = row_vz(L, x, i, j, k, (T *)nullptr);
+            v = mode == 0 ? b.c[c][u] - ax : ax;
+        }
+        out.c[c][u] = v;
+        if (out32.c[0]) out32.c[c][u] = (float)v;
+    }
+}
+
+// Boundary rows x_u = b_u + koef * x_t: residual (mode 0) b_u + koef x_t - x_u,
+// or operator (mode 1) x_u - koef x_t.
+template <typename T, typename S>
+__global__ void k_bc_rows(int nbc, const int *bu, const int *bt, const float *bk, Fields<T, S> x, Vec4<T> b,
+                          Vec4<T> out, Vec4<float> out32, int mode)
+{
+    int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= nbc) return;
+    int uc = bu[q], c = uc & 3, u = uc >> 2, t = bt[q];
+    const S *xs[4] = {x.p, x.vx, x.vy, x.vz};
+    T xt = t >= 0 ? (T)bk[q] * (T)xs[t & 3][t >> 2] : (T)0;
+    T v = mode == 0 ? b.c[c][u] + xt - (T)xs[c][u] : (T)xs[c][u] - xt;
+    out.c[c][u] = v;
+    if (out32.c[0]) out32.c[c][u] = (float)v;
+}
+
+// Apply boundary rows: x_u = b_u + koef * x_t (one depth group of copy chains).
+template <typename T>
+__global__ void k_bc_set(int nbc, const int *bu, const int *bt, const float *bk, Vec4<T> x, Vec4<T> b)
+{
+    int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= nbc) return;
+    int uc = bu[q], c = uc & 3, u = uc >> 2, t = bt[q];
+    T xt = t >= 0 ? (T)bk[q] * x.c[t & 3][t >> 2] : (T)0;
+    x.c[c][u] = b.c[c][u] + xt;
+}
+
+// ---------------------------------------------------------------------------
+// One colour pass of the cell-block smoother (diagonal Vanka / SCGS) over the
+// cells with (i+j+k)&1 == col.  Each cell corrects its six face velocities and
+// its pressure together with the velocity block replaced by its diagonal:
+//   d_v dv_v + g_v dp = r_v,  sum_v c_v dv_v = r_p.
+// Every cell of the colour reads the state from before the pass: velocities
+// are read from vin and written to vout (each face belongs to exactly one
+// cell of each colour), the pressure is updated in place (a cell's pressure is
+// read only by its own face rows among the cells of one colour).
+template <typename T>
+__global__ void k_vanka(LevelView<T> L, T *P, Vec4<T> vin, Vec4<T> vout, Vec4<T> b, T omega, int col)
+{
+    int half = (L.ny) / 2;  // >= number of cells of one colour on a y-line
+    long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    long lines = (long)(L.nx - 1) * (L.nz - 1);
+    if (t >= lines * half) return;
+    int jj = (int)(t % half);
+    long line = t / half;
+    int i = 1 + (int)(line % (L.nx - 1)), k = 1 + (int)(line / (L.nx - 1));
+    int j0 = (((1 + i + k) & 1) == col) ? 1 : 2;
+    int j = j0 + 2 * jj;
+    if (j > L.ny - 1) return;
+    Fields<T, T> x{P, vin.c[1], vin.c[2], vin.c[3]};
+    int u = P2IDX(L, i, j, k);
+    bool pbc = (L.bcm[u] & BC_P) != 0;
+    int fi[6], fc[6];
+    T g[6], cc[6], r[6], d[6];
+    fc[0] = 1; fi[0] = P2IDX(L, i - 1, j - 1, k - 1); g[0] = -L.ax.ihc[i - 1]; cc[0] = -L.ax.ih[i];
+    fc[1] = 1; fi[1] = P2IDX(L, i, j - 1, k - 1);     g[1] = L.ax.ihc[i];      cc[1] = L.ax.ih[i];
+    fc[2] = 2; fi[2] = P2IDX(L, i - 1, j - 1, k - 1); g[2] = -L.ay.ihc[j - 1]; cc[2] = -L.ay.ih[j];
+    fc[3] = 2; fi[3] = P2IDX(L, i - 1, j, k - 1);     g[3] = L.ay.ihc[j];      cc[3] = L.ay.ih[j];
+    fc[4] = 3; fi[4] = P2IDX(L, i - 1, j - 1, k - 1); g[4] = -L.az.ihc[k - 1]; cc[4] = -L.az.ih[k];
+    fc[5] = 3; fi[5] = P2IDX(L, i - 1, j - 1, k);     g[5] = L.az.ihc[k];      cc[5] = L.az.ih[k];
+    const int ofs[6][3] = {{-1, -1, -1}, {0, -1, -1}, {-1, -1, -1}, {-1, 0, -1}, {-1, -1, -1}, {-1, -1, 0}};
+    T num = 0, den = 0;
+#pragma unroll
+    for (int q = 0; q < 6; q++) {
+        int a = i + ofs[q][0], bb = j + ofs[q][1], c = k + ofs[q][2];
+        d[q] = 0;
+        r[q] = 0;
+        if (L.bcm[fi[q]] & (1 << fc[q])) continue;
+        T ax;
+        if (fc[q] == 1) ax = row_vx(L, x, a, bb, c, &d[q]);
+        else if (fc[q] == 2) ax = row_vy(L, x, a, bb, c, &d[q]);
+        else ax = row_vz(L, x, a, bb, c, &d[q]);
+        r[q] = b.c[fc[q]][fi[q]] - ax;
+        num += cc[q] * r[q] / d[q];
+        den += cc[q] * g[q] / d[q];
+    }
+    T dp = 0;
+    if (!pbc && den != (T)0) {
+        T rp = b.c[0][u] - row_p(L, x, i, j, k);
+        dp = (num - rp) / den;
+        P[u] += omega * dp;
+    }
+#pragma unroll
+    for (int q = 0; q < 6; q++) {
+        if (d[q] != (T)0) vout.c[fc[q]][fi[q]] = vin.c[fc[q]][fi[q]] + omega * (r[q] - g[q] * dp) / d[q];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Transfers.  Per-axis tables (host-built from the reference's index rules,
+// move3mgNew.c:3562-3575 and the corresponding blocks of vprestrict and
+// vpprolong): for a fine index m, the coarse interval lo[m] and the weights
+// w0 (coarse lo) and w1 (coarse lo+1).  Restriction uses the inverse lists.
+__device__ __forceinline__ int ax_type(int comp, int axis)
+{
+    if (comp == 0) return 2;
+    return (comp == axis + 1) ? 0 : 1;
+}
+
+// b_c = sum_f w r_f (P: * eta_f/eta_c) / sum_f w over non-boundary fine rows,
+// for non-boundary coarse rows (0 otherwise); x_c = 0 (vprestrict).
+template <typename T>
+__global__ void k_restrict(LevelView<T> F, Vec4<T> rf, LevelView<T> Cl, Vec4<T> bc, Vec4<T> xc, TransferView tv,
+                           int scale_p)
+{
+    int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= Cl.n) return;
+    int J = v % Cl.ny, I = (v / Cl.ny) % Cl.nx, K = v / (Cl.nx * Cl.ny);
+    uint8_t mc = Cl.bcm[v];
+    for (int c = 0; c < 4; c++) {
+        xc.c[c][v] = 0;
+        T out = 0;
+        if (valid_pos(c, I, J, K, Cl.nx, Cl.ny, Cl.nz) && !(mc & (1 << c))) {
+            const AxisMap &mx = tv.m[0][ax_type(c, 0)], &my = tv.m[1][ax_type(c, 1)], &mz = tv.m[2][ax_type(c, 2)];
+            T acc = 0, ws = 0;
+            T etac = c == 0 ? (T)Cl.ec[v] : (T)1;
+            for (int qz = mz.ptr[K]; qz < mz.ptr[K + 1]; qz++) {
+                int fk = mz.idx[qz];
+                T wz = (T)mz.w[qz];
+                for (int qx = mx.ptr[I]; qx < mx.ptr[I + 1]; qx++) {
+                    int fi = mx.idx[qx];
+                    T wzx = wz * (T)mx.w[qx];
+                    for (int qy = my.ptr[J]; qy < my.ptr[J + 1]; qy++) {
+                        int fj = my.idx[qy];
+                        int f = P2IDX(F, fi, fj, fk);
+                        if (F.bcm[f] & (1 << c)) continue;
+                        T w = wzx * (T)my.w[qy];
+                        T val = rf.c[c][f];
+                        if (c == 0 && scale_p) val *= (T)F.ec[f] / etac;
+                        acc += val * w;
+                        ws += w;
+                    }
+                }
+            }
+            out = ws != (T)0 ? acc / ws : (T)0;
+        }
+        bc.c[c][v] = out;
+    }
+}
+
+// x_f += sum_c w x_c * (p1koef | v1koef) over every fine unknown position.
+template <typename T>
+__global__ void k_prolong(LevelView<T> F, Vec4<T> xf, LevelView<T> Cl, Vec4<T> xc, TransferView tv, T p1, T v1)
+{
+    int u = blockIdx.x * blockDim.x + threadIdx.x;
+    if (u >= F.n) return;
+    int j = u % F.ny, i = (u / F.ny) % F.nx, k = u / (F.nx * F.ny);
+    for (int c = 0; c < 4; c++) {
+        if (!valid_pos(c, i, j, k, F.nx, F.ny, F.nz)) continue;
+        const AxisMap &mx = tv.m[0][ax_type(c, 0)], &my = tv.m[1][ax_type(c, 1)], &mz = tv.m[2][ax_type(c, 2)];
+        int lx = mx.lo[i], ly = my.lo[j], lz = mz.lo[k];
+        T wx0 = (T)mx.w0[i], wx1 = (T)mx.w1[i], wy0 = (T)my.w0[j], wy1 = (T)my.w1[j];
+        T wz0 = (T)mz.w0[k], wz1 = (T)mz.w1[k];
+        T s = 0;
+#pragma unroll
+        for (int d = 0; d < 2; d++)
+#pragma unroll
+            for (int a = 0; a < 2; a++)
+#pragma unroll
+                for (int e = 0; e < 2; e++) {
+                    T w = (d ? wz1 : wz0) * (a ? wx1 : wx0) * (e ? wy1 : wy0);
+                    s += xc.c[c][P2IDX(Cl, lx + a, ly + e, lz + d)] * w;
+                }
+        xf.c[c][u] += s * (c == 0 ? p1 : v1);
+    }
+}
+
+// ronurestrict (move3mgNew.c:3386-3527): coarse nu, ro as weighted averages
+// of the fine node values (nu averaged as nu, log nu or 1/nu per viscmod).
+__global__ void k_ronurestrict(int fnx, int fny, int fnz, const float *fnu, const float *fro, int cnx, int cny,
+                               int cnz, float *cnu, float *cro, AxisMap mx, AxisMap my, AxisMap mz, int viscmod)
+{
+    int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= cnx * cny * cnz) return;
+    int J = v % cny, I = (v / cny) % cnx, K = v / (cnx * cny);
+    double sn = 0, sr = 0, sw = 0;
+    for (int qz = mz.ptr[K]; qz < mz.ptr[K + 1]; qz++)
+        for (int qx = mx.ptr[I]; qx < mx.ptr[I + 1]; qx++)
+            for (int qy = my.ptr[J]; qy < my.ptr[J + 1]; qy++) {
+                int f = mz.idx[qz] * fnx * fny + mx.idx[qx] * fny + my.idx[qy];
+                double w = mz.w[qz] * mx.w[qx] * my.w[qy];
+                double nv = fnu[f];
+                double fv = viscmod == 0 ? nv : (viscmod == 1 ? log(nv) : 1.0 / nv);
+                sn += fv * w;
+                sr += (double)fro[f] * w;
+                sw += w;
+            }
+    double nv = sn / sw;
+    if (viscmod == 1) nv = exp(nv);
+    if (viscmod == 2) nv = 1.0 / nv;
+    cnu[v] = (float)nv;
+    cro[v] = (float)(sr / sw);
+}
+
+__device__ __forceinline__ double vmean(int viscmod, const double *v, int n)
+{
+    double s = 0;
+    if (viscmod == 0) {
+        for (int i = 0; i < n; i++) s += v[i];
+        return s / n;
+    }
+    if (viscmod == 1) {
+        for (int i = 0; i < n; i++) s += log(v[i]);
+        return exp(s / n);
+    }
+    for (int i = 0; i < n; i++) s += 1.0 / v[i];
+    return 1.0 / (s / n);
+}
+
+__device__ __forceinline__ double clampd(double v, double lo, double hi)
+{
+    if (v > hi) v = hi;
+    if (v < lo) v = lo;
+    return v;
+}
+
+// Per-stencil viscosities of one level, clamped to [nubeg, nuend]: level 0
+// from nxx..nyz (sxxcalc:36-38, sxycalc:433-435, ...); coarse levels from the
+// 8 cell-corner (sxx) or 2 edge-end (sxy, sxz, syz) nu values (41-47, 438-444).
+__global__ void k_level_eta(int nx, int ny, int nz, const float *nu, const float *nxx, const float *nxy,
+                            const float *nxz, const float *nyz, float *ec, float *exy, float *exz, float *eyz,
+                            double lo, double hi, int viscmod, int level0)
+{
+    int u = blockIdx.x * blockDim.x + threadIdx.x;
+    if (u >= nx * ny * nz) return;
+    if (level0) {
+        ec[u] = (float)clampd(nxx[u], lo, hi);
+        exy[u] = (float)clampd(nxy[u], lo, hi);
+        exz[u] = (float)clampd(nxz[u], lo, hi);
+        eyz[u] = (float)clampd(nyz[u], lo, hi);
+        return;
+    }
+    int j = u % ny, i = (u / ny) % nx, k = u / (nx * ny);
+    int xy = nx * ny;
+    if (i > 0 && j > 0 && k > 0) {
+        double v[8] = {nu[u - xy - ny - 1], nu[u - xy - ny], nu[u - xy - 1], nu[u - xy],
+                       nu[u - ny - 1],      nu[u - ny],      nu[u - 1],      nu[u]};
+        ec[u] = (float)clampd(vmean(viscmod, v, 8), lo, hi);
+    } else {
+        ec[u] = (float)lo;
+    }
+    double v2[2];
+    v2[0] = nu[u];
+    v2[1] = k + 1 < nz ? nu[u + xy] : nu[u];
+    exy[u] = (float)clampd(vmean(viscmod, v2, 2), lo, hi);
+    v2[1] = j + 1 < ny ? nu[u + 1] : nu[u];
+    exz[u] = (float)clampd(vmean(viscmod, v2, 2), lo, hi);
+    v2[1] = i + 1 < nx ? nu[u + ny] : nu[u];
+    eyz[u] = (float)clampd(vmean(viscmod, v2, 2), lo, hi);
+}
+
+// Level-0 right-hand sides of the Stokes rows (xstokserr:845, ystokserr:1060,
+// zstokserr:1279): -g * (sum of 4 float densities, summed in float) / 4.
+template <typename T>
+__global__ void k_rhs0(int nx, int ny, int nz, const float *ro, const uint8_t *bcm, Vec4<T> b, double gxk, double gyk,
+                       double gzk)
+{
+    int u = blockIdx.x * blockDim.x + threadIdx.x;
+    if (u >= nx * ny * nz) return;
+    int j = u % ny, i = (u / ny) % nx, k = u / (nx * ny);
+    int xy = nx * ny;
+    uint8_t m = bcm[u];
+    b.c[0][u] = 0;
+    T vx = 0, vy = 0, vz = 0;
+    if (valid_pos(1, i, j, k, nx, ny, nz) && !(m & BC_VX)) {
+        float s = ro[u] + ro[u + 1] + ro[u + xy] + ro[u + xy + 1];
+        vx = (T)(-gxk * (double)s / 4.0);
+    }
+    if (valid_pos(2, i, j, k, nx, ny, nz) && !(m & BC_VY)) {
+        float s = ro[u] + ro[u + ny] + ro[u + xy] + ro[u + xy + ny];
+        vy = (T)(-gyk * (double)s / 4.0);
+    }
+    if (valid_pos(3, i, j, k, nx, ny, nz) && !(m & BC_VZ)) {
+        float s = ro[u] + ro[u + 1] + ro[u + ny] + ro[u + ny + 1];
+        vz = (T)(-gzk * (double)s / 4.0);
+    }
+    b.c[1][u] = vx;
+    b.c[2][u] = vy;
+    b.c[3][u] = vz;
+}
+
+// Boundary-row constants into the level-0 right-hand side.
+template <typename T>
+__global__ void k_bc_consts(int nbc, const int *bu, const float *bconst, Vec4<T> b)
+{
+    int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= nbc) return;
+    int uc = bu[q];
+    b.c[uc & 3][uc >> 2] = (T)bconst[q];
+}
+
+// ---------------------------------------------------------------------------
+// Deterministic reductions: fixed grid, grid-stride, block tree, then one
+// block sums the partials in order.
+
+__device__ __forceinline__ double block_sum(double v, double *sh)
+{
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) sh[w] = v;
+    __syncthreads();
+    double s = 0;
+    if (threadIdx.x < 32) {
+        s = threadIdx.x < (blockDim.x >> 5) ? sh[threadIdx.x] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    }
+    __syncthreads();
+    return s;
+}
+
+// nd dot products of 4-field vectors: out[q] = sum a_q . b_q (pairs given by
+// pointer tables), skipping the pinned pressure cell when skip_node >= 0.
+__global__ void k_dots_partial(DotJobs jobs, int n, int skip_node, double *partial)
+{
+    __shared__ double sh[32];
+    for (int q = 0; q < jobs.nd; q++) {
+        double s = 0;
+        for (int c = 0; c < 4; c++) {
+            const double *a = jobs.j[q].a[c], *b = jobs.j[q].b[c];
+            for (int u = blockIdx.x * blockDim.x + threadIdx.x; u < n; u += gridDim.x * blockDim.x) {
+                if (c == 0 && u == skip_node) continue;
+                s += a[u] * b[u];
+            }
+        }
+        double t = block_sum(s, sh);
+        if (threadIdx.x == 0) partial[q * gridDim.x + blockIdx.x] = t;
+    }
+}
+
+__global__ void k_dots_final(int nd, int nparts, const double *partial, double *out)
+{
+    __shared__ double sh[32];
+    for (int q = 0; q < nd; q++) {
+        double s = 0;
+        for (int i = threadIdx.x; i < nparts; i += blockDim.x) s += partial[q * nparts + i];
+        double t = block_sum(s, sh);
+        if (threadIdx.x == 0) out[q] = t;
+    }
+}
+
+// Sum of volume * b_P over continuity rows and of the volumes (compatibility).
+template <typename T>
+__global__ void k_compat_partial(LevelView<T> L, const T *bp, double *partial)
+{
+    __shared__ double sh[32];
+    double s = 0, sv = 0;
+    for (int u = blockIdx.x * blockDim.x + threadIdx.x; u < L.n; u += gridDim.x * blockDim.x) {
+        int j = u % L.ny, i = (u / L.ny) % L.nx, k = u / (L.nx * L.ny);
+        if (i == 0 || j == 0 || k == 0 || (L.bcm[u] & BC_P)) continue;
+        double vol = 1.0 / ((double)L.ax.ih[i] * (double)L.ay.ih[j] * (double)L.az.ih[k]);
+        s += vol * (double)bp[u];
+        sv += vol;
+    }
+    double t = block_sum(s, sh);
+    if (threadIdx.x == 0) partial[blockIdx.x] = t;
+    t = block_sum(sv, sh);
+    if (threadIdx.x == 0) partial[gridDim.x + blockIdx.x] = t;
+}
+
+template <typename T>
+__global__ void k_compat_apply(LevelView<T> L, T *bp, const double *sums)
+{
+    int u = blockIdx.x * blockDim.x + threadIdx.x;
+    if (u >= L.n || sums[1] <= 0) return;
+    int j = u % L.ny, i = (u / L.ny) % L.nx, k = u / (L.nx * L.ny);
+    if (i == 0 || j == 0 || k == 0 || (L.bcm[u] & BC_P)) return;
+    bp[u] -= (T)(sums[0] / sums[1]);
+}
+
+// ---------------------------------------------------------------------------
+// Small vector kernels.
+__global__ void k_axpy4(int n, const double *alpha, double sign, Vec4<double> y, Vec4<double> x)
+{
+    int u = blockIdx.x * blockDim.x + threadIdx.x;
+    if (u >= n) return;
+    double a = sign * alpha[0];
+#pragma unroll
+    for (int c = 0; c < 4; c++) y.c[c][u] += a * x.c[c][u];
+}
+
+// y -= sum_q coef[q] * X_q  and  z -= sum_q coef[q] * Z_q  (classical Gram-Schmidt)
+__global__ void k_cgs_update(int n, const double *coef, Vec4<double> y, VecList X, Vec4<double> z, VecList Z)
+{
+    int u = blockIdx.x * blockDim.x + threadIdx.x;
+    if (u >= n) return;
+    for (int c = 0; c < 4; c++) {
+        double sy = y.c[c][u], sz = z.c[c][u];
+        for (int q = 0; q < X.nv; q++) {
+            sy -= coef[q] * X.v[q][c][u];
+            sz -= coef[q] * Z.v[q][c][u];
+        }
+        y.c[c][u] = sy;
+        z.c[c][u] = sz;
+    }
+}
+
+__global__ void k_f32_to_f64(int n, Vec4<float> a, Vec4<double> b)
+{
+    int u = blockIdx.x * blockDim.x + threadIdx.x;
+    if (u >= n) return;
+#pragma unroll
+    for (int c = 0; c < 4; c++) b.c[c][u] = (double)a.c[c][u];
+}
+
+// Pressure shift so that the pinned cell holds pin_value (move3mgNew.c:2834-2855).
+__global__ void k_pressure_shift_value(const double *p, int pin, double pin_value, double *shift)
+{
+    if (threadIdx.x == 0 && blockIdx.x == 0) shift[0] = pin >= 0 ? pin_value - p[pin] : 0.0;
+}
+__global__ void k_pressure_shift(int nx, int ny, int nz, double *p, const double *shift)
+{
+    int u = blockIdx.x * blockDim.x + threadIdx.x;
+    if (u >= nx * ny * nz) return;
+    int j = u % ny, i = (u / ny) % nx, k = u / (nx * ny);
+    if (i > 0 && j > 0 && k > 0) p[u] += shift[0];
+}
+
+}  // namespace p2

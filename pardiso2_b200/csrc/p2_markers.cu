@@ -1,0 +1,383 @@
+// Marker -> node interpolation (ronurecalc, pardiso/mark3mg.c:630-1133) on the
+// device, deterministic and with no floating-point atomics:
+//   1. per marker: validity (inside the box, type < 50: mark3mg.c:692) and
+//      cell (binary search on the gridlines, m1serch..m3serch 1138-1204);
+//   2. stable LSD radix sort of (cell, marker index) — own kernels;
+//   3. per cell: the [start, end) range in the sorted order;
+//   4. per node: the markers of the <= 8 adjacent cells are merged by marker
+//      index and accumulated in that order with the reference's arithmetic
+//      (float accumulators, double weights, no fused multiply-add), so the
+//      node fields equal those of the reference run on one thread.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "p2_internal.cuh"
+#include "p2_solver.h"
+
+namespace p2 {
+
+static inline unsigned nb(long n, int t = 256) { return (unsigned)((n + t - 1) / t); }
+
+__device__ __forceinline__ int serch(const double *g, int n, double x)
+{
+    int a = 0, b = n - 1, m;
+    do {
+        m = (a + b) / 2;
+        if (g[m] > x) b = m; else a = m;
+    } while (b - a > 1);
+    if (a > n - 2) a = n - 2;
+    return a;
+}
+
+__global__ void k_mark_keys(long nmark, const float *mx, const float *my, const float *mz, const signed char *mt,
+                            const double *gx, const double *gy, const double *gz, int nx, int ny, int nz,
+                            double xsize, double ysize, double zsize, unsigned sentinel, unsigned *key,
+                            unsigned *val)
+{
+    long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= nmark) return;
+    float x = mx[q], y = my[q], z = mz[q];
+    int t = mt[q];
+    unsigned kk = sentinel;
+    if (x > 0 && y > 0 && z > 0 && (double)x < xsize && (double)y < ysize && (double)z < zsize && t < 50) {
+        int c1 = serch(gx, nx, (double)x), c2 = serch(gy, ny, (double)y), c3 = serch(gz, nz, (double)z);
+        kk = (unsigned)c3 * (unsigned)((nx - 1) * (ny - 1)) + (unsigned)c1 * (unsigned)(ny - 1) + (unsigned)c2;
+    }
+    key[q] = kk;
+    val[q] = (unsigned)q;
+}
+
+// ---------------------------------------------------------------------------
+// Stable LSD radix sort, 8-bit digits.  A tile of kTile keys per block of 256
+// threads (8 warps x 16 chunks of 32); per pass: tile histograms, exclusive
+// scan in digit-major order, stable scatter (warp match + running counters).
+constexpr int kRadixBits = 8, kBuckets = 256, kChunks = 16, kTile = 8 * kChunks * 32;
+
+__global__ void k_radix_hist(long n, const unsigned *key, int shift, unsigned *hist, int ntiles)
+{
+    __shared__ unsigned h[kBuckets];
+    for (int i = threadIdx.x; i < kBuckets; i += blockDim.x) h[i] = 0;
+    __syncthreads();
+    long base = (long)blockIdx.x * kTile;
+    for (int i = threadIdx.x; i < kTile; i += blockDim.x) {
+        long q = base + i;
+        if (q < n) atomicAdd(&h[(key[q] >> shift) & (kBuckets - 1)], 1u);
+    }
+    __syncthreads();
+    for (int d = threadIdx.x; d < kBuckets; d += blockDim.x) hist[(long)d * ntiles + blockIdx.x] = h[d];
+}
+
+// exclusive scan of hist (kBuckets * ntiles entries) in one block
+__global__ void k_radix_scan(unsigned *hist, long len)
+{
+    __shared__ unsigned long long carry;
+    __shared__ unsigned long long part[1024];
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (long base = 0; base < len; base += 1024) {
+        long q = base + threadIdx.x;
+        unsigned long long v = q < len ? hist[q] : 0;
+        part[threadIdx.x] = v;
+        __syncthreads();
+        for (int o = 1; o < 1024; o <<= 1) {
+            unsigned long long t = threadIdx.x >= o ? part[threadIdx.x - o] : 0;
+            __syncthreads();
+            part[threadIdx.x] += t;
+            __syncthreads();
+        }
+        unsigned long long incl = part[threadIdx.x];
+        if (q < len) hist[q] = (unsigned)(carry + incl - v);
+        __syncthreads();
+        if (threadIdx.x == 1023) carry += incl;
+        __syncthreads();
+    }
+}
+
+__global__ void k_radix_scatter(long n, const unsigned *key, const unsigned *val, unsigned *key2, unsigned *val2,
+                                int shift, const unsigned *offs, int ntiles)
+{
+    __shared__ unsigned wcnt[8][kBuckets];   // per-warp digit counts, then exclusive offsets
+    __shared__ unsigned boff[kBuckets];
+    int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int i = threadIdx.x; i < 8 * kBuckets; i += blockDim.x) (&wcnt[0][0])[i] = 0;
+    for (int d = threadIdx.x; d < kBuckets; d += blockDim.x) boff[d] = offs[(long)d * ntiles + blockIdx.x];
+    __syncthreads();
+    long wbase = (long)blockIdx.x * kTile + (long)w * kChunks * 32;
+    // pass 1: per-warp counts
+    for (int ch = 0; ch < kChunks; ch++) {
+        long q = wbase + ch * 32 + lane;
+        bool ok = q < n;
+        unsigned d = ok ? (key[q] >> shift) & (kBuckets - 1) : 0xffffffffu;
+        unsigned peers = __match_any_sync(0xffffffffu, d);
+        if (ok && lane == __ffs(peers) - 1) wcnt[w][d] += __popc(peers);
+        __syncwarp();
+    }
+    __syncthreads();
+    // exclusive prefix over warps per digit
+    for (int d = threadIdx.x; d < kBuckets; d += blockDim.x) {
+        unsigned s = boff[d];
+        for (int ww = 0; ww < 8; ww++) {
+            unsigned c = wcnt[ww][d];
+            wcnt[ww][d] = s;
+            s += c;
+        }
+    }
+    __syncthreads();
+    // pass 2: stable placement
+    for (int ch = 0; ch < kChunks; ch++) {
+        long q = wbase + ch * 32 + lane;
+        bool ok = q < n;
+        unsigned kk = ok ? key[q] : 0, vv = ok ? val[q] : 0;
+        unsigned d = ok ? (kk >> shift) & (kBuckets - 1) : 0xffffffffu;
+        unsigned peers = __match_any_sync(0xffffffffu, d);
+        unsigned lt = peers & ((1u << lane) - 1u);
+        unsigned pos = 0;
+        if (ok) pos = wcnt[w][d] + __popc(lt);
+        __syncwarp();
+        if (ok && lane == __ffs(peers) - 1) wcnt[w][d] += __popc(peers);
+        __syncwarp();
+        if (ok) { key2[pos] = kk; val2[pos] = vv; }
+    }
+}
+
+// cell ranges from the sorted keys (cells without markers keep [0, 0))
+__global__ void k_cell_bounds(long n, const unsigned *key, unsigned sentinel, int *start, int *end)
+{
+    long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n) return;
+    unsigned k = key[q];
+    if (k == sentinel) return;
+    if (q == 0 || key[q - 1] != k) start[k] = (int)q;
+    if (q == n - 1 || key[q + 1] != k) end[k] = (int)(q + 1);
+}
+
+__global__ void k_permute(long n, const unsigned *idx, const float *mx, const float *my, const float *mz,
+                          const signed char *mt, float4 *sorted)
+{
+    long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n) return;
+    unsigned m = idx[q];
+    sorted[q] = make_float4(mx[m], my[m], mz[m], __int_as_float((int)mt[m]));
+}
+
+// ---------------------------------------------------------------------------
+struct Rock {
+    double nu, ro;  // clamped viscosity, density
+};
+
+__global__ void k_node_gather(int nx, int ny, int nz, const double *gx, const double *gy, const double *gz,
+                              const int *start, const int *end, const unsigned *idx, const float4 *mk,
+                              const double *rock_f, const double *rock_ro, double nukoef, int viscmod,
+                              double nubeg, double nuend, float *nu, float *ro, float *nxx, float *nxy, float *nxz,
+                              float *nyz)
+{
+    int u = blockIdx.x * blockDim.x + threadIdx.x;
+    if (u >= nx * ny * nz) return;
+    int m2 = u % ny, m1 = (u / ny) % nx, m3 = u / (nx * ny);
+    int nx1 = nx - 1, ny1 = ny - 1;
+    // the up-to-8 adjacent cells and their cursors
+    int cur[8], lim[8], cz[8], cx[8], cy[8], nc = 0;
+    for (int a = 0; a < 2; a++)
+        for (int b = 0; b < 2; b++)
+            for (int c = 0; c < 2; c++) {
+                int c3 = m3 - 1 + a, c1 = m1 - 1 + b, c2 = m2 - 1 + c;
+                if (c3 < 0 || c1 < 0 || c2 < 0 || c3 >= nz - 1 || c1 >= nx - 1 || c2 >= ny - 1) continue;
+                int cell = c3 * nx1 * ny1 + c1 * ny1 + c2;
+                int s = start[cell], e = end[cell];
+                if (s >= e) continue;
+                cur[nc] = s; lim[nc] = e; cz[nc] = c3; cx[nc] = c1; cy[nc] = c2;
+                nc++;
+            }
+    // float accumulators (the reference's per-thread float buffers) and double weights
+    float aN = 0.f, aR = 0.f, aXX = 0.f, aXY = 0.f, aXZ = 0.f, aYZ = 0.f;
+    double wN = 0, wR = 0, wXX = 0, wXY = 0, wXZ = 0, wYZ = 0;
+    const double gxm = gx[m1], gym = gy[m2], gzm = gz[m3];
+    for (;;) {
+        int best = -1;
+        unsigned bidx = 0xffffffffu;
+        for (int q = 0; q < nc; q++)
+            if (cur[q] < lim[q]) {
+                unsigned v = idx[cur[q]];
+                if (v < bidx) { bidx = v; best = q; }
+            }
+        if (best < 0) break;
+        float4 m = mk[cur[best]];
+        cur[best]++;
+        int t = __float_as_int(m.w);
+        int m10 = cx[best], m20 = cy[best], m30 = cz[best];
+        double dx = __dsub_rn(gx[m10 + 1], gx[m10]);
+        double dy = __dsub_rn(gy[m20 + 1], gy[m20]);
+        double dz = __dsub_rn(gz[m30 + 1], gz[m30]);
+        double ddz = __dsub_rn(1.0, fabs(__ddiv_rn(__dsub_rn(gzm, (double)m.z), dz)));
+        double ddx = __dsub_rn(1.0, fabs(__ddiv_rn(__dsub_rn(gxm, (double)m.x), dx)));
+        double ddy = __dsub_rn(1.0, fabs(__ddiv_rn(__dsub_rn(gym, (double)m.y), dy)));
+        double swt = __dmul_rn(__dmul_rn(ddx, ddy), ddz);
+        double f = rock_f[t];
+        if (ddx > nukoef && ddy > nukoef && ddz > nukoef) {
+            aN = __double2float_rn(__dadd_rn((double)aN, __dmul_rn(f, swt)));
+            wN = __dadd_rn(wN, swt);
+        }
+        if (m1 > m10 && m2 > m20 && m3 > m30) {
+            double s1 = __dmul_rn(__dmul_rn(__dmul_rn(8.0, __dsub_rn(0.5, fabs(__dsub_rn(ddx, 0.5)))),
+                                            __dsub_rn(0.5, fabs(__dsub_rn(ddy, 0.5)))),
+                                  __dsub_rn(0.5, fabs(__dsub_rn(ddz, 0.5))));
+            aXX = __double2float_rn(__dadd_rn((double)aXX, __dmul_rn(f, s1)));
+            wXX = __dadd_rn(wXX, s1);
+        }
+        if (m3 == m30 && ddx > 0.5 && ddy > 0.5) {
+            double s1 = __dmul_rn(__dmul_rn(__dmul_rn(8.0, __dsub_rn(ddx, 0.5)), __dsub_rn(ddy, 0.5)),
+                                  __dsub_rn(0.5, fabs(__dsub_rn(ddz, 0.5))));
+            aXY = __double2float_rn(__dadd_rn((double)aXY, __dmul_rn(f, s1)));
+            wXY = __dadd_rn(wXY, s1);
+        }
+        if (m2 == m20 && ddx > 0.5 && ddz > 0.5) {
+            double s1 = __dmul_rn(__dmul_rn(__dmul_rn(8.0, __dsub_rn(ddx, 0.5)),
+                                            __dsub_rn(0.5, fabs(__dsub_rn(ddy, 0.5)))),
+                                  __dsub_rn(ddz, 0.5));
+            aXZ = __double2float_rn(__dadd_rn((double)aXZ, __dmul_rn(f, s1)));
+            wXZ = __dadd_rn(wXZ, s1);
+        }
+        if (m1 == m10 && ddy > 0.5 && ddz > 0.5) {
+            double s1 = __dmul_rn(__dmul_rn(__dmul_rn(8.0, __dsub_rn(0.5, fabs(__dsub_rn(ddx, 0.5)))),
+                                            __dsub_rn(ddy, 0.5)),
+                                  __dsub_rn(ddz, 0.5));
+            aYZ = __double2float_rn(__dadd_rn((double)aYZ, __dmul_rn(f, s1)));
+            wYZ = __dadd_rn(wYZ, s1);
+        }
+        if (ddx > 0.5 && ddy > 0.5 && ddz > 0.5) {
+            double s1 = __dmul_rn(__dmul_rn(__dmul_rn(8.0, __dsub_rn(ddx, 0.5)), __dsub_rn(ddy, 0.5)),
+                                  __dsub_rn(ddz, 0.5));
+            aR = __double2float_rn(__dadd_rn((double)aR, __dmul_rn(rock_ro[t], s1)));
+            wR = __dadd_rn(wR, s1);
+        }
+    }
+    // normalise (mark3mg.c:958-1014), keep old values where no marker contributed, clamp viscosities
+    auto fin = [&](float a, double w, float old) -> float {
+        if (!(w > 0)) return old;
+        float v = __double2float_rn(__ddiv_rn((double)a, w));
+        if (viscmod == 1) v = __double2float_rn(exp((double)v));
+        if (viscmod == 2) v = __double2float_rn(__ddiv_rn(1.0, (double)v));
+        return v;
+    };
+    auto clampf = [&](float v) -> float {
+        if ((double)v < nubeg) v = __double2float_rn(nubeg);
+        if ((double)v > nuend) v = __double2float_rn(nuend);
+        return v;
+    };
+    nu[u] = clampf(fin(aN, wN, nu[u]));
+    nxx[u] = clampf(fin(aXX, wXX, nxx[u]));
+    nxy[u] = clampf(fin(aXY, wXY, nxy[u]));
+    nxz[u] = clampf(fin(aXZ, wXZ, nxz[u]));
+    nyz[u] = clampf(fin(aYZ, wYZ, nyz[u]));
+    if (wR > 0) ro[u] = __double2float_rn(__ddiv_rn((double)aR, wR));
+}
+
+// ---------------------------------------------------------------------------
+void Solver::upload_markers(long nmark, const float *mx, const float *my, const float *mz, const signed char *mt,
+                            int nrock, const double *n0, const double *n1, const double *rho)
+{
+    if (!grid_ready) throw Error(P2_ERR_STATE, "markers before p2_set_grid");
+    if (nmark < 0 || nmark > 0x7fffffffL) throw Error(P2_ERR_ARG, "marker count out of range");
+    if (nrock <= 0 || nrock > 256) throw Error(P2_ERR_ARG, "rock table size out of range");
+    // constant per-type viscosity (viscalc, mark3mg.c:1481-1482) and density (dencalc1, 1429)
+    std::vector<double> f(256, 1.0), r(256, 0.0);
+    for (int t = 0; t < nrock && t < 50; t++) {
+        if (n0[t] != n1[t])
+            throw Error(P2_ERR_UNSUPPORTED, "rock type " + std::to_string(t) +
+                                                " has a power-law viscosity (markn0 != markn1)");
+        double mnu = n0[t];
+        if (mnu < prm.nubeg) mnu = prm.nubeg;
+        if (mnu > prm.nuend) mnu = prm.nuend;
+        f[t] = prm.viscmod == 0 ? mnu : (prm.viscmod == 1 ? std::log(mnu) : 1.0 / mnu);
+        r[t] = rho[t];
+    }
+    // every marker with type < 50 must have a rock entry
+    marker_arena.release();
+    nmk = nmark;
+    long cap = std::max<long>(nmark, 1);
+    mk_x = (float *)marker_arena.alloc(sizeof(float) * cap);
+    mk_y = (float *)marker_arena.alloc(sizeof(float) * cap);
+    mk_z = (float *)marker_arena.alloc(sizeof(float) * cap);
+    mk_t = (signed char *)marker_arena.alloc(cap);
+    if (nmark) {
+        P2_CUDA_TRY(cudaMemcpyAsync(mk_x, mx, sizeof(float) * nmark, cudaMemcpyHostToDevice, st));
+        P2_CUDA_TRY(cudaMemcpyAsync(mk_y, my, sizeof(float) * nmark, cudaMemcpyHostToDevice, st));
+        P2_CUDA_TRY(cudaMemcpyAsync(mk_z, mz, sizeof(float) * nmark, cudaMemcpyHostToDevice, st));
+        P2_CUDA_TRY(cudaMemcpyAsync(mk_t, mt, nmark, cudaMemcpyHostToDevice, st));
+    }
+    for (long q = 0; q < nmark; q++)
+        if (mt[q] < 50 && (mt[q] < 0 || mt[q] >= nrock)) throw Error(P2_ERR_ARG, "marker type without rock entry");
+    rock_f = (double *)marker_arena.alloc(sizeof(double) * 256);
+    rock_ro = (double *)marker_arena.alloc(sizeof(double) * 256);
+    P2_CUDA_TRY(cudaMemcpy(rock_f, f.data(), sizeof(double) * 256, cudaMemcpyHostToDevice));
+    P2_CUDA_TRY(cudaMemcpy(rock_ro, r.data(), sizeof(double) * 256, cudaMemcpyHostToDevice));
+    // sort and node buffers
+    int ntiles = (int)((cap + kTile - 1) / kTile);
+    mk_key[0] = (unsigned *)marker_arena.alloc(sizeof(unsigned) * cap);
+    mk_key[1] = (unsigned *)marker_arena.alloc(sizeof(unsigned) * cap);
+    mk_val[0] = (unsigned *)marker_arena.alloc(sizeof(unsigned) * cap);
+    mk_val[1] = (unsigned *)marker_arena.alloc(sizeof(unsigned) * cap);
+    mk_hist = (unsigned *)marker_arena.alloc(sizeof(unsigned) * (size_t)kBuckets * ntiles);
+    mk_sorted = (float4 *)marker_arena.alloc(sizeof(float4) * cap);
+    const Level &L0 = L[0];
+    long ncell = (long)(L0.nx - 1) * (L0.ny - 1) * (L0.nz - 1);
+    cell_start = (int *)marker_arena.alloc(sizeof(int) * ncell);
+    cell_end = (int *)marker_arena.alloc(sizeof(int) * ncell);
+    d_g[0] = (double *)marker_arena.alloc(sizeof(double) * L0.nx);
+    d_g[1] = (double *)marker_arena.alloc(sizeof(double) * L0.ny);
+    d_g[2] = (double *)marker_arena.alloc(sizeof(double) * L0.nz);
+    for (int q = 0; q < 3; q++)
+        P2_CUDA_TRY(cudaMemcpy(d_g[q], L0.g[q].data(), sizeof(double) * L0.g[q].size(), cudaMemcpyHostToDevice));
+    for (int q = 0; q < 6; q++) mk_nodes[q] = (float *)marker_arena.alloc(sizeof(float) * L0.n);
+    markers_ready = true;
+}
+
+// Node fields in/out are mk_nodes[0..5] = nu, ro, nxx, nxy, nxz, nyz.
+void Solver::ronurecalc_device()
+{
+    if (!markers_ready) throw Error(P2_ERR_STATE, "ronurecalc before markers were uploaded");
+    const Level &L0 = L[0];
+    long n = nmk;
+    long ncell = (long)(L0.nx - 1) * (L0.ny - 1) * (L0.nz - 1);
+    unsigned sentinel = (unsigned)ncell;
+    int bits = 1;
+    while ((1ul << bits) <= (unsigned long)sentinel) bits++;
+    int passes = (bits + kRadixBits - 1) / kRadixBits;
+    double xsize = L0.g[0].back() - L0.g[0].front(), ysize = L0.g[1].back() - L0.g[1].front(),
+           zsize = L0.g[2].back() - L0.g[2].front();
+    P2_CUDA_TRY(cudaMemsetAsync(cell_start, 0, sizeof(int) * ncell, st));
+    P2_CUDA_TRY(cudaMemsetAsync(cell_end, 0, sizeof(int) * ncell, st));
+    if (n > 0) {
+        k_mark_keys<<<nb(n), 256, 0, st>>>(n, mk_x, mk_y, mk_z, mk_t, d_g[0], d_g[1], d_g[2], L0.nx, L0.ny, L0.nz,
+                                           xsize, ysize, zsize, sentinel, mk_key[0], mk_val[0]); P2_COUNT_LAUNCH();
+        int ntiles = (int)((n + kTile - 1) / kTile);
+        int a = 0;
+        for (int p = 0; p < passes; p++) {
+            int shift = p * kRadixBits;
+            k_radix_hist<<<ntiles, 256, 0, st>>>(n, mk_key[a], shift, mk_hist, ntiles); P2_COUNT_LAUNCH();
+            k_radix_scan<<<1, 1024, 0, st>>>(mk_hist, (long)kBuckets * ntiles); P2_COUNT_LAUNCH();
+            k_radix_scatter<<<ntiles, 256, 0, st>>>(n, mk_key[a], mk_val[a], mk_key[1 - a], mk_val[1 - a], shift,
+                                                    mk_hist, ntiles); P2_COUNT_LAUNCH();
+            a = 1 - a;
+        }
+        mk_cur = a;
+        k_cell_bounds<<<nb(n), 256, 0, st>>>(n, mk_key[a], sentinel, cell_start, cell_end); P2_COUNT_LAUNCH();
+        k_permute<<<nb(n), 256, 0, st>>>(n, mk_val[a], mk_x, mk_y, mk_z, mk_t, mk_sorted); P2_COUNT_LAUNCH();
+    }
+    k_node_gather<<<nb(L0.n, 128), 128, 0, st>>>(L0.nx, L0.ny, L0.nz, d_g[0], d_g[1], d_g[2], cell_start, cell_end,
+                                            mk_val[mk_cur], mk_sorted, rock_f, rock_ro, prm.nukoef, prm.viscmod,
+                                            prm.nubeg, prm.nuend, mk_nodes[0], mk_nodes[1], mk_nodes[2],
+                                            mk_nodes[3], mk_nodes[4], mk_nodes[5]); P2_COUNT_LAUNCH();
+    P2_CUDA_TRY(cudaGetLastError());
+    // the result becomes the solver's resident node fields
+    if (bc_ready) {
+        float *dst[6] = {L[0].nu, L[0].ro, f0.nxx, f0.nxy, f0.nxz, f0.nyz};
+        for (int q = 0; q < 6; q++)
+            P2_CUDA_TRY(cudaMemcpyAsync(dst[q], mk_nodes[q], sizeof(float) * L0.n, cudaMemcpyDeviceToDevice, st));
+        nodes_ready = true;
+    }
+}
+
+}  // namespace p2

@@ -1,0 +1,1105 @@
+// Host side of the p2cuda Stokes multigrid: level set-up, boundary tables,
+// transfer tables, the V-cycle (FP32 or FP64) and the FP64 outer loop.
+//
+// Solve structure (move3mgNew.c:1791 vpiterate is the reference entry point):
+//   outer FP64 GCR on the level-0 system, each iteration: true residual
+//   r = b - A x in FP64, z = V(r) one V-cycle (FP32 in mixed mode), q = A z,
+//   Gram-Schmidt against the previous directions, x += alpha z.
+//   V-cycle: on levels 0..L-1 cell-block smoothing + residual + restriction
+//   (vprestrict), dense inverse on the coarsest level (replaces PARDISO),
+//   prolongation (vpprolong) + smoothing back up.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "p2_kernels.cuh"
+#include "p2_solver.h"
+
+namespace p2 {
+
+int dense_lu_inverse(cudaStream_t st, double *A, int n, double *Ainv, int *d_ipiv, int *d_info);
+void d2f(cudaStream_t st, size_t n, const double *a, float *b);
+
+static inline unsigned nblk(long n, int t = kThreads) { return (unsigned)((n + t - 1) / t); }
+
+void *DeviceArena::alloc(size_t bytes)
+{
+    void *p = nullptr;
+    if (bytes == 0) bytes = 16;
+    cudaError_t e = cudaMalloc(&p, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        throw Error(P2_ERR_NOMEM, "cudaMalloc of " + std::to_string(bytes) + " bytes failed");
+    }
+    ptrs.push_back(p);
+    P2_CUDA_TRY(cudaMemset(p, 0, bytes));
+    return p;
+}
+void DeviceArena::release()
+{
+    for (void *p : ptrs) cudaFree(p);
+    ptrs.clear();
+}
+
+// ---------------------------------------------------------------------------
+// Transfer tables along one axis (oracle p2oracle.c axis_node/axis_mid/
+// axis_cell; reference move3mgNew.c:3562-3575 and the Vy/Vz/P blocks).
+static int cmin_common(int m, int nf, int nc)
+{
+    int r = (m - 2) / 2 + 2;
+    if (m < 3) r = m;
+    if (m > nf - 4) r = nc - (nf - m);
+    return r;
+}
+
+static void axis_table(const std::vector<double> &gf, const std::vector<double> &gc, int type, HostAxis &t)
+{
+    int nf = (int)gf.size(), nc = (int)gc.size();
+    t.lo.assign(nf, 0);
+    t.w0.assign(nf, 0.0);
+    t.w1.assign(nf, 0.0);
+    int m0 = 0, m1 = nf;
+    if (type == 1) m1 = nf - 1;   // mid-located: 0..nf-2
+    if (type == 2) m0 = 1;        // pressure cell: 1..nf-1
+    std::vector<std::vector<std::pair<int, double>>> inv(nc);
+    for (int m = m0; m < m1; m++) {
+        int lo = cmin_common(m, nf, nc);
+        double w0, w1;
+        if (type == 0) {
+            if (lo > nc - 2) lo = nc - 2;
+            double d = gc[lo + 1] - gc[lo];
+            w0 = 1.0 + (gc[lo] - gf[m]) / d;
+            w1 = 1.0 - (gc[lo + 1] - gf[m]) / d;
+        } else if (type == 1) {
+            if (lo > nc - 3) lo = nc - 3;
+            if ((gf[m] + gf[m + 1]) / 2.0 < (gc[lo] + gc[lo + 1]) / 2.0 && lo > 0) lo -= 1;
+            double d = (gc[lo + 2] - gc[lo]) / 2.0, xf = gf[m] + gf[m + 1];
+            w0 = 1.0 + (gc[lo] + gc[lo + 1] - xf) / 2.0 / d;
+            w1 = 1.0 - (gc[lo + 1] + gc[lo + 2] - xf) / 2.0 / d;
+        } else {
+            if (lo > nc - 2) lo = nc - 2;
+            if ((gf[m] + gf[m - 1]) / 2.0 < (gc[lo] + gc[lo - 1]) / 2.0 && lo > 1) lo -= 1;
+            double d = (gc[lo + 1] - gc[lo - 1]) / 2.0, xf = gf[m] + gf[m - 1];
+            w0 = 1.0 + (gc[lo] + gc[lo - 1] - xf) / 2.0 / d;
+            w1 = 1.0 - (gc[lo + 1] + gc[lo] - xf) / 2.0 / d;
+        }
+        t.lo[m] = lo;
+        t.w0[m] = w0;
+        t.w1[m] = w1;
+        inv[lo].push_back({m, w0});
+        inv[lo + 1].push_back({m, w1});
+    }
+    t.ptr.assign(nc + 1, 0);
+    t.idx.clear();
+    t.w.clear();
+    for (int I = 0; I < nc; I++) {
+        for (auto &pr : inv[I]) { t.idx.push_back(pr.first); t.w.push_back(pr.second); }
+        t.ptr[I + 1] = (int)t.idx.size();
+    }
+}
+
+// ronurestrict weights 1 - |x_c - x_f| / dx (move3mgNew.c:3442-3484)
+static void axis_table_ronu(const std::vector<double> &gf, const std::vector<double> &gc, HostAxis &t)
+{
+    int nf = (int)gf.size(), nc = (int)gc.size();
+    std::vector<std::vector<std::pair<int, double>>> inv(nc);
+    t.lo.assign(nf, 0);
+    t.w0.assign(nf, 0.0);
+    t.w1.assign(nf, 0.0);
+    for (int m = 0; m < nf; m++) {
+        int lo = cmin_common(m, nf, nc);
+        if (lo > nc - 2) lo = nc - 2;
+        double d = gc[lo + 1] - gc[lo];
+        double w0 = 1.0 - std::fabs((gc[lo] - gf[m]) / d);
+        double w1 = 1.0 - std::fabs((gc[lo + 1] - gf[m]) / d);
+        t.lo[m] = lo;
+        t.w0[m] = w0;
+        t.w1[m] = w1;
+        inv[lo].push_back({m, w0});
+        inv[lo + 1].push_back({m, w1});
+    }
+    t.ptr.assign(nc + 1, 0);
+    t.idx.clear();
+    t.w.clear();
+    for (int I = 0; I < nc; I++) {
+        for (auto &pr : inv[I]) { t.idx.push_back(pr.first); t.w.push_back(pr.second); }
+        t.ptr[I + 1] = (int)t.idx.size();
+    }
+}
+
+template <typename V>
+static V *upload(DeviceArena &A, const std::vector<V> &h)
+{
+    V *d = (V *)A.alloc(sizeof(V) * std::max<size_t>(h.size(), 1));
+    if (!h.empty()) P2_CUDA_TRY(cudaMemcpy(d, h.data(), sizeof(V) * h.size(), cudaMemcpyHostToDevice));
+    return d;
+}
+
+static AxisMap upload_axis(DeviceArena &A, const HostAxis &h)
+{
+    AxisMap m;
+    m.lo = upload(A, h.lo);
+    m.w0 = upload(A, h.w0);
+    m.w1 = upload(A, h.w1);
+    m.ptr = upload(A, h.ptr);
+    m.idx = upload(A, h.idx);
+    m.w = upload(A, h.w);
+    return m;
+}
+
+// ---------------------------------------------------------------------------
+Solver::Solver(int device) : dev(device)
+{
+    P2_CUDA_TRY(cudaSetDevice(dev));
+    P2_CUDA_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    for (int i = 0; i < 8; i++) P2_CUDA_TRY(cudaEventCreate(&ev[i]));
+}
+
+Solver::~Solver()
+{
+    cudaSetDevice(dev);
+    drop_graphs();
+    arena.release();
+    grid_arena.release();
+    marker_arena.release();
+    for (int i = 0; i < 8; i++) cudaEventDestroy(ev[i]);
+    if (st) cudaStreamDestroy(st);
+}
+
+void Solver::drop_graphs()
+{
+    for (auto &g : graphs) {
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+        g.exec = nullptr;
+    }
+}
+
+template <typename T>
+LevelView<T> Solver::view(int l, bool raw_clamp) const
+{
+    const Level &Lv = L[l];
+    LevelView<T> v;
+    v.nx = Lv.nx; v.ny = Lv.ny; v.nz = Lv.nz; v.n = Lv.n;
+    const T *tab = (const T *)(std::is_same<T, double>::value ? (const void *)Lv.tabd : (const void *)Lv.tabf);
+    int mx = Lv.tabstride;
+    v.ax = Axis<T>{tab + 0 * mx, tab + 1 * mx, tab + 2 * mx, tab + 3 * mx};
+    v.ay = Axis<T>{tab + 4 * mx, tab + 5 * mx, tab + 6 * mx, tab + 7 * mx};
+    v.az = Axis<T>{tab + 8 * mx, tab + 9 * mx, tab + 10 * mx, tab + 11 * mx};
+    if (raw_clamp) {
+        v.ec = f0.nxx; v.exy = f0.nxy; v.exz = f0.nxz; v.eyz = f0.nyz;
+        v.do_clamp = 1;
+    } else {
+        v.ec = Lv.ec; v.exy = Lv.exy; v.exz = Lv.exz; v.eyz = Lv.eyz;
+        v.do_clamp = 0;
+    }
+    v.clamp_lo = prm.nubeg;
+    v.clamp_hi = prm.nuend;
+    v.bcm = Lv.bcm;
+    v.pin = Lv.pin;
+    return v;
+}
+
+void Solver::set_grid(long nx, long ny, long nz, const double *gx, const double *gy, const double *gz,
+                      const p2_params &p)
+{
+    if (nx < 8 || ny < 8 || nz < 8) throw Error(P2_ERR_ARG, "grid too small (need >= 8 nodes per axis)");
+    if ((double)nx * ny * nz * 4.0 > 2.0e9) throw Error(P2_ERR_ARG, "grid too large for 32-bit unknown indices");
+    if (p.multinum < 0 || p.multinum + 1 > P2_MAX_LEVELS) throw Error(P2_ERR_ARG, "multinum out of range");
+    if (p.p2koef != 0.0) throw Error(P2_ERR_UNSUPPORTED, "p2koef != 0 (grad-div term) is not supported");
+    drop_graphs();
+    arena.release();
+    grid_arena.release();
+    prm = p;
+    bc_ready = nodes_ready = false;
+    L.clear();
+    int nl = p.multinum + 1;
+    L.resize(nl);
+    long off = 0;
+    std::vector<double> g0[3] = {std::vector<double>(gx, gx + nx), std::vector<double>(gy, gy + ny),
+                                 std::vector<double>(gz, gz + nz)};
+    for (int q = 0; q < 3; q++)
+        for (size_t i = 1; i < g0[q].size(); i++)
+            if (!(g0[q][i] > g0[q][i - 1])) throw Error(P2_ERR_ARG, "gridlines must increase strictly");
+    for (int l = 0; l < nl; l++) {
+        Level &Lv = L[l];
+        if (l == 0) { Lv.nx = (int)nx; Lv.ny = (int)ny; Lv.nz = (int)nz; }
+        else {
+            Lv.nx = (L[l - 1].nx - 5) / 2 + 5;
+            Lv.ny = (L[l - 1].ny - 5) / 2 + 5;
+            Lv.nz = (L[l - 1].nz - 5) / 2 + 5;
+        }
+        if (Lv.nx < 6 || Lv.ny < 6 || Lv.nz < 6) throw Error(P2_ERR_ARG, "too many levels for this grid");
+        Lv.n = Lv.nx * Lv.ny * Lv.nz;
+        Lv.off = off;
+        off += Lv.n;
+        int s = 1 << l;
+        // gridcheck(): outer three lines copied, interior (n2-2)*2^l+2 (load3mg.c:2079-2194)
+        for (int q = 0; q < 3; q++) {
+            int n = q == 0 ? Lv.nx : q == 1 ? Lv.ny : Lv.nz;
+            const std::vector<double> &g = g0[q];
+            int nf = (int)g.size();
+            std::vector<double> &o = Lv.g[q];
+            o.assign(n, 0.0);
+            o[0] = g[0]; o[1] = g[1]; o[2] = g[2];
+            o[n - 1] = g[nf - 1]; o[n - 2] = g[nf - 2]; o[n - 3] = g[nf - 3];
+            for (int n2 = 3; n2 < n - 3; n2++) o[n2] = g[(n2 - 2) * s + 2];
+        }
+        // spacing tables, 12 arrays of stride max(n)
+        int mx = std::max(Lv.nx, std::max(Lv.ny, Lv.nz));
+        Lv.tabstride = mx;
+        std::vector<double> td(12 * mx, 0.0);
+        for (int q = 0; q < 3; q++) {
+            const std::vector<double> &g = Lv.g[q];
+            int n = (int)g.size();
+            double *ih = &td[(4 * q + 0) * mx], *ihc = &td[(4 * q + 1) * mx], *ihe = &td[(4 * q + 2) * mx],
+                   *ihv = &td[(4 * q + 3) * mx];
+            for (int i = 1; i < n; i++) ih[i] = 1.0 / (g[i] - g[i - 1]);
+            for (int i = 1; i < n - 1; i++) { ihc[i] = 2.0 / (g[i + 1] - g[i - 1]); ihe[i] = 1.0 / (g[i + 1] - g[i - 1]); }
+            for (int i = 0; i < n - 1; i++) ihv[i] = 1.0 / (g[i + 1] - g[i]);
+        }
+        std::vector<float> tf(td.begin(), td.end());
+        Lv.tabd = upload(grid_arena, td);
+        Lv.tabf = upload(grid_arena, tf);
+    }
+    total_nodes = off;
+    // transfer tables between consecutive levels
+    for (int l = 0; l + 1 < nl; l++) {
+        Level &F = L[l], &Cl = L[l + 1];
+        for (int q = 0; q < 3; q++) {
+            for (int t = 0; t < 3; t++) {
+                HostAxis h;
+                axis_table(F.g[q], Cl.g[q], t, h);
+                F.tv.m[q][t] = upload_axis(grid_arena, h);
+            }
+            HostAxis hr;
+            axis_table_ronu(F.g[q], Cl.g[q], hr);
+            F.ronu[q] = upload_axis(grid_arena, hr);
+        }
+    }
+    grid_ready = true;
+}
+
+void Solver::set_bc(const int *bondm, long bondm_len, const float *bondv1, const int *bondn1, long bondnum)
+{
+    if (!grid_ready) throw Error(P2_ERR_STATE, "p2_set_bc before p2_set_grid");
+    if (bondm_len < 4 * total_nodes) throw Error(P2_ERR_ARG, "bondm shorter than 4 * (sum of level nodes)");
+    drop_graphs();
+    arena.release();
+    for (size_t l = 0; l < L.size(); l++) {
+        Level &Lv = L[l];
+        std::vector<uint8_t> m(Lv.n, 0);
+        Lv.pin = -1;
+        Lv.pinval = 0.0;
+        int npin = 0, pin_node = -1;
+        double pin_value = 0;
+        // rows of this level: (unknown, const, koef, target unknown or -1)
+        struct Row { int uc; float cst, k; int t; };
+        std::vector<Row> rows;
+        std::map<int, int> row_of;  // uc -> row index
+        for (int u = 0; u < Lv.n; u++)
+            for (int c = 0; c < 4; c++) {
+                long gidx = (Lv.off + u) * 4 + c;
+                int bi = bondm[gidx];
+                if (!bi) continue;
+                if (bi < 0 || bi > bondnum) throw Error(P2_ERR_ARG, "bondm entry out of range");
+                int j = u % Lv.ny, i = (u / Lv.ny) % Lv.nx, k = u / (Lv.nx * Lv.ny);
+                if (!valid_pos(c, i, j, k, Lv.nx, Lv.ny, Lv.nz)) continue;  // no equation there
+                Row r;
+                r.uc = u * 4 + c;
+                r.cst = bondv1[2 * bi];
+                r.k = bondv1[2 * bi + 1];
+                r.t = -1;
+                long tg = bondn1[bi];
+                if (tg) {
+                    tg -= 1;
+                    long tn = tg / 4 - Lv.off;
+                    if (tn < 0 || tn >= Lv.n) throw Error(P2_ERR_ARG, "boundary row couples across levels");
+                    r.t = (int)(tn * 4 + tg % 4);
+                } else if (c == 0) {
+                    npin++;
+                    pin_node = u;
+                    pin_value = r.cst;
+                }
+                row_of[r.uc] = (int)rows.size();
+                rows.push_back(r);
+                m[u] |= (uint8_t)(1 << c);
+            }
+        if (npin == 1) {
+            Lv.pin = pin_node;
+            Lv.pinval = pin_value;
+            m[pin_node] &= (uint8_t)~BC_P;
+            rows.erase(rows.begin() + row_of[pin_node * 4]);
+            row_of.clear();
+            for (size_t q = 0; q < rows.size(); q++) row_of[rows[q].uc] = (int)q;
+        }
+        // every non-boundary velocity row must keep its stencil inside the grid
+        for (int u = 0; u < Lv.n; u++) {
+            int j = u % Lv.ny, i = (u / Lv.ny) % Lv.nx, k = u / (Lv.nx * Lv.ny);
+            int nx = Lv.nx, ny = Lv.ny, nz = Lv.nz;
+            bool okx = i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 3 && k >= 1 && k <= nz - 3;
+            bool oky = i >= 1 && i <= nx - 3 && j >= 1 && j <= ny - 2 && k >= 1 && k <= nz - 3;
+            bool okz = i >= 1 && i <= nx - 3 && j >= 1 && j <= ny - 3 && k >= 1 && k <= nz - 2;
+            if (valid_pos(1, i, j, k, nx, ny, nz) && !(m[u] & BC_VX) && !okx)
+                throw Error(P2_ERR_UNSUPPORTED, "open boundary row (Vx) on level " + std::to_string(l) +
+                                                    ": periodic or missing boundary conditions are not supported");
+            if (valid_pos(2, i, j, k, nx, ny, nz) && !(m[u] & BC_VY) && !oky)
+                throw Error(P2_ERR_UNSUPPORTED, "open boundary row (Vy) on level " + std::to_string(l));
+            if (valid_pos(3, i, j, k, nx, ny, nz) && !(m[u] & BC_VZ) && !okz)
+                throw Error(P2_ERR_UNSUPPORTED, "open boundary row (Vz) on level " + std::to_string(l));
+        }
+        // chain depth: rows whose target is itself a boundary row run later
+        std::vector<int> depth(rows.size(), 0);
+        for (size_t q = 0; q < rows.size(); q++) {
+            int d = 0, t = rows[q].t;
+            while (t >= 0) {
+                auto it = row_of.find(t);
+                if (it == row_of.end()) break;
+                if (++d > 16) throw Error(P2_ERR_ARG, "cyclic boundary-row chain");
+                t = rows[it->second].t;
+            }
+            depth[q] = d;
+        }
+        std::vector<size_t> order(rows.size());
+        for (size_t q = 0; q < order.size(); q++) order[q] = q;
+        std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) { return depth[a] < depth[b]; });
+        std::vector<int> bu, bt;
+        std::vector<float> bk, bcst;
+        Lv.bc_groups.clear();
+        Lv.bc_groups.push_back(0);
+        int cur = 0;
+        for (size_t q : order) {
+            while (depth[q] > cur) { Lv.bc_groups.push_back((int)bu.size()); cur++; }
+            bu.push_back(rows[q].uc);
+            bt.push_back(rows[q].t);
+            bk.push_back(rows[q].k);
+            bcst.push_back(rows[q].cst);
+        }
+        Lv.bc_groups.push_back((int)bu.size());
+        Lv.nbc = (int)bu.size();
+        // resolved chains (target non-boundary, product of koefs) for the coarse elimination
+        Lv.h_bu = bu;
+        Lv.h_rt.assign(bu.size(), -1);
+        Lv.h_rk.assign(bu.size(), 0.0);
+        for (size_t q = 0; q < bu.size(); q++) {
+            int t = bt[q];
+            double kk = bk[q];
+            while (t >= 0) {
+                auto it = row_of.find(t);
+                if (it == row_of.end()) break;
+                kk *= rows[it->second].k;
+                t = rows[it->second].t;
+            }
+            Lv.h_rt[q] = t;
+            Lv.h_rk[q] = t >= 0 ? kk : 0.0;
+        }
+        Lv.h_bcm = m;
+        Lv.bcm = upload(arena, m);
+        Lv.bu = upload(arena, bu);
+        Lv.bt = upload(arena, bt);
+        Lv.bk = upload(arena, bk);
+        Lv.bconst = upload(arena, bcst);
+    }
+    allocate_work();
+    bc_ready = true;
+}
+
+void Solver::allocate_work()
+{
+    int nl = (int)L.size();
+    for (int l = 0; l < nl; l++) {
+        Level &Lv = L[l];
+        long n = Lv.n;
+        Lv.nu = (float *)arena.alloc(sizeof(float) * n);
+        Lv.ro = (float *)arena.alloc(sizeof(float) * n);
+        Lv.ec = (float *)arena.alloc(sizeof(float) * n);
+        Lv.exy = (float *)arena.alloc(sizeof(float) * n);
+        Lv.exz = (float *)arena.alloc(sizeof(float) * n);
+        Lv.eyz = (float *)arena.alloc(sizeof(float) * n);
+        auto v32 = [&](Vec4<float> &v) {
+            float *p = (float *)arena.alloc(sizeof(float) * 4 * n);
+            for (int c = 0; c < 4; c++) v.c[c] = p + c * n;
+            v.n = (int)n;
+        };
+        auto v64 = [&](Vec4<double> &v) {
+            double *p = (double *)arena.alloc(sizeof(double) * 4 * n);
+            for (int c = 0; c < 4; c++) v.c[c] = p + c * n;
+            v.n = (int)n;
+        };
+        v32(Lv.x32); v32(Lv.y32); v32(Lv.b32); v32(Lv.r32);
+        if (prm.precision == 1 || l == 0) { v64(Lv.x64); v64(Lv.y64); v64(Lv.b64); v64(Lv.r64); }
+        if (prm.precision == 1 && l > 0) {}
+    }
+    // level-0 raw fields
+    long n0 = L[0].n;
+    f0.nu = L[0].nu;
+    f0.ro = L[0].ro;
+    f0.nxx = (float *)arena.alloc(sizeof(float) * n0);
+    f0.nxy = (float *)arena.alloc(sizeof(float) * n0);
+    f0.nxz = (float *)arena.alloc(sizeof(float) * n0);
+    f0.nyz = (float *)arena.alloc(sizeof(float) * n0);
+    // outer loop vectors
+    int m = std::max(1, std::min(prm.restart, kMaxDots - 2));
+    restart = m;
+    auto v64n = [&](Vec4<double> &v) {
+        double *p = (double *)arena.alloc(sizeof(double) * 4 * n0);
+        for (int c = 0; c < 4; c++) v.c[c] = p + c * n0;
+        v.n = (int)n0;
+    };
+    v64n(gx); v64n(gb); v64n(gr);
+    Z.assign(m, Vec4<double>());
+    Q.assign(m, Vec4<double>());
+    for (int q = 0; q < m; q++) { v64n(Z[q]); v64n(Q[q]); }
+    partial = (double *)arena.alloc(sizeof(double) * kRedBlocks * kMaxDots);
+    dots = (double *)arena.alloc(sizeof(double) * kMaxDots * 2);
+    scal = (double *)arena.alloc(sizeof(double) * 64);  // [0,1] compat sums, [2] alpha, [3] shift, [8..] GS coefficients
+    P2_CUDA_TRY(cudaMallocHost(&hdots_raw, sizeof(double) * kMaxDots * 2));
+    hdots.reset(hdots_raw, [](double *p) { cudaFreeHost(p); });
+    // coarse free-unknown set
+    build_coarse_index();
+}
+
+void Solver::build_coarse_index()
+{
+    Level &C = L.back();
+    std::vector<int> col(C.n * 4, -1);
+    std::vector<int> fre;
+    for (int u = 0; u < C.n; u++) {
+        int j = u % C.ny, i = (u / C.ny) % C.nx, k = u / (C.nx * C.ny);
+        for (int c = 0; c < 4; c++) {
+            if (!valid_pos(c, i, j, k, C.nx, C.ny, C.nz)) continue;
+            if (C.h_bcm[u] & (1 << c)) continue;
+            if (c == 0 && u == C.pin) continue;  // pinned: fixed zero in the coarse correction
+            col[u * 4 + c] = (int)fre.size();
+            fre.push_back(u * 4 + c);
+        }
+    }
+    nF = (int)fre.size();
+    coarse_col = col;
+    d_free = upload(arena, fre);
+    d_colmap = upload(arena, col);
+    // resolved boundary rows of the coarsest level as a dense per-unknown map
+    std::vector<int> rt(C.n * 4, -2);
+    std::vector<float> rk(C.n * 4, 0.0f);
+    for (size_t q = 0; q < C.h_bu.size(); q++) {
+        rt[C.h_bu[q]] = C.h_rt[q];
+        rk[C.h_bu[q]] = (float)C.h_rk[q];
+    }
+    d_crt = upload(arena, rt);
+    d_crk = upload(arena, rk);
+    A_c = (double *)arena.alloc(sizeof(double) * (size_t)nF * nF);
+    Ainv64 = (double *)arena.alloc(sizeof(double) * (size_t)nF * nF);
+    Ainv32 = (float *)arena.alloc(sizeof(float) * (size_t)nF * nF);
+    d_ipiv = (int *)arena.alloc(sizeof(int) * nF);
+    d_info = (int *)arena.alloc(sizeof(int) * 4);
+    probes = (double *)arena.alloc(sizeof(double) * (size_t)C.n * 4 * 125);
+    cb64 = (double *)arena.alloc(sizeof(double) * nF);
+    cx64 = (double *)arena.alloc(sizeof(double) * nF);
+    cb32 = (float *)arena.alloc(sizeof(float) * nF);
+    cx32 = (float *)arena.alloc(sizeof(float) * nF);
+}
+
+// ---------------------------------------------------------------------------
+// Coarsest operator by probing: 125 colour classes (index mod 5 per axis) x 4
+// components; a probe sets 1 on the free unknowns of its class and koef on the
+// boundary unknowns whose resolved target is in the class, so that every
+// non-zero of a row is attributed to the unique free column of that class
+// within two nodes.
+__global__ void k_probe_build(int nx, int ny, int nz, int cls, int comp, const int *colmap, const int *rt,
+                              const float *rk, double *X)
+{
+    int u = blockIdx.x * blockDim.x + threadIdx.x;
+    int n = nx * ny * nz;
+    if (u >= n) return;
+    int j = u % ny, i = (u / ny) % nx, k = u / (nx * ny);
+    int cx = cls % 5, cy = (cls / 5) % 5, cz = cls / 25;
+    for (int c = 0; c < 4; c++) {
+        double v = 0;
+        int uc = u * 4 + c;
+        if (colmap[uc] >= 0) {
+            if (c == comp && i % 5 == cx && j % 5 == cy && k % 5 == cz) v = 1.0;
+        } else if (rt[uc] >= 0) {
+            int t = rt[uc], tn = t >> 2, tc = t & 3;
+            int tj = tn % ny, ti = (tn / ny) % nx, tk = tn / (nx * ny);
+            if (tc == comp && ti % 5 == cx && tj % 5 == cy && tk % 5 == cz && colmap[t] >= 0) v = rk[uc];
+        }
+        X[(size_t)c * n + u] = v;
+    }
+}
+
+__global__ void k_probe_rows(LevelView<double> Lc, const double *X, int cls, int comp, const int *colmap, double *A,
+                             int nF)
+{
+    int u = blockIdx.x * blockDim.x + threadIdx.x;
+    if (u >= Lc.n) return;
+    int n = Lc.n;
+    int j = u % Lc.ny, i = (u / Lc.ny) % Lc.nx, k = u / (Lc.nx * Lc.ny);
+    Fields<double, double> x{X, X + n, X + 2 * n, X + 3 * n};
+    int cx = cls % 5, cy = (cls / 5) % 5, cz = cls / 25;
+    // the unique node of this class within two nodes
+    int ci = i + ((cx - i) % 5 + 5) % 5, cj = j + ((cy - j) % 5 + 5) % 5, ck = k + ((cz - k) % 5 + 5) % 5;
+    if (ci > i + 2) ci -= 5;
+    if (cj > j + 2) cj -= 5;
+    if (ck > k + 2) ck -= 5;
+    if (ci < 0 || cj < 0 || ck < 0 || ci >= Lc.nx || cj >= Lc.ny || ck >= Lc.nz) return;
+    int col = colmap[P2IDX(Lc, ci, cj, ck) * 4 + comp];
+    if (col < 0) return;
+    for (int c = 0; c < 4; c++) {
+        int row = colmap[u * 4 + c];
+        if (row < 0) continue;
+        double a;
+        if (c == 0) a = row_p(Lc, x, i, j, k);
+        else if (c == 1) a = row_vx(Lc, x, i, j, k, (double *)nullptr);
+        else if (c == 2) a = row_vy(Lc, x, i, j, k, (double *)nullptr);
+        else a = row_vz(Lc, x, i, j, k, (double *)nullptr);
+        A[(size_t)col * nF + row] = a;
+    }
+}
+
+// b_F = b on the free unknowns
+template <typename T>
+__global__ void k_coarse_gather(int nF, const int *fre, Vec4<T> b, T *bF)
+{
+    int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= nF) return;
+    int uc = fre[q];
+    bF[q] = b.c[uc & 3][uc >> 2];
+}
+template <typename T>
+__global__ void k_coarse_scatter(int nF, const int *fre, const T *xF, Vec4<T> x)
+{
+    int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= nF) return;
+    int uc = fre[q];
+    x.c[uc & 3][uc >> 2] = xF[q];
+}
+// y = Ainv b  (column-major nF x nF), one warp per 32 rows slice of columns.
+template <typename T>
+__global__ void k_gemv(int n, const T *A, const T *b, T *y)
+{
+    // block: 256 threads = 8 warps; rows r0..r0+31 per block, warps split the columns
+    __shared__ T part[8][33];
+    int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int r = blockIdx.x * 32 + lane;
+    T s = 0;
+    if (r < n)
+        for (int c = w; c < n; c += 8) s += A[(size_t)c * n + r] * __ldg(b + c);
+    part[w][lane] = s;
+    __syncthreads();
+    if (w == 0 && r < n) {
+        T t = 0;
+        for (int q = 0; q < 8; q++) t += part[q][lane];
+        y[r] = t;
+    }
+}
+
+void Solver::coarse_setup()
+{
+    Level &C = L.back();
+    int nl = (int)L.size();
+    LevelView<double> Lc = view<double>(nl - 1, nl == 1);
+    P2_CUDA_TRY(cudaMemsetAsync(A_c, 0, sizeof(double) * (size_t)nF * nF, st));
+    for (int comp = 0; comp < 4; comp++)
+        for (int cls = 0; cls < 125; cls++) {
+            double *X = probes + (size_t)cls * C.n * 4;
+            k_probe_build<<<nblk(C.n), kThreads, 0, st>>>(C.nx, C.ny, C.nz, cls, comp, d_colmap, d_crt, d_crk, X); P2_COUNT_LAUNCH();
+            k_probe_rows<<<nblk(C.n), kThreads, 0, st>>>(Lc, X, cls, comp, d_colmap, A_c, nF); P2_COUNT_LAUNCH();
+        }
+    P2_CUDA_TRY(cudaGetLastError());
+    int info = dense_lu_inverse(st, A_c, nF, Ainv64, d_ipiv, d_info);
+    if (info) throw Error(P2_ERR_SINGULAR, "zero pivot in the coarsest LU at column " + std::to_string(info));
+    d2f(st, (size_t)nF * nF, Ainv64, Ainv32);
+}
+
+template <typename T>
+void Solver::coarse_solve(Vec4<T> &b, Vec4<T> &x)
+{
+    Level &C = L.back();
+    T *bF = std::is_same<T, double>::value ? (T *)cb64 : (T *)cb32;
+    T *xF = std::is_same<T, double>::value ? (T *)cx64 : (T *)cx32;
+    const T *Ai = std::is_same<T, double>::value ? (const T *)Ainv64 : (const T *)Ainv32;
+    k_coarse_gather<T><<<nblk(nF), kThreads, 0, st>>>(nF, d_free, b, bF); P2_COUNT_LAUNCH();
+    k_gemv<T><<<(nF + 31) / 32, 256, 0, st>>>(nF, Ai, bF, xF); P2_COUNT_LAUNCH();
+    for (int c = 0; c < 4; c++) P2_CUDA_TRY(cudaMemsetAsync(x.c[c], 0, sizeof(T) * C.n, st));
+    k_coarse_scatter<T><<<nblk(nF), kThreads, 0, st>>>(nF, d_free, xF, x); P2_COUNT_LAUNCH();
+    bc_set<T>((int)L.size() - 1, x, b);
+}
+
+// ---------------------------------------------------------------------------
+template <typename T>
+void Solver::bc_set(int l, Vec4<T> &x, Vec4<T> &b)
+{
+    Level &Lv = L[l];
+    for (size_t g = 0; g + 1 < Lv.bc_groups.size(); g++) {
+        int a = Lv.bc_groups[g], e = Lv.bc_groups[g + 1];
+        if (e > a)
+            k_bc_set<T><<<nblk(e - a), kThreads, 0, st>>>(e - a, Lv.bu + a, Lv.bt + a, Lv.bk + a, x, b); P2_COUNT_LAUNCH();
+    }
+}
+
+template <typename T>
+static Vec4<T> &vx_of(Level &Lv, int which);
+template <>
+Vec4<float> &vx_of<float>(Level &Lv, int which) { return which ? Lv.y32 : Lv.x32; }
+template <>
+Vec4<double> &vx_of<double>(Level &Lv, int which) { return which ? Lv.y64 : Lv.x64; }
+template <typename T>
+static Vec4<T> &b_of(Level &Lv);
+template <>
+Vec4<float> &b_of<float>(Level &Lv) { return Lv.b32; }
+template <>
+Vec4<double> &b_of<double>(Level &Lv) { return Lv.b64; }
+template <typename T>
+static Vec4<T> &r_of(Level &Lv);
+template <>
+Vec4<float> &r_of<float>(Level &Lv) { return Lv.r32; }
+template <>
+Vec4<double> &r_of<double>(Level &Lv) { return Lv.r64; }
+
+template <typename T>
+void Solver::smooth(int l, int sweeps)
+{
+    Level &Lv = L[l];
+    LevelView<T> V = view<T>(l, false);
+    Vec4<T> &x = vx_of<T>(Lv, 0), &y = vx_of<T>(Lv, 1), &b = b_of<T>(Lv);
+    bc_set<T>(l, x, b);
+    if (sweeps <= 0) return;
+    long cells = (long)(Lv.nx - 1) * (Lv.nz - 1) * (Lv.ny / 2);
+    T om = (T)prm.omega;
+    // colour 0 reads velocities from x and writes y, colour 1 goes back; the
+    // pressure is updated in place in x.c[0] (yy shares it)
+    Vec4<T> yy = y;
+    yy.c[0] = x.c[0];
+    for (int s = 0; s < sweeps; s++) {
+        k_vanka<T><<<nblk(cells), kThreads, 0, st>>>(V, x.c[0], x, yy, b, om, 0); P2_COUNT_LAUNCH();
+        bc_set<T>(l, yy, b);
+        k_vanka<T><<<nblk(cells), kThreads, 0, st>>>(V, x.c[0], yy, x, b, om, 1); P2_COUNT_LAUNCH();
+        bc_set<T>(l, x, b);
+    }
+}
+
+template <typename T>
+void Solver::level_residual(int l)
+{
+    Level &Lv = L[l];
+    LevelView<T> V = view<T>(l, false);
+    Vec4<T> &x = vx_of<T>(Lv, 0), &b = b_of<T>(Lv), &r = r_of<T>(Lv);
+    Fields<T, T> f{x.c[0], x.c[1], x.c[2], x.c[3]};
+    Vec4<float> none;
+    k_rows<T, T><<<nblk(Lv.n), kThreads, 0, st>>>(V, f, b, r, none, 0); P2_COUNT_LAUNCH();
+    if (Lv.nbc) k_bc_rows<T, T><<<nblk(Lv.nbc), kThreads, 0, st>>>(Lv.nbc, Lv.bu, Lv.bt, Lv.bk, f, b, r, none, 0); P2_COUNT_LAUNCH();
+}
+
+template <typename T>
+void Solver::vcycle()
+{
+    int nl = (int)L.size();
+    for (int l = 0; l < nl - 1; l++) {
+        smooth<T>(l, prm.npre[l]);
+        level_residual<T>(l);
+        Level &F = L[l], &Cl = L[l + 1];
+        LevelView<T> VF = view<T>(l, false), VC = view<T>(l + 1, false);
+        k_restrict<T><<<nblk(Cl.n), kThreads, 0, st>>>(VF, r_of<T>(F), VC, b_of<T>(Cl), vx_of<T>(Cl, 0), F.tv, 1); P2_COUNT_LAUNCH();
+        k_compat_partial<T><<<kRedBlocks, kThreads, 0, st>>>(VC, b_of<T>(Cl).c[0], partial); P2_COUNT_LAUNCH();
+        k_dots_final<<<1, 1024, 0, st>>>(2, kRedBlocks, partial, scal); P2_COUNT_LAUNCH();
+        k_compat_apply<T><<<nblk(Cl.n), kThreads, 0, st>>>(VC, b_of<T>(Cl).c[0], scal); P2_COUNT_LAUNCH();
+    }
+    if (nl > 1) coarse_solve<T>(b_of<T>(L[nl - 1]), vx_of<T>(L[nl - 1], 0));
+    else coarse_solve<T>(b_of<T>(L[0]), vx_of<T>(L[0], 0));
+    for (int l = nl - 2; l >= 0; l--) {
+        Level &F = L[l], &Cl = L[l + 1];
+        LevelView<T> VF = view<T>(l, false), VC = view<T>(l + 1, false);
+        k_prolong<T><<<nblk(F.n), kThreads, 0, st>>>(VF, vx_of<T>(F, 0), VC, vx_of<T>(Cl, 0), F.tv, (T)prm.p1koef,
+                                                     (T)prm.v1koef); P2_COUNT_LAUNCH();
+        smooth<T>(l, prm.npost[l]);
+    }
+}
+
+// ---------------------------------------------------------------------------
+void Solver::set_nodes_device()
+{
+    // coarse nu/ro (ronurestrict), per-stencil viscosities, level-0 rhs
+    int nl = (int)L.size();
+    for (int l = 1; l < nl; l++) {
+        Level &F = L[l - 1], &C = L[l];
+        k_ronurestrict<<<nblk(C.n), kThreads, 0, st>>>(F.nx, F.ny, F.nz, F.nu, F.ro, C.nx, C.ny, C.nz, C.nu, C.ro,
+                                                       F.ronu[0], F.ronu[1], F.ronu[2], prm.viscmod); P2_COUNT_LAUNCH();
+    }
+    for (int l = 0; l < nl; l++) {
+        Level &Lv = L[l];
+        k_level_eta<<<nblk(Lv.n), kThreads, 0, st>>>(Lv.nx, Lv.ny, Lv.nz, Lv.nu, f0.nxx, f0.nxy, f0.nxz, f0.nyz,
+                                                     Lv.ec, Lv.exy, Lv.exz, Lv.eyz, prm.nubeg, prm.nuend,
+                                                     prm.viscmod, l == 0); P2_COUNT_LAUNCH();
+    }
+    Level &L0 = L[0];
+    k_rhs0<double><<<nblk(L0.n), kThreads, 0, st>>>(L0.nx, L0.ny, L0.nz, L0.ro, L0.bcm, gb, prm.gxkoef, prm.gykoef,
+                                                    prm.gzkoef); P2_COUNT_LAUNCH();
+    if (L0.nbc) k_bc_consts<double><<<nblk(L0.nbc), kThreads, 0, st>>>(L0.nbc, L0.bu, L0.bconst, gb); P2_COUNT_LAUNCH();
+    P2_CUDA_TRY(cudaGetLastError());
+}
+
+void Solver::upload_nodes(const float *nu, const float *ro, const float *nxx, const float *nxy, const float *nxz,
+                          const float *nyz)
+{
+    if (!bc_ready) throw Error(P2_ERR_STATE, "node fields before p2_set_bc");
+    long n = L[0].n;
+    const float *src[6] = {nu, ro, nxx, nxy, nxz, nyz};
+    float *dst[6] = {L[0].nu, L[0].ro, f0.nxx, f0.nxy, f0.nxz, f0.nyz};
+    for (int q = 0; q < 6; q++) {
+        if (!src[q]) throw Error(P2_ERR_ARG, "null node field");
+        P2_CUDA_TRY(cudaMemcpyAsync(dst[q], src[q], sizeof(float) * n, cudaMemcpyHostToDevice, st));
+    }
+    nodes_ready = true;
+}
+
+void Solver::dots_sync(const DotJobs &jobs)
+{
+    k_dots_partial<<<kRedBlocks, kThreads, 0, st>>>(jobs, L[0].n, L[0].pin, partial); P2_COUNT_LAUNCH();
+    k_dots_final<<<1, 1024, 0, st>>>(jobs.nd, kRedBlocks, partial, dots); P2_COUNT_LAUNCH();
+    P2_CUDA_TRY(cudaMemcpyAsync(hdots.get(), dots, sizeof(double) * jobs.nd, cudaMemcpyDeviceToHost, st));
+    P2_CUDA_TRY(cudaStreamSynchronize(st));
+}
+
+static DotJob job(const Vec4<double> &a, const Vec4<double> &b)
+{
+    DotJob j;
+    for (int c = 0; c < 4; c++) { j.a[c] = a.c[c]; j.b[c] = b.c[c]; }
+    return j;
+}
+
+// out = b - A x (mode 0) or A x (mode 1) on level 0 in FP64; r32 optional.
+void Solver::rows0(const Vec4<double> &x, Vec4<double> &out, Vec4<float> *r32, int mode)
+{
+    Level &L0 = L[0];
+    LevelView<double> V = view<double>(0, true);
+    Fields<double, double> f{x.c[0], x.c[1], x.c[2], x.c[3]};
+    Vec4<float> o32 = r32 ? *r32 : Vec4<float>();
+    k_rows<double, double><<<nblk(L0.n), kThreads, 0, st>>>(V, f, gb, out, o32, mode); P2_COUNT_LAUNCH();
+    if (L0.nbc)
+        k_bc_rows<double, double><<<nblk(L0.nbc), kThreads, 0, st>>>(L0.nbc, L0.bu, L0.bt, L0.bk, f, gb, out, o32,
+                                                                   mode); P2_COUNT_LAUNCH();
+}
+
+// z = V(r): one preconditioning V-cycle for the level-0 right-hand side r.
+void Solver::precondition(Vec4<double> &z)
+{
+    Level &L0 = L[0];
+    if (prm.precision == 0) {
+        // r32 already holds float(r); run the FP32 cycle on b32 := r32
+        for (int c = 0; c < 4; c++)
+            P2_CUDA_TRY(cudaMemcpyAsync(L0.b32.c[c], L0.r32.c[c], sizeof(float) * L0.n, cudaMemcpyDeviceToDevice, st));
+        for (int c = 0; c < 4; c++) P2_CUDA_TRY(cudaMemsetAsync(L0.x32.c[c], 0, sizeof(float) * L0.n, st));
+        run_vcycle_graph<float>();
+        k_f32_to_f64<<<nblk(L0.n), kThreads, 0, st>>>(L0.n, L0.x32, z); P2_COUNT_LAUNCH();
+    } else {
+        for (int c = 0; c < 4; c++) {
+            P2_CUDA_TRY(cudaMemcpyAsync(L0.b64.c[c], gr.c[c], sizeof(double) * L0.n, cudaMemcpyDeviceToDevice, st));
+            P2_CUDA_TRY(cudaMemsetAsync(L0.x64.c[c], 0, sizeof(double) * L0.n, st));
+        }
+        run_vcycle_graph<double>();
+        for (int c = 0; c < 4; c++)
+            P2_CUDA_TRY(cudaMemcpyAsync(z.c[c], L0.x64.c[c], sizeof(double) * L0.n, cudaMemcpyDeviceToDevice, st));
+    }
+}
+
+template <typename T>
+void Solver::run_vcycle_graph()
+{
+    int key = std::is_same<T, double>::value ? 1 : 0;
+    GraphSlot &g = graphs[key];
+    if (!prm.use_graphs) {
+        vcycle<T>();
+        P2_CUDA_TRY(cudaGetLastError());
+        return;
+    }
+    if (!g.exec) {
+        cudaGraph_t graph;
+        long long before = g_launches;
+        P2_CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        vcycle<T>();
+        P2_CUDA_TRY(cudaStreamEndCapture(st, &graph));
+        g.kernels = g_launches - before;  // captured, not yet executed
+        g_launches = before;
+        P2_CUDA_TRY(cudaGraphInstantiate(&g.exec, graph, 0));
+        cudaGraphDestroy(graph);
+    }
+    P2_CUDA_TRY(cudaGraphLaunch(g.exec, st));
+    g_launches += g.kernels;
+}
+
+thread_local long long g_launches = 0;
+
+p2_solve_info Solver::solve()
+{
+    const char *vb = std::getenv("P2CUDA_VERBOSE");
+    verbose = vb && vb[0] == '1';
+    if (!nodes_ready) throw Error(P2_ERR_STATE, "solve before node fields were set");
+    p2_solve_info info{};
+    long long launches0 = g_launches;
+    Level &L0 = L[0];
+    long n = L0.n;
+    P2_CUDA_TRY(cudaEventRecord(ev[0], st));
+    set_nodes_device();
+    coarse_setup();
+    P2_CUDA_TRY(cudaEventRecord(ev[1], st));
+    // b-norm of the pinned system: every row but the pin cell's, plus the pin value
+    DotJobs J{};
+    J.j[0] = job(gb, gb);
+    J.nd = 1;
+    dots_sync(J);
+    double bnorm2 = hdots.get()[0] + (L0.pin >= 0 ? L0.pinval * L0.pinval : 0.0);
+    double bnorm = std::sqrt(bnorm2);
+    if (!(bnorm > 0)) bnorm = 1.0;
+    int m = restart, k = 0, it = 0;
+    std::vector<double> qq(m, 1.0);
+    float vc_ms = 0;
+    double rel = 0;
+    for (;;) {
+        // true FP64 residual (and its float copy for the mixed-precision cycle)
+        rows0(gx, gr, prm.precision == 0 ? &L0.r32 : nullptr, 0);
+        J.nd = 1;
+        J.j[0] = job(gr, gr);
+        dots_sync(J);
+        double rr = hdots.get()[0];
+        rel = std::sqrt(rr) / bnorm;
+        if (it == 0) info.rel_residual0 = rel;
+        if (verbose) std::fprintf(stderr, "p2cuda: iteration %d rel residual %.3e\n", it, rel);
+        if (!std::isfinite(rel)) { info.status = P2_ERR_NAN; break; }
+        if (rel <= prm.tol) { info.status = P2_OK; break; }
+        if (it >= prm.max_iter) { info.status = P2_ERR_NOT_CONVERGED; break; }
+        Vec4<double> &z = Z[k], &q = Q[k];
+        P2_CUDA_TRY(cudaEventRecord(ev[2], st));
+        precondition(z);
+        P2_CUDA_TRY(cudaEventRecord(ev[3], st));
+        rows0(z, q, nullptr, 1);
+        // classical Gram-Schmidt against the stored directions, plus (r,q)
+        J.nd = 0;
+        for (int j = 0; j < k; j++) J.j[J.nd++] = job(q, Q[j]);
+        if (k > 0) {
+            dots_sync(J);
+            std::vector<double> coef(k);
+            for (int j = 0; j < k; j++) coef[j] = hdots.get()[j] / qq[j];
+            P2_CUDA_TRY(cudaMemcpyAsync(scal + 8, coef.data(), sizeof(double) * k, cudaMemcpyHostToDevice, st));
+            VecList X{}, Zl{};
+            for (int j = 0; j < k; j++)
+                for (int c = 0; c < 4; c++) { X.v[j][c] = Q[j].c[c]; Zl.v[j][c] = Z[j].c[c]; }
+            X.nv = Zl.nv = k;
+            k_cgs_update<<<nblk(n), kThreads, 0, st>>>((int)n, scal + 8, q, X, z, Zl); P2_COUNT_LAUNCH();
+        }
+        J.nd = 2;
+        J.j[0] = job(q, q);
+        J.j[1] = job(gr, q);
+        dots_sync(J);
+        qq[k] = hdots.get()[0];
+        if (!(qq[k] > 0)) { info.status = P2_ERR_NAN; break; }
+        double alpha = hdots.get()[1] / qq[k];
+        P2_CUDA_TRY(cudaMemcpyAsync(scal + 2, &alpha, sizeof(double), cudaMemcpyHostToDevice, st));
+        k_axpy4<<<nblk(n), kThreads, 0, st>>>((int)n, scal + 2, 1.0, gx, z); P2_COUNT_LAUNCH();
+        float t = 0;
+        P2_CUDA_TRY(cudaEventSynchronize(ev[3]));
+        P2_CUDA_TRY(cudaEventElapsedTime(&t, ev[2], ev[3]));
+        vc_ms += t;
+        k = (k + 1) % m;
+        it++;
+    }
+    // pressure shift to the pinned value
+    k_pressure_shift_value<<<1, 32, 0, st>>>(gx.c[0], L0.pin, L0.pinval, scal + 3); P2_COUNT_LAUNCH();
+    k_pressure_shift<<<nblk(n), kThreads, 0, st>>>(L0.nx, L0.ny, L0.nz, gx.c[0], scal + 3); P2_COUNT_LAUNCH();
+    P2_CUDA_TRY(cudaEventRecord(ev[4], st));
+    P2_CUDA_TRY(cudaEventSynchronize(ev[4]));
+    float tt = 0, ts = 0;
+    P2_CUDA_TRY(cudaEventElapsedTime(&tt, ev[0], ev[4]));
+    P2_CUDA_TRY(cudaEventElapsedTime(&ts, ev[0], ev[1]));
+    info.iterations = it;
+    info.rel_residual = rel;
+    info.ms_total = tt;
+    info.ms_setup = ts;
+    info.ms_vcycles = vc_ms;
+    info.kernels = g_launches - launches0;
+    return info;
+}
+
+void Solver::set_initial(const float *vx, const float *vy, const float *vz, const double *pr)
+{
+    long n = L[0].n;
+    for (int c = 0; c < 4; c++) P2_CUDA_TRY(cudaMemsetAsync(gx.c[c], 0, sizeof(double) * n, st));
+    if (!vx && !vy && !vz && !pr) return;
+    std::vector<double> h(n);
+    const float *fs[3] = {vx, vy, vz};
+    for (int c = 1; c < 4; c++) {
+        if (!fs[c - 1]) continue;
+        for (long u = 0; u < n; u++) h[u] = fs[c - 1][u];
+        P2_CUDA_TRY(cudaMemcpy(gx.c[c], h.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
+    }
+    if (pr) P2_CUDA_TRY(cudaMemcpy(gx.c[0], pr, sizeof(double) * n, cudaMemcpyHostToDevice));
+}
+
+void Solver::get_solution(double *vx, double *vy, double *vz, double *pr)
+{
+    long n = L[0].n;
+    double *dst[4] = {pr, vx, vy, vz};
+    for (int c = 0; c < 4; c++)
+        if (dst[c]) P2_CUDA_TRY(cudaMemcpyAsync(dst[c], gx.c[c], sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+    P2_CUDA_TRY(cudaStreamSynchronize(st));
+    // zero the entries that are not unknowns (ghost positions)
+    const Level &L0 = L[0];
+    for (long u = 0; u < n; u++) {
+        int j = (int)(u % L0.ny), i = (int)((u / L0.ny) % L0.nx), k = (int)(u / ((long)L0.nx * L0.ny));
+        for (int c = 0; c < 4; c++)
+            if (dst[c] && !valid_pos(c, i, j, k, L0.nx, L0.ny, L0.nz)) dst[c][u] = 0.0;
+    }
+}
+
+
+// ---------------------------------------------------------------------------
+// Test hooks (FP64, interleaved [P,Vx,Vy,Vz] per node as the reference's sol0).
+static void to_vec4(cudaStream_t st, const double *h, int n, Vec4<double> &v)
+{
+    std::vector<double> tmp(n);
+    for (int c = 0; c < 4; c++) {
+        for (int u = 0; u < n; u++) tmp[u] = h[(size_t)u * 4 + c];
+        P2_CUDA_TRY(cudaMemcpyAsync(v.c[c], tmp.data(), sizeof(double) * n, cudaMemcpyHostToDevice, st));
+        P2_CUDA_TRY(cudaStreamSynchronize(st));
+    }
+}
+static void from_vec4(cudaStream_t st, const Vec4<double> &v, int n, double *h)
+{
+    std::vector<double> tmp(n);
+    for (int c = 0; c < 4; c++) {
+        P2_CUDA_TRY(cudaMemcpyAsync(tmp.data(), v.c[c], sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+        P2_CUDA_TRY(cudaStreamSynchronize(st));
+        for (int u = 0; u < n; u++) h[(size_t)u * 4 + c] = tmp[u];
+    }
+}
+struct TmpVec {
+    Vec4<double> v;
+    double *base = nullptr;
+    explicit TmpVec(int n)
+    {
+        P2_CUDA_TRY(cudaMalloc(&base, sizeof(double) * 4 * (size_t)n));
+        P2_CUDA_TRY(cudaMemset(base, 0, sizeof(double) * 4 * (size_t)n));
+        for (int c = 0; c < 4; c++) v.c[c] = base + (size_t)c * n;
+        v.n = n;
+    }
+    ~TmpVec() { cudaFree(base); }
+};
+
+void Solver::debug_prepare()
+{
+    if (!nodes_ready) throw Error(P2_ERR_STATE, "node fields not set");
+    set_nodes_device();
+    P2_CUDA_TRY(cudaStreamSynchronize(st));
+}
+
+// y = A x on level l: operator rows, boundary rows x - koef x_t, identity elsewhere.
+void Solver::debug_apply(int l, const double *x, double *y)
+{
+    if (l < 0 || l >= (int)L.size()) throw Error(P2_ERR_ARG, "level out of range");
+    debug_prepare();
+    Level &Lv = L[l];
+    TmpVec X(Lv.n), Y(Lv.n), B(Lv.n);
+    to_vec4(st, x, Lv.n, X.v);
+    LevelView<double> V = view<double>(l, l == 0);
+    Fields<double, double> f{X.v.c[0], X.v.c[1], X.v.c[2], X.v.c[3]};
+    Vec4<float> none;
+    k_rows<double, double><<<nblk(Lv.n), kThreads, 0, st>>>(V, f, B.v, Y.v, none, 1); P2_COUNT_LAUNCH();
+    if (Lv.nbc)
+        k_bc_rows<double, double><<<nblk(Lv.nbc), kThreads, 0, st>>>(Lv.nbc, Lv.bu, Lv.bt, Lv.bk, f, B.v, Y.v, none, 1); P2_COUNT_LAUNCH();
+    P2_CUDA_TRY(cudaGetLastError());
+    from_vec4(st, Y.v, Lv.n, y);
+    // identity on positions that are not unknowns, the pinned row as a boundary row
+    for (int u = 0; u < Lv.n; u++) {
+        int j = u % Lv.ny, i = (u / Lv.ny) % Lv.nx, k = u / (Lv.nx * Lv.ny);
+        for (int c = 0; c < 4; c++)
+            if (!valid_pos(c, i, j, k, Lv.nx, Lv.ny, Lv.nz)) y[(size_t)u * 4 + c] = x[(size_t)u * 4 + c];
+        if (u == Lv.pin) y[(size_t)u * 4] = x[(size_t)u * 4];
+    }
+}
+
+// coarse rhs from a fine residual (vprestrict), optionally with the compatibility shift
+void Solver::debug_restrict(int lc, const double *fine_res, double *coarse_rhs, int compat)
+{
+    if (lc < 1 || lc >= (int)L.size()) throw Error(P2_ERR_ARG, "level out of range");
+    debug_prepare();
+    Level &F = L[lc - 1], &Cl = L[lc];
+    TmpVec R(F.n), Bc(Cl.n), Xc(Cl.n);
+    to_vec4(st, fine_res, F.n, R.v);
+    LevelView<double> VF = view<double>(lc - 1, false), VC = view<double>(lc, false);
+    k_restrict<double><<<nblk(Cl.n), kThreads, 0, st>>>(VF, R.v, VC, Bc.v, Xc.v, F.tv, 1); P2_COUNT_LAUNCH();
+    if (compat) {
+        k_compat_partial<double><<<kRedBlocks, kThreads, 0, st>>>(VC, Bc.v.c[0], partial); P2_COUNT_LAUNCH();
+        k_dots_final<<<1, 1024, 0, st>>>(2, kRedBlocks, partial, scal); P2_COUNT_LAUNCH();
+        k_compat_apply<double><<<nblk(Cl.n), kThreads, 0, st>>>(VC, Bc.v.c[0], scal); P2_COUNT_LAUNCH();
+    }
+    P2_CUDA_TRY(cudaGetLastError());
+    from_vec4(st, Bc.v, Cl.n, coarse_rhs);
+}
+
+void Solver::debug_prolong(int lc, const double *coarse_x, double *fine_x)
+{
+    if (lc < 1 || lc >= (int)L.size()) throw Error(P2_ERR_ARG, "level out of range");
+    debug_prepare();
+    Level &F = L[lc - 1], &Cl = L[lc];
+    TmpVec Xf(F.n), Xc(Cl.n);
+    to_vec4(st, fine_x, F.n, Xf.v);
+    to_vec4(st, coarse_x, Cl.n, Xc.v);
+    LevelView<double> VF = view<double>(lc - 1, false), VC = view<double>(lc, false);
+    k_prolong<double><<<nblk(F.n), kThreads, 0, st>>>(VF, Xf.v, VC, Xc.v, F.tv, prm.p1koef, prm.v1koef); P2_COUNT_LAUNCH();
+    P2_CUDA_TRY(cudaGetLastError());
+    from_vec4(st, Xf.v, F.n, fine_x);
+}
+
+// nu, ro of every level (after ronurestrict), concatenated like the reference's nu[] / ro[]
+// Average time of one colour pass of the cell-block smoother on level l.
+double Solver::debug_time_smoother(int l, int passes)
+{
+    if (l < 0 || l >= (int)L.size() || passes < 2) throw Error(P2_ERR_ARG, "bad level or pass count");
+    if (!bc_ready) throw Error(P2_ERR_STATE, "no level data");
+    Level &Lv = L[l];
+    long cells = (long)(Lv.nx - 1) * (Lv.nz - 1) * (Lv.ny / 2);
+    P2_CUDA_TRY(cudaEventRecord(ev[5], st));
+    if (prm.precision == 0 || l > 0) {
+        LevelView<float> V = view<float>(l, false);
+        Vec4<float> x = Lv.x32, y = Lv.y32;
+        y.c[0] = x.c[0];
+        for (int p = 0; p < passes; p++) {
+            k_vanka<float><<<nblk(cells), kThreads, 0, st>>>(V, x.c[0], (p & 1) ? y : x, (p & 1) ? x : y, Lv.b32,
+                                                             (float)prm.omega, p & 1);
+        }
+    } else {
+        LevelView<double> V = view<double>(l, false);
+        Vec4<double> x = Lv.x64, y = Lv.y64;
+        y.c[0] = x.c[0];
+        for (int p = 0; p < passes; p++) {
+            k_vanka<double><<<nblk(cells), kThreads, 0, st>>>(V, x.c[0], (p & 1) ? y : x, (p & 1) ? x : y, Lv.b64,
+                                                              prm.omega, p & 1);
+        }
+    }
+    P2_CUDA_TRY(cudaEventRecord(ev[6], st));
+    P2_CUDA_TRY(cudaEventSynchronize(ev[6]));
+    P2_CUDA_TRY(cudaGetLastError());
+    float t = 0;
+    P2_CUDA_TRY(cudaEventElapsedTime(&t, ev[5], ev[6]));
+    return (double)t / passes;
+}
+
+void Solver::debug_level_fields(float *nu, float *ro)
+{
+    debug_prepare();
+    for (auto &Lv : L) {
+        P2_CUDA_TRY(cudaMemcpy(nu + Lv.off, Lv.nu, sizeof(float) * Lv.n, cudaMemcpyDeviceToHost));
+        P2_CUDA_TRY(cudaMemcpy(ro + Lv.off, Lv.ro, sizeof(float) * Lv.n, cudaMemcpyDeviceToHost));
+    }
+}
+
+template LevelView<float> Solver::view<float>(int, bool) const;
+template LevelView<double> Solver::view<double>(int, bool) const;
+
+}  // namespace p2

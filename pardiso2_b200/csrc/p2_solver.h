@@ -1,0 +1,156 @@
+// Solver state of the p2cuda library (one per p2_ctx, one device, one stream).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <array>
+#include <memory>
+#include <vector>
+
+#include "p2_internal.cuh"
+
+namespace p2 {
+
+struct DeviceArena {
+    std::vector<void *> ptrs;
+    void *alloc(size_t bytes);
+    void release();
+};
+
+struct HostAxis {
+    std::vector<int> lo;
+    std::vector<double> w0, w1;
+    std::vector<int> ptr, idx;
+    std::vector<double> w;
+};
+
+struct Level {
+    int nx = 0, ny = 0, nz = 0, n = 0;
+    long off = 0;                 // node offset of the level (mgp)
+    std::vector<double> g[3];     // gridlines mggx/mggy/mggz
+    int tabstride = 0;
+    double *tabd = nullptr;       // 12 spacing tables (ih, ihc, ihe, ihv per axis), FP64
+    float *tabf = nullptr;        // same in FP32
+    TransferView tv{};            // this level -> next coarser level
+    AxisMap ronu[3]{};            // ronurestrict weights
+    float *nu = nullptr, *ro = nullptr;
+    float *ec = nullptr, *exy = nullptr, *exz = nullptr, *eyz = nullptr;
+    uint8_t *bcm = nullptr;
+    std::vector<uint8_t> h_bcm;
+    int pin = -1;
+    double pinval = 0;
+    // boundary rows sorted by copy-chain depth
+    int nbc = 0;
+    std::vector<int> bc_groups;
+    int *bu = nullptr, *bt = nullptr;
+    float *bk = nullptr, *bconst = nullptr;
+    std::vector<int> h_bu, h_rt;  // unknown, resolved (non-boundary) target
+    std::vector<double> h_rk;     // resolved coefficient
+    // vectors: x (and y, the second velocity buffer of the smoother), b, r
+    Vec4<float> x32, y32, b32, r32;
+    Vec4<double> x64, y64, b64, r64;
+};
+
+struct GraphSlot {
+    cudaGraphExec_t exec = nullptr;
+    long long kernels = 0;  // kernel nodes replayed per launch
+};
+
+struct RawFields {
+    float *nu = nullptr, *ro = nullptr, *nxx = nullptr, *nxy = nullptr, *nxz = nullptr, *nyz = nullptr;
+};
+
+class Solver {
+  public:
+    explicit Solver(int device);
+    ~Solver();
+
+    void set_grid(long nx, long ny, long nz, const double *gx, const double *gy, const double *gz,
+                  const p2_params &p);
+    void set_bc(const int *bondm, long bondm_len, const float *bondv1, const int *bondn1, long bondnum);
+    void upload_nodes(const float *nu, const float *ro, const float *nxx, const float *nxy, const float *nxz,
+                      const float *nyz);
+    void set_initial(const float *vx, const float *vy, const float *vz, const double *pr);
+    p2_solve_info solve();
+    void get_solution(double *vx, double *vy, double *vz, double *pr);
+
+    void upload_markers(long nmark, const float *mx, const float *my, const float *mz, const signed char *mt,
+                        int nrock, const double *n0, const double *n1, const double *rho);
+    void ronurecalc_device();
+
+    // test hooks (FP64, interleaved [P,Vx,Vy,Vz] per node)
+    void debug_apply(int l, const double *x, double *y);
+    void debug_restrict(int lc, const double *fine_res, double *coarse_rhs, int compat);
+    void debug_prolong(int lc, const double *coarse_x, double *fine_x);
+    void debug_level_fields(float *nu, float *ro);
+    double debug_time_smoother(int level, int passes);
+    bool verbose = false;
+
+    int dev;
+    cudaStream_t st = nullptr;
+    cudaEvent_t ev[8];
+    p2_params prm{};
+    std::vector<Level> L;
+    long total_nodes = 0;
+    bool grid_ready = false, bc_ready = false, nodes_ready = false, markers_ready = false;
+    RawFields f0;
+
+    // markers
+    long nmk = 0;
+    float *mk_x = nullptr, *mk_y = nullptr, *mk_z = nullptr;
+    signed char *mk_t = nullptr;
+    unsigned *mk_key[2] = {nullptr, nullptr}, *mk_val[2] = {nullptr, nullptr}, *mk_hist = nullptr;
+    int mk_cur = 0;
+    float4 *mk_sorted = nullptr;
+    int *cell_start = nullptr, *cell_end = nullptr;
+    double *rock_f = nullptr, *rock_ro = nullptr;
+    double *d_g[3] = {nullptr, nullptr, nullptr};
+    float *mk_nodes[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+
+  private:
+    template <typename T>
+    LevelView<T> view(int l, bool raw_clamp) const;
+    void drop_graphs();
+    void allocate_work();
+    void build_coarse_index();
+    void coarse_setup();
+    template <typename T>
+    void coarse_solve(Vec4<T> &b, Vec4<T> &x);
+    template <typename T>
+    void bc_set(int l, Vec4<T> &x, Vec4<T> &b);
+    template <typename T>
+    void smooth(int l, int sweeps);
+    template <typename T>
+    void level_residual(int l);
+    template <typename T>
+    void vcycle();
+    template <typename T>
+    void run_vcycle_graph();
+    void set_nodes_device();
+    void dots_sync(const DotJobs &jobs);
+    void rows0(const Vec4<double> &x, Vec4<double> &out, Vec4<float> *r32, int mode);
+    void precondition(Vec4<double> &z);
+    void debug_prepare();
+
+    DeviceArena arena, grid_arena, marker_arena;
+    std::array<GraphSlot, 2> graphs;
+    int restart = 8;
+    Vec4<double> gx, gb, gr;
+    std::vector<Vec4<double>> Z, Q;
+    double *partial = nullptr, *dots = nullptr, *scal = nullptr;
+    double *hdots_raw = nullptr;
+    std::shared_ptr<double> hdots;
+    // coarsest level
+    int nF = 0;
+    std::vector<int> coarse_col;
+    int *d_free = nullptr, *d_colmap = nullptr, *d_crt = nullptr;
+    float *d_crk = nullptr;
+    double *A_c = nullptr, *Ainv64 = nullptr;
+    float *Ainv32 = nullptr;
+    int *d_ipiv = nullptr, *d_info = nullptr;
+    double *probes = nullptr;
+    double *cb64 = nullptr, *cx64 = nullptr;
+    float *cb32 = nullptr, *cx32 = nullptr;
+};
+
+}  // namespace p2

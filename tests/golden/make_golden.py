@@ -1,0 +1,127 @@
+"""Generate the golden vectors in tests/golden/*.npz from the reference itself.
+
+Runs the reference's own C sources (oracle/_ref/libp2ref.so, built by
+`make -C oracle ref` from the reference tree) single-threaded on small seeded
+models and stores, per case:
+  markers (x, y, z, type)          the exact inputs (float32 / int8)
+  ronurecalc node fields            pardiso/mark3mg.c:630 (one thread)
+  op_lev{l}                         y = A x of the reference's assembled rows
+                                    (gausmat2 row store, move3mgNew.c:2329-2662)
+                                    for x = probe_vector(level)
+  restrict_lev{l}, prolong_lev{l}   vprestrict / vpprolong (move3mgNew.c:3965,
+                                    3534) of probe vectors
+  level_nu, level_ro                nu/ro of all levels after ronurestrict
+  sol_{pr,vx,vy,vz}, rhs            the exact discrete solution of the
+                                    reference's level-0 system (direct sparse
+                                    LU of its assembled rows, pressure reset
+                                    to pinit at the pinned cell)
+
+Usage: OMP_NUM_THREADS=1 python tests/golden/make_golden.py
+"""
+import os
+import sys
+
+os.environ["OMP_NUM_THREADS"] = "1"
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+import scipy.sparse as sp  # noqa: E402
+import scipy.sparse.linalg as spl  # noqa: E402
+
+from pardiso2_b200 import model as M  # noqa: E402
+
+CASES = {
+    "sphere17": lambda: M.sphere_model(17, 2, (2, 2, 2), seed=1, eta_sphere=1e3),
+    "spheres21": lambda: M.random_spheres_model(21, 2, 4, (1e-2, 1e2), markers=(2, 2, 2), seed=7,
+                                                name="spheres21"),
+}
+
+
+def probe_vector(n_nodes: int, salt: int) -> np.ndarray:
+    """Deterministic test vector (no RNG stream dependence)."""
+    k = np.arange(n_nodes * 4, dtype=np.float64)
+    return np.sin(0.37 * k + salt) + 0.5 * np.cos(0.011 * k * (salt + 1))
+
+
+def pin_rows(m, lev):
+    """Unknown indices (level-local, interleaved) of pure-constant pressure rows."""
+    lv = m.levels
+    off = lv.mgp[lev]
+    out = []
+    for u in range(lv.mgn[lev]):
+        b = m.bc.bondm[(off + u) * 4]
+        if b and m.bc.bondn1[b] == 0:
+            out.append(u * 4)
+    return np.array(out, dtype=np.int64)
+
+
+def make_case(name, builder):
+    from oracle import refdrv
+    m = builder()
+    nl = m.multinum
+    r = refdrv.RefModel(m)
+    r.ronurecalc()
+    nodes = r.nodes()
+    r.first_iteration()
+    out = {"markx": m.markx, "marky": m.marky, "markz": m.markz, "markt": m.markt}
+    out.update({"node_" + k: v for k, v in nodes.items()})
+    lf = r.level_fields()
+    out["level_nu"], out["level_ro"] = lf["nu"], lf["ro"]
+    for lev in range(nl):
+        row, col, val, rhs = r.rows(lev)
+        N = int(r.mgn[lev]) * 4
+        x = probe_vector(int(r.mgn[lev]), lev)
+        y = np.zeros(N)
+        np.add.at(y, row, val * x[col])
+        has = np.zeros(N, bool)
+        has[row] = True
+        out["op_lev%d" % lev] = y
+        out["op_rows_lev%d" % lev] = has
+        if lev == 0:
+            out["rhs"] = rhs
+            g = np.where(~has)[0]
+            A = sp.coo_matrix((np.concatenate([val, np.ones(g.size)]),
+                               (np.concatenate([row, g]), np.concatenate([col, g]))), shape=(N, N)).tocsc()
+            b = rhs.copy()
+            b[g] = 0.0
+            lu = spl.splu(A)
+            x0 = lu.solve(b)
+            for _ in range(3):  # iterative refinement
+                x0 += lu.solve(b - A @ x0)
+            res = np.linalg.norm(A @ x0 - b) / np.linalg.norm(b)
+            assert res < 1e-11, res
+            out["sol_rel_residual"] = np.array(res)
+            p = m.params
+            nx, ny, nz = m.shape
+            pin = ((p.pin[2] * nx + p.pin[0]) * ny + p.pin[1]) * 4
+            x0[0::4] += p.pinit - x0[pin]
+            sol = x0.reshape(-1, 4)
+            kk, ii, jj = np.meshgrid(np.arange(nz), np.arange(nx), np.arange(ny), indexing="ij")
+            kk, ii, jj = kk.ravel(), ii.ravel(), jj.ravel()
+            out["sol_pr"] = np.where((ii > 0) & (jj > 0) & (kk > 0), sol[:, 0], 0.0)
+            out["sol_vx"] = np.where((jj < ny - 1) & (kk < nz - 1), sol[:, 1], 0.0)
+            out["sol_vy"] = np.where((ii < nx - 1) & (kk < nz - 1), sol[:, 2], 0.0)
+            out["sol_vz"] = np.where((ii < nx - 1) & (jj < ny - 1), sol[:, 3], 0.0)
+    for lc in range(1, nl + 1):
+        nf, nc = int(r.mgn[lc - 1]), int(r.mgn[lc])
+        fr = probe_vector(nf, 10 + lc)
+        fr[pin_rows(m, lc - 1)] = 0.0
+        out["restrict_in_lev%d" % lc] = fr
+        out["restrict_lev%d" % lc] = r.restrict(lc, fr)
+        xc = probe_vector(nc, 20 + lc)
+        xf = probe_vector(nf, 30 + lc)
+        out["prolong_lev%d" % lc] = r.prolong(lc, xc, xf)
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+    print(name, "written", {k: np.asarray(v).shape for k, v in out.items()})
+
+
+if __name__ == "__main__":
+    # the reference keeps its state in globals: one case per process
+    if len(sys.argv) > 1:
+        make_case(sys.argv[1], CASES[sys.argv[1]])
+    else:
+        import subprocess
+        for c in CASES:
+            subprocess.run([sys.executable, os.path.abspath(__file__), c], check=True)

@@ -1,0 +1,54 @@
+"""The C-ABI library loads and exports every entry point include/p2cuda.h
+declares; without a GPU, p2_create fails cleanly (CPU)."""
+import ctypes
+import os
+import re
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_functions():
+    src = open(os.path.join(ROOT, "include", "p2cuda.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(p2_[a-z_0-9]+)\s*\(", src)))
+
+
+def test_header_declares_the_reference_entry_points():
+    names = declared_functions()
+    for f in ("p2_stokes_solve", "p2_ronurecalc", "p2_set_grid", "p2_set_bc", "p2_set_nodes", "p2_create"):
+        assert f in names
+
+
+def test_library_exports_every_declared_symbol():
+    from pardiso2_b200 import capi
+    lib = capi.load()
+    for f in declared_functions():
+        assert hasattr(lib, f), f
+    assert set(capi.EXPORTED) == set(declared_functions())
+
+
+def test_library_is_sm100a_and_self_contained():
+    from pardiso2_b200 import capi
+    out = os.popen("ldd %s" % capi.LIB_PATH).read()
+    assert "libcudart" not in out  # cudart linked statically: the .so travels alone
+
+
+def test_create_without_gpu_reports_cuda_error(gpu_available):
+    if gpu_available:
+        pytest.skip("a GPU is present")
+    from pardiso2_b200 import capi
+    lib = capi.load()
+    h = ctypes.c_void_p()
+    assert lib.p2_create(ctypes.byref(h), 0) == 2  # P2_ERR_CUDA
+    assert not h.value
+
+
+def test_default_params_are_the_reference_defaults():
+    from pardiso2_b200 import capi
+    p = capi.default_params()
+    # pardiso/mode.t3c:89-93
+    assert (p.p0koef, p.p1koef, p.p2koef, p.v0koef, p.v1koef) == (0.3, 1.0, 0.0, 1.0, 1.0)
+    assert (p.nubeg, p.nuend, p.viscmod) == (1.0, 1e4, 0)
+    assert p.tol == 1e-8 and p.precision == 0
