@@ -130,6 +130,32 @@ p2_status p2_upload_markers(p2_ctx *ctx, long nmark, const float *markx, const f
 p2_status p2_ronurecalc_resident(p2_ctx *ctx, double *ms);
 p2_status p2_get_nodes(p2_ctx *ctx, float *nu, float *ro, float *nxx, float *nxy, float *nxz, float *nyz);
 
+/* The p2_ronurecalc interpolation for callers that cannot allocate device
+ * memory: a host code whose device memory is all handed out by its own pool
+ * at start-up, or one that cannot take the device-wide synchronisation that
+ * cudaMalloc/cudaFree imply inside its time loop.  This entry point has no
+ * counterpart in the reference.  It needs no p2_ctx and allocates nothing:
+ * its scratch is one fixed 9.1 MiB device array inside this library, which
+ * every GPU that loads the library holds until the process exits.
+ *   Limits: at most 262144 markers, 131072 cells and 1024 gridlines per axis;
+ *   larger sizes return P2_ERR_ARG and a message naming the limit.
+ *   Arrays: gridlines, params (viscmod, nukoef, nubeg, nuend are read) and the
+ *   rock tables are host arrays; markx..markt and nu..nyz are device arrays
+ *   on the current device (nu..nyz of nx*ny*nz floats, in/out as in
+ *   p2_ronurecalc).  Work runs on `stream` (a cudaStream_t; NULL = default).
+ *   The call waits once for the stream (a check of the marker types) and
+ *   returns with the node pass queued on it.
+ *   The first call on a device looks up the scratch array's device address
+ *   with that device current; make that first call before any stream capture
+ *   begins.  All calls share the one array: calls whose work overlaps on the
+ *   GPU (different streams or host threads without ordering) race.
+ *   On an error, a message is written to err (errlen bytes; may be NULL). */
+p2_status p2_ronurecalc_noalloc(int nx, int ny, int nz, const double *gx, const double *gy, const double *gz,
+                                const p2_params *prm, int nrock, const double *markn0, const double *markn1,
+                                const double *markro, long nmark, const float *markx, const float *marky,
+                                const float *markz, const signed char *markt, float *nu, float *ro, float *nxx,
+                                float *nxy, float *nxz, float *nyz, void *stream, char *err, long errlen);
+
 /* Test hooks (no counterpart in the reference; they expose single stages so
  * parity tests can compare them with the reference's own functions).  Vectors
  * are FP64, interleaved [P,Vx,Vy,Vz] per node of the given level (the layout

@@ -20,7 +20,7 @@ STATUS = {0: "P2_OK", 1: "P2_ERR_ARG", 2: "P2_ERR_CUDA", 3: "P2_ERR_NOMEM", 4: "
 EXPORTED = ["p2_default_params", "p2_create", "p2_destroy", "p2_last_error", "p2_set_grid", "p2_set_bc",
             "p2_set_nodes", "p2_stokes_solve", "p2_stokes_solve_resident", "p2_get_solution", "p2_ronurecalc",
             "p2_upload_markers", "p2_ronurecalc_resident", "p2_get_nodes", "p2_debug_apply", "p2_debug_restrict",
-            "p2_debug_prolong", "p2_debug_level_fields", "p2_debug_time_smoother"]
+            "p2_debug_prolong", "p2_debug_level_fields", "p2_debug_time_smoother", "p2_ronurecalc_noalloc"]
 
 
 class Params(C.Structure):

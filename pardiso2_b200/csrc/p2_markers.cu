@@ -11,6 +11,10 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <mutex>
 #include <vector>
 
 #include "p2_internal.cuh"
@@ -381,3 +385,209 @@ void Solver::ronurecalc_device()
 }
 
 }  // namespace p2
+
+// ---------------------------------------------------------------------------
+// p2_ronurecalc_noalloc: the interpolation above for callers that must not
+// allocate device memory (a host code whose device memory is all handed out
+// by its own pool at start-up, or one that cannot afford the device-wide
+// synchronisation cudaMalloc/cudaFree imply inside its time loop).  The sort
+// keys, indices, histograms, permuted markers, cell ranges, gridlines and rock
+// tables live in one file-scope device array of fixed size instead of a
+// context's buffers; markers and node fields are the caller's device arrays.
+// The kernels are the ones above, unchanged.
+namespace p2na {
+
+constexpr long kMaxMarkers = 1L << 18;  // 262144 markers
+constexpr long kMaxCells = 1L << 17;    // 131072 cells, e.g. 50 x 50 x 52
+constexpr int kMaxLines = 1024;         // gridlines per axis
+constexpr int kMaxTiles = (int)((kMaxMarkers + p2::kTile - 1) / p2::kTile);
+constexpr size_t up(size_t b) { return (b + 255) & ~(size_t)255; }
+constexpr size_t kKeyBytes = up(sizeof(unsigned) * kMaxMarkers);
+constexpr size_t kOffKeys = 0;  // key[0], key[1], idx[0], idx[1]
+constexpr size_t kOffSorted = kOffKeys + 4 * kKeyBytes;
+constexpr size_t kOffHist = kOffSorted + up(sizeof(float4) * kMaxMarkers);
+constexpr size_t kOffCells = kOffHist + up(sizeof(unsigned) * p2::kBuckets * kMaxTiles);
+constexpr size_t kCellBytes = up(sizeof(int) * kMaxCells);
+constexpr size_t kOffLines = kOffCells + 2 * kCellBytes;
+constexpr size_t kLineBytes = up(sizeof(double) * kMaxLines);
+constexpr size_t kOffRocks = kOffLines + 3 * kLineBytes;
+constexpr size_t kOffFlag = kOffRocks + 2 * up(sizeof(double) * 256);
+constexpr size_t kBytes = kOffFlag + 256;  // 9531648 bytes (9.1 MiB)
+constexpr int kMaxDevices = 64;
+
+}  // namespace p2na
+
+// Held by every GPU that loads this library, until the process exits.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[p2na::kBytes];
+
+namespace p2na {
+
+static std::mutex g_mu;
+static unsigned char *g_addr[kMaxDevices];  // device address of the array, per device
+
+// markers the gather would read a rock entry for (type < 50) without one
+__global__ void k_count_bad_types(long nmark, const signed char *mt, int nrock, unsigned *bad)
+{
+    long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= nmark) return;
+    int t = mt[q];
+    if (t < 50 && (t < 0 || t >= nrock)) atomicAdd(bad, 1u);
+}
+
+static p2_status fail(char *err, long errlen, p2_status code, const char *fmt, ...)
+{
+    if (err && errlen > 0) {
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(err, (size_t)errlen, fmt, ap);
+        va_end(ap);
+    }
+    return code;
+}
+
+static bool on_device(const void *p)
+{
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+static bool increasing(const double *g, int n)
+{
+    for (int i = 1; i < n; i++)
+        if (!(g[i] > g[i - 1])) return false;
+    return true;
+}
+
+}  // namespace p2na
+
+extern "C" p2_status p2_ronurecalc_noalloc(int nx, int ny, int nz, const double *gx, const double *gy,
+                                           const double *gz, const p2_params *prm, int nrock, const double *markn0,
+                                           const double *markn1, const double *markro, long nmark,
+                                           const float *markx, const float *marky, const float *markz,
+                                           const signed char *markt, float *nu, float *ro, float *nxx, float *nxy,
+                                           float *nxz, float *nyz, void *stream, char *err, long errlen)
+{
+    using namespace p2na;
+    using p2::nb;
+    if (err && errlen > 0) err[0] = 0;
+    if (!prm || !gx || !gy || !gz || !markn0 || !markn1 || !markro)
+        return fail(err, errlen, P2_ERR_ARG, "null parameter, gridline or rock-table pointer");
+    if (nx < 2 || ny < 2 || nz < 2 || nx > kMaxLines || ny > kMaxLines || nz > kMaxLines)
+        return fail(err, errlen, P2_ERR_ARG, "grid %d x %d x %d: each axis needs 2..%d gridlines", nx, ny, nz,
+                    kMaxLines);
+    long ncell = (long)(nx - 1) * (ny - 1) * (nz - 1);
+    if (ncell > kMaxCells)
+        return fail(err, errlen, P2_ERR_ARG, "%ld cells exceed the maximum of %ld for the static scratch", ncell,
+                    kMaxCells);
+    if (nmark < 0 || nmark > kMaxMarkers)
+        return fail(err, errlen, P2_ERR_ARG, "%ld markers: the static scratch holds 0..%ld", nmark, kMaxMarkers);
+    if (!increasing(gx, nx) || !increasing(gy, ny) || !increasing(gz, nz))
+        return fail(err, errlen, P2_ERR_ARG, "gridlines must be strictly increasing");
+    if (prm->viscmod < 0 || prm->viscmod > 2) return fail(err, errlen, P2_ERR_ARG, "viscmod must be 0, 1 or 2");
+    if (nrock <= 0 || nrock > 256) return fail(err, errlen, P2_ERR_ARG, "rock table size %d out of 1..256", nrock);
+    // rock tables as in upload_markers: constant per-type viscosity (mark3mg.c:1481-1482) and density (1429)
+    double f[256], r[256];
+    for (int t = 0; t < 256; t++) { f[t] = 1.0; r[t] = 0.0; }
+    for (int t = 0; t < nrock && t < 50; t++) {
+        if (markn0[t] != markn1[t])
+            return fail(err, errlen, P2_ERR_UNSUPPORTED, "rock type %d has a power-law viscosity (markn0 != markn1)",
+                        t);
+        double mnu = markn0[t];
+        if (mnu < prm->nubeg) mnu = prm->nubeg;
+        if (mnu > prm->nuend) mnu = prm->nuend;
+        f[t] = prm->viscmod == 0 ? mnu : (prm->viscmod == 1 ? std::log(mnu) : 1.0 / mnu);
+        r[t] = markro[t];
+    }
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+        cudaGetLastError();
+        return fail(err, errlen, P2_ERR_CUDA, "no usable current CUDA device");
+    }
+    float *outs[6] = {nu, ro, nxx, nxy, nxz, nyz};
+    for (int q = 0; q < 6; q++)
+        if (!outs[q] || !on_device(outs[q]))
+            return fail(err, errlen, P2_ERR_ARG, "node field %d is not a device array", q);
+    if (nmark > 0 && (!markx || !marky || !markz || !markt || !on_device(markx) || !on_device(marky) ||
+                      !on_device(markz) || !on_device(markt)))
+        return fail(err, errlen, P2_ERR_ARG, "marker arrays must be device arrays");
+    // the array's host-side name is not a device address: look the address up once per device
+    unsigned char *base;
+    {
+        std::lock_guard<std::mutex> lk(g_mu);
+        if (!g_addr[dev]) {
+            cudaError_t e = cudaGetSymbolAddress((void **)&g_addr[dev], g_noalloc_scratch);
+            if (e != cudaSuccess) {
+                g_addr[dev] = nullptr;
+                cudaGetLastError();
+                return fail(err, errlen, P2_ERR_CUDA, "cudaGetSymbolAddress(scratch): %s", cudaGetErrorString(e));
+            }
+        }
+        base = g_addr[dev];
+    }
+    unsigned *key[2] = {(unsigned *)(base + kOffKeys), (unsigned *)(base + kOffKeys + kKeyBytes)};
+    unsigned *val[2] = {(unsigned *)(base + kOffKeys + 2 * kKeyBytes), (unsigned *)(base + kOffKeys + 3 * kKeyBytes)};
+    float4 *sorted = (float4 *)(base + kOffSorted);
+    unsigned *hist = (unsigned *)(base + kOffHist);
+    int *cstart = (int *)(base + kOffCells), *cend = (int *)(base + kOffCells + kCellBytes);
+    double *dg[3] = {(double *)(base + kOffLines), (double *)(base + kOffLines + kLineBytes),
+                     (double *)(base + kOffLines + 2 * kLineBytes)};
+    double *rf = (double *)(base + kOffRocks), *rr = (double *)(base + kOffRocks + up(sizeof(double) * 256));
+    unsigned *bad = (unsigned *)(base + kOffFlag);
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaError_t e = cudaSuccess;
+#define P2NA_TRY(expr)                                                                                     \
+    do {                                                                                                   \
+        if ((e = (expr)) != cudaSuccess) {                                                                 \
+            cudaGetLastError();                                                                            \
+            return fail(err, errlen, P2_ERR_CUDA, "%s: %s", #expr, cudaGetErrorString(e));                 \
+        }                                                                                                  \
+    } while (0)
+    P2NA_TRY(cudaMemcpyAsync(dg[0], gx, sizeof(double) * nx, cudaMemcpyHostToDevice, s));
+    P2NA_TRY(cudaMemcpyAsync(dg[1], gy, sizeof(double) * ny, cudaMemcpyHostToDevice, s));
+    P2NA_TRY(cudaMemcpyAsync(dg[2], gz, sizeof(double) * nz, cudaMemcpyHostToDevice, s));
+    P2NA_TRY(cudaMemcpyAsync(rf, f, sizeof(f), cudaMemcpyHostToDevice, s));
+    P2NA_TRY(cudaMemcpyAsync(rr, r, sizeof(r), cudaMemcpyHostToDevice, s));
+    // the array keeps the previous call's contents: the cell ranges and the bad-type count start at zero
+    P2NA_TRY(cudaMemsetAsync(cstart, 0, sizeof(int) * ncell, s));
+    P2NA_TRY(cudaMemsetAsync(cend, 0, sizeof(int) * ncell, s));
+    P2NA_TRY(cudaMemsetAsync(bad, 0, sizeof(unsigned), s));
+    int cur = 0;
+    if (nmark > 0) {
+        p2na::k_count_bad_types<<<nb(nmark), 256, 0, s>>>(nmark, markt, nrock, bad);
+        P2NA_TRY(cudaGetLastError());
+        unsigned nbad = 0;
+        P2NA_TRY(cudaMemcpyAsync(&nbad, bad, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+        P2NA_TRY(cudaStreamSynchronize(s));
+        if (nbad)
+            return fail(err, errlen, P2_ERR_ARG, "%u markers have a type below 50 without a rock entry", nbad);
+        unsigned sentinel = (unsigned)ncell;
+        int bits = 1;
+        while ((1ul << bits) <= (unsigned long)sentinel) bits++;
+        int passes = (bits + p2::kRadixBits - 1) / p2::kRadixBits;
+        double xsize = gx[nx - 1] - gx[0], ysize = gy[ny - 1] - gy[0], zsize = gz[nz - 1] - gz[0];
+        p2::k_mark_keys<<<nb(nmark), 256, 0, s>>>(nmark, markx, marky, markz, markt, dg[0], dg[1], dg[2], nx, ny,
+                                                  nz, xsize, ysize, zsize, sentinel, key[0], val[0]);
+        int ntiles = (int)((nmark + p2::kTile - 1) / p2::kTile);
+        for (int p = 0; p < passes; p++) {
+            int shift = p * p2::kRadixBits;
+            p2::k_radix_hist<<<ntiles, 256, 0, s>>>(nmark, key[cur], shift, hist, ntiles);
+            p2::k_radix_scan<<<1, 1024, 0, s>>>(hist, (long)p2::kBuckets * ntiles);
+            p2::k_radix_scatter<<<ntiles, 256, 0, s>>>(nmark, key[cur], val[cur], key[1 - cur], val[1 - cur], shift,
+                                                       hist, ntiles);
+            cur = 1 - cur;
+        }
+        p2::k_cell_bounds<<<nb(nmark), 256, 0, s>>>(nmark, key[cur], sentinel, cstart, cend);
+        p2::k_permute<<<nb(nmark), 256, 0, s>>>(nmark, val[cur], markx, marky, markz, markt, sorted);
+    }
+    p2::k_node_gather<<<nb((long)nx * ny * nz, 128), 128, 0, s>>>(nx, ny, nz, dg[0], dg[1], dg[2], cstart, cend,
+                                                                  val[cur], sorted, rf, rr, prm->nukoef,
+                                                                  prm->viscmod, prm->nubeg, prm->nuend, nu, ro, nxx,
+                                                                  nxy, nxz, nyz);
+    P2NA_TRY(cudaGetLastError());
+#undef P2NA_TRY
+    return P2_OK;
+}
