@@ -1,12 +1,23 @@
-// Coarsest-level direct solve: dense FP64 LU with partial pivoting and its
-// explicit inverse, all on the device.
+// Coarsest-level direct solve: FP64 LU with partial pivoting and its explicit
+// inverse, all on the device.
 //
 // Replaces the MKL PARDISO call of the reference (pardiso/gaus3mg_SerieMG.c:
 // 64-309; phases 11/22/33 at 170/185/198).  The coarsest operator is reduced
 // to its free unknowns (boundary rows, ghosts and the pinned pressure cell are
-// eliminated), factored once per solve (P A = L U, right-looking, panel width
-// kNB), and inverted (X = U^-1 L^-1 P) so that each V-cycle applies it as one
-// GEMV on the B200.
+// eliminated).  In that ordering it is banded: row r has non-zeros only in
+// columns [r - kl, r + ku], about one z-plane of unknowns either side.  The
+// factorisation is the right-looking blocked LU of LAPACK's gbtrf, restricted
+// to the band and kept in dense column-major storage:
+//   per panel of kPB columns at k0 (rows [k0, r1), r1 = k0 + kPB + kl):
+//     1. factor the panel in shared memory (pivot = largest |a|, smallest row
+//        on ties), row interchanges applied inside the panel only;
+//     2. apply the interchanges to the columns [k0 + kPB, c1) (c1 = r1 + ku,
+//        the reach of U after pivoting) and solve U12 = L11^-1 A12;
+//     3. A22 -= L21 U12 on rows [k0 + kPB, r1) x columns [k0 + kPB, c1).
+// Interchanges are not applied to earlier columns, so L is the product of the
+// panels' (P_k, L_k) in order.  The inverse X = A^-1 replays them on the
+// identity (forward) and then solves with the banded U (backward), so each
+// V-cycle applies the coarsest solve as one GEMV.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -16,22 +27,98 @@
 
 namespace p2 {
 
-constexpr int kNB = 32;
+constexpr int kPB = 32;                                  // panel width
+constexpr int kPanelThreads = 512;
+constexpr int kMaxPanelBytes = 200 * 1024;               // shared-memory panel
+constexpr int kMaxPanelRows = kMaxPanelBytes / (8 * kPB);  // 800 rows
 
 // ---------------------------------------------------------------------------
-// Panel factorisation of columns [k0, k0+nb) over rows [k0, n) (column-major,
-// leading dimension n), one block.  Pivot: largest |a|, smallest row on ties.
-__global__ void k_lu_panel(double *A, int n, int k0, int nb, int *ipiv, int *info)
+// Panel [k0, k0+nb) x rows [k0, r1) factored in shared memory (column-major,
+// leading dimension m = r1 - k0).
+__global__ void __launch_bounds__(kPanelThreads) k_panel_smem(double *A, int lda, int k0, int nb, int r1, int *ipiv,
+                                                              int *info)
+{
+    extern __shared__ double P[];
+    __shared__ double sv[kPanelThreads / 32];
+    __shared__ int si[kPanelThreads / 32];
+    __shared__ int piv;
+    const int m = r1 - k0;
+    for (int t = threadIdx.x; t < m * nb; t += blockDim.x) {
+        int r = t % m, c = t / m;
+        P[t] = A[(size_t)(k0 + c) * lda + k0 + r];
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int jj = 0; jj < nb; jj++) {
+        double *cj = P + (size_t)jj * m;
+        double best = -1.0;
+        int bi = m;
+        for (int i = jj + threadIdx.x; i < m; i += blockDim.x) {
+            double v = fabs(cj[i]);
+            if (v > best) { best = v; bi = i; }
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            double ov = __shfl_down_sync(0xffffffffu, best, o);
+            int oi = __shfl_down_sync(0xffffffffu, bi, o);
+            if (ov > best || (ov == best && oi < bi)) { best = ov; bi = oi; }
+        }
+        if (lane == 0) { sv[w] = best; si[w] = bi; }
+        __syncthreads();
+        if (w == 0) {
+            constexpr int nw = kPanelThreads / 32;
+            best = lane < nw ? sv[lane] : -1.0;
+            bi = lane < nw ? si[lane] : m;
+            for (int o = 16; o > 0; o >>= 1) {
+                double ov = __shfl_down_sync(0xffffffffu, best, o);
+                int oi = __shfl_down_sync(0xffffffffu, bi, o);
+                if (ov > best || (ov == best && oi < bi)) { best = ov; bi = oi; }
+            }
+            if (lane == 0) {
+                if (!(best > 0.0)) {
+                    if (*info == 0) *info = k0 + jj + 1;
+                    bi = jj;
+                }
+                piv = bi;
+                ipiv[k0 + jj] = k0 + bi;
+            }
+        }
+        __syncthreads();
+        const int p = piv;
+        if (p != jj && threadIdx.x < nb) {
+            double *c = P + (size_t)threadIdx.x * m;
+            double t = c[jj];
+            c[jj] = c[p];
+            c[p] = t;
+        }
+        __syncthreads();
+        const double d = cj[jj];
+        const double inv = d != 0.0 ? 1.0 / d : 0.0;
+        for (int i = jj + 1 + threadIdx.x; i < m; i += blockDim.x) {
+            double l = cj[i] * inv;
+            cj[i] = l;
+            for (int c = jj + 1; c < nb; c++) P[(size_t)c * m + i] -= l * P[(size_t)c * m + jj];
+        }
+        __syncthreads();
+    }
+    for (int t = threadIdx.x; t < m * nb; t += blockDim.x) {
+        int r = t % m, c = t / m;
+        A[(size_t)(k0 + c) * lda + k0 + r] = P[t];
+    }
+}
+
+// Same factorisation in global memory, one block, for bands too wide for the
+// shared-memory panel.
+__global__ void k_panel_global(double *A, int lda, int k0, int nb, int r1, int *ipiv, int *info)
 {
     __shared__ double sv[32];
     __shared__ int si[32];
     __shared__ int piv;
     for (int jj = 0; jj < nb; jj++) {
         int j = k0 + jj;
-        double *colj = A + (size_t)j * n;
+        double *colj = A + (size_t)j * lda;
         double best = -1.0;
-        int bi = n;
-        for (int i = j + threadIdx.x; i < n; i += blockDim.x) {
+        int bi = r1;
+        for (int i = j + threadIdx.x; i < r1; i += blockDim.x) {
             double v = fabs(colj[i]);
             if (v > best) { best = v; bi = i; }
         }
@@ -46,7 +133,7 @@ __global__ void k_lu_panel(double *A, int n, int k0, int nb, int *ipiv, int *inf
         if (threadIdx.x < 32) {
             int nw = blockDim.x >> 5;
             best = threadIdx.x < nw ? sv[threadIdx.x] : -1.0;
-            bi = threadIdx.x < nw ? si[threadIdx.x] : n;
+            bi = threadIdx.x < nw ? si[threadIdx.x] : r1;
             for (int o = 16; o > 0; o >>= 1) {
                 double ov = __shfl_down_sync(0xffffffffu, best, o);
                 int oi = __shfl_down_sync(0xffffffffu, bi, o);
@@ -65,63 +152,64 @@ __global__ void k_lu_panel(double *A, int n, int k0, int nb, int *ipiv, int *inf
         int p = piv;
         if (p != j)
             for (int c = k0 + threadIdx.x; c < k0 + nb; c += blockDim.x) {
-                double t = A[(size_t)c * n + j];
-                A[(size_t)c * n + j] = A[(size_t)c * n + p];
-                A[(size_t)c * n + p] = t;
+                double t = A[(size_t)c * lda + j];
+                A[(size_t)c * lda + j] = A[(size_t)c * lda + p];
+                A[(size_t)c * lda + p] = t;
             }
         __syncthreads();
         double d = colj[j];
         if (d != 0.0) {
             double inv = 1.0 / d;
-            for (int i = j + 1 + threadIdx.x; i < n; i += blockDim.x) colj[i] *= inv;
+            for (int i = j + 1 + threadIdx.x; i < r1; i += blockDim.x) colj[i] *= inv;
         }
         __syncthreads();
-        for (int i = j + 1 + threadIdx.x; i < n; i += blockDim.x) {
+        for (int i = j + 1 + threadIdx.x; i < r1; i += blockDim.x) {
             double l = colj[i];
-            for (int c = j + 1; c < k0 + nb; c++) A[(size_t)c * n + i] -= l * A[(size_t)c * n + j];
+            for (int c = j + 1; c < k0 + nb; c++) A[(size_t)c * lda + i] -= l * A[(size_t)c * lda + j];
         }
         __syncthreads();
     }
 }
 
-// Apply the panel's row interchanges to the columns outside the panel.
-__global__ void k_lu_swap(double *A, int n, int k0, int nb, const int *ipiv)
+// For columns c in [c0, c1) of B: apply the panel's interchanges (rows k0..)
+// then B[k0:k0+nb, c] = L11^-1 B[k0:k0+nb, c], L11 unit lower from A.
+__global__ void k_swap_trsm_lower(const double *A, int lda, int k0, int nb, const int *ipiv, double *B, int ldb,
+                                  int c0, int c1)
 {
-    int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= n || (c >= k0 && c < k0 + nb)) return;
-    double *col = A + (size_t)c * n;
-    for (int jj = 0; jj < nb; jj++) {
-        int j = k0 + jj, p = ipiv[j];
-        if (p != j) { double t = col[j]; col[j] = col[p]; col[p] = t; }
-    }
-}
-
-// B[k0:k0+nb, c] = L11^-1 B[k0:k0+nb, c] (unit lower) for columns c in [c0, c1);
-// L11 = A[k0:k0+nb, k0:k0+nb].
-__global__ void k_trsm_lower(const double *A, int lda, int k0, int nb, double *B, int ldb, int c0, int c1)
-{
-    __shared__ double L[kNB][kNB + 1];
+    __shared__ double L[kPB][kPB + 1];
+    __shared__ int pv[kPB];
     for (int t = threadIdx.x; t < nb * nb; t += blockDim.x) {
         int r = t % nb, s = t / nb;
         L[r][s] = A[(size_t)(k0 + s) * lda + k0 + r];
     }
+    if (threadIdx.x < nb) pv[threadIdx.x] = ipiv ? ipiv[k0 + threadIdx.x] : k0 + threadIdx.x;
     __syncthreads();
     int c = c0 + blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= c1) return;
-    double x[kNB];
-    double *col = B + (size_t)c * ldb + k0;
-    for (int r = 0; r < nb; r++) {
-        double v = col[r];
-        for (int s = 0; s < r; s++) v -= L[r][s] * x[s];
-        x[r] = v;
+    double *col = B + (size_t)c * ldb;
+    for (int jj = 0; jj < nb; jj++) {
+        int j = k0 + jj, p = pv[jj];
+        if (p != j) { double t = col[j]; col[j] = col[p]; col[p] = t; }
     }
-    for (int r = 0; r < nb; r++) col[r] = x[r];
+    double x[kPB];
+    col += k0;
+#pragma unroll
+    for (int r = 0; r < kPB; r++) {
+        if (r < nb) {
+            double v = col[r];
+            for (int s = 0; s < r; s++) v -= L[r][s] * x[s];
+            x[r] = v;
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < kPB; r++)
+        if (r < nb) col[r] = x[r];
 }
 
-// B[k0:k0+nb, c] = U11^-1 B[k0:k0+nb, c] (non-unit upper).
+// B[k0:k0+nb, c] = U11^-1 B[k0:k0+nb, c] (non-unit upper) for c in [c0, c1).
 __global__ void k_trsm_upper(const double *A, int lda, int k0, int nb, double *B, int ldb, int c0, int c1)
 {
-    __shared__ double U[kNB][kNB + 1];
+    __shared__ double U[kPB][kPB + 1];
     for (int t = threadIdx.x; t < nb * nb; t += blockDim.x) {
         int r = t % nb, s = t / nb;
         U[r][s] = A[(size_t)(k0 + s) * lda + k0 + r];
@@ -129,14 +217,21 @@ __global__ void k_trsm_upper(const double *A, int lda, int k0, int nb, double *B
     __syncthreads();
     int c = c0 + blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= c1) return;
-    double x[kNB];
+    double x[kPB];
     double *col = B + (size_t)c * ldb + k0;
-    for (int r = nb - 1; r >= 0; r--) {
-        double v = col[r];
-        for (int s = r + 1; s < nb; s++) v -= U[r][s] * x[s];
-        x[r] = v / U[r][r];
+#pragma unroll
+    for (int r = kPB - 1; r >= 0; r--) {
+        if (r < nb) {
+            double v = col[r];
+#pragma unroll
+            for (int s = r + 1; s < kPB; s++)
+                if (s < nb) v -= U[r][s] * x[s];
+            x[r] = v / U[r][r];
+        }
     }
-    for (int r = 0; r < nb; r++) col[r] = x[r];
+#pragma unroll
+    for (int r = 0; r < kPB; r++)
+        if (r < nb) col[r] = x[r];
 }
 
 // C[m x nn] -= A[m x kk] * B[kk x nn], column-major, FP64.  64x64 tile per
@@ -180,11 +275,10 @@ __global__ void __launch_bounds__(256) k_dgemm_sub(int m, int nn, int kk, const 
         }
 }
 
-__global__ void k_perm_identity(double *B, int n, const int *perm)
+__global__ void k_identity(double *B, int n)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    B[(size_t)perm[i] * n + i] = 1.0;  // row i of P*I is e_{perm[i]}
+    if (i < n) B[(size_t)i * n + i] = 1.0;
 }
 
 __global__ void k_d2f(size_t n, const double *a, float *b)
@@ -201,52 +295,63 @@ static void dgemm_sub(cudaStream_t st, int m, int nn, int kk, const double *A, i
     k_dgemm_sub<<<grid, 256, 0, st>>>(m, nn, kk, A, lda, B, ldb, C, ldc); P2_COUNT_LAUNCH();
 }
 
-// Factor A (n x n, column-major, overwritten by L\U) and write its inverse
-// into Ainv (n x n).  Returns 0 or the first zero-pivot column + 1.
-int dense_lu_inverse(cudaStream_t st, double *A, int n, double *Ainv, int *d_ipiv, int *d_info)
+static bool smem_panel_ready = false;
+
+// Factor the banded A (n x n, column-major, lower/upper half-bandwidths kl,
+// ku) in place and write its inverse into Ainv.  Returns 0 or the first
+// zero-pivot column + 1.
+int band_lu_inverse(cudaStream_t st, double *A, int n, int kl, int ku, double *Ainv, int *d_ipiv, int *d_info)
 {
+    kl = std::max(0, std::min(kl, n - 1));
+    ku = std::max(0, std::min(ku, n - 1));
+    const bool smem = kPB + kl <= kMaxPanelRows;
+    if (smem && !smem_panel_ready) {
+        P2_CUDA_TRY(cudaFuncSetAttribute(k_panel_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxPanelBytes));
+        smem_panel_ready = true;
+    }
     P2_CUDA_TRY(cudaMemsetAsync(d_info, 0, sizeof(int), st));
-    for (int k0 = 0; k0 < n; k0 += kNB) {
-        int nb = std::min(kNB, n - k0);
-        k_lu_panel<<<1, 1024, 0, st>>>(A, n, k0, nb, d_ipiv, d_info); P2_COUNT_LAUNCH();
-        k_lu_swap<<<(n + 255) / 256, 256, 0, st>>>(A, n, k0, nb, d_ipiv); P2_COUNT_LAUNCH();
-        int rest = n - (k0 + nb);
-        if (rest > 0) {
-            k_trsm_lower<<<(rest + 127) / 128, 128, 0, st>>>(A, n, k0, nb, A, n, k0 + nb, n); P2_COUNT_LAUNCH();
-            dgemm_sub(st, rest, rest, nb, A + (size_t)k0 * n + k0 + nb, n, A + (size_t)(k0 + nb) * n + k0, n,
-                      A + (size_t)(k0 + nb) * n + k0 + nb, n);
+    for (int k0 = 0; k0 < n; k0 += kPB) {
+        const int nb = std::min(kPB, n - k0);
+        const int r1 = std::min(n, k0 + nb + kl);
+        const int c1 = std::min(n, r1 + ku);
+        if (smem) {
+            size_t bytes = sizeof(double) * (size_t)(r1 - k0) * nb;
+            k_panel_smem<<<1, kPanelThreads, bytes, st>>>(A, n, k0, nb, r1, d_ipiv, d_info); P2_COUNT_LAUNCH();
+        } else {
+            k_panel_global<<<1, 1024, 0, st>>>(A, n, k0, nb, r1, d_ipiv, d_info); P2_COUNT_LAUNCH();
+        }
+        const int cb = k0 + nb;
+        if (c1 > cb) {
+            k_swap_trsm_lower<<<(c1 - cb + 127) / 128, 128, 0, st>>>(A, n, k0, nb, d_ipiv, A, n, cb, c1); P2_COUNT_LAUNCH();
+            dgemm_sub(st, r1 - cb, c1 - cb, nb, A + (size_t)k0 * n + cb, n, A + (size_t)cb * n + k0, n,
+                      A + (size_t)cb * n + cb, n);
         }
     }
-    int info = 0;
-    std::vector<int> ipiv(n);
-    P2_CUDA_TRY(cudaMemcpyAsync(&info, d_info, sizeof(int), cudaMemcpyDeviceToHost, st));
-    P2_CUDA_TRY(cudaMemcpyAsync(ipiv.data(), d_ipiv, sizeof(int) * n, cudaMemcpyDeviceToHost, st));
-    P2_CUDA_TRY(cudaStreamSynchronize(st));
-    if (info) return info;
-    std::vector<int> perm(n);
-    for (int i = 0; i < n; i++) perm[i] = i;
-    for (int j = 0; j < n; j++) std::swap(perm[j], perm[ipiv[j]]);
-    // d_ipiv is reused to hold perm
-    P2_CUDA_TRY(cudaMemcpyAsync(d_ipiv, perm.data(), sizeof(int) * n, cudaMemcpyHostToDevice, st));
+    // forward: replay (P_k, L_k) on the identity; rows [k0, r1) of the partial
+    // product only have non-zeros in columns [0, r1)
     P2_CUDA_TRY(cudaMemsetAsync(Ainv, 0, sizeof(double) * (size_t)n * n, st));
-    k_perm_identity<<<(n + 255) / 256, 256, 0, st>>>(Ainv, n, d_ipiv); P2_COUNT_LAUNCH();
-    // forward: L Y = P I
-    for (int k0 = 0; k0 < n; k0 += kNB) {
-        int nb = std::min(kNB, n - k0);
-        k_trsm_lower<<<(n + 127) / 128, 128, 0, st>>>(A, n, k0, nb, Ainv, n, 0, n); P2_COUNT_LAUNCH();
-        int rest = n - (k0 + nb);
-        if (rest > 0)
-            dgemm_sub(st, rest, n, nb, A + (size_t)k0 * n + k0 + nb, n, Ainv + k0, n, Ainv + k0 + nb, n);
+    k_identity<<<(n + 255) / 256, 256, 0, st>>>(Ainv, n); P2_COUNT_LAUNCH();
+    for (int k0 = 0; k0 < n; k0 += kPB) {
+        const int nb = std::min(kPB, n - k0);
+        const int r1 = std::min(n, k0 + nb + kl);
+        k_swap_trsm_lower<<<(r1 + 127) / 128, 128, 0, st>>>(A, n, k0, nb, d_ipiv, Ainv, n, 0, r1); P2_COUNT_LAUNCH();
+        const int cb = k0 + nb;
+        if (r1 > cb) dgemm_sub(st, r1 - cb, r1, nb, A + (size_t)k0 * n + cb, n, Ainv + k0, n, Ainv + cb, n);
     }
-    // backward: U X = Y
-    int last = ((n - 1) / kNB) * kNB;
-    for (int k0 = last; k0 >= 0; k0 -= kNB) {
-        int nb = std::min(kNB, n - k0);
+    // backward: U X = Y with U's band (kl + ku above the diagonal)
+    const int kuu = std::min(n - 1, kl + ku);
+    const int last = ((n - 1) / kPB) * kPB;
+    for (int k0 = last; k0 >= 0; k0 -= kPB) {
+        const int nb = std::min(kPB, n - k0);
         k_trsm_upper<<<(n + 127) / 128, 128, 0, st>>>(A, n, k0, nb, Ainv, n, 0, n); P2_COUNT_LAUNCH();
-        if (k0 > 0) dgemm_sub(st, k0, n, nb, A + (size_t)k0 * n, n, Ainv + k0, n, Ainv, n);
+        const int a = std::max(0, k0 - kuu);
+        if (k0 > a) dgemm_sub(st, k0 - a, n, nb, A + (size_t)k0 * n + a, n, Ainv + k0, n, Ainv + a, n);
     }
     P2_CUDA_TRY(cudaGetLastError());
-    return 0;
+    int info = 0;
+    P2_CUDA_TRY(cudaMemcpyAsync(&info, d_info, sizeof(int), cudaMemcpyDeviceToHost, st));
+    P2_CUDA_TRY(cudaStreamSynchronize(st));
+    return info;
 }
 
 void d2f(cudaStream_t st, size_t n, const double *a, float *b)

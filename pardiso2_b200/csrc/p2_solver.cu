@@ -25,7 +25,8 @@
 
 namespace p2 {
 
-int dense_lu_inverse(cudaStream_t st, double *A, int n, double *Ainv, int *d_ipiv, int *d_info);
+constexpr int kProbes = 4 * 125;  // coarsest-operator probes: 125 colour classes x 4 components
+int band_lu_inverse(cudaStream_t st, double *A, int n, int kl, int ku, double *Ainv, int *d_ipiv, int *d_info);
 void d2f(cudaStream_t st, size_t n, const double *a, float *b);
 
 static inline unsigned nblk(long n, int t = kThreads) { return (unsigned)((n + t - 1) / t); }
@@ -499,7 +500,14 @@ void Solver::build_coarse_index()
     Ainv32 = (float *)arena.alloc(sizeof(float) * (size_t)nF * nF);
     d_ipiv = (int *)arena.alloc(sizeof(int) * nF);
     d_info = (int *)arena.alloc(sizeof(int) * 4);
-    probes = (double *)arena.alloc(sizeof(double) * (size_t)C.n * 4 * 125);
+    probes = (double *)arena.alloc(sizeof(double) * (size_t)C.n * 4 * kProbes);
+    d_bw = (int *)arena.alloc(sizeof(int) * 2);
+    if (!h_bw) {
+        int *p = nullptr;
+        P2_CUDA_TRY(cudaMallocHost(&p, sizeof(int) * 2));
+        h_bw_keep.reset(p, [](int *q) { cudaFreeHost(q); });
+        h_bw = p;
+    }
     cb64 = (double *)arena.alloc(sizeof(double) * nF);
     cx64 = (double *)arena.alloc(sizeof(double) * nF);
     cb32 = (float *)arena.alloc(sizeof(float) * nF);
@@ -511,13 +519,19 @@ void Solver::build_coarse_index()
 // components; a probe sets 1 on the free unknowns of its class and koef on the
 // boundary unknowns whose resolved target is in the class, so that every
 // non-zero of a row is attributed to the unique free column of that class
-// within two nodes.
-__global__ void k_probe_build(int nx, int ny, int nz, int cls, int comp, const int *colmap, const int *rt,
-                              const float *rk, double *X)
+// within two nodes.  All kProbes probes are built and applied in one launch
+// each (blockIdx.y = probe); the row kernel also records the band of the
+// operator in the free-unknown ordering (bw[0] = max row - col, bw[1] = max
+// col - row over the non-zeros).
+
+__global__ void k_probe_build(int nx, int ny, int nz, const int *colmap, const int *rt, const float *rk,
+                              double *probes)
 {
     int u = blockIdx.x * blockDim.x + threadIdx.x;
     int n = nx * ny * nz;
     if (u >= n) return;
+    const int cls = blockIdx.y % 125, comp = blockIdx.y / 125;
+    double *X = probes + (size_t)blockIdx.y * 4 * n;
     int j = u % ny, i = (u / ny) % nx, k = u / (nx * ny);
     int cx = cls % 5, cy = (cls / 5) % 5, cz = cls / 25;
     for (int c = 0; c < 4; c++) {
@@ -534,12 +548,14 @@ __global__ void k_probe_build(int nx, int ny, int nz, int cls, int comp, const i
     }
 }
 
-__global__ void k_probe_rows(LevelView<double> Lc, const double *X, int cls, int comp, const int *colmap, double *A,
-                             int nF)
+__global__ void k_probe_rows(LevelView<double> Lc, const double *probes, const int *colmap, double *A, int nF,
+                             int *bw)
 {
     int u = blockIdx.x * blockDim.x + threadIdx.x;
     if (u >= Lc.n) return;
     int n = Lc.n;
+    const int cls = blockIdx.y % 125, comp = blockIdx.y / 125;
+    const double *X = probes + (size_t)blockIdx.y * 4 * n;
     int j = u % Lc.ny, i = (u / Lc.ny) % Lc.nx, k = u / (Lc.nx * Lc.ny);
     Fields<double, double> x{X, X + n, X + 2 * n, X + 3 * n};
     int cx = cls % 5, cy = (cls / 5) % 5, cz = cls / 25;
@@ -560,6 +576,10 @@ __global__ void k_probe_rows(LevelView<double> Lc, const double *X, int cls, int
         else if (c == 2) a = row_vy(Lc, x, i, j, k, (double *)nullptr);
         else a = row_vz(Lc, x, i, j, k, (double *)nullptr);
         A[(size_t)col * nF + row] = a;
+        if (a != 0.0) {
+            if (row > col) atomicMax(&bw[0], row - col);
+            if (col > row) atomicMax(&bw[1], col - row);
+        }
     }
 }
 
@@ -606,14 +626,14 @@ void Solver::coarse_setup()
     int nl = (int)L.size();
     LevelView<double> Lc = view<double>(nl - 1, nl == 1);
     P2_CUDA_TRY(cudaMemsetAsync(A_c, 0, sizeof(double) * (size_t)nF * nF, st));
-    for (int comp = 0; comp < 4; comp++)
-        for (int cls = 0; cls < 125; cls++) {
-            double *X = probes + (size_t)cls * C.n * 4;
-            k_probe_build<<<nblk(C.n), kThreads, 0, st>>>(C.nx, C.ny, C.nz, cls, comp, d_colmap, d_crt, d_crk, X); P2_COUNT_LAUNCH();
-            k_probe_rows<<<nblk(C.n), kThreads, 0, st>>>(Lc, X, cls, comp, d_colmap, A_c, nF); P2_COUNT_LAUNCH();
-        }
+    P2_CUDA_TRY(cudaMemsetAsync(d_bw, 0, sizeof(int) * 2, st));
+    dim3 grid(nblk(C.n), kProbes);
+    k_probe_build<<<grid, kThreads, 0, st>>>(C.nx, C.ny, C.nz, d_colmap, d_crt, d_crk, probes); P2_COUNT_LAUNCH();
+    k_probe_rows<<<grid, kThreads, 0, st>>>(Lc, probes, d_colmap, A_c, nF, d_bw); P2_COUNT_LAUNCH();
     P2_CUDA_TRY(cudaGetLastError());
-    int info = dense_lu_inverse(st, A_c, nF, Ainv64, d_ipiv, d_info);
+    P2_CUDA_TRY(cudaMemcpyAsync(h_bw, d_bw, sizeof(int) * 2, cudaMemcpyDeviceToHost, st));
+    P2_CUDA_TRY(cudaStreamSynchronize(st));
+    int info = band_lu_inverse(st, A_c, nF, h_bw[0], h_bw[1], Ainv64, d_ipiv, d_info);
     if (info) throw Error(P2_ERR_SINGULAR, "zero pivot in the coarsest LU at column " + std::to_string(info));
     d2f(st, (size_t)nF * nF, Ainv64, Ainv32);
 }

@@ -149,6 +149,8 @@ class Solver {
     float *Ainv32 = nullptr;
     int *d_ipiv = nullptr, *d_info = nullptr;
     double *probes = nullptr;
+    int *d_bw = nullptr, *h_bw = nullptr;  // band of the coarsest operator (kl, ku)
+    std::shared_ptr<int> h_bw_keep;
     double *cb64 = nullptr, *cx64 = nullptr;
     float *cb32 = nullptr, *cx32 = nullptr;
 };
