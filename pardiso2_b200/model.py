@@ -426,7 +426,7 @@ def layered_model(n=257, multinum=6, markers=(2, 2, 2), seed=5, nlayers=45, name
     types must stay below 50: pardiso/mark3mg.c:692), an embedded dense slab
     block (density +1, viscosity 1e3) and a weak zone (viscosity 1e-2)."""
     zc = (np.arange(nlayers) + 0.5) / nlayers
-    eta_l = np.exp(-math.log(1e4) * zc)
+    eta_l = 1e4 * np.exp(-math.log(1e4) * zc)
     n0 = np.concatenate([eta_l, [1e3, 1e-2]])
     rocks = Rocks(n0, n0.copy(), np.concatenate([np.zeros(nlayers), [1.0, 0.0]]))
     params = SolverParams(nubeg=5e-3, nuend=2e4)
