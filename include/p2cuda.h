@@ -65,6 +65,8 @@ typedef struct {
     int restart;         /* GCR restart length (default 16, at most 18) */
     double omega;        /* cell-block smoother damping (default 0.7) */
     int use_graphs;      /* capture the V-cycle in a CUDA graph (default 1) */
+    int smoother;        /* cell-block smoother: 1 = exact 7x7 cell solve (default),
+                            0 = diagonal velocity block (cheaper, weak at stiff inclusions) */
 } p2_params;
 
 typedef struct {

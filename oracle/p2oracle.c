@@ -369,6 +369,125 @@ static void apply_bc_rows(p2o_ctx *C, int li)
 
 double p2o_vanka_omega = 0.7;
 
+/* Off-diagonal couplings between the 6 face velocities of cell (i,j,k) in
+ * their own momentum rows (faces: vx left/right, vy front/back, vz
+ * bottom/top).  Derived from the stencils above: through the normal stresses
+ * of the cell (sxxcalc..szzcalc, move3mgNew.c:3-387) and through the shear
+ * stresses on the edges the faces share (sxycalc..syzcalc, 388-795). */
+static void face_block(const p2o_level *l, int i, int j, int k, double M[6][6])
+{
+    const double Ec = l->ec[IDX(l, i, j, k)], hx = l->ihx[i], hy = l->ihy[j], hz = l->ihz[k];
+    double dn[3][6];
+    int a, b;
+#define EXY(a_, b_, c_) l->exy[IDX(l, a_, b_, c_)]
+#define EXZ(a_, b_, c_) l->exz[IDX(l, a_, b_, c_)]
+#define EYZ(a_, b_, c_) l->eyz[IDX(l, a_, b_, c_)]
+    for (a = 0; a < 6; a++)
+        for (b = 0; b < 6; b++) M[a][b] = 0.0;
+    /* d snn_d(cell) / d face */
+    dn[0][0] = -4.0 / 3 * hx; dn[0][1] = 4.0 / 3 * hx; dn[0][2] = 2.0 / 3 * hy; dn[0][3] = -2.0 / 3 * hy;
+    dn[0][4] = 2.0 / 3 * hz;  dn[0][5] = -2.0 / 3 * hz;
+    dn[1][0] = 2.0 / 3 * hx;  dn[1][1] = -2.0 / 3 * hx; dn[1][2] = -4.0 / 3 * hy; dn[1][3] = 4.0 / 3 * hy;
+    dn[1][4] = 2.0 / 3 * hz;  dn[1][5] = -2.0 / 3 * hz;
+    dn[2][0] = 2.0 / 3 * hx;  dn[2][1] = -2.0 / 3 * hx; dn[2][2] = 2.0 / 3 * hy; dn[2][3] = -2.0 / 3 * hy;
+    dn[2][4] = -4.0 / 3 * hz; dn[2][5] = 4.0 / 3 * hz;
+    for (b = 0; b < 6; b++) {
+        M[0][b] += Ec * dn[0][b] * l->ihxc[i - 1];
+        M[1][b] -= Ec * dn[0][b] * l->ihxc[i];
+        M[2][b] += Ec * dn[1][b] * l->ihyc[j - 1];
+        M[3][b] -= Ec * dn[1][b] * l->ihyc[j];
+        M[4][b] += Ec * dn[2][b] * l->ihzc[k - 1];
+        M[5][b] -= Ec * dn[2][b] * l->ihzc[k];
+    }
+    M[0][3] += 2 * EXY(i - 1, j, k - 1) * l->ihxe[i - 1] * l->ihyv[j - 1];
+    M[0][2] -= 2 * EXY(i - 1, j - 1, k - 1) * l->ihxe[i - 1] * l->ihyv[j - 1];
+    M[0][5] += 2 * EXZ(i - 1, j - 1, k) * l->ihxe[i - 1] * l->ihzv[k - 1];
+    M[0][4] -= 2 * EXZ(i - 1, j - 1, k - 1) * l->ihxe[i - 1] * l->ihzv[k - 1];
+    M[1][3] -= 2 * EXY(i, j, k - 1) * l->ihxe[i] * l->ihyv[j - 1];
+    M[1][2] += 2 * EXY(i, j - 1, k - 1) * l->ihxe[i] * l->ihyv[j - 1];
+    M[1][5] -= 2 * EXZ(i, j - 1, k) * l->ihxe[i] * l->ihzv[k - 1];
+    M[1][4] += 2 * EXZ(i, j - 1, k - 1) * l->ihxe[i] * l->ihzv[k - 1];
+    M[2][1] += 2 * EXY(i, j - 1, k - 1) * l->ihye[j - 1] * l->ihxv[i - 1];
+    M[2][0] -= 2 * EXY(i - 1, j - 1, k - 1) * l->ihye[j - 1] * l->ihxv[i - 1];
+    M[2][5] += 2 * EYZ(i - 1, j - 1, k) * l->ihye[j - 1] * l->ihzv[k - 1];
+    M[2][4] -= 2 * EYZ(i - 1, j - 1, k - 1) * l->ihye[j - 1] * l->ihzv[k - 1];
+    M[3][1] -= 2 * EXY(i, j, k - 1) * l->ihye[j] * l->ihxv[i - 1];
+    M[3][0] += 2 * EXY(i - 1, j, k - 1) * l->ihye[j] * l->ihxv[i - 1];
+    M[3][5] -= 2 * EYZ(i - 1, j, k) * l->ihye[j] * l->ihzv[k - 1];
+    M[3][4] += 2 * EYZ(i - 1, j, k - 1) * l->ihye[j] * l->ihzv[k - 1];
+    M[4][1] += 2 * EXZ(i, j - 1, k - 1) * l->ihze[k - 1] * l->ihxv[i - 1];
+    M[4][0] -= 2 * EXZ(i - 1, j - 1, k - 1) * l->ihze[k - 1] * l->ihxv[i - 1];
+    M[4][3] += 2 * EYZ(i - 1, j, k - 1) * l->ihze[k - 1] * l->ihyv[j - 1];
+    M[4][2] -= 2 * EYZ(i - 1, j - 1, k - 1) * l->ihze[k - 1] * l->ihyv[j - 1];
+    M[5][1] -= 2 * EXZ(i, j - 1, k) * l->ihze[k] * l->ihxv[i - 1];
+    M[5][0] += 2 * EXZ(i - 1, j - 1, k) * l->ihze[k] * l->ihxv[i - 1];
+    M[5][3] -= 2 * EYZ(i - 1, j, k) * l->ihze[k] * l->ihyv[j - 1];
+    M[5][2] += 2 * EYZ(i - 1, j - 1, k) * l->ihze[k] * l->ihyv[j - 1];
+#undef EXY
+#undef EXZ
+#undef EYZ
+}
+
+/* Solve the cell system [M g; cc^T 0] [dv; dp] = [r; rp] by its Schur
+ * complement, with M the 6x6 face block (diagonal d), inactive faces held
+ * (identity rows), and dp = 0 when the cell pressure is not updated.
+ * Gaussian elimination without pivoting: -M is diagonally dominant. */
+static void cell_solve(double M[6][6], const int act[6], const double g[6], const double cc[6], const double r[6],
+                       double rp, int pact, double dv[6], double *dp)
+{
+    double A[6][8];
+    int a, b, c;
+    for (a = 0; a < 6; a++) {
+        for (b = 0; b < 6; b++) A[a][b] = (act[a] && act[b]) ? M[a][b] : (a == b ? 1.0 : 0.0);
+        A[a][6] = act[a] ? r[a] : 0.0;
+        A[a][7] = act[a] ? g[a] : 0.0;
+    }
+    for (c = 0; c < 6; c++)
+        for (a = c + 1; a < 6; a++) {
+            double f = A[a][c] / A[c][c];
+            if (f == 0.0) continue;
+            for (b = c; b < 8; b++) A[a][b] -= f * A[c][b];
+        }
+    for (c = 5; c >= 0; c--) {
+        for (b = c + 1; b < 6; b++) {
+            A[c][6] -= A[c][b] * A[b][6];
+            A[c][7] -= A[c][b] * A[b][7];
+        }
+        A[c][6] /= A[c][c];
+        A[c][7] /= A[c][c];
+    }
+    *dp = 0.0;
+    if (pact) {
+        double num = -rp, den = 0.0;
+        for (a = 0; a < 6; a++) {
+            num += cc[a] * A[a][6];
+            den += cc[a] * A[a][7];
+        }
+        if (den != 0.0) *dp = num / den;
+    }
+    for (a = 0; a < 6; a++) dv[a] = act[a] ? A[a][6] - *dp * A[a][7] : 0.0;
+}
+
+int p2o_smoother = 2; /* 0: lexicographic GS + Uzawa (reference scheme), 1: diagonal cell-block Vanka,
+                         2: full cell-block Vanka (the default), 3: full where smooth_cell, else diagonal */
+double p2o_hybrid_ratio = 10.0;
+
+/* Cell whose viscosity is within p2o_hybrid_ratio of its six neighbour cells. */
+static int smooth_cell(const p2o_level *l, int i, int j, int k)
+{
+    const double e = l->ec[IDX(l, i, j, k)];
+    const int nb[6][3] = {{-1, 0, 0}, {1, 0, 0}, {0, -1, 0}, {0, 1, 0}, {0, 0, -1}, {0, 0, 1}};
+    int q;
+    for (q = 0; q < 6; q++) {
+        int a = i + nb[q][0], b = j + nb[q][1], c = k + nb[q][2];
+        double o;
+        if (a < 1 || b < 1 || c < 1 || a > l->nx - 1 || b > l->ny - 1 || c > l->nz - 1) continue;
+        o = l->ec[IDX(l, a, b, c)];
+        if (o > e * p2o_hybrid_ratio || e > o * p2o_hybrid_ratio) return 0;
+    }
+    return 1;
+}
+
 static void smooth_vanka(p2o_ctx *C, int li, int sweeps)
 {
     p2o_level *l = &C->L[li];
@@ -401,6 +520,23 @@ static void smooth_vanka(p2o_ctx *C, int li, int sweeps)
                             r[q] = l->b[vc[q]][vn[q]] - row_any(l, vc[q], vi[q], vj[q], vk[q], &d[q]);
                             if (!pbc) { num += cc[q] * r[q] / d[q]; den += cc[q] * g[q] / d[q]; }
                         }
+                        if (p2o_smoother == 3 && !smooth_cell(l, i, j, k)) {
+                            /* interface cell: fall through to the diagonal block */
+                        } else if (p2o_smoother >= 2) {
+                            double M[6][6], dv[6];
+                            int act[6];
+                            face_block(l, i, j, k, M);
+                            for (q = 0; q < 6; q++) {
+                                act[q] = d[q] != 0.0;
+                                M[q][q] = d[q];
+                            }
+                            rp = pbc ? 0.0 : l->b[0][u] - row_p(l, i, j, k);
+                            cell_solve(M, act, g, cc, r, rp, !pbc, dv, &dp);
+                            if (!pbc) dx[0][u] = dp;
+                            for (q = 0; q < 6; q++)
+                                if (act[q]) dx[vc[q]][vn[q]] = dv[q];
+                            continue;
+                        }
                         if (!pbc && den != 0.0) {
                             rp = l->b[0][u] - row_p(l, i, j, k);
                             dp = (num - rp) / den;
@@ -419,7 +555,6 @@ static void smooth_vanka(p2o_ctx *C, int li, int sweeps)
     for (c = 0; c < 4; c++) free(dx[c]);
 }
 
-int p2o_smoother = 1; /* 0: lexicographic GS + Uzawa (reference scheme), 1: coloured Vanka */
 
 /* ---------------------------------------------------------------------- */
 /* Transfer weights along one axis (vprestrict/vpprolong index rules).     */
@@ -595,10 +730,144 @@ static void prolong_level(p2o_ctx *C, int lc)
             }
 }
 
+/* Coarse-level viscosity scheme (a preconditioner choice; the level-0
+ * problem does not depend on it):
+ *   -1     the model's viscmod (the reference's ronurestrict,
+ *          move3mgNew.c:3386-3527, then 8-/2-node stencil means 45-47, 442-444);
+ *   0/1/2  the same chain with linear / log / inverse means;
+ *   3/4/5  stencil-consistent: each coarse stencil viscosity is the log /
+ *          linear / inverse mean of the finer level's viscosity of the same
+ *          kind (cells for ec; z-, y-, x-edges for exy, exz, eyz) over the
+ *          coarse position's control volume, weighted by overlap. */
+int p2o_coarse_avg = -1;
+
+static int coarse_mode(const p2o_ctx *C)
+{
+    return p2o_coarse_avg >= 0 && p2o_coarse_avg <= 2 ? p2o_coarse_avg : C->viscmod;
+}
+
+/* kind 0: cell m = [g[m-1], g[m]]; 1: segment [g[m], g[m+1]]; 2: dual of node m */
+static void span(const double *g, int n, int kind, int m, double *a, double *b)
+{
+    if (kind == 0) { *a = g[m - 1]; *b = g[m]; return; }
+    if (kind == 1) { *a = g[m]; *b = g[m + 1]; return; }
+    *a = m > 0 ? 0.5 * (g[m - 1] + g[m]) : g[0];
+    *b = m < n - 1 ? 0.5 * (g[m] + g[m + 1]) : g[n - 1];
+}
+
+static double overlap(double a0, double b0, double a1, double b1)
+{
+    double lo = a0 > a1 ? a0 : a1, hi = b0 < b1 ? b0 : b1;
+    return hi > lo ? hi - lo : 0.0;
+}
+
+static void consistent_viscosity(p2o_ctx *C, int li)
+{
+    p2o_level *l = &C->L[li], *f = &C->L[li - 1];
+    const int mode = p2o_coarse_avg;
+    /* position kind per field and axis (x, y, z) */
+    static const int kinds[4][3] = {{0, 0, 0}, {2, 2, 1}, {2, 1, 2}, {1, 2, 2}};
+    double *dst[4];
+    const double *src[4];
+    int nc[3], nf[3], q, k;
+    const double *gc[3], *gf[3];
+    dst[0] = l->ec; dst[1] = l->exy; dst[2] = l->exz; dst[3] = l->eyz;
+    src[0] = f->ec; src[1] = f->exy; src[2] = f->exz; src[3] = f->eyz;
+    nc[0] = l->nx; nc[1] = l->ny; nc[2] = l->nz;
+    nf[0] = f->nx; nf[1] = f->ny; nf[2] = f->nz;
+    gc[0] = l->gx; gc[1] = l->gy; gc[2] = l->gz;
+    gf[0] = f->gx; gf[1] = f->gy; gf[2] = f->gz;
+    for (q = 0; q < 4; q++)
+#pragma omp parallel for schedule(static)
+        for (k = 0; k < l->nz; k++) {
+            int i, j;
+            for (i = 0; i < l->nx; i++)
+                for (j = 0; j < l->ny; j++) {
+                    int I[3], ax, ok = 1, lo[3], hi[3], a, b2, d;
+                    double A[3], B[3], s = 0.0, ws = 0.0, m;
+                    long u = IDX(l, i, j, k);
+                    I[0] = i; I[1] = j; I[2] = k;
+                    for (ax = 0; ax < 3; ax++) {
+                        int kd = kinds[q][ax];
+                        if ((kd == 0 && I[ax] < 1) || (kd == 1 && I[ax] > nc[ax] - 2)) ok = 0;
+                    }
+                    if (!ok) continue;  /* keeps the value of the node-viscosity chain */
+                    for (ax = 0; ax < 3; ax++) {
+                        int c0 = 2 * I[ax] - 2;
+                        span(gc[ax], nc[ax], kinds[q][ax], I[ax], &A[ax], &B[ax]);
+                        lo[ax] = c0 - 4 < 0 ? 0 : c0 - 4;
+                        hi[ax] = c0 + 4 > nf[ax] - 1 ? nf[ax] - 1 : c0 + 4;
+                    }
+                    if (mode == 6 && q > 0) {
+                        /* shear viscosity: harmonic (in series) over the two gradient
+                         * directions, arithmetic (in parallel) along the edge */
+                        const int par = q == 1 ? 2 : (q == 2 ? 1 : 0);
+                        int t;
+                        for (t = lo[par]; t <= hi[par]; t++) {
+                            double wp, fa, fb, sh = 0.0, wh = 0.0;
+                            int kd = kinds[q][par];
+                            if ((kd == 0 && t < 1) || (kd == 1 && t > nf[par] - 2)) continue;
+                            span(gf[par], nf[par], kd, t, &fa, &fb);
+                            wp = overlap(A[par], B[par], fa, fb);
+                            if (wp <= 0.0) continue;
+                            for (d = lo[2]; d <= hi[2]; d++)
+                                for (a = lo[0]; a <= hi[0]; a++)
+                                    for (b2 = lo[1]; b2 <= hi[1]; b2++) {
+                                        int J[3];
+                                        double w = 1.0;
+                                        J[0] = a; J[1] = b2; J[2] = d;
+                                        if (J[par] != t) continue;
+                                        for (ax = 0; ax < 3; ax++) {
+                                            int kk2 = kinds[q][ax];
+                                            if (ax == par) continue;
+                                            if ((kk2 == 0 && J[ax] < 1) || (kk2 == 1 && J[ax] > nf[ax] - 2)) { w = 0.0; break; }
+                                            span(gf[ax], nf[ax], kk2, J[ax], &fa, &fb);
+                                            w *= overlap(A[ax], B[ax], fa, fb);
+                                            if (w <= 0.0) break;
+                                        }
+                                        if (w <= 0.0) continue;
+                                        sh += w / src[q][IDX(f, a, b2, d)];
+                                        wh += w;
+                                    }
+                            if (wh <= 0.0) continue;
+                            s += wp * (wh / sh);
+                            ws += wp;
+                        }
+                        if (ws <= 0.0) continue;
+                        dst[q][u] = clampd(C, s / ws);
+                        continue;
+                    }
+                    for (d = lo[2]; d <= hi[2]; d++)
+                        for (a = lo[0]; a <= hi[0]; a++)
+                            for (b2 = lo[1]; b2 <= hi[1]; b2++) {
+                                int J[3];
+                                double w = 1.0, fa, fb, v;
+                                J[0] = a; J[1] = b2; J[2] = d;
+                                for (ax = 0; ax < 3; ax++) {
+                                    int kd = kinds[q][ax];
+                                    if ((kd == 0 && J[ax] < 1) || (kd == 1 && J[ax] > nf[ax] - 2)) { w = 0.0; break; }
+                                    span(gf[ax], nf[ax], kd, J[ax], &fa, &fb);
+                                    w *= overlap(A[ax], B[ax], fa, fb);
+                                    if (w <= 0.0) break;
+                                }
+                                if (w <= 0.0) continue;
+                                v = src[q][IDX(f, a, b2, d)];
+                                s += w * ((mode == 3 || mode == 6) ? log(v) : mode == 4 ? v : 1.0 / v);
+                                ws += w;
+                            }
+                    if (ws <= 0.0) continue;
+                    m = s / ws;
+                    m = (mode == 3 || mode == 6) ? exp(m) : mode == 4 ? m : 1.0 / m;
+                    dst[q][u] = clampd(C, m);
+                }
+        }
+}
+
 /* nu, ro of level lc from level lc-1 (ronurestrict). */
 static void ronurestrict_level(p2o_ctx *C, int lc)
 {
     p2o_level *f = &C->L[lc - 1], *cl = &C->L[lc];
+    const int vm = coarse_mode(C);
     double *sn = calloc(cl->n, sizeof(double)), *sr = calloc(cl->n, sizeof(double)), *sw = calloc(cl->n, sizeof(double));
     int i, j, k, a, b2, d;
     long v;
@@ -625,8 +894,8 @@ static void ronurestrict_level(p2o_ctx *C, int lc)
                             double wy = 1.0 - fabs((gc[1][lo[1] + b2] - gf[1][j]) / (gc[1][lo[1] + 1] - gc[1][lo[1]]));
                             double w = wx * wy * wz, fv;
                             long t = IDX(cl, lo[0] + a, lo[1] + b2, lo[2] + d);
-                            if (C->viscmod == 0) fv = f->nu[u];
-                            else if (C->viscmod == 1) fv = log(f->nu[u]);
+                            if (vm == 0) fv = f->nu[u];
+                            else if (vm == 1) fv = log(f->nu[u]);
                             else fv = 1.0 / f->nu[u];
                             sn[t] += fv * w;
                             sr[t] += f->ro[u] * w;
@@ -635,8 +904,8 @@ static void ronurestrict_level(p2o_ctx *C, int lc)
             }
     for (v = 0; v < cl->n; v++) {
         double nv = sn[v] / sw[v];
-        if (C->viscmod == 1) nv = exp(nv);
-        if (C->viscmod == 2) nv = 1.0 / nv;
+        if (vm == 1) nv = exp(nv);
+        if (vm == 2) nv = 1.0 / nv;
         cl->nu[v] = (float)nv;
         cl->ro[v] = (float)(sr[v] / sw[v]);
     }
@@ -665,7 +934,7 @@ static void level_viscosity(p2o_ctx *C, int li, const float *nxx, const float *n
                     v[2] = l->nu[IDX(l, i, j - 1, k - 1)];     v[3] = l->nu[IDX(l, i, j, k - 1)];
                     v[4] = l->nu[IDX(l, i - 1, j - 1, k)];     v[5] = l->nu[IDX(l, i - 1, j, k)];
                     v[6] = l->nu[IDX(l, i, j - 1, k)];         v[7] = l->nu[IDX(l, i, j, k)];
-                    l->ec[u] = clampd(C, vavg(C->viscmod, v, 8));
+                    l->ec[u] = clampd(C, vavg(coarse_mode(C), v, 8));
                 } else {
                     l->ec[u] = C->nubeg;
                 }
@@ -673,11 +942,11 @@ static void level_viscosity(p2o_ctx *C, int li, const float *nxx, const float *n
                     double v[2];
                     v[0] = l->nu[u];
                     v[1] = k + 1 < l->nz ? l->nu[IDX(l, i, j, k + 1)] : l->nu[u];
-                    l->exy[u] = clampd(C, vavg(C->viscmod, v, 2));
+                    l->exy[u] = clampd(C, vavg(coarse_mode(C), v, 2));
                     v[1] = j + 1 < l->ny ? l->nu[IDX(l, i, j + 1, k)] : l->nu[u];
-                    l->exz[u] = clampd(C, vavg(C->viscmod, v, 2));
+                    l->exz[u] = clampd(C, vavg(coarse_mode(C), v, 2));
                     v[1] = i + 1 < l->nx ? l->nu[IDX(l, i + 1, j, k)] : l->nu[u];
-                    l->eyz[u] = clampd(C, vavg(C->viscmod, v, 2));
+                    l->eyz[u] = clampd(C, vavg(coarse_mode(C), v, 2));
                 }
             }
 }
@@ -906,7 +1175,10 @@ int p2o_set_fields(void *h, const float *nu, const float *ro, const float *nxx, 
     memcpy(l->ro, ro, sizeof(float) * l->n);
     for (li = 1; li < C->nlev; li++) ronurestrict_level(C, li);
     level_viscosity(C, 0, nxx, nxy, nxz, nyz);
-    for (li = 1; li < C->nlev; li++) level_viscosity(C, li, NULL, NULL, NULL, NULL);
+    for (li = 1; li < C->nlev; li++) {
+        level_viscosity(C, li, NULL, NULL, NULL, NULL);
+        if (p2o_coarse_avg >= 3) consistent_viscosity(C, li);
+    }
     /* level-0 right-hand sides (xstokserr:845, ystokserr:1060, zstokserr:1279) */
     for (k = 0; k < l->nz; k++)
         for (i = 0; i < l->nx; i++)

@@ -30,7 +30,7 @@ class Params(C.Structure):
                 ("pxinit", C.c_int), ("pyinit", C.c_int), ("pzinit", C.c_int), ("viscmod", C.c_int),
                 ("multinum", C.c_int), ("npre", C.c_int * P2_MAX_LEVELS), ("npost", C.c_int * P2_MAX_LEVELS),
                 ("tol", C.c_double), ("max_iter", C.c_int), ("precision", C.c_int), ("restart", C.c_int),
-                ("omega", C.c_double), ("use_graphs", C.c_int)]
+                ("omega", C.c_double), ("use_graphs", C.c_int), ("smoother", C.c_int)]
 
 
 class SolveInfo(C.Structure):

@@ -61,6 +61,7 @@ void p2_default_params(p2_params *p)
     p->restart = 16;
     p->omega = 0.7;
     p->use_graphs = 1;
+    p->smoother = 1;
 }
 
 p2_status p2_create(p2_ctx **out, int device)

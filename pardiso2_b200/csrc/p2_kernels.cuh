@@ -124,6 +124,169 @@ __global__ void k_vanka(LevelView<T> L, T *P, Vec4<T> vin, Vec4<T> vout, Vec4<T>
 }
 
 // ---------------------------------------------------------------------------
+// Full cell-block variant: the cell's 6 face velocities and its pressure are
+// solved together with the exact 7x7 cell system
+//   [M g; cc^T 0] [dv; dp] = [r; rp],
+// M the face-face block of the momentum rows.  Its off-diagonal entries come
+// from the cell's normal stresses (every face enters e_xx, e_yy, e_zz and the
+// divergence) and from the shear stresses on the edges two faces share; they
+// are the coefficients of the row functions above (checked entry by entry
+// against the assembled operator).  Faces under a boundary row are held; the
+// pressure is held where the cell pressure is a boundary unknown.  M is
+// eliminated without pivoting (-M is diagonally dominant).  Read/write
+// pattern and buffering as k_vanka.
+template <typename T>
+__device__ __forceinline__ void face_block(const LevelView<T> &L, int i, int j, int k, T M[6][6])
+{
+    const T Ec = eta_at(L, L.ec, P2IDX(L, i, j, k));
+    const T hx = L.ax.ih[i], hy = L.ay.ih[j], hz = L.az.ih[k];
+    const T t43 = (T)(4.0 / 3.0), t23 = (T)(2.0 / 3.0);
+    // d snn_d(cell) / d face, times Ec
+    const T dn[3][6] = {{-t43 * hx, t43 * hx, t23 * hy, -t23 * hy, t23 * hz, -t23 * hz},
+                        {t23 * hx, -t23 * hx, -t43 * hy, t43 * hy, t23 * hz, -t23 * hz},
+                        {t23 * hx, -t23 * hx, t23 * hy, -t23 * hy, -t43 * hz, t43 * hz}};
+    const T s0 = Ec * L.ax.ihc[i - 1], s1 = -Ec * L.ax.ihc[i], s2 = Ec * L.ay.ihc[j - 1], s3 = -Ec * L.ay.ihc[j],
+            s4 = Ec * L.az.ihc[k - 1], s5 = -Ec * L.az.ihc[k];
+#pragma unroll
+    for (int b = 0; b < 6; b++) {
+        M[0][b] = s0 * dn[0][b];
+        M[1][b] = s1 * dn[0][b];
+        M[2][b] = s2 * dn[1][b];
+        M[3][b] = s3 * dn[1][b];
+        M[4][b] = s4 * dn[2][b];
+        M[5][b] = s5 * dn[2][b];
+    }
+    const T two = (T)2.0;
+    const T exy00 = eta_at(L, L.exy, P2IDX(L, i - 1, j - 1, k - 1)), exy01 = eta_at(L, L.exy, P2IDX(L, i - 1, j, k - 1));
+    const T exy10 = eta_at(L, L.exy, P2IDX(L, i, j - 1, k - 1)), exy11 = eta_at(L, L.exy, P2IDX(L, i, j, k - 1));
+    const T exz00 = eta_at(L, L.exz, P2IDX(L, i - 1, j - 1, k - 1)), exz01 = eta_at(L, L.exz, P2IDX(L, i - 1, j - 1, k));
+    const T exz10 = eta_at(L, L.exz, P2IDX(L, i, j - 1, k - 1)), exz11 = eta_at(L, L.exz, P2IDX(L, i, j - 1, k));
+    const T eyz00 = eta_at(L, L.eyz, P2IDX(L, i - 1, j - 1, k - 1)), eyz01 = eta_at(L, L.eyz, P2IDX(L, i - 1, j - 1, k));
+    const T eyz10 = eta_at(L, L.eyz, P2IDX(L, i - 1, j, k - 1)), eyz11 = eta_at(L, L.eyz, P2IDX(L, i - 1, j, k));
+    const T hex0 = L.ax.ihe[i - 1], hex1 = L.ax.ihe[i], hey0 = L.ay.ihe[j - 1], hey1 = L.ay.ihe[j];
+    const T hez0 = L.az.ihe[k - 1], hez1 = L.az.ihe[k];
+    const T hvx = L.ax.ihv[i - 1], hvy = L.ay.ihv[j - 1], hvz = L.az.ihv[k - 1];
+    // vx faces: shear with the vy (front/back) and vz (bottom/top) faces
+    M[0][3] += two * exy01 * hex0 * hvy;  M[0][2] -= two * exy00 * hex0 * hvy;
+    M[0][5] += two * exz01 * hex0 * hvz;  M[0][4] -= two * exz00 * hex0 * hvz;
+    M[1][3] -= two * exy11 * hex1 * hvy;  M[1][2] += two * exy10 * hex1 * hvy;
+    M[1][5] -= two * exz11 * hex1 * hvz;  M[1][4] += two * exz10 * hex1 * hvz;
+    // vy faces
+    M[2][1] += two * exy10 * hey0 * hvx;  M[2][0] -= two * exy00 * hey0 * hvx;
+    M[2][5] += two * eyz01 * hey0 * hvz;  M[2][4] -= two * eyz00 * hey0 * hvz;
+    M[3][1] -= two * exy11 * hey1 * hvx;  M[3][0] += two * exy01 * hey1 * hvx;
+    M[3][5] -= two * eyz11 * hey1 * hvz;  M[3][4] += two * eyz10 * hey1 * hvz;
+    // vz faces
+    M[4][1] += two * exz10 * hez0 * hvx;  M[4][0] -= two * exz00 * hez0 * hvx;
+    M[4][3] += two * eyz10 * hez0 * hvy;  M[4][2] -= two * eyz00 * hez0 * hvy;
+    M[5][1] -= two * exz11 * hez1 * hvx;  M[5][0] += two * exz01 * hez1 * hvx;
+    M[5][3] -= two * eyz11 * hez1 * hvy;  M[5][2] += two * eyz01 * hez1 * hvy;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(128) k_vanka_full(LevelView<T> L, T *P, Vec4<T> vin, Vec4<T> vout, Vec4<T> b,
+                                                    T omega, int col)
+{
+    int half = (L.ny) / 2;
+    long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    long lines = (long)(L.nx - 1) * (L.nz - 1);
+    if (t >= lines * half) return;
+    int jj = (int)(t % half);
+    long line = t / half;
+    int i = 1 + (int)(line % (L.nx - 1)), k = 1 + (int)(line / (L.nx - 1));
+    int j0 = (((1 + i + k) & 1) == col) ? 1 : 2;
+    int j = j0 + 2 * jj;
+    if (j > L.ny - 1) return;
+    Fields<T, T> x{P, vin.c[1], vin.c[2], vin.c[3]};
+    int u = P2IDX(L, i, j, k);
+    const bool pact = (L.bcm[u] & BC_P) == 0;
+    int fi[6];
+    const int fc[6] = {1, 1, 2, 2, 3, 3};
+    T g[6], cc[6], r[6];
+    bool act[6];
+    fi[0] = P2IDX(L, i - 1, j - 1, k - 1); g[0] = -L.ax.ihc[i - 1]; cc[0] = -L.ax.ih[i];
+    fi[1] = P2IDX(L, i, j - 1, k - 1);     g[1] = L.ax.ihc[i];      cc[1] = L.ax.ih[i];
+    fi[2] = P2IDX(L, i - 1, j - 1, k - 1); g[2] = -L.ay.ihc[j - 1]; cc[2] = -L.ay.ih[j];
+    fi[3] = P2IDX(L, i - 1, j, k - 1);     g[3] = L.ay.ihc[j];      cc[3] = L.ay.ih[j];
+    fi[4] = P2IDX(L, i - 1, j - 1, k - 1); g[4] = -L.az.ihc[k - 1]; cc[4] = -L.az.ih[k];
+    fi[5] = P2IDX(L, i - 1, j - 1, k);     g[5] = L.az.ihc[k];      cc[5] = L.az.ih[k];
+    const int ofs[6][3] = {{-1, -1, -1}, {0, -1, -1}, {-1, -1, -1}, {-1, 0, -1}, {-1, -1, -1}, {-1, -1, 0}};
+    T M[6][6];
+    face_block(L, i, j, k, M);
+#pragma unroll
+    for (int q = 0; q < 6; q++) {
+        int a = i + ofs[q][0], bb = j + ofs[q][1], c = k + ofs[q][2];
+        T d = 0;
+        act[q] = !(L.bcm[fi[q]] & (1 << fc[q]));
+        r[q] = 0;
+        if (act[q]) {
+            T ax;
+            if (fc[q] == 1) ax = row_vx(L, x, a, bb, c, &d);
+            else if (fc[q] == 2) ax = row_vy(L, x, a, bb, c, &d);
+            else ax = row_vz(L, x, a, bb, c, &d);
+            r[q] = b.c[fc[q]][fi[q]] - ax;
+        }
+        M[q][q] = d;
+    }
+    // masked system: held faces become identity rows / zero columns
+    T y1[6], y2[6];
+#pragma unroll
+    for (int a = 0; a < 6; a++) {
+#pragma unroll
+        for (int c = 0; c < 6; c++)
+            if (!(act[a] && act[c])) M[a][c] = a == c ? (T)1 : (T)0;
+        y1[a] = act[a] ? r[a] : (T)0;
+        y2[a] = act[a] ? g[a] : (T)0;
+    }
+    // constant trip counts so that M, y1, y2 stay in registers
+#pragma unroll
+    for (int c = 0; c < 6; c++) {
+        const T ip = (T)1 / M[c][c];
+#pragma unroll
+        for (int a = 0; a < 6; a++) {
+            if (a > c) {
+                const T f = M[a][c] * ip;
+#pragma unroll
+                for (int e = 0; e < 6; e++)
+                    if (e > c) M[a][e] -= f * M[c][e];
+                y1[a] -= f * y1[c];
+                y2[a] -= f * y2[c];
+            }
+        }
+    }
+#pragma unroll
+    for (int cc5 = 0; cc5 < 6; cc5++) {
+        const int c = 5 - cc5;
+#pragma unroll
+        for (int e = 0; e < 6; e++) {
+            if (e > c) {
+                y1[c] -= M[c][e] * y1[e];
+                y2[c] -= M[c][e] * y2[e];
+            }
+        }
+        const T ip = (T)1 / M[c][c];
+        y1[c] *= ip;
+        y2[c] *= ip;
+    }
+    T dp = 0;
+    if (pact) {
+        T num = -(b.c[0][u] - row_p(L, x, i, j, k)), den = 0;
+#pragma unroll
+        for (int q = 0; q < 6; q++) {
+            num += cc[q] * y1[q];
+            den += cc[q] * y2[q];
+        }
+        if (den != (T)0) {
+            dp = num / den;
+            P[u] += omega * dp;
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < 6; q++)
+        if (act[q]) vout.c[fc[q]][fi[q]] = vin.c[fc[q]][fi[q]] + omega * (y1[q] - dp * y2[q]);
+}
+
+// ---------------------------------------------------------------------------
 // Transfers.  Per-axis tables (host-built from the reference's index rules,
 // move3mgNew.c:3562-3575 and the corresponding blocks of vprestrict and
 // vpprolong): for a fine index m, the coarse interval lo[m] and the weights

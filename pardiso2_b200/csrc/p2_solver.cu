@@ -697,11 +697,17 @@ void Solver::smooth(int l, int sweeps)
     // pressure is updated in place in x.c[0] (yy shares it)
     Vec4<T> yy = y;
     yy.c[0] = x.c[0];
+    const bool full = prm.smoother != 0;
     for (int s = 0; s < sweeps; s++) {
-        k_vanka<T><<<nblk(cells), kThreads, 0, st>>>(V, x.c[0], x, yy, b, om, 0); P2_COUNT_LAUNCH();
-        bc_set<T>(l, yy, b);
-        k_vanka<T><<<nblk(cells), kThreads, 0, st>>>(V, x.c[0], yy, x, b, om, 1); P2_COUNT_LAUNCH();
-        bc_set<T>(l, x, b);
+        for (int col = 0; col < 2; col++) {
+            Vec4<T> &vin = col ? yy : x, &vout = col ? x : yy;
+            if (full) {
+                k_vanka_full<T><<<nblk(cells, 128), 128, 0, st>>>(V, x.c[0], vin, vout, b, om, col); P2_COUNT_LAUNCH();
+            } else {
+                k_vanka<T><<<nblk(cells), kThreads, 0, st>>>(V, x.c[0], vin, vout, b, om, col); P2_COUNT_LAUNCH();
+            }
+            bc_set<T>(l, vout, b);
+        }
     }
 }
 
@@ -1090,16 +1096,24 @@ double Solver::debug_time_smoother(int l, int passes)
         Vec4<float> x = Lv.x32, y = Lv.y32;
         y.c[0] = x.c[0];
         for (int p = 0; p < passes; p++) {
-            k_vanka<float><<<nblk(cells), kThreads, 0, st>>>(V, x.c[0], (p & 1) ? y : x, (p & 1) ? x : y, Lv.b32,
-                                                             (float)prm.omega, p & 1);
+            if (prm.smoother)
+                k_vanka_full<float><<<nblk(cells, 128), 128, 0, st>>>(V, x.c[0], (p & 1) ? y : x, (p & 1) ? x : y,
+                                                                      Lv.b32, (float)prm.omega, p & 1);
+            else
+                k_vanka<float><<<nblk(cells), kThreads, 0, st>>>(V, x.c[0], (p & 1) ? y : x, (p & 1) ? x : y,
+                                                                 Lv.b32, (float)prm.omega, p & 1);
         }
     } else {
         LevelView<double> V = view<double>(l, false);
         Vec4<double> x = Lv.x64, y = Lv.y64;
         y.c[0] = x.c[0];
         for (int p = 0; p < passes; p++) {
-            k_vanka<double><<<nblk(cells), kThreads, 0, st>>>(V, x.c[0], (p & 1) ? y : x, (p & 1) ? x : y, Lv.b64,
-                                                              prm.omega, p & 1);
+            if (prm.smoother)
+                k_vanka_full<double><<<nblk(cells, 128), 128, 0, st>>>(V, x.c[0], (p & 1) ? y : x, (p & 1) ? x : y,
+                                                                       Lv.b64, prm.omega, p & 1);
+            else
+                k_vanka<double><<<nblk(cells), kThreads, 0, st>>>(V, x.c[0], (p & 1) ? y : x, (p & 1) ? x : y,
+                                                                  Lv.b64, prm.omega, p & 1);
         }
     }
     P2_CUDA_TRY(cudaEventRecord(ev[6], st));

