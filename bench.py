@@ -31,9 +31,17 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "ms per Stokes solve to rel.residual 1e-8 (mixed vs FP64, 1 B200); HBM GB/s"
-WORKLOAD = ("spheres65: 65^3 nodes, 4 levels, 8 spheres viscosity 1e-3..1e3 (contrast 1e6), "
-            "2x2x2 markers/cell, free-slip box, seed 2")
+WORKLOADS = {
+    1: "sphere33: 33^3 nodes, 3 levels, centred sphere viscosity 1e3 radius 0.2, 4x4x4 markers/cell, seed 1",
+    2: ("spheres65: 65^3 nodes, 4 levels, 8 spheres viscosity 1e-3..1e3 (contrast 1e6), "
+        "2x2x2 markers/cell, free-slip box, seed 2"),
+    3: ("spheres129: 129^3 nodes, 5 levels, 20 spheres viscosity 1e-2..1e4 (contrast 1e6), "
+        "2x2x2 markers/cell, free-slip box, seed 3"),
+    5: ("layered257: 257^3 nodes, 6 levels, 45 layers viscosity 1e4..1 with depth, slab 1e3 (density +1), "
+        "weak zone 1e-2, 2x2x2 markers/cell, free-slip box, seed 5"),
+}
 CONFIG_IDX = 2
+WORKLOAD = WORKLOADS[CONFIG_IDX]
 # Algorithmic bytes of one FP32 colour pass of the cell-block smoother per
 # node: read 3 velocity fields (12 B), pressure (4 B), 4 right-hand sides
 # (16 B) and 4 viscosity fields (16 B); write 3 velocity fields (12 B) and
@@ -52,6 +60,8 @@ def parse():
     ap.add_argument("--solve-only", action="store_true",
                     help="warm-up + timed resident solves + smoother timing only (profiling runs)")
     ap.add_argument("--restart", type=int, default=16, help="GCR restart length")
+    ap.add_argument("--tune-iters", type=int, default=12,
+                    help="outer iterations per autotuner trial (run once, before the timed region); 0 = no tuning")
     return ap.parse_args()
 
 
@@ -196,7 +206,8 @@ def run_reference(args):
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "ms", "n_gpus": args.gpus,
             "steps": len(timed), "warmup": args.warmup, "ms_per_step": v, "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "unknowns": m.real_dofs(), "iterations": its[-1]},
+            "config": {"workload": WORKLOADS.get(args.config, str(args.config)), "unknowns": m.real_dofs(),
+                       "iterations": its[-1]},
             "cpu_baseline": {"value": v, "unit": "ms", "cores": threads, "kind": "port",
                              "sample": "full solve of the workload to 1e-8 per step (oracle port: same discretisation"
                                        " and algorithm in C + OpenMP)"},
@@ -226,6 +237,13 @@ def main():
     prob = P.StokesProblem(m, device=local, precision=0, tol=1e-8, restart=args.restart)
     ronu_ms = [prob.ctx.upload_markers(m.markx, m.marky, m.markz, m.markt, m.rocks.n0, m.rocks.n1, m.rocks.ro)
                or prob.ctx.ronurecalc_resident() for _ in range(3)]
+    # smoother and sweep schedule for this model, chosen once (outside the timed region)
+    if args.tune_iters > 0:
+        tune = prob.autotune(args.tune_iters)
+    else:
+        from pardiso2_b200.capi import TuneInfo
+        tune = TuneInfo(smoother=1, sweep_growth=1, est_ms=float("nan"), rate=float("nan"), candidates=0,
+                        trial_iters=0)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
     def one(p):
@@ -265,6 +283,7 @@ def main():
     if args.solve_only:
         if rank == 0:
             print(json.dumps({"metric": METRIC, "value": value, "unit": "ms", "solve_only": True,
+                              "config": args.config, "autotune": tune.as_dict(),
                               "iterations": infos[-1].iterations, "gpu_launches": launches,
                               "smoother_ms_per_pass": pass_ms, "smoother_GBps": achieved}), flush=True)
         prob.close()
@@ -274,7 +293,8 @@ def main():
         return
 
     # FP64 V-cycle for comparison
-    p64 = P.StokesProblem(m, device=local, precision=1, tol=1e-8)
+    p64 = P.StokesProblem(m, device=local, precision=1, tol=1e-8, restart=args.restart, smoother=tune.smoother,
+                          sweep_growth=tune.sweep_growth)
     p64.ctx.upload_markers(m.markx, m.marky, m.markz, m.markt, m.rocks.n0, m.rocks.n1, m.rocks.ro)
     p64.ctx.ronurecalc_resident()
     for _ in range(max(1, args.warmup)):
@@ -314,8 +334,10 @@ def main():
         "metric": METRIC, "value": value, "unit": "ms", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": False, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32 V-cycle / f64 outer", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "unknowns": m.real_dofs(), "levels": m.multinum + 1,
-                   "sweeps": "4 pre + 4 post cell-block", "outer": "GCR(16) in FP64",
+        "config": {"workload": WORKLOADS[args.config], "unknowns": m.real_dofs(), "levels": m.multinum + 1,
+                   "smoother": ("full" if tune.smoother else "diagonal") + " cell-block Vanka, autotuned",
+                   "sweeps": "4 pre + 4 post on level 0, x%d per coarser level" % tune.sweep_growth,
+                   "outer": "GCR(%d) in FP64" % args.restart,
                    "l2": "flushed (256 MB write) before every step", "parallelism": "replicas" if world > 1 else "1 GPU"},
         "iterations": last.iterations, "rel_residual": last.rel_residual,
         "fp64_ms_per_solve": fp64_ms, "iterations_fp64": i64[-1].iterations,
@@ -331,7 +353,8 @@ def main():
         "clocks": clocks,
         "e2e": {"value": e2e_ms, "unit": "ms", "h2d_bytes_per_step": 24 * n + 32 * n, "d2h_bytes_per_step": 32 * n},
     }
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    line["autotune"] = tune.as_dict()
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and args.config <= 2:
         threads = os.cpu_count() or 1
         times, its = cpu_solve_ms(m, threads, steps=1)
         line["cpu_baseline"] = {"value": times[0], "unit": "ms", "cores": threads, "kind": "port",

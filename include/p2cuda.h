@@ -80,6 +80,16 @@ typedef struct {
     long long kernels;       /* kernels this library launched during the solve */
 } p2_solve_info;
 
+/* Choice made by p2_autotune. */
+typedef struct {
+    int smoother;        /* chosen p2_params.smoother */
+    int sweep_growth;    /* sweeps on level l = npre[0] * sweep_growth^l (pre and post) */
+    double est_ms;       /* estimated device time of one solve to tol with the choice */
+    double rate;         /* measured residual reduction per outer iteration */
+    int candidates;      /* configurations tried */
+    int trial_iters;     /* outer iterations per trial */
+} p2_tune_info;
+
 /* Fill p with the reference's defaults (mode.t3c) and this library's. */
 void p2_default_params(p2_params *p);
 
@@ -112,6 +122,15 @@ p2_status p2_stokes_solve(p2_ctx *ctx, float *vx, float *vy, float *vz, double *
  * device (no host transfers); read it back with p2_get_solution. */
 p2_status p2_stokes_solve_resident(p2_ctx *ctx, p2_solve_info *info);
 p2_status p2_get_solution(p2_ctx *ctx, double *vx, double *vy, double *vz, double *pr);
+
+/* Smoother autotuner (no counterpart in the reference, whose sweep counts
+ * come from mode.t3c multinnn): on the resident node fields, runs
+ * trial_iters outer iterations from a zero guess with each candidate (full
+ * or diagonal cell block, constant or doubling sweeps per coarser level),
+ * estimates each candidate's time to p2_params.tol from its measured rate
+ * and time per iteration, and keeps the cheapest in this context's
+ * parameters.  Call it once per model before the time loop. */
+p2_status p2_autotune(p2_ctx *ctx, int trial_iters, p2_tune_info *info);
 
 /* ronurecalc(): marker -> node viscosity/density interpolation.  Rock
  * viscosity is the per-type constant markn0 (pardiso/mark3mg.c:1481-1482;

@@ -76,6 +76,10 @@ class StokesProblem:
         info = self.ctx.stokes_solve(vx, vy, vz, pr)
         return {"vx": vx, "vy": vy, "vz": vz, "pr": pr}, info
 
+    def autotune(self, trial_iters: int = 16):
+        """Choose smoother and sweep schedule for this model (p2_autotune)."""
+        return self.ctx.autotune(trial_iters)
+
     def solve_fp64(self):
         """Solve on the resident node fields; FP64 solution arrays + info."""
         info = self.ctx.solve_resident()

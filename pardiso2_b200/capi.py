@@ -20,7 +20,7 @@ STATUS = {0: "P2_OK", 1: "P2_ERR_ARG", 2: "P2_ERR_CUDA", 3: "P2_ERR_NOMEM", 4: "
 EXPORTED = ["p2_default_params", "p2_create", "p2_destroy", "p2_last_error", "p2_set_grid", "p2_set_bc",
             "p2_set_nodes", "p2_stokes_solve", "p2_stokes_solve_resident", "p2_get_solution", "p2_ronurecalc",
             "p2_upload_markers", "p2_ronurecalc_resident", "p2_get_nodes", "p2_debug_apply", "p2_debug_restrict",
-            "p2_debug_prolong", "p2_debug_level_fields", "p2_debug_time_smoother", "p2_ronurecalc_noalloc"]
+            "p2_debug_prolong", "p2_debug_level_fields", "p2_debug_time_smoother", "p2_ronurecalc_noalloc", "p2_autotune"]
 
 
 class Params(C.Structure):
@@ -31,6 +31,14 @@ class Params(C.Structure):
                 ("multinum", C.c_int), ("npre", C.c_int * P2_MAX_LEVELS), ("npost", C.c_int * P2_MAX_LEVELS),
                 ("tol", C.c_double), ("max_iter", C.c_int), ("precision", C.c_int), ("restart", C.c_int),
                 ("omega", C.c_double), ("use_graphs", C.c_int), ("smoother", C.c_int)]
+
+
+class TuneInfo(C.Structure):
+    _fields_ = [("smoother", C.c_int), ("sweep_growth", C.c_int), ("est_ms", C.c_double), ("rate", C.c_double),
+                ("candidates", C.c_int), ("trial_iters", C.c_int)]
+
+    def as_dict(self) -> Dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
 
 
 class SolveInfo(C.Structure):
@@ -80,6 +88,8 @@ def load() -> C.CDLL:
     L.p2_upload_markers.argtypes = [vp, C.c_long, _fp, _fp, _fp, _bp, C.c_int, _dp, _dp, _dp]
     L.p2_ronurecalc_resident.argtypes = [vp, C.POINTER(C.c_double)]
     L.p2_get_nodes.argtypes = [vp] + [C.c_void_p] * 6
+    L.p2_autotune.argtypes = [vp, C.c_int, C.POINTER(TuneInfo)]
+    L.p2_autotune.restype = C.c_int
     for f in ("p2_create", "p2_set_grid", "p2_set_bc", "p2_set_nodes", "p2_stokes_solve", "p2_stokes_solve_resident",
               "p2_get_solution", "p2_ronurecalc", "p2_upload_markers", "p2_ronurecalc_resident", "p2_get_nodes"):
         getattr(L, f).restype = C.c_int
@@ -143,6 +153,12 @@ class Context:
         st = self.L.p2_stokes_solve(self.h, _ptr(vx), _ptr(vy), _ptr(vz), _ptr(pr), C.byref(info))
         if check:
             self._check(st, "p2_stokes_solve")
+        return info
+
+    def autotune(self, trial_iters: int = 16) -> TuneInfo:
+        """Pick the smoother configuration on the resident fields (p2_autotune)."""
+        info = TuneInfo()
+        self._check(self.L.p2_autotune(self.h, trial_iters, C.byref(info)), "p2_autotune")
         return info
 
     def solve_resident(self, check=True) -> SolveInfo:

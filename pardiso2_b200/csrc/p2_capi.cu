@@ -274,6 +274,16 @@ p2_status p2_debug_prolong(p2_ctx *ctx, int coarse_level, const double *coarse_x
     });
 }
 
+p2_status p2_autotune(p2_ctx *ctx, int trial_iters, p2_tune_info *info)
+{
+    return guard(ctx, [&] {
+        p2::Solver &S = *ctx->s;
+        P2_CUDA_TRY(cudaSetDevice(S.dev));
+        p2_tune_info r = S.autotune(trial_iters);
+        if (info) *info = r;
+    });
+}
+
 p2_status p2_debug_time_smoother(p2_ctx *ctx, int level, int passes, double *ms_per_pass)
 {
     return guard(ctx, [&] {

@@ -952,6 +952,71 @@ p2_solve_info Solver::solve()
     return info;
 }
 
+// Try each smoother configuration for trial_iters outer iterations; keep the
+// one with the least estimated time to prm.tol.
+p2_tune_info Solver::autotune(int trial_iters)
+{
+    if (!nodes_ready) throw Error(P2_ERR_STATE, "autotune before node fields were set");
+    if (trial_iters < 2 || trial_iters > 1000) throw Error(P2_ERR_ARG, "trial_iters out of 2..1000");
+    const p2_params saved = prm;
+    const int nl = (int)L.size();
+    const int base_pre = std::max(1, saved.npre[0]), base_post = std::max(1, saved.npost[0]);
+    p2_tune_info best{};
+    best.est_ms = INFINITY;
+    best.trial_iters = trial_iters;
+    const int smoothers[2] = {1, 0}, growths[2] = {1, 2};
+    for (int a = 0; a < 2; a++)
+        for (int g = 0; g < 2; g++) {
+            prm = saved;
+            prm.smoother = smoothers[a];
+            prm.max_iter = trial_iters;
+            for (int l = 0; l < nl; l++) {
+                long f = 1;
+                for (int q = 0; q < l; q++) f *= growths[g];
+                prm.npre[l] = (int)std::min<long>(64, base_pre * f);
+                prm.npost[l] = (int)std::min<long>(64, base_post * f);
+            }
+            drop_graphs();
+            set_initial(nullptr, nullptr, nullptr, nullptr);
+            p2_solve_info in = solve();
+            double est = INFINITY, rate = 1.0;
+            if (in.iterations > 0 && in.rel_residual > 0 && in.rel_residual0 > 0) {
+                rate = std::pow(in.rel_residual / in.rel_residual0, 1.0 / in.iterations);
+                double per_it = (in.ms_total - in.ms_setup) / in.iterations;
+                if (in.status == P2_OK) est = in.ms_total;
+                else if (rate < 1.0 && std::isfinite(rate))
+                    est = in.ms_setup + per_it * (in.iterations + std::log(saved.tol / in.rel_residual) / std::log(rate));
+            }
+            if (verbose)
+                std::fprintf(stderr, "p2cuda: autotune smoother %d growth %d: %d its, rate %.3f, est %.1f ms\n",
+                             prm.smoother, growths[g], in.iterations, rate, est);
+            best.candidates++;
+            if (est < best.est_ms) {
+                best.est_ms = est;
+                best.smoother = prm.smoother;
+                best.sweep_growth = growths[g];
+                best.rate = rate;
+            }
+        }
+    prm = saved;
+    if (!std::isfinite(best.est_ms)) {
+        // nothing converged within the trials: keep the defaults
+        best.smoother = saved.smoother;
+        best.sweep_growth = 1;
+    } else {
+        prm.smoother = best.smoother;
+        for (int l = 0; l < nl; l++) {
+            long f = 1;
+            for (int q = 0; q < l; q++) f *= best.sweep_growth;
+            prm.npre[l] = (int)std::min<long>(64, base_pre * f);
+            prm.npost[l] = (int)std::min<long>(64, base_post * f);
+        }
+    }
+    drop_graphs();
+    set_initial(nullptr, nullptr, nullptr, nullptr);
+    return best;
+}
+
 void Solver::set_initial(const float *vx, const float *vy, const float *vz, const double *pr)
 {
     long n = L[0].n;

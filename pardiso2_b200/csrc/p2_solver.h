@@ -84,6 +84,7 @@ class Solver {
     void debug_prolong(int lc, const double *coarse_x, double *fine_x);
     void debug_level_fields(float *nu, float *ro);
     double debug_time_smoother(int level, int passes);
+    p2_tune_info autotune(int trial_iters);
     bool verbose = false;
 
     int dev;

@@ -90,6 +90,34 @@ def test_solve_vs_reference_solution(gcase, precision):
         assert rel(sol[k], g["sol_" + k]) < 1e-6, (k, rel(sol[k], g["sol_" + k]))
 
 
+@pytest.mark.parametrize("smoother", [0, 1])
+def test_both_smoothers_reach_the_reference_solution(gcase, smoother):
+    """Diagonal and full cell-block smoothers are preconditioners only: both
+    converge to the same discrete solution."""
+    m, g, _ = gcase
+    prob = P.StokesProblem(m, tol=1e-8, smoother=smoother, sweep_growth=2)
+    prob.set_nodes({k: g["node_" + k] for k in FIELDS})
+    sol, info = prob.solve_fp64()
+    prob.close()
+    assert info.status == 0 and info.rel_residual <= 1e-8
+    for k in ("vx", "vy", "vz", "pr"):
+        assert rel(sol[k], g["sol_" + k]) < 1e-6, (k, rel(sol[k], g["sol_" + k]))
+
+
+def test_autotune_choice_reaches_the_reference_solution(gcase):
+    m, g, _ = gcase
+    prob = P.StokesProblem(m, tol=1e-8)
+    prob.set_nodes({k: g["node_" + k] for k in FIELDS})
+    tune = prob.autotune(6)
+    assert tune.candidates == 4 and tune.smoother in (0, 1) and tune.sweep_growth in (1, 2)
+    assert np.isfinite(tune.est_ms) and 0 < tune.rate < 1
+    sol, info = prob.solve_fp64()
+    prob.close()
+    assert info.status == 0 and info.rel_residual <= 1e-8
+    for k in ("vx", "vy", "vz", "pr"):
+        assert rel(sol[k], g["sol_" + k]) < 1e-6, k
+
+
 def test_vpiterate_host_arrays(gcase):
     """The reference-shaped call: float vx/vy/vz and double pr in/out."""
     m, g, _ = gcase
