@@ -77,7 +77,7 @@ def measured_peaks():
 def profile_traffic():
     """Per-launch DRAM bytes of the level-0 FP32 smoother pass from the
     committed ncu summary (None until one is captured)."""
-    p = os.path.join(ROOT, "profiles", "ncu_vanka_f32_level0_spheres65.txt")
+    p = os.path.join(ROOT, "profiles", "ncu_vanka_full_f32_level0.md")
     if not os.path.exists(p):
         return None
     m = re.search(r"dram_bytes_per_launch:\s*([0-9.eE+]+)", open(p).read())
@@ -249,7 +249,7 @@ def main():
     def one(p):
         flush.fill_(1.0)
         torch.cuda.synchronize()
-        info = p.ctx.solve_resident()
+        info = p.ctx.solve_resident(check=False)
         return info
 
     for _ in range(args.warmup):
@@ -279,7 +279,7 @@ def main():
     bytes_per_launch = SMOOTHER_BYTES_PER_NODE * n
     achieved = bytes_per_launch / (pass_ms * 1e-3) / 1e9
     peak, peak_kind = measured_peaks()
-    traffic = profile_traffic()
+    traffic = profile_traffic() if (args.config == CONFIG_IDX and tune.smoother) else None
     if args.solve_only:
         if rank == 0:
             print(json.dumps({"metric": METRIC, "value": value, "unit": "ms", "solve_only": True,
@@ -339,7 +339,7 @@ def main():
                    "sweeps": "4 pre + 4 post on level 0, x%d per coarser level" % tune.sweep_growth,
                    "outer": "GCR(%d) in FP64" % args.restart,
                    "l2": "flushed (256 MB write) before every step", "parallelism": "replicas" if world > 1 else "1 GPU"},
-        "iterations": last.iterations, "rel_residual": last.rel_residual,
+        "converged": all(i.status == 0 for i in infos), "iterations": last.iterations, "rel_residual": last.rel_residual,
         "fp64_ms_per_solve": fp64_ms, "iterations_fp64": i64[-1].iterations,
         "speedup_mixed_vs_fp64": fp64_ms / ms_per_step,
         "setup_ms": last.ms_setup, "vcycles_ms": last.ms_vcycles,
@@ -347,7 +347,7 @@ def main():
         "unknowns_per_s": m.real_dofs() * world / (ms_per_step * 1e-3),
         "gpu_launches": launches,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": traffic, "kernel": "k_vanka<float> level-0 colour pass",
+                     "traffic": traffic, "kernel": ("k_vanka_full<float>" if tune.smoother else "k_vanka<float>") + " level-0 colour pass",
                      "bytes_per_launch": bytes_per_launch, "ms_per_launch": pass_ms,
                      "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs, burst)"},
         "clocks": clocks,
