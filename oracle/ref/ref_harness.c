@@ -38,10 +38,22 @@ void PARDISO(void **pt, int *maxfct, int *mnum, int *mtype, int *phase, int *n,
 
 #include "head3mg.c"
 #include "load3mg.c"
+#ifdef P2REF_SHIM
+/* drop-in variant: vpiterate()/ronurecalc() come from move3mg_cuda.c (GPU) */
+#define vpiterate vpiterate_cpu
+#define ronurecalc ronurecalc_cpu
+#endif
 #include "move3mgNew.c"
 #include "mark3mg.c"
+#ifdef P2REF_SHIM
+#undef vpiterate
+#undef ronurecalc
+#endif
 #include "gaus3mg_SerieMG.c"
 #include "heat3mg.c"
+#ifdef P2REF_SHIM
+#include "move3mg_cuda.c"
+#endif
 
 /* ---------------------------------------------------------------------- */
 /* PARDISO-ABI shim.  A factorisation is cached across calls with the same

@@ -1,0 +1,24 @@
+/* Compile check (test infrastructure): the reference's unity build
+ * (pardiso/i3mg.c:1-19, without its main) with vpiterate() and ronurecalc()
+ * taken from pardiso2_b200/csrc/move3mg_cuda.c, exactly as INTEGRATION.md
+ * describes.  Built with -c only: it proves the shim compiles against the
+ * reference's globals and the p2cuda.h declarations. */
+#include <stdio.h>
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#include <omp.h>
+#include <time.h>
+#include <hdf5.h>
+
+#include "head3mg.c"
+#include "load3mg.c"
+#define vpiterate vpiterate_cpu
+#define ronurecalc ronurecalc_cpu
+#include "move3mgNew.c"
+#include "mark3mg.c"
+#undef vpiterate
+#undef ronurecalc
+#include "gaus3mg_SerieMG.c"
+#include "heat3mg.c"
+#include "move3mg_cuda.c"

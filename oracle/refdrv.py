@@ -15,24 +15,27 @@ import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "_ref", "libp2ref.so")
+# the same harness with vpiterate()/ronurecalc() from the drop-in shim
+# (pardiso2_b200/csrc/move3mg_cuda.c, calling libp2cuda.so on the GPU)
+SHIM_LIB_PATH = os.path.join(_HERE, "_ref", "libp2ref_shim.so")
 
 _dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
 _fp = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
 _ip = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
 _bp = np.ctypeslib.ndpointer(dtype=np.int8, flags="C_CONTIGUOUS")
 
-_lib: Optional[C.CDLL] = None
-_live = False
+_libs = {}
+_live = set()
 
 
-def available() -> bool:
-    return os.path.exists(LIB_PATH)
+def available(shim: bool = False) -> bool:
+    return os.path.exists(SHIM_LIB_PATH if shim else LIB_PATH)
 
 
-def _load() -> C.CDLL:
-    global _lib
-    if _lib is None:
-        lib = C.CDLL(LIB_PATH)
+def _load(shim: bool = False) -> C.CDLL:
+    path = SHIM_LIB_PATH if shim else LIB_PATH
+    if path not in _libs:
+        lib = C.CDLL(path)
         lib.p2ref_init.argtypes = [C.c_long, C.c_long, C.c_long, _dp, _dp, _dp, C.c_int, C.c_long]
         lib.p2ref_init.restype = C.c_int
         lib.p2ref_levels.argtypes = [_ip] * 5
@@ -63,25 +66,25 @@ def _load() -> C.CDLL:
         lib.p2ref_set_quiet.argtypes = [C.c_int]
         lib.p2ref_lu_count.restype = C.c_int
         lib.p2ref_num_threads.restype = C.c_int
-        _lib = lib
-    return _lib
+        _libs[path] = lib
+    return _libs[path]
 
 
 class RefModel:
     """The reference's global state set up for one Model (pardiso2_b200.model)."""
 
-    def __init__(self, model, npre=None, npost=None):
-        global _live
-        if _live:
-            raise RuntimeError("the reference keeps its state in globals: one RefModel per process")
-        lib = _load()
+    def __init__(self, model, npre=None, npost=None, shim: bool = False):
+        key = SHIM_LIB_PATH if shim else LIB_PATH
+        if key in _live:
+            raise RuntimeError("the reference keeps its state in globals: one RefModel per library and process")
+        lib = _load(shim)
         self.lib = lib
         self.m = model
         nx, ny, nz = model.shape
         nlev = lib.p2ref_init(nx, ny, nz, model.gx, model.gy, model.gz, model.multinum, model.markx.size)
         if nlev != model.multinum:
             raise RuntimeError("reference init failed")
-        _live = True
+        _live.add(key)
         L = nlev + 1
         self.mgx = np.zeros(L, np.int32)
         self.mgy = np.zeros(L, np.int32)
@@ -153,6 +156,14 @@ class RefModel:
             if verbose:
                 print("ref cycle %d rel %.3e" % (it, rel))
         return hist
+
+    def written(self):
+        """The arrays vpiterate() writes back: pr (double), vx, vy, vz (float)."""
+        n = self.m.nodenum
+        pr = np.zeros(n, np.float64)
+        v = [np.zeros(n, np.float32) for _ in range(3)]
+        self.lib.p2ref_get_written(pr, *v)
+        return {"pr": pr, "vx": v[0], "vy": v[1], "vz": v[2]}
 
     def solution(self):
         n = self.m.nodenum

@@ -1,0 +1,125 @@
+/*
+ * move3mg_cuda.c -- the reference's vpiterate() and ronurecalc() on top of
+ * libp2cuda.so (include/p2cuda.h).
+ *
+ * This file is compiled inside the reference's unity build (pardiso/i3mg.c
+ * includes head3mg.c, load3mg.c, move3mgNew.c, mark3mg.c, ... into one
+ * translation unit) and uses its globals (pardiso/head3mg.c) directly: the
+ * entry points keep their signatures and their data exchange through
+ * globals, so the time loop in i3mg.c is unchanged.  The two CPU functions it
+ * replaces are renamed out of the way before their files are included:
+ *
+ *     #define vpiterate  vpiterate_cpu     -- pardiso/move3mgNew.c:1791
+ *     #define ronurecalc ronurecalc_cpu    -- pardiso/mark3mg.c:630
+ *     #include "move3mgNew.c"
+ *     #include "mark3mg.c"
+ *     #undef vpiterate
+ *     #undef ronurecalc
+ *     #include "move3mg_cuda.c"
+ *
+ * Inputs read: xnumx, ynumy, znumz, gx, gy, gz, x/y/zperiodic, multinum,
+ * multinnn, mgp, mgn, bondm, bondv1, bondn1, bondnum, nu, ro, nxx, nxy, nxz,
+ * nyz, vx, vy, vz, pr, p0koef, p1koef, p2koef, v0koef, v1koef, nubeg, nuend,
+ * nukoef, viscmod, GXKOEF, GYKOEF, GZKOEF, pinit, pxinit, pyinit, pzinit;
+ * markers markx, marky, markz, markt, marknum and the rock tables markn0,
+ * markn1, markro (rocknum types).
+ * Outputs written: vx, vy, vz (float) and pr (double) by vpiterate; nu, ro,
+ * nxx, nxy, nxz, nyz by ronurecalc.  The stress and strain-rate fields and
+ * the time-step limit that the CPU vpiterate also derives are not computed
+ * here.
+ *
+ * Errors follow the reference's convention: a message on stdout and exit().
+ * The device is 0, or the value of the environment variable P2CUDA_DEVICE.
+ */
+
+#include "p2cuda.h"
+
+static p2_ctx *p2s_ctx = NULL;
+static long p2s_grid_nodes = -1;
+
+static void p2s_fail(const char *what, p2_status st)
+{
+    printf("%s failed (p2cuda status %d): %s\n", what, (int)st, p2s_ctx ? p2_last_error(p2s_ctx) : "no context");
+    exit(0);
+}
+
+static void p2s_params(p2_params *p)
+{
+    int l;
+    p2_default_params(p);
+    p->p0koef = p0koef;
+    p->p1koef = p1koef;
+    p->p2koef = p2koef;
+    p->v0koef = v0koef;
+    p->v1koef = v1koef;
+    p->nubeg = nubeg;
+    p->nuend = nuend;
+    p->nukoef = nukoef;
+    p->gxkoef = GXKOEF;
+    p->gykoef = GYKOEF;
+    p->gzkoef = GZKOEF;
+    p->pinit = pinit;
+    p->pxinit = (int)pxinit;
+    p->pyinit = (int)pyinit;
+    p->pzinit = (int)pzinit;
+    p->viscmod = viscmod;
+    p->multinum = multinum;
+    /* sweeps per level: multinnn[0][] before, multinnn[1][] after the coarse
+       correction (mode.t3c); the level-0 counts set the base of the schedule */
+    for (l = 0; l <= multinum && l < P2_MAX_LEVELS; l++) {
+        p->npre[l] = multinnn[0][l] > 0 ? multinnn[0][l] : 1;
+        p->npost[l] = multinnn[1][l] > 0 ? multinnn[1][l] : 1;
+    }
+}
+
+/* Context, grid and boundary tables: once, and again if the grid changes. */
+static void p2s_setup(void)
+{
+    p2_status st;
+    p2_params prm;
+    long nodes = xnumx * ynumy * znumz;
+    if (!p2s_ctx) {
+        const char *d = getenv("P2CUDA_DEVICE");
+        st = p2_create(&p2s_ctx, d ? atoi(d) : 0);
+        if (st != P2_OK) p2s_fail("p2_create", st);
+    }
+    if (p2s_grid_nodes == nodes) return;
+    p2s_params(&prm);
+    st = p2_set_grid(p2s_ctx, xnumx, ynumy, znumz, gx, gy, gz, xperiodic, yperiodic, zperiodic, &prm);
+    if (st != P2_OK) p2s_fail("p2_set_grid", st);
+    st = p2_set_bc(p2s_ctx, bondm, 4L * (mgp[multinum] + mgn[multinum]), &bondv1[0][0], bondn1, bondnum);
+    if (st != P2_OK) p2s_fail("p2_set_bc", st);
+    p2s_grid_nodes = nodes;
+}
+
+/* pardiso/move3mgNew.c:1791 (prototype pardiso/head3mg.c:362): the Stokes
+ * solve on the current node fields; vx, vy, vz, pr are the initial guess on
+ * entry and the solution on return.  m0 and f0 are the caller's loop
+ * counters, unused here as in the reference apart from its printing. */
+void vpiterate(int m0, int f0)
+{
+    p2_status st;
+    p2_solve_info info;
+    (void)m0;
+    (void)f0;
+    p2s_setup();
+    st = p2_set_nodes(p2s_ctx, nu, ro, nxx, nxy, nxz, nyz);
+    if (st != P2_OK) p2s_fail("p2_set_nodes", st);
+    st = p2_stokes_solve(p2s_ctx, vx, vy, vz, pr, &info);
+    if (st != P2_OK) p2s_fail("p2_stokes_solve", st);
+    printf("vpiterate (p2cuda): %d iterations, relative residual %e, %.2f ms\n", info.iterations, info.rel_residual,
+           info.ms_total);
+}
+
+/* pardiso/mark3mg.c:630 (prototype pardiso/head3mg.c:417): marker -> node
+ * viscosity and density; markers of type >= 50 are skipped as in the
+ * reference, every other type needs markn0 == markn1 (constant viscosity). */
+void ronurecalc(void)
+{
+    p2_status st;
+    int nrock = rocknum > 0 && rocknum <= MAXTMR ? rocknum : MAXTMR;
+    p2s_setup();
+    st = p2_ronurecalc(p2s_ctx, marknum, markx, marky, markz, (const signed char *)markt, nrock, markn0, markn1,
+                       markro, nu, ro, nxx, nxy, nxz, nyz);
+    if (st != P2_OK) p2s_fail("p2_ronurecalc", st);
+}

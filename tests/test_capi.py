@@ -52,3 +52,20 @@ def test_default_params_are_the_reference_defaults():
     assert (p.p0koef, p.p1koef, p.p2koef, p.v0koef, p.v1koef) == (0.3, 1.0, 0.0, 1.0, 1.0)
     assert (p.nubeg, p.nuend, p.viscmod) == (1.0, 1e4, 0)
     assert p.tol == 1e-8 and p.precision == 0
+
+
+def test_reference_shim_compiles_in_the_unity_build():
+    """pardiso2_b200/csrc/move3mg_cuda.c replaces vpiterate()/ronurecalc()
+    inside the reference's own unity build (needs the reference sources)."""
+    import subprocess
+    ref = os.environ.get("P2_REFERENCE_DIR", "/root/reference/pardiso")
+    if not os.path.isdir(ref):
+        pytest.skip("reference sources not present")
+    r = subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "shimcheck", "REF=" + ref],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stdout + r.stderr
+    syms = subprocess.run(["nm", os.path.join(ROOT, "oracle", "_ref", "shim_check.o")], capture_output=True,
+                          text=True).stdout
+    for name, kind in (("vpiterate", "T"), ("ronurecalc", "T"), ("vpiterate_cpu", "T"), ("ronurecalc_cpu", "T"),
+                       ("p2_stokes_solve", "U"), ("p2_ronurecalc", "U"), ("p2_set_grid", "U")):
+        assert any(ln.split()[-2:] == [kind, name] for ln in syms.splitlines()), (name, kind)

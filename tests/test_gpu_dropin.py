@@ -1,0 +1,39 @@
+"""The drop-in boundary end to end.
+
+The reference's own state (its globals, pardiso/head3mg.c, set up by the
+reference harness in oracle/ref/ref_harness.c) is driven through vpiterate()
+and ronurecalc() taken from pardiso2_b200/csrc/move3mg_cuda.c, the shim that
+replaces the reference's CPU functions and calls libp2cuda.so on the GPU.
+The arrays the shim writes back into the reference's globals (nu..nyz;
+vx, vy, vz as float and pr as double) must equal the golden vectors: node
+fields bit for bit, solutions within 1e-6 relative L2.
+
+Needs oracle/_ref/libp2ref_shim.so, built with the reference sources by
+`make -C oracle refshim`; skipped when it is absent.
+"""
+import numpy as np
+import pytest
+
+from oracle import refdrv
+from tests.test_oracle_golden import load_case, rel
+
+pytestmark = pytest.mark.gpu
+FIELDS = ("nu", "ro", "nxx", "nxy", "nxz", "nyz")
+
+
+def test_vpiterate_and_ronurecalc_through_the_reference_globals():
+    if not refdrv.available(shim=True):
+        pytest.skip("oracle/_ref/libp2ref_shim.so not built")
+    m, g = load_case("spheres21")
+    nl = m.multinum + 1
+    r = refdrv.RefModel(m, npre=[4] * nl, npost=[4] * nl, shim=True)
+    r.ronurecalc()                       # the shim's ronurecalc() -> p2_ronurecalc
+    f = r.nodes()
+    for k in FIELDS:
+        assert np.array_equal(f[k], g["node_" + k]), k
+    r.first_iteration()                  # the shim's vpiterate(0, 0) -> p2_stokes_solve
+    w = r.written()
+    assert w["vx"].dtype == np.float32 and w["pr"].dtype == np.float64
+    for k in ("vx", "vy", "vz", "pr"):
+        e = rel(w[k].astype(np.float64), g["sol_" + k])
+        assert e < 1e-6, (k, e)
