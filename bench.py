@@ -77,7 +77,7 @@ def measured_peaks():
 def profile_traffic():
     """Per-launch DRAM bytes of the level-0 FP32 smoother pass from the
     committed ncu summary (None until one is captured)."""
-    p = os.path.join(ROOT, "profiles", "ncu_vanka_full_f32_level0.md")
+    p = os.path.join(ROOT, "profiles", "ncu_vanka_full_f32_level0.txt")
     if not os.path.exists(p):
         return None
     m = re.search(r"dram_bytes_per_launch:\s*([0-9.eE+]+)", open(p).read())

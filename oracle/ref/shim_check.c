@@ -1,8 +1,9 @@
 /* Compile check (test infrastructure): the reference's unity build
  * (pardiso/i3mg.c:1-19, without its main) with vpiterate() and ronurecalc()
- * taken from pardiso2_b200/csrc/move3mg_cuda.c, exactly as INTEGRATION.md
- * describes.  Built with -c only: it proves the shim compiles against the
- * reference's globals and the p2cuda.h declarations. */
+ * taken from pardiso2_b200/csrc/move3mg_cuda.c: the CPU functions are renamed
+ * by two macros around their files and the shim is included after them.
+ * Built with -c only: it proves the shim compiles against the reference's
+ * globals and the p2cuda.h declarations. */
 #include <stdio.h>
 #include <math.h>
 #include <stdlib.h>
