@@ -51,15 +51,37 @@ __global__ void k_bc_rows(int nbc, const int *bu, const int *bt, const float *bk
     if (out32.c[0]) out32.c[c][u] = (float)v;
 }
 
-// Apply boundary rows: x_u = b_u + koef * x_t (one depth group of copy chains).
+// All boundary rows in one launch: each row walks its copy chain (the rows
+// owning its successive targets, bnext) and evaluates it from the innermost
+// row outwards, x = b + koef * x_target, the same arithmetic as applying the
+// chain-depth groups one after another.  Only the final target (a regular
+// unknown) is read from x, and each row writes only its own unknown.
+constexpr int kMaxBcChain = 8;
+
 template <typename T>
-__global__ void k_bc_set(int nbc, const int *bu, const int *bt, const float *bk, Vec4<T> x, Vec4<T> b)
+__global__ void k_bc_set_chain(int nbc, const int *bu, const int *bt, const float *bk, const int *bnext, Vec4<T> x,
+                               Vec4<T> b)
 {
     int q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= nbc) return;
-    int uc = bu[q], c = uc & 3, u = uc >> 2, t = bt[q];
-    T xt = t >= 0 ? (T)bk[q] * x.c[t & 3][t >> 2] : (T)0;
-    x.c[c][u] = b.c[c][u] + xt;
+    int chain[kMaxBcChain];
+    int m = 0, r = q;
+    chain[m++] = r;
+    while (bnext[r] >= 0 && m < kMaxBcChain) {
+        r = bnext[r];
+        chain[m++] = r;
+    }
+    const int t = bt[r];                      // innermost row's target (regular unknown or none)
+    T v = t >= 0 ? (T)bk[r] * x.c[t & 3][t >> 2] : (T)0;
+    int uc = bu[r];
+    v = b.c[uc & 3][uc >> 2] + v;
+    for (int s = m - 2; s >= 0; s--) {
+        const int rr = chain[s];
+        uc = bu[rr];
+        v = b.c[uc & 3][uc >> 2] + (T)bk[rr] * v;
+    }
+    uc = bu[q];
+    x.c[uc & 3][uc >> 2] = v;
 }
 
 // ---------------------------------------------------------------------------
@@ -297,35 +319,60 @@ __device__ __forceinline__ int ax_type(int comp, int axis)
     return (comp == axis + 1) ? 0 : 1;
 }
 
-// b_c = sum_f w r_f (P: * eta_f/eta_c) / sum_f w over non-boundary fine rows,
-// for non-boundary coarse rows (0 otherwise); x_c = 0 (vprestrict).
-template <typename T>
-__global__ void k_restrict(LevelView<T> F, Vec4<T> rf, LevelView<T> Cl, Vec4<T> bc, Vec4<T> xc, TransferView tv,
-                           int scale_p)
+__device__ __forceinline__ double block_sum(double v, double *sh);  // below (norms)
+
+// tv.m[axis][type] for a runtime type without copying the parameter struct
+__device__ __forceinline__ AxisMap pick_map(const AxisMap (&m)[3], int type)
 {
-    int v = blockIdx.x * blockDim.x + threadIdx.x;
-    if (v >= Cl.n) return;
-    int J = v % Cl.ny, I = (v / Cl.ny) % Cl.nx, K = v / (Cl.nx * Cl.ny);
-    uint8_t mc = Cl.bcm[v];
-    for (int c = 0; c < 4; c++) {
-        xc.c[c][v] = 0;
+    return type == 0 ? m[0] : (type == 1 ? m[1] : m[2]);
+}
+
+// Restriction (vprestrict, move3mgNew.c:3965-4353): b_c = sum_f w r_f / sum_f w
+// over the non-boundary fine rows (pressure residuals scaled by eta_f/eta_c,
+// 4308), for non-boundary coarse rows (0 otherwise); x_c = 0 (4351).  One
+// thread per (coarse node, component), components in consecutive blocks of
+// nodes.  Fused with the first half of the coarse
+// right-hand-side compatibility shift: every block adds its volume-weighted
+// continuity rows into partial[block]; the last block to finish (ticket
+// counter, reset by that block) sums the partials in block order and writes
+// sums[0] = sum of vol * b_P and sums[1] = vol_total (fixed per level).
+template <typename T>
+__global__ void k_restrict_compat(LevelView<T> F, Vec4<T> rf, LevelView<T> Cl, Vec4<T> bc, Vec4<T> xc,
+                                  TransferView tv, int scale_p, double vol_total, double *partial,
+                                  unsigned *ticket, double *sums)
+{
+    __shared__ double sh[32];
+    __shared__ bool last;
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int n = Cl.n;
+    double contrib = 0;
+    if (t < 4L * n) {
+        const int c = (int)(t / n), v = (int)(t % n);
+        const int J = v % Cl.ny, I = (v / Cl.ny) % Cl.nx, K = v / (Cl.nx * Cl.ny);
+        // component pointers by constant-index selects (no local copy of the parameters)
+        auto comp = [c](const Vec4<T> &V) { return c == 0 ? V.c[0] : (c == 1 ? V.c[1] : (c == 2 ? V.c[2] : V.c[3])); };
+        T *xcc = comp(xc), *bcc = comp(bc);
+        xcc[v] = 0;
         T out = 0;
-        if (valid_pos(c, I, J, K, Cl.nx, Cl.ny, Cl.nz) && !(mc & (1 << c))) {
-            const AxisMap &mx = tv.m[0][ax_type(c, 0)], &my = tv.m[1][ax_type(c, 1)], &mz = tv.m[2][ax_type(c, 2)];
+        if (valid_pos(c, I, J, K, Cl.nx, Cl.ny, Cl.nz) && !(Cl.bcm[v] & (1 << c))) {
+            const AxisMap mx = pick_map(tv.m[0], ax_type(c, 0)), my = pick_map(tv.m[1], ax_type(c, 1)),
+                          mz = pick_map(tv.m[2], ax_type(c, 2));
             T acc = 0, ws = 0;
-            T etac = c == 0 ? (T)Cl.ec[v] : (T)1;
+            const T etac = c == 0 ? (T)Cl.ec[v] : (T)1;
+            const int x0 = mx.ptr[I], x1 = mx.ptr[I + 1], y0 = my.ptr[J], y1 = my.ptr[J + 1];
+            const T *rfc = comp(rf);
             for (int qz = mz.ptr[K]; qz < mz.ptr[K + 1]; qz++) {
-                int fk = mz.idx[qz];
-                T wz = (T)mz.w[qz];
-                for (int qx = mx.ptr[I]; qx < mx.ptr[I + 1]; qx++) {
-                    int fi = mx.idx[qx];
-                    T wzx = wz * (T)mx.w[qx];
-                    for (int qy = my.ptr[J]; qy < my.ptr[J + 1]; qy++) {
-                        int fj = my.idx[qy];
-                        int f = P2IDX(F, fi, fj, fk);
+                const int fk = mz.idx[qz];
+                const T wz = (T)mz.w[qz];
+                for (int qx = x0; qx < x1; qx++) {
+                    const int fi = mx.idx[qx];
+                    const T wzx = wz * (T)mx.w[qx];
+                    const int base = fk * (F.nx * F.ny) + fi * F.ny;
+                    for (int qy = y0; qy < y1; qy++) {
+                        const int f = base + my.idx[qy];
                         if (F.bcm[f] & (1 << c)) continue;
-                        T w = wzx * (T)my.w[qy];
-                        T val = rf.c[c][f];
+                        const T w = wzx * (T)my.w[qy];
+                        T val = rfc[f];
                         if (c == 0 && scale_p) val *= (T)F.ec[f] / etac;
                         acc += val * w;
                         ws += w;
@@ -333,8 +380,28 @@ __global__ void k_restrict(LevelView<T> F, Vec4<T> rf, LevelView<T> Cl, Vec4<T> 
                 }
             }
             out = ws != (T)0 ? acc / ws : (T)0;
+            if (c == 0 && I > 0 && J > 0 && K > 0)
+                contrib = (double)out / ((double)Cl.ax.ih[I] * (double)Cl.ay.ih[J] * (double)Cl.az.ih[K]);
         }
-        bc.c[c][v] = out;
+        bcc[v] = out;
+    }
+    const double bsum = block_sum(contrib, sh);
+    if (threadIdx.x == 0) {
+        partial[blockIdx.x] = bsum;
+        __threadfence();
+        last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (last) {
+        __threadfence();
+        double s = 0;
+        for (int q = threadIdx.x; q < (int)gridDim.x; q += blockDim.x) s += ((volatile double *)partial)[q];
+        s = block_sum(s, sh);
+        if (threadIdx.x == 0) {
+            sums[0] = s;
+            sums[1] = vol_total;
+            *ticket = 0;
+        }
     }
 }
 
@@ -539,24 +606,6 @@ __global__ void k_dots_final(int nd, int nparts, const double *partial, double *
 }
 
 // Sum of volume * b_P over continuity rows and of the volumes (compatibility).
-template <typename T>
-__global__ void k_compat_partial(LevelView<T> L, const T *bp, double *partial)
-{
-    __shared__ double sh[32];
-    double s = 0, sv = 0;
-    for (int u = blockIdx.x * blockDim.x + threadIdx.x; u < L.n; u += gridDim.x * blockDim.x) {
-        int j = u % L.ny, i = (u / L.ny) % L.nx, k = u / (L.nx * L.ny);
-        if (i == 0 || j == 0 || k == 0 || (L.bcm[u] & BC_P)) continue;
-        double vol = 1.0 / ((double)L.ax.ih[i] * (double)L.ay.ih[j] * (double)L.az.ih[k]);
-        s += vol * (double)bp[u];
-        sv += vol;
-    }
-    double t = block_sum(s, sh);
-    if (threadIdx.x == 0) partial[blockIdx.x] = t;
-    t = block_sum(sv, sh);
-    if (threadIdx.x == 0) partial[gridDim.x + blockIdx.x] = t;
-}
-
 template <typename T>
 __global__ void k_compat_apply(LevelView<T> L, T *bp, const double *sums)
 {

@@ -385,6 +385,24 @@ void Solver::set_bc(const int *bondm, long bondm_len, const float *bondv1, const
         }
         Lv.bc_groups.push_back((int)bu.size());
         Lv.nbc = (int)bu.size();
+        // per row, the boundary row owning its target (-1: the target is a
+        // regular unknown or none), so one launch can evaluate whole chains
+        std::vector<int> bnext(bu.size(), -1);
+        {
+            std::map<int, int> pos;
+            for (size_t q = 0; q < bu.size(); q++) pos[bu[q]] = (int)q;
+            for (size_t q = 0; q < bu.size(); q++) {
+                auto it = bt[q] >= 0 ? pos.find(bt[q]) : pos.end();
+                if (it != pos.end()) bnext[q] = it->second;
+            }
+            for (size_t q = 0; q < bu.size(); q++) {
+                int d = 0;
+                for (int r = bnext[q]; r >= 0; r = bnext[r])
+                    if (++d >= kMaxBcChain)
+                        throw Error(P2_ERR_UNSUPPORTED, "boundary-row copy chain longer than " +
+                                                            std::to_string(kMaxBcChain));
+            }
+        }
         // resolved chains (target non-boundary, product of koefs) for the coarse elimination
         Lv.h_bu = bu;
         Lv.h_rt.assign(bu.size(), -1);
@@ -407,6 +425,7 @@ void Solver::set_bc(const int *bondm, long bondm_len, const float *bondv1, const
         Lv.bt = upload(arena, bt);
         Lv.bk = upload(arena, bk);
         Lv.bconst = upload(arena, bcst);
+        Lv.bnext = upload(arena, bnext);
     }
     allocate_work();
     bc_ready = true;
@@ -459,6 +478,25 @@ void Solver::allocate_work()
     Q.assign(m, Vec4<double>());
     for (int q = 0; q < m; q++) { v64n(Z[q]); v64n(Q[q]); }
     partial = (double *)arena.alloc(sizeof(double) * kRedBlocks * kMaxDots);
+    {
+        long maxc = 1;
+        for (int l = 1; l < nl; l++) maxc = std::max<long>(maxc, L[l].n);
+        rpartial = (double *)arena.alloc(sizeof(double) * nblk(4 * maxc));
+        rticket = (unsigned *)arena.alloc(sizeof(unsigned) * 4);
+        for (int l = 0; l < nl; l++) {
+            Level &Lv = L[l];
+            double vt = 0;
+            for (int k = 1; k < Lv.nz; k++)
+                for (int i = 1; i < Lv.nx; i++)
+                    for (int j = 1; j < Lv.ny; j++) {
+                        long u = (long)k * Lv.nx * Lv.ny + (long)i * Lv.ny + j;
+                        if (Lv.h_bcm[u] & BC_P) continue;
+                        vt += (Lv.g[0][i] - Lv.g[0][i - 1]) * (Lv.g[1][j] - Lv.g[1][j - 1]) *
+                              (Lv.g[2][k] - Lv.g[2][k - 1]);
+                    }
+            Lv.compat_vol = vt;
+        }
+    }
     dots = (double *)arena.alloc(sizeof(double) * kMaxDots * 2);
     scal = (double *)arena.alloc(sizeof(double) * 64);  // [0,1] compat sums, [2] alpha, [3] shift, [8..] GS coefficients
     P2_CUDA_TRY(cudaMallocHost(&hdots_raw, sizeof(double) * kMaxDots * 2));
@@ -657,10 +695,8 @@ template <typename T>
 void Solver::bc_set(int l, Vec4<T> &x, Vec4<T> &b)
 {
     Level &Lv = L[l];
-    for (size_t g = 0; g + 1 < Lv.bc_groups.size(); g++) {
-        int a = Lv.bc_groups[g], e = Lv.bc_groups[g + 1];
-        if (e > a)
-            k_bc_set<T><<<nblk(e - a), kThreads, 0, st>>>(e - a, Lv.bu + a, Lv.bt + a, Lv.bk + a, x, b); P2_COUNT_LAUNCH();
+    if (Lv.nbc > 0) {
+        k_bc_set_chain<T><<<nblk(Lv.nbc), kThreads, 0, st>>>(Lv.nbc, Lv.bu, Lv.bt, Lv.bk, Lv.bnext, x, b); P2_COUNT_LAUNCH();
     }
 }
 
@@ -732,9 +768,8 @@ void Solver::vcycle()
         level_residual<T>(l);
         Level &F = L[l], &Cl = L[l + 1];
         LevelView<T> VF = view<T>(l, false), VC = view<T>(l + 1, false);
-        k_restrict<T><<<nblk(Cl.n), kThreads, 0, st>>>(VF, r_of<T>(F), VC, b_of<T>(Cl), vx_of<T>(Cl, 0), F.tv, 1); P2_COUNT_LAUNCH();
-        k_compat_partial<T><<<kRedBlocks, kThreads, 0, st>>>(VC, b_of<T>(Cl).c[0], partial); P2_COUNT_LAUNCH();
-        k_dots_final<<<1, 1024, 0, st>>>(2, kRedBlocks, partial, scal); P2_COUNT_LAUNCH();
+        k_restrict_compat<T><<<nblk(4L * Cl.n), kThreads, 0, st>>>(VF, r_of<T>(F), VC, b_of<T>(Cl), vx_of<T>(Cl, 0),
+                                                                   F.tv, 1, Cl.compat_vol, rpartial, rticket, scal); P2_COUNT_LAUNCH();
         k_compat_apply<T><<<nblk(Cl.n), kThreads, 0, st>>>(VC, b_of<T>(Cl).c[0], scal); P2_COUNT_LAUNCH();
     }
     if (nl > 1) coarse_solve<T>(b_of<T>(L[nl - 1]), vx_of<T>(L[nl - 1], 0));
@@ -1123,10 +1158,10 @@ void Solver::debug_restrict(int lc, const double *fine_res, double *coarse_rhs, 
     TmpVec R(F.n), Bc(Cl.n), Xc(Cl.n);
     to_vec4(st, fine_res, F.n, R.v);
     LevelView<double> VF = view<double>(lc - 1, false), VC = view<double>(lc, false);
-    k_restrict<double><<<nblk(Cl.n), kThreads, 0, st>>>(VF, R.v, VC, Bc.v, Xc.v, F.tv, 1); P2_COUNT_LAUNCH();
+    // the V-cycle's restriction kernel (with its fused compatibility sums)
+    k_restrict_compat<double><<<nblk(4L * Cl.n), kThreads, 0, st>>>(VF, R.v, VC, Bc.v, Xc.v, F.tv, 1, Cl.compat_vol,
+                                                                     rpartial, rticket, scal); P2_COUNT_LAUNCH();
     if (compat) {
-        k_compat_partial<double><<<kRedBlocks, kThreads, 0, st>>>(VC, Bc.v.c[0], partial); P2_COUNT_LAUNCH();
-        k_dots_final<<<1, 1024, 0, st>>>(2, kRedBlocks, partial, scal); P2_COUNT_LAUNCH();
         k_compat_apply<double><<<nblk(Cl.n), kThreads, 0, st>>>(VC, Bc.v.c[0], scal); P2_COUNT_LAUNCH();
     }
     P2_CUDA_TRY(cudaGetLastError());

@@ -39,10 +39,11 @@ struct Level {
     std::vector<uint8_t> h_bcm;
     int pin = -1;
     double pinval = 0;
+    double compat_vol = 0;        // total volume of the non-boundary pressure cells
     // boundary rows sorted by copy-chain depth
     int nbc = 0;
     std::vector<int> bc_groups;
-    int *bu = nullptr, *bt = nullptr;
+    int *bu = nullptr, *bt = nullptr, *bnext = nullptr;  // bnext: row owning the target, or -1
     float *bk = nullptr, *bconst = nullptr;
     std::vector<int> h_bu, h_rt;  // unknown, resolved (non-boundary) target
     std::vector<double> h_rk;     // resolved coefficient
@@ -139,6 +140,8 @@ class Solver {
     Vec4<double> gx, gb, gr;
     std::vector<Vec4<double>> Z, Q;
     double *partial = nullptr, *dots = nullptr, *scal = nullptr;
+    double *rpartial = nullptr;   // per-block partial sums of the fused restriction
+    unsigned *rticket = nullptr;  // its last-block ticket (returns to zero)
     double *hdots_raw = nullptr;
     std::shared_ptr<double> hdots;
     // coarsest level
