@@ -66,7 +66,8 @@ typedef struct {
     double omega;        /* cell-block smoother damping (default 0.7) */
     int use_graphs;      /* capture the V-cycle in a CUDA graph (default 1) */
     int smoother;        /* cell-block smoother: 1 = exact 7x7 cell solve (default),
-                            0 = diagonal velocity block (cheaper, weak at stiff inclusions) */
+                            0 = diagonal velocity block (cheaper, weak at stiff inclusions),
+                            2 = the exact cell solve evaluated row by row (slower; a cross-check of 1) */
 } p2_params;
 
 typedef struct {

@@ -131,7 +131,47 @@ __device__ __forceinline__ T syz(const LevelView<T> &L, const Fields<T, S> &x, i
             (ld<T>(x.vz, P2IDX(L, a, b, c)) - ld<T>(x.vz, P2IDX(L, a, b - 1, c))) * L.ay.ihe[b]);
 }
 
-// (A x) of the x-, y-, z-Stokes rows at node (i,j,k) and their diagonals.
+// Diagonals of the x-, y-, z-Stokes rows at node (i,j,k).
+template <typename T>
+__device__ __forceinline__ T diag_vx(const LevelView<T> &L, int i, int j, int k)
+{
+    return -(L.ax.ihc[i] * (T)(4.0 / 3.0) *
+                 (eta_at(L, L.ec, P2IDX(L, i + 1, j + 1, k + 1)) * L.ax.ih[i + 1] +
+                  eta_at(L, L.ec, P2IDX(L, i, j + 1, k + 1)) * L.ax.ih[i]) +
+             L.ay.ihv[j] * (T)2.0 *
+                 (eta_at(L, L.exy, P2IDX(L, i, j + 1, k)) * L.ay.ihe[j + 1] +
+                  eta_at(L, L.exy, P2IDX(L, i, j, k)) * L.ay.ihe[j]) +
+             L.az.ihv[k] * (T)2.0 *
+                 (eta_at(L, L.exz, P2IDX(L, i, j, k + 1)) * L.az.ihe[k + 1] +
+                  eta_at(L, L.exz, P2IDX(L, i, j, k)) * L.az.ihe[k]));
+}
+template <typename T>
+__device__ __forceinline__ T diag_vy(const LevelView<T> &L, int i, int j, int k)
+{
+    return -(L.ay.ihc[j] * (T)(4.0 / 3.0) *
+                 (eta_at(L, L.ec, P2IDX(L, i + 1, j + 1, k + 1)) * L.ay.ih[j + 1] +
+                  eta_at(L, L.ec, P2IDX(L, i + 1, j, k + 1)) * L.ay.ih[j]) +
+             L.ax.ihv[i] * (T)2.0 *
+                 (eta_at(L, L.exy, P2IDX(L, i + 1, j, k)) * L.ax.ihe[i + 1] +
+                  eta_at(L, L.exy, P2IDX(L, i, j, k)) * L.ax.ihe[i]) +
+             L.az.ihv[k] * (T)2.0 *
+                 (eta_at(L, L.eyz, P2IDX(L, i, j, k + 1)) * L.az.ihe[k + 1] +
+                  eta_at(L, L.eyz, P2IDX(L, i, j, k)) * L.az.ihe[k]));
+}
+template <typename T>
+__device__ __forceinline__ T diag_vz(const LevelView<T> &L, int i, int j, int k)
+{
+    return -(L.az.ihc[k] * (T)(4.0 / 3.0) *
+                 (eta_at(L, L.ec, P2IDX(L, i + 1, j + 1, k + 1)) * L.az.ih[k + 1] +
+                  eta_at(L, L.ec, P2IDX(L, i + 1, j + 1, k)) * L.az.ih[k]) +
+             L.ax.ihv[i] * (T)2.0 *
+                 (eta_at(L, L.exz, P2IDX(L, i + 1, j, k)) * L.ax.ihe[i + 1] +
+                  eta_at(L, L.exz, P2IDX(L, i, j, k)) * L.ax.ihe[i]) +
+             L.ay.ihv[j] * (T)2.0 *
+                 (eta_at(L, L.eyz, P2IDX(L, i, j + 1, k)) * L.ay.ihe[j + 1] +
+                  eta_at(L, L.eyz, P2IDX(L, i, j, k)) * L.ay.ihe[j]));
+}
+
 template <typename T, typename S>
 __device__ __forceinline__ T row_vx(const LevelView<T> &L, const Fields<T, S> &x, int i, int j, int k, T *diag)
 {
@@ -139,16 +179,7 @@ __device__ __forceinline__ T row_vx(const LevelView<T> &L, const Fields<T, S> &x
           (sxy(L, x, i, j + 1, k) - sxy(L, x, i, j, k)) * L.ay.ihv[j] +
           (sxz(L, x, i, j, k + 1) - sxz(L, x, i, j, k)) * L.az.ihv[k] -
           (ld<T>(x.p, P2IDX(L, i + 1, j + 1, k + 1)) - ld<T>(x.p, P2IDX(L, i, j + 1, k + 1))) * L.ax.ihc[i];
-    if (diag)
-        *diag = -(L.ax.ihc[i] * (T)(4.0 / 3.0) *
-                      (eta_at(L, L.ec, P2IDX(L, i + 1, j + 1, k + 1)) * L.ax.ih[i + 1] +
-                       eta_at(L, L.ec, P2IDX(L, i, j + 1, k + 1)) * L.ax.ih[i]) +
-                  L.ay.ihv[j] * (T)2.0 *
-                      (eta_at(L, L.exy, P2IDX(L, i, j + 1, k)) * L.ay.ihe[j + 1] +
-                       eta_at(L, L.exy, P2IDX(L, i, j, k)) * L.ay.ihe[j]) +
-                  L.az.ihv[k] * (T)2.0 *
-                      (eta_at(L, L.exz, P2IDX(L, i, j, k + 1)) * L.az.ihe[k + 1] +
-                       eta_at(L, L.exz, P2IDX(L, i, j, k)) * L.az.ihe[k]));
+    if (diag) *diag = diag_vx(L, i, j, k);
     return v;
 }
 template <typename T, typename S>
@@ -158,16 +189,7 @@ __device__ __forceinline__ T row_vy(const LevelView<T> &L, const Fields<T, S> &x
           (sxy(L, x, i + 1, j, k) - sxy(L, x, i, j, k)) * L.ax.ihv[i] +
           (syz(L, x, i, j, k + 1) - syz(L, x, i, j, k)) * L.az.ihv[k] -
           (ld<T>(x.p, P2IDX(L, i + 1, j + 1, k + 1)) - ld<T>(x.p, P2IDX(L, i + 1, j, k + 1))) * L.ay.ihc[j];
-    if (diag)
-        *diag = -(L.ay.ihc[j] * (T)(4.0 / 3.0) *
-                      (eta_at(L, L.ec, P2IDX(L, i + 1, j + 1, k + 1)) * L.ay.ih[j + 1] +
-                       eta_at(L, L.ec, P2IDX(L, i + 1, j, k + 1)) * L.ay.ih[j]) +
-                  L.ax.ihv[i] * (T)2.0 *
-                      (eta_at(L, L.exy, P2IDX(L, i + 1, j, k)) * L.ax.ihe[i + 1] +
-                       eta_at(L, L.exy, P2IDX(L, i, j, k)) * L.ax.ihe[i]) +
-                  L.az.ihv[k] * (T)2.0 *
-                      (eta_at(L, L.eyz, P2IDX(L, i, j, k + 1)) * L.az.ihe[k + 1] +
-                       eta_at(L, L.eyz, P2IDX(L, i, j, k)) * L.az.ihe[k]));
+    if (diag) *diag = diag_vy(L, i, j, k);
     return v;
 }
 template <typename T, typename S>
@@ -177,16 +199,7 @@ __device__ __forceinline__ T row_vz(const LevelView<T> &L, const Fields<T, S> &x
           (sxz(L, x, i + 1, j, k) - sxz(L, x, i, j, k)) * L.ax.ihv[i] +
           (syz(L, x, i, j + 1, k) - syz(L, x, i, j, k)) * L.ay.ihv[j] -
           (ld<T>(x.p, P2IDX(L, i + 1, j + 1, k + 1)) - ld<T>(x.p, P2IDX(L, i + 1, j + 1, k))) * L.az.ihc[k];
-    if (diag)
-        *diag = -(L.az.ihc[k] * (T)(4.0 / 3.0) *
-                      (eta_at(L, L.ec, P2IDX(L, i + 1, j + 1, k + 1)) * L.az.ih[k + 1] +
-                       eta_at(L, L.ec, P2IDX(L, i + 1, j + 1, k)) * L.az.ih[k]) +
-                  L.ax.ihv[i] * (T)2.0 *
-                      (eta_at(L, L.exz, P2IDX(L, i + 1, j, k)) * L.ax.ihe[i + 1] +
-                       eta_at(L, L.exz, P2IDX(L, i, j, k)) * L.ax.ihe[i]) +
-                  L.ay.ihv[j] * (T)2.0 *
-                      (eta_at(L, L.eyz, P2IDX(L, i, j + 1, k)) * L.ay.ihe[j + 1] +
-                       eta_at(L, L.eyz, P2IDX(L, i, j, k)) * L.ay.ihe[j]));
+    if (diag) *diag = diag_vz(L, i, j, k);
     return v;
 }
 template <typename T, typename S>

@@ -309,6 +309,144 @@ __global__ void __launch_bounds__(128) k_vanka_full(LevelView<T> L, T *P, Vec4<T
 }
 
 // ---------------------------------------------------------------------------
+// k_vanka_full with the six momentum residuals assembled from shared
+// stresses: the cell's three normal stresses come from one set of strain
+// rates (each face row of the cell uses one of them), the twelve shear
+// stresses on the cell's edges are each evaluated once (every edge is shared
+// by two of the cell's faces), and the continuity residual is the cell's
+// divergence.  The six neighbour cells contribute one normal stress each.
+// Same terms as row_vx/row_vy/row_vz, about half the loads and arithmetic.
+template <typename T>
+__global__ void __launch_bounds__(128) k_vanka_fast(LevelView<T> L, T *P, Vec4<T> vin, Vec4<T> vout, Vec4<T> b,
+                                                    T omega, int col)
+{
+    int half = (L.ny) / 2;
+    long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    long lines = (long)(L.nx - 1) * (L.nz - 1);
+    if (t >= lines * half) return;
+    int jj = (int)(t % half);
+    long line = t / half;
+    const int i = 1 + (int)(line % (L.nx - 1)), k = 1 + (int)(line / (L.nx - 1));
+    const int j0 = (((1 + i + k) & 1) == col) ? 1 : 2;
+    const int j = j0 + 2 * jj;
+    if (j > L.ny - 1) return;
+    Fields<T, T> x{P, vin.c[1], vin.c[2], vin.c[3]};
+    const int u = P2IDX(L, i, j, k);
+    const bool pact = (L.bcm[u] & BC_P) == 0;
+    int fi[6];
+    const int fc[6] = {1, 1, 2, 2, 3, 3};
+    fi[0] = P2IDX(L, i - 1, j - 1, k - 1);
+    fi[1] = P2IDX(L, i, j - 1, k - 1);
+    fi[2] = fi[0];
+    fi[3] = P2IDX(L, i - 1, j, k - 1);
+    fi[4] = fi[0];
+    fi[5] = P2IDX(L, i - 1, j - 1, k);
+    const T g[6] = {-L.ax.ihc[i - 1], L.ax.ihc[i], -L.ay.ihc[j - 1], L.ay.ihc[j], -L.az.ihc[k - 1], L.az.ihc[k]};
+    const T hx = L.ax.ih[i], hy = L.ay.ih[j], hz = L.az.ih[k];
+    const T cc[6] = {-hx, hx, -hy, hy, -hz, hz};
+    // the cell's strain rates and normal stresses
+    const T exx = (ld<T>(x.vx, fi[1]) - ld<T>(x.vx, fi[0])) * hx;
+    const T eyy = (ld<T>(x.vy, fi[3]) - ld<T>(x.vy, fi[0])) * hy;
+    const T ezz = (ld<T>(x.vz, fi[5]) - ld<T>(x.vz, fi[0])) * hz;
+    const T div3 = (exx + eyy + ezz) / (T)3.0;
+    const T E2 = (T)2.0 * eta_at(L, L.ec, u);
+    const T s0 = E2 * (exx - div3), s1 = E2 * (eyy - div3), s2 = E2 * (ezz - div3);
+    // neighbour cells' normal stress along the face normal
+    const T sL = snn(L, x, 0, i - 1, j, k), sR = snn(L, x, 0, i + 1, j, k);
+    const T sF = snn(L, x, 1, i, j - 1, k), sB = snn(L, x, 1, i, j + 1, k);
+    const T sD = snn(L, x, 2, i, j, k - 1), sU = snn(L, x, 2, i, j, k + 1);
+    // the twelve edge shear stresses
+    const T xy00 = sxy(L, x, i - 1, j - 1, k - 1), xy01 = sxy(L, x, i - 1, j, k - 1);
+    const T xy10 = sxy(L, x, i, j - 1, k - 1), xy11 = sxy(L, x, i, j, k - 1);
+    const T xz00 = sxz(L, x, i - 1, j - 1, k - 1), xz01 = sxz(L, x, i - 1, j - 1, k);
+    const T xz10 = sxz(L, x, i, j - 1, k - 1), xz11 = sxz(L, x, i, j - 1, k);
+    const T yz00 = syz(L, x, i - 1, j - 1, k - 1), yz01 = syz(L, x, i - 1, j - 1, k);
+    const T yz10 = syz(L, x, i - 1, j, k - 1), yz11 = syz(L, x, i - 1, j, k);
+    const T p0 = ld<T>(x.p, u);
+    const T pL = ld<T>(x.p, P2IDX(L, i - 1, j, k)), pR = ld<T>(x.p, P2IDX(L, i + 1, j, k));
+    const T pF = ld<T>(x.p, P2IDX(L, i, j - 1, k)), pB = ld<T>(x.p, P2IDX(L, i, j + 1, k));
+    const T pD = ld<T>(x.p, P2IDX(L, i, j, k - 1)), pU = ld<T>(x.p, P2IDX(L, i, j, k + 1));
+    T ax[6];
+    ax[0] = (s0 - sL) * L.ax.ihc[i - 1] + (xy01 - xy00) * L.ay.ihv[j - 1] + (xz01 - xz00) * L.az.ihv[k - 1] -
+            (p0 - pL) * L.ax.ihc[i - 1];
+    ax[1] = (sR - s0) * L.ax.ihc[i] + (xy11 - xy10) * L.ay.ihv[j - 1] + (xz11 - xz10) * L.az.ihv[k - 1] -
+            (pR - p0) * L.ax.ihc[i];
+    ax[2] = (s1 - sF) * L.ay.ihc[j - 1] + (xy10 - xy00) * L.ax.ihv[i - 1] + (yz01 - yz00) * L.az.ihv[k - 1] -
+            (p0 - pF) * L.ay.ihc[j - 1];
+    ax[3] = (sB - s1) * L.ay.ihc[j] + (xy11 - xy01) * L.ax.ihv[i - 1] + (yz11 - yz10) * L.az.ihv[k - 1] -
+            (pB - p0) * L.ay.ihc[j];
+    ax[4] = (s2 - sD) * L.az.ihc[k - 1] + (xz10 - xz00) * L.ax.ihv[i - 1] + (yz10 - yz00) * L.ay.ihv[j - 1] -
+            (p0 - pD) * L.az.ihc[k - 1];
+    ax[5] = (sU - s2) * L.az.ihc[k] + (xz11 - xz01) * L.ax.ihv[i - 1] + (yz11 - yz01) * L.ay.ihv[j - 1] -
+            (pU - p0) * L.az.ihc[k];
+    T M[6][6];
+    face_block(L, i, j, k, M);
+    M[0][0] = diag_vx(L, i - 1, j - 1, k - 1);
+    M[1][1] = diag_vx(L, i, j - 1, k - 1);
+    M[2][2] = diag_vy(L, i - 1, j - 1, k - 1);
+    M[3][3] = diag_vy(L, i - 1, j, k - 1);
+    M[4][4] = diag_vz(L, i - 1, j - 1, k - 1);
+    M[5][5] = diag_vz(L, i - 1, j - 1, k);
+    bool act[6];
+    T y1[6], y2[6];
+#pragma unroll
+    for (int q = 0; q < 6; q++) act[q] = !(L.bcm[fi[q]] & (1 << fc[q]));
+#pragma unroll
+    for (int a = 0; a < 6; a++) {
+#pragma unroll
+        for (int c = 0; c < 6; c++)
+            if (!(act[a] && act[c])) M[a][c] = a == c ? (T)1 : (T)0;
+        y1[a] = act[a] ? b.c[fc[a]][fi[a]] - ax[a] : (T)0;
+        y2[a] = act[a] ? g[a] : (T)0;
+    }
+#pragma unroll
+    for (int c = 0; c < 6; c++) {
+        const T ip = (T)1 / M[c][c];
+#pragma unroll
+        for (int a = 0; a < 6; a++) {
+            if (a > c) {
+                const T f = M[a][c] * ip;
+#pragma unroll
+                for (int e = 0; e < 6; e++)
+                    if (e > c) M[a][e] -= f * M[c][e];
+                y1[a] -= f * y1[c];
+                y2[a] -= f * y2[c];
+            }
+        }
+    }
+#pragma unroll
+    for (int cc5 = 0; cc5 < 6; cc5++) {
+        const int c = 5 - cc5;
+#pragma unroll
+        for (int e = 0; e < 6; e++) {
+            if (e > c) {
+                y1[c] -= M[c][e] * y1[e];
+                y2[c] -= M[c][e] * y2[e];
+            }
+        }
+        const T ip = (T)1 / M[c][c];
+        y1[c] *= ip;
+        y2[c] *= ip;
+    }
+    T dp = 0;
+    if (pact) {
+        T num = -(b.c[0][u] - (exx + eyy + ezz)), den = 0;
+#pragma unroll
+        for (int q = 0; q < 6; q++) {
+            num += cc[q] * y1[q];
+            den += cc[q] * y2[q];
+        }
+        if (den != (T)0) {
+            dp = num / den;
+            P[u] += omega * dp;
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < 6; q++)
+        if (act[q]) vout.c[fc[q]][fi[q]] = vin.c[fc[q]][fi[q]] + omega * (y1[q] - dp * y2[q]);
+}
+
+// ---------------------------------------------------------------------------
 // Transfers.  Per-axis tables (host-built from the reference's index rules,
 // move3mgNew.c:3562-3575 and the corresponding blocks of vprestrict and
 // vpprolong): for a fine index m, the coarse interval lo[m] and the weights

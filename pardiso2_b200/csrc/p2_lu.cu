@@ -21,6 +21,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdio>
+#include <cstdlib>
 #include <vector>
 
 #include "p2_internal.cuh"
@@ -28,81 +30,88 @@
 namespace p2 {
 
 constexpr int kPB = 32;                                  // panel width
-constexpr int kPanelThreads = 512;
 constexpr int kMaxPanelBytes = 200 * 1024;               // shared-memory panel
 constexpr int kMaxPanelRows = kMaxPanelBytes / (8 * kPB);  // 800 rows
 
 // ---------------------------------------------------------------------------
-// Panel [k0, k0+nb) x rows [k0, r1) factored in shared memory (column-major,
-// leading dimension m = r1 - k0).
-__global__ void __launch_bounds__(kPanelThreads) k_panel_smem(double *A, int lda, int k0, int nb, int r1, int *ipiv,
-                                                              int *info)
+// Panel in shared memory with one thread per panel row and the pivot order
+// tracked instead of rows swapped: at step jj every row not yet chosen
+// competes (largest |a|, lowest storage row on ties), the chosen row stays
+// where it is and the others are eliminated against it.  Two barriers per
+// column.  At the end the LAPACK-style interchange sequence (swap logical rows
+// jj and ipiv[jj]) that produces the same final row order is rebuilt, and the
+// rows are written back in that order: the result of a row-swapping panel
+// factorisation (partial pivoting, LAPACK getf2) of the same columns.
+constexpr int kTrackThreads = 1024;
+static_assert(kMaxPanelRows <= kTrackThreads, "one thread per panel row");
+
+__global__ void __launch_bounds__(kTrackThreads) k_panel_track(double *A, int lda, int k0, int nb, int r1, int *ipiv,
+                                                               int *info)
 {
     extern __shared__ double P[];
-    __shared__ double sv[kPanelThreads / 32];
-    __shared__ int si[kPanelThreads / 32];
-    __shared__ int piv;
+    __shared__ double wv[32];
+    __shared__ int wi[32];
+    __shared__ int prow[kPB];
+    __shared__ int lmap[kMaxPanelRows], linv[kMaxPanelRows];
     const int m = r1 - k0;
     for (int t = threadIdx.x; t < m * nb; t += blockDim.x) {
         int r = t % m, c = t / m;
         P[t] = A[(size_t)(k0 + c) * lda + k0 + r];
     }
     __syncthreads();
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int row = threadIdx.x, lane = row & 31, w = row >> 5;
+    bool live = row < m;  // not yet chosen as a pivot
     for (int jj = 0; jj < nb; jj++) {
-        double *cj = P + (size_t)jj * m;
-        double best = -1.0;
-        int bi = m;
-        for (int i = jj + threadIdx.x; i < m; i += blockDim.x) {
-            double v = fabs(cj[i]);
-            if (v > best) { best = v; bi = i; }
-        }
+        double best = live ? fabs(P[(size_t)jj * m + row]) : -1.0;
+        int bi = live ? row : 0x7fffffff;
         for (int o = 16; o > 0; o >>= 1) {
             double ov = __shfl_down_sync(0xffffffffu, best, o);
             int oi = __shfl_down_sync(0xffffffffu, bi, o);
             if (ov > best || (ov == best && oi < bi)) { best = ov; bi = oi; }
         }
-        if (lane == 0) { sv[w] = best; si[w] = bi; }
+        if (lane == 0) { wv[w] = best; wi[w] = bi; }
         __syncthreads();
-        if (w == 0) {
-            constexpr int nw = kPanelThreads / 32;
-            best = lane < nw ? sv[lane] : -1.0;
-            bi = lane < nw ? si[lane] : m;
-            for (int o = 16; o > 0; o >>= 1) {
-                double ov = __shfl_down_sync(0xffffffffu, best, o);
-                int oi = __shfl_down_sync(0xffffffffu, bi, o);
-                if (ov > best || (ov == best && oi < bi)) { best = ov; bi = oi; }
-            }
-            if (lane == 0) {
-                if (!(best > 0.0)) {
-                    if (*info == 0) *info = k0 + jj + 1;
-                    bi = jj;
-                }
-                piv = bi;
-                ipiv[k0 + jj] = k0 + bi;
-            }
+        // every warp reduces the per-warp candidates itself (butterfly: all lanes agree)
+        best = lane < (int)(blockDim.x >> 5) ? wv[lane] : -1.0;
+        bi = lane < (int)(blockDim.x >> 5) ? wi[lane] : 0x7fffffff;
+        for (int o = 16; o > 0; o >>= 1) {
+            double ov = __shfl_xor_sync(0xffffffffu, best, o);
+            int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+            if (ov > best || (ov == best && oi < bi)) { best = ov; bi = oi; }
         }
-        __syncthreads();
-        const int p = piv;
-        if (p != jj && threadIdx.x < nb) {
-            double *c = P + (size_t)threadIdx.x * m;
-            double t = c[jj];
-            c[jj] = c[p];
-            c[p] = t;
+        const int p = bi;
+        if (row == 0) {
+            prow[jj] = p;
+            if (!(best > 0.0) && *info == 0) *info = k0 + jj + 1;
         }
-        __syncthreads();
-        const double d = cj[jj];
-        const double inv = d != 0.0 ? 1.0 / d : 0.0;
-        for (int i = jj + 1 + threadIdx.x; i < m; i += blockDim.x) {
-            double l = cj[i] * inv;
-            cj[i] = l;
-            for (int c = jj + 1; c < nb; c++) P[(size_t)c * m + i] -= l * P[(size_t)c * m + jj];
+        const double pv = P[(size_t)jj * m + p];
+        const double inv = pv != 0.0 ? 1.0 / pv : 0.0;
+        if (row == p) live = false;
+        if (live) {
+            const double l = P[(size_t)jj * m + row] * inv;
+            P[(size_t)jj * m + row] = l;
+#pragma unroll
+            for (int c = 0; c < kPB; c++)
+                if (c > jj && c < nb) P[(size_t)c * m + row] -= l * P[(size_t)c * m + p];
         }
         __syncthreads();
     }
+    // interchange sequence and final row order
+    for (int r = threadIdx.x; r < m; r += blockDim.x) { lmap[r] = r; linv[r] = r; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int jj = 0; jj < nb; jj++) {
+            const int p = prow[jj], q = linv[p];   // logical position of the chosen row (q >= jj)
+            ipiv[k0 + jj] = k0 + q;
+            const int a = lmap[jj];
+            lmap[jj] = p; linv[p] = jj;
+            lmap[q] = a;  linv[a] = q;
+        }
+    }
+    __syncthreads();
     for (int t = threadIdx.x; t < m * nb; t += blockDim.x) {
         int r = t % m, c = t / m;
-        A[(size_t)(k0 + c) * lda + k0 + r] = P[t];
+        A[(size_t)(k0 + c) * lda + k0 + r] = P[(size_t)c * m + lmap[r]];
     }
 }
 
@@ -172,48 +181,90 @@ __global__ void k_panel_global(double *A, int lda, int k0, int nb, int r1, int *
 }
 
 // For columns c in [c0, c1) of B: apply the panel's interchanges (rows k0..)
-// then B[k0:k0+nb, c] = L11^-1 B[k0:k0+nb, c], L11 unit lower from A.
-__global__ void k_swap_trsm_lower(const double *A, int lda, int k0, int nb, const int *ipiv, double *B, int ldb,
-                                  int c0, int c1)
+// then B[k0:k0+nb, c] = L11^-1 B[k0:k0+nb, c], L11 unit lower from A.  The
+// interchange sequence is turned into one permutation first: warp 0 replays the nb swaps on the set of rows they touch
+// (rows k0..k0+nb and the pivot rows below, at most 2 nb), recording for each
+// slot the row whose value ends there.  Each thread then loads its column's
+// values for the whole set at once (independent loads instead of a chain of
+// dependent swaps), solves with L11 and stores the set back.
+constexpr int kTrsmThreads = 128;
+
+__global__ void __launch_bounds__(kTrsmThreads) k_perm_trsm_lower(const double *A, int lda, int k0, int nb,
+                                                                  const int *ipiv, double *B, int ldb, int c0, int c1)
 {
     __shared__ double L[kPB][kPB + 1];
-    __shared__ int pv[kPB];
+    __shared__ int S[2 * kPB], src[2 * kPB];
+    __shared__ int nS;
+    __shared__ double ext[kPB][kTrsmThreads];
     for (int t = threadIdx.x; t < nb * nb; t += blockDim.x) {
         int r = t % nb, s = t / nb;
         L[r][s] = A[(size_t)(k0 + s) * lda + k0 + r];
     }
-    if (threadIdx.x < nb) pv[threadIdx.x] = ipiv ? ipiv[k0 + threadIdx.x] : k0 + threadIdx.x;
+    if (threadIdx.x < 32) {
+        const int lane = threadIdx.x;
+        int cnt = nb;
+        if (lane < nb) { S[lane] = k0 + lane; src[lane] = k0 + lane; }
+        __syncwarp();
+        for (int jj = 0; jj < nb; jj++) {
+            const int p = ipiv[k0 + jj];
+            int sp;
+            if (p < k0 + nb) {
+                sp = p - k0;
+            } else {
+                const int idx = nb + lane;
+                const bool hit = idx < cnt && S[idx] == p;
+                const unsigned bal = __ballot_sync(0xffffffffu, hit);
+                if (bal) {
+                    sp = nb + __ffs(bal) - 1;
+                } else {
+                    sp = cnt;
+                    if (lane == 0) { S[cnt] = p; src[cnt] = p; }
+                    cnt++;
+                }
+            }
+            __syncwarp();
+            if (lane == 0 && sp != jj) { int t = src[jj]; src[jj] = src[sp]; src[sp] = t; }
+            __syncwarp();
+        }
+        if (lane == 0) nS = cnt;
+    }
     __syncthreads();
-    int c = c0 + blockIdx.x * blockDim.x + threadIdx.x;
+    const int c = c0 + blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= c1) return;
     double *col = B + (size_t)c * ldb;
-    for (int jj = 0; jj < nb; jj++) {
-        int j = k0 + jj, p = pv[jj];
-        if (p != j) { double t = col[j]; col[j] = col[p]; col[p] = t; }
-    }
+    const int ne = nS - nb;
     double x[kPB];
-    col += k0;
+#pragma unroll
+    for (int r = 0; r < kPB; r++)
+        if (r < nb) x[r] = col[src[r]];
+    for (int e = 0; e < ne; e++) ext[e][threadIdx.x] = col[src[nb + e]];
 #pragma unroll
     for (int r = 0; r < kPB; r++) {
         if (r < nb) {
-            double v = col[r];
-            for (int s = 0; s < r; s++) v -= L[r][s] * x[s];
+            double v = x[r];
+#pragma unroll
+            for (int s = 0; s < kPB; s++)
+                if (s < r) v -= L[r][s] * x[s];
             x[r] = v;
         }
     }
 #pragma unroll
     for (int r = 0; r < kPB; r++)
-        if (r < nb) col[r] = x[r];
+        if (r < nb) col[k0 + r] = x[r];
+    for (int e = 0; e < ne; e++) col[S[nb + e]] = ext[e][threadIdx.x];
 }
 
 // B[k0:k0+nb, c] = U11^-1 B[k0:k0+nb, c] (non-unit upper) for c in [c0, c1).
 __global__ void k_trsm_upper(const double *A, int lda, int k0, int nb, double *B, int ldb, int c0, int c1)
 {
     __shared__ double U[kPB][kPB + 1];
+    __shared__ double Ur[kPB];  // reciprocals of the diagonal
     for (int t = threadIdx.x; t < nb * nb; t += blockDim.x) {
         int r = t % nb, s = t / nb;
         U[r][s] = A[(size_t)(k0 + s) * lda + k0 + r];
     }
+    __syncthreads();
+    if (threadIdx.x < nb) Ur[threadIdx.x] = 1.0 / U[threadIdx.x][threadIdx.x];
     __syncthreads();
     int c = c0 + blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= c1) return;
@@ -226,7 +277,7 @@ __global__ void k_trsm_upper(const double *A, int lda, int k0, int nb, double *B
 #pragma unroll
             for (int s = r + 1; s < kPB; s++)
                 if (s < nb) v -= U[r][s] * x[s];
-            x[r] = v / U[r][r];
+            x[r] = v * Ur[r];
         }
     }
 #pragma unroll
@@ -297,36 +348,82 @@ static void dgemm_sub(cudaStream_t st, int m, int nn, int kk, const double *A, i
 
 static bool smem_panel_ready = false;
 
+// Diagnostic per-kernel-type device times of the LU (environment variable
+// P2CUDA_LU_TIMING=1): every launch is bracketed by events and waited for, so
+// the totals are exact per kernel but the run itself is slower.
+struct LuTimer {
+    bool on = false;
+    cudaEvent_t a = nullptr, b = nullptr;
+    double ms[4] = {0, 0, 0, 0};  // panel, lower TRSM, GEMM, upper TRSM
+    int cnt[4] = {0, 0, 0, 0};
+    cudaStream_t st = nullptr;
+    void begin()
+    {
+        if (on) cudaEventRecord(a, st);
+    }
+    void end(int kind)
+    {
+        if (!on) return;
+        cudaEventRecord(b, st);
+        cudaEventSynchronize(b);
+        float t = 0;
+        cudaEventElapsedTime(&t, a, b);
+        ms[kind] += t;
+        cnt[kind]++;
+    }
+};
+
 // Factor the banded A (n x n, column-major, lower/upper half-bandwidths kl,
 // ku) in place and write its inverse into Ainv.  Returns 0 or the first
-// zero-pivot column + 1.
-int band_lu_inverse(cudaStream_t st, double *A, int n, int kl, int ku, double *Ainv, int *d_ipiv, int *d_info)
+// zero-pivot column + 1.  marks (optional, 2 events) are recorded after the
+// factorisation and after the forward half of the inverse.
+int band_lu_inverse(cudaStream_t st, double *A, int n, int kl, int ku, double *Ainv, int *d_ipiv, int *d_info,
+                    cudaEvent_t *marks)
 {
     kl = std::max(0, std::min(kl, n - 1));
     ku = std::max(0, std::min(ku, n - 1));
     const bool smem = kPB + kl <= kMaxPanelRows;
     if (smem && !smem_panel_ready) {
-        P2_CUDA_TRY(cudaFuncSetAttribute(k_panel_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxPanelBytes));
+        P2_CUDA_TRY(cudaFuncSetAttribute(k_panel_track, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxPanelBytes));
         smem_panel_ready = true;
     }
     P2_CUDA_TRY(cudaMemsetAsync(d_info, 0, sizeof(int), st));
+    LuTimer T;
+    {
+        const char *e = std::getenv("P2CUDA_LU_TIMING");
+        T.on = e && e[0] == '1';
+        T.st = st;
+        if (T.on) {
+            P2_CUDA_TRY(cudaEventCreate(&T.a));
+            P2_CUDA_TRY(cudaEventCreate(&T.b));
+        }
+    }
     for (int k0 = 0; k0 < n; k0 += kPB) {
         const int nb = std::min(kPB, n - k0);
         const int r1 = std::min(n, k0 + nb + kl);
         const int c1 = std::min(n, r1 + ku);
         if (smem) {
             size_t bytes = sizeof(double) * (size_t)(r1 - k0) * nb;
-            k_panel_smem<<<1, kPanelThreads, bytes, st>>>(A, n, k0, nb, r1, d_ipiv, d_info); P2_COUNT_LAUNCH();
+            const int thr = ((r1 - k0) + 31) / 32 * 32;  // one thread per panel row
+            T.begin();
+            k_panel_track<<<1, thr, bytes, st>>>(A, n, k0, nb, r1, d_ipiv, d_info); P2_COUNT_LAUNCH();
+            T.end(0);
         } else {
             k_panel_global<<<1, 1024, 0, st>>>(A, n, k0, nb, r1, d_ipiv, d_info); P2_COUNT_LAUNCH();
         }
         const int cb = k0 + nb;
         if (c1 > cb) {
-            k_swap_trsm_lower<<<(c1 - cb + 127) / 128, 128, 0, st>>>(A, n, k0, nb, d_ipiv, A, n, cb, c1); P2_COUNT_LAUNCH();
+            T.begin();
+            k_perm_trsm_lower<<<(c1 - cb + kTrsmThreads - 1) / kTrsmThreads, kTrsmThreads, 0, st>>>(
+                A, n, k0, nb, d_ipiv, A, n, cb, c1); P2_COUNT_LAUNCH();
+            T.end(1);
+            T.begin();
             dgemm_sub(st, r1 - cb, c1 - cb, nb, A + (size_t)k0 * n + cb, n, A + (size_t)cb * n + k0, n,
                       A + (size_t)cb * n + cb, n);
+            T.end(2);
         }
     }
+    if (marks) P2_CUDA_TRY(cudaEventRecord(marks[0], st));
     // forward: replay (P_k, L_k) on the identity; rows [k0, r1) of the partial
     // product only have non-zeros in columns [0, r1)
     P2_CUDA_TRY(cudaMemsetAsync(Ainv, 0, sizeof(double) * (size_t)n * n, st));
@@ -334,20 +431,37 @@ int band_lu_inverse(cudaStream_t st, double *A, int n, int kl, int ku, double *A
     for (int k0 = 0; k0 < n; k0 += kPB) {
         const int nb = std::min(kPB, n - k0);
         const int r1 = std::min(n, k0 + nb + kl);
-        k_swap_trsm_lower<<<(r1 + 127) / 128, 128, 0, st>>>(A, n, k0, nb, d_ipiv, Ainv, n, 0, r1); P2_COUNT_LAUNCH();
+        T.begin();
+        k_perm_trsm_lower<<<(r1 + kTrsmThreads - 1) / kTrsmThreads, kTrsmThreads, 0, st>>>(A, n, k0, nb, d_ipiv, Ainv,
+                                                                                         n, 0, r1); P2_COUNT_LAUNCH();
+        T.end(1);
         const int cb = k0 + nb;
+        T.begin();
         if (r1 > cb) dgemm_sub(st, r1 - cb, r1, nb, A + (size_t)k0 * n + cb, n, Ainv + k0, n, Ainv + cb, n);
+        T.end(2);
     }
+    if (marks) P2_CUDA_TRY(cudaEventRecord(marks[1], st));
     // backward: U X = Y with U's band (kl + ku above the diagonal)
     const int kuu = std::min(n - 1, kl + ku);
     const int last = ((n - 1) / kPB) * kPB;
     for (int k0 = last; k0 >= 0; k0 -= kPB) {
         const int nb = std::min(kPB, n - k0);
+        T.begin();
         k_trsm_upper<<<(n + 127) / 128, 128, 0, st>>>(A, n, k0, nb, Ainv, n, 0, n); P2_COUNT_LAUNCH();
+        T.end(3);
         const int a = std::max(0, k0 - kuu);
+        T.begin();
         if (k0 > a) dgemm_sub(st, k0 - a, n, nb, A + (size_t)k0 * n + a, n, Ainv + k0, n, Ainv + a, n);
+        T.end(2);
     }
     P2_CUDA_TRY(cudaGetLastError());
+    if (T.on) {
+        std::fprintf(stderr, "p2cuda LU timing: panel %.3f ms (%d), lower TRSM %.3f ms (%d), GEMM %.3f ms (%d), "
+                     "upper TRSM %.3f ms (%d)\n", T.ms[0], T.cnt[0], T.ms[1], T.cnt[1], T.ms[2], T.cnt[2], T.ms[3],
+                     T.cnt[3]);
+        cudaEventDestroy(T.a);
+        cudaEventDestroy(T.b);
+    }
     int info = 0;
     P2_CUDA_TRY(cudaMemcpyAsync(&info, d_info, sizeof(int), cudaMemcpyDeviceToHost, st));
     P2_CUDA_TRY(cudaStreamSynchronize(st));

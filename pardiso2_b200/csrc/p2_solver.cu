@@ -26,7 +26,8 @@
 namespace p2 {
 
 constexpr int kProbes = 4 * 125;  // coarsest-operator probes: 125 colour classes x 4 components
-int band_lu_inverse(cudaStream_t st, double *A, int n, int kl, int ku, double *Ainv, int *d_ipiv, int *d_info);
+int band_lu_inverse(cudaStream_t st, double *A, int n, int kl, int ku, double *Ainv, int *d_ipiv, int *d_info,
+                    cudaEvent_t *marks);
 void d2f(cudaStream_t st, size_t n, const double *a, float *b);
 
 static inline unsigned nblk(long n, int t = kThreads) { return (unsigned)((n + t - 1) / t); }
@@ -671,7 +672,16 @@ void Solver::coarse_setup()
     P2_CUDA_TRY(cudaGetLastError());
     P2_CUDA_TRY(cudaMemcpyAsync(h_bw, d_bw, sizeof(int) * 2, cudaMemcpyDeviceToHost, st));
     P2_CUDA_TRY(cudaStreamSynchronize(st));
-    int info = band_lu_inverse(st, A_c, nF, h_bw[0], h_bw[1], Ainv64, d_ipiv, d_info);
+    if (verbose) P2_CUDA_TRY(cudaEventRecord(ev[5], st));
+    int info = band_lu_inverse(st, A_c, nF, h_bw[0], h_bw[1], Ainv64, d_ipiv, d_info, verbose ? ev + 6 : nullptr);
+    if (verbose) {
+        float t0 = 0, t1 = 0, t2 = 0;
+        P2_CUDA_TRY(cudaEventElapsedTime(&t0, ev[0], ev[5]));
+        P2_CUDA_TRY(cudaEventElapsedTime(&t1, ev[5], ev[6]));
+        P2_CUDA_TRY(cudaEventElapsedTime(&t2, ev[6], ev[7]));
+        std::fprintf(stderr, "p2cuda: coarsest nF %d band kl %d ku %d; node fields + probing %.3f ms, "
+                     "factorisation %.3f ms, inverse (forward) %.3f ms\n", nF, h_bw[0], h_bw[1], t0, t1, t2);
+    }
     if (info) throw Error(P2_ERR_SINGULAR, "zero pivot in the coarsest LU at column " + std::to_string(info));
     d2f(st, (size_t)nF * nF, Ainv64, Ainv32);
 }
@@ -733,11 +743,12 @@ void Solver::smooth(int l, int sweeps)
     // pressure is updated in place in x.c[0] (yy shares it)
     Vec4<T> yy = y;
     yy.c[0] = x.c[0];
-    const bool full = prm.smoother != 0;
     for (int s = 0; s < sweeps; s++) {
         for (int col = 0; col < 2; col++) {
             Vec4<T> &vin = col ? yy : x, &vout = col ? x : yy;
-            if (full) {
+            if (prm.smoother == 1) {
+                k_vanka_fast<T><<<nblk(cells, 128), 128, 0, st>>>(V, x.c[0], vin, vout, b, om, col); P2_COUNT_LAUNCH();
+            } else if (prm.smoother == 2) {
                 k_vanka_full<T><<<nblk(cells, 128), 128, 0, st>>>(V, x.c[0], vin, vout, b, om, col); P2_COUNT_LAUNCH();
             } else {
                 k_vanka<T><<<nblk(cells), kThreads, 0, st>>>(V, x.c[0], vin, vout, b, om, col); P2_COUNT_LAUNCH();
@@ -910,6 +921,13 @@ p2_solve_info Solver::solve()
     set_nodes_device();
     coarse_setup();
     P2_CUDA_TRY(cudaEventRecord(ev[1], st));
+    if (verbose) {
+        float tb = 0;
+        P2_CUDA_TRY(cudaEventSynchronize(ev[1]));
+        P2_CUDA_TRY(cudaEventElapsedTime(&tb, ev[7], ev[1]));
+        std::fprintf(stderr, "p2cuda: inverse (backward) + FP32 copy %.3f ms; V-cycle graph %lld kernels\n", tb,
+                     graphs[prm.precision == 0 ? 0 : 1].kernels);
+    }
     // b-norm of the pinned system: every row but the pin cell's, plus the pin value
     DotJobs J{};
     J.j[0] = job(gb, gb);
@@ -1196,7 +1214,10 @@ double Solver::debug_time_smoother(int l, int passes)
         Vec4<float> x = Lv.x32, y = Lv.y32;
         y.c[0] = x.c[0];
         for (int p = 0; p < passes; p++) {
-            if (prm.smoother)
+            if (prm.smoother == 1)
+                k_vanka_fast<float><<<nblk(cells, 128), 128, 0, st>>>(V, x.c[0], (p & 1) ? y : x, (p & 1) ? x : y,
+                                                                      Lv.b32, (float)prm.omega, p & 1);
+            else if (prm.smoother == 2)
                 k_vanka_full<float><<<nblk(cells, 128), 128, 0, st>>>(V, x.c[0], (p & 1) ? y : x, (p & 1) ? x : y,
                                                                       Lv.b32, (float)prm.omega, p & 1);
             else
@@ -1208,7 +1229,10 @@ double Solver::debug_time_smoother(int l, int passes)
         Vec4<double> x = Lv.x64, y = Lv.y64;
         y.c[0] = x.c[0];
         for (int p = 0; p < passes; p++) {
-            if (prm.smoother)
+            if (prm.smoother == 1)
+                k_vanka_fast<double><<<nblk(cells, 128), 128, 0, st>>>(V, x.c[0], (p & 1) ? y : x, (p & 1) ? x : y,
+                                                                       Lv.b64, prm.omega, p & 1);
+            else if (prm.smoother == 2)
                 k_vanka_full<double><<<nblk(cells, 128), 128, 0, st>>>(V, x.c[0], (p & 1) ? y : x, (p & 1) ? x : y,
                                                                        Lv.b64, prm.omega, p & 1);
             else

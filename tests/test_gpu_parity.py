@@ -90,9 +90,9 @@ def test_solve_vs_reference_solution(gcase, precision):
         assert rel(sol[k], g["sol_" + k]) < 1e-6, (k, rel(sol[k], g["sol_" + k]))
 
 
-@pytest.mark.parametrize("smoother", [0, 1])
-def test_both_smoothers_reach_the_reference_solution(gcase, smoother):
-    """Diagonal and full cell-block smoothers are preconditioners only: both
+@pytest.mark.parametrize("smoother", [0, 1, 2])
+def test_every_smoother_reaches_the_reference_solution(gcase, smoother):
+    """Diagonal and full cell-block smoothers are preconditioners only: all
     converge to the same discrete solution."""
     m, g, _ = gcase
     prob = P.StokesProblem(m, tol=1e-8, smoother=smoother, sweep_growth=2)
@@ -102,6 +102,25 @@ def test_both_smoothers_reach_the_reference_solution(gcase, smoother):
     assert info.status == 0 and info.rel_residual <= 1e-8
     for k in ("vx", "vy", "vz", "pr"):
         assert rel(sol[k], g["sol_" + k]) < 1e-6, (k, rel(sol[k], g["sol_" + k]))
+
+
+def test_shared_stress_smoother_matches_row_by_row(gcase):
+    """The full cell-block smoother assembles its residuals from shared
+    stresses (smoother 1) or row by row (smoother 2): the same iteration in
+    FP32 up to rounding, so the outer iterations agree."""
+    m, g, _ = gcase
+    its, sols = [], []
+    for sm in (1, 2):
+        prob = P.StokesProblem(m, tol=1e-8, smoother=sm)
+        prob.set_nodes({k: g["node_" + k] for k in FIELDS})
+        sol, info = prob.solve_fp64()
+        prob.close()
+        assert info.status == 0
+        its.append(info.iterations)
+        sols.append(sol)
+    assert abs(its[0] - its[1]) <= 1, its
+    for k in ("vx", "vy", "vz", "pr"):
+        assert rel(sols[0][k], sols[1][k]) < 1e-6, k
 
 
 def test_autotune_choice_reaches_the_reference_solution(gcase):
