@@ -29,6 +29,15 @@ namespace p2 {
 // Kernels launched by this library on the calling host thread (a graph
 // launch adds the number of kernel nodes it replays).
 extern thread_local long long g_launches;
+
+// Replayable launch sequence of the coarsest LU and inverse (p2_lu.cu).
+struct LuGraph {
+    cudaGraphExec_t exec = nullptr;
+    int n = 0, kl = -1, ku = -1;
+    const double *A = nullptr, *Ainv = nullptr;
+    const int *ipiv = nullptr, *info = nullptr;
+    long long kernels = 0;
+};
 #define P2_COUNT_LAUNCH() (++p2::g_launches)
 
 struct Error {

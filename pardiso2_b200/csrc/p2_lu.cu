@@ -377,27 +377,11 @@ struct LuTimer {
 // ku) in place and write its inverse into Ainv.  Returns 0 or the first
 // zero-pivot column + 1.  marks (optional, 2 events) are recorded after the
 // factorisation and after the forward half of the inverse.
-int band_lu_inverse(cudaStream_t st, double *A, int n, int kl, int ku, double *Ainv, int *d_ipiv, int *d_info,
-                    cudaEvent_t *marks)
+static void lu_issue(cudaStream_t st, double *A, int n, int kl, int ku, double *Ainv, int *d_ipiv, int *d_info,
+                     cudaEvent_t *marks, LuTimer &T)
 {
-    kl = std::max(0, std::min(kl, n - 1));
-    ku = std::max(0, std::min(ku, n - 1));
     const bool smem = kPB + kl <= kMaxPanelRows;
-    if (smem && !smem_panel_ready) {
-        P2_CUDA_TRY(cudaFuncSetAttribute(k_panel_track, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxPanelBytes));
-        smem_panel_ready = true;
-    }
     P2_CUDA_TRY(cudaMemsetAsync(d_info, 0, sizeof(int), st));
-    LuTimer T;
-    {
-        const char *e = std::getenv("P2CUDA_LU_TIMING");
-        T.on = e && e[0] == '1';
-        T.st = st;
-        if (T.on) {
-            P2_CUDA_TRY(cudaEventCreate(&T.a));
-            P2_CUDA_TRY(cudaEventCreate(&T.b));
-        }
-    }
     for (int k0 = 0; k0 < n; k0 += kPB) {
         const int nb = std::min(kPB, n - k0);
         const int r1 = std::min(n, k0 + nb + kl);
@@ -455,6 +439,53 @@ int band_lu_inverse(cudaStream_t st, double *A, int n, int kl, int ku, double *A
         T.end(2);
     }
     P2_CUDA_TRY(cudaGetLastError());
+}
+
+int band_lu_inverse(cudaStream_t st, double *A, int n, int kl, int ku, double *Ainv, int *d_ipiv, int *d_info,
+                    cudaEvent_t *marks, LuGraph *cache)
+{
+    kl = std::max(0, std::min(kl, n - 1));
+    ku = std::max(0, std::min(ku, n - 1));
+    if (kPB + kl <= kMaxPanelRows && !smem_panel_ready) {
+        P2_CUDA_TRY(cudaFuncSetAttribute(k_panel_track, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxPanelBytes));
+        smem_panel_ready = true;
+    }
+    LuTimer T;
+    {
+        const char *e = std::getenv("P2CUDA_LU_TIMING");
+        T.on = e && e[0] == '1';
+        T.st = st;
+        if (T.on) {
+            P2_CUDA_TRY(cudaEventCreate(&T.a));
+            P2_CUDA_TRY(cudaEventCreate(&T.b));
+        }
+    }
+    if (cache && !T.on && !marks) {
+        // the ~800 dependent launches replayed as one graph; captured again
+        // only when the size, the band or the buffers change
+        const bool hit = cache->exec && cache->n == n && cache->kl == kl && cache->ku == ku && cache->A == A &&
+                         cache->Ainv == Ainv && cache->ipiv == d_ipiv && cache->info == d_info;
+        if (!hit) {
+            if (cache->exec) cudaGraphExecDestroy(cache->exec);
+            cache->exec = nullptr;
+            cudaGraph_t graph;
+            long long before = g_launches;
+            P2_CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+            lu_issue(st, A, n, kl, ku, Ainv, d_ipiv, d_info, nullptr, T);
+            P2_CUDA_TRY(cudaStreamEndCapture(st, &graph));
+            cache->kernels = g_launches - before;
+            g_launches = before;
+            cudaError_t e = cudaGraphInstantiate(&cache->exec, graph, 0);
+            cudaGraphDestroy(graph);
+            P2_CUDA_TRY(e);
+            cache->n = n; cache->kl = kl; cache->ku = ku; cache->A = A; cache->Ainv = Ainv;
+            cache->ipiv = d_ipiv; cache->info = d_info;
+        }
+        P2_CUDA_TRY(cudaGraphLaunch(cache->exec, st));
+        g_launches += cache->kernels;
+    } else {
+        lu_issue(st, A, n, kl, ku, Ainv, d_ipiv, d_info, marks, T);
+    }
     if (T.on) {
         std::fprintf(stderr, "p2cuda LU timing: panel %.3f ms (%d), lower TRSM %.3f ms (%d), GEMM %.3f ms (%d), "
                      "upper TRSM %.3f ms (%d)\n", T.ms[0], T.cnt[0], T.ms[1], T.cnt[1], T.ms[2], T.cnt[2], T.ms[3],

@@ -27,7 +27,7 @@ namespace p2 {
 
 constexpr int kProbes = 4 * 125;  // coarsest-operator probes: 125 colour classes x 4 components
 int band_lu_inverse(cudaStream_t st, double *A, int n, int kl, int ku, double *Ainv, int *d_ipiv, int *d_info,
-                    cudaEvent_t *marks);
+                    cudaEvent_t *marks, LuGraph *cache);
 void d2f(cudaStream_t st, size_t n, const double *a, float *b);
 
 static inline unsigned nblk(long n, int t = kThreads) { return (unsigned)((n + t - 1) / t); }
@@ -169,6 +169,7 @@ Solver::~Solver()
 {
     cudaSetDevice(dev);
     drop_graphs();
+    if (lu_graph.exec) cudaGraphExecDestroy(lu_graph.exec);
     arena.release();
     grid_arena.release();
     marker_arena.release();
@@ -673,7 +674,8 @@ void Solver::coarse_setup()
     P2_CUDA_TRY(cudaMemcpyAsync(h_bw, d_bw, sizeof(int) * 2, cudaMemcpyDeviceToHost, st));
     P2_CUDA_TRY(cudaStreamSynchronize(st));
     if (verbose) P2_CUDA_TRY(cudaEventRecord(ev[5], st));
-    int info = band_lu_inverse(st, A_c, nF, h_bw[0], h_bw[1], Ainv64, d_ipiv, d_info, verbose ? ev + 6 : nullptr);
+    int info = band_lu_inverse(st, A_c, nF, h_bw[0], h_bw[1], Ainv64, d_ipiv, d_info, verbose ? ev + 6 : nullptr,
+                               &lu_graph);
     if (verbose) {
         float t0 = 0, t1 = 0, t2 = 0;
         P2_CUDA_TRY(cudaEventElapsedTime(&t0, ev[0], ev[5]));

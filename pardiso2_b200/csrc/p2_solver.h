@@ -136,6 +136,7 @@ class Solver {
 
     DeviceArena arena, grid_arena, marker_arena;
     std::array<GraphSlot, 2> graphs;
+    LuGraph lu_graph;  // coarsest LU + inverse launch sequence
     int restart = 8;
     Vec4<double> gx, gb, gr;
     std::vector<Vec4<double>> Z, Q;
