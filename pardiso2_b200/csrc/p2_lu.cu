@@ -9,8 +9,8 @@
 // factorisation is the right-looking blocked LU of LAPACK's gbtrf, restricted
 // to the band and kept in dense column-major storage:
 //   per panel of kPB columns at k0 (rows [k0, r1), r1 = k0 + kPB + kl):
-//     1. factor the panel in shared memory (pivot = largest |a|, smallest row
-//        on ties), row interchanges applied inside the panel only;
+//     1. factor the panel in registers or shared memory (pivot = largest |a|,
+//        smallest row on ties), row interchanges applied inside the panel only;
 //     2. apply the interchanges to the columns [k0 + kPB, c1) (c1 = r1 + ku,
 //        the reach of U after pivoting) and solve U12 = L11^-1 A12;
 //     3. A22 -= L21 U12 on rows [k0 + kPB, r1) x columns [k0 + kPB, c1).
@@ -115,6 +115,98 @@ __global__ void __launch_bounds__(kTrackThreads) k_panel_track(double *A, int ld
     }
 }
 
+// The same panel factorisation with each row held in the registers of one
+// thread (the column loop fully unrolled, so every index is static), for
+// panels of at most kRegPanelRows rows.  Per column one barrier: every warp
+// reduces its candidates with shuffles and the winning lane of each warp
+// writes its whole row to shared memory; after the barrier every thread picks
+// the overall winner from the per-warp candidates and eliminates against the
+// copy of the pivot row.  Pivot choice (largest |a|, lowest row on ties), the
+// rebuilt interchange sequence and the output are those of k_panel_track.
+constexpr int kRegPanelRows = 640;
+
+__global__ void __launch_bounds__(kRegPanelRows) k_panel_reg(double *A, int lda, int k0, int r1, int *ipiv,
+                                                             int *info)
+{
+    __shared__ double cand[kRegPanelRows / 32][2][kPB];  // per-warp candidate row, double-buffered by column parity
+    __shared__ double cval[kRegPanelRows / 32][2];
+    __shared__ int cidx[kRegPanelRows / 32][2];
+    __shared__ int prow[kPB];
+    __shared__ int lmap[kRegPanelRows], linv[kRegPanelRows];
+    const int m = r1 - k0;
+    const int row = threadIdx.x, lane = row & 31, w = row >> 5, nw = blockDim.x >> 5;
+    double v[kPB];
+#pragma unroll
+    for (int c = 0; c < kPB; c++) v[c] = row < m ? A[(size_t)(k0 + c) * lda + k0 + row] : 0.0;
+    bool live = row < m;
+#pragma unroll
+    for (int jj = 0; jj < kPB; jj++) {
+        const int buf = jj & 1;
+        double best = live ? fabs(v[jj]) : -1.0;
+        int bi = live ? row : 0x7fffffff;
+        for (int o = 16; o > 0; o >>= 1) {
+            double ov = __shfl_xor_sync(0xffffffffu, best, o);
+            int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+            if (ov > best || (ov == best && oi < bi)) { best = ov; bi = oi; }
+        }
+        if (row == bi) {  // this warp's candidate publishes its row
+            cval[w][buf] = best;
+            cidx[w][buf] = bi;
+#pragma unroll
+            for (int c = 0; c < kPB; c++)
+                if (c >= jj) cand[w][buf][c] = v[c];
+        }
+        if (lane == 0 && bi == 0x7fffffff) {  // warp without live rows
+            cval[w][buf] = -1.0;
+            cidx[w][buf] = 0x7fffffff;
+        }
+        __syncthreads();
+        double gb = lane < nw ? cval[lane][buf] : -1.0;
+        int gi = lane < nw ? cidx[lane][buf] : 0x7fffffff;
+        int gw = lane;
+        for (int o = 16; o > 0; o >>= 1) {
+            double ov = __shfl_xor_sync(0xffffffffu, gb, o);
+            int oi = __shfl_xor_sync(0xffffffffu, gi, o);
+            int ow = __shfl_xor_sync(0xffffffffu, gw, o);
+            if (ov > gb || (ov == gb && oi < gi)) { gb = ov; gi = oi; gw = ow; }
+        }
+        const int p = gi;
+        if (row == 0) {
+            prow[jj] = p;
+            if (!(gb > 0.0) && *info == 0) *info = k0 + jj + 1;
+        }
+        const double pv = cand[gw][buf][jj];
+        const double inv = pv != 0.0 ? 1.0 / pv : 0.0;
+        if (row == p) live = false;
+        if (live) {
+            const double l = v[jj] * inv;
+            v[jj] = l;
+#pragma unroll
+            for (int c = jj + 1; c < kPB; c++) v[c] -= l * cand[gw][buf][c];
+        }
+        // the next column writes the other buffer, so one barrier per column suffices
+    }
+    // interchange sequence and final row order (as k_panel_track)
+    for (int r = threadIdx.x; r < m; r += blockDim.x) { lmap[r] = r; linv[r] = r; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int jj = 0; jj < kPB; jj++) {
+            const int p = prow[jj], q = linv[p];
+            ipiv[k0 + jj] = k0 + q;
+            const int a = lmap[jj];
+            lmap[jj] = p; linv[p] = jj;
+            lmap[q] = a;  linv[a] = q;
+        }
+    }
+    __syncthreads();
+    // rows go back to their final positions: the destination of physical row r is linv[r]
+    if (row < m) {
+        const int dst = linv[row];
+#pragma unroll
+        for (int c = 0; c < kPB; c++) A[(size_t)(k0 + c) * lda + k0 + dst] = v[c];
+    }
+}
+
 // Same factorisation in global memory, one block, for bands too wide for the
 // shared-memory panel.
 __global__ void k_panel_global(double *A, int lda, int k0, int nb, int r1, int *ipiv, int *info)
@@ -180,27 +272,31 @@ __global__ void k_panel_global(double *A, int lda, int k0, int nb, int r1, int *
     }
 }
 
-// For columns c in [c0, c1) of B: apply the panel's interchanges (rows k0..)
-// then B[k0:k0+nb, c] = L11^-1 B[k0:k0+nb, c], L11 unit lower from A.  The
-// interchange sequence is turned into one permutation first: warp 0 replays the nb swaps on the set of rows they touch
-// (rows k0..k0+nb and the pivot rows below, at most 2 nb), recording for each
-// slot the row whose value ends there.  Each thread then loads its column's
-// values for the whole set at once (independent loads instead of a chain of
-// dependent swaps), solves with L11 and stores the set back.
-constexpr int kTrsmThreads = 128;
+// Triangular solves on the columns c in [c0, c1) of B, one warp per column:
+//   lower: apply the panel's interchanges (rows k0..) to the column, then
+//          B[k0:k0+nb, c] = L11^-1 B[k0:k0+nb, c], L11 unit lower from A;
+//   upper: B[k0:k0+nb, c] = U11^-1 B[k0:k0+nb, c], U11 non-unit upper from A.
+// Lane r owns row k0 + r; the solved value of each row is broadcast with a
+// shuffle and the lanes below (lower) or above (upper) subtract its multiple.
+// The interchange sequence is first turned into one permutation: warp 0
+// replays the nb swaps on the set of rows they touch (rows k0..k0+nb and the
+// pivot rows below, at most 2 nb), recording for each slot the row whose
+// value ends there; every column then gathers that set with independent
+// loads, solves, and stores the set back.  kTrsmWarps columns per block.
+constexpr int kTrsmWarps = 8;
 
-__global__ void __launch_bounds__(kTrsmThreads) k_perm_trsm_lower(const double *A, int lda, int k0, int nb,
-                                                                  const int *ipiv, double *B, int ldb, int c0, int c1)
+__global__ void __launch_bounds__(32 * kTrsmWarps) k_perm_trsm_lower_w(const double *A, int lda, int k0, int nb,
+                                                                       const int *ipiv, double *B, int ldb, int c0,
+                                                                       int c1)
 {
     __shared__ double L[kPB][kPB + 1];
     __shared__ int S[2 * kPB], src[2 * kPB];
     __shared__ int nS;
-    __shared__ double ext[kPB][kTrsmThreads];
     for (int t = threadIdx.x; t < nb * nb; t += blockDim.x) {
         int r = t % nb, s = t / nb;
         L[r][s] = A[(size_t)(k0 + s) * lda + k0 + r];
     }
-    if (threadIdx.x < 32) {
+    if (threadIdx.x < 32) {  // the panel's interchanges as one permutation
         const int lane = threadIdx.x;
         int cnt = nb;
         if (lane < nb) { S[lane] = k0 + lane; src[lane] = k0 + lane; }
@@ -229,36 +325,29 @@ __global__ void __launch_bounds__(kTrsmThreads) k_perm_trsm_lower(const double *
         if (lane == 0) nS = cnt;
     }
     __syncthreads();
-    const int c = c0 + blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    const int c = c0 + blockIdx.x * kTrsmWarps + (threadIdx.x >> 5);
     if (c >= c1) return;
     double *col = B + (size_t)c * ldb;
     const int ne = nS - nb;
-    double x[kPB];
-#pragma unroll
-    for (int r = 0; r < kPB; r++)
-        if (r < nb) x[r] = col[src[r]];
-    for (int e = 0; e < ne; e++) ext[e][threadIdx.x] = col[src[nb + e]];
-#pragma unroll
-    for (int r = 0; r < kPB; r++) {
-        if (r < nb) {
-            double v = x[r];
-#pragma unroll
-            for (int s = 0; s < kPB; s++)
-                if (s < r) v -= L[r][s] * x[s];
-            x[r] = v;
-        }
+    // gather everything the permutation moves before writing any of it
+    double x = lane < nb ? col[src[lane]] : 0.0;
+    double e = lane < ne ? col[src[nb + lane]] : 0.0;
+    for (int r = 0; r < nb; r++) {
+        const double xr = __shfl_sync(0xffffffffu, x, r);
+        if (lane > r && lane < nb) x -= L[lane][r] * xr;
     }
-#pragma unroll
-    for (int r = 0; r < kPB; r++)
-        if (r < nb) col[k0 + r] = x[r];
-    for (int e = 0; e < ne; e++) col[S[nb + e]] = ext[e][threadIdx.x];
+    e = __shfl_sync(0xffffffffu, e, lane);  // consumes every gathered value before the first store
+    __syncwarp();
+    if (lane < nb) col[k0 + lane] = x;
+    if (lane < ne) col[S[nb + lane]] = e;
 }
 
-// B[k0:k0+nb, c] = U11^-1 B[k0:k0+nb, c] (non-unit upper) for c in [c0, c1).
-__global__ void k_trsm_upper(const double *A, int lda, int k0, int nb, double *B, int ldb, int c0, int c1)
+__global__ void __launch_bounds__(32 * kTrsmWarps) k_trsm_upper_w(const double *A, int lda, int k0, int nb, double *B,
+                                                                  int ldb, int c0, int c1)
 {
     __shared__ double U[kPB][kPB + 1];
-    __shared__ double Ur[kPB];  // reciprocals of the diagonal
+    __shared__ double Ur[kPB];
     for (int t = threadIdx.x; t < nb * nb; t += blockDim.x) {
         int r = t % nb, s = t / nb;
         U[r][s] = A[(size_t)(k0 + s) * lda + k0 + r];
@@ -266,23 +355,17 @@ __global__ void k_trsm_upper(const double *A, int lda, int k0, int nb, double *B
     __syncthreads();
     if (threadIdx.x < nb) Ur[threadIdx.x] = 1.0 / U[threadIdx.x][threadIdx.x];
     __syncthreads();
-    int c = c0 + blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    const int c = c0 + blockIdx.x * kTrsmWarps + (threadIdx.x >> 5);
     if (c >= c1) return;
-    double x[kPB];
     double *col = B + (size_t)c * ldb + k0;
-#pragma unroll
-    for (int r = kPB - 1; r >= 0; r--) {
-        if (r < nb) {
-            double v = col[r];
-#pragma unroll
-            for (int s = r + 1; s < kPB; s++)
-                if (s < nb) v -= U[r][s] * x[s];
-            x[r] = v * Ur[r];
-        }
+    double x = lane < nb ? col[lane] : 0.0;
+    for (int r = nb - 1; r >= 0; r--) {
+        if (lane == r) x *= Ur[r];
+        const double xr = __shfl_sync(0xffffffffu, x, r);
+        if (lane < r) x -= U[lane][r] * xr;
     }
-#pragma unroll
-    for (int r = 0; r < kPB; r++)
-        if (r < nb) col[r] = x[r];
+    if (lane < nb) col[lane] = x;
 }
 
 // C[m x nn] -= A[m x kk] * B[kk x nn], column-major, FP64.  64x64 tile per
@@ -338,10 +421,78 @@ __global__ void k_d2f(size_t n, const double *a, float *b)
     if (i < n) b[i] = (float)a[i];
 }
 
+// C[m x nn] -= A[m x kk] * B[kk x nn] for kk <= kPB (every update of the
+// blocked LU has kk = panel width): the whole kk slab of A and B in shared
+// memory with one barrier, the block's C values fetched into registers before
+// the products so their latency overlaps the tile loads.  TM x TN tile per
+// block of 256 threads (16 x 16 grid, TM/16 x TN/16 outputs per thread).
+template <int TM, int TN>
+__global__ void __launch_bounds__(256) k_dgemm_k32(int m, int nn, int kk, const double *A, int lda, const double *B,
+                                                   int ldb, double *C, int ldc)
+{
+    constexpr int RM = TM / 16, RN = TN / 16;
+    __shared__ double As[kPB][TM + 1];
+    __shared__ double Bs[kPB][TN + 1];
+    const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+    const int row0 = blockIdx.x * TM, col0 = blockIdx.y * TN;
+    double cv[RM][RN];
+#pragma unroll
+    for (int q = 0; q < RM; q++)
+#pragma unroll
+        for (int r = 0; r < RN; r++) {
+            const int gr = row0 + tx + 16 * q, gc = col0 + ty + 16 * r;
+            cv[q][r] = (gr < m && gc < nn) ? C[(size_t)gc * ldc + gr] : 0.0;
+        }
+    for (int t = threadIdx.x; t < kPB * TM; t += 256) {
+        const int r = t % TM, s = t / TM;
+        As[s][r] = (row0 + r < m && s < kk) ? A[(size_t)s * lda + row0 + r] : 0.0;
+    }
+    for (int t = threadIdx.x; t < kPB * TN; t += 256) {
+        const int kc = t % kPB, cc = t / kPB;
+        Bs[kc][cc] = (kc < kk && col0 + cc < nn) ? B[(size_t)(col0 + cc) * ldb + kc] : 0.0;
+    }
+    __syncthreads();
+    double acc[RM][RN];
+#pragma unroll
+    for (int q = 0; q < RM; q++)
+#pragma unroll
+        for (int r = 0; r < RN; r++) acc[q][r] = 0.0;
+#pragma unroll 8
+    for (int s = 0; s < kPB; s++) {
+        double a[RM], b[RN];
+#pragma unroll
+        for (int q = 0; q < RM; q++) a[q] = As[s][tx + 16 * q];
+#pragma unroll
+        for (int r = 0; r < RN; r++) b[r] = Bs[s][ty + 16 * r];
+#pragma unroll
+        for (int q = 0; q < RM; q++)
+#pragma unroll
+            for (int r = 0; r < RN; r++) acc[q][r] += a[q] * b[r];
+    }
+#pragma unroll
+    for (int q = 0; q < RM; q++)
+#pragma unroll
+        for (int r = 0; r < RN; r++) {
+            const int gr = row0 + tx + 16 * q, gc = col0 + ty + 16 * r;
+            if (gr < m && gc < nn) C[(size_t)gc * ldc + gr] = cv[q][r] - acc[q][r];
+        }
+}
+
 static void dgemm_sub(cudaStream_t st, int m, int nn, int kk, const double *A, int lda, const double *B, int ldb,
                       double *C, int ldc)
 {
     if (m <= 0 || nn <= 0 || kk <= 0) return;
+    if (kk <= kPB) {
+        const long big = (long)((m + 63) / 64) * ((nn + 63) / 64);
+        if (big >= 2 * 148) {
+            dim3 grid((m + 63) / 64, (nn + 63) / 64);
+            k_dgemm_k32<64, 64><<<grid, 256, 0, st>>>(m, nn, kk, A, lda, B, ldb, C, ldc); P2_COUNT_LAUNCH();
+        } else {
+            dim3 grid((m + 31) / 32, (nn + 31) / 32);
+            k_dgemm_k32<32, 32><<<grid, 256, 0, st>>>(m, nn, kk, A, lda, B, ldb, C, ldc); P2_COUNT_LAUNCH();
+        }
+        return;
+    }
     dim3 grid((m + 63) / 64, (nn + 63) / 64);
     k_dgemm_sub<<<grid, 256, 0, st>>>(m, nn, kk, A, lda, B, ldb, C, ldc); P2_COUNT_LAUNCH();
 }
@@ -390,7 +541,11 @@ static void lu_issue(cudaStream_t st, double *A, int n, int kl, int ku, double *
             size_t bytes = sizeof(double) * (size_t)(r1 - k0) * nb;
             const int thr = ((r1 - k0) + 31) / 32 * 32;  // one thread per panel row
             T.begin();
-            k_panel_track<<<1, thr, bytes, st>>>(A, n, k0, nb, r1, d_ipiv, d_info); P2_COUNT_LAUNCH();
+            if (nb == kPB && r1 - k0 <= kRegPanelRows) {
+                k_panel_reg<<<1, thr, 0, st>>>(A, n, k0, r1, d_ipiv, d_info); P2_COUNT_LAUNCH();
+            } else {
+                k_panel_track<<<1, thr, bytes, st>>>(A, n, k0, nb, r1, d_ipiv, d_info); P2_COUNT_LAUNCH();
+            }
             T.end(0);
         } else {
             k_panel_global<<<1, 1024, 0, st>>>(A, n, k0, nb, r1, d_ipiv, d_info); P2_COUNT_LAUNCH();
@@ -398,7 +553,7 @@ static void lu_issue(cudaStream_t st, double *A, int n, int kl, int ku, double *
         const int cb = k0 + nb;
         if (c1 > cb) {
             T.begin();
-            k_perm_trsm_lower<<<(c1 - cb + kTrsmThreads - 1) / kTrsmThreads, kTrsmThreads, 0, st>>>(
+            k_perm_trsm_lower_w<<<(c1 - cb + kTrsmWarps - 1) / kTrsmWarps, 32 * kTrsmWarps, 0, st>>>(
                 A, n, k0, nb, d_ipiv, A, n, cb, c1); P2_COUNT_LAUNCH();
             T.end(1);
             T.begin();
@@ -416,8 +571,8 @@ static void lu_issue(cudaStream_t st, double *A, int n, int kl, int ku, double *
         const int nb = std::min(kPB, n - k0);
         const int r1 = std::min(n, k0 + nb + kl);
         T.begin();
-        k_perm_trsm_lower<<<(r1 + kTrsmThreads - 1) / kTrsmThreads, kTrsmThreads, 0, st>>>(A, n, k0, nb, d_ipiv, Ainv,
-                                                                                         n, 0, r1); P2_COUNT_LAUNCH();
+        k_perm_trsm_lower_w<<<(r1 + kTrsmWarps - 1) / kTrsmWarps, 32 * kTrsmWarps, 0, st>>>(A, n, k0, nb, d_ipiv,
+                                                                                         Ainv, n, 0, r1); P2_COUNT_LAUNCH();
         T.end(1);
         const int cb = k0 + nb;
         T.begin();
@@ -431,7 +586,7 @@ static void lu_issue(cudaStream_t st, double *A, int n, int kl, int ku, double *
     for (int k0 = last; k0 >= 0; k0 -= kPB) {
         const int nb = std::min(kPB, n - k0);
         T.begin();
-        k_trsm_upper<<<(n + 127) / 128, 128, 0, st>>>(A, n, k0, nb, Ainv, n, 0, n); P2_COUNT_LAUNCH();
+        k_trsm_upper_w<<<(n + kTrsmWarps - 1) / kTrsmWarps, 32 * kTrsmWarps, 0, st>>>(A, n, k0, nb, Ainv, n, 0, n); P2_COUNT_LAUNCH();
         T.end(3);
         const int a = std::max(0, k0 - kuu);
         T.begin();
