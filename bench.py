@@ -47,6 +47,12 @@ WORKLOAD = WORKLOADS[CONFIG_IDX]
 # (16 B) and 4 viscosity fields (16 B); write 3 velocity fields (12 B) and
 # half of the pressures (2 B).
 SMOOTHER_BYTES_PER_NODE = 62
+# Marker advection: per marker read x, y, z (12 B) and the type (1 B), write
+# x, y, z (12 B); per node read the FP64 velocities (24 B) and write and
+# re-read their float copies (12 + 12 B) once (the 8-node gathers of the
+# four Runge-Kutta stages hit L2).
+MOVEMARK_BYTES_PER_MARKER = 25
+MOVEMARK_BYTES_PER_NODE = 48
 
 
 def parse():
@@ -77,7 +83,7 @@ def measured_peaks():
 def profile_traffic():
     """Per-launch DRAM bytes of the level-0 FP32 smoother pass from the
     committed ncu summary (None until one is captured)."""
-    p = os.path.join(ROOT, "profiles", "ncu_vanka_full_f32_level0.txt")
+    p = os.path.join(ROOT, "profiles", "ncu_vanka_fast_f32_level0.txt")
     if not os.path.exists(p):
         return None
     m = re.search(r"dram_bytes_per_launch:\s*([0-9.eE+]+)", open(p).read())
@@ -303,6 +309,18 @@ def main():
     fp64_ms = sum(i.ms_total for i in i64) / args.steps
     p64.close()
 
+    # one marker advection step (movemark, RK4) of the resident markers through
+    # the resident solution of the last timed solve; CFL 0.5 on the finest cell
+    sol = prob.ctx.solution(n)
+    vmax = max(float(np.abs(sol[k]).max()) for k in ("vx", "vy", "vz"))
+    hmin = min(float(np.diff(g).min()) for g in (m.gx, m.gy, m.gz))
+    dt_move = 0.5 * hmin / vmax
+    for _ in range(args.warmup):
+        prob.ctx.movemark_resident(dt_move)
+    move_ms = statistics.mean(prob.ctx.movemark_resident(dt_move) for _ in range(args.steps))
+    nmark = int(m.markx.size)
+    move_bytes = MOVEMARK_BYTES_PER_MARKER * nmark + MOVEMARK_BYTES_PER_NODE * n
+
     # end to end through the public C ABI with pinned host buffers
     keys = ("nu", "ro", "nxx", "nxy", "nxz", "nyz")
     host_nodes = prob.ctx.get_nodes(n)
@@ -347,12 +365,15 @@ def main():
         "unknowns_per_s": m.real_dofs() * world / (ms_per_step * 1e-3),
         "gpu_launches": launches,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": traffic, "kernel": ("k_vanka_full<float>" if tune.smoother else "k_vanka<float>") + " level-0 colour pass",
+                     "traffic": traffic, "kernel": ("k_vanka_fast<float>" if tune.smoother else "k_vanka<float>") + " level-0 colour pass",
                      "bytes_per_launch": bytes_per_launch, "ms_per_launch": pass_ms,
                      "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs, burst)"},
         "clocks": clocks,
         "e2e": {"value": e2e_ms, "unit": "ms", "h2d_bytes_per_step": 24 * n + 32 * n, "d2h_bytes_per_step": 32 * n},
     }
+    line["movemark"] = {"ms": move_ms, "markers": nmark, "markmod": "RK4", "dt": dt_move,
+                        "achieved_GBps": move_bytes / (move_ms * 1e-3) / 1e9, "bytes_per_step": move_bytes,
+                        "launches": 2}
     line["autotune"] = tune.as_dict()
     if rank == 0 and world == 1 and not args.no_cpu_baseline and args.config <= 2:
         threads = os.cpu_count() or 1

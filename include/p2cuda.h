@@ -19,6 +19,8 @@
  *                      pardisomat() PARDISO solve, pardiso/gaus3mg_SerieMG.c:64
  *   p2_ronurecalc      void ronurecalc(void), pardiso/mark3mg.c:630
  *                      (prototype pardiso/head3mg.c:417)
+ *   p2_movemark        void movemark(void), pardiso/mark3mg.c:174
+ *                      (prototype pardiso/head3mg.c:416)
  * A C shim with the reference's own signatures on top of these calls is in
  * pardiso2_b200/csrc/move3mg_cuda.c.
  */
@@ -151,6 +153,25 @@ p2_status p2_upload_markers(p2_ctx *ctx, long nmark, const float *markx, const f
                             const double *markro);
 p2_status p2_ronurecalc_resident(p2_ctx *ctx, double *ms);
 p2_status p2_get_nodes(p2_ctx *ctx, float *nu, float *ro, float *nxx, float *nxy, float *nxz, float *nyz);
+
+/* movemark(): marker advection over one time step, pardiso/mark3mg.c:174
+ * (prototype pardiso/head3mg.c:416): markmod 2 is the fourth-order
+ * Runge-Kutta branch, markmod 1 the single-velocity one, with the velocity at
+ * a point interpolated from the staggered
+ * vx, vy, vz nodes as vxyzcalc1 (mark3mg.c:2963) does; non-periodic boxes.
+ * Markers are moved when inside the box or, unless outgrid is 1, when their
+ * type is below 50 or at least 100; outgrid 2 keeps the motion of markers
+ * outside the box orthogonal to the wall.  Positions come out bit-identical
+ * to the reference's.  Not reproduced: the strain-rate side outputs (val1,
+ * marke), the temperature reset (markk = 0) of markers that leave the box,
+ * and the water/melt moves that the reference has switched off.
+ *   p2_movemark: vx, vy, vz host arrays (float, node layout) and markers in/out;
+ *   p2_movemark_resident: the resident markers (p2_upload_markers) with the
+ *   solution of the last resident solve; read them with p2_get_markers. */
+p2_status p2_movemark(p2_ctx *ctx, double timestep, int markmod, int outgrid, const float *vx, const float *vy, const float *vz,
+                      long nmark, float *markx, float *marky, float *markz, const signed char *markt);
+p2_status p2_movemark_resident(p2_ctx *ctx, double timestep, int markmod, int outgrid, double *ms);
+p2_status p2_get_markers(p2_ctx *ctx, float *markx, float *marky, float *markz);
 
 /* The p2_ronurecalc interpolation for callers that cannot allocate device
  * memory: a host code whose device memory is all handed out by its own pool

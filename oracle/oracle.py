@@ -47,6 +47,8 @@ def lib() -> C.CDLL:
         L.p2o_rel_residual.restype = C.c_double
         L.p2o_ronurecalc.argtypes = [C.c_int, C.c_int, C.c_int, _dp, _dp, _dp, C.c_long, _fp, _fp, _fp, _bp,
                                      _dp, _dp, C.c_double, C.c_double, C.c_double, C.c_int] + [_fp] * 6
+        L.p2o_movemark.argtypes = [C.c_int, C.c_int, C.c_int, _dp, _dp, _dp, _fp, _fp, _fp, C.c_double, C.c_int,
+                                   C.c_int, C.c_long, _fp, _fp, _fp, _bp, C.c_void_p]
         _lib = L
     return _lib
 
@@ -64,6 +66,21 @@ def ronurecalc(model, init=None):
                      np.ascontiguousarray(model.rocks.n0, np.float64), np.ascontiguousarray(model.rocks.ro, np.float64),
                      p.nubeg, p.nuend, p.nukoef, p.viscmod, *[out[k] for k in keys])
     return out
+
+
+def movemark(model, vel, timestep, markmod=2, outgrid=0, markers=None, markk=None):
+    """Marker advection by the oracle: returns new (markx, marky, markz) and,
+    when markk is given, the updated copy of it.  vel = (vx, vy, vz) float32
+    in the node layout; markers defaults to the model's."""
+    L = lib()
+    nx, ny, nz = model.shape
+    mx, my, mz, mt = markers if markers is not None else (model.markx, model.marky, model.markz, model.markt)
+    out = [np.array(a, np.float32) for a in (mx, my, mz)]
+    kk = None if markk is None else np.array(markk, np.float32)
+    L.p2o_movemark(nx, ny, nz, model.gx, model.gy, model.gz, *[np.ascontiguousarray(a, np.float32) for a in vel],
+                   timestep, markmod, outgrid, out[0].size, out[0], out[1], out[2],
+                   np.ascontiguousarray(mt, np.int8), None if kk is None else kk.ctypes.data)
+    return (*out, kk) if kk is not None else tuple(out)
 
 
 class OracleSolver:

@@ -22,6 +22,8 @@
  *   nu/ro restriction .................... pardiso/move3mgNew.c:3386-3527
  *   pressure reset to pinit .............. pardiso/move3mgNew.c:2834-2855
  *   marker -> node interpolation ......... pardiso/mark3mg.c:630-1133
+ *   marker advection (RK4 / simple) ...... pardiso/mark3mg.c:174-629, with
+ *     the staggered velocity interpolation vxyzcalc1 2963-3243
  *     (cell search m1serch..m3serch 1138-1204, constant rock viscosity
  *      viscalc 1481-1482, constant density dencalc1 1429)
  *   coarsest direct solve (MKL PARDISO) .. banded pivoted LU (banded_lu.h)
@@ -1499,6 +1501,116 @@ void p2o_ronurecalc(int nx, int ny, int nz, const double *gx, const double *gy, 
         }
     }
     for (q = 0; q < 6; q++) { free(A[q]); free(W[q]); }
+}
+
+/* ---------------------------------------------------------------------- */
+/* Marker advection (movemark, mark3mg.c:174-629, non-periodic box) with   */
+/* the staggered velocity interpolation vxyzcalc1 (mark3mg.c:2963-3243).   */
+typedef struct {
+    const double *g[3];
+    long n[3];
+    double size[3];
+} mv_grid;
+
+/* weights along the component's own axis: node interval of the cell */
+static void mv_node_axis(const double *g, long n, long m, double x, long *lo, double *w0, double *w1)
+{
+    long a = m;
+    double d;
+    if (a < 0) a = 0;
+    if (a > n - 2) a = n - 2;
+    d = g[a + 1] - g[a];
+    *lo = a;
+    *w0 = 1.0 - (-((g[a] - x) / d));
+    *w1 = 1.0 - (g[a + 1] - x) / d;
+}
+
+/* weights along a cross axis: between cell mid-points, the point clamped
+ * onto the first or last mid-point (mark3mg.c:2988-3024) */
+static void mv_mid_axis(const double *g, long n, long m, double x, long *lo, double *w0, double *w1)
+{
+    long a = m;
+    double X = x, d;
+    if (X < (g[a] + g[a + 1]) / 2.0) a -= 1;
+    if (a < 0) { a = 0; X = (g[0] + g[1]) / 2.0; }
+    if (a > n - 3) { a = n - 3; X = (g[a + 1] + g[a + 2]) / 2.0; }
+    d = (g[a + 2] - g[a]) / 2.0;
+    *lo = a;
+    *w0 = 1.0 - (-(((g[a] + g[a + 1]) / 2.0 - X) / d));
+    *w1 = 1.0 - ((g[a + 1] + g[a + 2]) / 2.0 - X) / d;
+}
+
+static void mv_velocity(const mv_grid *G, const float *const v[3], double x, double y, double z, double out[3])
+{
+    double p[3], w[3][2];
+    long cell[3], lo[3], nxy = G->n[0] * G->n[1];
+    int comp, a, b, c;
+    p[0] = x; p[1] = y; p[2] = z;
+    for (a = 0; a < 3; a++) {
+        if (p[a] < 0) p[a] = 0;
+        if (p[a] > G->size[a]) p[a] = G->size[a];
+        cell[a] = serch(G->g[a], G->n[a], p[a]);
+    }
+    for (comp = 0; comp < 3; comp++) {
+        double sum = 0;
+        for (a = 0; a < 3; a++) {
+            if (a == comp) mv_node_axis(G->g[a], G->n[a], cell[a], p[a], &lo[a], &w[a][0], &w[a][1]);
+            else mv_mid_axis(G->g[a], G->n[a], cell[a], p[a], &lo[a], &w[a][0], &w[a][1]);
+        }
+        /* z outer, x, y inner, as the three loops of vxyzcalc1 */
+        for (c = 0; c < 2; c++)
+            for (a = 0; a < 2; a++)
+                for (b = 0; b < 2; b++)
+                    sum += v[comp][(lo[2] + c) * nxy + (lo[0] + a) * G->n[1] + lo[1] + b] * (w[0][a] * w[1][b] * w[2][c]);
+        out[comp] = sum;
+    }
+}
+
+/* markmod 1: velocity at the marker; 2: fourth-order Runge-Kutta.  Markers
+ * are moved when inside the box or, unless outgrid is 1, when their type is
+ * below 50 or at least 100; outgrid 2 keeps the motion outside the box
+ * orthogonal to the wall.  markk (may be NULL) is set to 0 for moved markers
+ * of type below 100 that end outside the box (mark3mg.c:489-494). */
+void p2o_movemark(int nx, int ny, int nz, const double *gx, const double *gy, const double *gz, const float *vx,
+                  const float *vy, const float *vz, double dt, int markmod, int outgrid, long nmark, float *mx,
+                  float *my, float *mz, const signed char *mt, float *markk)
+{
+    mv_grid G;
+    const float *v[3];
+    long q;
+    int a;
+    G.g[0] = gx; G.g[1] = gy; G.g[2] = gz;
+    G.n[0] = nx; G.n[1] = ny; G.n[2] = nz;
+    G.size[0] = gx[nx - 1]; G.size[1] = gy[ny - 1]; G.size[2] = gz[nz - 1];
+    v[0] = vx; v[1] = vy; v[2] = vz;
+    for (q = 0; q < nmark; q++) {
+        double k1[3], k2[3], k3[3], k4[3], vel[3];
+        double x0 = mx[q], y0 = my[q], z0 = mz[q];
+        int t = mt[q];
+        int inside = mx[q] >= 0 && my[q] >= 0 && mz[q] >= 0 && x0 <= G.size[0] && y0 <= G.size[1] && z0 <= G.size[2];
+        if (!(inside || (outgrid != 1 && (t < 50 || t >= 100)))) continue;
+        mv_velocity(&G, v, x0, y0, z0, k1);
+        if (markmod == 1) {
+            for (a = 0; a < 3; a++) vel[a] = k1[a];
+        } else {
+            mv_velocity(&G, v, x0 + k1[0] * dt / 2.0, y0 + k1[1] * dt / 2.0, z0 + k1[2] * dt / 2.0, k2);
+            mv_velocity(&G, v, x0 + k2[0] * dt / 2.0, y0 + k2[1] * dt / 2.0, z0 + k2[2] * dt / 2.0, k3);
+            mv_velocity(&G, v, x0 + k3[0] * dt, y0 + k3[1] * dt, z0 + k3[2] * dt, k4);
+            for (a = 0; a < 3; a++) vel[a] = (k1[a] + 2.0 * k2[a] + 2.0 * k3[a] + k4[a]) / 6.0;
+        }
+        if (outgrid == 2) {
+            if (mx[q] < 0 || x0 > G.size[0]) vel[1] = vel[2] = 0;
+            if (my[q] < 0 || y0 > G.size[1]) vel[0] = vel[2] = 0;
+            if (mz[q] < 0 || z0 > G.size[2]) vel[0] = vel[1] = 0;
+        }
+        mx[q] = (float)(x0 + dt * vel[0]);
+        my[q] = (float)(y0 + dt * vel[1]);
+        mz[q] = (float)(z0 + dt * vel[2]);
+        if (markk && t < 100 &&
+            (mx[q] < 0 || my[q] < 0 || mz[q] < 0 || (double)mx[q] > G.size[0] || (double)my[q] > G.size[1] ||
+             (double)mz[q] > G.size[2]))
+            markk[q] = 0;
+    }
 }
 
 /* Debug/test helpers: sweeps of the level-0 smoother only; two-grid count. */

@@ -39,15 +39,17 @@ void PARDISO(void **pt, int *maxfct, int *mnum, int *mtype, int *phase, int *n,
 #include "head3mg.c"
 #include "load3mg.c"
 #ifdef P2REF_SHIM
-/* drop-in variant: vpiterate()/ronurecalc() come from move3mg_cuda.c (GPU) */
+/* drop-in variant: vpiterate()/ronurecalc()/movemark() come from move3mg_cuda.c (GPU) */
 #define vpiterate vpiterate_cpu
 #define ronurecalc ronurecalc_cpu
+#define movemark movemark_cpu
 #endif
 #include "move3mgNew.c"
 #include "mark3mg.c"
 #ifdef P2REF_SHIM
 #undef vpiterate
 #undef ronurecalc
+#undef movemark
 #endif
 #include "gaus3mg_SerieMG.c"
 #include "heat3mg.c"
@@ -165,6 +167,15 @@ int p2ref_init(long nx, long ny, long nz, const double *ggx, const double *ggy,
     dynmemall(1);
     dynmemall(2);
     unmute();
+    /* markk (temperature), markd, markw are read and written by movemark()
+     * (mark3mg.c:249, 494, 525-527) but dynmemall() never allocates them
+     * (load3mg.c:2323-2334; only the visualiser's load3viz.c:2141 does), so
+     * the stock program dereferences null pointers once a marker of type
+     * < 100 leaves the box or a marker of type >= 100 exists.  The harness
+     * gives them storage so that those branches can be exercised. */
+    if (!markk) markk = (float *)calloc((size_t)marknum0, sizeof(float));
+    if (!markd) markd = (float *)calloc((size_t)marknum0, sizeof(float));
+    if (!markw) markw = (float *)calloc((size_t)marknum0, sizeof(float));
     {
         long mcmax = mgp[multinum] + mgn[multinum];
         memset(bondm, 0, sizeof(int) * (size_t)(mcmax + nodenum8));
@@ -309,6 +320,41 @@ void p2ref_get_nodes(float *onu, float *oro, float *oxx, float *oxy, float *oxz,
     memcpy(oxy, nxy, sizeof(float) * (size_t)nodenum);
     memcpy(oxz, nxz, sizeof(float) * (size_t)nodenum);
     memcpy(oyz, nyz, sizeof(float) * (size_t)nodenum);
+}
+
+/* Float velocities in node layout, as vpiterate leaves them for movemark. */
+void p2ref_set_velocity(const float *ivx, const float *ivy, const float *ivz)
+{
+    memcpy(vx, ivx, sizeof(float) * (size_t)nodenum);
+    memcpy(vy, ivy, sizeof(float) * (size_t)nodenum);
+    memcpy(vz, ivz, sizeof(float) * (size_t)nodenum);
+}
+
+/* movemark() (mark3mg.c:174) over one step; returns its wall time in seconds. */
+double p2ref_movemark(double dt, int mmod, int og)
+{
+    double t0;
+    timestep = dt;
+    markmod = mmod;
+    outgrid = og;
+    mute();
+    t0 = omp_get_wtime();
+    movemark();
+    t0 = omp_get_wtime() - t0;
+    unmute();
+    return t0;
+}
+
+void p2ref_fill_markk(float v)
+{
+    long i;
+    for (i = 0; i < marknum; i++) markk[i] = v;
+}
+
+void p2ref_get_markers(float *mx, float *my, float *mz, float *mk)
+{
+    long i;
+    for (i = 0; i < marknum; i++) { mx[i] = markx[i]; my[i] = marky[i]; mz[i] = markz[i]; if (mk) mk[i] = markk[i]; }
 }
 
 /* Coarse-level nu/ro/nd after ronurestrict (all levels, concatenated). */

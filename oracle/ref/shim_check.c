@@ -1,5 +1,5 @@
 /* Compile check (test infrastructure): the reference's unity build
- * (pardiso/i3mg.c:1-19, without its main) with vpiterate() and ronurecalc()
+ * (pardiso/i3mg.c:1-19, without its main) with vpiterate(), ronurecalc() and movemark()
  * taken from pardiso2_b200/csrc/move3mg_cuda.c: the CPU functions are renamed
  * by two macros around their files and the shim is included after them.
  * Built with -c only: it proves the shim compiles against the reference's
@@ -16,10 +16,12 @@
 #include "load3mg.c"
 #define vpiterate vpiterate_cpu
 #define ronurecalc ronurecalc_cpu
+#define movemark movemark_cpu
 #include "move3mgNew.c"
 #include "mark3mg.c"
 #undef vpiterate
 #undef ronurecalc
+#undef movemark
 #include "gaus3mg_SerieMG.c"
 #include "heat3mg.c"
 #include "move3mg_cuda.c"

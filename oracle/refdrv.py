@@ -64,6 +64,11 @@ def _load(shim: bool = False) -> C.CDLL:
         lib.p2ref_restrict.argtypes = [C.c_int, _dp, _dp]
         lib.p2ref_prolong.argtypes = [C.c_int, _dp, _dp]
         lib.p2ref_set_quiet.argtypes = [C.c_int]
+        lib.p2ref_set_velocity.argtypes = [_fp] * 3
+        lib.p2ref_movemark.argtypes = [C.c_double, C.c_int, C.c_int]
+        lib.p2ref_movemark.restype = C.c_double
+        lib.p2ref_fill_markk.argtypes = [C.c_float]
+        lib.p2ref_get_markers.argtypes = [_fp] * 4
         lib.p2ref_lu_count.restype = C.c_int
         lib.p2ref_num_threads.restype = C.c_int
         _libs[path] = lib
@@ -164,6 +169,30 @@ class RefModel:
         v = [np.zeros(n, np.float32) for _ in range(3)]
         self.lib.p2ref_get_written(pr, *v)
         return {"pr": pr, "vx": v[0], "vy": v[1], "vz": v[2]}
+
+    def set_markers(self, mx, my, mz, mt):
+        """Replace the marker coordinates and types (same count as the model's)."""
+        if np.asarray(mx).size != self.m.markx.size:
+            raise ValueError("the reference's marker count is fixed at init")
+        self.lib.p2ref_set_markers(*[np.ascontiguousarray(a, np.float32) for a in (mx, my, mz)],
+                                   np.ascontiguousarray(mt, np.int8))
+
+    def set_velocity(self, vx, vy, vz):
+        self.lib.p2ref_set_velocity(*[np.ascontiguousarray(a, np.float32) for a in (vx, vy, vz)])
+
+    def movemark(self, timestep, markmod=2, outgrid=0) -> float:
+        """movemark() over one step; returns its wall time (s)."""
+        return self.lib.p2ref_movemark(timestep, markmod, outgrid)
+
+    def fill_markk(self, value):
+        self.lib.p2ref_fill_markk(value)
+
+    def markers(self):
+        """markx, marky, markz, markk after the reference's marker routines."""
+        n = self.m.markx.size
+        out = [np.zeros(n, np.float32) for _ in range(4)]
+        self.lib.p2ref_get_markers(*out)
+        return out
 
     def solution(self):
         n = self.m.nodenum

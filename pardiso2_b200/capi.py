@@ -20,7 +20,8 @@ STATUS = {0: "P2_OK", 1: "P2_ERR_ARG", 2: "P2_ERR_CUDA", 3: "P2_ERR_NOMEM", 4: "
 EXPORTED = ["p2_default_params", "p2_create", "p2_destroy", "p2_last_error", "p2_set_grid", "p2_set_bc",
             "p2_set_nodes", "p2_stokes_solve", "p2_stokes_solve_resident", "p2_get_solution", "p2_ronurecalc",
             "p2_upload_markers", "p2_ronurecalc_resident", "p2_get_nodes", "p2_debug_apply", "p2_debug_restrict",
-            "p2_debug_prolong", "p2_debug_level_fields", "p2_debug_time_smoother", "p2_ronurecalc_noalloc", "p2_autotune"]
+            "p2_debug_prolong", "p2_debug_level_fields", "p2_debug_time_smoother", "p2_ronurecalc_noalloc", "p2_autotune",
+            "p2_movemark", "p2_movemark_resident", "p2_get_markers"]
 
 
 class Params(C.Structure):
@@ -90,6 +91,11 @@ def load() -> C.CDLL:
     L.p2_get_nodes.argtypes = [vp] + [C.c_void_p] * 6
     L.p2_autotune.argtypes = [vp, C.c_int, C.POINTER(TuneInfo)]
     L.p2_autotune.restype = C.c_int
+    L.p2_movemark.argtypes = [vp, C.c_double, C.c_int, C.c_int, _fp, _fp, _fp, C.c_long, _fp, _fp, _fp, _bp]
+    L.p2_movemark_resident.argtypes = [vp, C.c_double, C.c_int, C.c_int, C.POINTER(C.c_double)]
+    L.p2_get_markers.argtypes = [vp, _fp, _fp, _fp]
+    for f in ("p2_movemark", "p2_movemark_resident", "p2_get_markers"):
+        getattr(L, f).restype = C.c_int
     for f in ("p2_create", "p2_set_grid", "p2_set_bc", "p2_set_nodes", "p2_stokes_solve", "p2_stokes_solve_resident",
               "p2_get_solution", "p2_ronurecalc", "p2_upload_markers", "p2_ronurecalc_resident", "p2_get_nodes"):
         getattr(L, f).restype = C.c_int
@@ -160,6 +166,25 @@ class Context:
         info = TuneInfo()
         self._check(self.L.p2_autotune(self.h, trial_iters, C.byref(info)), "p2_autotune")
         return info
+
+    def movemark(self, timestep: float, vx, vy, vz, mx, my, mz, mt, markmod: int = 2, outgrid: int = 0):
+        """movemark(): returns the moved marker coordinates (new float32 arrays)."""
+        out = [np.array(a, np.float32) for a in (mx, my, mz)]
+        self._check(self.L.p2_movemark(self.h, timestep, markmod, outgrid, np.ascontiguousarray(vx, np.float32),
+                                       np.ascontiguousarray(vy, np.float32), np.ascontiguousarray(vz, np.float32),
+                                       out[0].size, out[0], out[1], out[2], np.ascontiguousarray(mt, np.int8)),
+                    "p2_movemark")
+        return out
+
+    def movemark_resident(self, timestep: float, markmod: int = 2, outgrid: int = 0) -> float:
+        ms = C.c_double()
+        self._check(self.L.p2_movemark_resident(self.h, timestep, markmod, outgrid, C.byref(ms)), "p2_movemark_resident")
+        return ms.value
+
+    def get_markers(self, nmark: int):
+        out = [np.zeros(nmark, np.float32) for _ in range(3)]
+        self._check(self.L.p2_get_markers(self.h, *out), "p2_get_markers")
+        return out
 
     def solve_resident(self, check=True) -> SolveInfo:
         info = SolveInfo()

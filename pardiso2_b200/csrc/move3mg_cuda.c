@@ -1,20 +1,22 @@
 /*
- * move3mg_cuda.c -- the reference's vpiterate() and ronurecalc() on top of
- * libp2cuda.so (include/p2cuda.h).
+ * move3mg_cuda.c -- the reference's vpiterate(), ronurecalc() and movemark()
+ * on top of libp2cuda.so (include/p2cuda.h).
  *
  * This file is compiled inside the reference's unity build (pardiso/i3mg.c
  * includes head3mg.c, load3mg.c, move3mgNew.c, mark3mg.c, ... into one
  * translation unit) and uses its globals (pardiso/head3mg.c) directly: the
  * entry points keep their signatures and their data exchange through
- * globals, so the time loop in i3mg.c is unchanged.  The two CPU functions it
+ * globals, so the time loop in i3mg.c is unchanged.  The CPU functions it
  * replaces are renamed out of the way before their files are included:
  *
  *     #define vpiterate  vpiterate_cpu     -- pardiso/move3mgNew.c:1791
  *     #define ronurecalc ronurecalc_cpu    -- pardiso/mark3mg.c:630
+ *     #define movemark   movemark_cpu      -- pardiso/mark3mg.c:174
  *     #include "move3mgNew.c"
  *     #include "mark3mg.c"
  *     #undef vpiterate
  *     #undef ronurecalc
+ *     #undef movemark
  *     #include "move3mg_cuda.c"
  *
  * Inputs read: xnumx, ynumy, znumz, gx, gy, gz, x/y/zperiodic, multinum,
@@ -22,9 +24,11 @@
  * nyz, vx, vy, vz, pr, p0koef, p1koef, p2koef, v0koef, v1koef, nubeg, nuend,
  * nukoef, viscmod, GXKOEF, GYKOEF, GZKOEF, pinit, pxinit, pyinit, pzinit;
  * markers markx, marky, markz, markt, marknum and the rock tables markn0,
- * markn1, markro (rocknum types).
+ * markn1, markro (rocknum types); timestep, markmod, outgrid for movemark.
  * Outputs written: vx, vy, vz (float) and pr (double) by vpiterate; nu, ro,
- * nxx, nxy, nxz, nyz by ronurecalc.  The stress and strain-rate fields and
+ * nxx, nxy, nxz, nyz by ronurecalc; markx, marky, markz and the markk reset
+ * of markers that leave the box by movemark (val1 and marke, the strain-rate
+ * side outputs of the CPU movemark, are not updated).  The stress and strain-rate fields and
  * the time-step limit that the CPU vpiterate also derives are not computed
  * here.
  *
@@ -122,4 +126,41 @@ void ronurecalc(void)
     st = p2_ronurecalc(p2s_ctx, marknum, markx, marky, markz, (const signed char *)markt, nrock, markn0, markn1,
                        markro, nu, ro, nxx, nxy, nxz, nyz);
     if (st != P2_OK) p2s_fail("p2_ronurecalc", st);
+}
+
+/* pardiso/mark3mg.c:174 (prototype pardiso/head3mg.c:416): advect the markers
+ * through the current vx, vy, vz over timestep (markmod 1 or 2); periodic
+ * boxes are not supported.  Markers of type < 100 that end outside the box
+ * get markk = 0, as in the reference (mark3mg.c:489-494), when markk has
+ * storage (i3mg.c's dynmemall() leaves it null, and the CPU movemark would
+ * then fault on that store). */
+void movemark(void)
+{
+    p2_status st;
+    long m;
+    char *was_in = NULL;
+    if (markmod != 1 && markmod != 2) return;
+    p2s_setup();
+    if (marknum > 0) {
+        was_in = (char *)malloc((size_t)marknum);
+        if (!was_in) {
+            printf("movemark: out of host memory\n");
+            exit(0);
+        }
+        for (m = 0; m < marknum; m++)
+            was_in[m] = markx[m] >= 0 && marky[m] >= 0 && markz[m] >= 0 && (double)markx[m] <= xsize &&
+                        (double)marky[m] <= ysize && (double)markz[m] <= zsize;
+    }
+    st = p2_movemark(p2s_ctx, timestep, markmod, outgrid, vx, vy, vz, marknum, markx, marky, markz,
+                     (const signed char *)markt);
+    if (st != P2_OK) p2s_fail("p2_movemark", st);
+    for (m = 0; m < marknum; m++) {
+        int t = markt[m];
+        int moved = was_in[m] || (outgrid != 1 && (t < 50 || t >= 100));
+        if (markk && moved && t < 100 &&
+            (markx[m] < 0 || marky[m] < 0 || markz[m] < 0 || (double)markx[m] > xsize ||
+             (double)marky[m] > ysize || (double)markz[m] > zsize))
+            markk[m] = 0;
+    }
+    free(was_in);
 }

@@ -274,6 +274,40 @@ p2_status p2_debug_prolong(p2_ctx *ctx, int coarse_level, const double *coarse_x
     });
 }
 
+p2_status p2_movemark(p2_ctx *ctx, double timestep, int markmod, int outgrid, const float *vx, const float *vy, const float *vz,
+                      long nmark, float *markx, float *marky, float *markz, const signed char *markt)
+{
+    return guard(ctx, [&] {
+        if (!vx || !vy || !vz || (nmark > 0 && (!markx || !marky || !markz || !markt)))
+            throw p2::Error(P2_ERR_ARG, "null argument");
+        P2_CUDA_TRY(cudaSetDevice(ctx->s->dev));
+        ctx->s->movemark_host(timestep, markmod, outgrid, vx, vy, vz, nmark, markx, marky, markz, markt);
+    });
+}
+
+p2_status p2_movemark_resident(p2_ctx *ctx, double timestep, int markmod, int outgrid, double *ms)
+{
+    return guard(ctx, [&] {
+        p2::Solver &S = *ctx->s;
+        P2_CUDA_TRY(cudaSetDevice(S.dev));
+        P2_CUDA_TRY(cudaEventRecord(S.ev[5], S.st));
+        S.movemark_device(timestep, markmod, outgrid);
+        P2_CUDA_TRY(cudaEventRecord(S.ev[6], S.st));
+        P2_CUDA_TRY(cudaEventSynchronize(S.ev[6]));
+        float t = 0;
+        P2_CUDA_TRY(cudaEventElapsedTime(&t, S.ev[5], S.ev[6]));
+        if (ms) *ms = t;
+    });
+}
+
+p2_status p2_get_markers(p2_ctx *ctx, float *markx, float *marky, float *markz)
+{
+    return guard(ctx, [&] {
+        P2_CUDA_TRY(cudaSetDevice(ctx->s->dev));
+        ctx->s->get_markers(markx, marky, markz);
+    });
+}
+
 p2_status p2_autotune(p2_ctx *ctx, int trial_iters, p2_tune_info *info)
 {
     return guard(ctx, [&] {

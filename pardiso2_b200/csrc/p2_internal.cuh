@@ -30,6 +30,13 @@ namespace p2 {
 // launch adds the number of kernel nodes it replays).
 extern thread_local long long g_launches;
 
+// Level-0 gridlines on the device for marker kernels.
+struct Grid3 {
+    const double *g[3];
+    int n[3];        // xnumx, ynumy, znumz
+    double size[3];  // xsize, ysize, zsize
+};
+
 // Replayable launch sequence of the coarsest LU and inverse (p2_lu.cu).
 struct LuGraph {
     cudaGraphExec_t exec = nullptr;

@@ -279,6 +279,210 @@ __global__ void k_node_gather(int nx, int ny, int nz, const double *gx, const do
 }
 
 // ---------------------------------------------------------------------------
+// Marker advection (movemark, pardiso/mark3mg.c:174-629, fourth-order
+// Runge-Kutta branch, non-periodic box): velocity at a point by staggered
+// trilinear interpolation (vxyzcalc1, mark3mg.c:2963-3243) with the
+// reference's clamping of points and cell indices at the walls, in the same
+// double arithmetic without fused multiply-adds, so positions match the
+// reference bit for bit.
+__device__ __forceinline__ double dmid(const double *g, int m) { return __ddiv_rn(__dadd_rn(g[m], g[m + 1]), 2.0); }
+
+// component-aligned axis: the node interval of the cell (clamped), weights
+// from the node positions
+__device__ __forceinline__ void ax_node(const double *g, int n, int cell, double x, int &lo, double &w0, double &w1)
+{
+    lo = cell;
+    if (lo < 0) lo = 0;
+    if (lo > n - 2) lo = n - 2;
+    const double d = __dsub_rn(g[lo + 1], g[lo]);
+    w0 = __dsub_rn(1.0, -__ddiv_rn(__dsub_rn(g[lo], x), d));
+    w1 = __dsub_rn(1.0, __ddiv_rn(__dsub_rn(g[lo + 1], x), d));
+}
+
+// cross axis: cell mid-points (staggered), point clamped onto the first or
+// last mid-point outside the interior range
+__device__ __forceinline__ void ax_mid(const double *g, int n, int cell, double x, int &lo, double &w0, double &w1)
+{
+    lo = cell;
+    double X = x;
+    if (X < dmid(g, lo)) lo -= 1;
+    if (lo < 0) { lo = 0; X = dmid(g, 0); }
+    if (lo > n - 3) { lo = n - 3; X = dmid(g, lo + 1); }
+    const double d = __ddiv_rn(__dsub_rn(g[lo + 2], g[lo]), 2.0);
+    w0 = __dsub_rn(1.0, -__ddiv_rn(__dsub_rn(dmid(g, lo), X), d));
+    w1 = __dsub_rn(1.0, __ddiv_rn(__dsub_rn(dmid(g, lo + 1), X), d));
+}
+
+__device__ void vxyz_at(const Grid3 &G, const float *vx, const float *vy, const float *vz, double x, double y,
+                        double z, double out[3])
+{
+    const double p[3] = {x < 0 ? 0.0 : (x > G.size[0] ? G.size[0] : x), y < 0 ? 0.0 : (y > G.size[1] ? G.size[1] : y),
+                         z < 0 ? 0.0 : (z > G.size[2] ? G.size[2] : z)};
+    int cell[3];
+    for (int a = 0; a < 3; a++) cell[a] = serch(G.g[a], G.n[a], p[a]);
+    const long nxy = (long)G.n[0] * G.n[1], ny = G.n[1];
+    const float *v[3] = {vx, vy, vz};
+    for (int comp = 0; comp < 3; comp++) {
+        int lo[3];
+        double w[3][2];
+        for (int a = 0; a < 3; a++) {
+            if (a == comp) ax_node(G.g[a], G.n[a], cell[a], p[a], lo[a], w[a][0], w[a][1]);
+            else ax_mid(G.g[a], G.n[a], cell[a], p[a], lo[a], w[a][0], w[a][1]);
+        }
+        // accumulation order of the reference: z outer, x, y inner
+        double s = 0;
+        for (int c = 0; c < 2; c++)
+            for (int a = 0; a < 2; a++)
+                for (int b = 0; b < 2; b++) {
+                    const long idx = (long)(lo[2] + c) * nxy + (long)(lo[0] + a) * ny + (lo[1] + b);
+                    const double swt = __dmul_rn(__dmul_rn(w[0][a], w[1][b]), w[2][c]);
+                    s = __dadd_rn(s, __dmul_rn((double)v[comp][idx], swt));
+                }
+        out[comp] = s;
+    }
+}
+
+__global__ void k_movemark(long nmark, Grid3 G, const float *vx, const float *vy, const float *vz, float *mx,
+                           float *my, float *mz, const signed char *mt, double dt, int markmod, int outgrid)
+{
+    long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= nmark) return;
+    const float fx = mx[q], fy = my[q], fz = mz[q];
+    const int t = mt[q];
+    const bool inside = fx >= 0 && fy >= 0 && fz >= 0 && (double)fx <= G.size[0] && (double)fy <= G.size[1] &&
+                        (double)fz <= G.size[2];
+    if (!(inside || (outgrid != 1 && (t < 50 || t >= 100)))) return;
+    double v1[3], v2[3], v3[3], v4[3], v[3];
+    vxyz_at(G, vx, vy, vz, fx, fy, fz, v1);
+    if (markmod == 1) {  // velocity at the marker (mark3mg.c:317-323)
+        for (int a = 0; a < 3; a++) v[a] = v1[a];
+    } else {
+        vxyz_at(G, vx, vy, vz, __dadd_rn((double)fx, __ddiv_rn(__dmul_rn(v1[0], dt), 2.0)),
+                __dadd_rn((double)fy, __ddiv_rn(__dmul_rn(v1[1], dt), 2.0)),
+                __dadd_rn((double)fz, __ddiv_rn(__dmul_rn(v1[2], dt), 2.0)), v2);
+        vxyz_at(G, vx, vy, vz, __dadd_rn((double)fx, __ddiv_rn(__dmul_rn(v2[0], dt), 2.0)),
+                __dadd_rn((double)fy, __ddiv_rn(__dmul_rn(v2[1], dt), 2.0)),
+                __dadd_rn((double)fz, __ddiv_rn(__dmul_rn(v2[2], dt), 2.0)), v3);
+        vxyz_at(G, vx, vy, vz, __dadd_rn((double)fx, __dmul_rn(v3[0], dt)), __dadd_rn((double)fy, __dmul_rn(v3[1], dt)),
+                __dadd_rn((double)fz, __dmul_rn(v3[2], dt)), v4);
+        for (int a = 0; a < 3; a++)
+            v[a] = __ddiv_rn(__dadd_rn(__dadd_rn(__dadd_rn(v1[a], __dmul_rn(2.0, v2[a])), __dmul_rn(2.0, v3[a])), v4[a]),
+                             6.0);
+    }
+    if (outgrid == 2) {  // orthogonal motion only outside the box (mark3mg.c:437-459, non-periodic)
+        if (fx < 0 || (double)fx > G.size[0]) v[1] = v[2] = 0;
+        if (fy < 0 || (double)fy > G.size[1]) v[0] = v[2] = 0;
+        if (fz < 0 || (double)fz > G.size[2]) v[0] = v[1] = 0;
+    }
+    mx[q] = __double2float_rn(__dadd_rn((double)fx, __dmul_rn(dt, v[0])));
+    my[q] = __double2float_rn(__dadd_rn((double)fy, __dmul_rn(dt, v[1])));
+    mz[q] = __double2float_rn(__dadd_rn((double)fz, __dmul_rn(dt, v[2])));
+}
+
+// float velocities of the resident FP64 solution, zero at positions that are
+// not unknowns (what p2_get_solution hands back)
+__global__ void k_velocity_f32(int nx, int ny, int nz, const double *vx, const double *vy, const double *vz,
+                               float *ox, float *oy, float *oz)
+{
+    long u = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (u >= (long)nx * ny * nz) return;
+    int j = (int)(u % ny), i = (int)((u / ny) % nx), k = (int)(u / ((long)nx * ny));
+    ox[u] = valid_pos(1, i, j, k, nx, ny, nz) ? (float)vx[u] : 0.f;
+    oy[u] = valid_pos(2, i, j, k, nx, ny, nz) ? (float)vy[u] : 0.f;
+    oz[u] = valid_pos(3, i, j, k, nx, ny, nz) ? (float)vz[u] : 0.f;
+}
+
+Grid3 Solver::grid3() const
+{
+    const Level &L0 = L[0];
+    Grid3 G;
+    for (int a = 0; a < 3; a++) {
+        G.g[a] = d_g[a];
+        G.size[a] = L0.g[a].back() - L0.g[a].front();
+    }
+    G.n[0] = L0.nx; G.n[1] = L0.ny; G.n[2] = L0.nz;
+    return G;
+}
+
+void Solver::ensure_move_buffers(long nmark)
+{
+    const Level &L0 = L[0];
+    if (!d_g[0]) {
+        for (int q = 0; q < 3; q++) {
+            d_g[q] = (double *)grid_arena.alloc(sizeof(double) * L0.g[q].size());
+            P2_CUDA_TRY(cudaMemcpy(d_g[q], L0.g[q].data(), sizeof(double) * L0.g[q].size(), cudaMemcpyHostToDevice));
+        }
+    }
+    if (!mv_vel[0]) {
+        for (int q = 0; q < 3; q++) mv_vel[q] = (float *)grid_arena.alloc(sizeof(float) * L0.n);
+    }
+    if (nmark > mv_cap) {
+        move_arena.release();
+        mv_cap = std::max<long>(nmark, 1);
+        for (int q = 0; q < 3; q++) mv_pos[q] = (float *)move_arena.alloc(sizeof(float) * mv_cap);
+        mv_type = (signed char *)move_arena.alloc(mv_cap);
+    }
+}
+
+// movemark() on host arrays: velocities vx, vy, vz (float, node layout) and
+// markers in/out.
+void Solver::movemark_host(double dt, int markmod, int outgrid, const float *vx, const float *vy, const float *vz, long nmark,
+                           float *mx, float *my, float *mz, const signed char *mt)
+{
+    if (!grid_ready) throw Error(P2_ERR_STATE, "movemark before p2_set_grid");
+    if (nmark < 0 || nmark > 0x7fffffffL) throw Error(P2_ERR_ARG, "marker count out of range");
+    if (!(dt >= 0) || !std::isfinite(dt)) throw Error(P2_ERR_ARG, "time step must be finite and >= 0");
+    if (outgrid < 0 || outgrid > 2) throw Error(P2_ERR_ARG, "outgrid must be 0, 1 or 2");
+    if (markmod != 1 && markmod != 2) throw Error(P2_ERR_ARG, "markmod must be 1 (simple) or 2 (Runge-Kutta 4)");
+    ensure_move_buffers(nmark);
+    const Level &L0 = L[0];
+    const float *src[3] = {vx, vy, vz};
+    for (int q = 0; q < 3; q++)
+        P2_CUDA_TRY(cudaMemcpyAsync(mv_vel[q], src[q], sizeof(float) * L0.n, cudaMemcpyHostToDevice, st));
+    if (nmark > 0) {
+        float *pos[3] = {mx, my, mz};
+        for (int q = 0; q < 3; q++)
+            P2_CUDA_TRY(cudaMemcpyAsync(mv_pos[q], pos[q], sizeof(float) * nmark, cudaMemcpyHostToDevice, st));
+        P2_CUDA_TRY(cudaMemcpyAsync(mv_type, mt, nmark, cudaMemcpyHostToDevice, st));
+        k_movemark<<<nb(nmark), 256, 0, st>>>(nmark, grid3(), mv_vel[0], mv_vel[1], mv_vel[2], mv_pos[0], mv_pos[1],
+                                              mv_pos[2], mv_type, dt, markmod, outgrid); P2_COUNT_LAUNCH();
+        P2_CUDA_TRY(cudaGetLastError());
+        for (int q = 0; q < 3; q++)
+            P2_CUDA_TRY(cudaMemcpyAsync(pos[q], mv_pos[q], sizeof(float) * nmark, cudaMemcpyDeviceToHost, st));
+    }
+    P2_CUDA_TRY(cudaStreamSynchronize(st));
+}
+
+// movemark() on the resident markers with the resident solution.
+void Solver::movemark_device(double dt, int markmod, int outgrid)
+{
+    if (!markers_ready) throw Error(P2_ERR_STATE, "movemark before markers were uploaded");
+    if (!solution_ready) throw Error(P2_ERR_STATE, "movemark before a solve");
+    if (!(dt >= 0) || !std::isfinite(dt)) throw Error(P2_ERR_ARG, "time step must be finite and >= 0");
+    if (outgrid < 0 || outgrid > 2) throw Error(P2_ERR_ARG, "outgrid must be 0, 1 or 2");
+    if (markmod != 1 && markmod != 2) throw Error(P2_ERR_ARG, "markmod must be 1 (simple) or 2 (Runge-Kutta 4)");
+    ensure_move_buffers(0);
+    const Level &L0 = L[0];
+    k_velocity_f32<<<nb(L0.n), 256, 0, st>>>(L0.nx, L0.ny, L0.nz, gx.c[1], gx.c[2], gx.c[3], mv_vel[0],
+                                             mv_vel[1], mv_vel[2]); P2_COUNT_LAUNCH();
+    if (nmk > 0) {
+        k_movemark<<<nb(nmk), 256, 0, st>>>(nmk, grid3(), mv_vel[0], mv_vel[1], mv_vel[2], mk_x, mk_y, mk_z, mk_t, dt,
+                                            markmod, outgrid); P2_COUNT_LAUNCH();
+    }
+    P2_CUDA_TRY(cudaGetLastError());
+}
+
+void Solver::get_markers(float *mx, float *my, float *mz)
+{
+    if (!markers_ready) throw Error(P2_ERR_STATE, "no resident markers");
+    float *dst[3] = {mx, my, mz}, *src[3] = {mk_x, mk_y, mk_z};
+    for (int q = 0; q < 3; q++)
+        if (dst[q] && nmk > 0)
+            P2_CUDA_TRY(cudaMemcpyAsync(dst[q], src[q], sizeof(float) * nmk, cudaMemcpyDeviceToHost, st));
+    P2_CUDA_TRY(cudaStreamSynchronize(st));
+}
+
+// ---------------------------------------------------------------------------
 void Solver::upload_markers(long nmark, const float *mx, const float *my, const float *mz, const signed char *mt,
                             int nrock, const double *n0, const double *n1, const double *rho)
 {

@@ -173,6 +173,7 @@ Solver::~Solver()
     arena.release();
     grid_arena.release();
     marker_arena.release();
+    move_arena.release();
     for (int i = 0; i < 8; i++) cudaEventDestroy(ev[i]);
     if (st) cudaStreamDestroy(st);
 }
@@ -220,8 +221,14 @@ void Solver::set_grid(long nx, long ny, long nz, const double *gx, const double 
     drop_graphs();
     arena.release();
     grid_arena.release();
+    marker_arena.release();  // markers and their buffers belong to the previous grid
+    move_arena.release();
+    mv_cap = 0;
+    for (int q = 0; q < 3; q++) { d_g[q] = nullptr; mv_vel[q] = nullptr; mv_pos[q] = nullptr; }
+    for (int q = 0; q < 6; q++) mk_nodes[q] = nullptr;
+    mv_type = nullptr;
     prm = p;
-    bc_ready = nodes_ready = false;
+    bc_ready = nodes_ready = markers_ready = solution_ready = false;
     L.clear();
     int nl = p.multinum + 1;
     L.resize(nl);
@@ -998,6 +1005,7 @@ p2_solve_info Solver::solve()
     float tt = 0, ts = 0;
     P2_CUDA_TRY(cudaEventElapsedTime(&tt, ev[0], ev[4]));
     P2_CUDA_TRY(cudaEventElapsedTime(&ts, ev[0], ev[1]));
+    solution_ready = true;
     info.iterations = it;
     info.rel_residual = rel;
     info.ms_total = tt;

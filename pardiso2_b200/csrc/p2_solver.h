@@ -78,6 +78,10 @@ class Solver {
     void upload_markers(long nmark, const float *mx, const float *my, const float *mz, const signed char *mt,
                         int nrock, const double *n0, const double *n1, const double *rho);
     void ronurecalc_device();
+    void movemark_host(double dt, int markmod, int outgrid, const float *vx, const float *vy, const float *vz, long nmark,
+                       float *mx, float *my, float *mz, const signed char *mt);
+    void movemark_device(double dt, int markmod, int outgrid);
+    void get_markers(float *mx, float *my, float *mz);
 
     // test hooks (FP64, interleaved [P,Vx,Vy,Vz] per node)
     void debug_apply(int l, const double *x, double *y);
@@ -94,7 +98,7 @@ class Solver {
     p2_params prm{};
     std::vector<Level> L;
     long total_nodes = 0;
-    bool grid_ready = false, bc_ready = false, nodes_ready = false, markers_ready = false;
+    bool grid_ready = false, bc_ready = false, nodes_ready = false, markers_ready = false, solution_ready = false;
     RawFields f0;
 
     // markers
@@ -108,6 +112,11 @@ class Solver {
     double *rock_f = nullptr, *rock_ro = nullptr;
     double *d_g[3] = {nullptr, nullptr, nullptr};
     float *mk_nodes[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    // marker advection: float velocities and host-path marker buffers
+    float *mv_vel[3] = {nullptr, nullptr, nullptr};
+    float *mv_pos[3] = {nullptr, nullptr, nullptr};
+    signed char *mv_type = nullptr;
+    long mv_cap = 0;
 
   private:
     template <typename T>
@@ -133,8 +142,10 @@ class Solver {
     void rows0(const Vec4<double> &x, Vec4<double> &out, Vec4<float> *r32, int mode);
     void precondition(Vec4<double> &z);
     void debug_prepare();
+    Grid3 grid3() const;
+    void ensure_move_buffers(long nmark);
 
-    DeviceArena arena, grid_arena, marker_arena;
+    DeviceArena arena, grid_arena, marker_arena, move_arena;
     std::array<GraphSlot, 2> graphs;
     LuGraph lu_graph;  // coarsest LU + inverse launch sequence
     int restart = 8;

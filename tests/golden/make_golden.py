@@ -15,6 +15,12 @@ models and stores, per case:
                                     reference's level-0 system (direct sparse
                                     LU of its assembled rows, pressure reset
                                     to pinit at the pinned cell)
+and, in move17.npz, marker advection by the reference's movemark()
+(pardiso/mark3mg.c:174) through the float sphere17 solution velocities:
+  in_{x,y,z,t}, vx, vy, vz, dt      markers (some outside the box, types 0,
+                                    1, 60, 110) and the inputs of the step
+  out_<variant>_{x,y,z,k}           positions and markk after one step, for
+                                    variants (markmod, outgrid) in MOVE_VARIANTS
 
 Usage: OMP_NUM_THREADS=1 python tests/golden/make_golden.py
 """
@@ -37,6 +43,26 @@ CASES = {
     "spheres21": lambda: M.random_spheres_model(21, 2, 4, (1e-2, 1e2), markers=(2, 2, 2), seed=7,
                                                 name="spheres21"),
 }
+
+
+MOVE_VARIANTS = {"rk4_og0": (2, 0), "rk4_og1": (2, 1), "rk4_og2": (2, 2), "simple_og0": (1, 0)}
+
+
+def move_markers(m):
+    """Marker set for the movemark vectors: the model's markers, every 7th
+    pushed outside the box along one axis, types 60 (moved only inside) and
+    110 (immobile class, moved anywhere) mixed in."""
+    x, y, z = (np.array(a, np.float32) for a in (m.markx, m.marky, m.markz))
+    t = np.array(m.markt, np.int8)
+    q = np.arange(x.size)
+    for a, arr in enumerate((x, y, z)):
+        sel = (q % 7 == 0) & ((q // 7) % 3 == a)
+        lo = (q // 21) % 2 == 0
+        arr[sel & lo] = np.float32(-0.03) * arr[sel & lo]
+        arr[sel & ~lo] = np.float32(1.0) + np.float32(0.03) * arr[sel & ~lo]
+    t[q % 5 == 1] = 60
+    t[q % 11 == 2] = 110
+    return x, y, z, t
 
 
 def probe_vector(n_nodes: int, salt: int) -> np.ndarray:
@@ -117,11 +143,37 @@ def make_case(name, builder):
     print(name, "written", {k: np.asarray(v).shape for k, v in out.items()})
 
 
+def make_move_case():
+    """move17.npz: movemark() of the reference on sphere17's solution."""
+    from oracle import refdrv
+    src = np.load(os.path.join(HERE, "sphere17.npz"))
+    m = M.sphere_model(17, 2, (1, 1, 1), seed=3, eta_sphere=1e3)
+    vel = [np.asarray(src["sol_" + k], np.float32) for k in ("vx", "vy", "vz")]
+    h = 1.0 / 16
+    dt = 1.5 * h / max(float(np.abs(v).max()) for v in vel)
+    mx, my, mz, mt = move_markers(m)
+    r = refdrv.RefModel(m)
+    r.set_velocity(*vel)
+    out = {"in_x": mx, "in_y": my, "in_z": mz, "in_t": mt, "vx": vel[0], "vy": vel[1], "vz": vel[2],
+           "dt": np.array(dt)}
+    for name, (mmod, og) in MOVE_VARIANTS.items():
+        r.set_markers(mx, my, mz, mt)
+        r.fill_markk(300.0)
+        r.movemark(dt, mmod, og)
+        for k, a in zip("xyzk", r.markers()):
+            out["out_%s_%s" % (name, k)] = a
+    np.savez_compressed(os.path.join(HERE, "move17.npz"), **out)
+    print("move17 written", {k: np.asarray(v).shape for k, v in out.items()})
+
+
 if __name__ == "__main__":
     # the reference keeps its state in globals: one case per process
     if len(sys.argv) > 1:
-        make_case(sys.argv[1], CASES[sys.argv[1]])
+        if sys.argv[1] == "move17":
+            make_move_case()
+        else:
+            make_case(sys.argv[1], CASES[sys.argv[1]])
     else:
         import subprocess
-        for c in CASES:
+        for c in list(CASES) + ["move17"]:
             subprocess.run([sys.executable, os.path.abspath(__file__), c], check=True)

@@ -2,11 +2,13 @@
 
 The reference's own state (its globals, pardiso/head3mg.c, set up by the
 reference harness in oracle/ref/ref_harness.c) is driven through vpiterate()
-and ronurecalc() taken from pardiso2_b200/csrc/move3mg_cuda.c, the shim that
-replaces the reference's CPU functions and calls libp2cuda.so on the GPU.
-The arrays the shim writes back into the reference's globals (nu..nyz;
-vx, vy, vz as float and pr as double) must equal the golden vectors: node
-fields bit for bit, solutions within 1e-6 relative L2.
+ronurecalc() and movemark() taken from pardiso2_b200/csrc/move3mg_cuda.c, the
+shim that replaces the reference's CPU functions and calls libp2cuda.so on
+the GPU.  The arrays the shim writes back into the reference's globals
+(nu..nyz; vx, vy, vz as float and pr as double; markx, marky, markz, markk)
+must equal the golden vectors: node fields bit for bit, solutions within 1e-6
+relative L2; moved markers bit for bit with the oracle's movemark, which the
+CPU suite pins to the reference's own.
 
 Needs oracle/_ref/libp2ref_shim.so, built with the reference sources by
 `make -C oracle refshim`; skipped when it is absent.
@@ -15,13 +17,14 @@ import numpy as np
 import pytest
 
 from oracle import refdrv
+from tests.golden.make_golden import move_markers
 from tests.test_oracle_golden import load_case, rel
 
 pytestmark = pytest.mark.gpu
 FIELDS = ("nu", "ro", "nxx", "nxy", "nxz", "nyz")
 
 
-def test_vpiterate_and_ronurecalc_through_the_reference_globals():
+def test_vpiterate_ronurecalc_movemark_through_the_reference_globals(oracle_mod):
     if not refdrv.available(shim=True):
         pytest.skip("oracle/_ref/libp2ref_shim.so not built")
     m, g = load_case("spheres21")
@@ -37,3 +40,15 @@ def test_vpiterate_and_ronurecalc_through_the_reference_globals():
     for k in ("vx", "vy", "vz", "pr"):
         e = rel(w[k].astype(np.float64), g["sol_" + k])
         assert e < 1e-6, (k, e)
+    # the shim's movemark() -> p2_movemark on the velocities vpiterate wrote
+    mx, my, mz, mt = move_markers(m)
+    vel = (w["vx"], w["vy"], w["vz"])
+    dt = 1.5 / 20 / max(float(np.abs(v).max()) for v in vel)
+    r.set_markers(mx, my, mz, mt)
+    r.fill_markk(300.0)
+    r.movemark(dt, 2, 0)
+    got = r.markers()
+    ref = oracle_mod.movemark(m, vel, dt, 2, 0, markers=(mx, my, mz, mt), markk=np.full(mx.size, 300.0, np.float32))
+    for a, b, c in zip(got, ref, "xyzk"):
+        assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), c
+    assert int((got[3] == 0).sum()) > 0

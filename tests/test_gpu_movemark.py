@@ -1,0 +1,77 @@
+"""Marker advection (movemark, pardiso/mark3mg.c:174) on the GPU.
+
+Bit-exact bar: the moved marker coordinates (float) equal the reference's
+for every marker, through the host-array entry point (against the golden
+vectors the reference itself produced, tests/golden/move17.npz) and through
+the resident path after a resident solve (against the oracle restatement,
+which the CPU suite pins to the same golden vectors).
+"""
+import os
+
+import numpy as np
+import pytest
+
+import pardiso2_b200 as P
+from pardiso2_b200.capi import P2Error
+from pardiso2_b200 import model as M
+from tests.golden.make_golden import MOVE_VARIANTS, move_markers
+
+pytestmark = pytest.mark.gpu
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+@pytest.fixture(scope="module")
+def move17():
+    g = np.load(os.path.join(GOLDEN, "move17.npz"))
+    m = M.sphere_model(17, 2, (1, 1, 1), seed=3, eta_sphere=1e3)
+    prob = P.StokesProblem(m)
+    yield g, prob
+    prob.close()
+
+
+@pytest.mark.parametrize("variant", sorted(MOVE_VARIANTS))
+def test_movemark_host_arrays_vs_reference_golden(move17, variant):
+    g, prob = move17
+    markmod, outgrid = MOVE_VARIANTS[variant]
+    x, y, z = prob.ctx.movemark(float(g["dt"]), g["vx"], g["vy"], g["vz"], g["in_x"], g["in_y"], g["in_z"],
+                                g["in_t"], markmod=markmod, outgrid=outgrid)
+    for a, c in zip((x, y, z), "xyz"):
+        ref = g["out_%s_%s" % (variant, c)]
+        bad = np.flatnonzero(a.view(np.uint32) != ref.view(np.uint32))
+        assert bad.size == 0, (variant, c, bad[:5], a[bad[:5]], ref[bad[:5]])
+
+
+def test_movemark_zero_markers_and_bad_arguments(move17):
+    g, prob = move17
+    e = np.zeros(0, np.float32)
+    assert [a.size for a in prob.ctx.movemark(1.0, g["vx"], g["vy"], g["vz"], e, e, e, np.zeros(0, np.int8))] == [0] * 3
+    with pytest.raises(P2Error):
+        prob.ctx.movemark(1.0, g["vx"], g["vy"], g["vz"], g["in_x"], g["in_y"], g["in_z"], g["in_t"], markmod=3)
+    with pytest.raises(P2Error):
+        prob.ctx.movemark(float("nan"), g["vx"], g["vy"], g["vz"], g["in_x"], g["in_y"], g["in_z"], g["in_t"])
+
+
+@pytest.mark.parametrize("variant", ["rk4_og0", "rk4_og2"])
+def test_movemark_resident_after_resident_solve_vs_oracle(oracle_mod, variant):
+    """33^3, 4 spheres, 8 markers per cell (some outside, mixed types):
+    upload, ronurecalc, solve and advect on the device; the oracle advects
+    the same markers through the float cast of the FP64 solution."""
+    markmod, outgrid = MOVE_VARIANTS[variant]
+    m = M.random_spheres_model(33, 2, 4, (1e-2, 1e2), markers=(2, 2, 2), seed=5, name="move33")
+    mx, my, mz, mt = move_markers(m)
+    prob = P.StokesProblem(m, tol=1e-8)
+    r = m.rocks
+    prob.ctx.upload_markers(mx, my, mz, mt, r.n0, r.n1, r.ro)
+    prob.ctx.ronurecalc_resident()
+    info = prob.ctx.solve_resident()
+    assert info.status == 0
+    sol = prob.ctx.solution(m.nodenum)
+    vel = tuple(np.asarray(sol[k], np.float32) for k in ("vx", "vy", "vz"))
+    dt = 1.2 / 32 / max(float(np.abs(v).max()) for v in vel)
+    prob.ctx.movemark_resident(dt, markmod=markmod, outgrid=outgrid)
+    got = prob.ctx.get_markers(mx.size)
+    prob.close()
+    ref = oracle_mod.movemark(m, vel, dt, markmod, outgrid, markers=(mx, my, mz, mt))
+    for a, b, c in zip(got, ref, "xyz"):
+        assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), c
+    assert int(((got[0] != mx) | (got[1] != my) | (got[2] != mz)).sum()) > mx.size // 2

@@ -129,3 +129,20 @@ def test_live_reference_ronurecalc_and_rows(oracle_mod):
     has[row] = True
     y = s.apply(0, x)
     assert np.abs(y - ref)[has].max() < 1e-13 * np.abs(ref[has]).max()
+
+
+@pytest.mark.parametrize("variant", ["rk4_og0", "rk4_og1", "rk4_og2", "simple_og0"])
+def test_oracle_movemark_vs_reference_golden(oracle_mod, variant):
+    """Marker advection (movemark, mark3mg.c:174): positions and the markk
+    reset bit-exact with the reference's own run (move17.npz)."""
+    from tests.golden.make_golden import MOVE_VARIANTS
+    g = np.load(os.path.join(GOLDEN, "move17.npz"))
+    m = M.sphere_model(17, 2, (1, 1, 1), seed=3, eta_sphere=1e3)
+    markmod, outgrid = MOVE_VARIANTS[variant]
+    ins = (g["in_x"], g["in_y"], g["in_z"], g["in_t"])
+    out = oracle_mod.movemark(m, (g["vx"], g["vy"], g["vz"]), float(g["dt"]), markmod, outgrid, markers=ins,
+                              markk=np.full(ins[0].size, 300.0, np.float32))
+    for a, c in zip(out, "xyzk"):
+        assert np.array_equal(a.view(np.uint32), g["out_%s_%s" % (variant, c)].view(np.uint32)), c
+    moved = (out[0] != ins[0]) | (out[1] != ins[1]) | (out[2] != ins[2])
+    assert moved.sum() > ins[0].size // 2
