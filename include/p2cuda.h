@@ -173,6 +173,19 @@ p2_status p2_movemark(p2_ctx *ctx, double timestep, int markmod, int outgrid, co
 p2_status p2_movemark_resident(p2_ctx *ctx, double timestep, int markmod, int outgrid, double *ms);
 p2_status p2_get_markers(p2_ctx *ctx, float *markx, float *marky, float *markz);
 
+/* The post-solve fields of vpiterate (pardiso/move3mgNew.c:2908-3038):
+ * deviatoric stresses sxx..syz and strain rates exx..eyz on level 0 from the
+ * last solution's velocities rounded to float (what p2_stokes_solve returns)
+ * and the resident node viscosities clamped to [nubeg, nuend], bit-identical
+ * to the reference's value-mode stencils (sxxcalc .. syzcalc, ynval = 0).
+ * Arrays are in/out host arrays in the node layout: positions the reference
+ * does not write keep their values; a null pointer skips that field.
+ * vrange (may be null) receives {min vx, max vx, min vy, max vy, min vz,
+ * max vz} over the valid velocity positions, from which vpiterate limits the
+ * marker time step (move3mgNew.c:3293-3316). */
+p2_status p2_stress_strain(p2_ctx *ctx, float *sxx, float *syy, float *szz, float *sxy, float *sxz, float *syz,
+                           float *exx, float *eyy, float *ezz, float *exy, float *exz, float *eyz, double vrange[6]);
+
 /* The p2_ronurecalc interpolation for callers that cannot allocate device
  * memory: a host code whose device memory is all handed out by its own pool
  * at start-up, or one that cannot take the device-wide synchronisation that

@@ -49,8 +49,27 @@ def lib() -> C.CDLL:
                                      _dp, _dp, C.c_double, C.c_double, C.c_double, C.c_int] + [_fp] * 6
         L.p2o_movemark.argtypes = [C.c_int, C.c_int, C.c_int, _dp, _dp, _dp, _fp, _fp, _fp, C.c_double, C.c_int,
                                    C.c_int, C.c_long, _fp, _fp, _fp, _bp, C.c_void_p]
+        L.p2o_stress_strain.argtypes = [C.c_int, C.c_int, C.c_int, _dp, _dp, _dp] + [_fp] * 7 + [
+            C.c_double, C.c_double, C.POINTER(C.c_void_p)]
         _lib = L
     return _lib
+
+
+STRESS_KEYS = ("sxx", "syy", "szz", "sxy", "sxz", "syz", "exx", "eyy", "ezz", "exy", "exz", "eyz")
+
+
+def stress_strain(model, vel, nodes, init=0.0):
+    """Post-solve stresses and strain rates by the oracle (dict of float32
+    arrays; positions the reference does not write hold init)."""
+    L = lib()
+    nx, ny, nz = model.shape
+    out = {k: np.full(model.nodenum, init, np.float32) for k in STRESS_KEYS}
+    arr = (C.c_void_p * 12)(*[out[k].ctypes.data for k in STRESS_KEYS])
+    f = [np.ascontiguousarray(a, np.float32) for a in vel] + [np.ascontiguousarray(nodes[k], np.float32)
+                                                             for k in ("nxx", "nxy", "nxz", "nyz")]
+    p = model.params
+    L.p2o_stress_strain(nx, ny, nz, model.gx, model.gy, model.gz, *f, p.nubeg, p.nuend, arr)
+    return out
 
 
 def ronurecalc(model, init=None):

@@ -22,6 +22,7 @@
  *   nu/ro restriction .................... pardiso/move3mgNew.c:3386-3527
  *   pressure reset to pinit .............. pardiso/move3mgNew.c:2834-2855
  *   marker -> node interpolation ......... pardiso/mark3mg.c:630-1133
+ *   stresses / strain rates after a solve  pardiso/move3mgNew.c:2908-3038
  *   marker advection (RK4 / simple) ...... pardiso/mark3mg.c:174-629, with
  *     the staggered velocity interpolation vxyzcalc1 2963-3243
  *     (cell search m1serch..m3serch 1138-1204, constant rock viscosity
@@ -1611,6 +1612,71 @@ void p2o_movemark(int nx, int ny, int nz, const double *gx, const double *gy, co
              (double)mz[q] > G.size[2]))
             markk[q] = 0;
     }
+}
+
+/* ---------------------------------------------------------------------- */
+/* Post-solve stresses and strain rates (vpiterate, move3mgNew.c:2908-3038, */
+/* value mode of sxxcalc..syzcalc 3-794), non-periodic box.                */
+static double st_nu(float v, double nubeg, double nuend)
+{
+    double n = v;
+    if (n > nuend) n = nuend;
+    if (n < nubeg) n = nubeg;
+    return n;
+}
+
+/* float difference first, then scaled in double */
+static double st_d(float a, float b, double kf)
+{
+    float d = a - b;
+    return (double)d * kf;
+}
+
+static void st_put(float **out, int q, long u, double left, double nueff)
+{
+    out[6 + q][u] = (float)left;
+    out[q][u] = (float)(2.0 * nueff * left);
+}
+
+/* out: sxx syy szz sxy sxz syz exx eyy ezz exy exz eyz (float[nodenum]);
+ * positions the reference does not write are left alone. */
+void p2o_stress_strain(int nx, int ny, int nz, const double *gx, const double *gy, const double *gz, const float *vx,
+                       const float *vy, const float *vz, const float *nxx, const float *nxy, const float *nxz,
+                       const float *nyz, double nubeg, double nuend, float **out)
+{
+    long nxy_ = (long)nx * ny, u;
+    int i, j, k;
+    for (k = 0; k < nz; k++)
+        for (i = 0; i < nx; i++)
+            for (j = 0; j < ny; j++) {
+                u = k * nxy_ + (long)i * ny + j;
+                if (i > 0 && j > 0 && k > 0) {
+                    long v0 = u - nxy_ - ny - 1;
+                    double xkf = 1.0 / (gx[i] - gx[i - 1]), ykf = 1.0 / (gy[j] - gy[j - 1]);
+                    double zkf = 1.0 / (gz[k] - gz[k - 1]);
+                    double dx = st_d(vx[v0 + ny], vx[v0], xkf), dy = st_d(vy[v0 + 1], vy[v0], ykf);
+                    double dz = st_d(vz[v0 + nxy_], vz[v0], zkf);
+                    double nu = st_nu(nxx[u], nubeg, nuend);
+                    st_put(out, 0, u, dx - (dx + dy + dz) / 3.0, nu);
+                    st_put(out, 1, u, dy - (dx + dy + dz) / 3.0, nu);
+                    st_put(out, 2, u, dz - (dx + dy + dz) / 3.0, nu);
+                }
+                if (i > 0 && i < nx - 1 && j > 0 && j < ny - 1 && k < nz - 1) {
+                    double xkf = 1.0 / (gx[i + 1] - gx[i - 1]), ykf = 1.0 / (gy[j + 1] - gy[j - 1]);
+                    st_put(out, 3, u, st_d(vx[u], vx[u - 1], ykf) + st_d(vy[u], vy[u - ny], xkf),
+                           st_nu(nxy[u], nubeg, nuend));
+                }
+                if (i > 0 && i < nx - 1 && k > 0 && k < nz - 1 && j < ny - 1) {
+                    double xkf = 1.0 / (gx[i + 1] - gx[i - 1]), zkf = 1.0 / (gz[k + 1] - gz[k - 1]);
+                    st_put(out, 4, u, st_d(vx[u], vx[u - nxy_], zkf) + st_d(vz[u], vz[u - ny], xkf),
+                           st_nu(nxz[u], nubeg, nuend));
+                }
+                if (j > 0 && j < ny - 1 && k > 0 && k < nz - 1 && i < nx - 1) {
+                    double ykf = 1.0 / (gy[j + 1] - gy[j - 1]), zkf = 1.0 / (gz[k + 1] - gz[k - 1]);
+                    st_put(out, 5, u, st_d(vy[u], vy[u - nxy_], zkf) + st_d(vz[u], vz[u - 1], ykf),
+                           st_nu(nyz[u], nubeg, nuend));
+                }
+            }
 }
 
 /* Debug/test helpers: sweeps of the level-0 smoother only; two-grid count. */

@@ -345,6 +345,72 @@ double p2ref_movemark(double dt, int mmod, int og)
     return t0;
 }
 
+/* The post-solve stress / strain-rate pass of vpiterate (move3mgNew.c:
+ * 2908-3038, non-periodic branches) on the current vx, vy, vz and nxx..nyz,
+ * through the reference's own value-mode stencils (sxxcalc .. syzcalc with
+ * ynval = 0).  out: 12 float[nodenum] arrays sxx syy szz sxy sxz syz exx eyy
+ * ezz exy exz eyz; positions the reference does not write are left alone. */
+void p2ref_stress_strain(float **out)
+{
+    long m1, m2, m3, u;
+    double e1[100], ui[100];
+    long un[100];
+    int g = 0;
+    for (m3 = 0; m3 < mgz[g]; m3++)
+        for (m1 = 0; m1 < mgx[g]; m1++)
+            for (m2 = 0; m2 < mgy[g]; m2++) {
+                u = m3 * mgxy[g] + m1 * mgy[g] + m2;
+                un[0] = 0;
+                if (m1 > 0 && m2 > 0 && m3 > 0) {
+                    out[0][u] = (float)sxxcalc(m1, m2, m3, 0, g, e1, un, ui); out[6][u] = (float)e1[0];
+                    out[1][u] = (float)syycalc(m1, m2, m3, 0, g, e1, un, ui); out[7][u] = (float)e1[0];
+                    out[2][u] = (float)szzcalc(m1, m2, m3, 0, g, e1, un, ui); out[8][u] = (float)e1[0];
+                }
+                if (m1 > 0 && m1 < mgx[g] - 1 && m2 > 0 && m2 < mgy[g] - 1 && m3 < mgz[g] - 1) {
+                    out[3][u] = (float)sxycalc(m1, m2, m3, 0, g, e1, un, ui); out[9][u] = (float)e1[0];
+                }
+                if (m1 > 0 && m1 < mgx[g] - 1 && m3 > 0 && m3 < mgz[g] - 1 && m2 < mgy[g] - 1) {
+                    out[4][u] = (float)sxzcalc(m1, m2, m3, 0, g, e1, un, ui); out[10][u] = (float)e1[0];
+                }
+                if (m2 > 0 && m2 < mgy[g] - 1 && m3 > 0 && m3 < mgz[g] - 1 && m1 < mgx[g] - 1) {
+                    out[5][u] = (float)syzcalc(m1, m2, m3, 0, g, e1, un, ui); out[11][u] = (float)e1[0];
+                }
+            }
+}
+
+/* vpiterate's own stress / strain-rate globals: fill, read; step limits. */
+static float **stress_globals(float **g)
+{
+    g[0] = sxx; g[1] = syy; g[2] = szz; g[3] = sxy; g[4] = sxz; g[5] = syz;
+    g[6] = exx; g[7] = eyy; g[8] = ezz; g[9] = exy; g[10] = exz; g[11] = eyz;
+    return g;
+}
+
+void p2ref_fill_stress(float v)
+{
+    float *g[12];
+    long q, i;
+    stress_globals(g);
+    for (q = 0; q < 12; q++)
+        for (i = 0; i < nodenum; i++) g[q][i] = v;
+}
+
+void p2ref_get_stress(float **out)
+{
+    float *g[12];
+    long q;
+    stress_globals(g);
+    for (q = 0; q < 12; q++) memcpy(out[q], g[q], sizeof(float) * (size_t)nodenum);
+}
+
+void p2ref_set_step(double max_step, double ts)
+{
+    maxxystep = max_step;
+    timestep = ts;
+}
+
+double p2ref_get_timestep(void) { return timestep; }
+
 void p2ref_fill_markk(float v)
 {
     long i;

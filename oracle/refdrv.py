@@ -68,6 +68,11 @@ def _load(shim: bool = False) -> C.CDLL:
         lib.p2ref_movemark.argtypes = [C.c_double, C.c_int, C.c_int]
         lib.p2ref_movemark.restype = C.c_double
         lib.p2ref_fill_markk.argtypes = [C.c_float]
+        lib.p2ref_stress_strain.argtypes = [C.POINTER(C.c_void_p)]
+        lib.p2ref_fill_stress.argtypes = [C.c_float]
+        lib.p2ref_get_stress.argtypes = [C.POINTER(C.c_void_p)]
+        lib.p2ref_set_step.argtypes = [C.c_double, C.c_double]
+        lib.p2ref_get_timestep.restype = C.c_double
         lib.p2ref_get_markers.argtypes = [_fp] * 4
         lib.p2ref_lu_count.restype = C.c_int
         lib.p2ref_num_threads.restype = C.c_int
@@ -183,6 +188,35 @@ class RefModel:
     def movemark(self, timestep, markmod=2, outgrid=0) -> float:
         """movemark() over one step; returns its wall time (s)."""
         return self.lib.p2ref_movemark(timestep, markmod, outgrid)
+
+    STRESS_KEYS = ("sxx", "syy", "szz", "sxy", "sxz", "syz", "exx", "eyy", "ezz", "exy", "exz", "eyz")
+
+    def stress_strain(self, init=0.0):
+        """The reference's stress / strain-rate pass on its current vx, vy, vz
+        and node viscosities; untouched positions hold init."""
+        n = self.m.nodenum
+        out = {k: np.full(n, init, np.float32) for k in self.STRESS_KEYS}
+        arr = (C.c_void_p * 12)(*[out[k].ctypes.data for k in self.STRESS_KEYS])
+        self.lib.p2ref_stress_strain(arr)
+        return out
+
+    def fill_stress(self, value):
+        """Set vpiterate's stress / strain-rate globals to value everywhere."""
+        self.lib.p2ref_fill_stress(value)
+
+    def written_stress(self):
+        """vpiterate's stress / strain-rate globals (dict of float32 arrays)."""
+        n = self.m.nodenum
+        out = {k: np.zeros(n, np.float32) for k in self.STRESS_KEYS}
+        self.lib.p2ref_get_stress((C.c_void_p * 12)(*[out[k].ctypes.data for k in self.STRESS_KEYS]))
+        return out
+
+    def set_step(self, max_step, timestep):
+        """maxxystep and timestep, the inputs of vpiterate's time-step limit."""
+        self.lib.p2ref_set_step(max_step, timestep)
+
+    def timestep(self) -> float:
+        return self.lib.p2ref_get_timestep()
 
     def fill_markk(self, value):
         self.lib.p2ref_fill_markk(value)

@@ -21,7 +21,7 @@ EXPORTED = ["p2_default_params", "p2_create", "p2_destroy", "p2_last_error", "p2
             "p2_set_nodes", "p2_stokes_solve", "p2_stokes_solve_resident", "p2_get_solution", "p2_ronurecalc",
             "p2_upload_markers", "p2_ronurecalc_resident", "p2_get_nodes", "p2_debug_apply", "p2_debug_restrict",
             "p2_debug_prolong", "p2_debug_level_fields", "p2_debug_time_smoother", "p2_ronurecalc_noalloc", "p2_autotune",
-            "p2_movemark", "p2_movemark_resident", "p2_get_markers"]
+            "p2_movemark", "p2_movemark_resident", "p2_get_markers", "p2_stress_strain"]
 
 
 class Params(C.Structure):
@@ -94,7 +94,8 @@ def load() -> C.CDLL:
     L.p2_movemark.argtypes = [vp, C.c_double, C.c_int, C.c_int, _fp, _fp, _fp, C.c_long, _fp, _fp, _fp, _bp]
     L.p2_movemark_resident.argtypes = [vp, C.c_double, C.c_int, C.c_int, C.POINTER(C.c_double)]
     L.p2_get_markers.argtypes = [vp, _fp, _fp, _fp]
-    for f in ("p2_movemark", "p2_movemark_resident", "p2_get_markers"):
+    L.p2_stress_strain.argtypes = [vp] + [C.c_void_p] * 12 + [C.POINTER(C.c_double)]
+    for f in ("p2_movemark", "p2_movemark_resident", "p2_get_markers", "p2_stress_strain"):
         getattr(L, f).restype = C.c_int
     for f in ("p2_create", "p2_set_grid", "p2_set_bc", "p2_set_nodes", "p2_stokes_solve", "p2_stokes_solve_resident",
               "p2_get_solution", "p2_ronurecalc", "p2_upload_markers", "p2_ronurecalc_resident", "p2_get_nodes"):
@@ -185,6 +186,22 @@ class Context:
         out = [np.zeros(nmark, np.float32) for _ in range(3)]
         self._check(self.L.p2_get_markers(self.h, *out), "p2_get_markers")
         return out
+
+    STRESS_KEYS = ("sxx", "syy", "szz", "sxy", "sxz", "syz", "exx", "eyy", "ezz", "exy", "exz", "eyz")
+
+    def stress_strain(self, fields: Dict[str, np.ndarray]):
+        """Post-solve stresses and strain rates into float32 arrays (modified in
+        place; keys of STRESS_KEYS, missing keys skipped); returns the velocity
+        ranges (min vx, max vx, min vy, max vy, min vz, max vz)."""
+        ptrs = []
+        for k in self.STRESS_KEYS:
+            a = fields.get(k)
+            if a is not None and (a.dtype != np.float32 or not a.flags.c_contiguous):
+                raise ValueError("field %s must be a contiguous float32 array" % k)
+            ptrs.append(None if a is None else a.ctypes.data)
+        vr = (C.c_double * 6)()
+        self._check(self.L.p2_stress_strain(self.h, *ptrs, vr), "p2_stress_strain")
+        return tuple(vr)
 
     def solve_resident(self, check=True) -> SolveInfo:
         info = SolveInfo()

@@ -24,13 +24,13 @@
  * nyz, vx, vy, vz, pr, p0koef, p1koef, p2koef, v0koef, v1koef, nubeg, nuend,
  * nukoef, viscmod, GXKOEF, GYKOEF, GZKOEF, pinit, pxinit, pyinit, pzinit;
  * markers markx, marky, markz, markt, marknum and the rock tables markn0,
- * markn1, markro (rocknum types); timestep, markmod, outgrid for movemark.
- * Outputs written: vx, vy, vz (float) and pr (double) by vpiterate; nu, ro,
- * nxx, nxy, nxz, nyz by ronurecalc; markx, marky, markz and the markk reset
- * of markers that leave the box by movemark (val1 and marke, the strain-rate
- * side outputs of the CPU movemark, are not updated).  The stress and strain-rate fields and
- * the time-step limit that the CPU vpiterate also derives are not computed
- * here.
+ * markn1, markro (rocknum types); maxxystep and timestep for the time-step
+ * limit; timestep, markmod, outgrid for movemark.
+ * Outputs written: vx, vy, vz (float), pr (double), the stresses sxx..syz and
+ * strain rates exx..eyz (float) and the limited timestep by vpiterate; nu,
+ * ro, nxx, nxy, nxz, nyz by ronurecalc; markx, marky, markz and the markk
+ * reset of markers that leave the box by movemark (val1 and marke, the
+ * strain-rate side outputs of the CPU movemark, are not updated).
  *
  * Errors follow the reference's convention: a message on stdout and exit().
  * The device is 0, or the value of the environment variable P2CUDA_DEVICE.
@@ -104,6 +104,8 @@ void vpiterate(int m0, int f0)
 {
     p2_status st;
     p2_solve_info info;
+    double vr[6];
+    int c;
     (void)m0;
     (void)f0;
     p2s_setup();
@@ -111,6 +113,18 @@ void vpiterate(int m0, int f0)
     if (st != P2_OK) p2s_fail("p2_set_nodes", st);
     st = p2_stokes_solve(p2s_ctx, vx, vy, vz, pr, &info);
     if (st != P2_OK) p2s_fail("p2_stokes_solve", st);
+    /* stresses, strain rates and velocity ranges (move3mgNew.c:2908-3038) */
+    st = p2_stress_strain(p2s_ctx, sxx, syy, szz, sxy, sxz, syz, exx, eyy, ezz, exy, exz, eyz, vr);
+    if (st != P2_OK) p2s_fail("p2_stress_strain", st);
+    /* marker time step: no marker moves more than maxxystep along an axis
+       (move3mgNew.c:3293-3316) */
+    for (c = 0; c < 3; c++) {
+        double vmax = fabs(vr[2 * c]) > fabs(vr[2 * c + 1]) ? fabs(vr[2 * c]) : fabs(vr[2 * c + 1]);
+        if (vmax) {
+            vmax = maxxystep / vmax;
+            if (timestep > vmax) timestep = vmax;
+        }
+    }
     printf("vpiterate (p2cuda): %d iterations, relative residual %e, %.2f ms\n", info.iterations, info.rel_residual,
            info.ms_total);
 }

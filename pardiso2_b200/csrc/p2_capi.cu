@@ -308,6 +308,17 @@ p2_status p2_get_markers(p2_ctx *ctx, float *markx, float *marky, float *markz)
     });
 }
 
+p2_status p2_stress_strain(p2_ctx *ctx, float *sxx, float *syy, float *szz, float *sxy, float *sxz, float *syz,
+                           float *exx, float *eyy, float *ezz, float *exy, float *exz, float *eyz, double vrange[6])
+{
+    return guard(ctx, [&] {
+        P2_CUDA_TRY(cudaSetDevice(ctx->s->dev));
+        float *const s[6] = {sxx, syy, szz, sxy, sxz, syz};
+        float *const e[6] = {exx, eyy, ezz, exy, exz, eyz};
+        ctx->s->stress_strain(s, e, vrange);
+    });
+}
+
 p2_status p2_autotune(p2_ctx *ctx, int trial_iters, p2_tune_info *info)
 {
     return guard(ctx, [&] {

@@ -279,13 +279,17 @@ __global__ void k_node_gather(int nx, int ny, int nz, const double *gx, const do
 }
 
 // ---------------------------------------------------------------------------
-// Marker advection (movemark, pardiso/mark3mg.c:174-629, fourth-order
-// Runge-Kutta branch, non-periodic box): velocity at a point by staggered
-// trilinear interpolation (vxyzcalc1, mark3mg.c:2963-3243) with the
+// Marker advection (movemark, pardiso/mark3mg.c:174-629, Runge-Kutta and
+// single-velocity branches, non-periodic box): velocity at a point by
+// staggered trilinear interpolation (vxyzcalc1, mark3mg.c:2963-3243) with the
 // reference's clamping of points and cell indices at the walls, in the same
 // double arithmetic without fused multiply-adds, so positions match the
-// reference bit for bit.
-__device__ __forceinline__ double dmid(const double *g, int m) { return __ddiv_rn(__dadd_rn(g[m], g[m + 1]), 2.0); }
+// reference bit for bit.  Halvings are multiplications by 0.5 (the same
+// correctly rounded value as a division by 2).  Per stage each axis's weights
+// are computed once for the component aligned with it (node interval) and
+// once for the two others (cell mid-points); the gridlines sit in shared
+// memory for the binary searches.
+__device__ __forceinline__ double dmid(const double *g, int m) { return __dmul_rn(__dadd_rn(g[m], g[m + 1]), 0.5); }
 
 // component-aligned axis: the node interval of the cell (clamped), weights
 // from the node positions
@@ -305,46 +309,86 @@ __device__ __forceinline__ void ax_mid(const double *g, int n, int cell, double 
 {
     lo = cell;
     double X = x;
-    if (X < dmid(g, lo)) lo -= 1;
+    const double m0 = dmid(g, lo);
+    if (X < m0) lo -= 1;
     if (lo < 0) { lo = 0; X = dmid(g, 0); }
     if (lo > n - 3) { lo = n - 3; X = dmid(g, lo + 1); }
-    const double d = __ddiv_rn(__dsub_rn(g[lo + 2], g[lo]), 2.0);
+    const double d = __dmul_rn(__dsub_rn(g[lo + 2], g[lo]), 0.5);
     w0 = __dsub_rn(1.0, -__ddiv_rn(__dsub_rn(dmid(g, lo), X), d));
     w1 = __dsub_rn(1.0, __ddiv_rn(__dsub_rn(dmid(g, lo + 1), X), d));
 }
 
-__device__ void vxyz_at(const Grid3 &G, const float *vx, const float *vy, const float *vz, double x, double y,
+// gridlines of the three axes, concatenated (x, y, z)
+struct GridSh {
+    const double *g[3];
+    int n[3];
+    double size[3];
+};
+
+__device__ void vxyz_at(const GridSh &G, const float *vx, const float *vy, const float *vz, double x, double y,
                         double z, double out[3])
 {
     const double p[3] = {x < 0 ? 0.0 : (x > G.size[0] ? G.size[0] : x), y < 0 ? 0.0 : (y > G.size[1] ? G.size[1] : y),
                          z < 0 ? 0.0 : (z > G.size[2] ? G.size[2] : z)};
-    int cell[3];
-    for (int a = 0; a < 3; a++) cell[a] = serch(G.g[a], G.n[a], p[a]);
+    int lon[3], lom[3];
+    double wn[3][2], wm[3][2];
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        const int cell = serch(G.g[a], G.n[a], p[a]);
+        ax_node(G.g[a], G.n[a], cell, p[a], lon[a], wn[a][0], wn[a][1]);
+        ax_mid(G.g[a], G.n[a], cell, p[a], lom[a], wm[a][0], wm[a][1]);
+    }
     const long nxy = (long)G.n[0] * G.n[1], ny = G.n[1];
     const float *v[3] = {vx, vy, vz};
+#pragma unroll
     for (int comp = 0; comp < 3; comp++) {
         int lo[3];
         double w[3][2];
+#pragma unroll
         for (int a = 0; a < 3; a++) {
-            if (a == comp) ax_node(G.g[a], G.n[a], cell[a], p[a], lo[a], w[a][0], w[a][1]);
-            else ax_mid(G.g[a], G.n[a], cell[a], p[a], lo[a], w[a][0], w[a][1]);
+            lo[a] = a == comp ? lon[a] : lom[a];
+            w[a][0] = a == comp ? wn[a][0] : wm[a][0];
+            w[a][1] = a == comp ? wn[a][1] : wm[a][1];
         }
         // accumulation order of the reference: z outer, x, y inner
         double s = 0;
+#pragma unroll
         for (int c = 0; c < 2; c++)
+#pragma unroll
             for (int a = 0; a < 2; a++)
+#pragma unroll
                 for (int b = 0; b < 2; b++) {
                     const long idx = (long)(lo[2] + c) * nxy + (long)(lo[0] + a) * ny + (lo[1] + b);
                     const double swt = __dmul_rn(__dmul_rn(w[0][a], w[1][b]), w[2][c]);
-                    s = __dadd_rn(s, __dmul_rn((double)v[comp][idx], swt));
+                    s = __dadd_rn(s, __dmul_rn((double)__ldg(v[comp] + idx), swt));
                 }
         out[comp] = s;
     }
 }
 
-__global__ void k_movemark(long nmark, Grid3 G, const float *vx, const float *vy, const float *vz, float *mx,
-                           float *my, float *mz, const signed char *mt, double dt, int markmod, int outgrid)
+// gridlines in shared memory when they fit (kMoveShBytes), else read in place
+constexpr int kMoveThreads = 256;
+constexpr int kMoveShBytes = 96 * 1024;
+
+__global__ void __launch_bounds__(kMoveThreads, 3) k_movemark(long nmark, Grid3 G3, bool shared_grid, const float *vx,
+                                                           const float *vy, const float *vz, float *mx, float *my,
+                                                           float *mz, const signed char *mt, double dt, int markmod,
+                                                           int outgrid)
 {
+    extern __shared__ double gsh[];
+    GridSh G;
+    if (shared_grid) {
+        int off = 0;
+        for (int a = 0; a < 3; a++) {
+            for (int q = threadIdx.x; q < G3.n[a]; q += blockDim.x) gsh[off + q] = G3.g[a][q];
+            G.g[a] = gsh + off;
+            off += G3.n[a];
+        }
+        __syncthreads();
+    } else {
+        for (int a = 0; a < 3; a++) G.g[a] = G3.g[a];
+    }
+    for (int a = 0; a < 3; a++) { G.n[a] = G3.n[a]; G.size[a] = G3.size[a]; }
     long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= nmark) return;
     const float fx = mx[q], fy = my[q], fz = mz[q];
@@ -357,12 +401,13 @@ __global__ void k_movemark(long nmark, Grid3 G, const float *vx, const float *vy
     if (markmod == 1) {  // velocity at the marker (mark3mg.c:317-323)
         for (int a = 0; a < 3; a++) v[a] = v1[a];
     } else {
-        vxyz_at(G, vx, vy, vz, __dadd_rn((double)fx, __ddiv_rn(__dmul_rn(v1[0], dt), 2.0)),
-                __dadd_rn((double)fy, __ddiv_rn(__dmul_rn(v1[1], dt), 2.0)),
-                __dadd_rn((double)fz, __ddiv_rn(__dmul_rn(v1[2], dt), 2.0)), v2);
-        vxyz_at(G, vx, vy, vz, __dadd_rn((double)fx, __ddiv_rn(__dmul_rn(v2[0], dt), 2.0)),
-                __dadd_rn((double)fy, __ddiv_rn(__dmul_rn(v2[1], dt), 2.0)),
-                __dadd_rn((double)fz, __ddiv_rn(__dmul_rn(v2[2], dt), 2.0)), v3);
+        // (v dt) / 2 of the reference is v dt rounded, then halved exactly
+        vxyz_at(G, vx, vy, vz, __dadd_rn((double)fx, __dmul_rn(__dmul_rn(v1[0], dt), 0.5)),
+                __dadd_rn((double)fy, __dmul_rn(__dmul_rn(v1[1], dt), 0.5)),
+                __dadd_rn((double)fz, __dmul_rn(__dmul_rn(v1[2], dt), 0.5)), v2);
+        vxyz_at(G, vx, vy, vz, __dadd_rn((double)fx, __dmul_rn(__dmul_rn(v2[0], dt), 0.5)),
+                __dadd_rn((double)fy, __dmul_rn(__dmul_rn(v2[1], dt), 0.5)),
+                __dadd_rn((double)fz, __dmul_rn(__dmul_rn(v2[2], dt), 0.5)), v3);
         vxyz_at(G, vx, vy, vz, __dadd_rn((double)fx, __dmul_rn(v3[0], dt)), __dadd_rn((double)fy, __dmul_rn(v3[1], dt)),
                 __dadd_rn((double)fz, __dmul_rn(v3[2], dt)), v4);
         for (int a = 0; a < 3; a++)
@@ -377,6 +422,18 @@ __global__ void k_movemark(long nmark, Grid3 G, const float *vx, const float *vy
     mx[q] = __double2float_rn(__dadd_rn((double)fx, __dmul_rn(dt, v[0])));
     my[q] = __double2float_rn(__dadd_rn((double)fy, __dmul_rn(dt, v[1])));
     mz[q] = __double2float_rn(__dadd_rn((double)fz, __dmul_rn(dt, v[2])));
+}
+
+static void launch_movemark(cudaStream_t st, long nmark, const Grid3 &G, const float *const vel[3], float *const pos[3],
+                            const signed char *mt, double dt, int markmod, int outgrid)
+{
+    const size_t bytes = sizeof(double) * ((size_t)G.n[0] + G.n[1] + G.n[2]);
+    const bool sh = bytes <= (size_t)kMoveShBytes;
+    if (sh && bytes > 48 * 1024)
+        P2_CUDA_TRY(cudaFuncSetAttribute(k_movemark, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    k_movemark<<<nb(nmark, kMoveThreads), kMoveThreads, sh ? bytes : 0, st>>>(
+        nmark, G, sh, vel[0], vel[1], vel[2], pos[0], pos[1], pos[2], mt, dt, markmod, outgrid); P2_COUNT_LAUNCH();
+    P2_CUDA_TRY(cudaGetLastError());
 }
 
 // float velocities of the resident FP64 solution, zero at positions that are
@@ -424,6 +481,14 @@ void Solver::ensure_move_buffers(long nmark)
     }
 }
 
+// float copies of the resident solution velocities into mv_vel
+void Solver::velocity_f32()
+{
+    const Level &L0 = L[0];
+    k_velocity_f32<<<nb(L0.n), 256, 0, st>>>(L0.nx, L0.ny, L0.nz, gx.c[1], gx.c[2], gx.c[3], mv_vel[0],
+                                             mv_vel[1], mv_vel[2]); P2_COUNT_LAUNCH();
+}
+
 // movemark() on host arrays: velocities vx, vy, vz (float, node layout) and
 // markers in/out.
 void Solver::movemark_host(double dt, int markmod, int outgrid, const float *vx, const float *vy, const float *vz, long nmark,
@@ -444,9 +509,7 @@ void Solver::movemark_host(double dt, int markmod, int outgrid, const float *vx,
         for (int q = 0; q < 3; q++)
             P2_CUDA_TRY(cudaMemcpyAsync(mv_pos[q], pos[q], sizeof(float) * nmark, cudaMemcpyHostToDevice, st));
         P2_CUDA_TRY(cudaMemcpyAsync(mv_type, mt, nmark, cudaMemcpyHostToDevice, st));
-        k_movemark<<<nb(nmark), 256, 0, st>>>(nmark, grid3(), mv_vel[0], mv_vel[1], mv_vel[2], mv_pos[0], mv_pos[1],
-                                              mv_pos[2], mv_type, dt, markmod, outgrid); P2_COUNT_LAUNCH();
-        P2_CUDA_TRY(cudaGetLastError());
+        launch_movemark(st, nmark, grid3(), mv_vel, mv_pos, mv_type, dt, markmod, outgrid);
         for (int q = 0; q < 3; q++)
             P2_CUDA_TRY(cudaMemcpyAsync(pos[q], mv_pos[q], sizeof(float) * nmark, cudaMemcpyDeviceToHost, st));
     }
@@ -462,12 +525,10 @@ void Solver::movemark_device(double dt, int markmod, int outgrid)
     if (outgrid < 0 || outgrid > 2) throw Error(P2_ERR_ARG, "outgrid must be 0, 1 or 2");
     if (markmod != 1 && markmod != 2) throw Error(P2_ERR_ARG, "markmod must be 1 (simple) or 2 (Runge-Kutta 4)");
     ensure_move_buffers(0);
-    const Level &L0 = L[0];
-    k_velocity_f32<<<nb(L0.n), 256, 0, st>>>(L0.nx, L0.ny, L0.nz, gx.c[1], gx.c[2], gx.c[3], mv_vel[0],
-                                             mv_vel[1], mv_vel[2]); P2_COUNT_LAUNCH();
+    velocity_f32();
     if (nmk > 0) {
-        k_movemark<<<nb(nmk), 256, 0, st>>>(nmk, grid3(), mv_vel[0], mv_vel[1], mv_vel[2], mk_x, mk_y, mk_z, mk_t, dt,
-                                            markmod, outgrid); P2_COUNT_LAUNCH();
+        float *const pos[3] = {mk_x, mk_y, mk_z};
+        launch_movemark(st, nmk, grid3(), mv_vel, pos, mk_t, dt, markmod, outgrid);
     }
     P2_CUDA_TRY(cudaGetLastError());
 }

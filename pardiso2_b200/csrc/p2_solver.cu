@@ -174,6 +174,7 @@ Solver::~Solver()
     grid_arena.release();
     marker_arena.release();
     move_arena.release();
+    post_arena.release();
     for (int i = 0; i < 8; i++) cudaEventDestroy(ev[i]);
     if (st) cudaStreamDestroy(st);
 }
@@ -223,6 +224,10 @@ void Solver::set_grid(long nx, long ny, long nz, const double *gx, const double 
     grid_arena.release();
     marker_arena.release();  // markers and their buffers belong to the previous grid
     move_arena.release();
+    post_arena.release();
+    for (int q = 0; q < 12; q++) post_out[q] = nullptr;
+    post_partial = nullptr;
+    post_range = nullptr;
     mv_cap = 0;
     for (int q = 0; q < 3; q++) { d_g[q] = nullptr; mv_vel[q] = nullptr; mv_pos[q] = nullptr; }
     for (int q = 0; q < 6; q++) mk_nodes[q] = nullptr;

@@ -82,6 +82,7 @@ class Solver {
                        float *mx, float *my, float *mz, const signed char *mt);
     void movemark_device(double dt, int markmod, int outgrid);
     void get_markers(float *mx, float *my, float *mz);
+    void stress_strain(float *const s[6], float *const e[6], double vrange[6]);
 
     // test hooks (FP64, interleaved [P,Vx,Vy,Vz] per node)
     void debug_apply(int l, const double *x, double *y);
@@ -117,6 +118,10 @@ class Solver {
     float *mv_pos[3] = {nullptr, nullptr, nullptr};
     signed char *mv_type = nullptr;
     long mv_cap = 0;
+    // post-solve stress / strain-rate fields and velocity ranges
+    float *post_out[12] = {};
+    float *post_partial = nullptr;
+    double *post_range = nullptr;
 
   private:
     template <typename T>
@@ -144,8 +149,9 @@ class Solver {
     void debug_prepare();
     Grid3 grid3() const;
     void ensure_move_buffers(long nmark);
+    void velocity_f32();
 
-    DeviceArena arena, grid_arena, marker_arena, move_arena;
+    DeviceArena arena, grid_arena, marker_arena, move_arena, post_arena;
     std::array<GraphSlot, 2> graphs;
     LuGraph lu_graph;  // coarsest LU + inverse launch sequence
     int restart = 8;

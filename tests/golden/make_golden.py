@@ -21,6 +21,10 @@ and, in move17.npz, marker advection by the reference's movemark()
                                     1, 60, 110) and the inputs of the step
   out_<variant>_{x,y,z,k}           positions and markk after one step, for
                                     variants (markmod, outgrid) in MOVE_VARIANTS
+  st_{sxx..syz, exx..eyz}           the post-solve stress / strain-rate pass
+                                    of vpiterate (move3mgNew.c:2908-3038) on
+                                    those velocities and sphere17's node
+                                    fields (untouched positions hold -7)
 
 Usage: OMP_NUM_THREADS=1 python tests/golden/make_golden.py
 """
@@ -162,6 +166,9 @@ def make_move_case():
         r.movemark(dt, mmod, og)
         for k, a in zip("xyzk", r.markers()):
             out["out_%s_%s" % (name, k)] = a
+    r.set_nodes({k: src["node_" + k] for k in ("nu", "ro", "nxx", "nxy", "nxz", "nyz")})
+    for k, a in r.stress_strain(init=-7.0).items():
+        out["st_" + k] = a
     np.savez_compressed(os.path.join(HERE, "move17.npz"), **out)
     print("move17 written", {k: np.asarray(v).shape for k, v in out.items()})
 

@@ -5,10 +5,11 @@ reference harness in oracle/ref/ref_harness.c) is driven through vpiterate()
 ronurecalc() and movemark() taken from pardiso2_b200/csrc/move3mg_cuda.c, the
 shim that replaces the reference's CPU functions and calls libp2cuda.so on
 the GPU.  The arrays the shim writes back into the reference's globals
-(nu..nyz; vx, vy, vz as float and pr as double; markx, marky, markz, markk)
-must equal the golden vectors: node fields bit for bit, solutions within 1e-6
-relative L2; moved markers bit for bit with the oracle's movemark, which the
-CPU suite pins to the reference's own.
+(nu..nyz; vx, vy, vz as float and pr as double; sxx..syz, exx..eyz and
+timestep; markx, marky, markz, markk) must equal the golden vectors: node
+fields bit for bit, solutions within 1e-6 relative L2; stresses, strain
+rates, time step and moved markers bit for bit with the oracle on the
+written velocities (the CPU suite pins the oracle to the reference's own).
 
 Needs oracle/_ref/libp2ref_shim.so, built with the reference sources by
 `make -C oracle refshim`; skipped when it is absent.
@@ -18,7 +19,7 @@ import pytest
 
 from oracle import refdrv
 from tests.golden.make_golden import move_markers
-from tests.test_oracle_golden import load_case, rel
+from tests.test_oracle_golden import load_case, rel, vmax_valid
 
 pytestmark = pytest.mark.gpu
 FIELDS = ("nu", "ro", "nxx", "nxy", "nxz", "nyz")
@@ -34,15 +35,23 @@ def test_vpiterate_ronurecalc_movemark_through_the_reference_globals(oracle_mod)
     f = r.nodes()
     for k in FIELDS:
         assert np.array_equal(f[k], g["node_" + k]), k
+    r.fill_stress(-7.0)
+    r.set_step(0.01, 1e30)
     r.first_iteration()                  # the shim's vpiterate(0, 0) -> p2_stokes_solve
     w = r.written()
     assert w["vx"].dtype == np.float32 and w["pr"].dtype == np.float64
     for k in ("vx", "vy", "vz", "pr"):
         e = rel(w[k].astype(np.float64), g["sol_" + k])
         assert e < 1e-6, (k, e)
+    # stresses, strain rates (p2_stress_strain) and the time-step limit
+    vel = (w["vx"], w["vy"], w["vz"])
+    st = r.written_stress()
+    ref = oracle_mod.stress_strain(m, vel, f, init=-7.0)
+    for k in st:
+        assert np.array_equal(st[k].view(np.uint32), ref[k].view(np.uint32)), k
+    assert r.timestep() == min(0.01 / vmax_valid(m, v, c) for c, v in enumerate(vel, 1))
     # the shim's movemark() -> p2_movemark on the velocities vpiterate wrote
     mx, my, mz, mt = move_markers(m)
-    vel = (w["vx"], w["vy"], w["vz"])
     dt = 1.5 / 20 / max(float(np.abs(v).max()) for v in vel)
     r.set_markers(mx, my, mz, mt)
     r.fill_markk(300.0)

@@ -1,4 +1,5 @@
-"""Marker advection (movemark, pardiso/mark3mg.c:174) on the GPU.
+"""Marker advection (movemark, pardiso/mark3mg.c:174) and the post-solve
+stress / strain-rate pass of vpiterate on the GPU.
 
 Bit-exact bar: the moved marker coordinates (float) equal the reference's
 for every marker, through the host-array entry point (against the golden
@@ -75,3 +76,34 @@ def test_movemark_resident_after_resident_solve_vs_oracle(oracle_mod, variant):
     for a, b, c in zip(got, ref, "xyz"):
         assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), c
     assert int(((got[0] != mx) | (got[1] != my) | (got[2] != mz)).sum()) > mx.size // 2
+
+
+def test_stress_strain_after_solve_vs_oracle(oracle_mod):
+    """Post-solve stresses and strain rates (move3mgNew.c:2908-3038) from the
+    float velocities of a resident solve: bit-exact with the oracle's pass
+    (pinned to the reference's own in the CPU suite); untouched positions
+    keep the caller's values; velocity ranges over the valid positions."""
+    from tests.test_oracle_golden import load_case
+    m, g = load_case("sphere17")
+    nodes = {k: g["node_" + k] for k in ("nu", "ro", "nxx", "nxy", "nxz", "nyz")}
+    prob = P.StokesProblem(m, tol=1e-8)
+    prob.set_nodes(nodes)
+    assert prob.ctx.solve_resident().status == 0
+    sol = prob.ctx.solution(m.nodenum)
+    vel = tuple(np.asarray(sol[k], np.float32) for k in ("vx", "vy", "vz"))
+    keys = oracle_mod.STRESS_KEYS
+    got = {k: np.full(m.nodenum, -7.0, np.float32) for k in keys}
+    vr = prob.ctx.stress_strain(got)
+    part = {k: np.full(m.nodenum, -7.0, np.float32) for k in ("sxy", "ezz")}
+    prob.ctx.stress_strain(part)
+    prob.close()
+    ref = oracle_mod.stress_strain(m, vel, nodes, init=-7.0)
+    for k in keys:
+        assert np.array_equal(got[k].view(np.uint32), ref[k].view(np.uint32)), k
+    for k in part:
+        assert np.array_equal(part[k], got[k]), k
+    nx, ny, nz = m.shape
+    kk, ii, jj = (a.ravel() for a in np.meshgrid(np.arange(nz), np.arange(nx), np.arange(ny), indexing="ij"))
+    ok = [(jj < ny - 1) & (kk < nz - 1), (ii < nx - 1) & (kk < nz - 1), (ii < nx - 1) & (jj < ny - 1)]
+    for c in range(3):
+        assert vr[2 * c] == float(vel[c][ok[c]].min()) and vr[2 * c + 1] == float(vel[c][ok[c]].max()), c

@@ -31,6 +31,14 @@ def pin_mask(m, lev):
     return mask
 
 
+def vmax_valid(m, v, c):
+    """max |v| over the valid positions of velocity component c (1..3)."""
+    nx, ny, nz = m.shape
+    k, i, j = np.meshgrid(np.arange(nz), np.arange(nx), np.arange(ny), indexing="ij")
+    ok = [(j < ny - 1) & (k < nz - 1), (i < nx - 1) & (k < nz - 1), (i < nx - 1) & (j < ny - 1)][c - 1].ravel()
+    return float(np.abs(v[ok]).max())
+
+
 def rel(a, b):
     return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
 
@@ -118,7 +126,17 @@ def test_live_reference_ronurecalc_and_rows(oracle_mod):
     f = oracle_mod.ronurecalc(m)
     for k in nodes:
         assert np.array_equal(nodes[k], f[k]), k
+    r.fill_stress(-7.0)
+    r.set_step(0.01, 1e30)
     r.first_iteration()
+    # vpiterate's post-solve stresses, strain rates and time-step limit
+    w = r.written()
+    vel = (w["vx"], w["vy"], w["vz"])
+    st = r.written_stress()
+    ost = oracle_mod.stress_strain(m, vel, nodes, init=-7.0)
+    for k in st:
+        assert np.array_equal(st[k].view(np.uint32), ost[k].view(np.uint32)), k
+    assert r.timestep() == min(0.01 / vmax_valid(m, v, c) for c, v in enumerate(vel, 1))
     s = oracle_mod.OracleSolver(m)
     s.set_fields(nodes)
     row, col, val, rhs = r.rows(0)
@@ -146,3 +164,16 @@ def test_oracle_movemark_vs_reference_golden(oracle_mod, variant):
         assert np.array_equal(a.view(np.uint32), g["out_%s_%s" % (variant, c)].view(np.uint32)), c
     moved = (out[0] != ins[0]) | (out[1] != ins[1]) | (out[2] != ins[2])
     assert moved.sum() > ins[0].size // 2
+
+
+def test_oracle_stress_strain_vs_reference_golden(oracle_mod):
+    """The post-solve stress / strain-rate pass (move3mgNew.c:2908-3038)
+    bit-exact with the reference's value-mode stencils (move17.npz)."""
+    g = np.load(os.path.join(GOLDEN, "move17.npz"))
+    src = np.load(os.path.join(GOLDEN, "sphere17.npz"))
+    m = M.sphere_model(17, 2, (1, 1, 1), seed=3, eta_sphere=1e3)
+    nodes = {k: src["node_" + k] for k in ("nxx", "nxy", "nxz", "nyz")}
+    out = oracle_mod.stress_strain(m, (g["vx"], g["vy"], g["vz"]), nodes, init=-7.0)
+    for k, a in out.items():
+        assert np.array_equal(a.view(np.uint32), g["st_" + k].view(np.uint32)), k
+        assert (a != -7.0).sum() > 0.7 * a.size * (0.75 if k[1] != k[2] else 1.0), k
