@@ -37,6 +37,9 @@ WORKLOADS = {
         "2x2x2 markers/cell, free-slip box, seed 2"),
     3: ("spheres129: 129^3 nodes, 5 levels, 20 spheres viscosity 1e-2..1e4 (contrast 1e6), "
         "2x2x2 markers/cell, free-slip box, seed 3"),
+    4: ("batch64: 64 independent models, nodes per axis uniform in {33,49,65,81,97}, 1-10 spheres viscosity "
+        "1e-2..1e2, 2x2x2 markers/cell, free-slip boxes, seed 4; solved concurrently (one stream and CUDA graphs "
+        "per instance) vs one after another"),
     5: ("layered257: 257^3 nodes, 6 levels, 45 layers viscosity 1e4..1 with depth, slab 1e3 (density +1), "
         "weak zone 1e-2, 2x2x2 markers/cell, free-slip box, seed 5"),
 }
@@ -225,12 +228,149 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def shard_instances(sizes, world):
+    """Greedy balance of instances (by node count, largest first) over ranks:
+    returns the instance indices of every rank."""
+    load = [0] * world
+    parts = [[] for _ in range(world)]
+    for i in sorted(range(len(sizes)), key=lambda i: (-sizes[i], i)):
+        r = min(range(world), key=lambda r: (load[r], r))
+        parts[r].append(i)
+        load[r] += sizes[i]
+    return [sorted(p) for p in parts]
+
+
+def run_batch(args, rank, world, local, dist):
+    """The batched workload: this rank's share of the 64 instances, solved
+    one after another and then all at once (p2_stokes_solve_batch)."""
+    import numpy as np
+    import torch
+    import pardiso2_b200 as P
+    from pardiso2_b200 import capi
+    from pardiso2_b200 import model as M
+
+    specs = M.batch_specs(64, 4)
+    mine = shard_instances([n ** 3 for n, _, _ in specs], world)[rank]
+    models, probs, tunes = [], [], []
+    for i in mine:
+        m = M.batch_model(*specs[i])
+        p = P.StokesProblem(m, device=local, precision=0, tol=1e-8, restart=args.restart)
+        p.ctx.upload_markers(m.markx, m.marky, m.markz, m.markt, m.rocks.n0, m.rocks.n1, m.rocks.ro)
+        p.ctx.ronurecalc_resident()
+        tunes.append(p.autotune(min(args.tune_iters, 8)).as_dict() if args.tune_iters > 0 else None)
+        models.append(m)
+        probs.append(p)
+    ctxs = [p.ctx for p in probs]
+    dofs = sum(m.real_dofs() for m in models)
+    for _ in range(args.warmup):
+        capi.solve_batch(ctxs)
+    # one after another (each solve timed on its own stream)
+    seq = []
+    for _ in range(args.steps):
+        seq.append(sum(c.solve_resident(check=False).ms_total for c in ctxs))
+    # all at once
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clk = ClockSampler(local)
+    clk.start()
+    batch, lat, launches, ok = [], [], 0, True
+    for _ in range(args.steps):
+        infos, ms = capi.solve_batch(ctxs)
+        batch.append(ms)
+        lat.extend(x.ms_total for x in infos)
+        launches += sum(x.kernels for x in infos)
+        ok = ok and all(x.status == 0 for x in infos)
+    torch.cuda.synchronize()
+    clocks = clk.stop()
+    if dist:
+        dist.barrier()
+    batch_ms, seq_ms = statistics.mean(batch), statistics.mean(seq)
+    if dist:
+        t = torch.tensor([batch_ms, seq_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        batch_ms, seq_ms = float(t[0].item()), float(t[1].item())
+        d = torch.tensor([float(dofs)], dtype=torch.float64, device="cuda")
+        dist.all_reduce(d)
+        dofs_all = float(d.item())
+    else:
+        dofs_all = float(dofs)
+    # end to end: node fields from pinned host memory, the batch, solutions back
+    keys = ("nu", "ro", "nxx", "nxy", "nxz", "nyz")
+    host = []
+    for m, p in zip(models, probs):
+        f = p.ctx.get_nodes(m.nodenum)
+        pin = {k: torch.empty(m.nodenum, dtype=torch.float32, pin_memory=True).numpy() for k in keys}
+        for k in keys:
+            pin[k][:] = f[k]
+        sol = {k: torch.empty(m.nodenum, dtype=torch.float64, pin_memory=True).numpy() for k in ("vx", "vy", "vz", "pr")}
+        host.append((pin, sol))
+    e2e = []
+    for it in range(args.warmup + args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for p, (pin, _) in zip(probs, host):
+            p.ctx.set_nodes(pin)
+        capi.solve_batch(ctxs)
+        for p, (_, sol) in zip(probs, host):
+            p.ctx._check(p.ctx.L.p2_get_solution(p.ctx.h, *[capi._ptr(sol[k]) for k in ("vx", "vy", "vz", "pr")]),
+                         "p2_get_solution")
+        if it >= args.warmup:
+            e2e.append((time.perf_counter() - t0) * 1e3)
+    e2e_ms = statistics.mean(e2e)
+    if dist:
+        t = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    nodes = sum(m.nodenum for m in models)
+    # dominant kernel: level-0 colour pass of the smoother on the largest instance
+    big = max(range(len(models)), key=lambda i: models[i].nodenum)
+    pass_ms = capi.DebugHooks(ctxs[big]).time_smoother(0, 40)
+    bytes_per_launch = SMOOTHER_BYTES_PER_NODE * models[big].nodenum
+    achieved = bytes_per_launch / (pass_ms * 1e-3) / 1e9
+    peak, peak_kind = measured_peaks()
+    line = {
+        "metric": METRIC, "value": batch_ms, "unit": "ms", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": batch_ms, "higher_is_better": False, "scaling": "strong",
+        "vs_baseline": None, "dtype": "f32 V-cycle / f64 outer", "data": "synthetic",
+        "config": {"workload": WORKLOADS[4], "instances": len(specs), "instances_per_rank": len(mine),
+                   "unknowns": int(dofs_all), "l2": "working set of all instances (GBs) larger than L2",
+                   "parallelism": ("instances sharded over %d ranks, " % world if world > 1 else "")
+                   + "concurrent streams, host worker pool"},
+        "converged": ok, "sequential_ms": seq_ms, "speedup_batch_vs_sequential": seq_ms / batch_ms,
+        "unknowns_per_s": dofs_all / (batch_ms * 1e-3),
+        "unknowns_per_s_sequential": dofs_all / (seq_ms * 1e-3),
+        "instance_latency_ms": {"mean": statistics.mean(lat), "max": max(lat), "min": min(lat)},
+        "gpu_launches": launches,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": None, "kernel": "k_vanka_fast<float> level-0 colour pass, largest instance (%d^3)"
+                     % models[big].shape[0], "bytes_per_launch": bytes_per_launch, "ms_per_launch": pass_ms,
+                     "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs, burst)"},
+        "clocks": clocks,
+        "e2e": {"value": e2e_ms, "unit": "ms", "h2d_bytes_per_step": 24 * nodes, "d2h_bytes_per_step": 32 * nodes},
+        "autotune": {"smoother_full": sum(1 for t in tunes if t and t["smoother"] == 1),
+                     "sweep_growth_2": sum(1 for t in tunes if t and t["sweep_growth"] == 2)},
+    }
+    for p in probs:
+        p.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
         return
     rank, world, local, dist = dist_setup(args.gpus)
+    if args.config == 4:
+        import torch
+        torch.cuda.set_device(local)
+        run_batch(args, rank, world, local, dist)
+        return
     import numpy as np
     import torch
     import pardiso2_b200 as P

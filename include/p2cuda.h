@@ -124,6 +124,17 @@ p2_status p2_stokes_solve(p2_ctx *ctx, float *vx, float *vy, float *vz, double *
 /* Same solve on the resident node fields with the solution kept on the
  * device (no host transfers); read it back with p2_get_solution. */
 p2_status p2_stokes_solve_resident(p2_ctx *ctx, p2_solve_info *info);
+
+/* Batched solves (no counterpart in the reference, which solves one model per
+ * process): p2_stokes_solve_resident on each of count contexts at once.
+ * Every context must hold its grid, boundary tables and node fields; each
+ * has its own stream and graphs, so the device overlaps the instances'
+ * kernels.  host_threads workers (0: one per context, at most the hardware
+ * threads) take the contexts largest first.  infos[i] (may be null) gets
+ * context i's result; *ms (may be null) the device time from the first
+ * launch to the last result, measured with events on device 0 of the batch.
+ * Returns the first failing status in context order, else P2_OK. */
+p2_status p2_stokes_solve_batch(p2_ctx *const *ctxs, int count, int host_threads, p2_solve_info *infos, double *ms);
 p2_status p2_get_solution(p2_ctx *ctx, double *vx, double *vy, double *vz, double *pr);
 
 /* Smoother autotuner (no counterpart in the reference, whose sweep counts

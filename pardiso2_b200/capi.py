@@ -21,7 +21,8 @@ EXPORTED = ["p2_default_params", "p2_create", "p2_destroy", "p2_last_error", "p2
             "p2_set_nodes", "p2_stokes_solve", "p2_stokes_solve_resident", "p2_get_solution", "p2_ronurecalc",
             "p2_upload_markers", "p2_ronurecalc_resident", "p2_get_nodes", "p2_debug_apply", "p2_debug_restrict",
             "p2_debug_prolong", "p2_debug_level_fields", "p2_debug_time_smoother", "p2_ronurecalc_noalloc", "p2_autotune",
-            "p2_movemark", "p2_movemark_resident", "p2_get_markers", "p2_stress_strain"]
+            "p2_movemark", "p2_movemark_resident", "p2_get_markers", "p2_stress_strain",
+            "p2_stokes_solve_batch"]
 
 
 class Params(C.Structure):
@@ -95,6 +96,8 @@ def load() -> C.CDLL:
     L.p2_movemark_resident.argtypes = [vp, C.c_double, C.c_int, C.c_int, C.POINTER(C.c_double)]
     L.p2_get_markers.argtypes = [vp, _fp, _fp, _fp]
     L.p2_stress_strain.argtypes = [vp] + [C.c_void_p] * 12 + [C.POINTER(C.c_double)]
+    L.p2_stokes_solve_batch.argtypes = [C.POINTER(vp), C.c_int, C.c_int, C.c_void_p, C.POINTER(C.c_double)]
+    L.p2_stokes_solve_batch.restype = C.c_int
     for f in ("p2_movemark", "p2_movemark_resident", "p2_get_markers", "p2_stress_strain"):
         getattr(L, f).restype = C.c_int
     for f in ("p2_create", "p2_set_grid", "p2_set_bc", "p2_set_nodes", "p2_stokes_solve", "p2_stokes_solve_resident",
@@ -246,6 +249,23 @@ class Context:
                                          np.ascontiguousarray(n1, np.float64), np.ascontiguousarray(ro, np.float64),
                                          *[fields[k] for k in keys]), "p2_ronurecalc")
         return fields
+
+
+def solve_batch(contexts, host_threads: int = 0):
+    """p2_stokes_solve_batch: resident solves of several contexts at once.
+    Returns (list of SolveInfo, device ms of the whole batch); raises on the
+    first failing status."""
+    if not contexts:
+        return [], 0.0
+    L = contexts[0].L
+    hs = (C.c_void_p * len(contexts))(*[c.h for c in contexts])
+    infos = (SolveInfo * len(contexts))()
+    ms = C.c_double()
+    st = L.p2_stokes_solve_batch(hs, len(contexts), host_threads, C.cast(infos, C.c_void_p), C.byref(ms))
+    if st != 0:
+        bad = [i for i, x in enumerate(infos) if x.status != 0]
+        raise P2Error(st, "p2_stokes_solve_batch: status %d (instances %s)" % (st, bad[:8]))
+    return list(infos), ms.value
 
 
 def _debug_sigs(L):

@@ -1,9 +1,12 @@
 // extern "C" entry points of libp2cuda.so (declared in include/p2cuda.h).
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <atomic>
 #include <cstring>
 #include <new>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "p2_solver.h"
@@ -173,6 +176,77 @@ p2_status p2_stokes_solve_resident(p2_ctx *ctx, p2_solve_info *info)
     finish_info(info, r);
     if (st != P2_OK) return st;
     return (p2_status)r.status;
+}
+
+p2_status p2_stokes_solve_batch(p2_ctx *const *ctxs, int count, int host_threads, p2_solve_info *infos, double *ms)
+{
+    if (count < 0 || (count > 0 && !ctxs)) return P2_ERR_ARG;
+    for (int i = 0; i < count; i++)
+        if (!ctxs[i]) return P2_ERR_ARG;
+    if (count == 0) {
+        if (ms) *ms = 0;
+        return P2_OK;
+    }
+    // largest instances first, so that the longest solves start at once
+    std::vector<int> order(count);
+    for (int i = 0; i < count; i++) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+        const p2::Solver *sa = ctxs[a]->s, *sb = ctxs[b]->s;
+        const long na = sa->L.empty() ? 0 : sa->L[0].n, nb = sb->L.empty() ? 0 : sb->L[0].n;
+        return na > nb;
+    });
+    std::vector<p2_solve_info> res(count);
+    std::vector<p2_status> sts(count, P2_OK);
+    // device-side clock: events on a stream of the first context's device
+    p2::Solver &S0 = *ctxs[0]->s;
+    cudaStream_t clock_st = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    p2_status st0 = guard(ctxs[0], [&] {
+        P2_CUDA_TRY(cudaSetDevice(S0.dev));
+        P2_CUDA_TRY(cudaStreamCreateWithFlags(&clock_st, cudaStreamNonBlocking));
+        P2_CUDA_TRY(cudaEventCreate(&e0));
+        P2_CUDA_TRY(cudaEventCreate(&e1));
+        P2_CUDA_TRY(cudaEventRecord(e0, clock_st));
+        P2_CUDA_TRY(cudaEventSynchronize(e0));
+    });
+    if (st0 == P2_OK) {
+        std::atomic<int> next{0};
+        auto work = [&] {
+            for (int q = next++; q < count; q = next++) {
+                const int i = order[q];
+                sts[i] = p2_stokes_solve_resident(ctxs[i], &res[i]);
+            }
+        };
+        int nt = host_threads > 0 ? host_threads : count;
+        const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
+        if (host_threads <= 0) nt = std::min(nt, hw);
+        nt = std::max(1, std::min(nt, count));
+        std::vector<std::thread> pool;
+        try {
+            for (int t = 1; t < nt; t++) pool.emplace_back(work);
+        } catch (...) {
+            // fewer workers than asked: the ones that started and this thread finish the batch
+        }
+        work();
+        for (auto &t : pool) t.join();
+        st0 = guard(ctxs[0], [&] {
+            P2_CUDA_TRY(cudaSetDevice(S0.dev));
+            P2_CUDA_TRY(cudaEventRecord(e1, clock_st));
+            P2_CUDA_TRY(cudaEventSynchronize(e1));
+            float t = 0;
+            P2_CUDA_TRY(cudaEventElapsedTime(&t, e0, e1));
+            if (ms) *ms = t;
+        });
+    }
+    cudaSetDevice(S0.dev);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (clock_st) cudaStreamDestroy(clock_st);
+    if (infos)
+        for (int i = 0; i < count; i++) infos[i] = res[i];
+    for (int i = 0; i < count; i++)
+        if (sts[i] != P2_OK) return sts[i];
+    return st0;
 }
 
 p2_status p2_get_solution(p2_ctx *ctx, double *vx, double *vy, double *vz, double *pr)

@@ -497,7 +497,6 @@ static void dgemm_sub(cudaStream_t st, int m, int nn, int kk, const double *A, i
     k_dgemm_sub<<<grid, 256, 0, st>>>(m, nn, kk, A, lda, B, ldb, C, ldc); P2_COUNT_LAUNCH();
 }
 
-static bool smem_panel_ready = false;
 
 // Diagnostic per-kernel-type device times of the LU (environment variable
 // P2CUDA_LU_TIMING=1): every launch is bracketed by events and waited for, so
@@ -601,10 +600,9 @@ int band_lu_inverse(cudaStream_t st, double *A, int n, int kl, int ku, double *A
 {
     kl = std::max(0, std::min(kl, n - 1));
     ku = std::max(0, std::min(ku, n - 1));
-    if (kPB + kl <= kMaxPanelRows && !smem_panel_ready) {
+    // a per-device attribute, set on the current device (a host-side call)
+    if (kPB + kl <= kMaxPanelRows)
         P2_CUDA_TRY(cudaFuncSetAttribute(k_panel_track, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxPanelBytes));
-        smem_panel_ready = true;
-    }
     LuTimer T;
     {
         const char *e = std::getenv("P2CUDA_LU_TIMING");

@@ -458,6 +458,25 @@ def layered_model(n=257, multinum=6, markers=(2, 2, 2), seed=5, nlayers=45, name
     return _finish(name or ("layered%d" % n), n, multinum, *markers, seed, rocks, paint, params)
 
 
+BATCH_SIZES = {33: 2, 49: 3, 65: 3, 81: 4, 97: 4}  # nodes per axis -> multinum (coarsest 9..12 nodes)
+
+
+def batch_specs(count: int = 64, seed: int = 4):
+    """The batched workload: per instance (nodes per axis, spheres, seed),
+    sizes uniform in {33, 49, 65, 81, 97}, 1-10 spheres."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    sizes = rng.choice(sorted(BATCH_SIZES), size=count)
+    nsph = rng.integers(1, 11, size=count)
+    return [(int(n), int(s), seed * 1000 + i) for i, (n, s) in enumerate(zip(sizes, nsph))]
+
+
+def batch_model(n: int, nsph: int, seed: int) -> Model:
+    """One instance of the batched workload: nsph spheres with viscosity
+    log-uniform in [1e-2, 1e2] in an n^3 box, 2x2x2 markers per cell."""
+    return random_spheres_model(n, BATCH_SIZES[n], nsph, (1e-2, 1e2), markers=(2, 2, 2), seed=seed,
+                                name="batch%d_%d" % (n, seed))
+
+
 def config_model(idx: int, **kw) -> Model:
     """The five benchmark configurations (synthetic, seeded)."""
     if idx == 1:
