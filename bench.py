@@ -50,6 +50,15 @@ WORKLOAD = WORKLOADS[CONFIG_IDX]
 # (16 B) and 4 viscosity fields (16 B); write 3 velocity fields (12 B) and
 # half of the pressures (2 B).
 SMOOTHER_BYTES_PER_NODE = 62
+# The stored-factor variant also reads its cell factors: 22 floats per cell of
+# the active colour, i.e. 44 B per node and pass.
+SMOOTHER_FACTOR_BYTES_PER_NODE = 44
+KERNEL_OF_SMOOTHER = {0: "k_vanka<float>", 1: "k_vanka_stored<float>", 2: "k_vanka_full<float>",
+                      3: "k_vanka_fast<float>"}
+
+
+def smoother_bytes(smoother):
+    return SMOOTHER_BYTES_PER_NODE + (SMOOTHER_FACTOR_BYTES_PER_NODE if smoother == 1 else 0)
 # Marker advection: per marker read x, y, z (12 B) and the type (1 B), write
 # x, y, z (12 B); per node read the FP64 velocities (24 B) and write and
 # re-read their float copies (12 + 12 B) once (the 8-node gathers of the
@@ -86,7 +95,7 @@ def measured_peaks():
 def profile_traffic():
     """Per-launch DRAM bytes of the level-0 FP32 smoother pass from the
     committed ncu summary (None until one is captured)."""
-    p = os.path.join(ROOT, "profiles", "ncu_vanka_fast_f32_level0.txt")
+    p = os.path.join(ROOT, "profiles", "ncu_vanka_stored_f32_level0.txt")
     if not os.path.exists(p):
         return None
     m = re.search(r"dram_bytes_per_launch:\s*([0-9.eE+]+)", open(p).read())
@@ -325,8 +334,9 @@ def run_batch(args, rank, world, local, dist):
     nodes = sum(m.nodenum for m in models)
     # dominant kernel: level-0 colour pass of the smoother on the largest instance
     big = max(range(len(models)), key=lambda i: models[i].nodenum)
+    sm_big = tunes[big]["smoother"] if tunes[big] else 1
     pass_ms = capi.DebugHooks(ctxs[big]).time_smoother(0, 40)
-    bytes_per_launch = SMOOTHER_BYTES_PER_NODE * models[big].nodenum
+    bytes_per_launch = smoother_bytes(sm_big) * models[big].nodenum
     achieved = bytes_per_launch / (pass_ms * 1e-3) / 1e9
     peak, peak_kind = measured_peaks()
     line = {
@@ -343,8 +353,8 @@ def run_batch(args, rank, world, local, dist):
         "instance_latency_ms": {"mean": statistics.mean(lat), "max": max(lat), "min": min(lat)},
         "gpu_launches": launches,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": None, "kernel": "k_vanka_fast<float> level-0 colour pass, largest instance (%d^3)"
-                     % models[big].shape[0], "bytes_per_launch": bytes_per_launch, "ms_per_launch": pass_ms,
+                     "traffic": None, "kernel": KERNEL_OF_SMOOTHER[sm_big]
+                     + " level-0 colour pass, largest instance (%d^3)" % models[big].shape[0], "bytes_per_launch": bytes_per_launch, "ms_per_launch": pass_ms,
                      "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs, burst)"},
         "clocks": clocks,
         "e2e": {"value": e2e_ms, "unit": "ms", "h2d_bytes_per_step": 24 * nodes, "d2h_bytes_per_step": 32 * nodes},
@@ -422,10 +432,10 @@ def main():
     # the dominant kernel: level-0 FP32 colour pass of the cell-block smoother
     H = capi.DebugHooks(prob.ctx)
     pass_ms = H.time_smoother(0, 40)
-    bytes_per_launch = SMOOTHER_BYTES_PER_NODE * n
+    bytes_per_launch = smoother_bytes(tune.smoother) * n
     achieved = bytes_per_launch / (pass_ms * 1e-3) / 1e9
     peak, peak_kind = measured_peaks()
-    traffic = profile_traffic() if (args.config == CONFIG_IDX and tune.smoother) else None
+    traffic = profile_traffic() if (args.config == CONFIG_IDX and tune.smoother == 1) else None
     if args.solve_only:
         if rank == 0:
             print(json.dumps({"metric": METRIC, "value": value, "unit": "ms", "solve_only": True,
@@ -505,7 +515,7 @@ def main():
         "unknowns_per_s": m.real_dofs() * world / (ms_per_step * 1e-3),
         "gpu_launches": launches,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": traffic, "kernel": ("k_vanka_fast<float>" if tune.smoother else "k_vanka<float>") + " level-0 colour pass",
+                     "traffic": traffic, "kernel": KERNEL_OF_SMOOTHER[tune.smoother] + " level-0 colour pass",
                      "bytes_per_launch": bytes_per_launch, "ms_per_launch": pass_ms,
                      "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs, burst)"},
         "clocks": clocks,

@@ -67,9 +67,11 @@ typedef struct {
     int restart;         /* GCR restart length (default 16, at most 18) */
     double omega;        /* cell-block smoother damping (default 0.7) */
     int use_graphs;      /* capture the V-cycle in a CUDA graph (default 1) */
-    int smoother;        /* cell-block smoother: 1 = exact 7x7 cell solve (default),
+    int smoother;        /* cell-block smoother: 1 = exact 7x7 cell solve with the cell
+                            factors computed once per solve and stored (default),
+                            3 = the same solve factored on every sweep (no stored factors),
                             0 = diagonal velocity block (cheaper, weak at stiff inclusions),
-                            2 = the exact cell solve evaluated row by row (slower; a cross-check of 1) */
+                            2 = the exact cell solve evaluated row by row (slower; a cross-check) */
 } p2_params;
 
 typedef struct {

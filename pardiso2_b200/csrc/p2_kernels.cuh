@@ -308,77 +308,145 @@ __global__ void __launch_bounds__(128) k_vanka_full(LevelView<T> L, T *P, Vec4<T
         if (act[q]) vout.c[fc[q]][fi[q]] = vin.c[fc[q]][fi[q]] + omega * (y1[q] - dp * y2[q]);
 }
 
-// ---------------------------------------------------------------------------
-// k_vanka_full with the six momentum residuals assembled from shared
-// stresses: the cell's three normal stresses come from one set of strain
-// rates (each face row of the cell uses one of them), the twelve shear
-// stresses on the cell's edges are each evaluated once (every edge is shared
-// by two of the cell's faces), and the continuity residual is the cell's
-// divergence.  The six neighbour cells contribute one normal stress each.
-// Same terms as row_vx/row_vy/row_vz, about half the loads and arithmetic.
+// Momentum parts (A v + grad p) of the six face rows of cell (i, j, k) from
+// shared stresses, and the cell's divergence: the cell's three normal
+// stresses from one set of strain rates, the six neighbour cells' normal
+// stresses along their face normals, the twelve edge shear stresses once
+// each.  Every velocity, viscosity and pressure is loaded once, addressed
+// from the cell's low corner F = (i-1, j-1, k-1) (y stride 1, x stride ny, z
+// stride nx*ny); the deviatoric third is a multiplication by 1/3.  The same
+// terms as row_vx/row_vy/row_vz up to rounding.
 template <typename T>
-__global__ void __launch_bounds__(128) k_vanka_fast(LevelView<T> L, T *P, Vec4<T> vin, Vec4<T> vout, Vec4<T> b,
-                                                    T omega, int col)
+__device__ __forceinline__ void cell_rows(const LevelView<T> &L, const Fields<T, T> &x, int i, int j, int k,
+                                          const int fi[6], T ax[6], T &div)
 {
-    int half = (L.ny) / 2;
-    long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    long lines = (long)(L.nx - 1) * (L.nz - 1);
-    if (t >= lines * half) return;
-    int jj = (int)(t % half);
-    long line = t / half;
-    const int i = 1 + (int)(line % (L.nx - 1)), k = 1 + (int)(line / (L.nx - 1));
-    const int j0 = (((1 + i + k) & 1) == col) ? 1 : 2;
-    const int j = j0 + 2 * jj;
-    if (j > L.ny - 1) return;
-    Fields<T, T> x{P, vin.c[1], vin.c[2], vin.c[3]};
-    const int u = P2IDX(L, i, j, k);
-    const bool pact = (L.bcm[u] & BC_P) == 0;
-    int fi[6];
-    const int fc[6] = {1, 1, 2, 2, 3, 3};
+    const int sy = L.ny, sz = L.nx * L.ny;
+    const int F = fi[0];
+    const T *vx = x.vx + F, *vy = x.vy + F, *vz = x.vz + F;
+    // velocities around the cell (offsets from F)
+    const T vx0 = __ldg(vx), vxX = __ldg(vx + sy), vxXX = __ldg(vx + 2 * sy), vxm = __ldg(vx - sy);
+    const T vxY = __ldg(vx + 1), vxy_ = __ldg(vx - 1), vxXY = __ldg(vx + sy + 1), vxXy = __ldg(vx + sy - 1);
+    const T vxZ = __ldg(vx + sz), vxz_ = __ldg(vx - sz), vxXZ = __ldg(vx + sy + sz), vxXz = __ldg(vx + sy - sz);
+    const T vy0 = __ldg(vy), vyY = __ldg(vy + 1), vyYY = __ldg(vy + 2), vym = __ldg(vy - 1);
+    const T vyX = __ldg(vy + sy), vyx_ = __ldg(vy - sy), vyXY = __ldg(vy + sy + 1), vyxY = __ldg(vy - sy + 1);
+    const T vyZ = __ldg(vy + sz), vyz_ = __ldg(vy - sz), vyYZ = __ldg(vy + 1 + sz), vyYz = __ldg(vy + 1 - sz);
+    const T vz0 = __ldg(vz), vzZ = __ldg(vz + sz), vzZZ = __ldg(vz + 2 * sz), vzm = __ldg(vz - sz);
+    const T vzX = __ldg(vz + sy), vzx_ = __ldg(vz - sy), vzXZ = __ldg(vz + sy + sz), vzxZ = __ldg(vz - sy + sz);
+    const T vzY = __ldg(vz + 1), vzy_ = __ldg(vz - 1), vzYZ = __ldg(vz + 1 + sz), vzyZ = __ldg(vz - 1 + sz);
+    const T third = (T)(1.0 / 3.0), two = (T)2.0;
+    const T hx0 = L.ax.ih[i - 1], hx1 = L.ax.ih[i], hx2 = L.ax.ih[i + 1];
+    const T hy0 = L.ay.ih[j - 1], hy1 = L.ay.ih[j], hy2 = L.ay.ih[j + 1];
+    const T hz0 = L.az.ih[k - 1], hz1 = L.az.ih[k], hz2 = L.az.ih[k + 1];
+    const int u = F + sz + sy + 1;
+    // own cell
+    const T exx = (vxX - vx0) * hx1, eyy = (vyY - vy0) * hy1, ezz = (vzZ - vz0) * hz1;
+    div = exx + eyy + ezz;
+    const T E2 = two * eta_at(L, L.ec, u);
+    const T s0 = E2 * (exx - div * third), s1 = E2 * (eyy - div * third), s2 = E2 * (ezz - div * third);
+    // neighbour cells: normal stress along the shared face's normal
+    T sL, sR, sF, sB, sD, sU;
+    {   // cell (i-1, j, k): faces vx[F-sy], vx[F]; vy[F-sy], vy[F-sy+1]; vz[F-sy], vz[F-sy+sz]
+        const T a = (vx0 - vxm) * hx0, b = (vyxY - vyx_) * hy1, c = (vzxZ - vzx_) * hz1;
+        sL = two * eta_at(L, L.ec, u - sy) * (a - (a + b + c) * third);
+    }
+    {   // cell (i+1, j, k)
+        const T a = (vxXX - vxX) * hx2, b = (vyXY - vyX) * hy1, c = (vzXZ - vzX) * hz1;
+        sR = two * eta_at(L, L.ec, u + sy) * (a - (a + b + c) * third);
+    }
+    {   // cell (i, j-1, k)
+        const T a = (vxXy - vxy_) * hx1, b = (vy0 - vym) * hy0, c = (vzyZ - vzy_) * hz1;
+        sF = two * eta_at(L, L.ec, u - 1) * (b - (a + b + c) * third);
+    }
+    {   // cell (i, j+1, k)
+        const T a = (vxXY - vxY) * hx1, b = (vyYY - vyY) * hy2, c = (vzYZ - vzY) * hz1;
+        sB = two * eta_at(L, L.ec, u + 1) * (b - (a + b + c) * third);
+    }
+    {   // cell (i, j, k-1)
+        const T a = (vxXz - vxz_) * hx1, b = (vyYz - vyz_) * hy1, c = (vz0 - vzm) * hz0;
+        sD = two * eta_at(L, L.ec, u - sz) * (c - (a + b + c) * third);
+    }
+    {   // cell (i, j, k+1)
+        const T a = (vxXZ - vxZ) * hx1, b = (vyYZ - vyZ) * hy1, c = (vzZZ - vzZ) * hz2;
+        sU = two * eta_at(L, L.ec, u + sz) * (c - (a + b + c) * third);
+    }
+    // edge shear stresses (sxy, sxz, syz at the cell's twelve edges)
+    const T ex0 = L.ax.ihe[i - 1], ex1 = L.ax.ihe[i], ey0 = L.ay.ihe[j - 1], ey1 = L.ay.ihe[j];
+    const T ez0 = L.az.ihe[k - 1], ez1 = L.az.ihe[k];
+    const T xy00 = two * eta_at(L, L.exy, F) * ((vx0 - vxy_) * ey0 + (vy0 - vyx_) * ex0);
+    const T xy01 = two * eta_at(L, L.exy, F + 1) * ((vxY - vx0) * ey1 + (vyY - vyxY) * ex0);
+    const T xy10 = two * eta_at(L, L.exy, F + sy) * ((vxX - vxXy) * ey0 + (vyX - vy0) * ex1);
+    const T xy11 = two * eta_at(L, L.exy, F + sy + 1) * ((vxXY - vxX) * ey1 + (vyXY - vyY) * ex1);
+    const T xz00 = two * eta_at(L, L.exz, F) * ((vx0 - vxz_) * ez0 + (vz0 - vzx_) * ex0);
+    const T xz01 = two * eta_at(L, L.exz, F + sz) * ((vxZ - vx0) * ez1 + (vzZ - vzxZ) * ex0);
+    const T xz10 = two * eta_at(L, L.exz, F + sy) * ((vxX - vxXz) * ez0 + (vzX - vz0) * ex1);
+    const T xz11 = two * eta_at(L, L.exz, F + sy + sz) * ((vxXZ - vxX) * ez1 + (vzXZ - vzZ) * ex1);
+    const T yz00 = two * eta_at(L, L.eyz, F) * ((vy0 - vyz_) * ez0 + (vz0 - vzy_) * ey0);
+    const T yz01 = two * eta_at(L, L.eyz, F + sz) * ((vyZ - vy0) * ez1 + (vzZ - vzyZ) * ey0);
+    const T yz10 = two * eta_at(L, L.eyz, F + 1) * ((vyY - vyYz) * ez0 + (vzY - vz0) * ey1);
+    const T yz11 = two * eta_at(L, L.eyz, F + 1 + sz) * ((vyYZ - vyY) * ez1 + (vzYZ - vzZ) * ey1);
+    const T *pp = x.p + u;
+    const T p0 = __ldg(pp), pL = __ldg(pp - sy), pR = __ldg(pp + sy), pF = __ldg(pp - 1), pB = __ldg(pp + 1);
+    const T pD = __ldg(pp - sz), pU = __ldg(pp + sz);
+    const T cx0 = L.ax.ihc[i - 1], cx1 = L.ax.ihc[i], cy0 = L.ay.ihc[j - 1], cy1 = L.ay.ihc[j];
+    const T cz0 = L.az.ihc[k - 1], cz1 = L.az.ihc[k];
+    const T wx = L.ax.ihv[i - 1], wy = L.ay.ihv[j - 1], wz = L.az.ihv[k - 1];
+    ax[0] = (s0 - sL) * cx0 + (xy01 - xy00) * wy + (xz01 - xz00) * wz - (p0 - pL) * cx0;
+    ax[1] = (sR - s0) * cx1 + (xy11 - xy10) * wy + (xz11 - xz10) * wz - (pR - p0) * cx1;
+    ax[2] = (s1 - sF) * cy0 + (xy10 - xy00) * wx + (yz01 - yz00) * wz - (p0 - pF) * cy0;
+    ax[3] = (sB - s1) * cy1 + (xy11 - xy01) * wx + (yz11 - yz10) * wz - (pB - p0) * cy1;
+    ax[4] = (s2 - sD) * cz0 + (xz10 - xz00) * wx + (yz10 - yz00) * wy - (p0 - pD) * cz0;
+    ax[5] = (sU - s2) * cz1 + (xz11 - xz01) * wx + (yz11 - yz01) * wy - (pU - p0) * cz1;
+}
+
+// Cell of thread t in colour col (cells with (i + j + k) of one parity), or
+// false when the slot is past the last cell of its line.
+template <typename T>
+__device__ __forceinline__ bool colour_cell(const LevelView<T> &L, int col, long t, int &i, int &j, int &k)
+{
+    const int half = L.ny / 2;
+    const long lines = (long)(L.nx - 1) * (L.nz - 1);
+    if (t >= lines * half) return false;
+    const int jj = (int)(t % half);
+    const long line = t / half;
+    i = 1 + (int)(line % (L.nx - 1));
+    k = 1 + (int)(line / (L.nx - 1));
+    j = ((((1 + i + k) & 1) == col) ? 1 : 2) + 2 * jj;
+    return j <= L.ny - 1;
+}
+
+// the six faces of cell (i, j, k): low and high x, y, z faces
+template <typename T>
+__device__ __forceinline__ void cell_faces(const LevelView<T> &L, int i, int j, int k, int fi[6])
+{
     fi[0] = P2IDX(L, i - 1, j - 1, k - 1);
     fi[1] = P2IDX(L, i, j - 1, k - 1);
     fi[2] = fi[0];
     fi[3] = P2IDX(L, i - 1, j, k - 1);
     fi[4] = fi[0];
     fi[5] = P2IDX(L, i - 1, j - 1, k);
+}
+
+// ---------------------------------------------------------------------------
+// k_vanka_full with the six momentum residuals from cell_rows (shared
+// stresses): same terms as row_vx/row_vy/row_vz, about half the loads and
+// arithmetic.  The cell system is built and eliminated on every sweep.
+template <typename T>
+__global__ void __launch_bounds__(128) k_vanka_fast(LevelView<T> L, T *P, Vec4<T> vin, Vec4<T> vout, Vec4<T> b,
+                                                    T omega, int col)
+{
+    int i, j, k;
+    if (!colour_cell(L, col, (long)blockIdx.x * blockDim.x + threadIdx.x, i, j, k)) return;
+    Fields<T, T> x{P, vin.c[1], vin.c[2], vin.c[3]};
+    const int u = P2IDX(L, i, j, k);
+    const bool pact = (L.bcm[u] & BC_P) == 0;
+    int fi[6];
+    const int fc[6] = {1, 1, 2, 2, 3, 3};
+    cell_faces(L, i, j, k, fi);
     const T g[6] = {-L.ax.ihc[i - 1], L.ax.ihc[i], -L.ay.ihc[j - 1], L.ay.ihc[j], -L.az.ihc[k - 1], L.az.ihc[k]};
     const T hx = L.ax.ih[i], hy = L.ay.ih[j], hz = L.az.ih[k];
     const T cc[6] = {-hx, hx, -hy, hy, -hz, hz};
-    // the cell's strain rates and normal stresses
-    const T exx = (ld<T>(x.vx, fi[1]) - ld<T>(x.vx, fi[0])) * hx;
-    const T eyy = (ld<T>(x.vy, fi[3]) - ld<T>(x.vy, fi[0])) * hy;
-    const T ezz = (ld<T>(x.vz, fi[5]) - ld<T>(x.vz, fi[0])) * hz;
-    const T div3 = (exx + eyy + ezz) / (T)3.0;
-    const T E2 = (T)2.0 * eta_at(L, L.ec, u);
-    const T s0 = E2 * (exx - div3), s1 = E2 * (eyy - div3), s2 = E2 * (ezz - div3);
-    // neighbour cells' normal stress along the face normal
-    const T sL = snn(L, x, 0, i - 1, j, k), sR = snn(L, x, 0, i + 1, j, k);
-    const T sF = snn(L, x, 1, i, j - 1, k), sB = snn(L, x, 1, i, j + 1, k);
-    const T sD = snn(L, x, 2, i, j, k - 1), sU = snn(L, x, 2, i, j, k + 1);
-    // the twelve edge shear stresses
-    const T xy00 = sxy(L, x, i - 1, j - 1, k - 1), xy01 = sxy(L, x, i - 1, j, k - 1);
-    const T xy10 = sxy(L, x, i, j - 1, k - 1), xy11 = sxy(L, x, i, j, k - 1);
-    const T xz00 = sxz(L, x, i - 1, j - 1, k - 1), xz01 = sxz(L, x, i - 1, j - 1, k);
-    const T xz10 = sxz(L, x, i, j - 1, k - 1), xz11 = sxz(L, x, i, j - 1, k);
-    const T yz00 = syz(L, x, i - 1, j - 1, k - 1), yz01 = syz(L, x, i - 1, j - 1, k);
-    const T yz10 = syz(L, x, i - 1, j, k - 1), yz11 = syz(L, x, i - 1, j, k);
-    const T p0 = ld<T>(x.p, u);
-    const T pL = ld<T>(x.p, P2IDX(L, i - 1, j, k)), pR = ld<T>(x.p, P2IDX(L, i + 1, j, k));
-    const T pF = ld<T>(x.p, P2IDX(L, i, j - 1, k)), pB = ld<T>(x.p, P2IDX(L, i, j + 1, k));
-    const T pD = ld<T>(x.p, P2IDX(L, i, j, k - 1)), pU = ld<T>(x.p, P2IDX(L, i, j, k + 1));
-    T ax[6];
-    ax[0] = (s0 - sL) * L.ax.ihc[i - 1] + (xy01 - xy00) * L.ay.ihv[j - 1] + (xz01 - xz00) * L.az.ihv[k - 1] -
-            (p0 - pL) * L.ax.ihc[i - 1];
-    ax[1] = (sR - s0) * L.ax.ihc[i] + (xy11 - xy10) * L.ay.ihv[j - 1] + (xz11 - xz10) * L.az.ihv[k - 1] -
-            (pR - p0) * L.ax.ihc[i];
-    ax[2] = (s1 - sF) * L.ay.ihc[j - 1] + (xy10 - xy00) * L.ax.ihv[i - 1] + (yz01 - yz00) * L.az.ihv[k - 1] -
-            (p0 - pF) * L.ay.ihc[j - 1];
-    ax[3] = (sB - s1) * L.ay.ihc[j] + (xy11 - xy01) * L.ax.ihv[i - 1] + (yz11 - yz10) * L.az.ihv[k - 1] -
-            (pB - p0) * L.ay.ihc[j];
-    ax[4] = (s2 - sD) * L.az.ihc[k - 1] + (xz10 - xz00) * L.ax.ihv[i - 1] + (yz10 - yz00) * L.ay.ihv[j - 1] -
-            (p0 - pD) * L.az.ihc[k - 1];
-    ax[5] = (sU - s2) * L.az.ihc[k] + (xz11 - xz01) * L.ax.ihv[i - 1] + (yz11 - yz01) * L.ay.ihv[j - 1] -
-            (pU - p0) * L.az.ihc[k];
+    T ax[6], div;
+    cell_rows(L, x, i, j, k, fi, ax, div);
     T M[6][6];
     face_block(L, i, j, k, M);
     M[0][0] = diag_vx(L, i - 1, j - 1, k - 1);
@@ -430,7 +498,7 @@ __global__ void __launch_bounds__(128) k_vanka_fast(LevelView<T> L, T *P, Vec4<T
     }
     T dp = 0;
     if (pact) {
-        T num = -(b.c[0][u] - (exx + eyy + ezz)), den = 0;
+        T num = -(b.c[0][u] - div), den = 0;
 #pragma unroll
         for (int q = 0; q < 6; q++) {
             num += cc[q] * y1[q];
@@ -440,6 +508,176 @@ __global__ void __launch_bounds__(128) k_vanka_fast(LevelView<T> L, T *P, Vec4<T
             dp = num / den;
             P[u] += omega * dp;
         }
+    }
+#pragma unroll
+    for (int q = 0; q < 6; q++)
+        if (act[q]) vout.c[fc[q]][fi[q]] = vin.c[fc[q]][fi[q]] + omega * (y1[q] - dp * y2[q]);
+}
+
+// ---------------------------------------------------------------------------
+// Full cell-block smoother with stored cell factors.  The masked cell system
+// of k_vanka_full depends on the viscosities and the grid only, so once per
+// solve k_vanka_factor inverts the 6x6 face block M of every cell of one
+// colour (Gauss-Jordan without pivoting: -M is diagonally dominant; in FP64,
+// also for the FP32 cycle, whose factors are stored rounded to float).
+// Scaled by the faces' control volumes the block is symmetric: with
+// V'_a = ih / ihc along face a's normal (the face's control volume over the
+// cell's), S = diag(V') M = S^T, so M^-1 = S^-1 diag(V') with S^-1 symmetric,
+// and V'_a g_a = cc_a (the continuity coefficients).  Stored per cell,
+// entry-major so that a warp's loads are coalesced:
+//   entries 0..20  the upper triangle of S^-1 row by row (rows and columns
+//                  of held faces zero);
+//   entry 21       1/den, den = cc . S^-1 cc (0 where the cell pressure is a
+//                  boundary unknown or den = 0, which holds the pressure).
+// The sweep (k_vanka_stored) assembles the residuals with cell_rows and
+// applies the stored factors: y1 = S^-1 (V' r), y2 = S^-1 cc,
+// dp = (cc . y1 - r_p) / den, v += omega (y1 - dp y2), p += omega dp; the
+// same update as k_vanka_full up to rounding, without building and
+// eliminating the 6x6 block on every sweep.
+constexpr int kBlkEntries = 22;
+// minimum resident blocks per SM asked of the compiler for k_vanka_stored
+// (FP32 cycle; the FP64 cycle's kernel needs more registers)
+#ifndef P2_STORED_MIN_BLOCKS
+#define P2_STORED_MIN_BLOCKS 7
+#endif
+
+// packed upper-triangle index of (a, c), a <= c
+__host__ __device__ constexpr int tri_index(int a, int c) { return a * 6 - a * (a - 1) / 2 + (c - a); }
+
+template <typename T>
+__device__ __forceinline__ T face_ratio(T ih, T ihc) { return ih / ihc; }
+template <>
+__device__ __forceinline__ float face_ratio<float>(float ih, float ihc) { return __fdividef(ih, ihc); }
+
+template <typename T>
+__device__ __forceinline__ void face_volumes(const LevelView<T> &L, int i, int j, int k, T v[6])
+{
+    const T hx = L.ax.ih[i], hy = L.ay.ih[j], hz = L.az.ih[k];
+    v[0] = face_ratio(hx, L.ax.ihc[i - 1]);
+    v[1] = face_ratio(hx, L.ax.ihc[i]);
+    v[2] = face_ratio(hy, L.ay.ihc[j - 1]);
+    v[3] = face_ratio(hy, L.ay.ihc[j]);
+    v[4] = face_ratio(hz, L.az.ihc[k - 1]);
+    v[5] = face_ratio(hz, L.az.ihc[k]);
+}
+
+template <typename T, typename S>
+__global__ void __launch_bounds__(128) k_vanka_factor(LevelView<T> L, int col, S *blk, long stride)
+{
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    int i, j, k;
+    if (!colour_cell(L, col, t, i, j, k)) return;
+    const int u = P2IDX(L, i, j, k);
+    int fi[6];
+    const int fc[6] = {1, 1, 2, 2, 3, 3};
+    cell_faces(L, i, j, k, fi);
+    const T hx = L.ax.ih[i], hy = L.ay.ih[j], hz = L.az.ih[k];
+    const T cc[6] = {-hx, hx, -hy, hy, -hz, hz};
+    T M[6][6];
+    face_block(L, i, j, k, M);
+    M[0][0] = diag_vx(L, i - 1, j - 1, k - 1);
+    M[1][1] = diag_vx(L, i, j - 1, k - 1);
+    M[2][2] = diag_vy(L, i - 1, j - 1, k - 1);
+    M[3][3] = diag_vy(L, i - 1, j, k - 1);
+    M[4][4] = diag_vz(L, i - 1, j - 1, k - 1);
+    M[5][5] = diag_vz(L, i - 1, j - 1, k);
+    bool act[6];
+#pragma unroll
+    for (int q = 0; q < 6; q++) act[q] = !(L.bcm[fi[q]] & (1 << fc[q]));
+#pragma unroll
+    for (int a = 0; a < 6; a++)
+#pragma unroll
+        for (int c = 0; c < 6; c++)
+            if (!(act[a] && act[c])) M[a][c] = a == c ? (T)1 : (T)0;
+    // in-place Gauss-Jordan inverse
+#pragma unroll
+    for (int c = 0; c < 6; c++) {
+        const T ip = (T)1 / M[c][c];
+        M[c][c] = (T)1;
+#pragma unroll
+        for (int e = 0; e < 6; e++) M[c][e] *= ip;
+#pragma unroll
+        for (int a = 0; a < 6; a++) {
+            if (a != c) {
+                const T f = M[a][c];
+                M[a][c] = (T)0;
+#pragma unroll
+                for (int e = 0; e < 6; e++) M[a][e] -= f * M[c][e];
+            }
+        }
+    }
+    // S^-1 = M^-1 diag(V')^-1, symmetrised; held rows and columns zero
+    T v[6];
+    face_volumes(L, i, j, k, v);
+#pragma unroll
+    for (int a = 0; a < 6; a++)
+#pragma unroll
+        for (int c = 0; c < 6; c++)
+            M[a][c] = (act[a] && act[c]) ? M[a][c] / v[c] : (T)0;
+    T den = 0;
+#pragma unroll
+    for (int a = 0; a < 6; a++) {
+        T y2 = 0;
+#pragma unroll
+        for (int c = 0; c < 6; c++) y2 += (T)0.5 * (M[a][c] + M[c][a]) * cc[c];
+        den += cc[a] * y2;
+    }
+#pragma unroll
+    for (int a = 0; a < 6; a++)
+#pragma unroll
+        for (int c = a; c < 6; c++) blk[(long)tri_index(a, c) * stride + t] = (S)((T)0.5 * (M[a][c] + M[c][a]));
+    const bool pact = (L.bcm[u] & BC_P) == 0;
+    blk[21L * stride + t] = (S)((pact && den != (T)0) ? (T)1 / den : (T)0);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(128, sizeof(T) == 4 ? P2_STORED_MIN_BLOCKS : 3) k_vanka_stored(
+    LevelView<T> L, T *P, Vec4<T> vin, Vec4<T> vout, Vec4<T> b, T omega, int col, const T *__restrict__ blk,
+    long stride)
+{
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    int i, j, k;
+    if (!colour_cell(L, col, t, i, j, k)) return;
+    Fields<T, T> x{P, vin.c[1], vin.c[2], vin.c[3]};
+    const int u = P2IDX(L, i, j, k);
+    int fi[6];
+    const int fc[6] = {1, 1, 2, 2, 3, 3};
+    cell_faces(L, i, j, k, fi);
+    T ax[6], div;
+    cell_rows(L, x, i, j, k, fi, ax, div);
+    const T hx = L.ax.ih[i], hy = L.ay.ih[j], hz = L.az.ih[k];
+    const T cc[6] = {-hx, hx, -hy, hy, -hz, hz};
+    T v[6];
+    face_volumes(L, i, j, k, v);
+    bool act[6];
+    T vr[6];
+#pragma unroll
+    for (int q = 0; q < 6; q++) {
+        act[q] = !(L.bcm[fi[q]] & (1 << fc[q]));
+        vr[q] = act[q] ? (b.c[fc[q]][fi[q]] - ax[q]) * v[q] : (T)0;
+    }
+    T y1[6] = {0, 0, 0, 0, 0, 0}, y2[6] = {0, 0, 0, 0, 0, 0};
+#pragma unroll
+    for (int a = 0; a < 6; a++) {
+#pragma unroll
+        for (int c = a; c < 6; c++) {
+            const T m = __ldg(blk + (long)tri_index(a, c) * stride + t);
+            y1[a] += m * vr[c];
+            y2[a] += m * cc[c];
+            if (c != a) {
+                y1[c] += m * vr[a];
+                y2[c] += m * cc[a];
+            }
+        }
+    }
+    const T inv = __ldg(blk + 21L * stride + t);
+    T dp = 0;
+    if (inv != (T)0) {
+        T num = -(b.c[0][u] - div);
+#pragma unroll
+        for (int q = 0; q < 6; q++) num += cc[q] * y1[q];
+        dp = num * inv;
+        P[u] += omega * dp;
     }
 #pragma unroll
     for (int q = 0; q < 6; q++)
@@ -715,20 +953,30 @@ __device__ __forceinline__ double block_sum(double v, double *sh)
 
 // nd dot products of 4-field vectors: out[q] = sum a_q . b_q (pairs given by
 // pointer tables), skipping the pinned pressure cell when skip_node >= 0.
+// One sweep over the nodes for all pairs: a vector shared by several pairs
+// (the new direction against every stored one) comes from DRAM once and is
+// re-read from L1.
 __global__ void k_dots_partial(DotJobs jobs, int n, int skip_node, double *partial)
 {
     __shared__ double sh[32];
-    for (int q = 0; q < jobs.nd; q++) {
-        double s = 0;
-        for (int c = 0; c < 4; c++) {
-            const double *a = jobs.j[q].a[c], *b = jobs.j[q].b[c];
-            for (int u = blockIdx.x * blockDim.x + threadIdx.x; u < n; u += gridDim.x * blockDim.x) {
-                if (c == 0 && u == skip_node) continue;
-                s += a[u] * b[u];
-            }
+    double s[kMaxDots];
+#pragma unroll
+    for (int q = 0; q < kMaxDots; q++) s[q] = 0;
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+        for (int u = blockIdx.x * blockDim.x + threadIdx.x; u < n; u += gridDim.x * blockDim.x) {
+            if (c == 0 && u == skip_node) continue;
+#pragma unroll
+            for (int q = 0; q < kMaxDots; q++)
+                if (q < jobs.nd) s[q] += jobs.j[q].a[c][u] * jobs.j[q].b[c][u];
         }
-        double t = block_sum(s, sh);
-        if (threadIdx.x == 0) partial[q * gridDim.x + blockIdx.x] = t;
+    }
+#pragma unroll
+    for (int q = 0; q < kMaxDots; q++) {
+        if (q < jobs.nd) {  // uniform over the block: the barriers in block_sum are safe
+            const double t = block_sum(s[q], sh);
+            if (threadIdx.x == 0) partial[q * gridDim.x + blockIdx.x] = t;
+        }
     }
 }
 

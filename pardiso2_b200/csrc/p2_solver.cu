@@ -36,6 +36,7 @@ void *DeviceArena::alloc(size_t bytes)
 {
     void *p = nullptr;
     if (bytes == 0) bytes = 16;
+    bytes += guard;
     cudaError_t e = cudaMalloc(&p, bytes);
     if (e != cudaSuccess) {
         cudaGetLastError();
@@ -221,6 +222,13 @@ void Solver::set_grid(long nx, long ny, long nz, const double *gx, const double 
     if (p.p2koef != 0.0) throw Error(P2_ERR_UNSUPPORTED, "p2koef != 0 (grad-div term) is not supported");
     drop_graphs();
     arena.release();
+    // The cell-block smoothers load the neighbour cells of every cell,
+    // including the cell layer above the top one (its values are masked,
+    // since the top faces are boundary rows): one plane past the end of a
+    // level array.  Every level allocation carries a zero-filled plane of
+    // the finest level (the largest) after its end, so those loads stay in
+    // the allocation.
+    arena.guard = sizeof(double) * ((size_t)nx * ny + ny + 2);
     grid_arena.release();
     marker_arena.release();  // markers and their buffers belong to the previous grid
     move_arena.release();
@@ -468,6 +476,12 @@ void Solver::allocate_work()
             v.n = (int)n;
         };
         v32(Lv.x32); v32(Lv.y32); v32(Lv.b32); v32(Lv.r32);
+        {
+            const long slots = (long)(Lv.nx - 1) * (Lv.nz - 1) * (Lv.ny / 2);
+            Lv.blk_stride = (slots + 31) / 32 * 32;
+            const size_t tsz = prm.precision == 0 ? sizeof(float) : sizeof(double);
+            Lv.blk = arena.alloc(tsz * 2 * kBlkEntries * (size_t)Lv.blk_stride);
+        }
         if (prm.precision == 1 || l == 0) { v64(Lv.x64); v64(Lv.y64); v64(Lv.b64); v64(Lv.r64); }
         if (prm.precision == 1 && l > 0) {}
     }
@@ -743,6 +757,51 @@ Vec4<float> &r_of<float>(Level &Lv) { return Lv.r32; }
 template <>
 Vec4<double> &r_of<double>(Level &Lv) { return Lv.r64; }
 
+// One colour pass of the selected smoother on level l.
+template <typename T>
+void Solver::smoother_pass(int l, const LevelView<T> &V, T *P, Vec4<T> &vin, Vec4<T> &vout, Vec4<T> &b, int col)
+{
+    Level &Lv = L[l];
+    const long cells = (long)(Lv.nx - 1) * (Lv.nz - 1) * (Lv.ny / 2);
+    const T om = (T)prm.omega;
+    switch (prm.smoother) {
+    case 1: {
+        const T *blk = (const T *)Lv.blk + (size_t)col * kBlkEntries * Lv.blk_stride;
+        k_vanka_stored<T><<<nblk(cells, 128), 128, 0, st>>>(V, P, vin, vout, b, om, col, blk, Lv.blk_stride);
+        break;
+    }
+    case 2: k_vanka_full<T><<<nblk(cells, 128), 128, 0, st>>>(V, P, vin, vout, b, om, col); break;
+    case 3: k_vanka_fast<T><<<nblk(cells, 128), 128, 0, st>>>(V, P, vin, vout, b, om, col); break;
+    default: k_vanka<T><<<nblk(cells), kThreads, 0, st>>>(V, P, vin, vout, b, om, col); break;
+    }
+    P2_COUNT_LAUNCH();
+}
+
+// Cell factors of the stored-factor smoother on every level, both colours
+// (the level viscosities must be current), computed in FP64 and stored in
+// the V-cycle's type T.
+template <typename T>
+void Solver::factor_smoother()
+{
+    for (int l = 0; l < (int)L.size(); l++) {
+        Level &Lv = L[l];
+        LevelView<double> V = view<double>(l, false);
+        const long cells = (long)(Lv.nx - 1) * (Lv.nz - 1) * (Lv.ny / 2);
+        for (int col = 0; col < 2; col++) {
+            T *blk = (T *)Lv.blk + (size_t)col * kBlkEntries * Lv.blk_stride;
+            k_vanka_factor<double, T><<<nblk(cells, 128), 128, 0, st>>>(V, col, blk, Lv.blk_stride); P2_COUNT_LAUNCH();
+        }
+    }
+    P2_CUDA_TRY(cudaGetLastError());
+}
+
+void Solver::factor_cells()
+{
+    if (prm.smoother != 1) return;
+    if (prm.precision == 0) factor_smoother<float>();
+    else factor_smoother<double>();
+}
+
 template <typename T>
 void Solver::smooth(int l, int sweeps)
 {
@@ -751,8 +810,6 @@ void Solver::smooth(int l, int sweeps)
     Vec4<T> &x = vx_of<T>(Lv, 0), &y = vx_of<T>(Lv, 1), &b = b_of<T>(Lv);
     bc_set<T>(l, x, b);
     if (sweeps <= 0) return;
-    long cells = (long)(Lv.nx - 1) * (Lv.nz - 1) * (Lv.ny / 2);
-    T om = (T)prm.omega;
     // colour 0 reads velocities from x and writes y, colour 1 goes back; the
     // pressure is updated in place in x.c[0] (yy shares it)
     Vec4<T> yy = y;
@@ -760,13 +817,7 @@ void Solver::smooth(int l, int sweeps)
     for (int s = 0; s < sweeps; s++) {
         for (int col = 0; col < 2; col++) {
             Vec4<T> &vin = col ? yy : x, &vout = col ? x : yy;
-            if (prm.smoother == 1) {
-                k_vanka_fast<T><<<nblk(cells, 128), 128, 0, st>>>(V, x.c[0], vin, vout, b, om, col); P2_COUNT_LAUNCH();
-            } else if (prm.smoother == 2) {
-                k_vanka_full<T><<<nblk(cells, 128), 128, 0, st>>>(V, x.c[0], vin, vout, b, om, col); P2_COUNT_LAUNCH();
-            } else {
-                k_vanka<T><<<nblk(cells), kThreads, 0, st>>>(V, x.c[0], vin, vout, b, om, col); P2_COUNT_LAUNCH();
-            }
+            smoother_pass<T>(l, V, x.c[0], vin, vout, b, col);
             bc_set<T>(l, vout, b);
         }
     }
@@ -933,6 +984,7 @@ p2_solve_info Solver::solve()
     long n = L0.n;
     P2_CUDA_TRY(cudaEventRecord(ev[0], st));
     set_nodes_device();
+    factor_cells();
     coarse_setup();
     P2_CUDA_TRY(cudaEventRecord(ev[1], st));
     if (verbose) {
@@ -1222,38 +1274,18 @@ double Solver::debug_time_smoother(int l, int passes)
     if (l < 0 || l >= (int)L.size() || passes < 2) throw Error(P2_ERR_ARG, "bad level or pass count");
     if (!bc_ready) throw Error(P2_ERR_STATE, "no level data");
     Level &Lv = L[l];
-    long cells = (long)(Lv.nx - 1) * (Lv.nz - 1) * (Lv.ny / 2);
+    factor_cells();
     P2_CUDA_TRY(cudaEventRecord(ev[5], st));
-    if (prm.precision == 0 || l > 0) {
+    if (prm.precision == 0) {
         LevelView<float> V = view<float>(l, false);
         Vec4<float> x = Lv.x32, y = Lv.y32;
         y.c[0] = x.c[0];
-        for (int p = 0; p < passes; p++) {
-            if (prm.smoother == 1)
-                k_vanka_fast<float><<<nblk(cells, 128), 128, 0, st>>>(V, x.c[0], (p & 1) ? y : x, (p & 1) ? x : y,
-                                                                      Lv.b32, (float)prm.omega, p & 1);
-            else if (prm.smoother == 2)
-                k_vanka_full<float><<<nblk(cells, 128), 128, 0, st>>>(V, x.c[0], (p & 1) ? y : x, (p & 1) ? x : y,
-                                                                      Lv.b32, (float)prm.omega, p & 1);
-            else
-                k_vanka<float><<<nblk(cells), kThreads, 0, st>>>(V, x.c[0], (p & 1) ? y : x, (p & 1) ? x : y,
-                                                                 Lv.b32, (float)prm.omega, p & 1);
-        }
+        for (int p = 0; p < passes; p++) smoother_pass<float>(l, V, x.c[0], (p & 1) ? y : x, (p & 1) ? x : y, Lv.b32, p & 1);
     } else {
         LevelView<double> V = view<double>(l, false);
         Vec4<double> x = Lv.x64, y = Lv.y64;
         y.c[0] = x.c[0];
-        for (int p = 0; p < passes; p++) {
-            if (prm.smoother == 1)
-                k_vanka_fast<double><<<nblk(cells, 128), 128, 0, st>>>(V, x.c[0], (p & 1) ? y : x, (p & 1) ? x : y,
-                                                                       Lv.b64, prm.omega, p & 1);
-            else if (prm.smoother == 2)
-                k_vanka_full<double><<<nblk(cells, 128), 128, 0, st>>>(V, x.c[0], (p & 1) ? y : x, (p & 1) ? x : y,
-                                                                       Lv.b64, prm.omega, p & 1);
-            else
-                k_vanka<double><<<nblk(cells), kThreads, 0, st>>>(V, x.c[0], (p & 1) ? y : x, (p & 1) ? x : y,
-                                                                  Lv.b64, prm.omega, p & 1);
-        }
+        for (int p = 0; p < passes; p++) smoother_pass<double>(l, V, x.c[0], (p & 1) ? y : x, (p & 1) ? x : y, Lv.b64, p & 1);
     }
     P2_CUDA_TRY(cudaEventRecord(ev[6], st));
     P2_CUDA_TRY(cudaEventSynchronize(ev[6]));

@@ -13,6 +13,7 @@ namespace p2 {
 
 struct DeviceArena {
     std::vector<void *> ptrs;
+    size_t guard = 0;  // zero-filled bytes appended to every allocation
     void *alloc(size_t bytes);
     void release();
 };
@@ -40,6 +41,10 @@ struct Level {
     int pin = -1;
     double pinval = 0;
     double compat_vol = 0;        // total volume of the non-boundary pressure cells
+    // stored cell factors of the full cell-block smoother: per colour
+    // kBlkEntries x blk_stride values of the V-cycle's type, entry-major
+    void *blk = nullptr;
+    long blk_stride = 0;
     // boundary rows sorted by copy-chain depth
     int nbc = 0;
     std::vector<int> bc_groups;
@@ -136,6 +141,11 @@ class Solver {
     void bc_set(int l, Vec4<T> &x, Vec4<T> &b);
     template <typename T>
     void smooth(int l, int sweeps);
+    template <typename T>
+    void smoother_pass(int l, const LevelView<T> &V, T *P, Vec4<T> &vin, Vec4<T> &vout, Vec4<T> &b, int col);
+    template <typename T>
+    void factor_smoother();
+    void factor_cells();
     template <typename T>
     void level_residual(int l);
     template <typename T>
