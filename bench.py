@@ -92,14 +92,15 @@ def measured_peaks():
         return 6650.0, "fallback"
 
 
-def profile_traffic():
-    """Per-launch DRAM bytes of the level-0 FP32 smoother pass from the
-    committed ncu summary (None until one is captured)."""
+def profile_traffic(nodes):
+    """DRAM bytes of one level-0 FP32 stored-factor smoother pass from the
+    committed ncu summary (captured at 129^3; the pass streams every node
+    once, so its traffic scales with the node count), or None."""
     p = os.path.join(ROOT, "profiles", "ncu_vanka_stored_f32_level0.txt")
     if not os.path.exists(p):
         return None
-    m = re.search(r"dram_bytes_per_launch:\s*([0-9.eE+]+)", open(p).read())
-    return float(m.group(1)) if m else None
+    m = re.search(r"dram_bytes_per_node:\s*([0-9.eE+]+)", open(p).read())
+    return float(m.group(1)) * nodes if m else None
 
 
 class ClockSampler:
@@ -353,7 +354,8 @@ def run_batch(args, rank, world, local, dist):
         "instance_latency_ms": {"mean": statistics.mean(lat), "max": max(lat), "min": min(lat)},
         "gpu_launches": launches,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": None, "kernel": KERNEL_OF_SMOOTHER[sm_big]
+                     "traffic": profile_traffic(models[big].nodenum) if sm_big == 1 else None,
+                     "kernel": KERNEL_OF_SMOOTHER[sm_big]
                      + " level-0 colour pass, largest instance (%d^3)" % models[big].shape[0], "bytes_per_launch": bytes_per_launch, "ms_per_launch": pass_ms,
                      "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs, burst)"},
         "clocks": clocks,
@@ -435,7 +437,7 @@ def main():
     bytes_per_launch = smoother_bytes(tune.smoother) * n
     achieved = bytes_per_launch / (pass_ms * 1e-3) / 1e9
     peak, peak_kind = measured_peaks()
-    traffic = profile_traffic() if (args.config == CONFIG_IDX and tune.smoother == 1) else None
+    traffic = profile_traffic(n) if tune.smoother == 1 else None
     if args.solve_only:
         if rank == 0:
             print(json.dumps({"metric": METRIC, "value": value, "unit": "ms", "solve_only": True,
