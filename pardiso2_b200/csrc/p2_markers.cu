@@ -99,6 +99,60 @@ __global__ void k_radix_scan(unsigned *hist, long len)
     }
 }
 
+// Device-wide exclusive scan of the histograms (kBuckets * ntiles entries, up
+// to millions at 10^8 markers) in three launches: every block scans
+// kScanChunk consecutive entries and records its total; one block scans the
+// totals (k_radix_scan); every block adds its offset.
+constexpr int kScanThreads = 1024, kScanPer = 4, kScanChunk = kScanThreads * kScanPer;
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_local(unsigned *a, long len, unsigned *block_total)
+{
+    __shared__ unsigned wsum[kScanThreads / 32];
+    const long base = (long)blockIdx.x * kScanChunk + (long)threadIdx.x * kScanPer;
+    unsigned v[kScanPer], s = 0;
+#pragma unroll
+    for (int e = 0; e < kScanPer; e++) {
+        v[e] = base + e < len ? a[base + e] : 0u;
+        s += v[e];
+    }
+    // inclusive scan of the thread sums: warp shuffles, then the warp totals
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    unsigned inc = s;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned t = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += t;
+    }
+    if (lane == 31) wsum[w] = inc;
+    __syncthreads();
+    if (w == 0) {
+        unsigned x = wsum[lane];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned t = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += t;
+        }
+        wsum[lane] = x;  // inclusive over warps
+    }
+    __syncthreads();
+    unsigned run = inc - s + (w > 0 ? wsum[w - 1] : 0u);  // exclusive prefix of this thread
+#pragma unroll
+    for (int e = 0; e < kScanPer; e++) {
+        if (base + e < len) a[base + e] = run;
+        run += v[e];
+    }
+    if (threadIdx.x == kScanThreads - 1) block_total[blockIdx.x] = wsum[31];
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_add(unsigned *a, long len, const unsigned *block_offset)
+{
+    const unsigned off = block_offset[blockIdx.x];
+    const long base = (long)blockIdx.x * kScanChunk + (long)threadIdx.x * kScanPer;
+#pragma unroll
+    for (int e = 0; e < kScanPer; e++)
+        if (base + e < len) a[base + e] += off;
+}
+
 __global__ void k_radix_scatter(long n, const unsigned *key, const unsigned *val, unsigned *key2, unsigned *val2,
                                 int shift, const unsigned *offs, int ntiles)
 {
@@ -589,6 +643,8 @@ void Solver::upload_markers(long nmark, const float *mx, const float *my, const 
     mk_val[0] = (unsigned *)marker_arena.alloc(sizeof(unsigned) * cap);
     mk_val[1] = (unsigned *)marker_arena.alloc(sizeof(unsigned) * cap);
     mk_hist = (unsigned *)marker_arena.alloc(sizeof(unsigned) * (size_t)kBuckets * ntiles);
+    mk_scan = (unsigned *)marker_arena.alloc(sizeof(unsigned) *
+                                             (((size_t)kBuckets * ntiles + kScanChunk - 1) / kScanChunk));
     mk_sorted = (float4 *)marker_arena.alloc(sizeof(float4) * cap);
     const Level &L0 = L[0];
     long ncell = (long)(L0.nx - 1) * (L0.ny - 1) * (L0.nz - 1);
@@ -626,7 +682,11 @@ void Solver::ronurecalc_device()
         for (int p = 0; p < passes; p++) {
             int shift = p * kRadixBits;
             k_radix_hist<<<ntiles, 256, 0, st>>>(n, mk_key[a], shift, mk_hist, ntiles); P2_COUNT_LAUNCH();
-            k_radix_scan<<<1, 1024, 0, st>>>(mk_hist, (long)kBuckets * ntiles); P2_COUNT_LAUNCH();
+            const long hlen = (long)kBuckets * ntiles;
+            const unsigned sblocks = (unsigned)((hlen + kScanChunk - 1) / kScanChunk);
+            k_scan_local<<<sblocks, kScanThreads, 0, st>>>(mk_hist, hlen, mk_scan); P2_COUNT_LAUNCH();
+            k_radix_scan<<<1, 1024, 0, st>>>(mk_scan, (long)sblocks); P2_COUNT_LAUNCH();
+            k_scan_add<<<sblocks, kScanThreads, 0, st>>>(mk_hist, hlen, mk_scan); P2_COUNT_LAUNCH();
             k_radix_scatter<<<ntiles, 256, 0, st>>>(n, mk_key[a], mk_val[a], mk_key[1 - a], mk_val[1 - a], shift,
                                                     mk_hist, ntiles); P2_COUNT_LAUNCH();
             a = 1 - a;

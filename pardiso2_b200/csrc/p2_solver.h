@@ -112,6 +112,7 @@ class Solver {
     float *mk_x = nullptr, *mk_y = nullptr, *mk_z = nullptr;
     signed char *mk_t = nullptr;
     unsigned *mk_key[2] = {nullptr, nullptr}, *mk_val[2] = {nullptr, nullptr}, *mk_hist = nullptr;
+    unsigned *mk_scan = nullptr;  // per-block totals of the histogram scan
     int mk_cur = 0;
     float4 *mk_sorted = nullptr;
     int *cell_start = nullptr, *cell_end = nullptr;
