@@ -18,7 +18,8 @@
  *                      (prototype pardiso/head3mg.c:362); the coarsest
  *                      pardisomat() PARDISO solve, pardiso/gaus3mg_SerieMG.c:64
  *   p2_ronurecalc      void ronurecalc(void), pardiso/mark3mg.c:630
- *                      (prototype pardiso/head3mg.c:417)
+ *                      (prototype pardiso/head3mg.c:417); with power-law
+ *                      rocks p2_ronurecalc_powerlaw
  *   p2_movemark        void movemark(void), pardiso/mark3mg.c:174
  *                      (prototype pardiso/head3mg.c:416)
  * A C shim with the reference's own signatures on top of these calls is in
@@ -149,8 +150,9 @@ p2_status p2_get_solution(p2_ctx *ctx, double *vx, double *vy, double *vz, doubl
 p2_status p2_autotune(p2_ctx *ctx, int trial_iters, p2_tune_info *info);
 
 /* ronurecalc(): marker -> node viscosity/density interpolation.  Rock
- * viscosity is the per-type constant markn0 (pardiso/mark3mg.c:1481-1482;
- * types with markn0 != markn1 are rejected), density markro (densimod 0).
+ * viscosity is the per-type constant markn0 (pardiso/mark3mg.c:1479-1482;
+ * types 0..20 with markn0 != markn1 are power-law rocks and need
+ * p2_ronurecalc_powerlaw), density markro (densimod 0).
  * nu..nyz are in/out: nodes that receive no marker keep their input value,
  * then every viscosity is clamped to [nubeg, nuend], as in the reference.
  * The fields also become this context's resident node fields. */
@@ -158,6 +160,22 @@ p2_status p2_ronurecalc(p2_ctx *ctx, long nmark, const float *markx, const float
                         const signed char *markt, int nrock, const double *markn0, const double *markn1,
                         const double *markro, float *nu, float *ro, float *nxx, float *nxy, float *nxz,
                         float *nyz);
+
+/* ronurecalc() with power-law rocks (viscalc, pardiso/mark3mg.c:1463-1498):
+ * for a rock type t <= 20 with markn0[t] != markn1[t] a marker's viscosity is
+ * marknu[t] * val1^((1 - markmm[t]) / markmm[t]) clamped to
+ * [markn0[t], markn1[t]], val1 being the marker's strain-rate invariant (what
+ * movemark / p2_movemark_strain leaves per marker); other types as in
+ * p2_ronurecalc.  The power is the device's pow, whose last-place rounding
+ * can differ from the host C library's, so node fields of power-law markers
+ * agree with the reference's to a few units in the last place of a float.
+ * The reference also sets marke to 1e-20 where it is 0 for the markers it
+ * interpolates; that array is the caller's and is not touched here. */
+p2_status p2_ronurecalc_powerlaw(p2_ctx *ctx, long nmark, const float *markx, const float *marky,
+                                 const float *markz, const signed char *markt, int nrock, const double *markn0,
+                                 const double *markn1, const double *markro, const double *marknu,
+                                 const double *markmm, const double *val1, float *nu, float *ro, float *nxx,
+                                 float *nxy, float *nxz, float *nyz);
 
 /* Same interpolation on markers already resident on the device (see
  * p2_upload_markers), writing the resident node fields only. */
@@ -176,14 +194,31 @@ p2_status p2_get_nodes(p2_ctx *ctx, float *nu, float *ro, float *nxx, float *nxy
  * type is below 50 or at least 100; outgrid 2 keeps the motion of markers
  * outside the box orthogonal to the wall.  Positions come out bit-identical
  * to the reference's.  Not reproduced: the strain-rate side outputs (val1,
- * marke), the temperature reset (markk = 0) of markers that leave the box,
- * and the water/melt moves that the reference has switched off.
+ * marke: p2_movemark_strain below), the temperature reset (markk = 0) of
+ * markers that leave the box, and the water/melt moves that the reference
+ * has switched off.
  *   p2_movemark: vx, vy, vz host arrays (float, node layout) and markers in/out;
  *   p2_movemark_resident: the resident markers (p2_upload_markers) with the
  *   solution of the last resident solve; read them with p2_get_markers. */
 p2_status p2_movemark(p2_ctx *ctx, double timestep, int markmod, int outgrid, const float *vx, const float *vy, const float *vz,
                       long nmark, float *markx, float *marky, float *markz, const signed char *markt);
 p2_status p2_movemark_resident(p2_ctx *ctx, double timestep, int markmod, int outgrid, double *ms);
+/* p2_movemark with movemark's strain-rate outputs (mark3mg.c:218-220, 358-410,
+ * 488): val1[m] (double) = the second invariant
+ * sqrt(0.5 (exx^2 + eyy^2 + ezz^2) + exy^2 + exz^2 + eyz^2) of the strain
+ * rate at marker m before the move, interpolated from the node fields
+ * exx..eyz as epscalc1 (mark3mg.c:3244) does, written for the markers that
+ * move; for markers with marke > 0 the brittle strain marke (float, in/out)
+ * grows by timestep times the Runge-Kutta average of the invariant over the
+ * four stage points (markers of type < 100).  The invariant is taken with a
+ * correctly rounded square root where the reference calls pow(x, 0.5): the
+ * two agree to within one unit in the last place.  In the single-velocity
+ * branch (markmod 1) the reference adds an average left from an earlier
+ * marker; here the marker's own invariant is used. */
+p2_status p2_movemark_strain(p2_ctx *ctx, double timestep, int markmod, int outgrid, const float *vx,
+                             const float *vy, const float *vz, const float *exx, const float *eyy, const float *ezz,
+                             const float *exy, const float *exz, const float *eyz, long nmark, float *markx,
+                             float *marky, float *markz, const signed char *markt, double *val1, float *marke);
 p2_status p2_get_markers(p2_ctx *ctx, float *markx, float *marky, float *markz);
 
 /* The post-solve fields of vpiterate (pardiso/move3mgNew.c:2908-3038):

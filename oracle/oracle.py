@@ -46,9 +46,11 @@ def lib() -> C.CDLL:
         L.p2o_rel_residual.argtypes = [C.c_void_p]
         L.p2o_rel_residual.restype = C.c_double
         L.p2o_ronurecalc.argtypes = [C.c_int, C.c_int, C.c_int, _dp, _dp, _dp, C.c_long, _fp, _fp, _fp, _bp,
-                                     _dp, _dp, C.c_double, C.c_double, C.c_double, C.c_int] + [_fp] * 6
+                                     _dp, _dp, C.c_double, C.c_double, C.c_double, C.c_int] + [_fp] * 6 + [
+                                         C.c_void_p] * 4
         L.p2o_movemark.argtypes = [C.c_int, C.c_int, C.c_int, _dp, _dp, _dp, _fp, _fp, _fp, C.c_double, C.c_int,
-                                   C.c_int, C.c_long, _fp, _fp, _fp, _bp, C.c_void_p]
+                                   C.c_int, C.c_long, _fp, _fp, _fp, _bp, C.c_void_p, C.c_void_p, C.c_void_p,
+                                   C.c_void_p]
         L.p2o_stress_strain.argtypes = [C.c_int, C.c_int, C.c_int, _dp, _dp, _dp] + [_fp] * 7 + [
             C.c_double, C.c_double, C.POINTER(C.c_void_p)]
         _lib = L
@@ -72,34 +74,60 @@ def stress_strain(model, vel, nodes, init=0.0):
     return out
 
 
-def ronurecalc(model, init=None):
-    """Marker -> node fields (dict of float32 arrays) computed by the oracle."""
+def ronurecalc(model, init=None, marknu=None, markmm=None, val1=None, markers=None):
+    """Marker -> node fields (dict of float32 arrays) computed by the oracle;
+    with marknu, markmm and val1 (per marker) rock types <= 20 with markn0 !=
+    markn1 take the power-law viscosity.  markers = (x, y, z, type) defaults
+    to the model's."""
     L = lib()
     n = model.nodenum
     keys = ("nu", "ro", "nxx", "nxy", "nxz", "nyz")
     out = {k: (np.array(init[k], np.float32) if init is not None else np.zeros(n, np.float32)) for k in keys}
     p = model.params
     nx, ny, nz = model.shape
-    L.p2o_ronurecalc(nx, ny, nz, model.gx, model.gy, model.gz, model.markx.size, model.markx, model.marky,
-                     model.markz, np.ascontiguousarray(model.markt, np.int8),
+    mx, my, mz, mt = markers if markers is not None else (model.markx, model.marky, model.markz, model.markt)
+    extra = [None] * 4
+    keep = []
+    if val1 is not None:
+        arrs = [np.ascontiguousarray(a, np.float64) for a in (model.rocks.n1, marknu, markmm, val1)]
+        keep += arrs
+        extra = [a.ctypes.data for a in arrs]
+    L.p2o_ronurecalc(nx, ny, nz, model.gx, model.gy, model.gz, np.asarray(mx).size,
+                     np.ascontiguousarray(mx, np.float32), np.ascontiguousarray(my, np.float32),
+                     np.ascontiguousarray(mz, np.float32), np.ascontiguousarray(mt, np.int8),
                      np.ascontiguousarray(model.rocks.n0, np.float64), np.ascontiguousarray(model.rocks.ro, np.float64),
-                     p.nubeg, p.nuend, p.nukoef, p.viscmod, *[out[k] for k in keys])
+                     p.nubeg, p.nuend, p.nukoef, p.viscmod, *[out[k] for k in keys], *extra)
     return out
 
 
-def movemark(model, vel, timestep, markmod=2, outgrid=0, markers=None, markk=None):
+def movemark(model, vel, timestep, markmod=2, outgrid=0, markers=None, markk=None, strain=None, val1=None,
+             marke=None):
     """Marker advection by the oracle: returns new (markx, marky, markz) and,
-    when markk is given, the updated copy of it.  vel = (vx, vy, vz) float32
-    in the node layout; markers defaults to the model's."""
+    when markk is given, the updated copy of it; with strain = (exx, eyy, ezz,
+    exy, exz, eyz) node fields also the updated copies of val1 and marke.
+    vel = (vx, vy, vz) float32 in the node layout; markers defaults to the
+    model's."""
     L = lib()
     nx, ny, nz = model.shape
     mx, my, mz, mt = markers if markers is not None else (model.markx, model.marky, model.markz, model.markt)
     out = [np.array(a, np.float32) for a in (mx, my, mz)]
     kk = None if markk is None else np.array(markk, np.float32)
+    n = out[0].size
+    sp, v1, me = None, None, None
+    keep = []
+    if strain is not None:
+        fields = [np.ascontiguousarray(a, np.float32) for a in strain]
+        keep += fields
+        sp = (C.c_void_p * 6)(*[a.ctypes.data for a in fields])
+        v1 = np.zeros(n, np.float64) if val1 is None else np.array(val1, np.float64)
+        me = np.zeros(n, np.float32) if marke is None else np.array(marke, np.float32)
     L.p2o_movemark(nx, ny, nz, model.gx, model.gy, model.gz, *[np.ascontiguousarray(a, np.float32) for a in vel],
-                   timestep, markmod, outgrid, out[0].size, out[0], out[1], out[2],
-                   np.ascontiguousarray(mt, np.int8), None if kk is None else kk.ctypes.data)
-    return (*out, kk) if kk is not None else tuple(out)
+                   timestep, markmod, outgrid, n, out[0], out[1], out[2],
+                   np.ascontiguousarray(mt, np.int8), None if kk is None else kk.ctypes.data,
+                   None if sp is None else C.cast(sp, C.c_void_p), None if v1 is None else v1.ctypes.data,
+                   None if me is None else me.ctypes.data)
+    res = tuple(out) + ((kk,) if kk is not None else ())
+    return res + ((v1, me) if strain is not None else ())
 
 
 class OracleSolver:

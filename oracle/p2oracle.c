@@ -22,6 +22,7 @@
  *   nu/ro restriction .................... pardiso/move3mgNew.c:3386-3527
  *   pressure reset to pinit .............. pardiso/move3mgNew.c:2834-2855
  *   marker -> node interpolation ......... pardiso/mark3mg.c:630-1133
+ *     (power-law rock viscosity, viscalc 1463-1498)
  *   stresses / strain rates after a solve  pardiso/move3mgNew.c:2908-3038
  *   marker advection (RK4 / simple) ...... pardiso/mark3mg.c:174-629, with
  *     the staggered velocity interpolation vxyzcalc1 2963-3243
@@ -1421,7 +1422,8 @@ static long serch(const double *g, long n, double x)
 void p2o_ronurecalc(int nx, int ny, int nz, const double *gx, const double *gy, const double *gz,
                     long nmark, const float *mx, const float *my, const float *mz, const signed char *mt,
                     const double *markn0, const double *markro, double nubeg, double nuend, double nukoef,
-                    int viscmod, float *nu, float *ro, float *nxx, float *nxy, float *nxz, float *nyz)
+                    int viscmod, float *nu, float *ro, float *nxx, float *nxy, float *nxz, float *nyz,
+                    const double *markn1, const double *marknu, const double *markmm, const double *val1)
 {
     long nn = (long)nx * ny * nz, mm, v;
     double xsize = gx[nx - 1], ysize = gy[ny - 1], zsize = gz[nz - 1];
@@ -1437,6 +1439,13 @@ void p2o_ronurecalc(int nx, int ny, int nz, const double *gx, const double *gy, 
         int t = mt[mm];
         if (!(mx[mm] > 0 && my[mm] > 0 && mz[mm] > 0 && mx[mm] < xsize && my[mm] < ysize && mz[mm] < zsize && t < 50)) continue;
         mnu = markn0[t];
+        /* power-law rock (viscalc, mark3mg.c:1479-1498) when the tables are given */
+        if (val1 && t <= 20 && markn0[t] != markn1[t]) {
+            double n = markmm[t];
+            mnu = marknu[t] * pow(val1[mm] / 1.0, (1 - n) / n);
+            if (mnu < markn0[t]) mnu = markn0[t];
+            if (mnu > markn1[t]) mnu = markn1[t];
+        }
         mro = markro[t];
         if (mnu < nubeg) mnu = nubeg;
         if (mnu > nuend) mnu = nuend;
@@ -1572,9 +1581,100 @@ static void mv_velocity(const mv_grid *G, const float *const v[3], double x, dou
  * below 50 or at least 100; outgrid 2 keeps the motion outside the box
  * orthogonal to the wall.  markk (may be NULL) is set to 0 for moved markers
  * of type below 100 that end outside the box (mark3mg.c:489-494). */
+/* Strain rate at a point (epscalc1, mark3mg.c:3244-3642, non-periodic):
+ * normal components from cell centres, exy/exz/eyz from edges. */
+static void ep_centre(const double *g, long n, long m0, double x, long *lo, double *w0, double *w1)
+{
+    long m = m0;
+    double X = x, d;
+    if (X > (g[m] + g[m + 1]) / 2.0) m += 1;
+    if (m < 1) { m = 1; X = (g[1] + g[0]) / 2.0; }
+    if (m > n - 2) { m = n - 2; X = (g[m] + g[m + 1]) / 2.0; }
+    d = (g[m + 1] - g[m - 1]) / 2.0;
+    *lo = m;
+    *w0 = 1.0 - (-(((g[m] + g[m - 1]) / 2.0 - X) / d));
+    *w1 = 1.0 - ((g[m + 1] + g[m]) / 2.0 - X) / d;
+}
+
+static void ep_line(const double *g, long n, long m0, double x, long *lo, double *w0, double *w1)
+{
+    long m = m0;
+    double X = x, d;
+    if (m < 1) { m = 1; X = g[1]; }
+    if (m > n - 3) { m = n - 3; X = g[m + 1]; }
+    d = g[m + 1] - g[m];
+    *lo = m;
+    *w0 = 1.0 - (-((g[m] - X) / d));
+    *w1 = 1.0 - (g[m + 1] - X) / d;
+}
+
+static void ep_mid(const double *g, long n, long m0, double x, long *lo, double *w0, double *w1)
+{
+    long m = m0;
+    double X = x, d;
+    if (X < (g[m] + g[m + 1]) / 2.0) m -= 1;
+    if (m < 1) { m = 0; X = (g[0] + g[1]) / 2.0; }
+    if (m > n - 3) { m = n - 3; X = (g[m + 1] + g[m + 2]) / 2.0; }
+    d = (g[m + 2] - g[m]) / 2.0;
+    *lo = m;
+    *w0 = 1.0 - (-(((g[m] + g[m + 1]) / 2.0 - X) / d));
+    *w1 = 1.0 - ((g[m + 1] + g[m + 2]) / 2.0 - X) / d;
+}
+
+static double ep_sum(const float *f, const long lo[3], double w[3][2], long nxy, long ny)
+{
+    double s = 0;
+    int a, b, c;
+    for (c = 0; c < 2; c++)
+        for (a = 0; a < 2; a++)
+            for (b = 0; b < 2; b++)
+                s += f[(lo[2] + c) * nxy + (lo[0] + a) * ny + lo[1] + b] * (w[0][a] * w[1][b] * w[2][c]);
+    return s;
+}
+
+/* kind per axis: 0 centre, 1 line, 2 mid */
+static double ep_field(const mv_grid *G, const float *f, const long cell[3], const double p[3], const int kind[3])
+{
+    long lo[3];
+    double w[3][2];
+    int a;
+    for (a = 0; a < 3; a++) {
+        if (kind[a] == 0) ep_centre(G->g[a], G->n[a], cell[a], p[a], &lo[a], &w[a][0], &w[a][1]);
+        else if (kind[a] == 1) ep_line(G->g[a], G->n[a], cell[a], p[a], &lo[a], &w[a][0], &w[a][1]);
+        else ep_mid(G->g[a], G->n[a], cell[a], p[a], &lo[a], &w[a][0], &w[a][1]);
+    }
+    return ep_sum(f, lo, w, G->n[0] * G->n[1], G->n[1]);
+}
+
+/* second invariant of the strain rate at (x, y, z), as movemark forms val1 */
+static double ep_invariant(const mv_grid *G, const float *const e[6], double x, double y, double z)
+{
+    static const int kc[3] = {0, 0, 0}, kxy[3] = {1, 1, 2}, kxz[3] = {1, 2, 1}, kyz[3] = {2, 1, 1};
+    double p[3], ee[6];
+    long cell[3];
+    int a;
+    p[0] = x; p[1] = y; p[2] = z;
+    for (a = 0; a < 3; a++) {
+        if (p[a] < 0) p[a] = 0;
+        if (p[a] > G->size[a]) p[a] = G->size[a];
+        cell[a] = serch(G->g[a], G->n[a], p[a]);
+    }
+    for (a = 0; a < 3; a++) ee[a] = ep_field(G, e[a], cell, p, kc);
+    ee[3] = ep_field(G, e[3], cell, p, kxy);
+    ee[4] = ep_field(G, e[4], cell, p, kxz);
+    ee[5] = ep_field(G, e[5], cell, p, kyz);
+    return pow(0.5 * (ee[0] * ee[0] + ee[1] * ee[1] + ee[2] * ee[2]) + ee[3] * ee[3] + ee[4] * ee[4] + ee[5] * ee[5],
+               0.5);
+}
+
+/* strain: exx..eyz node fields or NULL; then val1 (per marker, written for
+ * moved markers) and marke (brittle strain, in/out) are updated as movemark
+ * does (mark3mg.c:218-220, 358-410, 488; in markmod 1 the marker's own
+ * invariant stands for the stage average). */
 void p2o_movemark(int nx, int ny, int nz, const double *gx, const double *gy, const double *gz, const float *vx,
                   const float *vy, const float *vz, double dt, int markmod, int outgrid, long nmark, float *mx,
-                  float *my, float *mz, const signed char *mt, float *markk)
+                  float *my, float *mz, const signed char *mt, float *markk, const float *const *strain,
+                  double *val1, float *marke)
 {
     mv_grid G;
     const float *v[3];
@@ -1590,13 +1690,28 @@ void p2o_movemark(int nx, int ny, int nz, const double *gx, const double *gy, co
         int t = mt[q];
         int inside = mx[q] >= 0 && my[q] >= 0 && mz[q] >= 0 && x0 <= G.size[0] && y0 <= G.size[1] && z0 <= G.size[2];
         if (!(inside || (outgrid != 1 && (t < 50 || t >= 100)))) continue;
+        int brittle = 0;
+        double e1 = 0, ee0 = 0;
         mv_velocity(&G, v, x0, y0, z0, k1);
+        if (strain) {
+            e1 = ep_invariant(&G, strain, x0, y0, z0);
+            val1[q] = e1;
+            brittle = marke[q] > 0;
+            ee0 = e1;
+        }
         if (markmod == 1) {
             for (a = 0; a < 3; a++) vel[a] = k1[a];
         } else {
+            double e2 = 0, e3 = 0, e4 = 0;
             mv_velocity(&G, v, x0 + k1[0] * dt / 2.0, y0 + k1[1] * dt / 2.0, z0 + k1[2] * dt / 2.0, k2);
+            if (brittle) e2 = ep_invariant(&G, strain, x0 + k1[0] * dt / 2.0, y0 + k1[1] * dt / 2.0, z0 + k1[2] * dt / 2.0);
             mv_velocity(&G, v, x0 + k2[0] * dt / 2.0, y0 + k2[1] * dt / 2.0, z0 + k2[2] * dt / 2.0, k3);
+            if (brittle) e3 = ep_invariant(&G, strain, x0 + k2[0] * dt / 2.0, y0 + k2[1] * dt / 2.0, z0 + k2[2] * dt / 2.0);
             mv_velocity(&G, v, x0 + k3[0] * dt, y0 + k3[1] * dt, z0 + k3[2] * dt, k4);
+            if (brittle) {
+                e4 = ep_invariant(&G, strain, x0 + k3[0] * dt, y0 + k3[1] * dt, z0 + k3[2] * dt);
+                ee0 = (e1 + 2.0 * e2 + 2.0 * e3 + e4) / 6.0;
+            }
             for (a = 0; a < 3; a++) vel[a] = (k1[a] + 2.0 * k2[a] + 2.0 * k3[a] + k4[a]) / 6.0;
         }
         if (outgrid == 2) {
@@ -1607,6 +1722,7 @@ void p2o_movemark(int nx, int ny, int nz, const double *gx, const double *gy, co
         mx[q] = (float)(x0 + dt * vel[0]);
         my[q] = (float)(y0 + dt * vel[1]);
         mz[q] = (float)(z0 + dt * vel[2]);
+        if (brittle && t < 100) marke[q] += (float)(ee0 * dt);
         if (markk && t < 100 &&
             (mx[q] < 0 || my[q] < 0 || mz[q] < 0 || (double)mx[q] > G.size[0] || (double)my[q] > G.size[1] ||
              (double)mz[q] > G.size[2]))

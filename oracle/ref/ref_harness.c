@@ -294,6 +294,14 @@ void p2ref_set_rocks(int nrock, const double *n0, const double *n1, const double
     for (i = 0; i < nrock; i++) { markn0[i] = n0[i]; markn1[i] = n1[i]; markro[i] = rho[i]; marknu[i] = n0[i]; markmm[i] = 1.0; }
 }
 
+/* Power-law rheology parameters per rock type and the markers' val1. */
+void p2ref_set_rheology(int nrock, const double *nu, const double *mm, const double *v1)
+{
+    long i;
+    for (i = 0; i < nrock; i++) { marknu[i] = nu[i]; markmm[i] = mm[i]; }
+    for (i = 0; i < marknum; i++) val1[i] = v1[i];
+}
+
 void p2ref_set_markers(const float *mx, const float *my, const float *mz, const signed char *mt)
 {
     long i;
@@ -410,6 +418,32 @@ void p2ref_set_step(double max_step, double ts)
 }
 
 double p2ref_get_timestep(void) { return timestep; }
+
+/* The stress / strain-rate pass run into vpiterate's own globals (what a
+ * vpiterate call leaves for movemark's strain-rate outputs). */
+void p2ref_update_stress(void)
+{
+    float *g[12];
+    p2ref_stress_strain(stress_globals(g));
+}
+
+void p2ref_set_marke(const float *v)
+{
+    long i;
+    for (i = 0; i < marknum; i++) marke[i] = v[i];
+}
+
+void p2ref_fill_val1(double v)
+{
+    long i;
+    for (i = 0; i < marknum; i++) val1[i] = v;
+}
+
+void p2ref_get_val1_marke(double *ov, float *oe)
+{
+    long i;
+    for (i = 0; i < marknum; i++) { ov[i] = val1[i]; oe[i] = marke[i]; }
+}
 
 void p2ref_fill_markk(float v)
 {

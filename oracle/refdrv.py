@@ -72,6 +72,10 @@ def _load(shim: bool = False) -> C.CDLL:
         lib.p2ref_fill_stress.argtypes = [C.c_float]
         lib.p2ref_get_stress.argtypes = [C.POINTER(C.c_void_p)]
         lib.p2ref_set_step.argtypes = [C.c_double, C.c_double]
+        lib.p2ref_set_marke.argtypes = [_fp]
+        lib.p2ref_set_rheology.argtypes = [C.c_int, _dp, _dp, _dp]
+        lib.p2ref_fill_val1.argtypes = [C.c_double]
+        lib.p2ref_get_val1_marke.argtypes = [_dp, _fp]
         lib.p2ref_get_timestep.restype = C.c_double
         lib.p2ref_get_markers.argtypes = [_fp] * 4
         lib.p2ref_lu_count.restype = C.c_int
@@ -210,6 +214,27 @@ class RefModel:
         out = {k: np.zeros(n, np.float32) for k in self.STRESS_KEYS}
         self.lib.p2ref_get_stress((C.c_void_p * 12)(*[out[k].ctypes.data for k in self.STRESS_KEYS]))
         return out
+
+    def update_stress(self):
+        """Run the stress / strain-rate pass into vpiterate's globals."""
+        self.lib.p2ref_update_stress()
+
+    def set_rheology(self, marknu, markmm, val1):
+        """Power-law parameters per rock type and val1 per marker."""
+        self.lib.p2ref_set_rheology(len(marknu), np.ascontiguousarray(marknu, np.float64),
+                                    np.ascontiguousarray(markmm, np.float64), np.ascontiguousarray(val1, np.float64))
+
+    def set_marke(self, marke):
+        self.lib.p2ref_set_marke(np.ascontiguousarray(marke, np.float32))
+
+    def fill_val1(self, value):
+        self.lib.p2ref_fill_val1(value)
+
+    def val1_marke(self):
+        n = self.m.markx.size
+        v, e = np.zeros(n, np.float64), np.zeros(n, np.float32)
+        self.lib.p2ref_get_val1_marke(v, e)
+        return v, e
 
     def set_step(self, max_step, timestep):
         """maxxystep and timestep, the inputs of vpiterate's time-step limit."""

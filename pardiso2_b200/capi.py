@@ -22,7 +22,7 @@ EXPORTED = ["p2_default_params", "p2_create", "p2_destroy", "p2_last_error", "p2
             "p2_upload_markers", "p2_ronurecalc_resident", "p2_get_nodes", "p2_debug_apply", "p2_debug_restrict",
             "p2_debug_prolong", "p2_debug_level_fields", "p2_debug_time_smoother", "p2_ronurecalc_noalloc", "p2_autotune",
             "p2_movemark", "p2_movemark_resident", "p2_get_markers", "p2_stress_strain",
-            "p2_stokes_solve_batch"]
+            "p2_stokes_solve_batch", "p2_movemark_strain", "p2_ronurecalc_powerlaw"]
 
 
 class Params(C.Structure):
@@ -98,6 +98,11 @@ def load() -> C.CDLL:
     L.p2_stress_strain.argtypes = [vp] + [C.c_void_p] * 12 + [C.POINTER(C.c_double)]
     L.p2_stokes_solve_batch.argtypes = [C.POINTER(vp), C.c_int, C.c_int, C.c_void_p, C.POINTER(C.c_double)]
     L.p2_stokes_solve_batch.restype = C.c_int
+    L.p2_movemark_strain.argtypes = [vp, C.c_double, C.c_int, C.c_int] + [_fp] * 9 + [C.c_long, _fp, _fp, _fp, _bp,
+                                                                                          _dp, _fp]
+    L.p2_movemark_strain.restype = C.c_int
+    L.p2_ronurecalc_powerlaw.argtypes = [vp, C.c_long, _fp, _fp, _fp, _bp, C.c_int] + [_dp] * 6 + [_fp] * 6
+    L.p2_ronurecalc_powerlaw.restype = C.c_int
     for f in ("p2_movemark", "p2_movemark_resident", "p2_get_markers", "p2_stress_strain"):
         getattr(L, f).restype = C.c_int
     for f in ("p2_create", "p2_set_grid", "p2_set_bc", "p2_set_nodes", "p2_stokes_solve", "p2_stokes_solve_resident",
@@ -180,6 +185,19 @@ class Context:
                     "p2_movemark")
         return out
 
+    def movemark_strain(self, timestep: float, vel, strain, markers, val1, marke, markmod: int = 2, outgrid: int = 0):
+        """movemark with its strain-rate outputs: vel = (vx, vy, vz), strain =
+        (exx, eyy, ezz, exy, exz, eyz) float node fields, markers = (x, y, z,
+        type).  Returns new (x, y, z, val1, marke) arrays."""
+        out = [np.array(a, np.float32) for a in markers[:3]]
+        v1 = np.array(val1, np.float64)
+        me = np.array(marke, np.float32)
+        f = [np.ascontiguousarray(a, np.float32) for a in list(vel) + list(strain)]
+        self._check(self.L.p2_movemark_strain(self.h, timestep, markmod, outgrid, *f, out[0].size, out[0], out[1],
+                                              out[2], np.ascontiguousarray(markers[3], np.int8), v1, me),
+                    "p2_movemark_strain")
+        return out[0], out[1], out[2], v1, me
+
     def movemark_resident(self, timestep: float, markmod: int = 2, outgrid: int = 0) -> float:
         ms = C.c_double()
         self._check(self.L.p2_movemark_resident(self.h, timestep, markmod, outgrid, C.byref(ms)), "p2_movemark_resident")
@@ -236,6 +254,20 @@ class Context:
         out = {k: np.zeros(n, np.float32) for k in keys}
         self._check(self.L.p2_get_nodes(self.h, *[_ptr(out[k]) for k in keys]), "p2_get_nodes")
         return out
+
+    def ronurecalc_powerlaw(self, mx, my, mz, mt, n0, n1, ro, nu0, mm, val1, fields: Dict[str, np.ndarray]):
+        """ronurecalc() with power-law rocks: in/out node fields (float32 arrays, modified in place)."""
+        keys = ("nu", "ro", "nxx", "nxy", "nxz", "nyz")
+        for k in keys:
+            if fields[k].dtype != np.float32 or not fields[k].flags.c_contiguous:
+                raise ValueError("node field %s must be a contiguous float32 array" % k)
+        d = [np.ascontiguousarray(a, np.float64) for a in (n0, n1, ro, nu0, mm, val1)]
+        self._check(self.L.p2_ronurecalc_powerlaw(self.h, np.asarray(mx).size, np.ascontiguousarray(mx, np.float32),
+                                                  np.ascontiguousarray(my, np.float32),
+                                                  np.ascontiguousarray(mz, np.float32),
+                                                  np.ascontiguousarray(mt, np.int8), len(d[0]), *d,
+                                                  *[fields[k] for k in keys]), "p2_ronurecalc_powerlaw")
+        return fields
 
     def ronurecalc(self, mx, my, mz, mt, n0, n1, ro, fields: Dict[str, np.ndarray]):
         """ronurecalc(): in/out node fields (dict of float32 arrays, modified in place)."""

@@ -26,11 +26,14 @@
  * markers markx, marky, markz, markt, marknum and the rock tables markn0,
  * markn1, markro (rocknum types); maxxystep and timestep for the time-step
  * limit; timestep, markmod, outgrid for movemark.
+ * With power-law rocks (types <= 20 with markn0 != markn1) ronurecalc also
+ * reads marknu, markmm and val1.
  * Outputs written: vx, vy, vz (float), pr (double), the stresses sxx..syz and
  * strain rates exx..eyz (float) and the limited timestep by vpiterate; nu,
- * ro, nxx, nxy, nxz, nyz by ronurecalc; markx, marky, markz and the markk
- * reset of markers that leave the box by movemark (val1 and marke, the
- * strain-rate side outputs of the CPU movemark, are not updated).
+ * ro, nxx, nxy, nxz, nyz and marke (0 -> 1e-20) by ronurecalc; markx, marky,
+ * markz and the markk
+ * reset of markers that leave the box, val1 (strain-rate invariant per
+ * marker) and marke (brittle strain) by movemark.
  *
  * Errors follow the reference's convention: a message on stdout and exit().
  * The device is 0, or the value of the environment variable P2CUDA_DEVICE.
@@ -131,15 +134,33 @@ void vpiterate(int m0, int f0)
 
 /* pardiso/mark3mg.c:630 (prototype pardiso/head3mg.c:417): marker -> node
  * viscosity and density; markers of type >= 50 are skipped as in the
- * reference, every other type needs markn0 == markn1 (constant viscosity). */
+ * reference; rock types <= 20 with markn0 != markn1 take the power-law
+ * viscosity from val1 (viscalc, mark3mg.c:1463-1498). */
 void ronurecalc(void)
 {
     p2_status st;
     int nrock = rocknum > 0 && rocknum <= MAXTMR ? rocknum : MAXTMR;
+    int t, power_law = 0;
+    long m;
     p2s_setup();
-    st = p2_ronurecalc(p2s_ctx, marknum, markx, marky, markz, (const signed char *)markt, nrock, markn0, markn1,
-                       markro, nu, ro, nxx, nxy, nxz, nyz);
-    if (st != P2_OK) p2s_fail("p2_ronurecalc", st);
+    for (t = 0; t < nrock && t <= 20; t++)
+        if (markn0[t] != markn1[t]) power_law = 1;
+    if (power_law) {
+        /* viscosity from each marker's strain-rate invariant val1 (viscalc) */
+        st = p2_ronurecalc_powerlaw(p2s_ctx, marknum, markx, marky, markz, (const signed char *)markt, nrock, markn0,
+                                    markn1, markro, marknu, markmm, val1, nu, ro, nxx, nxy, nxz, nyz);
+        if (st != P2_OK) p2s_fail("p2_ronurecalc_powerlaw", st);
+    } else {
+        st = p2_ronurecalc(p2s_ctx, marknum, markx, marky, markz, (const signed char *)markt, nrock, markn0, markn1,
+                           markro, nu, ro, nxx, nxy, nxz, nyz);
+        if (st != P2_OK) p2s_fail("p2_ronurecalc", st);
+    }
+    /* viscalc's side effect (mark3mg.c:1477) on the markers ronurecalc visits
+       (mark3mg.c:694): a zero brittle strain becomes 1e-20 */
+    for (m = 0; m < marknum; m++)
+        if (markx[m] > 0 && marky[m] > 0 && markz[m] > 0 && markx[m] < xsize && marky[m] < ysize &&
+            markz[m] < zsize && markt[m] < 50 && marke[m] == 0.0)
+            marke[m] = 1e-20;
 }
 
 /* pardiso/mark3mg.c:174 (prototype pardiso/head3mg.c:416): advect the markers
@@ -165,9 +186,10 @@ void movemark(void)
             was_in[m] = markx[m] >= 0 && marky[m] >= 0 && markz[m] >= 0 && (double)markx[m] <= xsize &&
                         (double)marky[m] <= ysize && (double)markz[m] <= zsize;
     }
-    st = p2_movemark(p2s_ctx, timestep, markmod, outgrid, vx, vy, vz, marknum, markx, marky, markz,
-                     (const signed char *)markt);
-    if (st != P2_OK) p2s_fail("p2_movemark", st);
+    /* exx..eyz as vpiterate left them; val1 and marke per marker */
+    st = p2_movemark_strain(p2s_ctx, timestep, markmod, outgrid, vx, vy, vz, exx, eyy, ezz, exy, exz, eyz, marknum,
+                            markx, marky, markz, (const signed char *)markt, val1, marke);
+    if (st != P2_OK) p2s_fail("p2_movemark_strain", st);
     for (m = 0; m < marknum; m++) {
         int t = markt[m];
         int moved = was_in[m] || (outgrid != 1 && (t < 50 || t >= 100));

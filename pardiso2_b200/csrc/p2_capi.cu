@@ -322,6 +322,32 @@ p2_status p2_ronurecalc(p2_ctx *ctx, long nmark, const float *markx, const float
     return p2_get_nodes(ctx, nu, ro, nxx, nxy, nxz, nyz);
 }
 
+p2_status p2_ronurecalc_powerlaw(p2_ctx *ctx, long nmark, const float *markx, const float *marky,
+                                 const float *markz, const signed char *markt, int nrock, const double *markn0,
+                                 const double *markn1, const double *markro, const double *marknu,
+                                 const double *markmm, const double *val1, float *nu, float *ro, float *nxx,
+                                 float *nxy, float *nxz, float *nyz)
+{
+    p2_status st = guard(ctx, [&] {
+        if (nmark > 0 && (!markx || !marky || !markz || !markt || !val1))
+            throw p2::Error(P2_ERR_ARG, "null marker array");
+        if (!markn0 || !markn1 || !markro || !marknu || !markmm) throw p2::Error(P2_ERR_ARG, "null rock table");
+        p2::Solver &S = *ctx->s;
+        P2_CUDA_TRY(cudaSetDevice(S.dev));
+        S.upload_markers(nmark, markx, marky, markz, markt, nrock, markn0, markn1, markro, marknu, markmm, val1);
+        float *src[6] = {nu, ro, nxx, nxy, nxz, nyz};
+        for (int q = 0; q < 6; q++) {
+            if (!src[q]) throw p2::Error(P2_ERR_ARG, "null node field");
+            P2_CUDA_TRY(cudaMemcpyAsync(S.mk_nodes[q], src[q], sizeof(float) * S.L[0].n, cudaMemcpyHostToDevice,
+                                        S.st));
+        }
+    });
+    if (st != P2_OK) return st;
+    st = p2_ronurecalc_resident(ctx, nullptr);
+    if (st != P2_OK) return st;
+    return p2_get_nodes(ctx, nu, ro, nxx, nxy, nxz, nyz);
+}
+
 p2_status p2_debug_apply(p2_ctx *ctx, int level, const double *x, double *y)
 {
     return guard(ctx, [&] {
@@ -357,6 +383,23 @@ p2_status p2_movemark(p2_ctx *ctx, double timestep, int markmod, int outgrid, co
             throw p2::Error(P2_ERR_ARG, "null argument");
         P2_CUDA_TRY(cudaSetDevice(ctx->s->dev));
         ctx->s->movemark_host(timestep, markmod, outgrid, vx, vy, vz, nmark, markx, marky, markz, markt);
+    });
+}
+
+p2_status p2_movemark_strain(p2_ctx *ctx, double timestep, int markmod, int outgrid, const float *vx,
+                             const float *vy, const float *vz, const float *exx, const float *eyy, const float *ezz,
+                             const float *exy, const float *exz, const float *eyz, long nmark, float *markx,
+                             float *marky, float *markz, const signed char *markt, double *val1, float *marke)
+{
+    return guard(ctx, [&] {
+        if (!vx || !vy || !vz || !exx || !eyy || !ezz || !exy || !exz || !eyz)
+            throw p2::Error(P2_ERR_ARG, "null field");
+        if (nmark > 0 && (!markx || !marky || !markz || !markt || !val1 || !marke))
+            throw p2::Error(P2_ERR_ARG, "null marker array");
+        P2_CUDA_TRY(cudaSetDevice(ctx->s->dev));
+        const float *const e[6] = {exx, eyy, ezz, exy, exz, eyz};
+        ctx->s->movemark_strain_host(timestep, markmod, outgrid, vx, vy, vz, e, nmark, markx, marky, markz, markt,
+                                     val1, marke);
     });
 }
 

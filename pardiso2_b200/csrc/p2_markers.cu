@@ -225,11 +225,14 @@ struct Rock {
     double nu, ro;  // clamped viscosity, density
 };
 
+// power-law table per rock type: {flag, marknu, (1 - n) / n, markn0, markn1}
+constexpr int kPowerLawStride = 5;
+
 __global__ void k_node_gather(int nx, int ny, int nz, const double *gx, const double *gy, const double *gz,
                               const int *start, const int *end, const unsigned *idx, const float4 *mk,
                               const double *rock_f, const double *rock_ro, double nukoef, int viscmod,
                               double nubeg, double nuend, float *nu, float *ro, float *nxx, float *nxy, float *nxz,
-                              float *nyz)
+                              float *nyz, const double *pl = nullptr, const double *val1 = nullptr)
 {
     int u = blockIdx.x * blockDim.x + threadIdx.x;
     if (u >= nx * ny * nz) return;
@@ -273,6 +276,17 @@ __global__ void k_node_gather(int nx, int ny, int nz, const double *gx, const do
         double ddy = __dsub_rn(1.0, fabs(__ddiv_rn(__dsub_rn(gym, (double)m.y), dy)));
         double swt = __dmul_rn(__dmul_rn(ddx, ddy), ddz);
         double f = rock_f[t];
+        if (pl && pl[kPowerLawStride * t] != 0) {
+            // power-law rock (viscalc, mark3mg.c:1489-1498): marknu * val1^((1-n)/n) clamped to
+            // [markn0, markn1], then to [nubeg, nuend]
+            const double *r = pl + kPowerLawStride * t;
+            double mnu = __dmul_rn(r[1], pow(val1[bidx], r[2]));
+            if (mnu < r[3]) mnu = r[3];
+            if (mnu > r[4]) mnu = r[4];
+            if (mnu < nubeg) mnu = nubeg;
+            if (mnu > nuend) mnu = nuend;
+            f = viscmod == 0 ? mnu : (viscmod == 1 ? log(mnu) : __ddiv_rn(1.0, mnu));
+        }
         if (ddx > nukoef && ddy > nukoef && ddz > nukoef) {
             aN = __double2float_rn(__dadd_rn((double)aN, __dmul_rn(f, swt)));
             wN = __dadd_rn(wN, swt);
@@ -421,13 +435,126 @@ __device__ void vxyz_at(const GridSh &G, const float *vx, const float *vy, const
 }
 
 // gridlines in shared memory when they fit (kMoveShBytes), else read in place
+// Strain rate at a point (epscalc1, mark3mg.c:3244-3642, non-periodic box):
+// the normal components from the cell centres, exy / exz / eyz from their
+// edges, each by trilinear weights with the reference's clamping per axis and
+// accumulation order (z outer, x, y inner).  Three axis kinds:
+//   centre  normal strain rates, stored at the cell's upper corner node;
+//   line    the edge direction's nodes (clamped to [1, n-3]);
+//   mid     an axis across the edge: between cell mid-points.
+struct StrainF {
+    const float *e[6];  // exx eyy ezz exy exz eyz, node layout
+};
+
+__device__ __forceinline__ void ax_centre(const double *g, int n, int cell, double x, int &lo, double &w0,
+                                          double &w1)
+{
+    int m = cell;
+    double X = x;
+    if (X > dmid(g, m)) m += 1;
+    if (m < 1) { m = 1; X = __dmul_rn(__dadd_rn(g[1], g[0]), 0.5); }
+    if (m > n - 2) { m = n - 2; X = __dmul_rn(__dadd_rn(g[m], g[m + 1]), 0.5); }
+    const double d = __dmul_rn(__dsub_rn(g[m + 1], g[m - 1]), 0.5);
+    lo = m;
+    w0 = __dsub_rn(1.0, -__ddiv_rn(__dsub_rn(__dmul_rn(__dadd_rn(g[m], g[m - 1]), 0.5), X), d));
+    w1 = __dsub_rn(1.0, __ddiv_rn(__dsub_rn(__dmul_rn(__dadd_rn(g[m + 1], g[m]), 0.5), X), d));
+}
+
+__device__ __forceinline__ void ax_line(const double *g, int n, int cell, double x, int &lo, double &w0, double &w1)
+{
+    int m = cell;
+    double X = x;
+    if (m < 1) { m = 1; X = g[1]; }
+    if (m > n - 3) { m = n - 3; X = g[m + 1]; }
+    const double d = __dsub_rn(g[m + 1], g[m]);
+    lo = m;
+    w0 = __dsub_rn(1.0, -__ddiv_rn(__dsub_rn(g[m], X), d));
+    w1 = __dsub_rn(1.0, __ddiv_rn(__dsub_rn(g[m + 1], X), d));
+}
+
+// as ax_mid, but the lower clamp also applies at m == 0 (mark3mg.c:3408, 3485, 3559)
+__device__ __forceinline__ void ax_mid_eps(const double *g, int n, int cell, double x, int &lo, double &w0,
+                                           double &w1)
+{
+    int m = cell;
+    double X = x;
+    if (X < dmid(g, m)) m -= 1;
+    if (m < 1) { m = 0; X = dmid(g, 0); }
+    if (m > n - 3) { m = n - 3; X = dmid(g, m + 1); }
+    const double d = __dmul_rn(__dsub_rn(g[m + 2], g[m]), 0.5);
+    lo = m;
+    w0 = __dsub_rn(1.0, -__ddiv_rn(__dsub_rn(dmid(g, m), X), d));
+    w1 = __dsub_rn(1.0, __ddiv_rn(__dsub_rn(dmid(g, m + 1), X), d));
+}
+
+// weighted sum over the 8 nodes, z outer, x, y inner
+__device__ __forceinline__ double trilin(const float *f, const int lo[3], const double w[3][2], long nxy, int ny)
+{
+    double s = 0;
+#pragma unroll
+    for (int c = 0; c < 2; c++)
+#pragma unroll
+        for (int a = 0; a < 2; a++)
+#pragma unroll
+            for (int b = 0; b < 2; b++) {
+                const long idx = (long)(lo[2] + c) * nxy + (long)(lo[0] + a) * ny + (lo[1] + b);
+                s = __dadd_rn(s, __dmul_rn((double)__ldg(f + idx), __dmul_rn(__dmul_rn(w[0][a], w[1][b]), w[2][c])));
+            }
+    return s;
+}
+
+// second invariant sqrt(0.5 (exx^2 + eyy^2 + ezz^2) + exy^2 + exz^2 + eyz^2)
+// of the strain rate at (x, y, z) (mark3mg.c:219, 361)
+__device__ double strain_ii(const GridSh &G, const StrainF &S, double x, double y, double z)
+{
+    const double p[3] = {x < 0 ? 0.0 : (x > G.size[0] ? G.size[0] : x), y < 0 ? 0.0 : (y > G.size[1] ? G.size[1] : y),
+                         z < 0 ? 0.0 : (z > G.size[2] ? G.size[2] : z)};
+    int cell[3];
+    for (int a = 0; a < 3; a++) cell[a] = serch(G.g[a], G.n[a], p[a]);
+    const long nxy = (long)G.n[0] * G.n[1];
+    const int ny = G.n[1];
+    int loC[3], loL[3], loM[3];
+    double wC[3][2], wL[3][2], wM[3][2];
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        ax_centre(G.g[a], G.n[a], cell[a], p[a], loC[a], wC[a][0], wC[a][1]);
+        ax_line(G.g[a], G.n[a], cell[a], p[a], loL[a], wL[a][0], wL[a][1]);
+        ax_mid_eps(G.g[a], G.n[a], cell[a], p[a], loM[a], wM[a][0], wM[a][1]);
+    }
+    const double exx = trilin(S.e[0], loC, wC, nxy, ny), eyy = trilin(S.e[1], loC, wC, nxy, ny),
+                 ezz = trilin(S.e[2], loC, wC, nxy, ny);
+    // exy: x, y along the edge's nodes, z between mid-points; exz: x, z lines,
+    // y mid; eyz: y, z lines, x mid
+    int lo[3];
+    double w[3][2];
+    lo[0] = loL[0]; lo[1] = loL[1]; lo[2] = loM[2];
+    w[0][0] = wL[0][0]; w[0][1] = wL[0][1]; w[1][0] = wL[1][0]; w[1][1] = wL[1][1]; w[2][0] = wM[2][0]; w[2][1] = wM[2][1];
+    const double exy = trilin(S.e[3], lo, w, nxy, ny);
+    lo[1] = loM[1]; lo[2] = loL[2];
+    w[1][0] = wM[1][0]; w[1][1] = wM[1][1]; w[2][0] = wL[2][0]; w[2][1] = wL[2][1];
+    const double exz = trilin(S.e[4], lo, w, nxy, ny);
+    lo[0] = loM[0]; lo[1] = loL[1];
+    w[0][0] = wM[0][0]; w[0][1] = wM[0][1]; w[1][0] = wL[1][0]; w[1][1] = wL[1][1];
+    const double eyz = trilin(S.e[5], lo, w, nxy, ny);
+    const double nn = __dadd_rn(__dadd_rn(__dmul_rn(exx, exx), __dmul_rn(eyy, eyy)), __dmul_rn(ezz, ezz));
+    double q = __dmul_rn(0.5, nn);
+    q = __dadd_rn(q, __dmul_rn(exy, exy));
+    q = __dadd_rn(q, __dmul_rn(exz, exz));
+    q = __dadd_rn(q, __dmul_rn(eyz, eyz));
+    return __dsqrt_rn(q);
+}
+
 constexpr int kMoveThreads = 256;
 constexpr int kMoveShBytes = 96 * 1024;
 
+// kStrain: also val1 (strain-rate invariant at the marker before the move) and
+// the brittle strain marke (RK4 of the invariant over the stages, for markers
+// with marke > 0), as movemark does (mark3mg.c:218-220, 358-410, 488).
+template <bool kStrain>
 __global__ void __launch_bounds__(kMoveThreads, 3) k_movemark(long nmark, Grid3 G3, bool shared_grid, const float *vx,
                                                            const float *vy, const float *vz, float *mx, float *my,
                                                            float *mz, const signed char *mt, double dt, int markmod,
-                                                           int outgrid)
+                                                           int outgrid, StrainF S, double *val1, float *marke)
 {
     extern __shared__ double gsh[];
     GridSh G;
@@ -451,19 +578,39 @@ __global__ void __launch_bounds__(kMoveThreads, 3) k_movemark(long nmark, Grid3 
                         (double)fz <= G.size[2];
     if (!(inside || (outgrid != 1 && (t < 50 || t >= 100)))) return;
     double v1[3], v2[3], v3[3], v4[3], v[3];
+    double ee0 = 0;
+    bool brittle = false;
     vxyz_at(G, vx, vy, vz, fx, fy, fz, v1);
+    if constexpr (kStrain) {
+        const double e1 = strain_ii(G, S, fx, fy, fz);
+        val1[q] = e1;
+        brittle = marke[q] > 0;
+        ee0 = e1;  // the single-velocity branch keeps the marker's own rate
+    }
     if (markmod == 1) {  // velocity at the marker (mark3mg.c:317-323)
         for (int a = 0; a < 3; a++) v[a] = v1[a];
     } else {
         // (v dt) / 2 of the reference is v dt rounded, then halved exactly
-        vxyz_at(G, vx, vy, vz, __dadd_rn((double)fx, __dmul_rn(__dmul_rn(v1[0], dt), 0.5)),
-                __dadd_rn((double)fy, __dmul_rn(__dmul_rn(v1[1], dt), 0.5)),
-                __dadd_rn((double)fz, __dmul_rn(__dmul_rn(v1[2], dt), 0.5)), v2);
-        vxyz_at(G, vx, vy, vz, __dadd_rn((double)fx, __dmul_rn(__dmul_rn(v2[0], dt), 0.5)),
-                __dadd_rn((double)fy, __dmul_rn(__dmul_rn(v2[1], dt), 0.5)),
-                __dadd_rn((double)fz, __dmul_rn(__dmul_rn(v2[2], dt), 0.5)), v3);
-        vxyz_at(G, vx, vy, vz, __dadd_rn((double)fx, __dmul_rn(v3[0], dt)), __dadd_rn((double)fy, __dmul_rn(v3[1], dt)),
-                __dadd_rn((double)fz, __dmul_rn(v3[2], dt)), v4);
+        double X[3];
+        for (int a = 0; a < 3; a++) X[a] = __dadd_rn((double)(a == 0 ? fx : a == 1 ? fy : fz), __dmul_rn(__dmul_rn(v1[a], dt), 0.5));
+        vxyz_at(G, vx, vy, vz, X[0], X[1], X[2], v2);
+        double e2 = 0, e3 = 0, e4 = 0;
+        if constexpr (kStrain) {
+            if (brittle) e2 = strain_ii(G, S, X[0], X[1], X[2]);
+        }
+        for (int a = 0; a < 3; a++) X[a] = __dadd_rn((double)(a == 0 ? fx : a == 1 ? fy : fz), __dmul_rn(__dmul_rn(v2[a], dt), 0.5));
+        vxyz_at(G, vx, vy, vz, X[0], X[1], X[2], v3);
+        if constexpr (kStrain) {
+            if (brittle) e3 = strain_ii(G, S, X[0], X[1], X[2]);
+        }
+        for (int a = 0; a < 3; a++) X[a] = __dadd_rn((double)(a == 0 ? fx : a == 1 ? fy : fz), __dmul_rn(v3[a], dt));
+        vxyz_at(G, vx, vy, vz, X[0], X[1], X[2], v4);
+        if constexpr (kStrain) {
+            if (brittle) {
+                e4 = strain_ii(G, S, X[0], X[1], X[2]);
+                ee0 = __ddiv_rn(__dadd_rn(__dadd_rn(__dadd_rn(ee0, __dmul_rn(2.0, e2)), __dmul_rn(2.0, e3)), e4), 6.0);
+            }
+        }
         for (int a = 0; a < 3; a++)
             v[a] = __ddiv_rn(__dadd_rn(__dadd_rn(__dadd_rn(v1[a], __dmul_rn(2.0, v2[a])), __dmul_rn(2.0, v3[a])), v4[a]),
                              6.0);
@@ -476,17 +623,32 @@ __global__ void __launch_bounds__(kMoveThreads, 3) k_movemark(long nmark, Grid3 
     mx[q] = __double2float_rn(__dadd_rn((double)fx, __dmul_rn(dt, v[0])));
     my[q] = __double2float_rn(__dadd_rn((double)fy, __dmul_rn(dt, v[1])));
     mz[q] = __double2float_rn(__dadd_rn((double)fz, __dmul_rn(dt, v[2])));
+    if constexpr (kStrain) {
+        // brittle strain of normal markers (mark3mg.c:488)
+        if (brittle && t < 100) marke[q] = __fadd_rn(marke[q], __double2float_rn(__dmul_rn(ee0, dt)));
+    }
 }
 
 static void launch_movemark(cudaStream_t st, long nmark, const Grid3 &G, const float *const vel[3], float *const pos[3],
-                            const signed char *mt, double dt, int markmod, int outgrid)
+                            const signed char *mt, double dt, int markmod, int outgrid, const StrainF *S = nullptr,
+                            double *val1 = nullptr, float *marke = nullptr)
 {
     const size_t bytes = sizeof(double) * ((size_t)G.n[0] + G.n[1] + G.n[2]);
     const bool sh = bytes <= (size_t)kMoveShBytes;
-    if (sh && bytes > 48 * 1024)
-        P2_CUDA_TRY(cudaFuncSetAttribute(k_movemark, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
-    k_movemark<<<nb(nmark, kMoveThreads), kMoveThreads, sh ? bytes : 0, st>>>(
-        nmark, G, sh, vel[0], vel[1], vel[2], pos[0], pos[1], pos[2], mt, dt, markmod, outgrid); P2_COUNT_LAUNCH();
+    const unsigned grid = nb(nmark, kMoveThreads);
+    if (S) {
+        if (sh && bytes > 48 * 1024)
+            P2_CUDA_TRY(cudaFuncSetAttribute(k_movemark<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+        k_movemark<true><<<grid, kMoveThreads, sh ? bytes : 0, st>>>(nmark, G, sh, vel[0], vel[1], vel[2], pos[0],
+                                                                     pos[1], pos[2], mt, dt, markmod, outgrid, *S,
+                                                                     val1, marke); P2_COUNT_LAUNCH();
+    } else {
+        if (sh && bytes > 48 * 1024)
+            P2_CUDA_TRY(cudaFuncSetAttribute(k_movemark<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+        k_movemark<false><<<grid, kMoveThreads, sh ? bytes : 0, st>>>(nmark, G, sh, vel[0], vel[1], vel[2], pos[0],
+                                                                      pos[1], pos[2], mt, dt, markmod, outgrid,
+                                                                      StrainF{}, nullptr, nullptr); P2_COUNT_LAUNCH();
+    }
     P2_CUDA_TRY(cudaGetLastError());
 }
 
@@ -529,10 +691,55 @@ void Solver::ensure_move_buffers(long nmark)
     }
     if (nmark > mv_cap) {
         move_arena.release();
+        mv_val1 = nullptr;
+        mv_marke = nullptr;
         mv_cap = std::max<long>(nmark, 1);
         for (int q = 0; q < 3; q++) mv_pos[q] = (float *)move_arena.alloc(sizeof(float) * mv_cap);
         mv_type = (signed char *)move_arena.alloc(mv_cap);
     }
+}
+
+// movemark() with its strain-rate outputs, on host arrays: velocities and the
+// strain-rate fields exx..eyz (float, node layout, as vpiterate leaves them),
+// markers in/out, val1 (double per marker) out, marke (float) in/out.
+void Solver::movemark_strain_host(double dt, int markmod, int outgrid, const float *vx, const float *vy,
+                                  const float *vz, const float *const e[6], long nmark, float *mx, float *my, float *mz,
+                                  const signed char *mt, double *val1, float *marke)
+{
+    if (!grid_ready) throw Error(P2_ERR_STATE, "movemark before p2_set_grid");
+    if (nmark < 0 || nmark > 0x7fffffffL) throw Error(P2_ERR_ARG, "marker count out of range");
+    if (!(dt >= 0) || !std::isfinite(dt)) throw Error(P2_ERR_ARG, "time step must be finite and >= 0");
+    if (outgrid < 0 || outgrid > 2) throw Error(P2_ERR_ARG, "outgrid must be 0, 1 or 2");
+    if (markmod != 1 && markmod != 2) throw Error(P2_ERR_ARG, "markmod must be 1 (simple) or 2 (Runge-Kutta 4)");
+    ensure_move_buffers(nmark);
+    const Level &L0 = L[0];
+    if (!mv_e[0])
+        for (int q = 0; q < 6; q++) mv_e[q] = (float *)grid_arena.alloc(sizeof(float) * L0.n);
+    if (!mv_val1) {
+        mv_val1 = (double *)move_arena.alloc(sizeof(double) * mv_cap);
+        mv_marke = (float *)move_arena.alloc(sizeof(float) * mv_cap);
+    }
+    const float *src[3] = {vx, vy, vz};
+    for (int q = 0; q < 3; q++)
+        P2_CUDA_TRY(cudaMemcpyAsync(mv_vel[q], src[q], sizeof(float) * L0.n, cudaMemcpyHostToDevice, st));
+    for (int q = 0; q < 6; q++)
+        P2_CUDA_TRY(cudaMemcpyAsync(mv_e[q], e[q], sizeof(float) * L0.n, cudaMemcpyHostToDevice, st));
+    if (nmark > 0) {
+        float *pos[3] = {mx, my, mz};
+        for (int q = 0; q < 3; q++)
+            P2_CUDA_TRY(cudaMemcpyAsync(mv_pos[q], pos[q], sizeof(float) * nmark, cudaMemcpyHostToDevice, st));
+        P2_CUDA_TRY(cudaMemcpyAsync(mv_type, mt, nmark, cudaMemcpyHostToDevice, st));
+        P2_CUDA_TRY(cudaMemcpyAsync(mv_val1, val1, sizeof(double) * nmark, cudaMemcpyHostToDevice, st));
+        P2_CUDA_TRY(cudaMemcpyAsync(mv_marke, marke, sizeof(float) * nmark, cudaMemcpyHostToDevice, st));
+        StrainF S;
+        for (int q = 0; q < 6; q++) S.e[q] = mv_e[q];
+        launch_movemark(st, nmark, grid3(), mv_vel, mv_pos, mv_type, dt, markmod, outgrid, &S, mv_val1, mv_marke);
+        for (int q = 0; q < 3; q++)
+            P2_CUDA_TRY(cudaMemcpyAsync(pos[q], mv_pos[q], sizeof(float) * nmark, cudaMemcpyDeviceToHost, st));
+        P2_CUDA_TRY(cudaMemcpyAsync(val1, mv_val1, sizeof(double) * nmark, cudaMemcpyDeviceToHost, st));
+        P2_CUDA_TRY(cudaMemcpyAsync(marke, mv_marke, sizeof(float) * nmark, cudaMemcpyDeviceToHost, st));
+    }
+    P2_CUDA_TRY(cudaStreamSynchronize(st));
 }
 
 // float copies of the resident solution velocities into mv_vel
@@ -599,17 +806,34 @@ void Solver::get_markers(float *mx, float *my, float *mz)
 
 // ---------------------------------------------------------------------------
 void Solver::upload_markers(long nmark, const float *mx, const float *my, const float *mz, const signed char *mt,
-                            int nrock, const double *n0, const double *n1, const double *rho)
+                            int nrock, const double *n0, const double *n1, const double *rho, const double *marknu,
+                            const double *markmm, const double *val1)
 {
     if (!grid_ready) throw Error(P2_ERR_STATE, "markers before p2_set_grid");
     if (nmark < 0 || nmark > 0x7fffffffL) throw Error(P2_ERR_ARG, "marker count out of range");
     if (nrock <= 0 || nrock > 256) throw Error(P2_ERR_ARG, "rock table size out of range");
-    // constant per-type viscosity (viscalc, mark3mg.c:1481-1482) and density (dencalc1, 1429)
-    std::vector<double> f(256, 1.0), r(256, 0.0);
+    const bool have_pl = marknu && markmm && (val1 || nmark == 0);
+    // per-type viscosity (viscalc, mark3mg.c:1479-1482: types above 20 and
+    // types with markn0 == markn1 are constant) and density (dencalc1, 1429);
+    // power-law types (markn0 != markn1, type <= 20) need marknu, markmm and
+    // every marker's strain-rate invariant val1
+    std::vector<double> f(256, 1.0), r(256, 0.0), pl(kPowerLawStride * 256, 0.0);
+    bool any_pl = false;
     for (int t = 0; t < nrock && t < 50; t++) {
-        if (n0[t] != n1[t])
-            throw Error(P2_ERR_UNSUPPORTED, "rock type " + std::to_string(t) +
-                                                " has a power-law viscosity (markn0 != markn1)");
+        if (n0[t] != n1[t] && t <= 20) {
+            if (!have_pl)
+                throw Error(P2_ERR_UNSUPPORTED, "rock type " + std::to_string(t) +
+                                                    " has a power-law viscosity (markn0 != markn1): use "
+                                                    "p2_ronurecalc_powerlaw");
+            if (!(markmm[t] != 0)) throw Error(P2_ERR_ARG, "markmm must be nonzero for power-law rock types");
+            double *e = &pl[kPowerLawStride * t];
+            e[0] = 1.0;
+            e[1] = marknu[t];
+            e[2] = (1 - markmm[t]) / markmm[t];
+            e[3] = n0[t];
+            e[4] = n1[t];
+            any_pl = true;
+        }
         double mnu = n0[t];
         if (mnu < prm.nubeg) mnu = prm.nubeg;
         if (mnu > prm.nuend) mnu = prm.nuend;
@@ -636,6 +860,14 @@ void Solver::upload_markers(long nmark, const float *mx, const float *my, const 
     rock_ro = (double *)marker_arena.alloc(sizeof(double) * 256);
     P2_CUDA_TRY(cudaMemcpy(rock_f, f.data(), sizeof(double) * 256, cudaMemcpyHostToDevice));
     P2_CUDA_TRY(cudaMemcpy(rock_ro, r.data(), sizeof(double) * 256, cudaMemcpyHostToDevice));
+    rock_pl = nullptr;
+    mk_val1 = nullptr;
+    if (any_pl) {
+        rock_pl = (double *)marker_arena.alloc(sizeof(double) * pl.size());
+        P2_CUDA_TRY(cudaMemcpy(rock_pl, pl.data(), sizeof(double) * pl.size(), cudaMemcpyHostToDevice));
+        mk_val1 = (double *)marker_arena.alloc(sizeof(double) * cap);
+        if (nmark) P2_CUDA_TRY(cudaMemcpyAsync(mk_val1, val1, sizeof(double) * nmark, cudaMemcpyHostToDevice, st));
+    }
     // sort and node buffers
     int ntiles = (int)((cap + kTile - 1) / kTile);
     mk_key[0] = (unsigned *)marker_arena.alloc(sizeof(unsigned) * cap);
@@ -698,7 +930,7 @@ void Solver::ronurecalc_device()
     k_node_gather<<<nb(L0.n, 128), 128, 0, st>>>(L0.nx, L0.ny, L0.nz, d_g[0], d_g[1], d_g[2], cell_start, cell_end,
                                             mk_val[mk_cur], mk_sorted, rock_f, rock_ro, prm.nukoef, prm.viscmod,
                                             prm.nubeg, prm.nuend, mk_nodes[0], mk_nodes[1], mk_nodes[2],
-                                            mk_nodes[3], mk_nodes[4], mk_nodes[5]); P2_COUNT_LAUNCH();
+                                            mk_nodes[3], mk_nodes[4], mk_nodes[5], rock_pl, mk_val1); P2_COUNT_LAUNCH();
     P2_CUDA_TRY(cudaGetLastError());
     // the result becomes the solver's resident node fields
     if (bc_ready) {

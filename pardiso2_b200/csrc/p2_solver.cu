@@ -238,6 +238,9 @@ void Solver::set_grid(long nx, long ny, long nz, const double *gx, const double 
     post_range = nullptr;
     mv_cap = 0;
     for (int q = 0; q < 3; q++) { d_g[q] = nullptr; mv_vel[q] = nullptr; mv_pos[q] = nullptr; }
+    for (int q = 0; q < 6; q++) mv_e[q] = nullptr;
+    mv_val1 = nullptr;
+    mv_marke = nullptr;
     for (int q = 0; q < 6; q++) mk_nodes[q] = nullptr;
     mv_type = nullptr;
     prm = p;

@@ -81,11 +81,15 @@ class Solver {
     void get_solution(double *vx, double *vy, double *vz, double *pr);
 
     void upload_markers(long nmark, const float *mx, const float *my, const float *mz, const signed char *mt,
-                        int nrock, const double *n0, const double *n1, const double *rho);
+                        int nrock, const double *n0, const double *n1, const double *rho,
+                        const double *marknu = nullptr, const double *markmm = nullptr, const double *val1 = nullptr);
     void ronurecalc_device();
     void movemark_host(double dt, int markmod, int outgrid, const float *vx, const float *vy, const float *vz, long nmark,
                        float *mx, float *my, float *mz, const signed char *mt);
     void movemark_device(double dt, int markmod, int outgrid);
+    void movemark_strain_host(double dt, int markmod, int outgrid, const float *vx, const float *vy, const float *vz,
+                              const float *const e[6], long nmark, float *mx, float *my, float *mz,
+                              const signed char *mt, double *val1, float *marke);
     void get_markers(float *mx, float *my, float *mz);
     void stress_strain(float *const s[6], float *const e[6], double vrange[6]);
 
@@ -117,6 +121,7 @@ class Solver {
     float4 *mk_sorted = nullptr;
     int *cell_start = nullptr, *cell_end = nullptr;
     double *rock_f = nullptr, *rock_ro = nullptr;
+    double *rock_pl = nullptr, *mk_val1 = nullptr;  // power-law table per type, val1 per marker
     double *d_g[3] = {nullptr, nullptr, nullptr};
     float *mk_nodes[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
     // marker advection: float velocities and host-path marker buffers
@@ -124,6 +129,9 @@ class Solver {
     float *mv_pos[3] = {nullptr, nullptr, nullptr};
     signed char *mv_type = nullptr;
     long mv_cap = 0;
+    float *mv_e[6] = {};             // strain-rate fields for the strain-rate outputs of movemark
+    double *mv_val1 = nullptr;       // per marker
+    float *mv_marke = nullptr;
     // post-solve stress / strain-rate fields and velocity ranges
     float *post_out[12] = {};
     float *post_partial = nullptr;

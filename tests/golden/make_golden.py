@@ -21,6 +21,16 @@ and, in move17.npz, marker advection by the reference's movemark()
                                     1, 60, 110) and the inputs of the step
   out_<variant>_{x,y,z,k}           positions and markk after one step, for
                                     variants (markmod, outgrid) in MOVE_VARIANTS
+  strain_<variant>_{x,y,z,val1,marke}  movemark with strain-rate fields set
+                                    by that pass (rk4_og0, simple_og0):
+                                    positions, val1 (filled with -1 before)
+                                    and marke (in: marke_in, 0 for two
+                                    thirds of the markers; all 0 for
+                                    simple_og0)
+and, in pl17.npz, ronurecalc with power-law rocks (viscalc,
+pardiso/mark3mg.c:1463-1498): markers, rock tables (n0, n1, ro, nu, mm),
+val1 per marker, the node fields, and marke after the call (the reference
+sets it to 1e-20 where it was 0 for the markers it interpolates).
   st_{sxx..syz, exx..eyz}           the post-solve stress / strain-rate pass
                                     of vpiterate (move3mgNew.c:2908-3038) on
                                     those velocities and sphere17's node
@@ -169,8 +179,59 @@ def make_move_case():
     r.set_nodes({k: src["node_" + k] for k in ("nu", "ro", "nxx", "nxy", "nxz", "nyz")})
     for k, a in r.stress_strain(init=-7.0).items():
         out["st_" + k] = a
+    # movemark's strain-rate outputs, with the pass's fields in the globals
+    r.fill_stress(-7.0)
+    r.update_stress()
+    q = np.arange(mx.size)
+    marke_in = np.where(q % 3 == 0, np.float32(0.05) + np.float32(1e-4) * (q % 17), np.float32(0)).astype(np.float32)
+    out["marke_in"] = marke_in
+    for name in ("rk4_og0", "simple_og0"):
+        mmod, og = MOVE_VARIANTS[name]
+        r.set_markers(mx, my, mz, mt)
+        # in the single-velocity branch the reference adds a Runge-Kutta average
+        # left over from an earlier marker to marke: that case is not recorded
+        r.set_marke(marke_in if mmod == 2 else np.zeros_like(marke_in))
+        r.fill_val1(-1.0)
+        r.movemark(dt, mmod, og)
+        x, y, z, _ = r.markers()
+        v1, me = r.val1_marke()
+        for k, a in zip(("x", "y", "z", "val1", "marke"), (x, y, z, v1, me)):
+            out["strain_%s_%s" % (name, k)] = a
     np.savez_compressed(os.path.join(HERE, "move17.npz"), **out)
     print("move17 written", {k: np.asarray(v).shape for k, v in out.items()})
+
+
+def power_law_model():
+    """sphere17 markers with a power-law sphere (type 1), a type-25 block
+    (markn0 != markn1 but above type 20: constant markn0) and a constant
+    background, plus seeded val1 per marker (log-uniform, some zeros)."""
+    m = M.sphere_model(17, 2, (2, 2, 2), seed=11, eta_sphere=1e2)
+    t = np.array(m.markt, np.int8)
+    t[(m.markx > 0.8) & (m.marky < 0.5)] = 25
+    m.markt = t
+    n0 = np.ones(26); n1 = np.ones(26); ro = np.zeros(26); nu = np.ones(26); mm = np.ones(26)
+    n0[1], n1[1], nu[1], mm[1], ro[1] = 1e-1, 1e3, 5.0, 3.0, 1.0
+    n0[25], n1[25], ro[25] = 2.0, 50.0, -0.5
+    m.rocks = M.Rocks(n0, n1, ro)
+    rng = np.random.Generator(np.random.PCG64(17))
+    val1 = 10.0 ** rng.uniform(-5, 1, m.markx.size)
+    val1[::97] = 0.0
+    return m, nu, mm, val1
+
+
+def make_pl_case():
+    from oracle import refdrv
+    m, nu, mm, val1 = power_law_model()
+    r = refdrv.RefModel(m)
+    r.set_rheology(nu, mm, val1)
+    r.ronurecalc()
+    nodes = r.nodes()
+    _, marke = r.val1_marke()
+    out = {"markx": m.markx, "marky": m.marky, "markz": m.markz, "markt": m.markt, "n0": m.rocks.n0,
+           "n1": m.rocks.n1, "ro": m.rocks.ro, "nu": nu, "mm": mm, "val1": val1, "marke_after": marke}
+    out.update({"node_" + k: v for k, v in nodes.items()})
+    np.savez_compressed(os.path.join(HERE, "pl17.npz"), **out)
+    print("pl17 written", {k: np.asarray(v).shape for k, v in out.items()})
 
 
 if __name__ == "__main__":
@@ -178,9 +239,11 @@ if __name__ == "__main__":
     if len(sys.argv) > 1:
         if sys.argv[1] == "move17":
             make_move_case()
+        elif sys.argv[1] == "pl17":
+            make_pl_case()
         else:
             make_case(sys.argv[1], CASES[sys.argv[1]])
     else:
         import subprocess
-        for c in list(CASES) + ["move17"]:
+        for c in list(CASES) + ["move17", "pl17"]:
             subprocess.run([sys.executable, os.path.abspath(__file__), c], check=True)

@@ -55,9 +55,43 @@ def test_vpiterate_ronurecalc_movemark_through_the_reference_globals(oracle_mod)
     dt = 1.5 / 20 / max(float(np.abs(v).max()) for v in vel)
     r.set_markers(mx, my, mz, mt)
     r.fill_markk(300.0)
+    r.fill_val1(-1.0)
     r.movemark(dt, 2, 0)
     got = r.markers()
+    # val1: the strain-rate invariant at every moved marker, from the fields
+    # vpiterate wrote (the device takes sqrt where the reference takes pow(., 0.5))
+    v1, _ = r.val1_marke()
+    strain = [st[k] for k in ("exx", "eyy", "ezz", "exy", "exz", "eyz")]
+    ref_v1 = oracle_mod.movemark(m, vel, dt, 2, 0, markers=(mx, my, mz, mt), strain=strain,
+                                 val1=np.full(mx.size, -1.0))[3]
+    assert np.array_equal(v1 < 0, ref_v1 < 0)
+    assert np.abs(v1.view(np.int64) - ref_v1.view(np.int64)).max() <= 1
     ref = oracle_mod.movemark(m, vel, dt, 2, 0, markers=(mx, my, mz, mt), markk=np.full(mx.size, 300.0, np.float32))
     for a, b, c in zip(got, ref, "xyzk"):
         assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), c
     assert int((got[3] == 0).sum()) > 0
+    # ronurecalc with a power-law rock: the shim's ronurecalc() ->
+    # p2_ronurecalc_powerlaw with marknu, markmm and the val1 movemark left;
+    # marke becomes 1e-20 where it was 0 for the markers it interpolates
+    n0 = np.array(m.rocks.n0, np.float64)
+    n1 = np.array(m.rocks.n1, np.float64)
+    n1[1] = n0[1] * 1e3
+    nu = np.array(n0) * 2.0
+    mm = np.ones(n0.size)
+    mm[1] = 3.0
+    r.lib.p2ref_set_rocks(n0.size, n0, n1, np.ascontiguousarray(m.rocks.ro, np.float64))
+    v1pl = np.where(v1 >= 0, v1, 1e-3)   # markers that did not move kept val1 = -1
+    r.set_rheology(nu, mm, v1pl)
+    r.set_markers(m.markx, m.marky, m.markz, m.markt)
+    r.set_marke(np.zeros(m.markx.size, np.float32))
+    r.ronurecalc()
+    f = r.nodes()
+    mpl = m
+    mpl.rocks = type(m.rocks)(n0, n1, m.rocks.ro)
+    ref = oracle_mod.ronurecalc(mpl, marknu=nu, markmm=mm, val1=v1pl, init={k: g["node_" + k] for k in FIELDS})
+    for k in FIELDS:
+        err = np.abs(f[k].astype(np.float64) - ref[k]) / np.maximum(np.abs(ref[k]), 1e-30)
+        assert err.max() <= 1e-6, (k, float(err.max()))
+    _, me = r.val1_marke()
+    inside = (m.markx > 0) & (m.marky > 0) & (m.markz > 0) & (m.markx < 1) & (m.marky < 1) & (m.markz < 1) & (m.markt < 50)
+    assert np.all(me[inside] == np.float32(1e-20)) and np.all(me[~inside] == 0)

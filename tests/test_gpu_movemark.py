@@ -107,3 +107,30 @@ def test_stress_strain_after_solve_vs_oracle(oracle_mod):
     ok = [(jj < ny - 1) & (kk < nz - 1), (ii < nx - 1) & (kk < nz - 1), (ii < nx - 1) & (jj < ny - 1)]
     for c in range(3):
         assert vr[2 * c] == float(vel[c][ok[c]].min()) and vr[2 * c + 1] == float(vel[c][ok[c]].max()), c
+
+
+def _ulps(a, b):
+    """Distance in units in the last place between equal-signed floats."""
+    it = np.int64 if a.dtype == np.float64 else np.int32
+    return np.abs(a.view(it).astype(np.int64) - b.view(it).astype(np.int64))
+
+
+@pytest.mark.parametrize("variant", ["rk4_og0", "simple_og0"])
+def test_movemark_strain_outputs_vs_reference_golden(move17, variant):
+    """p2_movemark_strain: positions bit-exact; val1 and marke within one unit
+    in the last place of the reference's (it takes pow(x, 0.5) where the
+    device takes a correctly rounded square root)."""
+    g, prob = move17
+    markmod, outgrid = MOVE_VARIANTS[variant]
+    strain = [g["st_" + k] for k in ("exx", "eyy", "ezz", "exy", "exz", "eyz")]
+    me_in = g["marke_in"] if markmod == 2 else np.zeros_like(g["marke_in"])
+    x, y, z, v1, me = prob.ctx.movemark_strain(float(g["dt"]), (g["vx"], g["vy"], g["vz"]), strain,
+                                               (g["in_x"], g["in_y"], g["in_z"], g["in_t"]),
+                                               np.full(me_in.size, -1.0), me_in, markmod=markmod, outgrid=outgrid)
+    for a, c in zip((x, y, z), "xyz"):
+        assert np.array_equal(a.view(np.uint32), g["strain_%s_%s" % (variant, c)].view(np.uint32)), c
+    rv, re_ = g["strain_%s_val1" % variant], g["strain_%s_marke" % variant]
+    assert np.array_equal(v1 < 0, rv < 0)
+    assert _ulps(v1, rv).max() <= 1 and _ulps(me, re_).max() <= 1
+    if markmod == 2:
+        assert int((me != me_in).sum()) > 1000

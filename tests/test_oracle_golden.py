@@ -177,3 +177,37 @@ def test_oracle_stress_strain_vs_reference_golden(oracle_mod):
     for k, a in out.items():
         assert np.array_equal(a.view(np.uint32), g["st_" + k].view(np.uint32)), k
         assert (a != -7.0).sum() > 0.7 * a.size * (0.75 if k[1] != k[2] else 1.0), k
+
+
+@pytest.mark.parametrize("variant", ["rk4_og0", "simple_og0"])
+def test_oracle_movemark_strain_outputs_vs_reference_golden(oracle_mod, variant):
+    """movemark's strain-rate outputs (epscalc1 at the markers, val1; the
+    Runge-Kutta brittle strain marke): bit-exact with the reference's run."""
+    from tests.golden.make_golden import MOVE_VARIANTS
+    g = np.load(os.path.join(GOLDEN, "move17.npz"))
+    m = M.sphere_model(17, 2, (1, 1, 1), seed=3, eta_sphere=1e3)
+    markmod, outgrid = MOVE_VARIANTS[variant]
+    strain = [g["st_" + k] for k in ("exx", "eyy", "ezz", "exy", "exz", "eyz")]
+    me_in = g["marke_in"] if markmod == 2 else np.zeros_like(g["marke_in"])
+    out = oracle_mod.movemark(m, (g["vx"], g["vy"], g["vz"]), float(g["dt"]), markmod, outgrid,
+                              markers=(g["in_x"], g["in_y"], g["in_z"], g["in_t"]), strain=strain,
+                              val1=np.full(me_in.size, -1.0), marke=me_in)
+    for a, k in zip(out, ("x", "y", "z", "val1", "marke")):
+        ref = g["strain_%s_%s" % (variant, k)]
+        assert np.array_equal(a, ref) and np.array_equal(np.signbit(a), np.signbit(ref)), k
+    if markmod == 2:
+        assert int((out[4] != me_in).sum()) > 1000
+
+
+def test_oracle_ronurecalc_power_law_vs_reference_golden(oracle_mod):
+    """ronurecalc with power-law rocks (viscalc, mark3mg.c:1463-1498): node
+    fields bit-exact with the reference's own run (pl17.npz); types above 20
+    stay constant even with markn0 != markn1."""
+    from tests.golden.make_golden import power_law_model
+    g = np.load(os.path.join(GOLDEN, "pl17.npz"))
+    m, nu, mm, val1 = power_law_model()
+    assert np.array_equal(val1, g["val1"]) and np.array_equal(m.markt, g["markt"])
+    f = oracle_mod.ronurecalc(m, marknu=nu, markmm=mm, val1=val1)
+    for k in f:
+        assert np.array_equal(f[k], g["node_" + k]), k
+    assert np.abs(oracle_mod.ronurecalc(m)["nu"] - f["nu"]).max() > 1.0
