@@ -47,6 +47,22 @@ struct LuGraph {
 };
 #define P2_COUNT_LAUNCH() (++p2::g_launches)
 
+// Programmatic dependent launch (the V-cycle's kernels are launched with
+// programmatic stream serialization, so the next grid is scheduled while the
+// previous one drains): a kernel first waits until its predecessor grid has
+// completed and its writes are visible (griddepcontrol.wait; a no-op when the
+// launch has no programmatic dependency), then, if it fits in one wave, lets
+// its own successor be scheduled.  Larger grids leave that to their exit, so
+// waiting blocks of the next grid never take SM slots from their later waves.
+constexpr unsigned kPdlOneWave = 296;  // two blocks per SM
+__device__ __forceinline__ void pdl_enter()
+{
+#ifndef P2_NO_PDL
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    if (gridDim.x * gridDim.y * gridDim.z <= kPdlOneWave) asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+#endif
+}
+
 struct Error {
     p2_status code;
     std::string msg;

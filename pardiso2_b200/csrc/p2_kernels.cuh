@@ -15,6 +15,7 @@ constexpr int kThreads = 256;
 template <typename T, typename S>
 __global__ void k_rows(LevelView<T> L, Fields<T, S> x, Vec4<T> b, Vec4<T> out, Vec4<float> out32, int mode)
 {
+    pdl_enter();
     int u = blockIdx.x * blockDim.x + threadIdx.x;
     if (u >= L.n) return;
     int j = u % L.ny, i = (u / L.ny) % L.nx, k = u / (L.nx * L.ny);
@@ -41,6 +42,7 @@ template <typename T, typename S>
 __global__ void k_bc_rows(int nbc, const int *bu, const int *bt, const float *bk, Fields<T, S> x, Vec4<T> b,
                           Vec4<T> out, Vec4<float> out32, int mode)
 {
+    pdl_enter();
     int q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= nbc) return;
     int uc = bu[q], c = uc & 3, u = uc >> 2, t = bt[q];
@@ -62,6 +64,7 @@ template <typename T>
 __global__ void k_bc_set_chain(int nbc, const int *bu, const int *bt, const float *bk, const int *bnext, Vec4<T> x,
                                Vec4<T> b)
 {
+    pdl_enter();
     int q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= nbc) return;
     int chain[kMaxBcChain];
@@ -96,6 +99,7 @@ __global__ void k_bc_set_chain(int nbc, const int *bu, const int *bt, const floa
 template <typename T>
 __global__ void k_vanka(LevelView<T> L, T *P, Vec4<T> vin, Vec4<T> vout, Vec4<T> b, T omega, int col)
 {
+    pdl_enter();
     int half = (L.ny) / 2;  // >= number of cells of one colour on a y-line
     long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
     long lines = (long)(L.nx - 1) * (L.nz - 1);
@@ -209,6 +213,7 @@ template <typename T>
 __global__ void __launch_bounds__(128) k_vanka_full(LevelView<T> L, T *P, Vec4<T> vin, Vec4<T> vout, Vec4<T> b,
                                                     T omega, int col)
 {
+    pdl_enter();
     int half = (L.ny) / 2;
     long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
     long lines = (long)(L.nx - 1) * (L.nz - 1);
@@ -434,6 +439,7 @@ template <typename T>
 __global__ void __launch_bounds__(128) k_vanka_fast(LevelView<T> L, T *P, Vec4<T> vin, Vec4<T> vout, Vec4<T> b,
                                                     T omega, int col)
 {
+    pdl_enter();
     int i, j, k;
     if (!colour_cell(L, col, (long)blockIdx.x * blockDim.x + threadIdx.x, i, j, k)) return;
     Fields<T, T> x{P, vin.c[1], vin.c[2], vin.c[3]};
@@ -635,6 +641,7 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? P2_STORED_MIN_BLOCKS : 3
     LevelView<T> L, T *P, Vec4<T> vin, Vec4<T> vout, Vec4<T> b, T omega, int col, const T *__restrict__ blk,
     long stride)
 {
+    pdl_enter();
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
     int i, j, k;
     if (!colour_cell(L, col, t, i, j, k)) return;
@@ -717,6 +724,7 @@ __global__ void k_restrict_compat(LevelView<T> F, Vec4<T> rf, LevelView<T> Cl, V
                                   TransferView tv, int scale_p, double vol_total, double *partial,
                                   unsigned *ticket, double *sums)
 {
+    pdl_enter();
     __shared__ double sh[32];
     __shared__ bool last;
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -785,6 +793,7 @@ __global__ void k_restrict_compat(LevelView<T> F, Vec4<T> rf, LevelView<T> Cl, V
 template <typename T>
 __global__ void k_prolong(LevelView<T> F, Vec4<T> xf, LevelView<T> Cl, Vec4<T> xc, TransferView tv, T p1, T v1)
 {
+    pdl_enter();
     int u = blockIdx.x * blockDim.x + threadIdx.x;
     if (u >= F.n) return;
     int j = u % F.ny, i = (u / F.ny) % F.nx, k = u / (F.nx * F.ny);
@@ -995,6 +1004,7 @@ __global__ void k_dots_final(int nd, int nparts, const double *partial, double *
 template <typename T>
 __global__ void k_compat_apply(LevelView<T> L, T *bp, const double *sums)
 {
+    pdl_enter();
     int u = blockIdx.x * blockDim.x + threadIdx.x;
     if (u >= L.n || sums[1] <= 0) return;
     int j = u % L.ny, i = (u / L.ny) % L.nx, k = u / (L.nx * L.ny);

@@ -32,6 +32,29 @@ void d2f(cudaStream_t st, size_t n, const double *a, float *b);
 
 static inline unsigned nblk(long n, int t = kThreads) { return (unsigned)((n + t - 1) / t); }
 
+// Launch with programmatic stream serialization (see pdl_enter): kernels
+// launched this way start with pdl_enter().
+template <typename... KArgs, typename... Args>
+static void pdl_launch(cudaStream_t st, dim3 grid, dim3 block, void (*kern)(KArgs...), Args &&...args)
+{
+#ifdef P2_NO_PDL
+    kern<<<grid, block, 0, st>>>(std::forward<Args>(args)...);
+#else
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    P2_CUDA_TRY(cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...));
+#endif
+    P2_COUNT_LAUNCH();
+}
+
 void *DeviceArena::alloc(size_t bytes)
 {
     void *p = nullptr;
@@ -656,6 +679,7 @@ __global__ void k_probe_rows(LevelView<double> Lc, const double *probes, const i
 template <typename T>
 __global__ void k_coarse_gather(int nF, const int *fre, Vec4<T> b, T *bF)
 {
+    pdl_enter();
     int q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= nF) return;
     int uc = fre[q];
@@ -664,6 +688,7 @@ __global__ void k_coarse_gather(int nF, const int *fre, Vec4<T> b, T *bF)
 template <typename T>
 __global__ void k_coarse_scatter(int nF, const int *fre, const T *xF, Vec4<T> x)
 {
+    pdl_enter();
     int q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= nF) return;
     int uc = fre[q];
@@ -673,6 +698,7 @@ __global__ void k_coarse_scatter(int nF, const int *fre, const T *xF, Vec4<T> x)
 template <typename T>
 __global__ void k_gemv(int n, const T *A, const T *b, T *y)
 {
+    pdl_enter();
     // block: 256 threads = 8 warps; rows r0..r0+31 per block, warps split the columns
     __shared__ T part[8][33];
     int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -724,10 +750,10 @@ void Solver::coarse_solve(Vec4<T> &b, Vec4<T> &x)
     T *bF = std::is_same<T, double>::value ? (T *)cb64 : (T *)cb32;
     T *xF = std::is_same<T, double>::value ? (T *)cx64 : (T *)cx32;
     const T *Ai = std::is_same<T, double>::value ? (const T *)Ainv64 : (const T *)Ainv32;
-    k_coarse_gather<T><<<nblk(nF), kThreads, 0, st>>>(nF, d_free, b, bF); P2_COUNT_LAUNCH();
-    k_gemv<T><<<(nF + 31) / 32, 256, 0, st>>>(nF, Ai, bF, xF); P2_COUNT_LAUNCH();
     for (int c = 0; c < 4; c++) P2_CUDA_TRY(cudaMemsetAsync(x.c[c], 0, sizeof(T) * C.n, st));
-    k_coarse_scatter<T><<<nblk(nF), kThreads, 0, st>>>(nF, d_free, xF, x); P2_COUNT_LAUNCH();
+    pdl_launch(st, nblk(nF), kThreads, k_coarse_gather<T>, nF, (const int *)d_free, b, bF);
+    pdl_launch(st, (nF + 31) / 32, 256, k_gemv<T>, nF, Ai, (const T *)bF, xF);
+    pdl_launch(st, nblk(nF), kThreads, k_coarse_scatter<T>, nF, (const int *)d_free, (const T *)xF, x);
     bc_set<T>((int)L.size() - 1, x, b);
 }
 
@@ -737,7 +763,8 @@ void Solver::bc_set(int l, Vec4<T> &x, Vec4<T> &b)
 {
     Level &Lv = L[l];
     if (Lv.nbc > 0) {
-        k_bc_set_chain<T><<<nblk(Lv.nbc), kThreads, 0, st>>>(Lv.nbc, Lv.bu, Lv.bt, Lv.bk, Lv.bnext, x, b); P2_COUNT_LAUNCH();
+        pdl_launch(st, nblk(Lv.nbc), kThreads, k_bc_set_chain<T>, Lv.nbc, (const int *)Lv.bu, (const int *)Lv.bt,
+                   (const float *)Lv.bk, (const int *)Lv.bnext, x, b);
     }
 }
 
@@ -770,14 +797,13 @@ void Solver::smoother_pass(int l, const LevelView<T> &V, T *P, Vec4<T> &vin, Vec
     switch (prm.smoother) {
     case 1: {
         const T *blk = (const T *)Lv.blk + (size_t)col * kBlkEntries * Lv.blk_stride;
-        k_vanka_stored<T><<<nblk(cells, 128), 128, 0, st>>>(V, P, vin, vout, b, om, col, blk, Lv.blk_stride);
+        pdl_launch(st, nblk(cells, 128), 128, k_vanka_stored<T>, V, P, vin, vout, b, om, col, blk, Lv.blk_stride);
         break;
     }
-    case 2: k_vanka_full<T><<<nblk(cells, 128), 128, 0, st>>>(V, P, vin, vout, b, om, col); break;
-    case 3: k_vanka_fast<T><<<nblk(cells, 128), 128, 0, st>>>(V, P, vin, vout, b, om, col); break;
-    default: k_vanka<T><<<nblk(cells), kThreads, 0, st>>>(V, P, vin, vout, b, om, col); break;
+    case 2: pdl_launch(st, nblk(cells, 128), 128, k_vanka_full<T>, V, P, vin, vout, b, om, col); break;
+    case 3: pdl_launch(st, nblk(cells, 128), 128, k_vanka_fast<T>, V, P, vin, vout, b, om, col); break;
+    default: pdl_launch(st, nblk(cells), kThreads, k_vanka<T>, V, P, vin, vout, b, om, col); break;
     }
-    P2_COUNT_LAUNCH();
 }
 
 // Cell factors of the stored-factor smoother on every level, both colours
@@ -834,8 +860,10 @@ void Solver::level_residual(int l)
     Vec4<T> &x = vx_of<T>(Lv, 0), &b = b_of<T>(Lv), &r = r_of<T>(Lv);
     Fields<T, T> f{x.c[0], x.c[1], x.c[2], x.c[3]};
     Vec4<float> none;
-    k_rows<T, T><<<nblk(Lv.n), kThreads, 0, st>>>(V, f, b, r, none, 0); P2_COUNT_LAUNCH();
-    if (Lv.nbc) k_bc_rows<T, T><<<nblk(Lv.nbc), kThreads, 0, st>>>(Lv.nbc, Lv.bu, Lv.bt, Lv.bk, f, b, r, none, 0); P2_COUNT_LAUNCH();
+    pdl_launch(st, nblk(Lv.n), kThreads, k_rows<T, T>, V, f, b, r, none, 0);
+    if (Lv.nbc)
+        pdl_launch(st, nblk(Lv.nbc), kThreads, k_bc_rows<T, T>, Lv.nbc, (const int *)Lv.bu, (const int *)Lv.bt,
+                   (const float *)Lv.bk, f, b, r, none, 0);
 }
 
 template <typename T>
@@ -847,17 +875,17 @@ void Solver::vcycle()
         level_residual<T>(l);
         Level &F = L[l], &Cl = L[l + 1];
         LevelView<T> VF = view<T>(l, false), VC = view<T>(l + 1, false);
-        k_restrict_compat<T><<<nblk(4L * Cl.n), kThreads, 0, st>>>(VF, r_of<T>(F), VC, b_of<T>(Cl), vx_of<T>(Cl, 0),
-                                                                   F.tv, 1, Cl.compat_vol, rpartial, rticket, scal); P2_COUNT_LAUNCH();
-        k_compat_apply<T><<<nblk(Cl.n), kThreads, 0, st>>>(VC, b_of<T>(Cl).c[0], scal); P2_COUNT_LAUNCH();
+        pdl_launch(st, nblk(4L * Cl.n), kThreads, k_restrict_compat<T>, VF, r_of<T>(F), VC, b_of<T>(Cl),
+                   vx_of<T>(Cl, 0), F.tv, 1, Cl.compat_vol, rpartial, rticket, scal);
+        pdl_launch(st, nblk(Cl.n), kThreads, k_compat_apply<T>, VC, b_of<T>(Cl).c[0], (const double *)scal);
     }
     if (nl > 1) coarse_solve<T>(b_of<T>(L[nl - 1]), vx_of<T>(L[nl - 1], 0));
     else coarse_solve<T>(b_of<T>(L[0]), vx_of<T>(L[0], 0));
     for (int l = nl - 2; l >= 0; l--) {
         Level &F = L[l], &Cl = L[l + 1];
         LevelView<T> VF = view<T>(l, false), VC = view<T>(l + 1, false);
-        k_prolong<T><<<nblk(F.n), kThreads, 0, st>>>(VF, vx_of<T>(F, 0), VC, vx_of<T>(Cl, 0), F.tv, (T)prm.p1koef,
-                                                     (T)prm.v1koef); P2_COUNT_LAUNCH();
+        pdl_launch(st, nblk(F.n), kThreads, k_prolong<T>, VF, vx_of<T>(F, 0), VC, vx_of<T>(Cl, 0), F.tv,
+                   (T)prm.p1koef, (T)prm.v1koef);
         smooth<T>(l, prm.npost[l]);
     }
 }
@@ -949,6 +977,24 @@ void Solver::precondition(Vec4<double> &z)
     }
 }
 
+// Capture (once per configuration) and upload the V-cycle graph.
+template <typename T>
+void Solver::capture_vcycle_graph()
+{
+    GraphSlot &g = graphs[std::is_same<T, double>::value ? 1 : 0];
+    if (g.exec || !prm.use_graphs) return;
+    cudaGraph_t graph;
+    long long before = g_launches;
+    P2_CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    vcycle<T>();
+    P2_CUDA_TRY(cudaStreamEndCapture(st, &graph));
+    g.kernels = g_launches - before;  // captured, not yet executed
+    g_launches = before;
+    P2_CUDA_TRY(cudaGraphInstantiate(&g.exec, graph, 0));
+    cudaGraphDestroy(graph);
+    P2_CUDA_TRY(cudaGraphUpload(g.exec, st));
+}
+
 template <typename T>
 void Solver::run_vcycle_graph()
 {
@@ -959,17 +1005,7 @@ void Solver::run_vcycle_graph()
         P2_CUDA_TRY(cudaGetLastError());
         return;
     }
-    if (!g.exec) {
-        cudaGraph_t graph;
-        long long before = g_launches;
-        P2_CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-        vcycle<T>();
-        P2_CUDA_TRY(cudaStreamEndCapture(st, &graph));
-        g.kernels = g_launches - before;  // captured, not yet executed
-        g_launches = before;
-        P2_CUDA_TRY(cudaGraphInstantiate(&g.exec, graph, 0));
-        cudaGraphDestroy(graph);
-    }
+    capture_vcycle_graph<T>();
     P2_CUDA_TRY(cudaGraphLaunch(g.exec, st));
     g_launches += g.kernels;
 }
@@ -1087,6 +1123,7 @@ p2_tune_info Solver::autotune(int trial_iters)
     p2_tune_info best{};
     best.est_ms = INFINITY;
     best.trial_iters = trial_iters;
+    double setup_ms = INFINITY;
     const int smoothers[2] = {1, 0}, growths[2] = {1, 2};
     for (int a = 0; a < 2; a++)
         for (int g = 0; g < 2; g++) {
@@ -1101,15 +1138,22 @@ p2_tune_info Solver::autotune(int trial_iters)
             }
             drop_graphs();
             set_initial(nullptr, nullptr, nullptr, nullptr);
+            // the candidate's V-cycle graph is captured before its trial, so the
+            // timed iterations hold no capture; the set-up (coarse viscosities,
+            // factors, coarsest LU) is the same for every candidate and is left
+            // out of the comparison (the first trial also captures the LU graph)
+            if (prm.precision == 0) capture_vcycle_graph<float>();
+            else capture_vcycle_graph<double>();
             p2_solve_info in = solve();
             double est = INFINITY, rate = 1.0;
             if (in.iterations > 0 && in.rel_residual > 0 && in.rel_residual0 > 0) {
                 rate = std::pow(in.rel_residual / in.rel_residual0, 1.0 / in.iterations);
                 double per_it = (in.ms_total - in.ms_setup) / in.iterations;
-                if (in.status == P2_OK) est = in.ms_total;
+                if (in.status == P2_OK) est = in.ms_total - in.ms_setup;
                 else if (rate < 1.0 && std::isfinite(rate))
-                    est = in.ms_setup + per_it * (in.iterations + std::log(saved.tol / in.rel_residual) / std::log(rate));
+                    est = per_it * (in.iterations + std::log(saved.tol / in.rel_residual) / std::log(rate));
             }
+            setup_ms = std::min(setup_ms, (double)in.ms_setup);
             if (verbose)
                 std::fprintf(stderr, "p2cuda: autotune smoother %d growth %d: %d its, rate %.3f, est %.1f ms\n",
                              prm.smoother, growths[g], in.iterations, rate, est);
@@ -1122,6 +1166,7 @@ p2_tune_info Solver::autotune(int trial_iters)
             }
         }
     prm = saved;
+    if (std::isfinite(best.est_ms) && std::isfinite(setup_ms)) best.est_ms += setup_ms;
     if (!std::isfinite(best.est_ms)) {
         // nothing converged within the trials: keep the defaults
         best.smoother = saved.smoother;

@@ -161,6 +161,8 @@ class Solver {
     void vcycle();
     template <typename T>
     void run_vcycle_graph();
+    template <typename T>
+    void capture_vcycle_graph();
     void set_nodes_device();
     void dots_sync(const DotJobs &jobs);
     void rows0(const Vec4<double> &x, Vec4<double> &out, Vec4<float> *r32, int mode);
