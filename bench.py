@@ -521,7 +521,10 @@ def main():
                      "bytes_per_launch": bytes_per_launch, "ms_per_launch": pass_ms,
                      "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs, burst)"},
         "clocks": clocks,
-        "e2e": {"value": e2e_ms, "unit": "ms", "h2d_bytes_per_step": 24 * n + 32 * n, "d2h_bytes_per_step": 32 * n},
+        "e2e": {"value": e2e_ms, "unit": "ms",
+                # node fields (6 float) and the initial guess (3 float + double pressure) up,
+                # the solution (3 float + double pressure) down
+                "h2d_bytes_per_step": 24 * n + 20 * n, "d2h_bytes_per_step": 20 * n},
     }
     line["movemark"] = {"ms": move_ms, "markers": nmark, "markmod": "RK4", "dt": dt_move,
                         "achieved_GBps": move_bytes / (move_ms * 1e-3) / 1e9, "bytes_per_step": move_bytes,

@@ -150,14 +150,7 @@ p2_status p2_stokes_solve(p2_ctx *ctx, float *vx, float *vy, float *vz, double *
         if (!S.bc_ready) throw p2::Error(P2_ERR_STATE, "solve before p2_set_bc");
         S.set_initial(vx, vy, vz, pr);
         r = S.solve();
-        long n = S.L[0].n;
-        std::vector<double> hv[3];
-        for (int q = 0; q < 3; q++) hv[q].resize(n);
-        S.get_solution(vx ? hv[0].data() : nullptr, vy ? hv[1].data() : nullptr, vz ? hv[2].data() : nullptr, pr);
-        float *dst[3] = {vx, vy, vz};
-        for (int q = 0; q < 3; q++)
-            if (dst[q])
-                for (long u = 0; u < n; u++) dst[q][u] = (float)hv[q][u];
+        S.get_solution_f32(vx, vy, vz, pr);
     });
     finish_info(info, r);
     if (st != P2_OK) return st;

@@ -1185,35 +1185,77 @@ p2_tune_info Solver::autotune(int trial_iters)
     return best;
 }
 
+// float -> double of one field (the initial guess of the host-array call)
+__global__ void k_field_f32_to_f64(long n, const float *a, double *b)
+{
+    const long u = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (u < n) b[u] = (double)a[u];
+}
+
+// the solution with the entries that are not unknowns (ghost positions) zero
+__global__ void k_solution_masked(int nx, int ny, int nz, Vec4<double> x, Vec4<double> out)
+{
+    const long u = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (u >= (long)nx * ny * nz) return;
+    const int j = (int)(u % ny), i = (int)((u / ny) % nx), k = (int)(u / ((long)nx * ny));
+#pragma unroll
+    for (int c = 0; c < 4; c++)
+        if (out.c[c]) out.c[c][u] = valid_pos(c, i, j, k, nx, ny, nz) ? x.c[c][u] : 0.0;
+}
+
+// Initial guess: float velocities and double pressure from the caller's
+// arrays (copied as they are, converted on the device), or zero.
 void Solver::set_initial(const float *vx, const float *vy, const float *vz, const double *pr)
 {
     long n = L[0].n;
     for (int c = 0; c < 4; c++) P2_CUDA_TRY(cudaMemsetAsync(gx.c[c], 0, sizeof(double) * n, st));
     if (!vx && !vy && !vz && !pr) return;
-    std::vector<double> h(n);
+    ensure_move_buffers(0);
     const float *fs[3] = {vx, vy, vz};
     for (int c = 1; c < 4; c++) {
         if (!fs[c - 1]) continue;
-        for (long u = 0; u < n; u++) h[u] = fs[c - 1][u];
-        P2_CUDA_TRY(cudaMemcpy(gx.c[c], h.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
+        P2_CUDA_TRY(cudaMemcpyAsync(mv_vel[c - 1], fs[c - 1], sizeof(float) * n, cudaMemcpyHostToDevice, st));
+        k_field_f32_to_f64<<<nblk(n), kThreads, 0, st>>>(n, mv_vel[c - 1], gx.c[c]); P2_COUNT_LAUNCH();
     }
-    if (pr) P2_CUDA_TRY(cudaMemcpy(gx.c[0], pr, sizeof(double) * n, cudaMemcpyHostToDevice));
+    if (pr) P2_CUDA_TRY(cudaMemcpyAsync(gx.c[0], pr, sizeof(double) * n, cudaMemcpyHostToDevice, st));
+    P2_CUDA_TRY(cudaStreamSynchronize(st));  // the caller's arrays may be reused after return
 }
 
+// FP64 solution into the caller's arrays (nullptr skips), ghost positions 0.
 void Solver::get_solution(double *vx, double *vy, double *vz, double *pr)
 {
-    long n = L[0].n;
-    double *dst[4] = {pr, vx, vy, vz};
-    for (int c = 0; c < 4; c++)
-        if (dst[c]) P2_CUDA_TRY(cudaMemcpyAsync(dst[c], gx.c[c], sizeof(double) * n, cudaMemcpyDeviceToHost, st));
-    P2_CUDA_TRY(cudaStreamSynchronize(st));
-    // zero the entries that are not unknowns (ghost positions)
     const Level &L0 = L[0];
-    for (long u = 0; u < n; u++) {
-        int j = (int)(u % L0.ny), i = (int)((u / L0.ny) % L0.nx), k = (int)(u / ((long)L0.nx * L0.ny));
-        for (int c = 0; c < 4; c++)
-            if (dst[c] && !valid_pos(c, i, j, k, L0.nx, L0.ny, L0.nz)) dst[c][u] = 0.0;
+    long n = L0.n;
+    double *dst[4] = {pr, vx, vy, vz};
+    Vec4<double> out = gr;  // the residual work vector is free after a solve
+    for (int c = 0; c < 4; c++)
+        if (!dst[c]) out.c[c] = nullptr;
+    k_solution_masked<<<nblk(n), kThreads, 0, st>>>(L0.nx, L0.ny, L0.nz, gx, out); P2_COUNT_LAUNCH();
+    for (int c = 0; c < 4; c++)
+        if (dst[c]) P2_CUDA_TRY(cudaMemcpyAsync(dst[c], out.c[c], sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+    P2_CUDA_TRY(cudaStreamSynchronize(st));
+}
+
+// The host-array form of the solution (vpiterate's write-back): float
+// velocities (the FP64 solution rounded, ghost positions 0) and the double
+// pressure, converted on the device and copied straight into the caller's
+// arrays (nullptr skips).
+void Solver::get_solution_f32(float *vx, float *vy, float *vz, double *pr)
+{
+    const Level &L0 = L[0];
+    long n = L0.n;
+    ensure_move_buffers(0);
+    velocity_f32();
+    if (pr) {
+        Vec4<double> out{};
+        out.c[0] = gr.c[0];
+        k_solution_masked<<<nblk(n), kThreads, 0, st>>>(L0.nx, L0.ny, L0.nz, gx, out); P2_COUNT_LAUNCH();
+        P2_CUDA_TRY(cudaMemcpyAsync(pr, gr.c[0], sizeof(double) * n, cudaMemcpyDeviceToHost, st));
     }
+    float *dst[3] = {vx, vy, vz};
+    for (int c = 0; c < 3; c++)
+        if (dst[c]) P2_CUDA_TRY(cudaMemcpyAsync(dst[c], mv_vel[c], sizeof(float) * n, cudaMemcpyDeviceToHost, st));
+    P2_CUDA_TRY(cudaStreamSynchronize(st));
 }
 
 

@@ -79,6 +79,7 @@ class Solver {
     void set_initial(const float *vx, const float *vy, const float *vz, const double *pr);
     p2_solve_info solve();
     void get_solution(double *vx, double *vy, double *vz, double *pr);
+    void get_solution_f32(float *vx, float *vy, float *vz, double *pr);
 
     void upload_markers(long nmark, const float *mx, const float *my, const float *mz, const signed char *mt,
                         int nrock, const double *n0, const double *n1, const double *rho,
