@@ -527,6 +527,9 @@ struct LuTimer {
 // ku) in place and write its inverse into Ainv.  Returns 0 or the first
 // zero-pivot column + 1.  marks (optional, 2 events) are recorded after the
 // factorisation and after the forward half of the inverse.
+// panels per group in the backward half of the inverse
+constexpr int kInvGroup = 4;
+
 static void lu_issue(cudaStream_t st, double *A, int n, int kl, int ku, double *Ainv, int *d_ipiv, int *d_info,
                      cudaEvent_t *marks, LuTimer &T)
 {
@@ -579,17 +582,29 @@ static void lu_issue(cudaStream_t st, double *A, int n, int kl, int ku, double *
         T.end(2);
     }
     if (marks) P2_CUDA_TRY(cudaEventRecord(marks[1], st));
-    // backward: U X = Y with U's band (kl + ku above the diagonal)
+    // backward: U X = Y with U's band (kl + ku above the diagonal), in groups
+    // of kInvGroup panels: inside a group every panel's rows are solved and
+    // propagated to the group's rows above it; then the rows above the group
+    // that U couples to it (within kl + ku) get one update with K = the
+    // group's height, instead of one K = kPB update per panel
     const int kuu = std::min(n - 1, kl + ku);
-    const int last = ((n - 1) / kPB) * kPB;
-    for (int k0 = last; k0 >= 0; k0 -= kPB) {
-        const int nb = std::min(kPB, n - k0);
+    const int G = kInvGroup * kPB;
+    for (int g0 = ((n - 1) / G) * G; g0 >= 0; g0 -= G) {
+        const int g1 = std::min(n, g0 + G);
+        for (int k0 = g0 + ((g1 - 1 - g0) / kPB) * kPB; k0 >= g0; k0 -= kPB) {
+            const int nb = std::min(kPB, n - k0);
+            T.begin();
+            k_trsm_upper_w<<<(n + kTrsmWarps - 1) / kTrsmWarps, 32 * kTrsmWarps, 0, st>>>(A, n, k0, nb, Ainv, n, 0,
+                                                                                       n); P2_COUNT_LAUNCH();
+            T.end(3);
+            const int a = std::max(g0, k0 - kuu);
+            T.begin();
+            if (k0 > a) dgemm_sub(st, k0 - a, n, nb, A + (size_t)k0 * n + a, n, Ainv + k0, n, Ainv + a, n);
+            T.end(2);
+        }
+        const int a = std::max(0, g0 - kuu);
         T.begin();
-        k_trsm_upper_w<<<(n + kTrsmWarps - 1) / kTrsmWarps, 32 * kTrsmWarps, 0, st>>>(A, n, k0, nb, Ainv, n, 0, n); P2_COUNT_LAUNCH();
-        T.end(3);
-        const int a = std::max(0, k0 - kuu);
-        T.begin();
-        if (k0 > a) dgemm_sub(st, k0 - a, n, nb, A + (size_t)k0 * n + a, n, Ainv + k0, n, Ainv + a, n);
+        if (g0 > a) dgemm_sub(st, g0 - a, n, g1 - g0, A + (size_t)g0 * n + a, n, Ainv + g0, n, Ainv + a, n);
         T.end(2);
     }
     P2_CUDA_TRY(cudaGetLastError());
