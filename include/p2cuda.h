@@ -22,6 +22,8 @@
  *                      rocks p2_ronurecalc_powerlaw
  *   p2_movemark        void movemark(void), pardiso/mark3mg.c:174
  *                      (prototype pardiso/head3mg.c:416)
+ *   p2_effbulk_visc    void effbulkvisccalc(int), pardiso/mark3mg.c:2
+ *                      (prototype pardiso/head3mg.c:435), mode 1
  * A C shim with the reference's own signatures on top of these calls is in
  * pardiso2_b200/csrc/move3mg_cuda.c.
  */
@@ -233,6 +235,30 @@ p2_status p2_get_markers(p2_ctx *ctx, float *markx, float *marky, float *markz);
  * marker time step (move3mgNew.c:3293-3316). */
 p2_status p2_stress_strain(p2_ctx *ctx, float *sxx, float *syy, float *szz, float *sxy, float *sxz, float *syz,
                            float *exx, float *eyy, float *ezz, float *exy, float *exz, float *eyz, double vrange[6]);
+
+/* Effective bulk viscosity diagnostics of a solution: effbulkvisccalc(1)
+ * (pardiso/mark3mg.c:2-150; prototype pardiso/head3mg.c:435).  Over the
+ * level-0 nodes with ro > 1500 and every index > 0: the averages of the
+ * strain-rate and stress second invariants of the cell behind the node
+ * (eiin, siin; shear terms averaged over the cell's four edges of each
+ * orientation), of the visco-plastic strain-rate invariant from the stresses
+ * (eiivp), of the dissipation (hsn) and of nxx * eiin (tau2), the harmonic
+ * mean of nxx (nubulkn), nubulk1..4 formed from them, and the averages of the
+ * twelve tensor components (exx eyy ezz exy exz eyz sxx syy szz sxy sxz syz)
+ * over inclusion nodes (ro > 3850) and matrix nodes.  Inputs are host arrays
+ * in the node layout, as vpiterate / p2_stress_strain leave them.  Per-node
+ * values follow the reference's float/double operations; the sums run in a
+ * different (fixed) order, so results agree to about 1e-12 relative. */
+typedef struct {
+    double eiin, siin, eiivp, tau2, hsn, nubulkn;
+    double nubulk1, nubulk2, nubulk3, nubulk4;
+    double matrix[12], incl[12];
+    long numtot, nummat, numinc;
+} p2_effbulk;
+p2_status p2_effbulk_visc(p2_ctx *ctx, const float *ro, const float *nxx, const float *nxy, const float *nxz,
+                          const float *nyz, const float *exx, const float *eyy, const float *ezz, const float *exy,
+                          const float *exz, const float *eyz, const float *sxx, const float *syy, const float *szz,
+                          const float *sxy, const float *sxz, const float *syz, p2_effbulk *out);
 
 /* The p2_ronurecalc interpolation for callers that cannot allocate device
  * memory: a host code whose device memory is all handed out by its own pool

@@ -53,8 +53,28 @@ def lib() -> C.CDLL:
                                    C.c_void_p]
         L.p2o_stress_strain.argtypes = [C.c_int, C.c_int, C.c_int, _dp, _dp, _dp] + [_fp] * 7 + [
             C.c_double, C.c_double, C.POINTER(C.c_void_p)]
+        L.p2o_effbulk.argtypes = [C.c_int, C.c_int, C.c_int, C.POINTER(C.c_void_p), _dp,
+                                  np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS")]
         _lib = L
     return _lib
+
+
+BULK_KEYS = ("ro", "nxx", "nxy", "nxz", "nyz", "exx", "eyy", "ezz", "exy", "exz", "eyz",
+             "sxx", "syy", "szz", "sxy", "sxz", "syz")
+
+
+def effbulk(model, fields):
+    """effbulkvisccalc(1) diagnostics by the oracle: (out[34], counts[3]) with
+    out = eiin siin eiivp tau2 hsn nubulkn nubulk1..4, matrix[12], incl[12]
+    and counts = numtot nummat numinc."""
+    L = lib()
+    nx, ny, nz = model.shape
+    arrs = [np.ascontiguousarray(fields[k], np.float32) for k in BULK_KEYS]
+    ptrs = (C.c_void_p * 17)(*[a.ctypes.data for a in arrs])
+    out = np.zeros(34, np.float64)
+    counts = np.zeros(3, np.int64)
+    L.p2o_effbulk(nx, ny, nz, ptrs, out, counts)
+    return out, counts
 
 
 STRESS_KEYS = ("sxx", "syy", "szz", "sxy", "sxz", "syz", "exx", "eyy", "ezz", "exy", "exz", "eyz")

@@ -24,6 +24,7 @@
  *   marker -> node interpolation ......... pardiso/mark3mg.c:630-1133
  *     (power-law rock viscosity, viscalc 1463-1498)
  *   stresses / strain rates after a solve  pardiso/move3mgNew.c:2908-3038
+ *   effective bulk viscosity diagnostics . pardiso/mark3mg.c:2-150
  *   marker advection (RK4 / simple) ...... pardiso/mark3mg.c:174-629, with
  *     the staggered velocity interpolation vxyzcalc1 2963-3243
  *     (cell search m1serch..m3serch 1138-1204, constant rock viscosity
@@ -1793,6 +1794,83 @@ void p2o_stress_strain(int nx, int ny, int nz, const double *gx, const double *g
                            st_nu(nyz[u], nubeg, nuend));
                 }
             }
+}
+
+/* ---------------------------------------------------------------------- */
+/* Effective bulk viscosity diagnostics (effbulkvisccalc mode 1,           */
+/* mark3mg.c:2-150), in the reference's order and float/double mix.        */
+/* in: ro nxx nxy nxz nyz exx eyy ezz exy exz eyz sxx syy szz sxy sxz syz;  */
+/* out: eiin siin eiivp tau2 hsn nubulkn nubulk1..4, matrix[12], incl[12]; */
+/* counts: numtot nummat numinc.                                          */
+void p2o_effbulk(int nx, int ny, int nz, const float *const *in, double *out, long *counts)
+{
+    const float *ro = in[0], *nxx = in[1], *nxy = in[2], *nxz = in[3], *nyz = in[4];
+    const float *exx = in[5], *eyy = in[6], *ezz = in[7], *exy = in[8], *exz = in[9], *eyz = in[10];
+    const float *sxx = in[11], *syy = in[12], *szz = in[13], *sxy = in[14], *sxz = in[15], *syz = in[16];
+    long m1, m2, m3, m4, v1[8], numtot = 0, numinc = 0, nummat = 0, sy = ny, sz = (long)nx * ny;
+    double tau2 = 0, siin = 0, eiin = 0, eiivp = 0, hsn = 0, nubulkn = 0, ac[12] = {0}, ai[12] = {0};
+    int q;
+    for (m3 = 0; m3 < nz; m3++)
+        for (m1 = 0; m1 < nx; m1++)
+            for (m2 = 0; m2 < ny; m2++) {
+                double Exy, Exz, Eyz, Sxy, Sxz, Syz, eiinloc, siinloc, eiivploc, hsnloc, *acc;
+                float c[12];
+                m4 = m3 * sz + m1 * sy + m2;
+                if (!(ro[m4] > 1500 && m1 > 0 && m2 > 0 && m3 > 0)) continue;
+                numtot += 1;
+                nubulkn += 1 / nxx[m4];
+                v1[0] = (m3 - 1) * sz + (m1 - 1) * sy + (m2 - 1); v1[1] = v1[0] + 1;
+                v1[2] = v1[0] + sy; v1[3] = v1[2] + 1;
+                v1[4] = v1[0] + sz; v1[5] = v1[4] + 1;
+                v1[6] = v1[4] + sy; v1[7] = v1[6] + 1;
+                Exy = (exy[v1[0]] * exy[v1[0]] + exy[v1[1]] * exy[v1[1]] + exy[v1[2]] * exy[v1[2]] + exy[v1[3]] * exy[v1[3]]) / 4;
+                Exz = (exz[v1[0]] * exz[v1[0]] + exz[v1[2]] * exz[v1[2]] + exz[v1[4]] * exz[v1[4]] + exz[v1[6]] * exz[v1[6]]) / 4;
+                Eyz = (eyz[v1[0]] * eyz[v1[0]] + eyz[v1[1]] * eyz[v1[1]] + eyz[v1[4]] * eyz[v1[4]] + eyz[v1[5]] * eyz[v1[5]]) / 4;
+                Sxy = (sxy[v1[0]] * sxy[v1[0]] + sxy[v1[1]] * sxy[v1[1]] + sxy[v1[2]] * sxy[v1[2]] + sxy[v1[3]] * sxy[v1[3]]) / 4;
+                Sxz = (sxz[v1[0]] * sxz[v1[0]] + sxz[v1[2]] * sxz[v1[2]] + sxz[v1[4]] * sxz[v1[4]] + sxz[v1[6]] * sxz[v1[6]]) / 4;
+                Syz = (syz[v1[0]] * syz[v1[0]] + syz[v1[1]] * syz[v1[1]] + syz[v1[4]] * syz[v1[4]] + syz[v1[5]] * syz[v1[5]]) / 4;
+                eiinloc = pow(0.5 * (exx[m4] * exx[m4] + eyy[m4] * eyy[m4] + ezz[m4] * ezz[m4]) + Exy + Exz + Eyz, 0.5);
+                siinloc = pow(0.5 * (sxx[m4] * sxx[m4] + syy[m4] * syy[m4] + szz[m4] * szz[m4]) + Sxy + Sxz + Syz, 0.5);
+                Exy = (pow(sxy[v1[0]] / 2 / nxy[v1[0]], 2) + pow(sxy[v1[1]] / 2 / nxy[v1[1]], 2) +
+                       pow(sxy[v1[2]] / 2 / nxy[v1[2]], 2) + pow(sxy[v1[3]] / 2 / nxy[v1[3]], 2)) / 4;
+                Exz = (pow(sxz[v1[0]] / 2 / nxz[v1[0]], 2) + pow(sxz[v1[2]] / 2 / nxz[v1[2]], 2) +
+                       pow(sxz[v1[4]] / 2 / nxz[v1[4]], 2) + pow(sxz[v1[6]] / 2 / nxz[v1[6]], 2)) / 4;
+                Eyz = (pow(syz[v1[0]] / 2 / nyz[v1[0]], 2) + pow(syz[v1[1]] / 2 / nyz[v1[1]], 2) +
+                       pow(syz[v1[4]] / 2 / nyz[v1[4]], 2) + pow(syz[v1[5]] / 2 / nyz[v1[5]], 2)) / 4;
+                eiivploc = pow(0.5 * (pow(sxx[m4] / 2 / nxx[m4], 2) + pow(syy[m4] / 2 / nxx[m4], 2) +
+                                      pow(szz[m4] / 2 / nxx[m4], 2)) + Exy + Exz + Eyz, 0.5);
+                Sxy = (sxy[v1[0]] * sxy[v1[0]] / 2 / nxy[v1[0]] + sxy[v1[1]] * sxy[v1[1]] / 2 / nxy[v1[1]] +
+                       sxy[v1[2]] * sxy[v1[2]] / 2 / nxy[v1[2]] + sxy[v1[3]] * sxy[v1[3]] / 2 / nxy[v1[3]]) / 4;
+                Sxz = (sxz[v1[0]] * sxz[v1[0]] / 2 / nxz[v1[0]] + sxz[v1[2]] * sxz[v1[2]] / 2 / nxz[v1[2]] +
+                       sxz[v1[4]] * sxz[v1[4]] / 2 / nxz[v1[4]] + sxz[v1[6]] * sxz[v1[6]] / 2 / nxz[v1[6]]) / 4;
+                Syz = (syz[v1[0]] * syz[v1[0]] / 2 / nyz[v1[0]] + syz[v1[1]] * syz[v1[1]] / 2 / nyz[v1[1]] +
+                       syz[v1[4]] * syz[v1[4]] / 2 / nyz[v1[4]] + syz[v1[5]] * syz[v1[5]] / 2 / nyz[v1[5]]) / 4;
+                hsnloc = (sxx[m4] * sxx[m4] + syy[m4] * syy[m4] + szz[m4] * szz[m4]) / 2 / nxx[m4] + 2.0 * (Sxy + Sxz + Syz);
+                eiin += eiinloc;
+                tau2 += nxx[m4] * eiinloc;
+                siin += siinloc;
+                hsn += hsnloc;
+                eiivp += eiivploc;
+                c[0] = exx[m4]; c[1] = eyy[m4]; c[2] = ezz[m4];
+                c[3] = (exy[v1[0]] + exy[v1[1]] + exy[v1[2]] + exy[v1[3]]) / 4;
+                c[4] = (exz[v1[0]] + exz[v1[2]] + exz[v1[4]] + exz[v1[6]]) / 4;
+                c[5] = (eyz[v1[0]] + eyz[v1[1]] + eyz[v1[4]] + eyz[v1[5]]) / 4;
+                c[6] = sxx[m4]; c[7] = syy[m4]; c[8] = szz[m4];
+                c[9] = (sxy[v1[0]] + sxy[v1[1]] + sxy[v1[2]] + sxy[v1[3]]) / 4;
+                c[10] = (sxz[v1[0]] + sxz[v1[2]] + sxz[v1[4]] + sxz[v1[6]]) / 4;
+                c[11] = (syz[v1[0]] + syz[v1[1]] + syz[v1[4]] + syz[v1[5]]) / 4;
+                if (ro[m4] > 3850) { numinc += 1; acc = ai; } else { nummat += 1; acc = ac; }
+                for (q = 0; q < 12; q++) acc[q] += c[q];
+            }
+    eiin /= numtot; siin /= numtot; hsn /= numtot; eiivp /= numtot; nubulkn = numtot / nubulkn; tau2 /= numtot;
+    for (q = 0; q < 12; q++) {
+        if (nummat > 0) ac[q] /= nummat;
+        if (numinc > 0) ai[q] /= numinc;
+    }
+    out[0] = eiin; out[1] = siin; out[2] = eiivp; out[3] = tau2; out[4] = hsn; out[5] = nubulkn;
+    out[6] = tau2 / eiin; out[7] = hsn / 4 / eiin / eiin; out[8] = hsn / 4 / eiivp / eiivp; out[9] = siin / 2 / eiin;
+    for (q = 0; q < 12; q++) { out[10 + q] = ac[q]; out[22 + q] = ai[q]; }
+    counts[0] = numtot; counts[1] = nummat; counts[2] = numinc;
 }
 
 /* Debug/test helpers: sweeps of the level-0 smoother only; two-grid count. */

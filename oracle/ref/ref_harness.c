@@ -43,6 +43,7 @@ void PARDISO(void **pt, int *maxfct, int *mnum, int *mtype, int *phase, int *n,
 #define vpiterate vpiterate_cpu
 #define ronurecalc ronurecalc_cpu
 #define movemark movemark_cpu
+#define effbulkvisccalc effbulkvisccalc_cpu
 #endif
 #include "move3mgNew.c"
 #include "mark3mg.c"
@@ -50,6 +51,7 @@ void PARDISO(void **pt, int *maxfct, int *mnum, int *mtype, int *phase, int *n,
 #undef vpiterate
 #undef ronurecalc
 #undef movemark
+#undef effbulkvisccalc
 #endif
 #include "gaus3mg_SerieMG.c"
 #include "heat3mg.c"
@@ -443,6 +445,16 @@ void p2ref_get_val1_marke(double *ov, float *oe)
 {
     long i;
     for (i = 0; i < marknum; i++) { ov[i] = val1[i]; oe[i] = marke[i]; }
+}
+
+/* effbulkvisccalc(1) (mark3mg.c:2-150) on vpiterate's globals; it appends a
+ * line to effbulkvisc.txt in the current directory and prints. */
+void p2ref_effbulk(const float *iro)
+{
+    memcpy(ro, iro, sizeof(float) * (size_t)nodenum);
+    mute();
+    effbulkvisccalc(1);
+    unmute();
 }
 
 void p2ref_fill_markk(float v)

@@ -17,11 +17,13 @@
 #define vpiterate vpiterate_cpu
 #define ronurecalc ronurecalc_cpu
 #define movemark movemark_cpu
+#define effbulkvisccalc effbulkvisccalc_cpu
 #include "move3mgNew.c"
 #include "mark3mg.c"
 #undef vpiterate
 #undef ronurecalc
 #undef movemark
+#undef effbulkvisccalc
 #include "gaus3mg_SerieMG.c"
 #include "heat3mg.c"
 #include "move3mg_cuda.c"

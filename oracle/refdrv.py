@@ -74,6 +74,7 @@ def _load(shim: bool = False) -> C.CDLL:
         lib.p2ref_set_step.argtypes = [C.c_double, C.c_double]
         lib.p2ref_set_marke.argtypes = [_fp]
         lib.p2ref_set_rheology.argtypes = [C.c_int, _dp, _dp, _dp]
+        lib.p2ref_effbulk.argtypes = [_fp]
         lib.p2ref_fill_val1.argtypes = [C.c_double]
         lib.p2ref_get_val1_marke.argtypes = [_dp, _fp]
         lib.p2ref_get_timestep.restype = C.c_double
@@ -218,6 +219,20 @@ class RefModel:
     def update_stress(self):
         """Run the stress / strain-rate pass into vpiterate's globals."""
         self.lib.p2ref_update_stress()
+
+    def effbulk(self, ro, workdir):
+        """effbulkvisccalc(1) with density ro on the current node fields and
+        vpiterate's stress globals; returns the 36 numbers of the line it
+        appends to workdir/effbulkvisc.txt (printed with %e)."""
+        here = os.getcwd()
+        os.chdir(workdir)
+        try:
+            self.lib.p2ref_effbulk(np.ascontiguousarray(ro, np.float32))
+            with open(os.path.join(workdir, "effbulkvisc.txt")) as f:
+                line = f.read().strip().splitlines()[-1]
+        finally:
+            os.chdir(here)
+        return np.array([float(v) for v in line.split()])
 
     def set_rheology(self, marknu, markmm, val1):
         """Power-law parameters per rock type and val1 per marker."""

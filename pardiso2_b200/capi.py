@@ -22,7 +22,7 @@ EXPORTED = ["p2_default_params", "p2_create", "p2_destroy", "p2_last_error", "p2
             "p2_upload_markers", "p2_ronurecalc_resident", "p2_get_nodes", "p2_debug_apply", "p2_debug_restrict",
             "p2_debug_prolong", "p2_debug_level_fields", "p2_debug_time_smoother", "p2_ronurecalc_noalloc", "p2_autotune",
             "p2_movemark", "p2_movemark_resident", "p2_get_markers", "p2_stress_strain",
-            "p2_stokes_solve_batch", "p2_movemark_strain", "p2_ronurecalc_powerlaw"]
+            "p2_stokes_solve_batch", "p2_movemark_strain", "p2_ronurecalc_powerlaw", "p2_effbulk_visc"]
 
 
 class Params(C.Structure):
@@ -41,6 +41,19 @@ class TuneInfo(C.Structure):
 
     def as_dict(self) -> Dict:
         return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class EffBulk(C.Structure):
+    _fields_ = [("eiin", C.c_double), ("siin", C.c_double), ("eiivp", C.c_double), ("tau2", C.c_double),
+                ("hsn", C.c_double), ("nubulkn", C.c_double), ("nubulk1", C.c_double), ("nubulk2", C.c_double),
+                ("nubulk3", C.c_double), ("nubulk4", C.c_double), ("matrix", C.c_double * 12),
+                ("incl", C.c_double * 12), ("numtot", C.c_long), ("nummat", C.c_long), ("numinc", C.c_long)]
+
+    def as_dict(self) -> Dict:
+        d = {k: getattr(self, k) for k, _ in self._fields_}
+        d["matrix"] = list(self.matrix)
+        d["incl"] = list(self.incl)
+        return d
 
 
 class SolveInfo(C.Structure):
@@ -103,6 +116,8 @@ def load() -> C.CDLL:
     L.p2_movemark_strain.restype = C.c_int
     L.p2_ronurecalc_powerlaw.argtypes = [vp, C.c_long, _fp, _fp, _fp, _bp, C.c_int] + [_dp] * 6 + [_fp] * 6
     L.p2_ronurecalc_powerlaw.restype = C.c_int
+    L.p2_effbulk_visc.argtypes = [vp] + [_fp] * 17 + [C.POINTER(EffBulk)]
+    L.p2_effbulk_visc.restype = C.c_int
     for f in ("p2_movemark", "p2_movemark_resident", "p2_get_markers", "p2_stress_strain"):
         getattr(L, f).restype = C.c_int
     for f in ("p2_create", "p2_set_grid", "p2_set_bc", "p2_set_nodes", "p2_stokes_solve", "p2_stokes_solve_resident",
@@ -197,6 +212,16 @@ class Context:
                                               out[2], np.ascontiguousarray(markers[3], np.int8), v1, me),
                     "p2_movemark_strain")
         return out[0], out[1], out[2], v1, me
+
+    BULK_KEYS = ("ro", "nxx", "nxy", "nxz", "nyz", "exx", "eyy", "ezz", "exy", "exz", "eyz",
+                 "sxx", "syy", "szz", "sxy", "sxz", "syz")
+
+    def effbulk_visc(self, fields: Dict[str, np.ndarray]) -> EffBulk:
+        """effbulkvisccalc(1) diagnostics of node fields (keys BULK_KEYS)."""
+        out = EffBulk()
+        self._check(self.L.p2_effbulk_visc(self.h, *[np.ascontiguousarray(fields[k], np.float32)
+                                                     for k in self.BULK_KEYS], C.byref(out)), "p2_effbulk_visc")
+        return out
 
     def movemark_resident(self, timestep: float, markmod: int = 2, outgrid: int = 0) -> float:
         ms = C.c_double()

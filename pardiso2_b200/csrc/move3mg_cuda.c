@@ -1,6 +1,6 @@
 /*
- * move3mg_cuda.c -- the reference's vpiterate(), ronurecalc() and movemark()
- * on top of libp2cuda.so (include/p2cuda.h).
+ * move3mg_cuda.c -- the reference's vpiterate(), ronurecalc(), movemark()
+ * and effbulkvisccalc() on top of libp2cuda.so (include/p2cuda.h).
  *
  * This file is compiled inside the reference's unity build (pardiso/i3mg.c
  * includes head3mg.c, load3mg.c, move3mgNew.c, mark3mg.c, ... into one
@@ -12,11 +12,13 @@
  *     #define vpiterate  vpiterate_cpu     -- pardiso/move3mgNew.c:1791
  *     #define ronurecalc ronurecalc_cpu    -- pardiso/mark3mg.c:630
  *     #define movemark   movemark_cpu      -- pardiso/mark3mg.c:174
+ *     #define effbulkvisccalc effbulkvisccalc_cpu  -- pardiso/mark3mg.c:2
  *     #include "move3mgNew.c"
  *     #include "mark3mg.c"
  *     #undef vpiterate
  *     #undef ronurecalc
  *     #undef movemark
+ *     #undef effbulkvisccalc
  *     #include "move3mg_cuda.c"
  *
  * Inputs read: xnumx, ynumy, znumz, gx, gy, gz, x/y/zperiodic, multinum,
@@ -199,4 +201,39 @@ void movemark(void)
             markk[m] = 0;
     }
     free(was_in);
+}
+
+/* pardiso/mark3mg.c:2 (prototype pardiso/head3mg.c:435): effective bulk
+ * viscosity diagnostics.  Mode 1 (node fields) runs on the GPU
+ * (p2_effbulk_visc) and prints and appends to effbulkvisc.txt what the
+ * reference does; mode 2 (the brittle-strain budget of marker types 7-10)
+ * stays the reference's own effbulkvisccalc_cpu. */
+void effbulkvisccalc(int nodemark)
+{
+    p2_status st;
+    p2_effbulk r;
+    FILE *f;
+    if (nodemark != 1) {
+        effbulkvisccalc_cpu(nodemark);
+        return;
+    }
+    p2s_setup();
+    st = p2_effbulk_visc(p2s_ctx, ro, nxx, nxy, nxz, nyz, exx, eyy, ezz, exy, exz, eyz, sxx, syy, szz, sxy, sxz,
+                         syz, &r);
+    if (st != P2_OK) p2s_fail("p2_effbulk_visc", st);
+    printf("\n Siin = %e Eiin = %e Eiivp = %e Tau2n = %e Hsn = %e Nubulkn = %e Tot Num = %ld\n", r.siin, r.eiin,
+           r.eiivp, r.tau2, r.hsn, r.nubulkn, r.numtot);
+    printf("\n Nubulk1 = Tau2n/Eiin %e \n", r.nubulk1);
+    printf("\n Nubulk2 = Hs/4/Eiin^2 %e \n", r.nubulk2);
+    printf("\n Nubulk3 = Hs/4/Eiivp^2 %e \n", r.nubulk3);
+    printf("\n Nubulk4 = Siin/2/Eiin %e \n", r.nubulk4);
+    f = fopen("effbulkvisc.txt", "at");
+    if (!f) return;
+    fprintf(f, "%e %e %ld %ld %ld %e %e %e %e %e %e %e %e %e %e %e %e %e %e %e %e %e %e %e %e %e %e %e %e %e %e %e %e "
+               "%e %e %e\n",
+            timesum, timestep, r.numinc, r.nummat, r.numtot, r.matrix[0], r.matrix[1], r.matrix[2], r.matrix[3],
+            r.matrix[4], r.matrix[5], r.matrix[6], r.matrix[7], r.matrix[8], r.matrix[9], r.matrix[10], r.matrix[11],
+            r.incl[0], r.incl[1], r.incl[2], r.incl[3], r.incl[4], r.incl[5], r.incl[6], r.incl[7], r.incl[8],
+            r.incl[9], r.incl[10], r.incl[11], r.siin, r.eiin, r.eiivp, r.hsn, r.nubulk2, r.nubulk3, r.nubulk4);
+    fclose(f);
 }

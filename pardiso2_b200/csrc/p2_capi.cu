@@ -430,6 +430,19 @@ p2_status p2_stress_strain(p2_ctx *ctx, float *sxx, float *syy, float *szz, floa
     });
 }
 
+p2_status p2_effbulk_visc(p2_ctx *ctx, const float *ro, const float *nxx, const float *nxy, const float *nxz,
+                          const float *nyz, const float *exx, const float *eyy, const float *ezz, const float *exy,
+                          const float *exz, const float *eyz, const float *sxx, const float *syy, const float *szz,
+                          const float *sxy, const float *sxz, const float *syz, p2_effbulk *out)
+{
+    return guard(ctx, [&] {
+        P2_CUDA_TRY(cudaSetDevice(ctx->s->dev));
+        const float *const e[6] = {exx, eyy, ezz, exy, exz, eyz};
+        const float *const s[6] = {sxx, syy, szz, sxy, sxz, syz};
+        ctx->s->effbulk(ro, nxx, nxy, nxz, nyz, e, s, out);
+    });
+}
+
 p2_status p2_autotune(p2_ctx *ctx, int trial_iters, p2_tune_info *info)
 {
     return guard(ctx, [&] {

@@ -148,7 +148,189 @@ __global__ void k_vrange_final(int nparts, const float *partial, double *out)
     out[q] = (double)a;
 }
 
+// ---------------------------------------------------------------------------
+// Effective bulk viscosity diagnostics (effbulkvisccalc mode 1,
+// pardiso/mark3mg.c:2-150): over the level-0 nodes with ro > 1500 (and index
+// > 0 on every axis), the strain-rate and stress invariants of the cell
+// behind the node (shear terms averaged over the cell's four edges of each
+// orientation), their visco-plastic variant, the dissipation, the averages
+// of the tensor components split into inclusions (ro > 3850) and matrix, and
+// the harmonic mean of nxx.  Per-node values follow the reference's float /
+// double mix operation by operation; the sums are taken per block and then
+// in block order (deterministic, a different order from the reference's
+// sequential loop).
+constexpr int kBulkSums = 30;  // see k_effbulk for the slots
+constexpr int kBulkBlocks = 296;
+
+struct BulkIn {
+    const float *ro, *nxx, *nxy, *nxz, *nyz;
+    const float *e[6], *s[6];  // exx eyy ezz exy exz eyz, sxx .. syz
+};
+
+__device__ __forceinline__ float sq(float a) { return __fmul_rn(a, a); }
+// (a[0]^2 + a[1]^2 + a[2]^2 + a[3]^2) / 4 in float
+__device__ __forceinline__ float avg_sq4(float a, float b, float c, float d)
+{
+    return __fdiv_rn(__fadd_rn(__fadd_rn(__fadd_rn(sq(a), sq(b)), sq(c)), sq(d)), 4.0f);
+}
+// (a + b + c + d) / 4 in float
+__device__ __forceinline__ float avg4(float a, float b, float c, float d)
+{
+    return __fdiv_rn(__fadd_rn(__fadd_rn(__fadd_rn(a, b), c), d), 4.0f);
+}
+// pow(s / 2 / n, 2): the quotient in float, squared in double
+__device__ __forceinline__ double vp2(float s, float n)
+{
+    const double q = (double)__fdiv_rn(__fdiv_rn(s, 2.0f), n);
+    return __dmul_rn(q, q);
+}
+// s * s / 2 / n in float
+__device__ __forceinline__ float heat1(float s, float n) { return __fdiv_rn(__fdiv_rn(sq(s), 2.0f), n); }
+
+__global__ void __launch_bounds__(256) k_effbulk(int nx, int ny, int nz, BulkIn in, double *partial)
+{
+    // slots: 0 eiin, 1 tau2, 2 siin, 3 hsn, 4 eiivp, 5 nubulkn, 6 numtot, 7 numinc, 8 nummat,
+    //        9..14 inclusion exx..eyz, 15..20 inclusion sxx..syz, 21..26 matrix exx..eyz,
+    //        27..29 matrix sxx, syy, szz (the matrix shear stresses go to 30..32 below)
+    __shared__ double sh[32];
+    double acc[kBulkSums + 3];
+#pragma unroll
+    for (int q = 0; q < kBulkSums + 3; q++) acc[q] = 0;
+    const long n = (long)nx * ny * nz, sxy_ = ny, sz = (long)nx * ny;
+    for (long m4 = (long)blockIdx.x * blockDim.x + threadIdx.x; m4 < n; m4 += (long)gridDim.x * blockDim.x) {
+        const int m2 = (int)(m4 % ny), m1 = (int)((m4 / ny) % nx), m3 = (int)(m4 / sz);
+        if (!((double)in.ro[m4] > 1500 && m1 > 0 && m2 > 0 && m3 > 0)) continue;
+        const long v0 = m4 - sz - sxy_ - 1, v1 = v0 + 1, v2 = v0 + sxy_, v3 = v2 + 1, v4 = v0 + sz, v5 = v4 + 1,
+                   v6 = v4 + sxy_;
+        const float *const *e = in.e, *const *s = in.s;
+        const float nxx = in.nxx[m4];
+        acc[6] += 1;
+        acc[5] = __dadd_rn(acc[5], (double)__fdiv_rn(1.0f, nxx));
+        // strain-rate and stress second invariants
+        const double Exy = avg_sq4(e[3][v0], e[3][v1], e[3][v2], e[3][v3]);
+        const double Exz = avg_sq4(e[4][v0], e[4][v2], e[4][v4], e[4][v6]);
+        const double Eyz = avg_sq4(e[5][v0], e[5][v1], e[5][v4], e[5][v5]);
+        const double Sxy = avg_sq4(s[3][v0], s[3][v1], s[3][v2], s[3][v3]);
+        const double Sxz = avg_sq4(s[4][v0], s[4][v2], s[4][v4], s[4][v6]);
+        const double Syz = avg_sq4(s[5][v0], s[5][v1], s[5][v4], s[5][v5]);
+        const double ne = (double)__fadd_rn(__fadd_rn(sq(e[0][m4]), sq(e[1][m4])), sq(e[2][m4]));
+        const double ns = (double)__fadd_rn(__fadd_rn(sq(s[0][m4]), sq(s[1][m4])), sq(s[2][m4]));
+        const double eii = __dsqrt_rn(__dadd_rn(__dadd_rn(__dadd_rn(__dmul_rn(0.5, ne), Exy), Exz), Eyz));
+        const double sii = __dsqrt_rn(__dadd_rn(__dadd_rn(__dadd_rn(__dmul_rn(0.5, ns), Sxy), Sxz), Syz));
+        // visco-plastic strain rate from the stresses
+        const float *nxy = in.nxy, *nxz = in.nxz, *nyz = in.nyz;
+        const double Vxy = __ddiv_rn(__dadd_rn(__dadd_rn(__dadd_rn(vp2(s[3][v0], nxy[v0]), vp2(s[3][v1], nxy[v1])),
+                                                         vp2(s[3][v2], nxy[v2])), vp2(s[3][v3], nxy[v3])), 4.0);
+        const double Vxz = __ddiv_rn(__dadd_rn(__dadd_rn(__dadd_rn(vp2(s[4][v0], nxz[v0]), vp2(s[4][v2], nxz[v2])),
+                                                         vp2(s[4][v4], nxz[v4])), vp2(s[4][v6], nxz[v6])), 4.0);
+        const double Vyz = __ddiv_rn(__dadd_rn(__dadd_rn(__dadd_rn(vp2(s[5][v0], nyz[v0]), vp2(s[5][v1], nyz[v1])),
+                                                         vp2(s[5][v4], nyz[v4])), vp2(s[5][v5], nyz[v5])), 4.0);
+        const double vn = __dadd_rn(__dadd_rn(vp2(s[0][m4], nxx), vp2(s[1][m4], nxx)), vp2(s[2][m4], nxx));
+        const double eiivp = __dsqrt_rn(__dadd_rn(__dadd_rn(__dadd_rn(__dmul_rn(0.5, vn), Vxy), Vxz), Vyz));
+        // dissipation
+        const double Hxy = avg4(heat1(s[3][v0], nxy[v0]), heat1(s[3][v1], nxy[v1]), heat1(s[3][v2], nxy[v2]),
+                                heat1(s[3][v3], nxy[v3]));
+        const double Hxz = avg4(heat1(s[4][v0], nxz[v0]), heat1(s[4][v2], nxz[v2]), heat1(s[4][v4], nxz[v4]),
+                                heat1(s[4][v6], nxz[v6]));
+        const double Hyz = avg4(heat1(s[5][v0], nyz[v0]), heat1(s[5][v1], nyz[v1]), heat1(s[5][v4], nyz[v4]),
+                                heat1(s[5][v5], nyz[v5]));
+        const double hs = __dadd_rn((double)__fdiv_rn(__fdiv_rn(__fadd_rn(__fadd_rn(sq(s[0][m4]), sq(s[1][m4])),
+                                                                          sq(s[2][m4])), 2.0f), nxx),
+                                    __dmul_rn(2.0, __dadd_rn(__dadd_rn(Hxy, Hxz), Hyz)));
+        acc[0] = __dadd_rn(acc[0], eii);
+        acc[1] = __dadd_rn(acc[1], __dmul_rn((double)nxx, eii));
+        acc[2] = __dadd_rn(acc[2], sii);
+        acc[3] = __dadd_rn(acc[3], hs);
+        acc[4] = __dadd_rn(acc[4], eiivp);
+        // tensor components: inclusions (ro > 3850) or matrix
+        const int base = (double)in.ro[m4] > 3850 ? 9 : 21;
+        acc[(double)in.ro[m4] > 3850 ? 7 : 8] += 1;
+        const float comp[12] = {e[0][m4], e[1][m4], e[2][m4], avg4(e[3][v0], e[3][v1], e[3][v2], e[3][v3]),
+                                avg4(e[4][v0], e[4][v2], e[4][v4], e[4][v6]), avg4(e[5][v0], e[5][v1], e[5][v4], e[5][v5]),
+                                s[0][m4], s[1][m4], s[2][m4], avg4(s[3][v0], s[3][v1], s[3][v2], s[3][v3]),
+                                avg4(s[4][v0], s[4][v2], s[4][v4], s[4][v6]), avg4(s[5][v0], s[5][v1], s[5][v4], s[5][v5])};
+#pragma unroll
+        for (int q = 0; q < 12; q++) {
+            const int slot = base + q;  // 21..32 for the matrix
+            acc[slot] = __dadd_rn(acc[slot], (double)comp[q]);
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < kBulkSums + 3; q++) {
+        double v = acc[q];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double t = 0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += sh[w];
+            partial[(long)q * gridDim.x + blockIdx.x] = t;
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void k_effbulk_final(int nparts, const double *partial, double *out)
+{
+    const int q = threadIdx.x;
+    if (q >= kBulkSums + 3) return;
+    double t = 0;
+    for (int b = 0; b < nparts; b++) t += partial[(long)q * nparts + b];
+    out[q] = t;
+}
+
 }  // namespace
+
+// effbulkvisccalc(1) on host arrays of the level-0 node fields; out[] as
+// p2_effbulk (include/p2cuda.h).
+void Solver::effbulk(const float *ro, const float *nxx, const float *nxy, const float *nxz, const float *nyz,
+                     const float *const e[6], const float *const s[6], p2_effbulk *res)
+{
+    if (!grid_ready) throw Error(P2_ERR_STATE, "diagnostics before p2_set_grid");
+    const Level &L0 = L[0];
+    const long n = L0.n;
+    if (!bulk_in[0]) {
+        for (int q = 0; q < 17; q++) bulk_in[q] = (float *)post_arena.alloc(sizeof(float) * n);
+        bulk_partial = (double *)post_arena.alloc(sizeof(double) * (kBulkSums + 3) * kBulkBlocks);
+        bulk_out = (double *)post_arena.alloc(sizeof(double) * (kBulkSums + 3));
+    }
+    const float *src[17] = {ro, nxx, nxy, nxz, nyz, e[0], e[1], e[2], e[3], e[4], e[5],
+                            s[0], s[1], s[2], s[3], s[4], s[5]};
+    for (int q = 0; q < 17; q++) {
+        if (!src[q]) throw Error(P2_ERR_ARG, "null node field");
+        P2_CUDA_TRY(cudaMemcpyAsync(bulk_in[q], src[q], sizeof(float) * n, cudaMemcpyHostToDevice, st));
+    }
+    BulkIn in;
+    in.ro = bulk_in[0]; in.nxx = bulk_in[1]; in.nxy = bulk_in[2]; in.nxz = bulk_in[3]; in.nyz = bulk_in[4];
+    for (int q = 0; q < 6; q++) { in.e[q] = bulk_in[5 + q]; in.s[q] = bulk_in[11 + q]; }
+    k_effbulk<<<kBulkBlocks, 256, 0, st>>>(L0.nx, L0.ny, L0.nz, in, bulk_partial); P2_COUNT_LAUNCH();
+    k_effbulk_final<<<1, 64, 0, st>>>(kBulkBlocks, bulk_partial, bulk_out); P2_COUNT_LAUNCH();
+    P2_CUDA_TRY(cudaGetLastError());
+    double a[kBulkSums + 3];
+    P2_CUDA_TRY(cudaMemcpyAsync(a, bulk_out, sizeof(a), cudaMemcpyDeviceToHost, st));
+    P2_CUDA_TRY(cudaStreamSynchronize(st));
+    // the reference's final divisions (mark3mg.c:101-114)
+    p2_effbulk r{};
+    r.numtot = (long)a[6];
+    r.numinc = (long)a[7];
+    r.nummat = (long)a[8];
+    const double nt = (double)r.numtot;
+    r.eiin = a[0] / nt;
+    r.tau2 = a[1] / nt;
+    r.siin = a[2] / nt;
+    r.hsn = a[3] / nt;
+    r.eiivp = a[4] / nt;
+    r.nubulkn = nt / a[5];
+    for (int q = 0; q < 12; q++) {
+        r.incl[q] = r.numinc > 0 ? a[9 + q] / (double)r.numinc : 0.0;
+        r.matrix[q] = r.nummat > 0 ? a[21 + q] / (double)r.nummat : 0.0;
+    }
+    r.nubulk1 = r.tau2 / r.eiin;
+    r.nubulk2 = r.hsn / 4 / r.eiin / r.eiin;
+    r.nubulk3 = r.hsn / 4 / r.eiivp / r.eiivp;
+    r.nubulk4 = r.siin / 2 / r.eiin;
+    if (res) *res = r;
+}
 
 // Stress and strain-rate fields from the last solution: in/out host arrays
 // (nullptr skips a field), vrange = {min vx, max vx, min vy, max vy, min vz,

@@ -259,6 +259,8 @@ void Solver::set_grid(long nx, long ny, long nz, const double *gx, const double 
     for (int q = 0; q < 12; q++) post_out[q] = nullptr;
     post_partial = nullptr;
     post_range = nullptr;
+    for (int q = 0; q < 17; q++) bulk_in[q] = nullptr;
+    bulk_partial = bulk_out = nullptr;
     mv_cap = 0;
     for (int q = 0; q < 3; q++) { d_g[q] = nullptr; mv_vel[q] = nullptr; mv_pos[q] = nullptr; }
     for (int q = 0; q < 6; q++) mv_e[q] = nullptr;

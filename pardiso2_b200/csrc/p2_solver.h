@@ -93,6 +93,8 @@ class Solver {
                               const signed char *mt, double *val1, float *marke);
     void get_markers(float *mx, float *my, float *mz);
     void stress_strain(float *const s[6], float *const e[6], double vrange[6]);
+    void effbulk(const float *ro, const float *nxx, const float *nxy, const float *nxz, const float *nyz,
+                 const float *const e[6], const float *const s[6], p2_effbulk *res);
 
     // test hooks (FP64, interleaved [P,Vx,Vy,Vz] per node)
     void debug_apply(int l, const double *x, double *y);
@@ -137,6 +139,8 @@ class Solver {
     float *post_out[12] = {};
     float *post_partial = nullptr;
     double *post_range = nullptr;
+    float *bulk_in[17] = {};         // effbulk inputs
+    double *bulk_partial = nullptr, *bulk_out = nullptr;
 
   private:
     template <typename T>

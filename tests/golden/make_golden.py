@@ -27,6 +27,12 @@ and, in move17.npz, marker advection by the reference's movemark()
                                     and marke (in: marke_in, 0 for two
                                     thirds of the markers; all 0 for
                                     simple_og0)
+and, in bulk21.npz, effbulkvisccalc(1) (pardiso/mark3mg.c:2-150) on the
+spheres21 node fields and the stresses / strain rates of its solution:
+  ro (a synthetic density above 1500 everywhere, above 3850 in the stiff
+  spheres), st_{sxx..eyz}, and line: the 36 numbers it appends to
+  effbulkvisc.txt (timesum timestep numinc nummat numtot, matrix exx..syz,
+  inclusion exx..syz, siin eiin eiivp hsn nubulk2 nubulk3 nubulk4; %e)
 and, in pl17.npz, ronurecalc with power-law rocks (viscalc,
 pardiso/mark3mg.c:1463-1498): markers, rock tables (n0, n1, ro, nu, mm),
 val1 per marker, the node fields, and marke after the call (the reference
@@ -201,6 +207,27 @@ def make_move_case():
     print("move17 written", {k: np.asarray(v).shape for k, v in out.items()})
 
 
+def make_bulk_case():
+    import tempfile
+    from oracle import refdrv
+    src = np.load(os.path.join(HERE, "spheres21.npz"))
+    m = CASES["spheres21"]()
+    m.markx, m.marky, m.markz, m.markt = src["markx"], src["marky"], src["markz"], src["markt"]
+    r = refdrv.RefModel(m)
+    r.set_nodes({k: src["node_" + k] for k in ("nu", "ro", "nxx", "nxy", "nxz", "nyz")})
+    r.set_velocity(*[np.asarray(src["sol_" + k], np.float32) for k in ("vx", "vy", "vz")])
+    r.fill_stress(0.0)
+    r.update_stress()
+    st = r.written_stress()
+    ro = np.where(src["node_nu"] > 1.0, 4000.0, 3300.0).astype(np.float32)
+    with tempfile.TemporaryDirectory() as d:
+        line = r.effbulk(ro, d)
+    out = {"ro": ro, "line": line}
+    out.update({"st_" + k: v for k, v in st.items()})
+    np.savez_compressed(os.path.join(HERE, "bulk21.npz"), **out)
+    print("bulk21 written", line[:5])
+
+
 def power_law_model():
     """sphere17 markers with a power-law sphere (type 1), a type-25 block
     (markn0 != markn1 but above type 20: constant markn0) and a constant
@@ -241,9 +268,11 @@ if __name__ == "__main__":
             make_move_case()
         elif sys.argv[1] == "pl17":
             make_pl_case()
+        elif sys.argv[1] == "bulk21":
+            make_bulk_case()
         else:
             make_case(sys.argv[1], CASES[sys.argv[1]])
     else:
         import subprocess
-        for c in list(CASES) + ["move17", "pl17"]:
+        for c in list(CASES) + ["move17", "pl17", "bulk21"]:
             subprocess.run([sys.executable, os.path.abspath(__file__), c], check=True)

@@ -50,6 +50,18 @@ def test_vpiterate_ronurecalc_movemark_through_the_reference_globals(oracle_mod)
     for k in st:
         assert np.array_equal(st[k].view(np.uint32), ref[k].view(np.uint32)), k
     assert r.timestep() == min(0.01 / vmax_valid(m, v, c) for c, v in enumerate(vel, 1))
+    # effbulkvisccalc(1) through the shim (p2_effbulk_visc): the line it
+    # appends equals the oracle's values on the same fields to 7 digits
+    import tempfile
+    from tests.test_oracle_golden import bulk_line_values
+    ro = np.where(f["nu"] > 1.0, 4000.0, 3300.0).astype(np.float32)
+    with tempfile.TemporaryDirectory() as d:
+        line = r.effbulk(ro, d)
+    bf = {"ro": ro, "nxx": f["nxx"], "nxy": f["nxy"], "nxz": f["nxz"], "nyz": f["nyz"]}
+    bf.update(st)
+    out, counts = oracle_mod.effbulk(m, bf)
+    mine = bulk_line_values(out, counts)
+    assert np.all(np.abs(mine - line[2:]) <= 6e-7 * np.abs(line[2:]))
     # the shim's movemark() -> p2_movemark on the velocities vpiterate wrote
     mx, my, mz, mt = move_markers(m)
     dt = 1.5 / 20 / max(float(np.abs(v).max()) for v in vel)

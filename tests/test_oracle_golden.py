@@ -211,3 +211,31 @@ def test_oracle_ronurecalc_power_law_vs_reference_golden(oracle_mod):
     for k in f:
         assert np.array_equal(f[k], g["node_" + k]), k
     assert np.abs(oracle_mod.ronurecalc(m)["nu"] - f["nu"]).max() > 1.0
+
+
+def _bulk_fields(g, nodes):
+    f = {k: nodes["node_" + k] for k in ("nxx", "nxy", "nxz", "nyz")}
+    f["ro"] = g["ro"]
+    f.update({k: g["st_" + k] for k in ("exx", "eyy", "ezz", "exy", "exz", "eyz", "sxx", "syy", "szz", "sxy", "sxz",
+                                        "syz")})
+    return f
+
+
+def bulk_line_values(out, counts):
+    """The oracle's diagnostics in the order of the reference's printed line
+    (after timesum, timestep): counts, matrix[12], incl[12], siin eiin eiivp
+    hsn nubulk2 nubulk3 nubulk4."""
+    return np.concatenate([[counts[2], counts[1], counts[0]], out[10:22], out[22:34],
+                           [out[1], out[0], out[2], out[4], out[7], out[8], out[9]]])
+
+
+def test_oracle_effbulk_vs_reference_golden(oracle_mod):
+    """effbulkvisccalc(1) (mark3mg.c:2-150): the oracle's values equal the
+    line the reference itself printed, to the 7 digits of its %e format."""
+    g = np.load(os.path.join(GOLDEN, "bulk21.npz"))
+    m, s = load_case("spheres21")
+    out, counts = oracle_mod.effbulk(m, _bulk_fields(g, s))
+    ref = g["line"][2:]
+    mine = bulk_line_values(out, counts)
+    assert np.all(np.abs(mine - ref) <= 6e-7 * np.abs(ref)), np.max(np.abs(mine - ref) / np.abs(ref))
+    assert counts[2] > 1000 and counts[1] > 1000
