@@ -303,7 +303,9 @@ p2_status p2_debug_prolong(p2_ctx *ctx, int coarse_level, const double *coarse_x
 p2_status p2_debug_level_fields(p2_ctx *ctx, float *nu, float *ro);
 /* Average device time (CUDA events on the library's stream) of one colour
  * pass of the cell-block smoother on `level` (FP32 when precision is 0),
- * over `passes` back-to-back passes on the state left by the last solve. */
+ * over `passes` passes on the state left by the last solve, each timed alone
+ * after a 256 MB write that evicts the level from L2 (allocated and freed by
+ * this call). */
 p2_status p2_debug_time_smoother(p2_ctx *ctx, int level, int passes, double *ms_per_pass);
 
 #ifdef __cplusplus

@@ -1367,24 +1367,42 @@ double Solver::debug_time_smoother(int l, int passes)
     if (!bc_ready) throw Error(P2_ERR_STATE, "no level data");
     Level &Lv = L[l];
     factor_cells();
-    P2_CUDA_TRY(cudaEventRecord(ev[5], st));
-    if (prm.precision == 0) {
-        LevelView<float> V = view<float>(l, false);
-        Vec4<float> x = Lv.x32, y = Lv.y32;
-        y.c[0] = x.c[0];
-        for (int p = 0; p < passes; p++) smoother_pass<float>(l, V, x.c[0], (p & 1) ? y : x, (p & 1) ? x : y, Lv.b32, p & 1);
-    } else {
-        LevelView<double> V = view<double>(l, false);
-        Vec4<double> x = Lv.x64, y = Lv.y64;
-        y.c[0] = x.c[0];
-        for (int p = 0; p < passes; p++) smoother_pass<double>(l, V, x.c[0], (p & 1) ? y : x, (p & 1) ? x : y, Lv.b64, p & 1);
+    // Each pass is timed alone after a 256 MB write (twice the 126 MB L2), so
+    // the level's fields come from HBM as they do in a V-cycle whose other
+    // levels and Krylov vectors have evicted them.
+    const size_t flush_bytes = (size_t)256 << 20;
+    void *flush = nullptr;
+    P2_CUDA_TRY(cudaMalloc(&flush, flush_bytes));
+    struct Free { void *p; ~Free() { if (p) cudaFree(p); } } hold{flush};
+    double total = 0;
+    cudaError_t err = cudaSuccess;
+    for (int p = 0; p < passes && err == cudaSuccess; p++) {
+        err = cudaMemsetAsync(flush, p & 0xff, flush_bytes, st);
+        if (err == cudaSuccess) err = cudaEventRecord(ev[5], st);
+        if (err != cudaSuccess) break;
+        if (prm.precision == 0) {
+            LevelView<float> V = view<float>(l, false);
+            Vec4<float> x = Lv.x32, y = Lv.y32;
+            y.c[0] = x.c[0];
+            smoother_pass<float>(l, V, x.c[0], (p & 1) ? y : x, (p & 1) ? x : y, Lv.b32, p & 1);
+        } else {
+            LevelView<double> V = view<double>(l, false);
+            Vec4<double> x = Lv.x64, y = Lv.y64;
+            y.c[0] = x.c[0];
+            smoother_pass<double>(l, V, x.c[0], (p & 1) ? y : x, (p & 1) ? x : y, Lv.b64, p & 1);
+        }
+        err = cudaEventRecord(ev[6], st);
+        if (err == cudaSuccess) err = cudaEventSynchronize(ev[6]);
+        if (err == cudaSuccess) err = cudaGetLastError();
+        float t = 0;
+        if (err == cudaSuccess) err = cudaEventElapsedTime(&t, ev[5], ev[6]);
+        total += t;
     }
-    P2_CUDA_TRY(cudaEventRecord(ev[6], st));
-    P2_CUDA_TRY(cudaEventSynchronize(ev[6]));
-    P2_CUDA_TRY(cudaGetLastError());
-    float t = 0;
-    P2_CUDA_TRY(cudaEventElapsedTime(&t, ev[5], ev[6]));
-    return (double)t / passes;
+    hold.p = nullptr;
+    cudaError_t ferr = cudaFree(flush);
+    P2_CUDA_TRY(err);
+    P2_CUDA_TRY(ferr);
+    return total / passes;
 }
 
 void Solver::debug_level_fields(float *nu, float *ro)
