@@ -24,6 +24,8 @@
  *                      (prototype pardiso/head3mg.c:416)
  *   p2_effbulk_visc    void effbulkvisccalc(int), pardiso/mark3mg.c:2
  *                      (prototype pardiso/head3mg.c:435), mode 1
+ *   p2_titerate        void titerate(int m0), pardiso/heat3mg.c:292
+ *                      (called from pardiso/i3mg.c:148 when tempmod is set)
  * A C shim with the reference's own signatures on top of these calls is in
  * pardiso2_b200/csrc/move3mg_cuda.c.
  */
@@ -259,6 +261,61 @@ p2_status p2_effbulk_visc(p2_ctx *ctx, const float *ro, const float *nxx, const 
                           const float *nyz, const float *exx, const float *eyy, const float *ezz, const float *exy,
                           const float *exz, const float *eyz, const float *sxx, const float *syy, const float *szz,
                           const float *sxy, const float *sxz, const float *syz, p2_effbulk *out);
+
+/* titerate() (pardiso/heat3mg.c:292; prototype pardiso/head3mg.c:386): one
+ * thermal step of `timestep` seconds on the level-0 temperature tk.
+ *   T boundary rows first go in through p2_heat_set_bc: bondm in the
+ *   reference layout, whose rows for the temperature start at 8 * nodenum
+ *   (bondm[8*nodenum + u] for the node u of every level, in3mg.c:367-383),
+ *   bondm_len >= 8 * nodenum + (sum of level nodes).  Every node on a wall of
+ *   every level needs a T boundary row; chains of copy rows are followed.
+ *   The step: heat sources ht (+ adiabatic heating with adiabyn 1 or 2 from
+ *   vx, vy, vz, gravity of p2_params, and pr; + shear heating with frictyn 1
+ *   from the twelve float fields sxx syy szz sxy sxz syz exx eyy ezz exy exz
+ *   eyz) give the right-hand side and the sub-step limit maxtkstep / max
+ *   |dT/dt|; each sub-step solves the implicit conduction rows with V-cycles
+ *   on levels 0..multinumt (multittt[0][l] pre-sweeps, multittt[1][l] sweeps
+ *   on the way up, multicyct cycles between error checks) until the RMS error
+ *   of the rows times the sub-step is at most heatmin (at most max_cycles
+ *   checks per sub-step; 0 = 10000; P2_OK with converged = 0 when reached).
+ *   Then the markers (optional, nmark 0 skips them): types 50..99 take the
+ *   node temperature, types below 50 the numerical-diffusion update of
+ *   markk (heatdif, tdeep, zdeep), as heat3mg.c:640-818 does.
+ *   tk and markk are updated in place; kt, cp, ro, ht, et are level-0 float
+ *   fields (ro of the node layout, as ronurecalc writes it).
+ *   The smoother is Gauss-Seidel in two colours (the reference sweeps the
+ *   rows in order), so the iterates differ and the temperatures agree with
+ *   the reference's to the tolerance heatmin sets. */
+typedef struct {
+    double maxtkstep;      /* K per sub-step */
+    double heatmin;        /* HEATMIN, K */
+    double t0koef, t1koef; /* smoother damping, prolongation factor */
+    double heatdif;        /* numerical diffusion of marker temperatures */
+    double tdeep, zdeep;   /* temperature of markers arriving below zdeep */
+    int multinumt, multicyct;
+    int multittt[2][P2_MAX_LEVELS];
+    int frictyn, adiabyn;
+    int max_cycles;
+} p2_heat_params;
+typedef struct {
+    double tktimestep;     /* sub-step limit (1e30 when no node heats) */
+    double maxtkrate;      /* max |dT/dt| of the right-hand side, K/s */
+    int substeps;          /* thermal sub-steps taken */
+    int cycles;            /* error checks, all sub-steps */
+    int converged;         /* 1 when every sub-step reached heatmin */
+    double heatsum;        /* RMS error after the last check, K */
+    double mintk, maxtk;   /* temperature range after the step */
+    double ms_total;       /* device time of the call, transfers included */
+    long long kernels;     /* kernel launches */
+} p2_heat_info;
+void p2_default_heat_params(p2_heat_params *hp);
+p2_status p2_heat_set_bc(p2_ctx *ctx, const int *bondm, long bondm_len, const float *bondv1, const int *bondn1,
+                         long bondnum);
+p2_status p2_titerate(p2_ctx *ctx, const p2_heat_params *hp, double timestep, float *tk, const float *kt,
+                      const float *cp, const float *ro, const float *ht, const float *et, const float *vx,
+                      const float *vy, const float *vz, const double *pr, const float *const *stress_strain,
+                      long marknum, const float *markx, const float *marky, const float *markz,
+                      const signed char *markt, float *markk, p2_heat_info *info);
 
 /* The p2_ronurecalc interpolation for callers that cannot allocate device
  * memory: a host code whose device memory is all handed out by its own pool

@@ -55,6 +55,11 @@ def lib() -> C.CDLL:
             C.c_double, C.c_double, C.POINTER(C.c_void_p)]
         L.p2o_effbulk.argtypes = [C.c_int, C.c_int, C.c_int, C.POINTER(C.c_void_p), _dp,
                                   np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS")]
+        L.p2o_titerate.argtypes = [C.c_int, C.c_int, C.c_int, _dp, _dp, _dp, C.c_int, _ip, _fp, _ip, _dp, _ip,
+                                   _fp, _fp, _fp, _fp, _fp, _fp, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                   C.c_void_p, C.c_long, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                   C.c_void_p, _dp]
+        L.p2o_titerate.restype = C.c_int
         _lib = L
     return _lib
 
@@ -234,3 +239,61 @@ def prolong(solver: "OracleSolver", lc: int, coarse_x, fine_x):
     f = np.array(fine_x, np.float64)
     _transfer_sigs().p2o_prolong(solver.h, lc, np.ascontiguousarray(coarse_x, np.float64), f)
     return f
+
+
+HEAT_DPAR = ("timestep", "maxtkstep", "heatmin", "t0koef", "t1koef", "heatdif", "tdeep", "zdeep", "gx", "gy", "gz")
+
+
+def heat_ipar(multinumt, multicyct, frictyn, adiabyn, max_cycles, pre, post):
+    """ipar of p2o_titerate: multicyct, frictyn, adiabyn, max_cycles,
+    multittt[0][0..15], multittt[1][0..15]."""
+    ip = np.zeros(36, np.int32)
+    ip[0], ip[1], ip[2], ip[3] = multicyct, frictyn, adiabyn, max_cycles
+    ip[4:4 + len(pre)] = pre
+    ip[20:20 + len(post)] = post
+    return ip
+
+
+def titerate(gx, gy, gz, multinumt, bondt, bondv1, bondn1, hp: dict, thermal, vel=None, pr=None, se=None,
+             markers=None, markk=None):
+    """titerate() restated (heat3mg.c:292-829): returns (tk, markk, info).
+    hp holds HEAT_DPAR keys and multicyct, frictyn, adiabyn, max_cycles,
+    pre (multittt[0]), post (multittt[1])."""
+    L = lib()
+    nx, ny, nz = len(gx), len(gy), len(gz)
+    dpar = np.array([hp[k] for k in HEAT_DPAR], np.float64)
+    ipar = heat_ipar(multinumt, hp["multicyct"], hp["frictyn"], hp["adiabyn"], hp.get("max_cycles", 0),
+                     hp["pre"], hp["post"])
+    tk = np.array(thermal.tk, np.float32, copy=True)
+    f = lambda a: np.ascontiguousarray(a, np.float32)
+    keep = []
+
+    def vp(a, dt):
+        if a is None:
+            return None
+        a = np.ascontiguousarray(a, dt)
+        keep.append(a)
+        return a.ctypes.data_as(C.c_void_p)
+
+    sep = None
+    if se is not None:
+        arrs = [np.ascontiguousarray(a, np.float32) for a in se]
+        keep.extend(arrs)
+        sep_arr = (C.c_void_p * 12)(*[a.ctypes.data_as(C.c_void_p) for a in arrs])
+        keep.append(sep_arr)
+        sep = C.cast(sep_arr, C.c_void_p)
+    nm = 0 if markers is None else len(markers[0])
+    mk = None if markk is None else np.array(markk, np.float32, copy=True)
+    info = np.zeros(8, np.float64)
+    L.p2o_titerate(nx, ny, nz, np.ascontiguousarray(gx, np.float64), np.ascontiguousarray(gy, np.float64),
+                   np.ascontiguousarray(gz, np.float64), multinumt, np.ascontiguousarray(bondt, np.int32),
+                   np.ascontiguousarray(np.asarray(bondv1, np.float32).reshape(-1)),
+                   np.ascontiguousarray(bondn1, np.int32), dpar, ipar, tk, f(thermal.kt), f(thermal.cp),
+                   f(thermal.ro), f(thermal.ht), f(thermal.et),
+                   *(vp(v, np.float32) for v in (vel if vel is not None else (None, None, None))),
+                   vp(pr, np.float64), sep, nm,
+                   *(vp(a, np.float32) for a in (markers[:3] if markers is not None else (None, None, None))),
+                   vp(markers[3] if markers is not None else None, np.int8),
+                   None if mk is None else mk.ctypes.data_as(C.c_void_p), info)
+    return tk, mk, {"tktimestep": info[0], "substeps": int(info[1]), "cycles": int(info[2]), "heatsum": info[3],
+                    "mintk": info[4], "maxtk": info[5], "capped": int(info[6]), "maxtkrate": info[7]}

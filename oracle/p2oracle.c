@@ -1915,3 +1915,548 @@ void p2o_prolong(void *h, int lc, const double *coarse_x, double *fine_x)
     for (u = 0; u < f->n; u++)
         for (c = 0; c < 4; c++) fine_x[u * 4 + c] = f->x[c][u];
 }
+
+/* ---------------------------------------------------------------------- */
+/* Heat equation step (titerate, pardiso/heat3mg.c:292-829), single thread. */
+/* Restated literally: the level-0 right-hand side heaterr mode 0 (6-291),  */
+/* the step limit from maxtkstep (331-374), rocprestrict (1248-1332), the   */
+/* implicit 7-point rows heaterr mode 1 and the boundary rows tbonderr      */
+/* (832-884) stored as gausmat2 does (gaus3mg_SerieMG.c:312-365), the       */
+/* damped lexicographic Gauss-Seidel gausmatt (1063-1121), trestrict        */
+/* (1124-1245), tprolong (957-1060), the error heaterr mode 2 and the       */
+/* marker temperatures with numerical diffusion (640-829, tkcalc1           */
+/* pardiso/mark3mg.c:1212-1282).  Float arrays (tk, tk0, tk1, tk2, kt, cp,  */
+/* ro, ht, et) and the float arithmetic of the reference's expressions on   */
+/* them are kept.  The reference loops until the error is below HEATMIN     */
+/* with no cap; here at most max_cycles batches of V-cycles run per step.   */
+typedef struct {
+    int nl;                        /* levels 0..nl-1 */
+    int nx[MAXLEV], ny[MAXLEV], nz[MAXLEV];
+    long off[MAXLEV], n[MAXLEV], tot;
+    double *g[MAXLEV][3];
+} ht_grid;
+
+static void ht_grid_build(ht_grid *G, int nx, int ny, int nz, const double *gx, const double *gy, const double *gz,
+                          int nl)
+{
+    int li, q, n2;
+    long off = 0;
+    G->nl = nl;
+    for (li = 0; li < nl; li++) {
+        int s = 1 << li;
+        if (li == 0) { G->nx[0] = nx; G->ny[0] = ny; G->nz[0] = nz; }
+        else {
+            G->nx[li] = (G->nx[li - 1] - 5) / 2 + 5;
+            G->ny[li] = (G->ny[li - 1] - 5) / 2 + 5;
+            G->nz[li] = (G->nz[li - 1] - 5) / 2 + 5;
+        }
+        G->n[li] = (long)G->nx[li] * G->ny[li] * G->nz[li];
+        G->off[li] = off;
+        off += G->n[li];
+        for (q = 0; q < 3; q++) {
+            int n = q == 0 ? G->nx[li] : q == 1 ? G->ny[li] : G->nz[li], nf = q == 0 ? nx : q == 1 ? ny : nz;
+            const double *g = q == 0 ? gx : q == 1 ? gy : gz;
+            double *o = malloc(sizeof(double) * n);
+            o[0] = g[0]; o[1] = g[1]; o[2] = g[2];
+            o[n - 1] = g[nf - 1]; o[n - 2] = g[nf - 2]; o[n - 3] = g[nf - 3];
+            for (n2 = 3; n2 < n - 3; n2++) o[n2] = g[(n2 - 2) * s + 2];
+            G->g[li][q] = o;
+        }
+    }
+    G->tot = off;
+}
+
+static void ht_grid_free(ht_grid *G)
+{
+    int li, q;
+    for (li = 0; li < G->nl; li++)
+        for (q = 0; q < 3; q++) free(G->g[li][q]);
+}
+
+/* coarse cell index of a fine line (heat3mg.c:979-990, 1160-1171, 1276-1287) */
+static long ht_cmin(long m, long nf, long nc)
+{
+    long c = (m - 2) / 2 + 2;
+    if (m < 3) c = m;
+    if (m > nf - 4) c = nc - (nf - m);
+    if (c > nc - 2) c = nc - 2;
+    return c;
+}
+
+typedef struct {
+    ht_grid G;
+    const int *bct;                /* T boundary row number per node, all levels */
+    const float *bondv1;
+    const int *bondn1;
+    float *kt, *cp, *ro;           /* all levels */
+    double *sol0, *sol1, *fre0, *fre1, *val1;
+    long *lin0, *pos0;
+    int *num0;
+    double t0koef, t1koef;
+} ht_ctx;
+
+/* Coarse level fields from the finer one: rocprestrict (heat3mg.c:1248-1332),
+ * float accumulators with double weights as the reference's arrays are. */
+static void ht_rocprestrict(ht_ctx *H, int lc)
+{
+    ht_grid *G = &H->G;
+    int lf = lc - 1;
+    long m1, m2, m3, u;
+    for (u = G->off[lc]; u < G->off[lc] + G->n[lc]; u++) { H->cp[u] = 0; H->kt[u] = 0; H->ro[u] = 0; H->sol1[u] = 0; }
+    for (m3 = 0; m3 < G->nz[lf]; m3++)
+        for (m1 = 0; m1 < G->nx[lf]; m1++)
+            for (m2 = 0; m2 < G->ny[lf]; m2++) {
+                long m4 = G->off[lf] + m3 * G->nx[lf] * G->ny[lf] + m1 * G->ny[lf] + m2, m10, m20, m30;
+                long c1 = ht_cmin(m1, G->nx[lf], G->nx[lc]), c2 = ht_cmin(m2, G->ny[lf], G->ny[lc]);
+                long c3 = ht_cmin(m3, G->nz[lf], G->nz[lc]);
+                double dx = G->g[lc][0][c1 + 1] - G->g[lc][0][c1], dy = G->g[lc][1][c2 + 1] - G->g[lc][1][c2];
+                double dz = G->g[lc][2][c3 + 1] - G->g[lc][2][c3];
+                for (m30 = c3; m30 <= c3 + 1; m30++) {
+                    double ddz = 1.0 - fabs((G->g[lc][2][m30] - G->g[lf][2][m3]) / dz);
+                    for (m10 = c1; m10 <= c1 + 1; m10++) {
+                        double ddx = 1.0 - fabs((G->g[lc][0][m10] - G->g[lf][0][m1]) / dx);
+                        for (m20 = c2; m20 <= c2 + 1; m20++) {
+                            double ddy = 1.0 - fabs((G->g[lc][1][m20] - G->g[lf][1][m2]) / dy);
+                            long m40 = G->off[lc] + m30 * G->nx[lc] * G->ny[lc] + m10 * G->ny[lc] + m20;
+                            double swt = ddx * ddy * ddz;
+                            H->cp[m40] += H->cp[m4] * swt;
+                            H->kt[m40] += H->kt[m4] * swt;
+                            H->ro[m40] += H->ro[m4] * swt;
+                            H->sol1[m40] += swt;
+                        }
+                    }
+                }
+            }
+    for (u = G->off[lc]; u < G->off[lc] + G->n[lc]; u++) {
+        H->cp[u] /= H->sol1[u];
+        H->kt[u] /= H->sol1[u];
+        H->ro[u] /= H->sol1[u];
+        H->sol1[u] = 0;
+    }
+}
+
+/* trestrict (heat3mg.c:1124-1245) */
+static void ht_restrict(ht_ctx *H, int lc)
+{
+    ht_grid *G = &H->G;
+    int lf = lc - 1;
+    long m1, m2, m3, u;
+    for (u = G->off[lc]; u < G->off[lc] + G->n[lc]; u++) { H->fre1[u] = 0; H->sol1[u] = 0; }
+    for (m3 = 0; m3 < G->nz[lf]; m3++)
+        for (m1 = 0; m1 < G->nx[lf]; m1++)
+            for (m2 = 0; m2 < G->ny[lf]; m2++) {
+                long m4 = G->off[lf] + m3 * G->nx[lf] * G->ny[lf] + m1 * G->ny[lf] + m2, m10, m20, m30;
+                long c1 = ht_cmin(m1, G->nx[lf], G->nx[lc]), c2 = ht_cmin(m2, G->ny[lf], G->ny[lc]);
+                long c3 = ht_cmin(m3, G->nz[lf], G->nz[lc]);
+                double dx = G->g[lc][0][c1 + 1] - G->g[lc][0][c1], dy = G->g[lc][1][c2 + 1] - G->g[lc][1][c2];
+                double dz = G->g[lc][2][c3 + 1] - G->g[lc][2][c3];
+                for (m30 = c3; m30 <= c3 + 1; m30++) {
+                    double ddz = (G->g[lc][2][m30] - G->g[lf][2][m3]) / dz;
+                    if (m30 == c3) ddz = -ddz;
+                    ddz = 1.0 - ddz;
+                    for (m10 = c1; m10 <= c1 + 1; m10++) {
+                        double ddx = (G->g[lc][0][m10] - G->g[lf][0][m1]) / dx;
+                        if (m10 == c1) ddx = -ddx;
+                        ddx = 1.0 - ddx;
+                        for (m20 = c2; m20 <= c2 + 1; m20++) {
+                            double ddy = (G->g[lc][1][m20] - G->g[lf][1][m2]) / dy;
+                            long m40 = G->off[lc] + m30 * G->nx[lc] * G->ny[lc] + m10 * G->ny[lc] + m20;
+                            if (m20 == c2) ddy = -ddy;
+                            ddy = 1.0 - ddy;
+                            if (!H->bct[m40]) {
+                                double swt = ddx * ddy * ddz;
+                                H->fre1[m40] += H->fre0[m4] * swt;
+                                H->sol1[m40] += swt;
+                            }
+                        }
+                    }
+                }
+            }
+    for (u = G->off[lc]; u < G->off[lc] + G->n[lc]; u++) {
+        if (H->sol1[u]) { H->fre1[u] /= H->sol1[u]; H->sol1[u] = 0; }
+        H->sol0[u] = 0;
+    }
+}
+
+/* tprolong with ynreset 0 (heat3mg.c:957-1060) */
+static void ht_prolong(ht_ctx *H, int lc)
+{
+    ht_grid *G = &H->G;
+    int lf = lc - 1;
+    long m1, m2, m3;
+    for (m3 = 0; m3 < G->nz[lf]; m3++)
+        for (m1 = 0; m1 < G->nx[lf]; m1++)
+            for (m2 = 0; m2 < G->ny[lf]; m2++) {
+                long m4 = G->off[lf] + m3 * G->nx[lf] * G->ny[lf] + m1 * G->ny[lf] + m2, m10, m20, m30;
+                long c1, c2, c3;
+                double dx, dy, dz;
+                if (H->bct[m4]) continue;
+                c1 = ht_cmin(m1, G->nx[lf], G->nx[lc]); c2 = ht_cmin(m2, G->ny[lf], G->ny[lc]);
+                c3 = ht_cmin(m3, G->nz[lf], G->nz[lc]);
+                dx = G->g[lc][0][c1 + 1] - G->g[lc][0][c1]; dy = G->g[lc][1][c2 + 1] - G->g[lc][1][c2];
+                dz = G->g[lc][2][c3 + 1] - G->g[lc][2][c3];
+                for (m30 = c3; m30 <= c3 + 1; m30++) {
+                    double ddz = (G->g[lc][2][m30] - G->g[lf][2][m3]) / dz;
+                    if (m30 == c3) ddz = -ddz;
+                    ddz = 1.0 - ddz;
+                    for (m10 = c1; m10 <= c1 + 1; m10++) {
+                        double ddx = (G->g[lc][0][m10] - G->g[lf][0][m1]) / dx;
+                        if (m10 == c1) ddx = -ddx;
+                        ddx = 1.0 - ddx;
+                        for (m20 = c2; m20 <= c2 + 1; m20++) {
+                            double ddy = (G->g[lc][1][m20] - G->g[lf][1][m2]) / dy;
+                            long m40 = G->off[lc] + m30 * G->nx[lc] * G->ny[lc] + m10 * G->ny[lc] + m20;
+                            if (m20 == c2) ddy = -ddy;
+                            ddy = 1.0 - ddy;
+                            H->sol0[m4] += H->sol0[m40] * (ddx * ddy * ddz) * H->t1koef;
+                        }
+                    }
+                }
+            }
+}
+
+/* gausmatt (heat3mg.c:1063-1121) on the rows of one level */
+static void ht_gausmatt(ht_ctx *H, int am, long mcmax, long mcmin)
+{
+    long m1;
+    int m2, m3;
+    for (m3 = 0; m3 < am; m3++)
+        for (m1 = mcmin; m1 <= mcmax; m1++)
+            if (H->num0[m1]) {
+                double ival = -H->fre1[m1], ival1 = H->val1[H->pos0[m1]];
+                for (m2 = 0; m2 < H->num0[m1]; m2++) ival += H->val1[H->pos0[m1] + m2] * H->sol0[H->lin0[H->pos0[m1] + m2]];
+                H->sol0[m1] -= ival / ival1 * H->t0koef;
+            }
+    for (m1 = mcmin; m1 <= mcmax; m1++)
+        if (H->num0[m1]) {
+            double ival = H->fre1[m1];
+            for (m2 = 0; m2 < H->num0[m1]; m2++) ival -= H->val1[H->pos0[m1] + m2] * H->sol0[H->lin0[H->pos0[m1] + m2]];
+            H->fre0[m1] = ival;
+        }
+}
+
+static void ht_row(ht_ctx *H, long u, int nn, const long *un, const double *ui, double rhs)
+{
+    int q;
+    H->fre1[u] = rhs;
+    H->pos0[u] = u * 7;
+    H->num0[u] = nn;
+    for (q = 0; q < nn; q++) { H->lin0[u * 7 + q] = un[q]; H->val1[u * 7 + q] = ui[q]; }
+}
+
+/* Inverse spacing factors of heaterr (heat3mg.c:21-24) */
+#define HT_KF(g, m) (2.0 / ((g)[(m) + 1] - (g)[(m) - 1]))
+
+/* dpar: timestep, maxtkstep, HEATMIN, t0koef, t1koef, heatdif, tdeep, zdeep, GX, GY, GZ
+ * ipar: multicyct, frictyn, adiabyn, max_cycles, multittt[0][0..15], multittt[1][0..15]
+ * se:   sxx, syy, szz, sxy, sxz, syz, exx, eyy, ezz, exy, exz, eyz (NULL: frictyn must be 0)
+ * info: tktimestep, substeps, V-cycle batches, last error, min tk, max tk, status (0 ok, 1 cap reached),
+ *       maxtkrate */
+int p2o_titerate(int nx, int ny, int nz, const double *gx, const double *gy, const double *gz, int multinumt,
+                 const int *bct, const float *bondv1, const int *bondn1, const double *dpar, const int *ipar,
+                 float *tk, const float *kt0, const float *cp0, const float *ro0, const float *ht, const float *et,
+                 const float *vx, const float *vy, const float *vz, const double *pr, const float *const *se,
+                 long nmark, const float *markx, const float *marky, const float *markz, const signed char *markt,
+                 float *markk, double *info)
+{
+    ht_ctx HC, *H = &HC;
+    ht_grid *G = &H->G;
+    long nxy = (long)nx * ny, nn = nxy * nz, u, m1, m2, m3, mk;
+    double timestep = dpar[0], maxtkstep = dpar[1], heatmin = dpar[2], heatdif = dpar[5];
+    double tdeep = dpar[6], zdeep = dpar[7], GXK = dpar[8], GYK = dpar[9], GZK = dpar[10];
+    int multicyct = ipar[0], frictyn = ipar[1], adiabyn = ipar[2], maxcyc = ipar[3];
+    double maxtkrate = 0, tktimestep = 1e30, tktimesum, tktimesum0, heatsum = 0, mintk = 1e30, maxtk = -1e30;
+    float *tk0, *tk1, *tk2;
+    int li, status = 0;
+    long nsub = 0, ncyc = 0;
+    const double *gl[3];
+    mv_grid MG;
+    const float *vel[3];
+    memset(info, 0, sizeof(double) * 8);
+    if (multinumt + 1 > MAXLEV || (frictyn && !se)) return -1;
+    memset(H, 0, sizeof(*H));
+    ht_grid_build(G, nx, ny, nz, gx, gy, gz, multinumt + 1);
+    H->bct = bct; H->bondv1 = bondv1; H->bondn1 = bondn1;
+    H->t0koef = dpar[3]; H->t1koef = dpar[4];
+    H->kt = calloc(G->tot, sizeof(float)); H->cp = calloc(G->tot, sizeof(float)); H->ro = calloc(G->tot, sizeof(float));
+    memcpy(H->kt, kt0, sizeof(float) * nn); memcpy(H->cp, cp0, sizeof(float) * nn); memcpy(H->ro, ro0, sizeof(float) * nn);
+    H->sol0 = calloc(G->tot, sizeof(double)); H->sol1 = calloc(G->tot, sizeof(double));
+    H->fre0 = calloc(G->tot, sizeof(double)); H->fre1 = calloc(G->tot, sizeof(double));
+    H->val1 = calloc(G->tot * 7, sizeof(double)); H->lin0 = calloc(G->tot * 7, sizeof(long));
+    H->pos0 = calloc(G->tot, sizeof(long)); H->num0 = calloc(G->tot, sizeof(int));
+    tk0 = malloc(sizeof(float) * nn); tk1 = calloc(nn, sizeof(float)); tk2 = malloc(sizeof(float) * nn);
+    gl[0] = gx; gl[1] = gy; gl[2] = gz;
+    MG.g[0] = gx; MG.g[1] = gy; MG.g[2] = gz; MG.n[0] = nx; MG.n[1] = ny; MG.n[2] = nz;
+    MG.size[0] = gx[nx - 1] - gx[0]; MG.size[1] = gy[ny - 1] - gy[0]; MG.size[2] = gz[nz - 1] - gz[0];
+    vel[0] = vx; vel[1] = vy; vel[2] = vz;
+
+    for (u = 0; u < nn; u++) { tk0[u] = tk[u]; if (tk[u] > maxtk) maxtk = tk[u]; if (tk[u] < mintk) mintk = tk[u]; }
+    /* right-hand side per level-0 node and the step limit (heaterr mode 0) */
+    for (m3 = 0; m3 < nz; m3++)
+        for (m1 = 0; m1 < nx; m1++)
+            for (m2 = 0; m2 < ny; m2++) {
+                long v3 = m3 * nxy + m1 * ny + m2;
+                double ival, rocpkf, xkf, ykf, zkf, x = 0, y = 0, z = 0, vxyz[3] = {0, 0, 0};
+                long p[8];
+                if (bct[v3]) continue;
+                xkf = HT_KF(gx, m1); ykf = HT_KF(gy, m2); zkf = HT_KF(gz, m3);
+                rocpkf = H->ro[v3] * H->cp[v3];
+                if (rocpkf < 2e+6) rocpkf = 2e+6;
+                ival = ht[v3];
+                if (adiabyn == 2 || frictyn) {
+                    p[0] = v3; p[1] = p[0] + 1; p[2] = p[0] + ny; p[3] = p[2] + 1;
+                    p[4] = p[0] + nxy; p[5] = p[4] + 1; p[6] = p[4] + ny; p[7] = p[6] + 1;
+                    x = (gx[m1] - gx[m1 - 1]) / 2.0 * xkf;
+                    y = (gy[m2] - gy[m2 - 1]) / 2.0 * ykf;
+                    z = (gz[m3] - gz[m3 - 1]) / 2.0 * zkf;
+                }
+                if (adiabyn) mv_velocity(&MG, vel, gx[m1], gy[m2], gz[m3], vxyz);
+                if (adiabyn == 2 && H->ro[v3] > 2e+3) {
+                    double dpdx = xkf * ((1.0 - y) * (1.0 - z) * (pr[p[2]] - pr[p[0]]) + y * (1.0 - z) * (pr[p[3]] - pr[p[1]]) +
+                                         (1.0 - y) * z * (pr[p[6]] - pr[p[4]]) + y * z * (pr[p[7]] - pr[p[5]]));
+                    double dpdy = ykf * ((1.0 - x) * (1.0 - z) * (pr[p[1]] - pr[p[0]]) + x * (1.0 - z) * (pr[p[3]] - pr[p[2]]) +
+                                         (1.0 - x) * z * (pr[p[5]] - pr[p[4]]) + x * z * (pr[p[7]] - pr[p[6]]));
+                    double dpdz = zkf * ((1.0 - x) * (1.0 - y) * (pr[p[4]] - pr[p[0]]) + x * (1.0 - y) * (pr[p[6]] - pr[p[2]]) +
+                                         (1.0 - x) * y * (pr[p[5]] - pr[p[1]]) + x * y * (pr[p[7]] - pr[p[3]]));
+                    ival += et[v3] * tk0[v3] * (vxyz[0] * dpdx + vxyz[1] * dpdy + vxyz[2] * dpdz);
+                }
+                if (adiabyn == 1 && H->ro[v3] > 2e+3)
+                    ival += et[v3] * tk0[v3] * H->ro[v3] * (vxyz[0] * GXK + vxyz[1] * GYK + vxyz[2] * GZK);
+                if (frictyn && H->ro[v3] > 2e+3) {
+                    const float *sxx = se[0], *syy = se[1], *szz = se[2], *sxy = se[3], *sxz = se[4], *syz = se[5];
+                    const float *exx = se[6], *eyy = se[7], *ezz = se[8], *exy = se[9], *exz = se[10], *eyz = se[11];
+                    double ev;
+#define HT_D(q) (sxx[p[q]] * exx[p[q]] + syy[p[q]] * eyy[p[q]] + szz[p[q]] * ezz[p[q]])
+                    ev = (1.0 - x) * (1.0 - y) * (1.0 - z) * HT_D(0);
+                    ev += (1.0 - x) * (y) * (1.0 - z) * HT_D(1);
+                    ev += (x) * (1.0 - y) * (1.0 - z) * HT_D(2);
+                    ev += (x) * (y) * (1.0 - z) * HT_D(3);
+                    ev += (1.0 - x) * (1.0 - y) * (z) * HT_D(4);
+                    ev += (1.0 - x) * (y) * (z) * HT_D(5);
+                    ev += (x) * (1.0 - y) * (z) * HT_D(6);
+                    ev += (x) * (y) * (z) * HT_D(7);
+#undef HT_D
+                    ev += 2.0 * ((1.0 - z) * (sxy[v3 - nxy] * exy[v3 - nxy]) + z * (sxy[v3] * exy[v3]));
+                    ev += 2.0 * ((1.0 - y) * (sxz[v3 - 1] * exz[v3 - 1]) + y * (sxz[v3] * exz[v3]));
+                    ev += 2.0 * ((1.0 - x) * (syz[v3 - ny] * eyz[v3 - ny]) + x * (syz[v3] * eyz[v3]));
+                    ival += ev;
+                }
+                tk1[v3] = (float)ival;
+                ival = fabs(ival / rocpkf);
+                if (ival > maxtkrate) maxtkrate = ival;
+            }
+    if (maxtkrate) tktimestep = maxtkstep / maxtkrate;
+    info[0] = tktimestep;
+    info[7] = maxtkrate;
+    if (timestep == 0 || tktimestep == 0) goto done;
+    for (u = 0; u < nn; u++) tk2[u] = tk[u];
+    for (li = 1; li <= multinumt; li++) ht_rocprestrict(H, li);
+    tktimesum = 0;
+    tktimesum0 = timestep;
+    do {
+        timestep = tktimesum0 < tktimestep ? tktimesum0 : tktimestep;
+        if (timestep > (tktimesum0 - tktimesum)) timestep = tktimesum0 - tktimesum;
+        for (u = 0; u < nn; u++) tk0[u] = tk[u];
+        for (u = 0; u < nn; u++) H->sol0[u] = tk[u];
+        nsub++;
+        /* rows of every level (heaterr mode 1, tbonderr) */
+        for (li = 0; li <= multinumt; li++) {
+            const double *g0 = G->g[li][0], *g1 = G->g[li][1], *g2 = G->g[li][2];
+            long lnx = G->nx[li], lny = G->ny[li], lnxy = lnx * lny;
+            for (m3 = 0; m3 < G->nz[li]; m3++)
+                for (m1 = 0; m1 < lnx; m1++)
+                    for (m2 = 0; m2 < lny; m2++) {
+                        long v[7], un[7];
+                        double ui[7], rhs, rocpkf, ival, xkf, ykf, zkf;
+                        v[3] = G->off[li] + m3 * lnxy + m1 * lny + m2;
+                        if (bct[v[3]]) {
+                            int b = bct[v[3]], k = 1;
+                            un[0] = v[3]; ui[0] = 1.0;
+                            if (bondn1[b]) { un[1] = bondn1[b] - 1; ui[1] = -bondv1[2 * b + 1]; k = 2; }
+                            ht_row(H, v[3], k, un, ui, bondv1[2 * b]);
+                            continue;
+                        }
+                        v[0] = v[3] - lnxy; v[1] = v[3] - lny; v[2] = v[3] - 1; v[4] = v[3] + 1; v[5] = v[3] + lny;
+                        v[6] = v[3] + lnxy;
+                        xkf = HT_KF(g0, m1); ykf = HT_KF(g1, m2); zkf = HT_KF(g2, m3);
+                        rocpkf = H->ro[v[3]] * H->cp[v[3]];
+                        if (rocpkf < 2e+6) rocpkf = 2e+6;
+                        rhs = li == 0 ? tk1[v[3]] + tk0[v[3]] / timestep * rocpkf : 0;
+                        ui[0] = rocpkf / timestep; un[0] = v[3];
+                        ival = (H->kt[v[1]] + H->kt[v[3]]) / 2.0 * xkf / (g0[m1] - g0[m1 - 1]);
+                        ui[1] = -ival; un[1] = v[1]; ui[0] += ival;
+                        ival = (H->kt[v[3]] + H->kt[v[5]]) / 2.0 * xkf / (g0[m1 + 1] - g0[m1]);
+                        ui[0] += ival; ui[2] = -ival; un[2] = v[5];
+                        ival = (H->kt[v[2]] + H->kt[v[3]]) / 2.0 * ykf / (g1[m2] - g1[m2 - 1]);
+                        ui[3] = -ival; un[3] = v[2]; ui[0] += ival;
+                        ival = (H->kt[v[3]] + H->kt[v[4]]) / 2.0 * ykf / (g1[m2 + 1] - g1[m2]);
+                        ui[0] += ival; ui[4] = -ival; un[4] = v[4];
+                        ival = (H->kt[v[0]] + H->kt[v[3]]) / 2.0 * zkf / (g2[m3] - g2[m3 - 1]);
+                        ui[5] = -ival; un[5] = v[0]; ui[0] += ival;
+                        ival = (H->kt[v[3]] + H->kt[v[6]]) / 2.0 * zkf / (g2[m3 + 1] - g2[m3]);
+                        ui[0] += ival; ui[6] = -ival; un[6] = v[6];
+                        ht_row(H, v[3], 7, un, ui, rhs);
+                    }
+        }
+        do {
+            int n1, n2;
+            double bsum = 0, hnum = 0;
+            for (n1 = 0; n1 < multicyct; n1++) {
+                if (multinumt > 0) {
+                    for (n2 = 0; n2 < multinumt; n2++) {
+                        ht_gausmatt(H, ipar[4 + n2], G->off[n2] + G->n[n2] - 1, G->off[n2]);
+                        ht_restrict(H, n2 + 1);
+                    }
+                    for (n2 = multinumt; n2 > 0; n2--) {
+                        ht_gausmatt(H, ipar[20 + n2], G->off[n2] + G->n[n2] - 1, G->off[n2]);
+                        ht_prolong(H, n2);
+                    }
+                } else
+                    ht_gausmatt(H, ipar[4], G->off[0] + G->n[0] - 1, G->off[0]);
+            }
+            ncyc++;
+            mintk = 1e30; maxtk = -1e30;
+            for (u = 0; u < nn; u++) {
+                tk[u] = (float)H->sol0[u];
+                if (tk[u] < mintk) mintk = tk[u];
+                if (tk[u] > maxtk) maxtk = tk[u];
+            }
+            /* error of the heat rows (heaterr mode 2) */
+            heatsum = 0;
+            for (m3 = 0; m3 < nz; m3++)
+                for (m1 = 0; m1 < nx; m1++)
+                    for (m2 = 0; m2 < ny; m2++) {
+                        long v[7];
+                        double rocpkf, ival, ival1, xkf, ykf, zkf;
+                        v[3] = m3 * nxy + m1 * ny + m2;
+                        if (bct[v[3]]) continue;
+                        v[0] = v[3] - nxy; v[1] = v[3] - ny; v[2] = v[3] - 1; v[4] = v[3] + 1; v[5] = v[3] + ny;
+                        v[6] = v[3] + nxy;
+                        xkf = HT_KF(gx, m1); ykf = HT_KF(gy, m2); zkf = HT_KF(gz, m3);
+                        rocpkf = H->ro[v[3]] * H->cp[v[3]];
+                        if (rocpkf < 2e+6) rocpkf = 2e+6;
+                        ival1 = (tk[v[3]] - tk0[v[3]]) / timestep;
+                        ival = (H->kt[v[1]] + H->kt[v[3]]) / 2.0 * xkf / (gx[m1] - gx[m1 - 1]) / rocpkf;
+                        ival1 += (tk[v[3]] - tk[v[1]]) * ival;
+                        ival = (H->kt[v[3]] + H->kt[v[5]]) / 2.0 * xkf / (gx[m1 + 1] - gx[m1]) / rocpkf;
+                        ival1 -= (tk[v[5]] - tk[v[3]]) * ival;
+                        ival = (H->kt[v[2]] + H->kt[v[3]]) / 2.0 * ykf / (gy[m2] - gy[m2 - 1]) / rocpkf;
+                        ival1 += (tk[v[3]] - tk[v[2]]) * ival;
+                        ival = (H->kt[v[3]] + H->kt[v[4]]) / 2.0 * ykf / (gy[m2 + 1] - gy[m2]) / rocpkf;
+                        ival1 -= (tk[v[4]] - tk[v[3]]) * ival;
+                        ival = (H->kt[v[0]] + H->kt[v[3]]) / 2.0 * zkf / (gz[m3] - gz[m3 - 1]) / rocpkf;
+                        ival1 += (tk[v[3]] - tk[v[0]]) * ival;
+                        ival = (H->kt[v[3]] + H->kt[v[6]]) / 2.0 * zkf / (gz[m3 + 1] - gz[m3]) / rocpkf;
+                        ival1 -= (tk[v[6]] - tk[v[3]]) * ival;
+                        ival1 -= tk1[v[3]] / rocpkf;
+                        ival1 *= timestep;
+                        heatsum += ival1 * ival1;
+                        hnum += 1.0;
+                    }
+            heatsum = pow(heatsum / hnum, 0.5);
+            (void)bsum;
+            if (heatsum > heatmin && maxcyc > 0 && ncyc >= maxcyc) { status = 1; break; }
+        } while (heatsum > heatmin);
+        tktimesum += timestep;
+        if (status) break;
+    } while (tktimesum < tktimesum0);
+    timestep = tktimesum0;
+    (void)gl;
+
+    /* marker temperatures (heat3mg.c:640-829) */
+    if (nmark > 0 && markk) {
+        double *S0 = calloc(nn, sizeof(double)), *S1 = calloc(nn, sizeof(double));
+        double xs = gx[nx - 1] - gx[0], ys = gy[ny - 1] - gy[0], zs = gz[nz - 1] - gz[0];
+        for (mk = 0; mk < nmark; mk++) {
+            long wn[11];
+            double wi[11], e2, e3;
+            int inside = markx[mk] > 0 && marky[mk] > 0 && markz[mk] > 0 && (double)markx[mk] < xs &&
+                         (double)marky[mk] < ys && (double)markz[mk] < zs;
+            int t = markt[mk];
+            if (!inside || t >= 100) continue;
+            /* tkcalc1 (mark3mg.c:1212-1282) */
+            {
+                double x = markx[mk], y = marky[mk], z = markz[mk], dx, dy, dz;
+                long a1 = serch(gx, nx, x), a2 = serch(gy, ny, y), a3 = serch(gz, nz, z), c3, c1, c2;
+                int n1 = 0;
+                wn[0] = a1; wn[1] = a2; wn[2] = a3;
+                wi[0] = dx = gx[a1 + 1] - gx[a1]; wi[1] = dy = gy[a2 + 1] - gy[a2]; wi[2] = dz = gz[a3 + 1] - gz[a3];
+                e2 = e3 = 0;
+                for (c3 = a3; c3 <= a3 + 1; c3++) {
+                    double ddz = 1.0 - fabs((gz[c3] - z) / dz);
+                    for (c1 = a1; c1 <= a1 + 1; c1++) {
+                        double ddx = 1.0 - fabs((gx[c1] - x) / dx);
+                        for (c2 = a2; c2 <= a2 + 1; c2++) {
+                            double ddy = 1.0 - fabs((gy[c2] - y) / dy), swt = ddx * ddy * ddz;
+                            long m4 = c3 * nxy + c1 * ny + c2;
+                            wi[3 + n1] = swt; wn[3 + n1] = m4;
+                            e2 += swt * tk[m4];
+                            e3 += swt * tk2[m4];
+                            n1++;
+                        }
+                    }
+                }
+            }
+            if (t >= 50) { markk[mk] = (float)e2; continue; }
+            if (markk[mk] <= 0) {
+                markk[mk] = (float)e3;
+                if (marky[mk] > zdeep && markk[mk] < tdeep) markk[mk] = tdeep;
+            }
+            if (heatdif) {
+                double mkt = 0, mcp = 0, mro = 0, mtk = tk[wn[3]], dtk, dtk1, rocpkf;
+                int n1;
+                for (n1 = 0; n1 < 8; n1++) {
+                    long m4 = wn[3 + n1];
+                    double w = wi[3 + n1];
+                    mkt += H->kt[m4] * w; mcp += H->cp[m4] * w; mro += H->ro[m4] * w;
+                    if (tk[m4] > mtk) mtk = tk[m4];
+                }
+                if ((wn[0] <= 0 || wn[0] >= nx - 2 || wn[1] <= 0 || wn[1] >= ny - 2 || wn[2] <= 0 || wn[2] >= nz - 2) &&
+                    (markk[mk] + e2 - e3) > mtk)
+                    markk[mk] = mtk - e2 + e3;
+                dtk = e3 - (double)markk[mk];
+                rocpkf = mro * mcp;
+                if (rocpkf < 2e+6) rocpkf = 2e+6;
+                dtk1 = -heatdif * mkt / rocpkf * 2.0 * (1.0 / wi[0] / wi[0] + 1.0 / wi[1] / wi[1] + 1.0 / wi[2] / wi[2]) * timestep;
+                if (dtk1 < -150.0) dtk1 = -150.0;
+                dtk1 = dtk * (1.0 - exp(dtk1));
+                markk[mk] += (float)dtk1;
+                for (n1 = 0; n1 < 8; n1++) { S1[wn[3 + n1]] += dtk1 * wi[3 + n1]; S0[wn[3 + n1]] += wi[3 + n1]; }
+            }
+            markk[mk] += (float)(e2 - e3);
+        }
+        if (heatdif) {
+            for (u = 0; u < nn; u++)
+                if (S0[u]) S1[u] /= S0[u];
+            for (mk = 0; mk < nmark; mk++) {
+                int inside = markx[mk] > 0 && marky[mk] > 0 && markz[mk] > 0 && (double)markx[mk] < xs &&
+                             (double)marky[mk] < ys && (double)markz[mk] < zs;
+                long a1, a2, a3, c1, c2, c3;
+                double x, y, z, dx, dy, dz;
+                if (!inside || markt[mk] >= 50) continue;
+                x = markx[mk]; y = marky[mk]; z = markz[mk];
+                a1 = serch(gx, nx, x); a2 = serch(gy, ny, y); a3 = serch(gz, nz, z);
+                dx = gx[a1 + 1] - gx[a1]; dy = gy[a2 + 1] - gy[a2]; dz = gz[a3 + 1] - gz[a3];
+                for (c3 = a3; c3 <= a3 + 1; c3++) {
+                    double ddz = 1.0 - fabs((gz[c3] - z) / dz);
+                    for (c1 = a1; c1 <= a1 + 1; c1++) {
+                        double ddx = 1.0 - fabs((gx[c1] - x) / dx);
+                        for (c2 = a2; c2 <= a2 + 1; c2++) {
+                            double ddy = 1.0 - fabs((gy[c2] - y) / dy);
+                            long m4 = c3 * nxy + c1 * ny + c2;
+                            if (S1[m4]) markk[mk] -= (float)(S1[m4] * (ddx * ddy * ddz));
+                        }
+                    }
+                }
+            }
+        }
+        free(S0); free(S1);
+    }
+done:
+    info[1] = (double)nsub; info[2] = (double)ncyc; info[3] = heatsum; info[4] = mintk; info[5] = maxtk;
+    info[6] = status;
+    free(H->kt); free(H->cp); free(H->ro); free(H->sol0); free(H->sol1); free(H->fre0); free(H->fre1);
+    free(H->val1); free(H->lin0); free(H->pos0); free(H->num0); free(tk0); free(tk1); free(tk2);
+    ht_grid_free(G);
+    return status;
+}

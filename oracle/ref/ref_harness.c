@@ -413,6 +413,14 @@ void p2ref_get_stress(float **out)
     for (q = 0; q < 12; q++) memcpy(out[q], g[q], sizeof(float) * (size_t)nodenum);
 }
 
+void p2ref_set_stress(float **in)
+{
+    float *g[12];
+    long q;
+    stress_globals(g);
+    for (q = 0; q < 12; q++) memcpy(g[q], in[q], sizeof(float) * (size_t)nodenum);
+}
+
 void p2ref_set_step(double max_step, double ts)
 {
     maxxystep = max_step;
@@ -685,4 +693,66 @@ void p2ref_smooth(int mgi, int am)
     mute();
     gausmat4(am, (mgp[mgi] + mgn[mgi]) * 4 - 1, mgp[mgi] * 4, mgi);
     unmute();
+}
+
+/* ---------------------------------------------------------------------- */
+/* titerate() (heat3mg.c:292) on the harness globals.  The active build's  */
+/* dynmemall() never allocates tk, tk0, tk1, tk2, cp, kt, ht and et        */
+/* (load3mg.c:2239-2334; mode.t3c sets tempmod 0), so the harness gives    */
+/* them storage for every level (rocprestrict writes the coarse levels).   */
+static void heat_arrays(void)
+{
+    size_t n = (size_t)nodenum * 2;
+    if (!tk) {
+        tk = calloc(n, sizeof(float)); tk0 = calloc(n, sizeof(float)); tk1 = calloc(n, sizeof(float));
+        tk2 = calloc(n, sizeof(float)); cp = calloc(n, sizeof(float)); kt = calloc(n, sizeof(float));
+        ht = calloc(n, sizeof(float)); et = calloc(n, sizeof(float));
+    }
+}
+
+/* T boundary rows: bondm[nodenum8 + u] for the nodes u of every level
+ * (in3mg.c:367-383); the rows themselves come with p2ref_set_bc. */
+void p2ref_set_tbc(const int *bt)
+{
+    long mcmax = mgp[multinum] + mgn[multinum], i;
+    for (i = 0; i < mcmax; i++) bondm[nodenum8 + i] = bt[i];
+}
+
+/* dpar: timestep, maxtkstep, HEATMIN, t0koef, t1koef, heatdif, tdeep, zdeep
+ * ipar: multinumt, multicyct, frictyn, adiabyn, multittt[0][0..15], multittt[1][0..15]
+ * Node fields are level 0; tk and markk are updated in place; out[0] is the
+ * step limit tktimestep the first loop found, out[1] the timestep after. */
+void p2ref_titerate(const double *dpar, const int *ipar, float *itk, const float *ikt, const float *icp,
+                    const float *iht, const float *iet, const double *ipr, float *imarkk, double *out)
+{
+    long i, keep;
+    int l;
+    heat_arrays();
+    memcpy(tk, itk, sizeof(float) * (size_t)nodenum);
+    memcpy(kt, ikt, sizeof(float) * (size_t)nodenum);
+    memcpy(cp, icp, sizeof(float) * (size_t)nodenum);
+    memcpy(ht, iht, sizeof(float) * (size_t)nodenum);
+    memcpy(et, iet, sizeof(float) * (size_t)nodenum);
+    if (ipr) memcpy(pr, ipr, sizeof(double) * (size_t)nodenum);
+    /* The second marker loop runs to marknum inclusive (heat3mg.c:666) and
+     * marknum0 == marknum (MRKNEW 1.0), so it reads one slot past the
+     * arrays: the harness's last marker is that slot, kept outside the box,
+     * and titerate sees marknum - 1 markers. */
+    keep = marknum;
+    if (keep < 1) return;
+    marknum = keep - 1;
+    markx[marknum] = -1.0f;
+    for (i = 0; i < marknum; i++) markk[i] = imarkk[i];
+    timestep = dpar[0]; maxtkstep = dpar[1]; HEATMIN = dpar[2]; t0koef = dpar[3]; t1koef = dpar[4];
+    heatdif = dpar[5]; tdeep = dpar[6]; zdeep = dpar[7];
+    multinumt = ipar[0]; multicyct = ipar[1]; frictyn = ipar[2]; adiabyn = ipar[3];
+    for (l = 0; l < 16; l++) { multittt[0][l] = ipar[4 + l]; multittt[1][l] = ipar[20 + l]; }
+    mute();
+    titerate(0);
+    unmute();
+    memcpy(itk, tk, sizeof(float) * (size_t)nodenum);
+    for (i = 0; i < marknum; i++) imarkk[i] = markk[i];
+    marknum = keep;
+    out[0] = 0;
+    out[1] = timestep;
 }

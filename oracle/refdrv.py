@@ -79,6 +79,9 @@ def _load(shim: bool = False) -> C.CDLL:
         lib.p2ref_get_val1_marke.argtypes = [_dp, _fp]
         lib.p2ref_get_timestep.restype = C.c_double
         lib.p2ref_get_markers.argtypes = [_fp] * 4
+        lib.p2ref_set_tbc.argtypes = [_ip]
+        lib.p2ref_set_stress.argtypes = [C.POINTER(C.c_void_p)]
+        lib.p2ref_titerate.argtypes = [_dp, _ip, _fp, _fp, _fp, _fp, _fp, C.c_void_p, _fp, _dp]
         lib.p2ref_lu_count.restype = C.c_int
         lib.p2ref_num_threads.restype = C.c_int
         _libs[path] = lib
@@ -301,3 +304,45 @@ class RefModel:
 
     def num_threads(self):
         return self.lib.p2ref_num_threads()
+
+
+    # -- heat equation ------------------------------------------------------
+    def set_tbc(self, bc):
+        """Boundary tables including the temperature rows (model.BCTables with
+        bondt): the Stokes rows and the shared row table, then the T section."""
+        lib = self.lib
+        if lib.p2ref_set_bc(np.ascontiguousarray(bc.bondm, np.int32), bc.bondnum,
+                            np.ascontiguousarray(bc.bondv1.reshape(-1), np.float32),
+                            np.ascontiguousarray(bc.bondn1, np.int32)):
+            raise RuntimeError("too many boundary equations for the reference (MAXBON)")
+        lib.p2ref_set_tbc(np.ascontiguousarray(bc.bondt, np.int32))
+
+    def titerate(self, hp: dict, multinumt: int, thermal, markk, pr=None):
+        """The reference's titerate(0) on the harness globals (markers from
+        set_markers, velocities from set_velocity, stresses from
+        fill_stress / update_stress).  The harness's last marker is the slot
+        the reference reads past the marker arrays and stays outside the box;
+        markk covers the others.  Returns (tk, markk)."""
+        dpar = np.array([hp[k] for k in ("timestep", "maxtkstep", "heatmin", "t0koef", "t1koef", "heatdif", "tdeep",
+                                         "zdeep")], np.float64)
+        ip = np.zeros(36, np.int32)
+        ip[0], ip[1], ip[2], ip[3] = multinumt, hp["multicyct"], hp["frictyn"], hp["adiabyn"]
+        ip[4:4 + len(hp["pre"])] = hp["pre"]
+        ip[20:20 + len(hp["post"])] = hp["post"]
+        tk = np.array(thermal.tk, np.float32, copy=True)
+        mk = np.zeros(self.m.markx.size, np.float32)
+        mk[:len(markk)] = markk
+        out = np.zeros(2, np.float64)
+        f = lambda a: np.ascontiguousarray(a, np.float32)
+        prp = None
+        if pr is not None:
+            prp = np.ascontiguousarray(pr, np.float64)
+        self.lib.p2ref_titerate(dpar, ip, tk, f(thermal.kt), f(thermal.cp), f(thermal.ht), f(thermal.et),
+                                None if prp is None else prp.ctypes.data_as(C.c_void_p), mk, out)
+        return tk, mk[:len(markk)]
+
+    def set_stress(self, arrays):
+        """sxx syy szz sxy sxz syz exx eyy ezz exy exz eyz (float, node layout)."""
+        arrs = [np.ascontiguousarray(a, np.float32) for a in arrays]
+        ptrs = (C.c_void_p * 12)(*[a.ctypes.data_as(C.c_void_p) for a in arrs])
+        self.lib.p2ref_set_stress(ptrs)

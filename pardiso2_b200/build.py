@@ -12,10 +12,14 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libp2cuda.so")
-SOURCES = ["p2_solver.cu", "p2_lu.cu", "p2_markers.cu", "p2_post.cu", "p2_capi.cu"]
-HEADERS = ["p2_internal.cuh", "p2_kernels.cuh", "p2_solver.h"]
+SOURCES = ["p2_solver.cu", "p2_lu.cu", "p2_markers.cu", "p2_post.cu", "p2_heat.cu", "p2_capi.cu"]
+HEADERS = ["p2_internal.cuh", "p2_kernels.cuh", "p2_interp.cuh", "p2_solver.h"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
               "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall", "--expt-relaxed-constexpr"]
+
+# the heat equation restates the reference's float/double expressions term
+# by term: no contraction into fused multiply-adds there
+EXTRA_FLAGS = {"p2_heat.cu": ["--fmad=false"]}
 
 
 def _nvcc() -> str:
@@ -40,7 +44,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     objs = []
     for src in SOURCES:
         obj = os.path.join(objdir, src.replace(".cu", ".o"))
-        cmd = [_nvcc(), *NVCC_FLAGS, "-c", os.path.join(CSRC, src), "-o", obj]
+        cmd = [_nvcc(), *NVCC_FLAGS, *EXTRA_FLAGS.get(src, []), "-c", os.path.join(CSRC, src), "-o", obj]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)

@@ -22,7 +22,8 @@ EXPORTED = ["p2_default_params", "p2_create", "p2_destroy", "p2_last_error", "p2
             "p2_upload_markers", "p2_ronurecalc_resident", "p2_get_nodes", "p2_debug_apply", "p2_debug_restrict",
             "p2_debug_prolong", "p2_debug_level_fields", "p2_debug_time_smoother", "p2_ronurecalc_noalloc", "p2_autotune",
             "p2_movemark", "p2_movemark_resident", "p2_get_markers", "p2_stress_strain",
-            "p2_stokes_solve_batch", "p2_movemark_strain", "p2_ronurecalc_powerlaw", "p2_effbulk_visc"]
+            "p2_stokes_solve_batch", "p2_movemark_strain", "p2_ronurecalc_powerlaw", "p2_effbulk_visc",
+            "p2_default_heat_params", "p2_heat_set_bc", "p2_titerate"]
 
 
 class Params(C.Structure):
@@ -63,6 +64,39 @@ class SolveInfo(C.Structure):
 
     def as_dict(self) -> Dict:
         return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class HeatParams(C.Structure):
+    _fields_ = [("maxtkstep", C.c_double), ("heatmin", C.c_double), ("t0koef", C.c_double), ("t1koef", C.c_double),
+                ("heatdif", C.c_double), ("tdeep", C.c_double), ("zdeep", C.c_double), ("multinumt", C.c_int),
+                ("multicyct", C.c_int), ("multittt", (C.c_int * 12) * 2), ("frictyn", C.c_int),
+                ("adiabyn", C.c_int), ("max_cycles", C.c_int)]
+
+
+class HeatInfo(C.Structure):
+    _fields_ = [("tktimestep", C.c_double), ("maxtkrate", C.c_double), ("substeps", C.c_int), ("cycles", C.c_int),
+                ("converged", C.c_int), ("heatsum", C.c_double), ("mintk", C.c_double), ("maxtk", C.c_double),
+                ("ms_total", C.c_double), ("kernels", C.c_longlong)]
+
+    def as_dict(self) -> Dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+def heat_params(**kw) -> HeatParams:
+    """p2_default_heat_params (mode.t3c values) with keyword overrides;
+    pre / post set multittt[0] / multittt[1] per level."""
+    hp = HeatParams()
+    load().p2_default_heat_params(C.byref(hp))
+    for k, v in kw.items():
+        if k in ("pre", "post"):
+            row = hp.multittt[0 if k == "pre" else 1]
+            for i, n in enumerate(v):
+                row[i] = int(n)
+        elif k in ("gx", "gy", "gz", "timestep"):
+            continue
+        else:
+            setattr(hp, k, v)
+    return hp
 
 
 class P2Error(RuntimeError):
@@ -118,6 +152,13 @@ def load() -> C.CDLL:
     L.p2_ronurecalc_powerlaw.restype = C.c_int
     L.p2_effbulk_visc.argtypes = [vp] + [_fp] * 17 + [C.POINTER(EffBulk)]
     L.p2_effbulk_visc.restype = C.c_int
+    L.p2_default_heat_params.argtypes = [C.POINTER(HeatParams)]
+    L.p2_default_heat_params.restype = None
+    L.p2_heat_set_bc.argtypes = [vp, _ip, C.c_long, _fp, _ip, C.c_long]
+    L.p2_heat_set_bc.restype = C.c_int
+    L.p2_titerate.argtypes = [vp, C.POINTER(HeatParams), C.c_double, _fp] + [_fp] * 5 + [C.c_void_p] * 5 + [
+        C.c_long] + [C.c_void_p] * 5 + [C.POINTER(HeatInfo)]
+    L.p2_titerate.restype = C.c_int
     for f in ("p2_movemark", "p2_movemark_resident", "p2_get_markers", "p2_stress_strain"):
         getattr(L, f).restype = C.c_int
     for f in ("p2_create", "p2_set_grid", "p2_set_bc", "p2_set_nodes", "p2_stokes_solve", "p2_stokes_solve_resident",
@@ -215,6 +256,48 @@ class Context:
 
     BULK_KEYS = ("ro", "nxx", "nxy", "nxz", "nyz", "exx", "eyy", "ezz", "exy", "exz", "eyz",
                  "sxx", "syy", "szz", "sxy", "sxz", "syz")
+
+    def heat_set_bc(self, bc, nodenum: int):
+        """Temperature boundary rows from model.BCTables (with bondt)."""
+        bm = bc.reference_bondm(nodenum)
+        bv = np.ascontiguousarray(np.asarray(bc.bondv1, np.float32).reshape(-1))
+        bn = np.ascontiguousarray(bc.bondn1, np.int32)
+        self._check(self.L.p2_heat_set_bc(self.h, bm, bm.size, bv, bn, bn.size - 1), "p2_heat_set_bc")
+
+    def titerate(self, hp: HeatParams, timestep: float, thermal, vel=None, pr=None, se=None, markers=None,
+                 markk=None):
+        """One titerate() step: returns (tk, markk, HeatInfo); the inputs are
+        not modified."""
+        tk = np.array(thermal.tk, np.float32, copy=True)
+        f = lambda a: np.ascontiguousarray(a, np.float32)
+        keep = []
+
+        def vp(a, dt):
+            if a is None:
+                return None
+            a = np.ascontiguousarray(a, dt)
+            keep.append(a)
+            return a.ctypes.data_as(C.c_void_p)
+
+        sep = None
+        if se is not None:
+            arrs = [np.ascontiguousarray(a, np.float32) for a in se]
+            keep.extend(arrs)
+            sep_arr = (C.c_void_p * 12)(*[a.ctypes.data_as(C.c_void_p) for a in arrs])
+            keep.append(sep_arr)
+            sep = C.cast(sep_arr, C.c_void_p)
+        nm = 0 if markers is None else len(markers[0])
+        mk = None if markk is None else np.array(markk, np.float32, copy=True)
+        info = HeatInfo()
+        v3 = vel if vel is not None else (None, None, None)
+        m4 = markers if markers is not None else (None, None, None, None)
+        self._check(self.L.p2_titerate(self.h, C.byref(hp), timestep, tk, f(thermal.kt), f(thermal.cp),
+                                       f(thermal.ro), f(thermal.ht), f(thermal.et),
+                                       *(vp(v, np.float32) for v in v3), vp(pr, np.float64), sep, nm,
+                                       *(vp(a, np.float32) for a in m4[:3]), vp(m4[3], np.int8),
+                                       None if mk is None else mk.ctypes.data_as(C.c_void_p), C.byref(info)),
+                    "p2_titerate")
+        return tk, mk, info
 
     def effbulk_visc(self, fields: Dict[str, np.ndarray]) -> EffBulk:
         """effbulkvisccalc(1) diagnostics of node fields (keys BULK_KEYS)."""

@@ -443,6 +443,53 @@ p2_status p2_effbulk_visc(p2_ctx *ctx, const float *ro, const float *nxx, const 
     });
 }
 
+void p2_default_heat_params(p2_heat_params *hp)
+{
+    if (!hp) return;
+    std::memset(hp, 0, sizeof(*hp));
+    // pardiso/mode.t3c:100-110 (T_ITERATIONS_PARAMETERS), 118-121, and the
+    // maxtkstep column of the SAVEFL lines (mode.t3c:9-13)
+    hp->heatmin = 1e-4;
+    hp->multinumt = 0;
+    hp->multicyct = 1;
+    hp->multittt[0][0] = 10;
+    hp->multittt[1][0] = 0;
+    hp->t0koef = 1.0;
+    hp->t1koef = 1.0;
+    hp->heatdif = 1.0;
+    hp->frictyn = 1;
+    hp->adiabyn = 1;
+    hp->tdeep = 3055;
+    hp->zdeep = 3800;
+    hp->maxtkstep = 25.0;
+    hp->max_cycles = 10000;
+}
+
+p2_status p2_heat_set_bc(p2_ctx *ctx, const int *bondm, long bondm_len, const float *bondv1, const int *bondn1,
+                         long bondnum)
+{
+    return guard(ctx, [&] {
+        if (!bondm || !bondv1 || !bondn1 || bondnum < 0) throw p2::Error(P2_ERR_ARG, "bad boundary tables");
+        P2_CUDA_TRY(cudaSetDevice(ctx->s->dev));
+        ctx->s->heat_set_bc(bondm, bondm_len, bondv1, bondn1, bondnum);
+    });
+}
+
+p2_status p2_titerate(p2_ctx *ctx, const p2_heat_params *hp, double timestep, float *tk, const float *kt,
+                      const float *cp, const float *ro, const float *ht, const float *et, const float *vx,
+                      const float *vy, const float *vz, const double *pr, const float *const *stress_strain,
+                      long marknum, const float *markx, const float *marky, const float *markz,
+                      const signed char *markt, float *markk, p2_heat_info *info)
+{
+    return guard(ctx, [&] {
+        if (!hp) throw p2::Error(P2_ERR_ARG, "null parameters");
+        P2_CUDA_TRY(cudaSetDevice(ctx->s->dev));
+        p2_heat_info r = ctx->s->titerate(*hp, timestep, tk, kt, cp, ro, ht, et, vx, vy, vz, pr, stress_strain,
+                                          marknum, markx, marky, markz, markt, markk);
+        if (info) *info = r;
+    });
+}
+
 p2_status p2_autotune(p2_ctx *ctx, int trial_iters, p2_tune_info *info)
 {
     return guard(ctx, [&] {

@@ -199,6 +199,9 @@ Solver::~Solver()
     marker_arena.release();
     move_arena.release();
     post_arena.release();
+    heat_arena.release();
+    heat_mk_arena.release();
+    heat = HeatState{};
     for (int i = 0; i < 8; i++) cudaEventDestroy(ev[i]);
     if (st) cudaStreamDestroy(st);
 }
@@ -256,6 +259,9 @@ void Solver::set_grid(long nx, long ny, long nz, const double *gx, const double 
     marker_arena.release();  // markers and their buffers belong to the previous grid
     move_arena.release();
     post_arena.release();
+    heat_arena.release();  // heat rows and fields belong to the previous grid
+    heat_mk_arena.release();
+    heat = HeatState{};
     for (int q = 0; q < 12; q++) post_out[q] = nullptr;
     post_partial = nullptr;
     post_range = nullptr;

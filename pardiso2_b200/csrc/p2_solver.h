@@ -66,6 +66,36 @@ struct RawFields {
     float *nu = nullptr, *ro = nullptr, *nxx = nullptr, *nxy = nullptr, *nxz = nullptr, *nyz = nullptr;
 };
 
+// heat equation state (p2_heat.cu)
+struct HeatLevel {
+    const double *g[3] = {nullptr, nullptr, nullptr};  // gridlines
+    int *bci = nullptr;                   // per node: 0 heat row, q + 1 boundary row q
+    int nbc = 0;
+    int *bu = nullptr, *bt = nullptr;     // boundary row: unknown, resolved heat-row target (-1 none)
+    double *bk = nullptr, *bconst = nullptr;
+    float *kt = nullptr, *cp = nullptr, *ro = nullptr;  // coarse levels (level 0: HeatState)
+    double *x = nullptr, *b = nullptr, *r = nullptr, *a = nullptr;
+    AxisMap map[3]{};                     // this level -> next coarser level
+};
+
+struct HeatState {
+    bool ready = false;
+    std::vector<HeatLevel> lv;
+    float *tk = nullptr, *tk0 = nullptr, *tk1 = nullptr, *tk2 = nullptr;
+    float *kt = nullptr, *cp = nullptr, *ro = nullptr, *ht = nullptr, *et = nullptr;
+    float *vel[3] = {nullptr, nullptr, nullptr};
+    double *pr = nullptr;
+    float *se[12] = {};
+    int nblk = 0;
+    double *partial = nullptr, *scal = nullptr, *S0 = nullptr, *S1 = nullptr;
+    double *host = nullptr;
+    std::shared_ptr<double> host_owner;
+    long mcap = 0;
+    float *mx = nullptr, *my = nullptr, *mz = nullptr, *mk = nullptr;
+    signed char *mt = nullptr;
+    long long kernels = 0;
+};
+
 class Solver {
   public:
     explicit Solver(int device);
@@ -93,6 +123,11 @@ class Solver {
                               const signed char *mt, double *val1, float *marke);
     void get_markers(float *mx, float *my, float *mz);
     void stress_strain(float *const s[6], float *const e[6], double vrange[6]);
+    void heat_set_bc(const int *bondm, long bondm_len, const float *bondv1, const int *bondn1, long bondnum);
+    p2_heat_info titerate(const p2_heat_params &hp, double timestep, float *tk, const float *kt, const float *cp,
+                          const float *ro, const float *ht, const float *et, const float *vx, const float *vy,
+                          const float *vz, const double *pr, const float *const *se, long nmark, const float *mx,
+                          const float *my, const float *mz, const signed char *mt, float *markk);
     void effbulk(const float *ro, const float *nxx, const float *nxy, const float *nxz, const float *nyz,
                  const float *const e[6], const float *const s[6], p2_effbulk *res);
 
@@ -177,7 +212,10 @@ class Solver {
     void ensure_move_buffers(long nmark);
     void velocity_f32();
 
-    DeviceArena arena, grid_arena, marker_arena, move_arena, post_arena;
+    void heat_smooth(int l, int sweeps, double t0koef);
+
+    DeviceArena arena, grid_arena, marker_arena, move_arena, post_arena, heat_arena, heat_mk_arena;
+    HeatState heat;
     std::array<GraphSlot, 2> graphs;
     LuGraph lu_graph;  // coarsest LU + inverse launch sequence
     int restart = 8;

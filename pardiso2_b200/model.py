@@ -22,7 +22,7 @@ from typing import List, Optional, Sequence, Tuple
 
 import numpy as np
 
-P, VX, VY, VZ = 0, 1, 2, 3
+P, VX, VY, VZ, T = 0, 1, 2, 3, 4
 
 
 # --------------------------------------------------------------------------
@@ -120,10 +120,24 @@ class BCTables:
     bondm: np.ndarray   # int32[4 * total_nodes]; 0 = no BC, else row in bondv1/bondn1
     bondv1: np.ndarray  # float32[bondnum + 1, 2] = (const, koef)
     bondn1: np.ndarray  # int32[bondnum + 1]; 1 + unknown index of the coupled unknown, 0 = none
+    # temperature rows per node of every level (bondm[8*nodenum + u] in the
+    # reference layout), None when the lines have no T entries
+    bondt: Optional[np.ndarray] = None
 
     @property
     def bondnum(self) -> int:
         return int(self.bondv1.shape[0] - 1)
+
+    def reference_bondm(self, nodenum: int) -> np.ndarray:
+        """bondm as the reference lays it out: the four Stokes unknowns per
+        node of every level from 0, the temperature rows from 8 * nodenum
+        (pardiso/load3mg.c:2250, in3mg.c:367-383)."""
+        total = self.bondm.size // 4
+        out = np.zeros(max(self.bondm.size, 8 * nodenum + total), dtype=np.int32)
+        out[:self.bondm.size] = self.bondm
+        if self.bondt is not None:
+            out[8 * nodenum:8 * nodenum + total] = self.bondt
+        return out
 
 
 def _map_index(m: int, nfine: int, nlev: int, s: int) -> int:
@@ -139,6 +153,7 @@ def _map_index(m: int, nfine: int, nlev: int, s: int) -> int:
 def build_bc_tables(lv: Levels, lines: Sequence[BCLine]) -> BCTables:
     nx, ny, nz = lv.mgx[0], lv.mgy[0], lv.mgz[0]
     bondm = np.zeros(4 * lv.total_nodes, dtype=np.int32)
+    bondt = np.zeros(lv.total_nodes, dtype=np.int32) if any(ln.var == T for ln in lines) else None
     consts: List[np.ndarray] = []
     koefs: List[np.ndarray] = []
     targets: List[np.ndarray] = []
@@ -177,11 +192,14 @@ def build_bc_tables(lv: Levels, lines: Sequence[BCLine]) -> BCTables:
             m6 = m4 + sz * lv.mgxy[l] + sx * lv.mgy[l] + sy
             cnt = m4.size
             ids = np.arange(bondnum + 1, bondnum + cnt + 1, dtype=np.int64)
-            bondm[m4 * 4 + ln.var] = ids
+            if ln.var == T:
+                bondt[m4] = ids   # in3mg.c:367-383: node index, target m6 + 1
+            else:
+                bondm[m4 * 4 + ln.var] = ids
             consts.append(np.full(cnt, ln.const, dtype=np.float32))
             if has_shift:
                 koefs.append(np.full(cnt, ln.koef, dtype=np.float32))
-                targets.append((m6 * 4 + ln.var + 1).astype(np.int64))
+                targets.append((m6 + 1 if ln.var == T else m6 * 4 + ln.var + 1).astype(np.int64))
             else:
                 koefs.append(np.zeros(cnt, dtype=np.float32))
                 targets.append(np.zeros(cnt, dtype=np.int64))
@@ -192,7 +210,59 @@ def build_bc_tables(lv: Levels, lines: Sequence[BCLine]) -> BCTables:
         bondv1[1:, 0] = np.concatenate(consts)
         bondv1[1:, 1] = np.concatenate(koefs)
         bondn1[1:] = np.concatenate(targets).astype(np.int32)
-    return BCTables(bondm, bondv1, bondn1)
+    return BCTables(bondm, bondv1, bondn1, bondt)
+
+
+def thermal_lines(t_low: float = 273.0, t_high: float = 1573.0) -> List[BCLine]:
+    """Temperature rows of a closed box: fixed temperatures on the z = 0 and
+    z = max planes, insulating x and y walls (the wall node copies its inner
+    neighbour, koef 1).  The x walls come after the y walls, so the vertical
+    edges copy a y-wall node (a chain of two rows); the z planes come last."""
+    return [BCLine(T, 0, -1, 0, 0, 0, -1, 0.0, 1.0, (0, +1, 0)),
+            BCLine(T, 0, -1, -1, -1, 0, -1, 0.0, 1.0, (0, -1, 0)),
+            BCLine(T, 0, 0, 0, -1, 0, -1, 0.0, 1.0, (+1, 0, 0)),
+            BCLine(T, -1, -1, 0, -1, 0, -1, 0.0, 1.0, (-1, 0, 0)),
+            BCLine(T, 0, -1, 0, -1, 0, 0, t_low),
+            BCLine(T, 0, -1, 0, -1, -1, -1, t_high)]
+
+
+@dataclasses.dataclass
+class Thermal:
+    """Level-0 node fields of the heat equation (float32, node layout)."""
+    tk: np.ndarray
+    kt: np.ndarray
+    cp: np.ndarray
+    ro: np.ndarray
+    ht: np.ndarray
+    et: np.ndarray
+
+
+def thermal_fields(model: "Model", seed: int = 7, t_low: float = 273.0, t_high: float = 1573.0,
+                   sphere_dt: float = 200.0, heat: Tuple[float, float] = (500.0, 2000.0)) -> Thermal:
+    """Synthetic thermal state on the model's grid: a linear profile in z
+    between the fixed planes plus a hot sphere, rock-like conductivity,
+    heat capacity, density (above 2000, where the adiabatic and shear
+    heating terms apply) and heat sources, with seeded +-5 % noise."""
+    nx, ny, nz = model.shape
+    Z, X, Y = np.meshgrid(model.gz, model.gx, model.gy, indexing="ij")
+    zs = (Z - model.gz[0]) / (model.gz[-1] - model.gz[0])
+    inside = ((X - 0.5) ** 2 + (Y - 0.5) ** 2 + (Z - 0.5) ** 2) < 0.2 ** 2
+    rng = np.random.Generator(np.random.PCG64(seed))
+    noise = lambda: 1.0 + 0.05 * (rng.random(Z.shape) - 0.5) * 2
+    tk = t_low + (t_high - t_low) * zs + sphere_dt * inside
+    kt = np.where(inside, 4.5, 2.5) * noise()
+    cp = 1000.0 * noise()
+    ro = np.where(inside, 3300.0, 3000.0) * noise()
+    ht = np.where(inside, heat[1], heat[0]) * noise()
+    et = 3e-5 * noise()
+    f = lambda a: np.ascontiguousarray(a.reshape(-1), np.float32)
+    return Thermal(f(tk), f(kt), f(cp), f(ro), f(ht), f(et))
+
+
+def with_thermal_bc(model: "Model", t_low: float = 273.0, t_high: float = 1573.0) -> BCTables:
+    """The model's free-slip tables with the thermal box rows added."""
+    return build_bc_tables(model.levels, free_slip_lines(model.params.pin, model.params.pinit)
+                           + thermal_lines(t_low, t_high))
 
 
 def free_slip_lines(pin: Tuple[int, int, int] = (2, 2, 2), pin_value: float = 0.0) -> List[BCLine]:

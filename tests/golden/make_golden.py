@@ -36,7 +36,10 @@ spheres21 node fields and the stresses / strain rates of its solution:
 and, in pl17.npz, ronurecalc with power-law rocks (viscalc,
 pardiso/mark3mg.c:1463-1498): markers, rock tables (n0, n1, ro, nu, mm),
 val1 per marker, the node fields, and marke after the call (the reference
-sets it to 1e-20 where it was 0 for the markers it interpolates).
+sets it to 1e-20 where it was 0 for the markers it interpolates),
+and, in heat17.npz, titerate (pardiso/heat3mg.c:292) per HEAT_VARIANTS on
+the heat_inputs of heat_model: tk_<variant>, markk_<variant> (in: markk_in)
+and info_<variant> (sub-steps, error checks, sub-step limit of the oracle).
   st_{sxx..syz, exx..eyz}           the post-solve stress / strain-rate pass
                                     of vpiterate (move3mgNew.c:2908-3038) on
                                     those velocities and sphere17's node
@@ -261,6 +264,67 @@ def make_pl_case():
     print("pl17 written", {k: np.asarray(v).shape for k, v in out.items()})
 
 
+HEAT_VARIANTS = {
+    # multinumt, multicyct, pre, post, frictyn, adiabyn, heatdif, timestep
+    "mg": dict(multinumt=1, multicyct=2, pre=[3, 0], post=[0, 8], frictyn=1, adiabyn=1, heatdif=1.0, timestep=1e5),
+    "single": dict(multinumt=0, multicyct=2, pre=[6], post=[0], frictyn=0, adiabyn=2, heatdif=0.0, timestep=3e4),
+}
+HEAT_COMMON = dict(maxtkstep=25.0, heatmin=5e-3, t0koef=1.0, t1koef=1.0, tdeep=1200.0, zdeep=0.6)
+
+
+def heat_inputs(m):
+    """Seeded inputs of the heat17 vectors (shared with the tests)."""
+    th = M.thermal_fields(m, seed=11)
+    n = m.nodenum
+    rng = np.random.Generator(np.random.PCG64(12))
+    f = lambda lo, hi: (lo + (hi - lo) * rng.random(n)).astype(np.float32)
+    vel = [f(-1.0, 1.0) for _ in range(3)]
+    se = [f(-100.0, 100.0) for _ in range(6)] + [f(-1.0, 1.0) for _ in range(6)]
+    pr = (1e5 * rng.random(n)).astype(np.float64)
+    mx, my, mz, mt = move_markers(m)
+    q = np.arange(mx.size - 1)
+    markk = np.where(q % 4 == 0, np.float32(0), np.float32(800) + np.float32(50) * (q % 13)).astype(np.float32)
+    return th, vel, se, pr, (mx, my, mz, mt), markk
+
+
+def heat_model():
+    m = M.sphere_model(17, 2, (1, 1, 1), seed=11, eta_sphere=1e3)
+    m.bc = M.with_thermal_bc(m)
+    return m
+
+
+def make_heat_case():
+    """heat17.npz: titerate() of the reference (pardiso/heat3mg.c:292) on a
+    17^3 box with fixed z planes and insulating walls, for HEAT_VARIANTS.
+    The harness's last marker is the slot the reference reads past the
+    marker arrays: the vectors cover the others."""
+    from oracle import oracle as O
+    from oracle import refdrv
+    m = heat_model()
+    th, vel, se, pr, mk, markk = heat_inputs(m)
+    mx, my, mz, mt = mk
+    r = refdrv.RefModel(m)
+    r.set_tbc(m.bc)
+    r.set_markers(mx, my, mz, mt)
+    r.set_nodes({"nu": np.ones_like(th.ro), "ro": th.ro, "nxx": np.ones_like(th.ro), "nxy": np.ones_like(th.ro),
+                 "nxz": np.ones_like(th.ro), "nyz": np.ones_like(th.ro)})
+    r.set_velocity(*vel)
+    r.set_stress(se)
+    out = {"markk_in": markk}
+    for name, v in HEAT_VARIANTS.items():
+        hp = dict(HEAT_COMMON, **v, gx=m.params.gx, gy=m.params.gy, gz=m.params.gz, max_cycles=200)
+        # the oracle first, with a cap: the reference itself loops until heatmin
+        _, _, info = O.titerate(m.gx, m.gy, m.gz, v["multinumt"], m.bc.bondt, m.bc.bondv1, m.bc.bondn1, hp, th,
+                                vel=vel, pr=pr, se=se, markers=(mx[:-1], my[:-1], mz[:-1], mt[:-1]), markk=markk)
+        assert not info["capped"], (name, info)
+        tk, mko = r.titerate(hp, v["multinumt"], th, markk, pr=pr)
+        out["tk_" + name] = tk
+        out["markk_" + name] = mko
+        out["info_" + name] = np.array([info["substeps"], info["cycles"], info["tktimestep"]])
+    np.savez_compressed(os.path.join(HERE, "heat17.npz"), **out)
+    print("heat17 written", {k: np.asarray(v).shape for k, v in out.items()})
+
+
 if __name__ == "__main__":
     # the reference keeps its state in globals: one case per process
     if len(sys.argv) > 1:
@@ -270,9 +334,11 @@ if __name__ == "__main__":
             make_pl_case()
         elif sys.argv[1] == "bulk21":
             make_bulk_case()
+        elif sys.argv[1] == "heat17":
+            make_heat_case()
         else:
             make_case(sys.argv[1], CASES[sys.argv[1]])
     else:
         import subprocess
-        for c in list(CASES) + ["move17", "pl17", "bulk21"]:
+        for c in list(CASES) + ["move17", "pl17", "bulk21", "heat17"]:
             subprocess.run([sys.executable, os.path.abspath(__file__), c], check=True)

@@ -239,3 +239,35 @@ def test_oracle_effbulk_vs_reference_golden(oracle_mod):
     mine = bulk_line_values(out, counts)
     assert np.all(np.abs(mine - ref) <= 6e-7 * np.abs(ref)), np.max(np.abs(mine - ref) / np.abs(ref))
     assert counts[2] > 1000 and counts[1] > 1000
+
+
+# -- heat equation (titerate) -------------------------------------------------
+def _heat_case():
+    from tests.golden.make_golden import HEAT_COMMON, HEAT_VARIANTS, heat_inputs, heat_model
+    g = np.load(os.path.join(GOLDEN, "heat17.npz"))
+    m = heat_model()
+    return m, g, heat_inputs(m), HEAT_COMMON, HEAT_VARIANTS
+
+
+@pytest.mark.parametrize("variant", ["mg", "single"])
+def test_oracle_titerate_vs_reference_golden(oracle_mod, variant):
+    """heat3mg.c:292-829 restated (lexicographic Gauss-Seidel, the same
+    V-cycle, sub-steps and marker update): the temperatures and marker
+    temperatures of the reference's own titerate() bit for bit, and the same
+    number of sub-steps and error checks."""
+    m, g, (th, vel, se, pr, mk, markk), common, variants = _heat_case()
+    np.testing.assert_array_equal(g["markk_in"], markk)
+    v = variants[variant]
+    hp = dict(common, **v, gx=m.params.gx, gy=m.params.gy, gz=m.params.gz, max_cycles=200)
+    mx, my, mz, mt = mk
+    tk, mko, info = oracle_mod.titerate(m.gx, m.gy, m.gz, v["multinumt"], m.bc.bondt, m.bc.bondv1, m.bc.bondn1, hp,
+                                        th, vel=vel, pr=pr, se=se, markers=(mx[:-1], my[:-1], mz[:-1], mt[:-1]),
+                                        markk=markk)
+    assert not info["capped"]
+    assert info["substeps"] == int(g["info_" + variant][0]) and info["substeps"] > 1
+    np.testing.assert_array_equal(tk, g["tk_" + variant])
+    np.testing.assert_array_equal(mko, g["markk_" + variant])
+    # the step moved temperatures and every marker class
+    assert np.abs(tk - th.tk).max() > 10
+    assert np.abs(mko - markk)[mt[:-1] < 50].max() > 1
+    assert np.abs(mko - markk)[(mt[:-1] >= 50) & (mt[:-1] < 100)].max() > 1
