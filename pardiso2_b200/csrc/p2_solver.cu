@@ -66,7 +66,11 @@ void *DeviceArena::alloc(size_t bytes)
         throw Error(P2_ERR_NOMEM, "cudaMalloc of " + std::to_string(bytes) + " bytes failed");
     }
     ptrs.push_back(p);
-    P2_CUDA_TRY(cudaMemset(p, 0, bytes));
+    // Zero-fill on the legacy stream and wait for it: the library's own
+    // streams are non-blocking, so without the wait a fill still in flight
+    // could land after a copy that the caller queues on its stream.
+    P2_CUDA_TRY(cudaMemsetAsync(p, 0, bytes, 0));
+    P2_CUDA_TRY(cudaStreamSynchronize(0));
     return p;
 }
 void DeviceArena::release()
@@ -1293,7 +1297,8 @@ struct TmpVec {
     explicit TmpVec(int n)
     {
         P2_CUDA_TRY(cudaMalloc(&base, sizeof(double) * 4 * (size_t)n));
-        P2_CUDA_TRY(cudaMemset(base, 0, sizeof(double) * 4 * (size_t)n));
+        P2_CUDA_TRY(cudaMemsetAsync(base, 0, sizeof(double) * 4 * (size_t)n, 0));
+        P2_CUDA_TRY(cudaStreamSynchronize(0));  // ordered before copies on the non-blocking stream
         for (int c = 0; c < 4; c++) v.c[c] = base + (size_t)c * n;
         v.n = n;
     }
