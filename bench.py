@@ -250,6 +250,59 @@ def shard_instances(sizes, world):
     return [sorted(p) for p in parts]
 
 
+def heat_leg(prob, m, args, with_cpu: bool):
+    """One thermal step (titerate) on the workload's grid through the public
+    API: fixed z planes and insulating walls on every level, seeded thermal
+    fields (thermal_fields), the resident solution's velocities (adiabatic
+    heating) and its stresses / strain rates (shear heating), the workload's
+    markers with types 0/1 (diffused) and 70 (reset to the node
+    temperature).  All levels of the grid, 3 smoothing sweeps down and up,
+    10 on the coarsest; a 2000 s step (about 2.5 diffusion times of a cell of
+    the 65^3 unit box) in sub-steps of at most 25 K, errors below 1e-3 K."""
+    import numpy as np
+    from pardiso2_b200 import capi
+    from pardiso2_b200 import model as M
+    n = m.nodenum
+    bc = M.with_thermal_bc(m)
+    prob.ctx.heat_set_bc(bc, n)
+    th = M.thermal_fields(m, seed=31, heat=(2e4, 8e4))
+    sol = prob.ctx.solution(n)
+    vel = [np.ascontiguousarray(sol[k], np.float32) for k in ("vx", "vy", "vz")]
+    st = {k: np.zeros(n, np.float32) for k in capi.Context.STRESS_KEYS}
+    prob.ctx.stress_strain(st)
+    se = [st[k] for k in capi.Context.STRESS_KEYS]
+    nt = m.multinum
+    pre = [3] * nt + [0]
+    post = [0] + [3] * (nt - 1) + [10]
+    hp = capi.heat_params(multinumt=nt, multicyct=1, pre=pre, post=post, heatmin=1e-3, max_cycles=200)
+    q = np.arange(m.markx.size)
+    mt = np.where(q % 9 == 4, 70, m.markt).astype(np.int8)
+    markk = np.where(q % 3 == 0, 0.0, 900.0).astype(np.float32)
+    markers = (m.markx, m.marky, m.markz, mt)
+    dt = 2000.0
+    for _ in range(max(1, args.warmup)):
+        prob.ctx.titerate(hp, dt, th, vel=vel, se=se, markers=markers, markk=markk)
+    runs = [prob.ctx.titerate(hp, dt, th, vel=vel, se=se, markers=markers, markk=markk)[2] for _ in range(args.steps)]
+    info = runs[-1]
+    out = {"ms": statistics.mean(r.ms_total for r in runs), "nodes": n, "markers": int(q.size), "levels": nt + 1,
+           "substeps": info.substeps, "error_checks": info.cycles, "heatsum": info.heatsum, "heatmin": hp.heatmin,
+           "converged": bool(info.converged), "launches": int(info.kernels),
+           "timing": "CUDA events around the call, host<->device copies of the fields and markers included"}
+    if with_cpu:
+        sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__))))
+        from oracle import oracle as O
+        hpd = dict(timestep=dt, maxtkstep=hp.maxtkstep, heatmin=hp.heatmin, t0koef=1.0, t1koef=1.0, heatdif=1.0,
+                   tdeep=hp.tdeep, zdeep=hp.zdeep, gx=m.params.gx, gy=m.params.gy, gz=m.params.gz, multicyct=1,
+                   frictyn=1, adiabyn=1, max_cycles=200, pre=pre, post=post)
+        t0 = time.perf_counter()
+        _, _, oi = O.titerate(m.gx, m.gy, m.gz, nt, bc.bondt, bc.bondv1, bc.bondn1, hpd, th, vel=vel, se=se,
+                              markers=markers, markk=markk)
+        out["cpu_baseline"] = {"value": (time.perf_counter() - t0) * 1e3, "unit": "ms", "cores": 1, "kind": "port",
+                               "sample": "the same step with the oracle port (lexicographic Gauss-Seidel, %d error "
+                                         "checks)" % oi["cycles"]}
+    return out
+
+
 def run_batch(args, rank, world, local, dist):
     """The batched workload: this rank's share of the 64 instances, solved
     one after another and then all at once (p2_stokes_solve_batch)."""
@@ -531,6 +584,7 @@ def main():
     line["movemark"] = {"ms": move_ms, "markers": nmark, "markmod": "RK4", "dt": dt_move,
                         "achieved_GBps": move_bytes / (move_ms * 1e-3) / 1e9, "bytes_per_step": move_bytes,
                         "launches": 2}
+    line["heat"] = heat_leg(prob, m, args, rank == 0 and world == 1 and not args.no_cpu_baseline and args.config <= 2)
     line["autotune"] = tune.as_dict()
     if rank == 0 and world == 1 and not args.no_cpu_baseline and args.config <= 2:
         threads = os.cpu_count() or 1

@@ -54,8 +54,12 @@ void PARDISO(void **pt, int *maxfct, int *mnum, int *mtype, int *phase, int *n,
 #undef effbulkvisccalc
 #endif
 #include "gaus3mg_SerieMG.c"
+#ifdef P2REF_SHIM
+#define titerate titerate_cpu
+#endif
 #include "heat3mg.c"
 #ifdef P2REF_SHIM
+#undef titerate
 #include "move3mg_cuda.c"
 #endif
 

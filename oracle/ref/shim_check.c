@@ -1,7 +1,8 @@
 /* Compile check (test infrastructure): the reference's unity build
- * (pardiso/i3mg.c:1-19, without its main) with vpiterate(), ronurecalc() and movemark()
- * taken from pardiso2_b200/csrc/move3mg_cuda.c: the CPU functions are renamed
- * by two macros around their files and the shim is included after them.
+ * (pardiso/i3mg.c:1-19, without its main) with vpiterate(), ronurecalc(),
+ * movemark(), effbulkvisccalc() and titerate() taken from
+ * pardiso2_b200/csrc/move3mg_cuda.c: the CPU functions are renamed by macros
+ * around their files and the shim is included after them.
  * Built with -c only: it proves the shim compiles against the reference's
  * globals and the p2cuda.h declarations. */
 #include <stdio.h>
@@ -25,5 +26,7 @@
 #undef movemark
 #undef effbulkvisccalc
 #include "gaus3mg_SerieMG.c"
+#define titerate titerate_cpu
 #include "heat3mg.c"
+#undef titerate
 #include "move3mg_cuda.c"

@@ -1,6 +1,6 @@
 /*
- * move3mg_cuda.c -- the reference's vpiterate(), ronurecalc(), movemark()
- * and effbulkvisccalc() on top of libp2cuda.so (include/p2cuda.h).
+ * move3mg_cuda.c -- the reference's vpiterate(), ronurecalc(), movemark(),
+ * effbulkvisccalc() and titerate() on top of libp2cuda.so (include/p2cuda.h).
  *
  * This file is compiled inside the reference's unity build (pardiso/i3mg.c
  * includes head3mg.c, load3mg.c, move3mgNew.c, mark3mg.c, ... into one
@@ -19,6 +19,10 @@
  *     #undef ronurecalc
  *     #undef movemark
  *     #undef effbulkvisccalc
+ *     #include "gaus3mg_SerieMG.c"
+ *     #define titerate titerate_cpu        -- pardiso/heat3mg.c:292
+ *     #include "heat3mg.c"
+ *     #undef titerate
  *     #include "move3mg_cuda.c"
  *
  * Inputs read: xnumx, ynumy, znumz, gx, gy, gz, x/y/zperiodic, multinum,
@@ -36,6 +40,10 @@
  * markz and the markk
  * reset of markers that leave the box, val1 (strain-rate invariant per
  * marker) and marke (brittle strain) by movemark.
+ * titerate reads tk, kt, cp, ro, ht, et, the T rows of bondm (from
+ * 8 * nodenum), HEATMIN, multinumt, multicyct, multittt, t0koef, t1koef,
+ * heatdif, frictyn, adiabyn, tdeep, zdeep, maxtkstep, timestep, GX/GY/GZKOEF,
+ * vx, vy, vz, pr, sxx..syz, exx..eyz and the markers, and writes tk and markk.
  *
  * Errors follow the reference's convention: a message on stdout and exit().
  * The device is 0, or the value of the environment variable P2CUDA_DEVICE.
@@ -236,4 +244,58 @@ void effbulkvisccalc(int nodemark)
             r.incl[0], r.incl[1], r.incl[2], r.incl[3], r.incl[4], r.incl[5], r.incl[6], r.incl[7], r.incl[8],
             r.incl[9], r.incl[10], r.incl[11], r.siin, r.eiin, r.eiivp, r.hsn, r.nubulk2, r.nubulk3, r.nubulk4);
     fclose(f);
+}
+
+/* pardiso/heat3mg.c:292 (prototype pardiso/head3mg.c:386): one thermal step
+ * of timestep seconds on tk and on the marker temperatures markk (markers are
+ * skipped when markk has no storage).  The coarse-level kt, cp, ro and the
+ * work arrays tk0, tk1, tk2 stay on the device.  The reference repeats its
+ * V-cycles until the error is below HEATMIN; the library stops after 10000
+ * error checks per sub-step and the shim reports it. */
+static long p2s_heat_nodes = -1;
+
+void titerate(int m0)
+{
+    p2_status st;
+    p2_heat_params hp;
+    p2_heat_info info;
+    const float *se[12];
+    int l;
+    p2s_setup();
+    if (p2s_heat_nodes != p2s_grid_nodes) {
+        st = p2_heat_set_bc(p2s_ctx, bondm, nodenum8 + mgp[multinum] + mgn[multinum], &bondv1[0][0], bondn1,
+                            bondnum);
+        if (st != P2_OK) p2s_fail("p2_heat_set_bc", st);
+        p2s_heat_nodes = p2s_grid_nodes;
+    }
+    p2_default_heat_params(&hp);
+    hp.maxtkstep = maxtkstep;
+    hp.heatmin = HEATMIN;
+    hp.t0koef = t0koef;
+    hp.t1koef = t1koef;
+    hp.heatdif = heatdif;
+    hp.tdeep = tdeep;
+    hp.zdeep = zdeep;
+    hp.multinumt = multinumt;
+    hp.multicyct = multicyct;
+    for (l = 0; l < P2_MAX_LEVELS; l++) {
+        hp.multittt[0][l] = l <= multinumt ? multittt[0][l] : 0;
+        hp.multittt[1][l] = l <= multinumt ? multittt[1][l] : 0;
+    }
+    hp.frictyn = frictyn;
+    hp.adiabyn = adiabyn;
+    hp.max_cycles = 0;
+    se[0] = sxx; se[1] = syy; se[2] = szz; se[3] = sxy; se[4] = sxz; se[5] = syz;
+    se[6] = exx; se[7] = eyy; se[8] = ezz; se[9] = exy; se[10] = exz; se[11] = eyz;
+    st = p2_titerate(p2s_ctx, &hp, timestep, tk, kt, cp, ro, ht, et, vx, vy, vz, pr, se, markk ? marknum : 0, markx,
+                     marky, markz, (const signed char *)markt, markk, &info);
+    if (st != P2_OK) p2s_fail("p2_titerate", st);
+    if (!info.converged)
+        printf("\n T ITERATIONS STOPPED: %d checks, err = %e > HEATMIN = %e\n", info.cycles, info.heatsum, HEATMIN);
+    if (printmod) {
+        printf("\n KRUG %2d \n", m0 + 1);
+        printf("THERMAL STEP = %e YEARS    SUBSTEPS = %d\n", timestep / 3.15576e+7, info.substeps);
+        printf("TEMPERATURE    : min = %e max = %e \n", info.mintk, info.maxtk);
+        printf("TERMAL EQUATION: err = %e \n", info.heatsum);
+    }
 }
