@@ -327,9 +327,10 @@ __global__ void __launch_bounds__(256) k_heat_prolong(HeatLv F, HeatLv C, AxisMa
 // tk = (float) x on level 0, the error of every heat row (heaterr mode 2,
 // times dt) squared, and the temperature range: per-block partials
 // [sum, count, min, max].
-__global__ void __launch_bounds__(256) k_heat_error(HeatLv L, double dt, float *tk, const float *tk0, const float *tk1,
-                                                    double *partial)
+__global__ void __launch_bounds__(256) k_heat_error(HeatLv L, const double *dtp, float *tk, const float *tk0,
+                                                    const float *tk1, double *partial)
 {
+    const double dt = *dtp;
     const long u = (long)blockIdx.x * blockDim.x + threadIdx.x;
     double e2 = 0, cnt = 0, tmin = 1e30, tmax = -1e30;
     if (u < L.n) {
@@ -661,7 +662,7 @@ void Solver::heat_set_bc(const int *bondm, long bondm_len, const float *bondv1, 
     heat.scal = (double *)heat_arena.alloc(sizeof(double) * 8);
     heat.S0 = (double *)heat_arena.alloc(sizeof(double) * n0);
     heat.S1 = (double *)heat_arena.alloc(sizeof(double) * n0);
-    P2_CUDA_TRY(cudaMallocHost((void **)&heat.host, sizeof(double) * 8));
+    P2_CUDA_TRY(cudaMallocHost((void **)&heat.host, sizeof(double) * 8));  // [0..3] error, range; [4] sub-step
     heat.host_owner.reset(heat.host, [](double *p) { cudaFreeHost(p); });
     P2_CUDA_TRY(cudaStreamSynchronize(st));
     heat.ready = true;
@@ -695,6 +696,37 @@ void Solver::heat_smooth(int l, int sweeps, double t0koef)
         }
     k_heat_resid<<<hb(V.n), 256, 0, st>>>(V, B, l == 0);
     heat.kernels++;
+}
+
+// multicyct V-cycles on levels 0..multinumt (heat3mg.c:459-497), then the
+// level-0 error and temperature range into heat.scal[0..3]
+void Solver::heat_batch(const p2_heat_params &hp)
+{
+    const int nt = hp.multinumt;
+    for (int c = 0; c < hp.multicyct; c++) {
+        if (nt > 0) {
+            for (int l = 0; l < nt; l++) {
+                heat_smooth(l, hp.multittt[0][l], hp.t0koef);
+                const HeatLv F = heat_view(L[l], heat.lv[l], heat, l), C = heat_view(L[l + 1], heat.lv[l + 1], heat, l + 1);
+                const AxisMap *m = heat.lv[l].map;
+                k_heat_restrict<<<hb(C.n), 256, 0, st>>>(F, C, m[0], m[1], m[2]);
+                heat.kernels++;
+            }
+            for (int l = nt; l > 0; l--) {
+                heat_smooth(l, hp.multittt[1][l], hp.t0koef);
+                const HeatLv F = heat_view(L[l - 1], heat.lv[l - 1], heat, l - 1), C = heat_view(L[l], heat.lv[l], heat, l);
+                const AxisMap *m = heat.lv[l - 1].map;
+                k_heat_prolong<<<hb(F.n), 256, 0, st>>>(F, C, m[0], m[1], m[2], hp.t1koef);
+                heat.kernels++;
+            }
+        } else {
+            heat_smooth(0, hp.multittt[0][0], hp.t0koef);
+        }
+    }
+    const HeatLv V0 = heat_view(L[0], heat.lv[0], heat, 0);
+    k_heat_error<<<heat.nblk, 256, 0, st>>>(V0, heat.scal + 4, heat.tk, heat.tk0, heat.tk1, heat.partial);
+    k_heat_error_final<<<1, 1024, 0, st>>>(heat.partial, heat.nblk, heat.scal);
+    heat.kernels += 2;
 }
 
 p2_heat_info Solver::titerate(const p2_heat_params &hp, double timestep, float *tk, const float *kt, const float *cp,
@@ -780,6 +812,11 @@ p2_heat_info Solver::titerate(const p2_heat_params &hp, double timestep, float *
         heat.kernels++;
     }
     const int maxcyc = hp.max_cycles > 0 ? hp.max_cycles : 10000;
+    struct Batch {
+        cudaGraphExec_t exec = nullptr;
+        long long kernels = 0;
+        ~Batch() { if (exec) cudaGraphExecDestroy(exec); }
+    } batch;
     double tktimesum = 0, tktimesum0 = timestep, heatsum = 0;
     do {
         double dt = tktimesum0 < tktimestep ? tktimesum0 : tktimestep;
@@ -793,31 +830,27 @@ p2_heat_info Solver::titerate(const p2_heat_params &hp, double timestep, float *
             k_heat_rows<<<hb(V.n), 256, 0, st>>>(V, dt, l ? nullptr : heat.tk0, heat.tk1);
             heat.kernels++;
         }
+        // the sub-step size for the error kernel (device memory, so that one
+        // captured batch serves every sub-step)
+        heat.host[4] = dt;
+        P2_CUDA_TRY(cudaMemcpyAsync(heat.scal + 4, heat.host + 4, sizeof(double), cudaMemcpyHostToDevice, st));
+        if (!batch.exec) {
+            // multicyct V-cycles and the error reduction as one graph
+            const long long k0 = heat.kernels;
+            cudaGraph_t g = nullptr;
+            P2_CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+            heat_batch(hp);
+            P2_CUDA_TRY(cudaStreamEndCapture(st, &g));
+            const cudaError_t e = cudaGraphInstantiate(&batch.exec, g, 0);
+            cudaGraphDestroy(g);
+            P2_CUDA_TRY(e);
+            batch.kernels = heat.kernels - k0;
+            heat.kernels = k0;
+        }
         int cyc = 0;
         do {
-            for (int c = 0; c < hp.multicyct; c++) {
-                if (nt > 0) {
-                    for (int l = 0; l < nt; l++) {
-                        heat_smooth(l, hp.multittt[0][l], hp.t0koef);
-                        const HeatLv F = heat_view(L[l], heat.lv[l], heat, l), C = heat_view(L[l + 1], heat.lv[l + 1], heat, l + 1);
-                        const AxisMap *m = heat.lv[l].map;
-                        k_heat_restrict<<<hb(C.n), 256, 0, st>>>(F, C, m[0], m[1], m[2]);
-                        heat.kernels++;
-                    }
-                    for (int l = nt; l > 0; l--) {
-                        heat_smooth(l, hp.multittt[1][l], hp.t0koef);
-                        const HeatLv F = heat_view(L[l - 1], heat.lv[l - 1], heat, l - 1), C = heat_view(L[l], heat.lv[l], heat, l);
-                        const AxisMap *m = heat.lv[l - 1].map;
-                        k_heat_prolong<<<hb(F.n), 256, 0, st>>>(F, C, m[0], m[1], m[2], hp.t1koef);
-                        heat.kernels++;
-                    }
-                } else {
-                    heat_smooth(0, hp.multittt[0][0], hp.t0koef);
-                }
-            }
-            k_heat_error<<<heat.nblk, 256, 0, st>>>(V0, dt, heat.tk, heat.tk0, heat.tk1, heat.partial);
-            k_heat_error_final<<<1, 1024, 0, st>>>(heat.partial, heat.nblk, heat.scal);
-            heat.kernels += 2;
+            P2_CUDA_TRY(cudaGraphLaunch(batch.exec, st));
+            heat.kernels += batch.kernels;
             P2_CUDA_TRY(cudaMemcpyAsync(heat.host, heat.scal, sizeof(double) * 4, cudaMemcpyDeviceToHost, st));
             P2_CUDA_TRY(cudaStreamSynchronize(st));
             P2_CUDA_TRY(cudaGetLastError());

@@ -213,6 +213,7 @@ class Solver {
     void velocity_f32();
 
     void heat_smooth(int l, int sweeps, double t0koef);
+    void heat_batch(const p2_heat_params &hp);
 
     DeviceArena arena, grid_arena, marker_arena, move_arena, post_arena, heat_arena, heat_mk_arena;
     HeatState heat;
