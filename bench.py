@@ -77,6 +77,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--solve-only", action="store_true",
                     help="warm-up + timed resident solves + smoother timing only (profiling runs)")
+    ap.add_argument("--heat-only", action="store_true",
+                    help="only the heat-equation step on the workload's grid, with seeded velocities and "
+                         "stresses instead of a solve (profiling runs)")
     ap.add_argument("--restart", type=int, default=16, help="GCR restart length")
     ap.add_argument("--tune-iters", type=int, default=12,
                     help="outer iterations per autotuner trial (run once, before the timed region); 0 = no tuning")
@@ -250,7 +253,7 @@ def shard_instances(sizes, world):
     return [sorted(p) for p in parts]
 
 
-def heat_leg(prob, m, args, with_cpu: bool):
+def heat_leg(prob, m, args, with_cpu: bool, synthetic: bool = False):
     """One thermal step (titerate) on the workload's grid through the public
     API: fixed z planes and insulating walls on every level, seeded thermal
     fields (thermal_fields), the resident solution's velocities (adiabatic
@@ -266,11 +269,16 @@ def heat_leg(prob, m, args, with_cpu: bool):
     bc = M.with_thermal_bc(m)
     prob.ctx.heat_set_bc(bc, n)
     th = M.thermal_fields(m, seed=31, heat=(2e4, 8e4))
-    sol = prob.ctx.solution(n)
-    vel = [np.ascontiguousarray(sol[k], np.float32) for k in ("vx", "vy", "vz")]
-    st = {k: np.zeros(n, np.float32) for k in capi.Context.STRESS_KEYS}
-    prob.ctx.stress_strain(st)
-    se = [st[k] for k in capi.Context.STRESS_KEYS]
+    if synthetic:
+        rng = np.random.Generator(np.random.PCG64(32))
+        vel = [(rng.random(n) * 0.02 - 0.01).astype(np.float32) for _ in range(3)]
+        se = [(rng.random(n) * 2 - 1).astype(np.float32) for _ in range(12)]
+    else:
+        sol = prob.ctx.solution(n)
+        vel = [np.ascontiguousarray(sol[k], np.float32) for k in ("vx", "vy", "vz")]
+        st = {k: np.zeros(n, np.float32) for k in capi.Context.STRESS_KEYS}
+        prob.ctx.stress_strain(st)
+        se = [st[k] for k in capi.Context.STRESS_KEYS]
     nt = m.multinum
     pre = [3] * nt + [0]
     post = [0] + [3] * (nt - 1) + [10]
@@ -447,6 +455,13 @@ def main():
     m = M.config_model(args.config)
     n = m.nodenum
     prob = P.StokesProblem(m, device=local, precision=0, tol=1e-8, restart=args.restart)
+    if args.heat_only:
+        heat = heat_leg(prob, m, args, False, synthetic=True)
+        prob.close()
+        if rank == 0:
+            print(json.dumps({"metric": "ms per heat-equation step (titerate)", "value": heat["ms"], "unit": "ms",
+                              "heat_only": True, "config": args.config, "heat": heat}), flush=True)
+        return
     ronu_ms = [prob.ctx.upload_markers(m.markx, m.marky, m.markz, m.markt, m.rocks.n0, m.rocks.n1, m.rocks.ro)
                or prob.ctx.ronurecalc_resident() for _ in range(3)]
     # smoother and sweep schedule for this model, chosen once (outside the timed region)

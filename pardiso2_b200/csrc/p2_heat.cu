@@ -6,10 +6,11 @@
 //   coarse kt, cp, ro                k_heat_rocp     rocprestrict 1248-1332
 //   implicit 7-point rows            k_heat_rows     heaterr mode 1 (193-246)
 //   smoother                         k_heat_gs       gausmatt 1063-1121, here
-//                                    k_heat_bc       red-black over the heat rows
-//                                                    with the boundary rows
-//                                                    (tbonderr 832-884) set after
-//                                                    each colour
+//                                                    red-black over the heat rows,
+//                                                    each colour pass also setting
+//                                                    the boundary rows (tbonderr
+//                                                    832-884) of the other colour's
+//                                                    targets
 //   residual                         k_heat_resid    gausmatt 1103-1119
 //   residual restriction             k_heat_restrict trestrict 1124-1245
 //   correction prolongation          k_heat_prolong  tprolong 957-1060
@@ -49,9 +50,20 @@ struct HeatLv {
     const double *g[3];
     const int *bci;      // 0 heat row, q + 1 boundary row q
     const float *kt, *cp, *ro;
-    double *x, *b, *r;
-    double *a;           // 7 x n: diagonal, x-, x+, y-, y+, z-, z+
+    double *x, *r;       // node order
+    // colour order: node (i, j, k) of colour c = (i + j + k) & 1 at
+    // c * nh + (k * nx + i) * nyh + j / 2, nyh = (ny + 1) / 2, nh = nx * nz * nyh,
+    // so that one colour pass reads its rows contiguously
+    double *b;           // right-hand side
+    double *a;           // 7 planes of 2 * nh: diagonal (0 on boundary rows), x-, x+, y-, y+, z-, z+
+    long nh;
 };
+
+__device__ __forceinline__ long heat_ci(const HeatLv &L, int i, int j, int k)
+{
+    const int nyh = (L.ny + 1) / 2;
+    return ((i + j + k) & 1) * L.nh + ((long)k * L.nx + i) * nyh + (j >> 1);
+}
 
 __device__ __forceinline__ double heat_kf(const double *g, int m) { return 2.0 / (g[m + 1] - g[m - 1]); }
 
@@ -189,78 +201,86 @@ __global__ void k_heat_rocp(HeatLv F, HeatLv C, AxisMap mx, AxisMap my, AxisMap 
 __global__ void __launch_bounds__(256) k_heat_rows(HeatLv L, double dt, const float *tk0, const float *tk1)
 {
     const long u = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (u >= L.n || L.bci[u]) return;
-    const long nxy = (long)L.nx * L.ny, ny = L.ny, n = L.n;
+    if (u >= L.n) return;
+    const long nxy = (long)L.nx * L.ny, ny = L.ny, A = 2 * L.nh;
     const int m3 = (int)(u / nxy), m1 = (int)((u / ny) % L.nx), m2 = (int)(u % ny);
+    const long c = heat_ci(L, m1, m2, m3);
+    double *a = L.a;
+    if (L.bci[u]) { a[c] = 0; return; }
     const double *gx = L.g[0], *gy = L.g[1], *gz = L.g[2];
     const double xkf = heat_kf(gx, m1), ykf = heat_kf(gy, m2), zkf = heat_kf(gz, m3);
     const double rocpkf = rocp(L.ro[u], L.cp[u]);
     const float *kt = L.kt;
     const float k3 = kt[u];
     double d = rocpkf / dt, v;
-    double *a = L.a;
     v = (kt[u - ny] + k3) / 2.0 * xkf / (gx[m1] - gx[m1 - 1]);
-    a[n + u] = -v; d += v;
+    a[A + c] = -v; d += v;
     v = (k3 + kt[u + ny]) / 2.0 * xkf / (gx[m1 + 1] - gx[m1]);
-    d += v; a[2 * n + u] = -v;
+    d += v; a[2 * A + c] = -v;
     v = (kt[u - 1] + k3) / 2.0 * ykf / (gy[m2] - gy[m2 - 1]);
-    a[3 * n + u] = -v; d += v;
+    a[3 * A + c] = -v; d += v;
     v = (k3 + kt[u + 1]) / 2.0 * ykf / (gy[m2 + 1] - gy[m2]);
-    d += v; a[4 * n + u] = -v;
+    d += v; a[4 * A + c] = -v;
     v = (kt[u - nxy] + k3) / 2.0 * zkf / (gz[m3] - gz[m3 - 1]);
-    a[5 * n + u] = -v; d += v;
+    a[5 * A + c] = -v; d += v;
     v = (k3 + kt[u + nxy]) / 2.0 * zkf / (gz[m3 + 1] - gz[m3]);
-    d += v; a[6 * n + u] = -v;
-    a[u] = d;
-    if (tk0) L.b[u] = tk1[u] + tk0[u] / dt * rocpkf;
+    d += v; a[6 * A + c] = -v;
+    a[c] = d;
+    if (tk0) L.b[c] = tk1[u] + tk0[u] / dt * rocpkf;
 }
 
-// A x of a heat row in the reference's term order (centre, x-, x+, y-, y+, z-, z+)
-__device__ __forceinline__ double heat_ax(const HeatLv &L, long u, double ival)
+// A x of the heat row of node u (colour index c) in the reference's term
+// order (centre, x-, x+, y-, y+, z-, z+)
+__device__ __forceinline__ double heat_ax(const HeatLv &L, long u, long c, double ival)
 {
-    const long nxy = (long)L.nx * L.ny, ny = L.ny, n = L.n;
+    const long nxy = (long)L.nx * L.ny, ny = L.ny, A = 2 * L.nh;
     const double *a = L.a, *x = L.x;
-    ival += a[u] * x[u];
-    ival += a[n + u] * x[u - ny];
-    ival += a[2 * n + u] * x[u + ny];
-    ival += a[3 * n + u] * x[u - 1];
-    ival += a[4 * n + u] * x[u + 1];
-    ival += a[5 * n + u] * x[u - nxy];
-    ival += a[6 * n + u] * x[u + nxy];
+    ival += a[c] * x[u];
+    ival += a[A + c] * x[u - ny];
+    ival += a[2 * A + c] * x[u + ny];
+    ival += a[3 * A + c] * x[u - 1];
+    ival += a[4 * A + c] * x[u + 1];
+    ival += a[5 * A + c] * x[u - nxy];
+    ival += a[6 * A + c] * x[u + nxy];
     return ival;
 }
 
-// one colour of Gauss-Seidel over the heat rows: (i + j + k) & 1 == colour
-__global__ void __launch_bounds__(256) k_heat_gs(HeatLv L, int colour, double t0koef)
+struct HeatBc {
+    int nbc;
+    const int *bu, *bt;            // unknown, resolved heat-row target (-1: none)
+    const double *bk, *bconst;
+    const unsigned char *bpass;    // colour pass that sets the row: the one after its target's
+};
+
+// One colour of Gauss-Seidel over the heat rows ((i + j + k) & 1 == colour),
+// and in the same launch the boundary rows x_u = c + k x_t (c only on level
+// 0) whose target has the other colour: those targets do not change in this
+// pass, and each boundary row is set once per sweep, right after its target.
+__global__ void __launch_bounds__(256) k_heat_gs(HeatLv L, HeatBc B, int colour, double t0koef, int level0)
 {
     const int nyh = (L.ny + 1) / 2;
+    const long half = (long)nyh * L.nx * L.nz;
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (long)nyh * L.nx * L.nz) return;
+    if (t >= half) {
+        const long q = t - half;
+        if (q < B.nbc && B.bpass[q] == colour) {
+            const double c = level0 ? B.bconst[q] : 0.0;
+            const int tg = B.bt[q];
+            L.x[B.bu[q]] = tg >= 0 ? c + B.bk[q] * L.x[tg] : c;
+        }
+        return;
+    }
     const int jj = (int)(t % nyh);
     const long rest = t / nyh;
     const int i = (int)(rest % L.nx), k = (int)(rest / L.nx);
     const int j = 2 * jj + ((i + k + colour) & 1);
     if (j >= L.ny) return;
+    const long c = colour * L.nh + t;
+    const double d = L.a[c];
+    if (d == 0) return;  // boundary row
     const long u = (long)k * L.nx * L.ny + (long)i * L.ny + j;
-    if (L.bci[u]) return;
-    const double ival = heat_ax(L, u, -L.b[u]);
-    L.x[u] -= ival / L.a[u] * t0koef;
-}
-
-struct HeatBc {
-    int nbc;
-    const int *bu, *bt;     // unknown, resolved heat-row target (-1: none)
-    const double *bk, *bconst;
-};
-
-// boundary rows x_u = c + k x_t (c only on level 0)
-__global__ void k_heat_bc(HeatBc B, double *x, int level0)
-{
-    const int q = blockIdx.x * blockDim.x + threadIdx.x;
-    if (q >= B.nbc) return;
-    const double c = level0 ? B.bconst[q] : 0.0;
-    const int t = B.bt[q];
-    x[B.bu[q]] = t >= 0 ? c + B.bk[q] * x[t] : c;
+    const double ival = heat_ax(L, u, c, -L.b[c]);
+    L.x[u] -= ival / d * t0koef;
 }
 
 __global__ void __launch_bounds__(256) k_heat_resid(HeatLv L, HeatBc B, int level0)
@@ -269,7 +289,9 @@ __global__ void __launch_bounds__(256) k_heat_resid(HeatLv L, HeatBc B, int leve
     if (u >= L.n) return;
     const int q = L.bci[u];
     if (!q) {
-        L.r[u] = L.b[u] - (heat_ax(L, u, 0.0));
+        const long nxy = (long)L.nx * L.ny;
+        const long c = heat_ci(L, (int)((u / L.ny) % L.nx), (int)(u % L.ny), (int)(u / nxy));
+        L.r[u] = L.b[c] - (heat_ax(L, u, c, 0.0));
         return;
     }
     const double c = level0 ? B.bconst[q - 1] : 0.0;
@@ -285,9 +307,10 @@ __global__ void k_heat_restrict(HeatLv F, HeatLv C, AxisMap mx, AxisMap my, Axis
     const long u = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (u >= C.n) return;
     C.x[u] = 0;
-    if (C.bci[u]) { C.b[u] = 0; return; }
     const long cnxy = (long)C.nx * C.ny, fnxy = (long)F.nx * F.ny;
     const int c3 = (int)(u / cnxy), c1 = (int)((u / C.ny) % C.nx), c2 = (int)(u % C.ny);
+    const long ci = heat_ci(C, c1, c2, c3);
+    if (C.bci[u]) { C.b[ci] = 0; return; }
     double num = 0, den = 0;
     for (int qz = mz.ptr[c3]; qz < mz.ptr[c3 + 1]; qz++) {
         const double wz = mz.w[qz];
@@ -302,7 +325,7 @@ __global__ void k_heat_restrict(HeatLv F, HeatLv C, AxisMap mx, AxisMap my, Axis
             }
         }
     }
-    C.b[u] = den != 0 ? num / den : num;
+    C.b[ci] = den != 0 ? num / den : num;
 }
 
 // tprolong: x_f += t1koef * trilinear(x_c) on the heat rows of the finer level
@@ -592,6 +615,7 @@ void Solver::heat_set_bc(const int *bondm, long bondm_len, const float *bondv1, 
         const long n = Lv.n;
         std::vector<int> bci(n, 0), bu, bt;
         std::vector<double> bk, bc;
+        std::vector<unsigned char> bpass;
         for (long v = 0; v < n; v++) {
             const long u = Lv.off + v;
             const int b0 = bt_all[u];
@@ -620,6 +644,13 @@ void Solver::heat_set_bc(const int *bondm, long bondm_len, const float *bondv1, 
             bt.push_back(t >= 0 ? (int)(t - Lv.off) : -1);
             bk.push_back(t >= 0 ? kk : 0.0);
             bc.push_back(c);
+            if (t >= 0) {
+                const long tl = t - Lv.off;
+                const int ti = (int)((tl / Lv.ny) % Lv.nx), tj = (int)(tl % Lv.ny), tk = (int)(tl / ((long)Lv.nx * Lv.ny));
+                bpass.push_back((unsigned char)(1 - ((ti + tj + tk) & 1)));
+            } else {
+                bpass.push_back(0);
+            }
         }
         H.nbc = (int)bu.size();
         H.bci = heat_put(heat_arena, st, bci);
@@ -627,16 +658,19 @@ void Solver::heat_set_bc(const int *bondm, long bondm_len, const float *bondv1, 
         H.bt = heat_put(heat_arena, st, bt);
         H.bk = heat_put(heat_arena, st, bk);
         H.bconst = heat_put(heat_arena, st, bc);
+        H.bpass = heat_put(heat_arena, st, bpass);
         for (int a = 0; a < 3; a++) H.g[a] = heat_put(heat_arena, st, Lv.g[a]);
         H.kt = l ? (float *)heat_arena.alloc(sizeof(float) * n) : nullptr;
         H.cp = l ? (float *)heat_arena.alloc(sizeof(float) * n) : nullptr;
         H.ro = l ? (float *)heat_arena.alloc(sizeof(float) * n) : nullptr;
         H.x = (double *)heat_arena.alloc(sizeof(double) * n);
-        H.b = (double *)heat_arena.alloc(sizeof(double) * n);
+        const long nh = (long)Lv.nx * Lv.nz * ((Lv.ny + 1) / 2);
+        H.nh = nh;
+        H.b = (double *)heat_arena.alloc(sizeof(double) * 2 * nh);
         H.r = (double *)heat_arena.alloc(sizeof(double) * n);
-        H.a = (double *)heat_arena.alloc(sizeof(double) * 7 * n);
+        H.a = (double *)heat_arena.alloc(sizeof(double) * 7 * 2 * nh);
         P2_CUDA_TRY(cudaMemsetAsync(H.x, 0, sizeof(double) * n, st));
-        P2_CUDA_TRY(cudaMemsetAsync(H.b, 0, sizeof(double) * n, st));
+        P2_CUDA_TRY(cudaMemsetAsync(H.b, 0, sizeof(double) * 2 * nh, st));
         if (l > 0) {
             for (int a = 0; a < 3; a++) {
                 HostAxis ax;
@@ -677,11 +711,11 @@ static HeatLv heat_view(const Level &Lv, const HeatLevel &H, const HeatState &S,
     v.kt = l ? H.kt : S.kt;
     v.cp = l ? H.cp : S.cp;
     v.ro = l ? H.ro : S.ro;
-    v.x = H.x; v.b = H.b; v.r = H.r; v.a = H.a;
+    v.x = H.x; v.b = H.b; v.r = H.r; v.a = H.a; v.nh = H.nh;
     return v;
 }
 
-static HeatBc heat_bc_view(const HeatLevel &H) { return HeatBc{H.nbc, H.bu, H.bt, H.bk, H.bconst}; }
+static HeatBc heat_bc_view(const HeatLevel &H) { return HeatBc{H.nbc, H.bu, H.bt, H.bk, H.bconst, H.bpass}; }
 
 void Solver::heat_smooth(int l, int sweeps, double t0koef)
 {
@@ -690,9 +724,8 @@ void Solver::heat_smooth(int l, int sweeps, double t0koef)
     const long half = (long)((V.ny + 1) / 2) * V.nx * V.nz;
     for (int s = 0; s < sweeps; s++)
         for (int c = 0; c < 2; c++) {
-            k_heat_gs<<<hb(half), 256, 0, st>>>(V, c, t0koef);
-            if (B.nbc) k_heat_bc<<<hb(B.nbc), 256, 0, st>>>(B, V.x, l == 0);
-            heat.kernels += B.nbc ? 2 : 1;
+            k_heat_gs<<<hb(half + B.nbc), 256, 0, st>>>(V, B, c, t0koef, l == 0);
+            heat.kernels++;
         }
     k_heat_resid<<<hb(V.n), 256, 0, st>>>(V, B, l == 0);
     heat.kernels++;

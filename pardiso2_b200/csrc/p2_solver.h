@@ -73,8 +73,10 @@ struct HeatLevel {
     int nbc = 0;
     int *bu = nullptr, *bt = nullptr;     // boundary row: unknown, resolved heat-row target (-1 none)
     double *bk = nullptr, *bconst = nullptr;
+    unsigned char *bpass = nullptr;       // colour pass that sets the row (after its target's)
     float *kt = nullptr, *cp = nullptr, *ro = nullptr;  // coarse levels (level 0: HeatState)
-    double *x = nullptr, *b = nullptr, *r = nullptr, *a = nullptr;
+    double *x = nullptr, *b = nullptr, *r = nullptr, *a = nullptr;  // b, a in colour order
+    long nh = 0;                          // nodes per colour slot range
     AxisMap map[3]{};                     // this level -> next coarser level
 };
 
