@@ -34,6 +34,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <thread>
 #include <vector>
 
 #include "p2_internal.cuh"
@@ -696,6 +697,16 @@ void Solver::heat_set_bc(const int *bondm, long bondm_len, const float *bondv1, 
     heat.scal = (double *)heat_arena.alloc(sizeof(double) * 8);
     heat.S0 = (double *)heat_arena.alloc(sizeof(double) * n0);
     heat.S1 = (double *)heat_arena.alloc(sizeof(double) * n0);
+    {
+        cudaStream_t s2 = nullptr;
+        P2_CUDA_TRY(cudaStreamCreateWithFlags(&s2, cudaStreamNonBlocking));
+        heat.mst_owner.reset(s2, [](CUstream_st *p) { cudaStreamDestroy(p); });
+        heat.mst = s2;
+        cudaEvent_t e2 = nullptr;
+        P2_CUDA_TRY(cudaEventCreateWithFlags(&e2, cudaEventDisableTiming));
+        heat.mev_owner.reset(e2, [](CUevent_st *p) { cudaEventDestroy(p); });
+        heat.mev = e2;
+    }
     P2_CUDA_TRY(cudaMallocHost((void **)&heat.host, sizeof(double) * 8));  // [0..3] error, range; [4] sub-step
     heat.host_owner.reset(heat.host, [](double *p) { cudaFreeHost(p); });
     P2_CUDA_TRY(cudaStreamSynchronize(st));
@@ -836,6 +847,44 @@ p2_heat_info Solver::titerate(const p2_heat_params &hp, double timestep, float *
         info.kernels = heat.kernels;
         return info;
     }
+    // The markers are needed only after the last sub-step: a helper thread
+    // copies them on a second stream while the sub-steps run (the copies
+    // from pageable memory block the thread that issues them).
+    struct Uploader {
+        std::thread th;
+        cudaError_t err = cudaSuccess;
+        ~Uploader()
+        {
+            if (th.joinable()) th.join();
+        }
+    } up;
+    if (nmark > 0) {
+        if (nmark > heat.mcap) {
+            P2_CUDA_TRY(cudaStreamSynchronize(st));
+            heat_mk_arena.release();
+            heat_mk_arena.guard = 0;
+            heat.mx = (float *)heat_mk_arena.alloc(sizeof(float) * nmark);
+            heat.my = (float *)heat_mk_arena.alloc(sizeof(float) * nmark);
+            heat.mz = (float *)heat_mk_arena.alloc(sizeof(float) * nmark);
+            heat.mk = (float *)heat_mk_arena.alloc(sizeof(float) * nmark);
+            heat.mt = (signed char *)heat_mk_arena.alloc(nmark);
+            heat.mcap = nmark;
+        }
+        const int device = dev;
+        Uploader *u = &up;
+        const HeatState *H = &heat;
+        up.th = std::thread([u, H, device, nmark, mx, my, mz, mt, markk] {
+            const size_t mb = sizeof(float) * nmark;
+            cudaError_t e = cudaSetDevice(device);
+            if (e == cudaSuccess) e = cudaMemcpyAsync(H->mx, mx, mb, cudaMemcpyHostToDevice, H->mst);
+            if (e == cudaSuccess) e = cudaMemcpyAsync(H->my, my, mb, cudaMemcpyHostToDevice, H->mst);
+            if (e == cudaSuccess) e = cudaMemcpyAsync(H->mz, mz, mb, cudaMemcpyHostToDevice, H->mst);
+            if (e == cudaSuccess) e = cudaMemcpyAsync(H->mk, markk, mb, cudaMemcpyHostToDevice, H->mst);
+            if (e == cudaSuccess) e = cudaMemcpyAsync(H->mt, mt, nmark, cudaMemcpyHostToDevice, H->mst);
+            if (e == cudaSuccess) e = cudaEventRecord(H->mev, H->mst);
+            u->err = e;
+        });
+    }
     P2_CUDA_TRY(cudaMemcpyAsync(heat.tk2, heat.tk, fb, cudaMemcpyDeviceToDevice, st));
     const int nt = hp.multinumt;
     for (int l = 1; l <= nt; l++) {
@@ -901,23 +950,10 @@ p2_heat_info Solver::titerate(const p2_heat_params &hp, double timestep, float *
     info.heatsum = heatsum;
 
     if (nmark > 0) {
-        if (nmark > heat.mcap) {
-            P2_CUDA_TRY(cudaStreamSynchronize(st));
-            heat_mk_arena.release();
-            heat_mk_arena.guard = 0;
-            heat.mx = (float *)heat_mk_arena.alloc(sizeof(float) * nmark);
-            heat.my = (float *)heat_mk_arena.alloc(sizeof(float) * nmark);
-            heat.mz = (float *)heat_mk_arena.alloc(sizeof(float) * nmark);
-            heat.mk = (float *)heat_mk_arena.alloc(sizeof(float) * nmark);
-            heat.mt = (signed char *)heat_mk_arena.alloc(nmark);
-            heat.mcap = nmark;
-        }
         const size_t mb = sizeof(float) * nmark;
-        P2_CUDA_TRY(cudaMemcpyAsync(heat.mx, mx, mb, cudaMemcpyHostToDevice, st));
-        P2_CUDA_TRY(cudaMemcpyAsync(heat.my, my, mb, cudaMemcpyHostToDevice, st));
-        P2_CUDA_TRY(cudaMemcpyAsync(heat.mz, mz, mb, cudaMemcpyHostToDevice, st));
-        P2_CUDA_TRY(cudaMemcpyAsync(heat.mk, markk, mb, cudaMemcpyHostToDevice, st));
-        P2_CUDA_TRY(cudaMemcpyAsync(heat.mt, mt, nmark, cudaMemcpyHostToDevice, st));
+        up.th.join();
+        P2_CUDA_TRY(up.err);
+        P2_CUDA_TRY(cudaStreamWaitEvent(st, heat.mev, 0));
         P2_CUDA_TRY(cudaMemsetAsync(heat.S0, 0, sizeof(double) * n0, st));
         P2_CUDA_TRY(cudaMemsetAsync(heat.S1, 0, sizeof(double) * n0, st));
         HeatMarkArgs M;

@@ -95,6 +95,10 @@ struct HeatState {
     long mcap = 0;
     float *mx = nullptr, *my = nullptr, *mz = nullptr, *mk = nullptr;
     signed char *mt = nullptr;
+    cudaStream_t mst = nullptr;  // marker copies, overlapped with the sub-steps
+    cudaEvent_t mev = nullptr;
+    std::shared_ptr<CUstream_st> mst_owner;
+    std::shared_ptr<CUevent_st> mev_owner;
     long long kernels = 0;
 };
 
