@@ -69,3 +69,32 @@ def test_reference_shim_compiles_in_the_unity_build():
     for name, kind in (("vpiterate", "T"), ("ronurecalc", "T"), ("vpiterate_cpu", "T"), ("ronurecalc_cpu", "T"),
                        ("p2_stokes_solve", "U"), ("p2_ronurecalc", "U"), ("p2_set_grid", "U")):
         assert any(ln.split()[-2:] == [kind, name] for ln in syms.splitlines()), (name, kind)
+
+
+def test_ctypes_structs_match_the_header(tmp_path):
+    """The ctypes mirrors of the parameter / result structs have the C
+    layout (size and every field offset), checked against gcc on the header."""
+    import shutil
+    import subprocess
+
+    from pardiso2_b200 import capi
+    if shutil.which("gcc") is None:
+        pytest.skip("gcc not available")
+    structs = {"p2_params": capi.Params, "p2_solve_info": capi.SolveInfo, "p2_tune_info": capi.TuneInfo,
+               "p2_effbulk": capi.EffBulk, "p2_heat_params": capi.HeatParams, "p2_heat_info": capi.HeatInfo}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "p2cuda.h"', "int main(void) {"]
+    for cname, cls in structs.items():
+        lines.append('printf("%s size %%zu\\n", sizeof(%s));' % (cname, cname))
+        for f, _ in cls._fields_:
+            lines.append('printf("%s.%s %%zu\\n", offsetof(%s, %s));' % (cname, f, cname, f))
+    lines.append("return 0; }")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    out = dict(l.rsplit(" ", 1) for l in subprocess.run([str(exe)], check=True, capture_output=True,
+                                                           text=True).stdout.split("\n") if l)
+    for cname, cls in structs.items():
+        assert int(out["%s size" % cname]) == ctypes.sizeof(cls), cname
+        for f, _ in cls._fields_:
+            assert int(out["%s.%s" % (cname, f)]) == getattr(cls, f).offset, (cname, f)
