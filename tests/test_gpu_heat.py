@@ -144,3 +144,37 @@ def test_titerate_argument_errors():
         prob.ctx.titerate(_hp(m, HEAT_VARIANTS["mg"]), 1e4, th)
     assert e.value.code == 1
     prob.close()
+
+
+def test_titerate_vs_oracle_65_all_levels(oracle_mod):
+    """The bench's heat step (spheres65 grid, all four levels, 2.1 M markers,
+    2000 s in sub-steps of at most 25 K, heatmin 1e-3 K) against the oracle:
+    same sub-steps, temperatures within the heatmin bar."""
+    m = M.config_model(2)
+    n = m.nodenum
+    bc = M.with_thermal_bc(m)
+    th = M.thermal_fields(m, seed=31, heat=(2e4, 8e4))
+    rng = np.random.Generator(np.random.PCG64(32))
+    vel = [(rng.random(n) * 0.02 - 0.01).astype(np.float32) for _ in range(3)]
+    se = [(rng.random(n) * 2 - 1).astype(np.float32) for _ in range(12)]
+    nt = m.multinum
+    v = dict(multinumt=nt, multicyct=1, pre=[3] * nt + [0], post=[0] + [3] * (nt - 1) + [10], frictyn=1, adiabyn=1,
+             heatdif=1.0)
+    q = np.arange(m.markx.size)
+    mt = np.where(q % 9 == 4, 70, m.markt).astype(np.int8)
+    markk = np.where(q % 3 == 0, 0.0, 900.0).astype(np.float32)
+    markers = (m.markx, m.marky, m.markz, mt)
+    hpd = dict(HEAT_COMMON, **v, heatmin=1e-3, gx=m.params.gx, gy=m.params.gy, gz=m.params.gz, max_cycles=200,
+               timestep=2000.0)
+    tko, mko, oi = oracle_mod.titerate(m.gx, m.gy, m.gz, nt, bc.bondt, bc.bondv1, bc.bondn1, hpd, th, vel=vel, se=se,
+                                       markers=markers, markk=markk)
+    assert not oi["capped"] and oi["substeps"] == 3
+    m.bc = bc
+    prob = _problem(m)
+    tk, mk, info = prob.ctx.titerate(_hp(m, v, heatmin=1e-3), 2000.0, th, vel=vel, se=se, markers=markers,
+                                     markk=markk)
+    assert info.converged == 1 and info.substeps == oi["substeps"]
+    d = tk.astype(np.float64) - tko
+    assert np.abs(d).max() <= TK_MAX and np.sqrt(np.mean(d * d)) <= TK_RMS
+    assert np.abs(mk.astype(np.float64) - mko).max() <= TK_MAX
+    prob.close()
