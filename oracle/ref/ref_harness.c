@@ -738,7 +738,7 @@ void p2ref_titerate(const double *dpar, const int *ipar, float *itk, const float
     memcpy(ht, iht, sizeof(float) * (size_t)nodenum);
     memcpy(et, iet, sizeof(float) * (size_t)nodenum);
     if (ipr) memcpy(pr, ipr, sizeof(double) * (size_t)nodenum);
-    /* The second marker loop runs to marknum inclusive (heat3mg.c:666) and
+    /* The marker loops run to marknum inclusive (heat3mg.c:660, 796) and
      * marknum0 == marknum (MRKNEW 1.0), so it reads one slot past the
      * arrays: the harness's last marker is that slot, kept outside the box,
      * and titerate sees marknum - 1 markers. */
