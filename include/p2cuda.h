@@ -280,7 +280,7 @@ p2_status p2_effbulk_visc(p2_ctx *ctx, const float *ro, const float *nxx, const 
  *   checks per sub-step; 0 = 10000; P2_OK with converged = 0 when reached).
  *   Then the markers (optional, nmark 0 skips them): types 50..99 take the
  *   node temperature, types below 50 the numerical-diffusion update of
- *   markk (heatdif, tdeep, zdeep), as heat3mg.c:640-818 does.
+ *   markk (heatdif, tdeep, zdeep), as heat3mg.c:641-829 does.
  *   tk and markk are updated in place; kt, cp, ro, ht, et are level-0 float
  *   fields (ro of the node layout, as ronurecalc writes it).
  *   The smoother is Gauss-Seidel in two colours (the reference sweeps the

@@ -1919,12 +1919,12 @@ void p2o_prolong(void *h, int lc, const double *coarse_x, double *fine_x)
 /* ---------------------------------------------------------------------- */
 /* Heat equation step (titerate, pardiso/heat3mg.c:292-829), single thread. */
 /* Restated literally: the level-0 right-hand side heaterr mode 0 (6-291),  */
-/* the step limit from maxtkstep (331-374), rocprestrict (1248-1332), the   */
+/* the step limit from maxtkstep (331-374), rocprestrict (1235-1332), the   */
 /* implicit 7-point rows heaterr mode 1 and the boundary rows tbonderr      */
-/* (832-884) stored as gausmat2 does (gaus3mg_SerieMG.c:312-365), the       */
-/* damped lexicographic Gauss-Seidel gausmatt (1063-1121), trestrict        */
-/* (1124-1245), tprolong (957-1060), the error heaterr mode 2 and the       */
-/* marker temperatures with numerical diffusion (640-829, tkcalc1           */
+/* (841-893) stored as gausmat2 does (gaus3mg_SerieMG.c:312-365), the       */
+/* damped lexicographic Gauss-Seidel gausmatt (1057-1120), trestrict        */
+/* (1122-1233), tprolong (954-1054), the error heaterr mode 2 and the       */
+/* marker temperatures with numerical diffusion (641-829, tkcalc1           */
 /* pardiso/mark3mg.c:1212-1282).  Float arrays (tk, tk0, tk1, tk2, kt, cp,  */
 /* ro, ht, et) and the float arithmetic of the reference's expressions on   */
 /* them are kept.  The reference loops until the error is below HEATMIN     */
@@ -1995,7 +1995,7 @@ typedef struct {
     double t0koef, t1koef;
 } ht_ctx;
 
-/* Coarse level fields from the finer one: rocprestrict (heat3mg.c:1248-1332),
+/* Coarse level fields from the finer one: rocprestrict (heat3mg.c:1235-1332),
  * float accumulators with double weights as the reference's arrays are. */
 static void ht_rocprestrict(ht_ctx *H, int lc)
 {
@@ -2035,7 +2035,7 @@ static void ht_rocprestrict(ht_ctx *H, int lc)
     }
 }
 
-/* trestrict (heat3mg.c:1124-1245) */
+/* trestrict (heat3mg.c:1122-1233) */
 static void ht_restrict(ht_ctx *H, int lc)
 {
     ht_grid *G = &H->G;
@@ -2078,7 +2078,7 @@ static void ht_restrict(ht_ctx *H, int lc)
     }
 }
 
-/* tprolong with ynreset 0 (heat3mg.c:957-1060) */
+/* tprolong with ynreset 0 (heat3mg.c:954-1054) */
 static void ht_prolong(ht_ctx *H, int lc)
 {
     ht_grid *G = &H->G;
@@ -2115,7 +2115,7 @@ static void ht_prolong(ht_ctx *H, int lc)
             }
 }
 
-/* gausmatt (heat3mg.c:1063-1121) on the rows of one level */
+/* gausmatt (heat3mg.c:1057-1120) on the rows of one level */
 static void ht_gausmatt(ht_ctx *H, int am, long mcmax, long mcmin)
 {
     long m1;
@@ -2363,7 +2363,7 @@ int p2o_titerate(int nx, int ny, int nz, const double *gx, const double *gy, con
     timestep = tktimesum0;
     (void)gl;
 
-    /* marker temperatures (heat3mg.c:640-829) */
+    /* marker temperatures (heat3mg.c:641-829) */
     if (nmark > 0 && markk) {
         double *S0 = calloc(nn, sizeof(double)), *S1 = calloc(nn, sizeof(double));
         double xs = gx[nx - 1] - gx[0], ys = gy[ny - 1] - gy[0], zs = gz[nz - 1] - gz[0];

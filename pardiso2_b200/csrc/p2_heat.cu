@@ -3,22 +3,22 @@
 // What runs where:
 //   right-hand side and step limit   k_heat_rhs      heaterr mode 0 (6-291),
 //                                                    the max |dT/dt| loop 331-374
-//   coarse kt, cp, ro                k_heat_rocp     rocprestrict 1248-1332
-//   implicit 7-point rows            k_heat_rows     heaterr mode 1 (193-246)
-//   smoother                         k_heat_gs       gausmatt 1063-1121, here
+//   coarse kt, cp, ro                k_heat_rocp     rocprestrict 1235-1332
+//   implicit 7-point rows            k_heat_rows     heaterr mode 1 (196-248)
+//   smoother                         k_heat_gs       gausmatt 1057-1120, here
 //                                                    red-black over the heat rows,
 //                                                    each colour pass also setting
 //                                                    the boundary rows (tbonderr
-//                                                    832-884) of the other colour's
+//                                                    841-893) of the other colour's
 //                                                    targets
 //   residual                         k_heat_resid    gausmatt 1103-1119
-//   residual restriction             k_heat_restrict trestrict 1124-1245
-//   correction prolongation          k_heat_prolong  tprolong 957-1060
-//   error and float temperatures     k_heat_error    heaterr mode 2 (249-289),
-//                                                    the reload 491-509
-//   marker temperatures              k_heat_markers  640-760 with tkcalc1
+//   residual restriction             k_heat_restrict trestrict 1122-1233
+//   correction prolongation          k_heat_prolong  tprolong 954-1054
+//   error and float temperatures     k_heat_error    heaterr mode 2 (250-289),
+//                                                    the reload 505-512
+//   marker temperatures              k_heat_markers  641-768 with tkcalc1
 //                                    k_heat_anti     (mark3mg.c:1212-1282),
-//                                                    antidiffusion 769-818
+//                                                    antidiffusion 770-829
 // The V-cycle has the reference's shape: pre-smoothing and restriction down
 // to multinumt, then smoothing and prolongation back up, with no smoothing
 // on level 0 after the last prolongation.  The smoother is the one
@@ -478,7 +478,7 @@ __device__ __forceinline__ bool tk_inside(const HeatMarkArgs &A, long q)
     return x > 0 && y > 0 && z > 0 && (double)x < A.G.size[0] && (double)y < A.G.size[1] && (double)z < A.G.size[2];
 }
 
-// marker temperatures after the step (heat3mg.c:640-760): types 50..99 take
+// marker temperatures after the step (heat3mg.c:641-768): types 50..99 take
 // the new node temperature; types below 50 are initialised where markk <= 0,
 // relaxed towards the old node temperature by the numerical diffusion and
 // shifted by the node temperature change.
@@ -537,7 +537,7 @@ __global__ void k_heat_node_mean(long n, const double *S0, double *S1)
     if (u < n && S0[u] != 0) S1[u] /= S0[u];
 }
 
-// antidiffusion (heat3mg.c:796-818): the mean node change taken back from
+// antidiffusion (heat3mg.c:770-829): the mean node change taken back from
 // the markers of types below 50
 __global__ void __launch_bounds__(256) k_heat_anti(HeatMarkArgs A)
 {
@@ -742,7 +742,7 @@ void Solver::heat_smooth(int l, int sweeps, double t0koef)
     heat.kernels++;
 }
 
-// multicyct V-cycles on levels 0..multinumt (heat3mg.c:459-497), then the
+// multicyct V-cycles on levels 0..multinumt (heat3mg.c:462-500), then the
 // level-0 error and temperature range into heat.scal[0..3]
 void Solver::heat_batch(const p2_heat_params &hp)
 {
