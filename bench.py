@@ -260,8 +260,10 @@ def heat_leg(prob, m, args, with_cpu: bool, synthetic: bool = False):
     heating) and its stresses / strain rates (shear heating), the workload's
     markers with types 0/1 (diffused) and 70 (reset to the node
     temperature).  All levels of the grid, 3 smoothing sweeps down and up,
-    10 on the coarsest; a 2000 s step (about 2.5 diffusion times of a cell of
-    the 65^3 unit box) in sub-steps of at most 25 K, errors below 1e-3 K."""
+    10 on the coarsest; a step of about 2.5 diffusion times of a cell (2000 s
+    on the 65^3 unit box, scaled with the squared spacing on other grids) in
+    sub-steps of at most 25 K, errors below 2e-3 K (above the float
+    temperatures' error floor, about 1.2e-3 K at 129^3)."""
     import numpy as np
     from pardiso2_b200 import capi
     from pardiso2_b200 import model as M
@@ -282,17 +284,18 @@ def heat_leg(prob, m, args, with_cpu: bool, synthetic: bool = False):
     nt = m.multinum
     pre = [3] * nt + [0]
     post = [0] + [3] * (nt - 1) + [10]
-    hp = capi.heat_params(multinumt=nt, multicyct=1, pre=pre, post=post, heatmin=1e-3, max_cycles=200)
+    hp = capi.heat_params(multinumt=nt, multicyct=1, pre=pre, post=post, heatmin=2e-3, max_cycles=200)
     q = np.arange(m.markx.size)
     mt = np.where(q % 9 == 4, 70, m.markt).astype(np.int8)
     markk = np.where(q % 3 == 0, 0.0, 900.0).astype(np.float32)
     markers = (m.markx, m.marky, m.markz, mt)
-    dt = 2000.0
+    dt = 2000.0 * (64.0 / (m.shape[0] - 1)) ** 2
     for _ in range(max(1, args.warmup)):
         prob.ctx.titerate(hp, dt, th, vel=vel, se=se, markers=markers, markk=markk)
     runs = [prob.ctx.titerate(hp, dt, th, vel=vel, se=se, markers=markers, markk=markk)[2] for _ in range(args.steps)]
     info = runs[-1]
     out = {"ms": statistics.mean(r.ms_total for r in runs), "nodes": n, "markers": int(q.size), "levels": nt + 1,
+           "dt_s": dt,
            "substeps": info.substeps, "error_checks": info.cycles, "heatsum": info.heatsum, "heatmin": hp.heatmin,
            "converged": bool(info.converged), "launches": int(info.kernels),
            "timing": "CUDA events around the call, host<->device copies of the fields and markers included"}
