@@ -611,7 +611,7 @@ static void lu_issue(cudaStream_t st, double *A, int n, int kl, int ku, double *
 }
 
 int band_lu_inverse(cudaStream_t st, double *A, int n, int kl, int ku, double *Ainv, int *d_ipiv, int *d_info,
-                    cudaEvent_t *marks, LuGraph *cache)
+                    cudaEvent_t *marks, LuGraph *cache, bool wait)
 {
     kl = std::max(0, std::min(kl, n - 1));
     ku = std::max(0, std::min(ku, n - 1));
@@ -662,6 +662,7 @@ int band_lu_inverse(cudaStream_t st, double *A, int n, int kl, int ku, double *A
         cudaEventDestroy(T.b);
     }
     int info = 0;
+    if (!wait) return 0;  // the caller reads d_info once the stream has finished
     P2_CUDA_TRY(cudaMemcpyAsync(&info, d_info, sizeof(int), cudaMemcpyDeviceToHost, st));
     P2_CUDA_TRY(cudaStreamSynchronize(st));
     return info;

@@ -27,7 +27,20 @@ namespace p2 {
 
 constexpr int kProbes = 4 * 125;  // coarsest-operator probes: 125 colour classes x 4 components
 int band_lu_inverse(cudaStream_t st, double *A, int n, int kl, int ku, double *Ainv, int *d_ipiv, int *d_info,
-                    cudaEvent_t *marks, LuGraph *cache);
+                    cudaEvent_t *marks, LuGraph *cache, bool wait = true);
+// sweeps of the diagonal cell smoother on the coarsest level standing in for
+// its direct solve while the LU is still running
+constexpr int kCoarseApxSweeps = 16;
+// Outer iterations that use the smoothed coarsest level: kOverlapScale *
+// nF / n0, the LU's latency-bound panel chain (about linear in nF) over the
+// fine work of one iteration (linear in n0), fixed from the grid sizes so
+// that the iterates do not depend on timing (10 at 65^3, 2 at 129^3, 0 at
+// 257^3 with nF = 6912); none on grids of fewer than four levels, where the
+// coarsest level is too large a part of the problem for smoothing to stand
+// in for it.  The solve waits for the LU at that iteration if it is still
+// running.
+constexpr double kOverlapScale = 400.0;
+constexpr int kOverlapMax = 16;
 void d2f(cudaStream_t st, size_t n, const double *a, float *b);
 
 static inline unsigned nblk(long n, int t = kThreads) { return (unsigned)((n + t - 1) / t); }
@@ -190,12 +203,21 @@ Solver::Solver(int device) : dev(device)
 {
     P2_CUDA_TRY(cudaSetDevice(dev));
     P2_CUDA_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    {
+        // the coarsest LU's panel chain is latency-bound: its kernels go first
+        // when they share the device with the V-cycles
+        int lo = 0, hi = 0;
+        P2_CUDA_TRY(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+        P2_CUDA_TRY(cudaStreamCreateWithPriority(&st_lu, cudaStreamNonBlocking, hi));
+    }
+    P2_CUDA_TRY(cudaEventCreateWithFlags(&ev_lu, cudaEventDisableTiming));
     for (int i = 0; i < 8; i++) P2_CUDA_TRY(cudaEventCreate(&ev[i]));
 }
 
 Solver::~Solver()
 {
     cudaSetDevice(dev);
+    if (st_lu) cudaStreamSynchronize(st_lu);
     drop_graphs();
     if (lu_graph.exec) cudaGraphExecDestroy(lu_graph.exec);
     arena.release();
@@ -207,12 +229,18 @@ Solver::~Solver()
     heat_mk_arena.release();
     heat = HeatState{};
     for (int i = 0; i < 8; i++) cudaEventDestroy(ev[i]);
+    if (ev_lu) cudaEventDestroy(ev_lu);
+    if (st_lu) cudaStreamDestroy(st_lu);
     if (st) cudaStreamDestroy(st);
 }
 
 void Solver::drop_graphs()
 {
     for (auto &g : graphs) {
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+        g.exec = nullptr;
+    }
+    for (auto &g : graphs_apx) {
         if (g.exec) cudaGraphExecDestroy(g.exec);
         g.exec = nullptr;
     }
@@ -729,6 +757,9 @@ __global__ void k_gemv(int n, const T *A, const T *b, T *y)
 
 void Solver::coarse_setup()
 {
+    // an LU left running by a solve that ended in an error still reads A_c
+    P2_CUDA_TRY(cudaStreamSynchronize(st_lu));
+    lu_pending = false;
     Level &C = L.back();
     int nl = (int)L.size();
     LevelView<double> Lc = view<double>(nl - 1, nl == 1);
@@ -740,7 +771,19 @@ void Solver::coarse_setup()
     P2_CUDA_TRY(cudaGetLastError());
     P2_CUDA_TRY(cudaMemcpyAsync(h_bw, d_bw, sizeof(int) * 2, cudaMemcpyDeviceToHost, st));
     P2_CUDA_TRY(cudaStreamSynchronize(st));
-    if (verbose) P2_CUDA_TRY(cudaEventRecord(ev[5], st));
+    if (!verbose) {
+        // The LU and the inverse run on their own stream (st has no work in
+        // flight after the synchronisation above); the solve goes on with a
+        // smoothed coarsest level until ev_lu reports them done (lu_finish).
+        band_lu_inverse(st_lu, A_c, nF, h_bw[0], h_bw[1], Ainv64, d_ipiv, d_info, nullptr, &lu_graph, false);
+        d2f(st_lu, (size_t)nF * nF, Ainv64, Ainv32);
+        P2_CUDA_TRY(cudaEventRecord(ev_lu, st_lu));
+        lu_pending = true;
+        lu_overlap_iters = L.size() < 4 ? 0
+                           : (int)std::min<double>(kOverlapMax, std::floor(kOverlapScale * nF / (double)L[0].n + 0.5));
+        return;
+    }
+    P2_CUDA_TRY(cudaEventRecord(ev[5], st));
     int info = band_lu_inverse(st, A_c, nF, h_bw[0], h_bw[1], Ainv64, d_ipiv, d_info, verbose ? ev + 6 : nullptr,
                                &lu_graph);
     if (verbose) {
@@ -755,9 +798,47 @@ void Solver::coarse_setup()
     d2f(st, (size_t)nF * nF, Ainv64, Ainv32);
 }
 
+// The overlapped LU: once ev_lu has completed (block: wait for it), check
+// its pivots and order the solve's stream after it.
+void Solver::lu_finish(bool block)
+{
+    if (!lu_pending) return;
+    if (block) {
+        P2_CUDA_TRY(cudaEventSynchronize(ev_lu));
+    } else {
+        const cudaError_t q = cudaEventQuery(ev_lu);
+        if (q == cudaErrorNotReady) return;
+        P2_CUDA_TRY(q);
+    }
+    int info = 0;
+    P2_CUDA_TRY(cudaMemcpyAsync(&info, d_info, sizeof(int), cudaMemcpyDeviceToHost, st_lu));
+    P2_CUDA_TRY(cudaStreamSynchronize(st_lu));
+    P2_CUDA_TRY(cudaStreamWaitEvent(st, ev_lu, 0));
+    lu_pending = false;
+    if (info) throw Error(P2_ERR_SINGULAR, "zero pivot in the coarsest LU at column " + std::to_string(info));
+}
+
+// Stand-in for the coarsest direct solve: x = 0, then sweeps of the diagonal
+// cell smoother (no stored factors needed) on the coarsest level.
+template <typename T>
+void Solver::coarse_approx(Vec4<T> &b, Vec4<T> &x)
+{
+    Level &C = L.back();
+    for (int c = 0; c < 4; c++) P2_CUDA_TRY(cudaMemsetAsync(x.c[c], 0, sizeof(T) * C.n, st));
+    const int keep = prm.smoother;
+    prm.smoother = 0;
+    smooth<T>((int)L.size() - 1, kCoarseApxSweeps);
+    prm.smoother = keep;
+    (void)b;
+}
+
 template <typename T>
 void Solver::coarse_solve(Vec4<T> &b, Vec4<T> &x)
 {
+    if (coarse_mode) {
+        coarse_approx<T>(b, x);
+        return;
+    }
     Level &C = L.back();
     T *bF = std::is_same<T, double>::value ? (T *)cb64 : (T *)cb32;
     T *xF = std::is_same<T, double>::value ? (T *)cx64 : (T *)cx32;
@@ -993,7 +1074,7 @@ void Solver::precondition(Vec4<double> &z)
 template <typename T>
 void Solver::capture_vcycle_graph()
 {
-    GraphSlot &g = graphs[std::is_same<T, double>::value ? 1 : 0];
+    GraphSlot &g = (coarse_mode ? graphs_apx : graphs)[std::is_same<T, double>::value ? 1 : 0];
     if (g.exec || !prm.use_graphs) return;
     cudaGraph_t graph;
     long long before = g_launches;
@@ -1011,7 +1092,7 @@ template <typename T>
 void Solver::run_vcycle_graph()
 {
     int key = std::is_same<T, double>::value ? 1 : 0;
-    GraphSlot &g = graphs[key];
+    GraphSlot &g = (coarse_mode ? graphs_apx : graphs)[key];
     if (!prm.use_graphs) {
         vcycle<T>();
         P2_CUDA_TRY(cudaGetLastError());
@@ -1071,6 +1152,8 @@ p2_solve_info Solver::solve()
         if (rel <= prm.tol) { info.status = P2_OK; break; }
         if (it >= prm.max_iter) { info.status = P2_ERR_NOT_CONVERGED; break; }
         Vec4<double> &z = Z[k], &q = Q[k];
+        if (it >= lu_overlap_iters) lu_finish(true);
+        coarse_mode = lu_pending ? 1 : 0;
         P2_CUDA_TRY(cudaEventRecord(ev[2], st));
         precondition(z);
         P2_CUDA_TRY(cudaEventRecord(ev[3], st));
@@ -1105,6 +1188,10 @@ p2_solve_info Solver::solve()
         k = (k + 1) % m;
         it++;
     }
+    // the overlapped LU has to be finished (and its pivots checked) before
+    // the solve returns; the graphs after it use the exact coarsest solve
+    coarse_mode = 0;
+    lu_finish(true);
     // pressure shift to the pinned value
     k_pressure_shift_value<<<1, 32, 0, st>>>(gx.c[0], L0.pin, L0.pinval, scal + 3); P2_COUNT_LAUNCH();
     k_pressure_shift<<<nblk(n), kThreads, 0, st>>>(L0.nx, L0.ny, L0.nz, gx.c[0], scal + 3); P2_COUNT_LAUNCH();
