@@ -112,3 +112,39 @@ def test_markers_seeded_and_inside():
     for arr in (a.markx, a.marky, a.markz):
         assert arr.min() > 0 and arr.max() < 1
     assert set(np.unique(a.markt)) <= {0, 1}
+
+
+def test_thermal_rows_cover_every_wall_node():
+    """The heat equation needs a T boundary row on every wall node of every
+    level (heaterr reads all six neighbours of a heat row); copy targets stay
+    on their level and chains end within two rows at a heat row or a fixed
+    temperature."""
+    import numpy as np
+    from pardiso2_b200 import model as M
+    m = M.sphere_model(33, 3, (1, 1, 1), seed=5)
+    bc = M.with_thermal_bc(m, 300.0, 1600.0)
+    lv = m.levels
+    assert bc.bondt is not None and bc.bondt.size == lv.total_nodes
+    for l in range(lv.multinum + 1):
+        nx, ny, nz, off = lv.mgx[l], lv.mgy[l], lv.mgz[l], lv.mgp[l]
+        k, i, j = np.meshgrid(np.arange(nz), np.arange(nx), np.arange(ny), indexing="ij")
+        wall = ((i == 0) | (j == 0) | (k == 0) | (i == nx - 1) | (j == ny - 1) | (k == nz - 1)).ravel()
+        rows = bc.bondt[off:off + lv.mgn[l]]
+        assert np.all(rows[wall] > 0) and np.all(rows[~wall] == 0), l
+        for u in np.nonzero(wall)[0]:
+            r, depth = rows[u], 0
+            while bc.bondn1[r]:
+                t = bc.bondn1[r] - 1
+                assert off <= t < off + lv.mgn[l]
+                r = bc.bondt[t]
+                depth += 1
+                if not r:
+                    break
+            assert depth <= 2
+    # z planes fixed, walls insulating copies
+    z0 = bc.bondt[lv.mgp[0] + (lv.mgn[0] - 1)]  # top corner node: fixed plane wins
+    assert bc.bondn1[z0] == 0 and bc.bondv1[z0, 0] == np.float32(1600.0)
+    ref = bc.reference_bondm(m.nodenum)
+    assert ref.size >= 8 * m.nodenum + lv.total_nodes
+    np.testing.assert_array_equal(ref[8 * m.nodenum:8 * m.nodenum + lv.total_nodes], bc.bondt)
+    np.testing.assert_array_equal(ref[:bc.bondm.size], bc.bondm)
