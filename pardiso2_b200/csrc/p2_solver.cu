@@ -774,7 +774,7 @@ void Solver::coarse_setup()
     if (!verbose) {
         // The LU and the inverse run on their own stream (st has no work in
         // flight after the synchronisation above); the solve goes on with a
-        // smoothed coarsest level until ev_lu reports them done (lu_finish).
+        // smoothed coarsest level for lu_overlap_iters outer iterations.
         band_lu_inverse(st_lu, A_c, nF, h_bw[0], h_bw[1], Ainv64, d_ipiv, d_info, nullptr, &lu_graph, false);
         d2f(st_lu, (size_t)nF * nF, Ainv64, Ainv32);
         P2_CUDA_TRY(cudaEventRecord(ev_lu, st_lu));
@@ -798,18 +798,12 @@ void Solver::coarse_setup()
     d2f(st, (size_t)nF * nF, Ainv64, Ainv32);
 }
 
-// The overlapped LU: once ev_lu has completed (block: wait for it), check
-// its pivots and order the solve's stream after it.
-void Solver::lu_finish(bool block)
+// The overlapped LU: wait for it, check its pivots and order the solve's
+// stream after it.
+void Solver::lu_finish()
 {
     if (!lu_pending) return;
-    if (block) {
-        P2_CUDA_TRY(cudaEventSynchronize(ev_lu));
-    } else {
-        const cudaError_t q = cudaEventQuery(ev_lu);
-        if (q == cudaErrorNotReady) return;
-        P2_CUDA_TRY(q);
-    }
+    P2_CUDA_TRY(cudaEventSynchronize(ev_lu));
     int info = 0;
     P2_CUDA_TRY(cudaMemcpyAsync(&info, d_info, sizeof(int), cudaMemcpyDeviceToHost, st_lu));
     P2_CUDA_TRY(cudaStreamSynchronize(st_lu));
@@ -1152,7 +1146,7 @@ p2_solve_info Solver::solve()
         if (rel <= prm.tol) { info.status = P2_OK; break; }
         if (it >= prm.max_iter) { info.status = P2_ERR_NOT_CONVERGED; break; }
         Vec4<double> &z = Z[k], &q = Q[k];
-        if (it >= lu_overlap_iters) lu_finish(true);
+        if (it >= lu_overlap_iters) lu_finish();
         coarse_mode = lu_pending ? 1 : 0;
         P2_CUDA_TRY(cudaEventRecord(ev[2], st));
         precondition(z);
@@ -1191,7 +1185,7 @@ p2_solve_info Solver::solve()
     // the overlapped LU has to be finished (and its pivots checked) before
     // the solve returns; the graphs after it use the exact coarsest solve
     coarse_mode = 0;
-    lu_finish(true);
+    lu_finish();
     // pressure shift to the pinned value
     k_pressure_shift_value<<<1, 32, 0, st>>>(gx.c[0], L0.pin, L0.pinval, scal + 3); P2_COUNT_LAUNCH();
     k_pressure_shift<<<nblk(n), kThreads, 0, st>>>(L0.nx, L0.ny, L0.nz, gx.c[0], scal + 3); P2_COUNT_LAUNCH();

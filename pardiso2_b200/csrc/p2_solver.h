@@ -225,14 +225,14 @@ class Solver {
     HeatState heat;
     std::array<GraphSlot, 2> graphs;
     // Coarsest LU + inverse on a second stream, overlapped with the first
-    // V-cycles, which use a smoothed coarsest level until ev_lu completes.
+    // lu_overlap_iters outer iterations, whose V-cycles smooth the coarsest level.
     std::array<GraphSlot, 2> graphs_apx;
     cudaStream_t st_lu = nullptr;
     cudaEvent_t ev_lu = nullptr;
     bool lu_pending = false;
     int coarse_mode = 0;  // 0: exact coarsest solve (inverse), 1: smoothing sweeps
     int lu_overlap_iters = 0;
-    void lu_finish(bool block);
+    void lu_finish();
     template <typename T>
     void coarse_approx(Vec4<T> &b, Vec4<T> &x);
     LuGraph lu_graph;  // coarsest LU + inverse launch sequence
