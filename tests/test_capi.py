@@ -58,14 +58,15 @@ def test_reference_shim_compiles_in_the_unity_build():
     """pardiso2_b200/csrc/move3mg_cuda.c replaces vpiterate()/ronurecalc()
     inside the reference's own unity build (needs the reference sources)."""
     import subprocess
-    ref = os.environ.get("P2_REFERENCE_DIR", "/root/reference/pardiso")
-    if not os.path.isdir(ref):
-        pytest.skip("reference sources not present")
-    r = subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "shimcheck", "REF=" + ref],
-                       capture_output=True, text=True)
-    assert r.returncode == 0, r.stdout + r.stderr
-    syms = subprocess.run(["nm", os.path.join(ROOT, "oracle", "_ref", "shim_check.o")], capture_output=True,
-                          text=True).stdout
+    obj = os.path.join(ROOT, "oracle", "_ref", "shim_check.o")
+    ref = os.environ.get("P2_REFERENCE_DIR")
+    if ref and os.path.isdir(ref):
+        r = subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "shimcheck", "REF=" + ref],
+                           capture_output=True, text=True)
+        assert r.returncode == 0, r.stdout + r.stderr
+    if not os.path.exists(obj):
+        pytest.skip("shim check object not built (build() with the reference sources, or P2_REFERENCE_DIR)")
+    syms = subprocess.run(["nm", obj], capture_output=True, text=True).stdout
     for name, kind in (("vpiterate", "T"), ("ronurecalc", "T"), ("vpiterate_cpu", "T"), ("ronurecalc_cpu", "T"),
                        ("p2_stokes_solve", "U"), ("p2_ronurecalc", "U"), ("p2_set_grid", "U")):
         assert any(ln.split()[-2:] == [kind, name] for ln in syms.splitlines()), (name, kind)
