@@ -332,10 +332,14 @@ p2_status p2_titerate(p2_ctx *ctx, const p2_heat_params *hp, double timestep, fl
  *   p2_ronurecalc).  Work runs on `stream` (a cudaStream_t; NULL = default).
  *   The call waits once for the stream (a check of the marker types) and
  *   returns with the node pass queued on it.
- *   The first call on a device looks up the scratch array's device address
- *   with that device current; make that first call before any stream capture
- *   begins.  All calls share the one array: calls whose work overlaps on the
- *   GPU (different streams or host threads without ordering) race.
+ *   Rock types 0..20 with markn0 != markn1 (power law) return
+ *   P2_ERR_UNSUPPORTED; types above 20 take markn0, as p2_ronurecalc does.
+ *   The first call on a device (and the first after a cudaDeviceReset, which
+ *   unloads the array) looks up the scratch array's device address with that
+ *   device current; make that first call before any stream capture begins.
+ *   All calls share the one array: calls whose work overlaps on the GPU
+ *   (different streams or host threads without ordering) race, so serialise
+ *   them (one stream, or ordering by the caller).
  *   On an error, a message is written to err (errlen bytes; may be NULL). */
 p2_status p2_ronurecalc_noalloc(int nx, int ny, int nz, const double *gx, const double *gy, const double *gz,
                                 const p2_params *prm, int nrock, const double *markn0, const double *markn1,

@@ -904,14 +904,17 @@ static p2_status fail(char *err, long errlen, p2_status code, const char *fmt, .
     return code;
 }
 
-static bool on_device(const void *p)
+// device (or managed) memory that the current device `dev` can use: a device
+// array of another GPU is refused (its kernels would read peer memory)
+static bool on_device(const void *p, int dev)
 {
     cudaPointerAttributes a;
     if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
         cudaGetLastError();
         return false;
     }
-    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+    if (a.type == cudaMemoryTypeManaged) return true;
+    return a.type == cudaMemoryTypeDevice && a.device == dev;
 }
 
 static bool increasing(const double *g, int n)
@@ -952,7 +955,9 @@ extern "C" p2_status p2_ronurecalc_noalloc(int nx, int ny, int nz, const double 
     double f[256], r[256];
     for (int t = 0; t < 256; t++) { f[t] = 1.0; r[t] = 0.0; }
     for (int t = 0; t < nrock && t < 50; t++) {
-        if (markn0[t] != markn1[t])
+        // only types up to 20 take the power law (mark3mg.c:1481-1498); above
+        // that markn0 is the viscosity whatever markn1 holds
+        if (markn0[t] != markn1[t] && t <= 20)
             return fail(err, errlen, P2_ERR_UNSUPPORTED, "rock type %d has a power-law viscosity (markn0 != markn1)",
                         t);
         double mnu = markn0[t];
@@ -968,15 +973,18 @@ extern "C" p2_status p2_ronurecalc_noalloc(int nx, int ny, int nz, const double 
     }
     float *outs[6] = {nu, ro, nxx, nxy, nxz, nyz};
     for (int q = 0; q < 6; q++)
-        if (!outs[q] || !on_device(outs[q]))
-            return fail(err, errlen, P2_ERR_ARG, "node field %d is not a device array", q);
-    if (nmark > 0 && (!markx || !marky || !markz || !markt || !on_device(markx) || !on_device(marky) ||
-                      !on_device(markz) || !on_device(markt)))
-        return fail(err, errlen, P2_ERR_ARG, "marker arrays must be device arrays");
+        if (!outs[q] || !on_device(outs[q], dev))
+            return fail(err, errlen, P2_ERR_ARG, "node field %d is not a device array of the current device", q);
+    if (nmark > 0 && (!markx || !marky || !markz || !markt || !on_device(markx, dev) || !on_device(marky, dev) ||
+                      !on_device(markz, dev) || !on_device(markt, dev)))
+        return fail(err, errlen, P2_ERR_ARG, "marker arrays must be device arrays of the current device");
     // the array's host-side name is not a device address: look the address up once per device
     unsigned char *base;
     {
         std::lock_guard<std::mutex> lk(g_mu);
+        // a cudaDeviceReset unloads the module: an address cached before it is
+        // looked up again when it no longer names device memory of this device
+        if (g_addr[dev] && !on_device(g_addr[dev], dev)) g_addr[dev] = nullptr;
         if (!g_addr[dev]) {
             cudaError_t e = cudaGetSymbolAddress((void **)&g_addr[dev], g_noalloc_scratch);
             if (e != cudaSuccess) {

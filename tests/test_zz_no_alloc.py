@@ -111,3 +111,66 @@ def test_noalloc_rejects_sizes_beyond_its_scratch():
     st = f(len(g), len(g), len(g), pg, pg, pg, C.byref(params), len(rk), pr, pr, pr, 0, *([None] * 4),
            *([host.ctypes.data_as(C.c_void_p)] * 6), None, err, len(err))
     assert st == 1 and b"device" in err.value
+
+
+def _with_high_type_law(m):
+    """The model with its rock table extended to type 30 holding markn0 !=
+    markn1 (a power-law pair above type 20, which the reference reads as the
+    constant markn0) and a tenth of its markers moved to that type."""
+    import copy
+    mm = copy.copy(m)
+    r = copy.copy(m.rocks)
+    n0 = np.concatenate([r.n0, np.full(31 - r.n0.size, 1.0)])
+    n1 = n0.copy()
+    ro = np.concatenate([r.ro, np.zeros(31 - r.ro.size)])
+    n0[30], n1[30], ro[30] = 5.0, 50.0, 0.5
+    r.n0, r.n1, r.ro = n0, n1, ro
+    mm.rocks = r
+    mt = np.array(m.markt, np.int8)
+    mt[::10] = 30
+    mm.markt = mt
+    return mm
+
+
+@pytest.mark.gpu
+def test_noalloc_type_above_20_with_distinct_markn1_matches_ronurecalc():
+    import pardiso2_b200 as P
+    from pardiso2_b200 import model as M
+    f = _bind()
+    m = _with_high_type_law(M.sphere_model(17, 2, (2, 2, 2), seed=1, eta_sphere=1e3))
+    init = _init(m, 13)
+    want = _existing(m, {k: v.copy() for k, v in init.items()})
+    got = _noalloc(f, m, P.params_for(m), init)
+    for k in KEYS:
+        assert np.array_equal(got[k], want[k]), k
+
+
+@pytest.mark.gpu
+def test_noalloc_without_markers_matches_ronurecalc():
+    import copy
+    import pardiso2_b200 as P
+    from pardiso2_b200 import model as M
+    f = _bind()
+    m = copy.copy(M.sphere_model(17, 2, (2, 2, 2), seed=1))
+    for k in ("markx", "marky", "markz"):
+        setattr(m, k, np.zeros(0, np.float32))
+    m.markt = np.zeros(0, np.int8)
+    init = _init(m, 14)
+    want = _existing(m, {k: v.copy() for k, v in init.items()})
+    got = _noalloc(f, m, P.params_for(m), init)
+    for k in KEYS:
+        assert np.array_equal(got[k], want[k]), k
+
+
+@pytest.mark.gpu
+def test_noalloc_refuses_marker_types_without_a_rock_entry():
+    import copy
+    import pardiso2_b200 as P
+    from pardiso2_b200 import model as M
+    f = _bind()
+    m = copy.copy(M.sphere_model(17, 2, (2, 2, 2), seed=1))
+    mt = np.array(m.markt, np.int8)
+    mt[5] = 40  # below 50, past the two-entry rock table
+    m.markt = mt
+    with pytest.raises(AssertionError, match="without a rock entry"):
+        _noalloc(f, m, P.params_for(m), _init(m, 15))
