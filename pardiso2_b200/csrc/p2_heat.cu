@@ -34,6 +34,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstring>
 #include <thread>
 #include <vector>
 
@@ -442,9 +443,31 @@ struct HeatMarkArgs {
     float *mk;
     GridSh G;
     const float *tk, *tk2, *kt, *cp, *ro;
-    double *S0, *S1;   // per node: sum of weights, sum of weighted diffusion changes
+    // per node, fixed point (two's complement in 64 bits): sum of weights
+    // (scale 2^40) and sum of weighted diffusion changes (scale 2^32); after
+    // k_heat_node_mean S1 holds their quotient as a double
+    unsigned long long *S0, *S1;
+    unsigned long long *range;  // set when a change is beyond the fixed-point range
     double heatdif, dt, tdeep, zdeep;
 };
+
+// Marker sums into the nodes are integer additions of fixed-point values, so
+// their result does not depend on the order in which the markers arrive (the
+// reference adds per-thread arrays in thread order).  The scales leave a
+// resolution of 2^-40 for the weights (at most 8 per marker, all in [0, 1])
+// and 2^-32 K for the temperature changes; |change x weight| must stay below
+// 2^29 K, far above any temperature, else `range` is set and the host fails.
+constexpr double kHeatW = 1099511627776.0;  // 2^40
+constexpr double kHeatT = 4294967296.0;     // 2^32
+__device__ __forceinline__ unsigned long long heat_fixed(double v, double scale, unsigned long long *range)
+{
+    const double f = v * scale;
+    if (!(fabs(f) < 2305843009213693952.0)) {  // 2^61
+        atomicOr(range, 1ull);
+        return 0ull;
+    }
+    return (unsigned long long)__double2ll_rn(f);
+}
 
 // tkcalc1: cell, spacings and the 8 node weights (z outer, x, y inner)
 __device__ __forceinline__ void tk_weights(const GridSh &G, double x, double y, double z, int c[3], double h[3],
@@ -523,18 +546,22 @@ __global__ void __launch_bounds__(256) k_heat_markers(HeatMarkArgs A)
         dtk1 = dtk * (1.0 - exp(dtk1));
         mk += (float)dtk1;
         for (int n1 = 0; n1 < 8; n1++) {
-            atomicAdd(A.S1 + wn[n1], dtk1 * wi[n1]);
-            atomicAdd(A.S0 + wn[n1], wi[n1]);
+            atomicAdd(A.S1 + wn[n1], heat_fixed(dtk1 * wi[n1], kHeatT, A.range));
+            atomicAdd(A.S0 + wn[n1], heat_fixed(wi[n1], kHeatW, A.range));
         }
     }
     mk += (float)(e2 - e3);
     A.mk[q] = mk;
 }
 
-__global__ void k_heat_node_mean(long n, const double *S0, double *S1)
+// mean diffusion change per node, written over the fixed-point sum S1
+__global__ void k_heat_node_mean(long n, const unsigned long long *S0, unsigned long long *S1)
 {
     const long u = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (u < n && S0[u] != 0) S1[u] /= S0[u];
+    if (u >= n) return;
+    const long long w = (long long)S0[u], d = (long long)S1[u];
+    const double mean = w != 0 ? ((double)d / kHeatT) / ((double)w / kHeatW) : 0.0;
+    reinterpret_cast<double *>(S1)[u] = mean;
 }
 
 // antidiffusion (heat3mg.c:770-829): the mean node change taken back from
@@ -549,7 +576,7 @@ __global__ void __launch_bounds__(256) k_heat_anti(HeatMarkArgs A)
     tk_weights(A.G, A.mx[q], A.my[q], A.mz[q], c, h, wn, wi);
     float mk = A.mk[q];
     for (int n1 = 0; n1 < 8; n1++) {
-        const double s = A.S1[wn[n1]];
+        const double s = reinterpret_cast<const double *>(A.S1)[wn[n1]];
         if (s != 0) mk -= (float)(s * wi[n1]);
     }
     A.mk[q] = mk;
@@ -960,16 +987,19 @@ p2_heat_info Solver::titerate(const p2_heat_params &hp, double timestep, float *
         M.nmark = nmark; M.mx = heat.mx; M.my = heat.my; M.mz = heat.mz; M.mt = heat.mt; M.mk = heat.mk;
         M.G = G;
         M.tk = heat.tk; M.tk2 = heat.tk2; M.kt = heat.kt; M.cp = heat.cp; M.ro = heat.ro;
-        M.S0 = heat.S0; M.S1 = heat.S1;
+        M.S0 = (unsigned long long *)heat.S0; M.S1 = (unsigned long long *)heat.S1;
+        M.range = (unsigned long long *)(heat.scal + 6);
+        P2_CUDA_TRY(cudaMemsetAsync(heat.scal + 6, 0, sizeof(double), st));
         M.heatdif = hp.heatdif; M.dt = tktimesum0; M.tdeep = hp.tdeep; M.zdeep = hp.zdeep;
         k_heat_markers<<<hb(nmark), 256, 0, st>>>(M);
         heat.kernels++;
         if (hp.heatdif != 0) {
-            k_heat_node_mean<<<hb(n0), 256, 0, st>>>(n0, heat.S0, heat.S1);
+            k_heat_node_mean<<<hb(n0), 256, 0, st>>>(n0, M.S0, M.S1);
             k_heat_anti<<<hb(nmark), 256, 0, st>>>(M);
             heat.kernels += 2;
         }
         P2_CUDA_TRY(cudaMemcpyAsync(markk, heat.mk, mb, cudaMemcpyDeviceToHost, st));
+        P2_CUDA_TRY(cudaMemcpyAsync(heat.host + 6, heat.scal + 6, sizeof(double), cudaMemcpyDeviceToHost, st));
     }
     P2_CUDA_TRY(cudaMemcpyAsync(tk, heat.tk, fb, cudaMemcpyDeviceToHost, st));
     P2_CUDA_TRY(cudaEventRecord(ev[1], st));
@@ -977,6 +1007,11 @@ p2_heat_info Solver::titerate(const p2_heat_params &hp, double timestep, float *
     P2_CUDA_TRY(cudaGetLastError());
     float ms = 0;
     P2_CUDA_TRY(cudaEventElapsedTime(&ms, ev[0], ev[1]));
+    if (nmark > 0) {
+        unsigned long long range = 0;
+        std::memcpy(&range, heat.host + 6, sizeof(range));
+        if (range) throw Error(P2_ERR_ARG, "a marker temperature change is beyond 2^29 K (markk or tk corrupt)");
+    }
     info.ms_total = ms;
     info.kernels = heat.kernels;
     return info;

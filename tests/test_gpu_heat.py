@@ -174,4 +174,9 @@ def test_titerate_vs_oracle_65_all_levels(oracle_mod):
     d = tk.astype(np.float64) - tko
     assert np.abs(d).max() <= TK_MAX and np.sqrt(np.mean(d * d)) <= TK_RMS
     assert np.abs(mk.astype(np.float64) - mko).max() <= TK_MAX
+    # the marker sums into the nodes do not depend on the order the markers
+    # arrive in: a second identical call gives the same markk bit for bit
+    tk2, mk2, _ = prob.ctx.titerate(_hp(m, v, heatmin=1e-3), 2000.0, th, vel=vel, se=se, markers=markers,
+                                    markk=markk)
+    assert np.array_equal(tk2, tk) and np.array_equal(mk2, mk)
     prob.close()
