@@ -73,7 +73,10 @@ typedef struct {
     double omega;        /* cell-block smoother damping (default 0.7) */
     int use_graphs;      /* capture the V-cycle in a CUDA graph (default 1) */
     int smoother;        /* cell-block smoother: 1 = exact 7x7 cell solve with the cell
-                            factors computed once per solve and stored (default),
+                            factors computed once per solve and stored (default; one
+                            launch per colour), 5 = the same with both colours of a sweep
+                            in one launch on large levels (z-marching tiles in shared
+                            memory; slower on B200 as measured, kept for comparison),
                             3 = the same solve factored on every sweep (no stored factors),
                             0 = diagonal velocity block (cheaper, weak at stiff inclusions),
                             2 = the exact cell solve evaluated row by row (slower; a cross-check) */
@@ -368,6 +371,14 @@ p2_status p2_debug_level_fields(p2_ctx *ctx, float *nu, float *ro);
  * after a 256 MB write that evicts the level from L2 (allocated and freed by
  * this call). */
 p2_status p2_debug_time_smoother(p2_ctx *ctx, int level, int passes, double *ms_per_pass);
+/* `sweeps` sweeps of the configured smoother on `level` as the V-cycle runs
+ * them (in its precision; fused sweeps where the level allows), applied to the
+ * state x (in/out) for the right-hand side b, both interleaved as above. */
+p2_status p2_debug_smooth(p2_ctx *ctx, int level, int sweeps, const double *b, double *x);
+/* Average device time of one smoother sweep on `level` as the V-cycle runs it
+ * (both colours with their boundary rows), `sweeps` sweeps timed together
+ * after a 256 MB write that evicts L2, mean of 10 repetitions. */
+p2_status p2_debug_time_sweep(p2_ctx *ctx, int level, int sweeps, double *ms_per_sweep);
 
 #ifdef __cplusplus
 }

@@ -20,7 +20,8 @@ STATUS = {0: "P2_OK", 1: "P2_ERR_ARG", 2: "P2_ERR_CUDA", 3: "P2_ERR_NOMEM", 4: "
 EXPORTED = ["p2_default_params", "p2_create", "p2_destroy", "p2_last_error", "p2_set_grid", "p2_set_bc",
             "p2_set_nodes", "p2_stokes_solve", "p2_stokes_solve_resident", "p2_get_solution", "p2_ronurecalc",
             "p2_upload_markers", "p2_ronurecalc_resident", "p2_get_nodes", "p2_debug_apply", "p2_debug_restrict",
-            "p2_debug_prolong", "p2_debug_level_fields", "p2_debug_time_smoother", "p2_ronurecalc_noalloc", "p2_autotune",
+            "p2_debug_prolong", "p2_debug_level_fields", "p2_debug_time_smoother", "p2_debug_smooth",
+            "p2_debug_time_sweep", "p2_ronurecalc_noalloc", "p2_autotune",
             "p2_movemark", "p2_movemark_resident", "p2_get_markers", "p2_stress_strain",
             "p2_stokes_solve_batch", "p2_movemark_strain", "p2_ronurecalc_powerlaw", "p2_effbulk_visc",
             "p2_default_heat_params", "p2_heat_set_bc", "p2_titerate"]
@@ -416,8 +417,10 @@ def _debug_sigs(L):
     L.p2_debug_prolong.argtypes = [C.c_void_p, C.c_int, _dpp, _dpp]
     L.p2_debug_level_fields.argtypes = [C.c_void_p, _fpp, _fpp]
     L.p2_debug_time_smoother.argtypes = [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_double)]
+    L.p2_debug_smooth.argtypes = [C.c_void_p, C.c_int, C.c_int, _dpp, _dpp]
+    L.p2_debug_time_sweep.argtypes = [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_double)]
     for f in ("p2_debug_apply", "p2_debug_restrict", "p2_debug_prolong", "p2_debug_level_fields",
-              "p2_debug_time_smoother"):
+              "p2_debug_time_smoother", "p2_debug_smooth", "p2_debug_time_sweep"):
         getattr(L, f).restype = C.c_int
 
 
@@ -450,6 +453,17 @@ class DebugHooks:
         ms = C.c_double()
         self.ctx._check(self.ctx.L.p2_debug_time_smoother(self.ctx.h, level, passes, C.byref(ms)),
                         "p2_debug_time_smoother")
+        return ms.value
+
+    def smooth(self, level: int, sweeps: int, b: np.ndarray, x: np.ndarray) -> np.ndarray:
+        out = np.array(x, np.float64)
+        self.ctx._check(self.ctx.L.p2_debug_smooth(self.ctx.h, level, sweeps, np.ascontiguousarray(b, np.float64),
+                                                   out), "p2_debug_smooth")
+        return out
+
+    def time_sweep(self, level: int = 0, sweeps: int = 2) -> float:
+        ms = C.c_double()
+        self.ctx._check(self.ctx.L.p2_debug_time_sweep(self.ctx.h, level, sweeps, C.byref(ms)), "p2_debug_time_sweep")
         return ms.value
 
     def level_fields(self, total_nodes: int):

@@ -22,6 +22,7 @@
 
 #include "p2_kernels.cuh"
 #include "p2_solver.h"
+#include "p2_sweep.cuh"
 
 namespace p2 {
 
@@ -31,6 +32,8 @@ int band_lu_inverse(cudaStream_t st, double *A, int n, int kl, int ku, double *A
 // sweeps of the diagonal cell smoother on the coarsest level standing in for
 // its direct solve while the LU is still running
 constexpr int kCoarseApxSweeps = 16;
+// cell planes per block of the fused sweep (each block starts 3 planes early)
+constexpr int kSweepChunk = 32;
 // Outer iterations that use the smoothed coarsest level: kOverlapScale *
 // nF / n0, the LU's latency-bound panel chain (about linear in nF) over the
 // fine work of one iteration (linear in n0), fixed from the grid sizes so
@@ -507,6 +510,28 @@ void Solver::set_bc(const int *bondm, long bondm_len, const float *bondv1, const
             Lv.h_rt[q] = t;
             Lv.h_rk[q] = t >= 0 ? kk : 0.0;
         }
+        // fused sweeps: boundary rows by node, and whether every resolved
+        // target lies within one node of its unknown
+        {
+            Lv.fuse_ok = true;
+            for (size_t q = 0; q < bu.size() && Lv.fuse_ok; q++) {
+                const int t = Lv.h_rt[q];
+                if (t < 0) continue;
+                const int u = bu[q] >> 2, v = t >> 2;
+                const int du[3] = {u / (Lv.nx * Lv.ny), (u / Lv.ny) % Lv.nx, u % Lv.ny};
+                const int dv[3] = {v / (Lv.nx * Lv.ny), (v / Lv.ny) % Lv.nx, v % Lv.ny};
+                for (int a = 0; a < 3; a++)
+                    if (std::abs(du[a] - dv[a]) > 1) Lv.fuse_ok = false;
+            }
+            std::vector<int> order(bu.size());
+            for (size_t q = 0; q < order.size(); q++) order[q] = (int)q;
+            std::sort(order.begin(), order.end(), [&](int a, int b2) { return bu[a] < bu[b2]; });
+            std::vector<int> first(Lv.n, 0);
+            for (size_t r = order.size(); r-- > 0;) first[bu[order[r]] >> 2] = (int)r;
+            Lv.sw_first = upload(arena, first);
+            if (order.empty()) order.push_back(0);
+            Lv.sw_order = upload(arena, order);
+        }
         Lv.h_bcm = m;
         Lv.bcm = upload(arena, m);
         Lv.bu = upload(arena, bu);
@@ -882,7 +907,8 @@ void Solver::smoother_pass(int l, const LevelView<T> &V, T *P, Vec4<T> &vin, Vec
     const long cells = (long)(Lv.nx - 1) * (Lv.nz - 1) * (Lv.ny / 2);
     const T om = (T)prm.omega;
     switch (prm.smoother) {
-    case 1: {
+    case 1:
+    case 5: {
         const T *blk = (const T *)Lv.blk + (size_t)col * kBlkEntries * Lv.blk_stride;
         pdl_launch(st, nblk(cells, 128), 128, k_vanka_stored<T>, V, P, vin, vout, b, om, col, blk, Lv.blk_stride);
         break;
@@ -913,9 +939,63 @@ void Solver::factor_smoother()
 
 void Solver::factor_cells()
 {
-    if (prm.smoother != 1) return;
+    if (prm.smoother != 1 && prm.smoother != 5) return;
     if (prm.precision == 0) factor_smoother<float>();
     else factor_smoother<double>();
+}
+
+// Fused sweeps (smoother 5) on levels whose planes hold enough tiles to fill
+// the device and whose boundary rows are local; other levels, and smoother 1,
+// run the two colour passes.
+constexpr long kFuseMinPlaneCells = 48L * 48L;
+
+bool Solver::use_fused(int l) const
+{
+    const Level &Lv = L[l];
+    return prm.smoother == 5 && Lv.fuse_ok && (long)(Lv.nx - 1) * (Lv.ny - 1) >= kFuseMinPlaneCells &&
+           Lv.nz - 1 >= 8;
+}
+
+template <typename T>
+static void sweep_kernel_setup()
+{
+    static bool done = false;  // per instantiation, per process (the attribute is per function)
+    if (!done) {
+        P2_CUDA_TRY(cudaFuncSetAttribute(k_vanka_sweep<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)sweep_smem_bytes<T>()));
+        done = true;
+    }
+}
+
+// One fused sweep xin -> xout on level l (boundary rows of xout not set).
+template <typename T>
+void Solver::sweep_fused(int l, const LevelView<T> &V, Vec4<T> &xin, Vec4<T> &xout, Vec4<T> &b)
+{
+    Level &Lv = L[l];
+    sweep_kernel_setup<T>();
+    const int chunk = kSweepChunk;
+    dim3 grid((Lv.nx - 1 + kSwTX - 1) / kSwTX, (Lv.ny - 1 + kSwTY - 1) / kSwTY, (Lv.nz - 1 + chunk - 1) / chunk);
+    const T *blk0 = (const T *)Lv.blk, *blk1 = blk0 + (size_t)kBlkEntries * Lv.blk_stride;
+    SweepBC bc{Lv.sw_first, Lv.sw_order, Lv.bu, Lv.bt, Lv.bnext, Lv.bk};
+#ifdef P2_NO_PDL
+    k_vanka_sweep<T><<<grid, kSwThreads, sweep_smem_bytes<T>(), st>>>(V, xin, xout, b, (T)prm.omega, blk0, blk1,
+                                                                      Lv.blk_stride, bc, chunk);
+    P2_COUNT_LAUNCH();
+#else
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = dim3(kSwThreads);
+    cfg.dynamicSmemBytes = sweep_smem_bytes<T>();
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    P2_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_vanka_sweep<T>, V, xin, xout, b, (T)prm.omega, blk0, blk1,
+                                   Lv.blk_stride, bc, chunk));
+    P2_COUNT_LAUNCH();
+#endif
 }
 
 template <typename T>
@@ -930,6 +1010,26 @@ void Solver::smooth(int l, int sweeps)
     // pressure is updated in place in x.c[0] (yy shares it)
     Vec4<T> yy = y;
     yy.c[0] = x.c[0];
+    int s0 = 0;
+    if (use_fused(l)) {
+        // pairs of fused sweeps x -> y -> x (y with its own pressure field);
+        // an odd count starts with one sweep of colour passes
+        if (sweeps & 1) {
+            for (int col = 0; col < 2; col++) {
+                Vec4<T> &vin = col ? yy : x, &vout = col ? x : yy;
+                smoother_pass<T>(l, V, x.c[0], vin, vout, b, col);
+                bc_set<T>(l, vout, b);
+            }
+            s0 = 1;
+        }
+        for (int s = s0; s < sweeps; s += 2) {
+            sweep_fused<T>(l, V, x, y, b);
+            bc_set<T>(l, y, b);
+            sweep_fused<T>(l, V, y, x, b);
+            bc_set<T>(l, x, b);
+        }
+        return;
+    }
     for (int s = 0; s < sweeps; s++) {
         for (int col = 0; col < 2; col++) {
             Vec4<T> &vin = col ? yy : x, &vout = col ? x : yy;
@@ -1449,6 +1549,68 @@ void Solver::debug_prolong(int lc, const double *coarse_x, double *fine_x)
     k_prolong<double><<<nblk(F.n), kThreads, 0, st>>>(VF, Xf.v, VC, Xc.v, F.tv, prm.p1koef, prm.v1koef); P2_COUNT_LAUNCH();
     P2_CUDA_TRY(cudaGetLastError());
     from_vec4(st, Xf.v, F.n, fine_x);
+}
+
+// `sweeps` sweeps of the configured smoother (as the V-cycle runs them, in its
+// precision) on level l: state x (in/out) for the right-hand side b, both
+// interleaved FP64 [P,Vx,Vy,Vz] per node of the level.
+void Solver::debug_smooth(int l, int sweeps, const double *b, double *x)
+{
+    if (l < 0 || l >= (int)L.size() || sweeps < 0 || sweeps > 64) throw Error(P2_ERR_ARG, "bad level or sweep count");
+    debug_prepare();
+    factor_cells();
+    Level &Lv = L[l];
+    TmpVec X(Lv.n), B(Lv.n);
+    to_vec4(st, x, Lv.n, X.v);
+    to_vec4(st, b, Lv.n, B.v);
+    if (prm.precision == 0) {
+        for (int c = 0; c < 4; c++) {
+            d2f(st, (size_t)Lv.n, X.v.c[c], Lv.x32.c[c]);
+            d2f(st, (size_t)Lv.n, B.v.c[c], Lv.b32.c[c]);
+        }
+        smooth<float>(l, sweeps);
+        k_f32_to_f64<<<nblk(Lv.n), kThreads, 0, st>>>(Lv.n, Lv.x32, X.v); P2_COUNT_LAUNCH();
+    } else {
+        for (int c = 0; c < 4; c++) {
+            P2_CUDA_TRY(cudaMemcpyAsync(Lv.x64.c[c], X.v.c[c], sizeof(double) * Lv.n, cudaMemcpyDeviceToDevice, st));
+            P2_CUDA_TRY(cudaMemcpyAsync(Lv.b64.c[c], B.v.c[c], sizeof(double) * Lv.n, cudaMemcpyDeviceToDevice, st));
+        }
+        smooth<double>(l, sweeps);
+        for (int c = 0; c < 4; c++)
+            P2_CUDA_TRY(cudaMemcpyAsync(X.v.c[c], Lv.x64.c[c], sizeof(double) * Lv.n, cudaMemcpyDeviceToDevice, st));
+    }
+    P2_CUDA_TRY(cudaGetLastError());
+    from_vec4(st, X.v, Lv.n, x);
+}
+
+// Average device time of one smoother sweep on level l as the V-cycle runs
+// it (both colours and their boundary rows; fused where the level allows),
+// on the state left by the last solve: `sweeps` sweeps timed together after
+// a 256 MB write that evicts L2, repeated 10 times.
+double Solver::debug_time_sweep(int l, int sweeps)
+{
+    if (l < 0 || l >= (int)L.size() || sweeps < 1 || sweeps > 64) throw Error(P2_ERR_ARG, "bad level or sweep count");
+    if (!bc_ready) throw Error(P2_ERR_STATE, "no level data");
+    factor_cells();
+    const size_t flush_bytes = (size_t)256 << 20;
+    void *flush = nullptr;
+    P2_CUDA_TRY(cudaMalloc(&flush, flush_bytes));
+    struct Free { void *p; ~Free() { if (p) cudaFree(p); } } hold{flush};
+    double total = 0;
+    const int reps = 10;
+    for (int r = 0; r < reps; r++) {
+        P2_CUDA_TRY(cudaMemsetAsync(flush, r & 0xff, flush_bytes, st));
+        P2_CUDA_TRY(cudaEventRecord(ev[5], st));
+        if (prm.precision == 0) smooth<float>(l, sweeps);
+        else smooth<double>(l, sweeps);
+        P2_CUDA_TRY(cudaEventRecord(ev[6], st));
+        P2_CUDA_TRY(cudaEventSynchronize(ev[6]));
+        float ms = 0;
+        P2_CUDA_TRY(cudaEventElapsedTime(&ms, ev[5], ev[6]));
+        total += ms;
+    }
+    P2_CUDA_TRY(cudaGetLastError());
+    return total / reps / sweeps;
 }
 
 // nu, ro of every level (after ronurestrict), concatenated like the reference's nu[] / ro[]

@@ -45,6 +45,10 @@ struct Level {
     // kBlkEntries x blk_stride values of the V-cycle's type, entry-major
     void *blk = nullptr;
     long blk_stride = 0;
+    // fused sweeps (k_vanka_sweep): every boundary row's resolved target
+    // within one node; the rows by node (first row per node, row order)
+    bool fuse_ok = false;
+    int *sw_first = nullptr, *sw_order = nullptr;
     // boundary rows sorted by copy-chain depth
     int nbc = 0;
     std::vector<int> bc_groups;
@@ -143,6 +147,8 @@ class Solver {
     void debug_prolong(int lc, const double *coarse_x, double *fine_x);
     void debug_level_fields(float *nu, float *ro);
     double debug_time_smoother(int level, int passes);
+    double debug_time_sweep(int level, int sweeps);
+    void debug_smooth(int level, int sweeps, const double *b, double *x);
     p2_tune_info autotune(int trial_iters);
     bool verbose = false;
 
@@ -198,6 +204,9 @@ class Solver {
     void smooth(int l, int sweeps);
     template <typename T>
     void smoother_pass(int l, const LevelView<T> &V, T *P, Vec4<T> &vin, Vec4<T> &vout, Vec4<T> &b, int col);
+    bool use_fused(int l) const;
+    template <typename T>
+    void sweep_fused(int l, const LevelView<T> &V, Vec4<T> &xin, Vec4<T> &xout, Vec4<T> &b);
     template <typename T>
     void factor_smoother();
     void factor_cells();

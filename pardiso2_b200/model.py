@@ -468,7 +468,7 @@ def sphere_model(n=33, multinum=2, markers=(4, 4, 4), seed=1, eta_sphere=1e3, dr
 
 
 def random_spheres_model(n, multinum, nsph, eta_range, rad_range=(0.05, 0.12), drho_range=(-1.0, 1.0),
-                         markers=(2, 2, 2), seed=2, name=None, gap=None):
+                         markers=(2, 2, 2), seed=2, name=None, gap=None, shape=None):
     """nsph spheres: radius U[rad_range], centre U[0,1]^3, viscosity
     log-uniform in eta_range, density contrast U[drho_range]; background
     type 0 (viscosity 1, density 0).  Later spheres paint over earlier ones.
@@ -501,7 +501,8 @@ def random_spheres_model(n, multinum, nsph, eta_range, rad_range=(0.05, 0.12), d
         for s in range(nsph):
             paint_ellipsoid(mx, my, mz, mt, cen[s, 0], cen[s, 1], cen[s, 2], rad[s], rad[s], rad[s], s + 1)
 
-    return _finish(name or ("spheres%d_%d" % (n, nsph)), n, multinum, *markers, seed, rocks, paint, params)
+    return _finish(name or ("spheres%d_%d" % (n, nsph)), n, multinum, *markers, seed, rocks, paint, params,
+                   shape=shape)
 
 
 def layered_model(n=257, multinum=6, markers=(2, 2, 2), seed=5, nlayers=45, name=None):

@@ -91,3 +91,40 @@ def test_context_survives_errors():
     assert info.status == 0
     prob.close()
     prob2.close()
+
+
+def test_singular_coarsest_system_reports_singular():
+    """A coarsest-level cell whose six faces are all fixed-value boundary rows
+    leaves its pressure with neither an equation nor a coupling in the
+    coarsest system: the direct solve meets an exactly zero pivot and the
+    solve returns P2_ERR_SINGULAR (a status, not a device fault)."""
+    m = small()
+    lv = m.levels
+    c = lv.multinum
+    nx, ny, off = lv.mgx[c], lv.mgy[c], lv.mgp[c]
+    i, j, k = nx // 2, ny // 2, lv.mgz[c] // 2
+    faces = [(i - 1, j - 1, k - 1, 1), (i, j - 1, k - 1, 1), (i - 1, j - 1, k - 1, 2), (i - 1, j, k - 1, 2),
+             (i - 1, j - 1, k - 1, 3), (i - 1, j - 1, k, 3)]
+    bondm = m.bc.bondm.copy()
+    bondv1 = [m.bc.bondv1]
+    bondn1 = [m.bc.bondn1]
+    row = m.bc.bondnum
+    for (a, b, d, comp) in faces:
+        u = off + d * lv.mgxy[c] + a * ny + b
+        assert bondm[4 * u + comp] == 0
+        row += 1
+        bondm[4 * u + comp] = row
+        bondv1.append(np.array([[0.0, 0.0]], np.float32))
+        bondn1.append(np.array([0], np.int32))
+    prob = P.StokesProblem(m, tol=1e-8)
+    prob.ctx.set_bc(bondm, np.concatenate(bondv1), np.concatenate(bondn1))
+    prob.ronurecalc()
+    with pytest.raises(capi.P2Error) as e:
+        prob.ctx.solve_resident()
+    assert e.value.code == 6  # P2_ERR_SINGULAR
+    # the context stays usable: the original tables solve
+    prob.ctx.set_bc(m.bc.bondm, m.bc.bondv1, m.bc.bondn1)
+    prob.ronurecalc()
+    _, info = prob.solve_fp64()
+    assert info.status == 0
+    prob.close()
