@@ -94,6 +94,10 @@ def parse():
                     help="only the heat-equation step on the workload's grid, with seeded velocities and "
                          "stresses instead of a solve (profiling runs)")
     ap.add_argument("--restart", type=int, default=16, help="GCR restart length")
+    ap.add_argument("--smoother", type=int, default=1,
+                    help="smoother when --tune-iters 0 (profiling runs; the default run autotunes)")
+    ap.add_argument("--sweep-growth", type=int, default=2, help="sweep growth per level when --tune-iters 0")
+    ap.add_argument("--max-iter", type=int, default=200, help="outer iteration cap (profiling runs)")
     ap.add_argument("--tune-iters", type=int, default=12,
                     help="outer iterations per autotuner trial (run once, before the timed region); 0 = no tuning")
     return ap.parse_args()
@@ -594,7 +598,8 @@ def main():
     m = M.config_model(args.config)
     n = m.nodenum
     big = n > 8_000_000
-    prob = P.StokesProblem(m, device=local, precision=0, tol=1e-8, restart=args.restart)
+    prob = P.StokesProblem(m, device=local, precision=0, tol=1e-8, restart=args.restart, max_iter=args.max_iter,
+                           smoother=args.smoother, sweep_growth=args.sweep_growth)
     if args.heat_only:
         heat = heat_leg(prob, m, args, False, synthetic=True)
         prob.close()
@@ -609,8 +614,8 @@ def main():
         tune = prob.autotune(args.tune_iters)
     else:
         from pardiso2_b200.capi import TuneInfo
-        tune = TuneInfo(smoother=1, sweep_growth=1, est_ms=float("nan"), rate=float("nan"), candidates=0,
-                        trial_iters=0)
+        tune = TuneInfo(smoother=args.smoother, sweep_growth=args.sweep_growth, est_ms=float("nan"),
+                        rate=float("nan"), candidates=0, trial_iters=0, sweep_max=64)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
     def one(p):
@@ -664,7 +669,7 @@ def main():
     # the plain FP64 solve (FP64 GCR, FP64 V-cycle) for comparison; fewer
     # steps on the large grids (each is about a second there)
     p64 = P.StokesProblem(m, device=local, precision=1, tol=1e-8, restart=args.restart, smoother=tune.smoother,
-                          sweep_growth=tune.sweep_growth)
+                          sweep_growth=tune.sweep_growth, sweep_max=tune.sweep_max)
     p64.ctx.upload_markers(m.markx, m.marky, m.markz, m.markt, m.rocks.n0, m.rocks.n1, m.rocks.ro)
     p64.ctx.ronurecalc_resident()
     k64 = min(args.steps, 3) if big else args.steps
@@ -742,7 +747,8 @@ def main():
         "vs_baseline": None, "dtype": "f32 V-cycle / f64 outer GCR", "data": "synthetic",
         "config": config_dict(args.config, m, world),
         "solver": {"smoother": ("full" if tune.smoother else "diagonal") + " cell-block Vanka, autotuned",
-                   "sweeps": "4 pre + 4 post on level 0, x%d per coarser level" % tune.sweep_growth,
+                   "sweeps": "4 pre + 4 post on level 0, x%d per coarser level, at most %d" % (tune.sweep_growth,
+                                                                                                tune.sweep_max),
                    "mixed": "FP64 GCR(%d) (true residual and update in FP64), FP32 V-cycle" % args.restart,
                    "fp64": "FP64 GCR(%d), FP64 V-cycle" % args.restart},
         "converged": all(i.status == 0 for i in infos), "iterations": last.iterations,

@@ -96,11 +96,13 @@ typedef struct {
 /* Choice made by p2_autotune. */
 typedef struct {
     int smoother;        /* chosen p2_params.smoother */
-    int sweep_growth;    /* sweeps on level l = npre[0] * sweep_growth^l (pre and post) */
+    int sweep_growth;    /* sweep growth per coarser level (pre and post), see sweep_max */
     double est_ms;       /* estimated device time of one solve to tol with the choice */
     double rate;         /* measured residual reduction per outer iteration */
     int candidates;      /* configurations tried */
     int trial_iters;     /* outer iterations per trial */
+    int sweep_max;       /* most sweeps on any level: sweeps on level l =
+                            min(sweep_max, npre[0] * sweep_growth^l) */
 } p2_tune_info;
 
 /* Fill p with the reference's defaults (mode.t3c) and this library's. */

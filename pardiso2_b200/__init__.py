@@ -23,7 +23,7 @@ __all__ = ["capi", "model", "Context", "P2Error", "Params", "SolveInfo", "defaul
 
 def params_for(m: "model.Model", precision: int = 0, tol: float = 1e-8, npre=None, npost=None, omega: float = 0.7,
                restart: int = 16, max_iter: int = 200, use_graphs: bool = True, smoother: int = 1,
-               sweep_growth: int = 1) -> Params:
+               sweep_growth: int = 1, sweep_max: int = 64) -> Params:
     """C-ABI parameters for a model (its mode.t3c-equivalent knobs plus solver controls)."""
     p = default_params()
     sp = m.params
@@ -35,8 +35,8 @@ def params_for(m: "model.Model", precision: int = 0, tol: float = 1e-8, npre=Non
     p.multinum = m.multinum
     nl = m.multinum + 1
     for l in range(nl):
-        p.npre[l] = (npre[l] if npre is not None else 4 * sweep_growth ** l)
-        p.npost[l] = (npost[l] if npost is not None else 4 * sweep_growth ** l)
+        p.npre[l] = (npre[l] if npre is not None else min(sweep_max, 4 * sweep_growth ** l))
+        p.npost[l] = (npost[l] if npost is not None else min(sweep_max, 4 * sweep_growth ** l))
     p.tol, p.max_iter, p.precision, p.restart, p.omega = tol, max_iter, precision, restart, omega
     p.use_graphs = 1 if use_graphs else 0
     p.smoother = smoother

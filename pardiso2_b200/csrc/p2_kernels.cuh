@@ -5,6 +5,18 @@
 
 namespace p2 {
 
+// Storage type of the stored cell factors of a V-cycle computing in T (the
+// cycle's own type: bfloat16 factors for the FP32 cycle were measured to cost
+// 26 -> 31 outer iterations at 257^3 for a 1 % faster pass, which is latency-
+// rather than bandwidth-bound).
+template <typename T>
+using factor_t = T;
+
+__device__ __forceinline__ float ld_factor(const float *p) { return __ldg(p); }
+__device__ __forceinline__ double ld_factor(const double *p) { return __ldg(p); }
+template <typename S>
+__device__ __forceinline__ S to_factor(double v) { return (S)v; }
+
 constexpr int kThreads = 256;
 
 // ---------------------------------------------------------------------------
@@ -631,15 +643,15 @@ __global__ void __launch_bounds__(128) k_vanka_factor(LevelView<T> L, int col, S
 #pragma unroll
     for (int a = 0; a < 6; a++)
 #pragma unroll
-        for (int c = a; c < 6; c++) blk[(long)tri_index(a, c) * stride + t] = (S)((T)0.5 * (M[a][c] + M[c][a]));
+        for (int c = a; c < 6; c++) blk[(long)tri_index(a, c) * stride + t] = to_factor<S>((T)0.5 * (M[a][c] + M[c][a]));
     const bool pact = (L.bcm[u] & BC_P) == 0;
-    blk[21L * stride + t] = (S)((pact && den != (T)0) ? (T)1 / den : (T)0);
+    blk[21L * stride + t] = to_factor<S>((pact && den != (T)0) ? (T)1 / den : (T)0);
 }
 
 template <typename T>
 __global__ void __launch_bounds__(128, sizeof(T) == 4 ? P2_STORED_MIN_BLOCKS : 3) k_vanka_stored(
-    LevelView<T> L, T *P, Vec4<T> vin, Vec4<T> vout, Vec4<T> b, T omega, int col, const T *__restrict__ blk,
-    long stride)
+    LevelView<T> L, T *P, Vec4<T> vin, Vec4<T> vout, Vec4<T> b, T omega, int col,
+    const factor_t<T> *__restrict__ blk, long stride)
 {
     pdl_enter();
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -668,7 +680,7 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? P2_STORED_MIN_BLOCKS : 3
     for (int a = 0; a < 6; a++) {
 #pragma unroll
         for (int c = a; c < 6; c++) {
-            const T m = __ldg(blk + (long)tri_index(a, c) * stride + t);
+            const T m = ld_factor(blk + (long)tri_index(a, c) * stride + t);
             y1[a] += m * vr[c];
             y2[a] += m * cc[c];
             if (c != a) {
@@ -677,7 +689,7 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? P2_STORED_MIN_BLOCKS : 3
             }
         }
     }
-    const T inv = __ldg(blk + 21L * stride + t);
+    const T inv = ld_factor(blk + 21L * stride + t);
     T dp = 0;
     if (inv != (T)0) {
         T num = -(b.c[0][u] - div);

@@ -570,7 +570,7 @@ void Solver::allocate_work()
         {
             const long slots = (long)(Lv.nx - 1) * (Lv.nz - 1) * (Lv.ny / 2);
             Lv.blk_stride = (slots + 31) / 32 * 32;
-            const size_t tsz = prm.precision == 0 ? sizeof(float) : sizeof(double);
+            const size_t tsz = prm.precision == 0 ? sizeof(factor_t<float>) : sizeof(factor_t<double>);
             Lv.blk = arena.alloc(tsz * 2 * kBlkEntries * (size_t)Lv.blk_stride);
         }
         if (prm.precision == 1 || l == 0) { v64(Lv.x64); v64(Lv.y64); v64(Lv.b64); v64(Lv.r64); }
@@ -909,7 +909,7 @@ void Solver::smoother_pass(int l, const LevelView<T> &V, T *P, Vec4<T> &vin, Vec
     switch (prm.smoother) {
     case 1:
     case 5: {
-        const T *blk = (const T *)Lv.blk + (size_t)col * kBlkEntries * Lv.blk_stride;
+        const factor_t<T> *blk = (const factor_t<T> *)Lv.blk + (size_t)col * kBlkEntries * Lv.blk_stride;
         pdl_launch(st, nblk(cells, 128), 128, k_vanka_stored<T>, V, P, vin, vout, b, om, col, blk, Lv.blk_stride);
         break;
     }
@@ -930,8 +930,8 @@ void Solver::factor_smoother()
         LevelView<double> V = view<double>(l, false);
         const long cells = (long)(Lv.nx - 1) * (Lv.nz - 1) * (Lv.ny / 2);
         for (int col = 0; col < 2; col++) {
-            T *blk = (T *)Lv.blk + (size_t)col * kBlkEntries * Lv.blk_stride;
-            k_vanka_factor<double, T><<<nblk(cells, 128), 128, 0, st>>>(V, col, blk, Lv.blk_stride); P2_COUNT_LAUNCH();
+            factor_t<T> *blk = (factor_t<T> *)Lv.blk + (size_t)col * kBlkEntries * Lv.blk_stride;
+            k_vanka_factor<double, factor_t<T>><<<nblk(cells, 128), 128, 0, st>>>(V, col, blk, Lv.blk_stride); P2_COUNT_LAUNCH();
         }
     }
     P2_CUDA_TRY(cudaGetLastError());
@@ -975,7 +975,7 @@ void Solver::sweep_fused(int l, const LevelView<T> &V, Vec4<T> &xin, Vec4<T> &xo
     sweep_kernel_setup<T>();
     const int chunk = kSweepChunk;
     dim3 grid((Lv.nx - 1 + kSwTX - 1) / kSwTX, (Lv.ny - 1 + kSwTY - 1) / kSwTY, (Lv.nz - 1 + chunk - 1) / chunk);
-    const T *blk0 = (const T *)Lv.blk, *blk1 = blk0 + (size_t)kBlkEntries * Lv.blk_stride;
+    const factor_t<T> *blk0 = (const factor_t<T> *)Lv.blk, *blk1 = blk0 + (size_t)kBlkEntries * Lv.blk_stride;
     SweepBC bc{Lv.sw_first, Lv.sw_order, Lv.bu, Lv.bt, Lv.bnext, Lv.bk};
 #ifdef P2_NO_PDL
     k_vanka_sweep<T><<<grid, kSwThreads, sweep_smem_bytes<T>(), st>>>(V, xin, xout, b, (T)prm.omega, blk0, blk1,
@@ -1317,17 +1317,19 @@ p2_tune_info Solver::autotune(int trial_iters)
     best.est_ms = INFINITY;
     best.trial_iters = trial_iters;
     double setup_ms = INFINITY;
-    const int smoothers[2] = {1, 0}, growths[2] = {1, 2};
-    for (int a = 0; a < 2; a++)
-        for (int g = 0; g < 2; g++) {
+    // candidates: smoother x (sweep growth per coarser level, most sweeps per level)
+    struct Cand { int smoother, growth, cap; };
+    const Cand cands[6] = {{1, 1, 64}, {1, 2, 64}, {1, 2, 16}, {0, 1, 64}, {0, 2, 64}, {0, 2, 16}};
+    for (const Cand &cd : cands) {
+        {
             prm = saved;
-            prm.smoother = smoothers[a];
+            prm.smoother = cd.smoother;
             prm.max_iter = trial_iters;
             for (int l = 0; l < nl; l++) {
                 long f = 1;
-                for (int q = 0; q < l; q++) f *= growths[g];
-                prm.npre[l] = (int)std::min<long>(64, base_pre * f);
-                prm.npost[l] = (int)std::min<long>(64, base_post * f);
+                for (int q = 0; q < l; q++) f *= cd.growth;
+                prm.npre[l] = (int)std::min<long>(cd.cap, base_pre * f);
+                prm.npost[l] = (int)std::min<long>(cd.cap, base_post * f);
             }
             drop_graphs();
             set_initial(nullptr, nullptr, nullptr, nullptr);
@@ -1348,29 +1350,32 @@ p2_tune_info Solver::autotune(int trial_iters)
             }
             setup_ms = std::min(setup_ms, (double)in.ms_setup);
             if (verbose)
-                std::fprintf(stderr, "p2cuda: autotune smoother %d growth %d: %d its, rate %.3f, est %.1f ms\n",
-                             prm.smoother, growths[g], in.iterations, rate, est);
+                std::fprintf(stderr, "p2cuda: autotune smoother %d growth %d cap %d: %d its, rate %.3f, est %.1f ms\n",
+                             prm.smoother, cd.growth, cd.cap, in.iterations, rate, est);
             best.candidates++;
             if (est < best.est_ms) {
                 best.est_ms = est;
                 best.smoother = prm.smoother;
-                best.sweep_growth = growths[g];
+                best.sweep_growth = cd.growth;
+                best.sweep_max = cd.cap;
                 best.rate = rate;
             }
         }
+    }
     prm = saved;
     if (std::isfinite(best.est_ms) && std::isfinite(setup_ms)) best.est_ms += setup_ms;
     if (!std::isfinite(best.est_ms)) {
         // nothing converged within the trials: keep the defaults
         best.smoother = saved.smoother;
         best.sweep_growth = 1;
+        best.sweep_max = 64;
     } else {
         prm.smoother = best.smoother;
         for (int l = 0; l < nl; l++) {
             long f = 1;
             for (int q = 0; q < l; q++) f *= best.sweep_growth;
-            prm.npre[l] = (int)std::min<long>(64, base_pre * f);
-            prm.npost[l] = (int)std::min<long>(64, base_post * f);
+            prm.npre[l] = (int)std::min<long>(best.sweep_max, base_pre * f);
+            prm.npost[l] = (int)std::min<long>(best.sweep_max, base_post * f);
         }
     }
     drop_graphs();

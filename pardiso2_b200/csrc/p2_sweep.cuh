@@ -163,7 +163,8 @@ __device__ __forceinline__ void cell_rows_acc(const LevelView<T> &L, const Acc &
 // vnew[q] (valid where act[q]) and the new pressure pnew.
 template <typename T, typename Acc>
 __device__ __forceinline__ void vanka_update(const LevelView<T> &L, const Acc &A, int i, int j, int k, int F,
-                                             const uint8_t fm[6], const T *__restrict__ blk, long stride, long t,
+                                             const uint8_t fm[6], const factor_t<T> *__restrict__ blk, long stride,
+                                             long t,
                                              const Vec4<T> &b, T omega, T vnew[6], bool act[6], T &pnew)
 {
     const int sy = L.ny, sz = L.nx * L.ny;
@@ -186,7 +187,7 @@ __device__ __forceinline__ void vanka_update(const LevelView<T> &L, const Acc &A
     for (int a = 0; a < 6; a++) {
 #pragma unroll
         for (int c = a; c < 6; c++) {
-            const T m = __ldg(blk + (long)tri_index(a, c) * stride + t);
+            const T m = ld_factor(blk + (long)tri_index(a, c) * stride + t);
             y1[a] += m * vr[c];
             y2[a] += m * cc[c];
             if (c != a) {
@@ -195,7 +196,7 @@ __device__ __forceinline__ void vanka_update(const LevelView<T> &L, const Acc &A
             }
         }
     }
-    const T inv = __ldg(blk + 21L * stride + t);
+    const T inv = ld_factor(blk + 21L * stride + t);
     const T pold = A.v(0, 1, 1, 1);
     T dp = 0;
     pnew = pold;
@@ -226,8 +227,8 @@ __device__ __forceinline__ long colour_slot(int nx, int ny, int i, int j, int k)
 // colour 0 ((i + j + k) even), black colour 1.
 template <typename T>
 __global__ void __launch_bounds__(kSwThreads) k_vanka_sweep(LevelView<T> L, Vec4<T> xin, Vec4<T> xout, Vec4<T> b,
-                                                           T omega, const T *__restrict__ blk0,
-                                                           const T *__restrict__ blk1, long stride, SweepBC bc,
+                                                           T omega, const factor_t<T> *__restrict__ blk0,
+                                                           const factor_t<T> *__restrict__ blk1, long stride, SweepBC bc,
                                                            int chunk)
 {
     pdl_enter();
