@@ -322,6 +322,42 @@ p2_status p2_titerate(p2_ctx *ctx, const p2_heat_params *hp, double timestep, fl
                       long marknum, const float *markx, const float *marky, const float *markz,
                       const signed char *markt, float *markk, p2_heat_info *info);
 
+/* The reference's binary model file (.prn), the branch of loader() and
+ * saver() that needs no HDF5: pardiso/load3mg.c:745-905 (read) and
+ * 1298-1443 (write).  Host code only (no device, no context).  The file holds
+ * the writer's sizeof(int/long/float/double) in its first four bytes; a file
+ * written with other sizes is refused, as the reference refuses it.  Arrays
+ * keep the file's layout; p2_prn_read_header gives the sizes to allocate. */
+typedef struct {
+    long xnumx, ynumy, znumz;   /* nodes per axis */
+    long mnumx, mnumy, mnumz;   /* markers per cell (the generator's counts) */
+    double xsize, ysize, zsize;
+    long pxinit, pyinit, pzinit;
+    double pinit, gxkoef, gykoef, gzkoef;
+    int rocknum;
+    long bondnum, marknum;
+    int cycle;                  /* the saver's cycle number n0 */
+    double timesum_years;       /* timesum / 3.15576e7 as stored; the reference multiplies it back */
+    double gridcur, gridtot;
+} p2_prn_header;
+typedef struct {
+    double *rocks;         /* 24 * rocknum: markn0 markn1 marks0 marks1 marknu markdh markdv markss
+                              markmm markll marka0 marka1 markb0 markb1 marke0 marke1 markro markbb
+                              markaa markcp markkt markkf markkp markht, one table after another */
+    float *nodes;          /* 11 per node (node order of the grid): pr vx vy vz ro nu tk cp et kt ht */
+    float *gx, *gy, *gz;   /* gridlines (float in the file) */
+    long *bond_index;      /* bondnum: the bondm index of the row (4 * node + unknown, or
+                              8 * nodenum + node for a temperature row) */
+    long *bond_row;        /* bondnum: the row number (the value of bondm there) */
+    float *bond_value;     /* 2 * bondnum: bondv1 const, koef */
+    long *bond_target;     /* bondnum: bondn1 of the row (1 + coupled unknown, 0 none) */
+    float *markers;        /* 7 per marker: x y z markk markw markd marke */
+    signed char *markt;    /* marknum types */
+} p2_prn_data;
+p2_status p2_prn_read_header(const char *path, p2_prn_header *h, char *err, long errlen);
+p2_status p2_prn_read(const char *path, const p2_prn_header *h, const p2_prn_data *d, char *err, long errlen);
+p2_status p2_prn_write(const char *path, const p2_prn_header *h, const p2_prn_data *d, char *err, long errlen);
+
 /* The p2_ronurecalc interpolation for callers that cannot allocate device
  * memory: a host code whose device memory is all handed out by its own pool
  * at start-up, or one that cannot take the device-wide synchronisation that

@@ -714,6 +714,55 @@ static void heat_arrays(void)
     }
 }
 
+/* saver() (load3mg.c:1275-1443) in its binary branch (fl1otp 1) to `path`
+ * (shorter than fl1out's 60 characters): the harness's node fields, with tk,
+ * cp, et, kt, ht (level 0) and the markers' markk, markw, markd, marke set
+ * from the arguments first, the gridlines, the boundary rows, the rock table
+ * and the markers.  Returns -1 when the path is too long. */
+int p2ref_save(const char *path, int cycle, const float *itk, const float *icp, const float *iet, const float *ikt,
+               const float *iht, const float *imk, const float *imw, const float *imd, const float *ime)
+{
+    if (strlen(path) >= sizeof(fl1out)) return -1;
+    heat_arrays();
+    /* saver() scans bondm[0 .. 10 * nodenum) (load3mg.c:1399-1400) while
+     * dynmemall() allocates mcmax + 8 * nodenum entries (load3mg.c:2250):
+     * the stock program reads past the array.  The harness extends it with
+     * zeros so that the scan stays in bounds (every row index is below
+     * 8 * nodenum + mcmax, so the extension adds no row). */
+    {
+        long mcmax = mgp[multinum] + mgn[multinum], have = mcmax + nodenum8, need = nodenum * 10;
+        if (need > have) {
+            int *nb = (int *)realloc(bondm, sizeof(int) * (size_t)need);
+            if (!nb) return -2;
+            memset(nb + have, 0, sizeof(int) * (size_t)(need - have));
+            bondm = nb;
+        }
+    }
+    memcpy(tk, itk, sizeof(float) * (size_t)nodenum);
+    memcpy(cp, icp, sizeof(float) * (size_t)nodenum);
+    memcpy(et, iet, sizeof(float) * (size_t)nodenum);
+    memcpy(kt, ikt, sizeof(float) * (size_t)nodenum);
+    memcpy(ht, iht, sizeof(float) * (size_t)nodenum);
+    memcpy(markk, imk, sizeof(float) * (size_t)marknum);
+    memcpy(markw, imw, sizeof(float) * (size_t)marknum);
+    memcpy(markd, imd, sizeof(float) * (size_t)marknum);
+    memcpy(marke, ime, sizeof(float) * (size_t)marknum);
+    strcpy(fl1out, path);
+    fl1otp = 1;
+    /* saver() ends by reading stop.yn from the working directory
+     * (load3mg.c:1744-1761), which loadconf() creates in the stock program */
+    {
+        FILE *sf = fopen("stop.yn", "wt");
+        if (!sf) return -3;
+        fprintf(sf, "n\n");
+        fclose(sf);
+    }
+    mute();
+    saver(0, cycle);
+    unmute();
+    return 0;
+}
+
 /* T boundary rows: bondm[nodenum8 + u] for the nodes u of every level
  * (in3mg.c:367-383); the rows themselves come with p2ref_set_bc. */
 void p2ref_set_tbc(const int *bt)

@@ -82,6 +82,8 @@ def _load(shim: bool = False) -> C.CDLL:
         lib.p2ref_set_tbc.argtypes = [_ip]
         lib.p2ref_set_stress.argtypes = [C.POINTER(C.c_void_p)]
         lib.p2ref_titerate.argtypes = [_dp, _ip, _fp, _fp, _fp, _fp, _fp, C.c_void_p, _fp, _dp]
+        lib.p2ref_save.argtypes = [C.c_char_p, C.c_int] + [_fp] * 9
+        lib.p2ref_save.restype = C.c_int
         lib.p2ref_lu_count.restype = C.c_int
         lib.p2ref_num_threads.restype = C.c_int
         _libs[path] = lib
@@ -307,6 +309,18 @@ class RefModel:
 
 
     # -- heat equation ------------------------------------------------------
+    def save_prn(self, path: str, cycle: int, tk, cp, et, kt, ht, markk, markw, markd, marke):
+        """The reference's saver() in its binary branch (load3mg.c:1275) to
+        path (under 60 characters): the harness's node fields with the given
+        thermal fields (level 0) and marker properties."""
+        f = lambda a: np.ascontiguousarray(a, np.float32)
+        st = self.lib.p2ref_save(path.encode(), cycle, f(tk), f(cp), f(et), f(kt), f(ht), f(markk), f(markw), f(markd),
+                                 f(marke))
+        if st == -1:
+            raise ValueError("path too long for the reference's file-name buffer: %s" % path)
+        if st:
+            raise MemoryError("could not extend the reference's bondm array")
+
     def set_tbc(self, bc):
         """Boundary tables including the temperature rows (model.BCTables with
         bondt): the Stokes rows and the shared row table, then the T section."""

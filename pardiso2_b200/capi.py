@@ -24,7 +24,8 @@ EXPORTED = ["p2_default_params", "p2_create", "p2_destroy", "p2_last_error", "p2
             "p2_debug_time_sweep", "p2_ronurecalc_noalloc", "p2_autotune",
             "p2_movemark", "p2_movemark_resident", "p2_get_markers", "p2_stress_strain",
             "p2_stokes_solve_batch", "p2_movemark_strain", "p2_ronurecalc_powerlaw", "p2_effbulk_visc",
-            "p2_default_heat_params", "p2_heat_set_bc", "p2_titerate"]
+            "p2_default_heat_params", "p2_heat_set_bc", "p2_titerate", "p2_prn_read_header", "p2_prn_read",
+            "p2_prn_write"]
 
 
 class Params(C.Structure):
