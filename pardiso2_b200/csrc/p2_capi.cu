@@ -109,8 +109,8 @@ p2_status p2_set_grid(p2_ctx *ctx, long xnumx, long ynumy, long znumz, const dou
             throw p2::Error(P2_ERR_UNSUPPORTED, "periodic boundaries are not supported");
         if (prm->precision != 0 && prm->precision != 1) throw p2::Error(P2_ERR_ARG, "precision must be 0 or 1");
         if (!(prm->omega > 0 && prm->omega < 2)) throw p2::Error(P2_ERR_ARG, "omega must be in (0, 2)");
-        if (prm->smoother < 0 || prm->smoother > 5 || prm->smoother == 4)
-            throw p2::Error(P2_ERR_ARG, "smoother must be 0, 1, 2, 3 or 5");
+        if (prm->smoother < 0 || prm->smoother > 6 || prm->smoother == 4)
+            throw p2::Error(P2_ERR_ARG, "smoother must be 0, 1, 2, 3, 5 or 6");
         if (!(prm->tol > 0)) throw p2::Error(P2_ERR_ARG, "tol must be positive");
         if (!(prm->nubeg > 0) || !(prm->nuend >= prm->nubeg)) throw p2::Error(P2_ERR_ARG, "bad nubeg/nuend");
         P2_CUDA_TRY(cudaSetDevice(ctx->s->dev));

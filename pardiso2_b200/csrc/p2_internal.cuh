@@ -96,10 +96,12 @@ struct LevelView {
     int pin;                            // pinned pressure cell node, -1 if none
 };
 
+// Plain loads (not __ldg): the row functions below also run on level views
+// whose arrays are shared-memory copies of a brick (k_rows_tiled).
 template <typename T>
 __device__ __forceinline__ T eta_at(const LevelView<T> &L, const float *a, int i)
 {
-    T v = (T)__ldg(a + i);
+    T v = (T)a[i];
     if (L.do_clamp) {
         if (v > (T)L.clamp_hi) v = (T)L.clamp_hi;
         if (v < (T)L.clamp_lo) v = (T)L.clamp_lo;
@@ -116,7 +118,7 @@ struct Fields {
 template <typename T, typename S>
 __device__ __forceinline__ T ld(const S *a, int i)
 {
-    return (T)__ldg(a + i);
+    return (T)a[i];
 }
 
 #define P2IDX(L, i, j, k) ((k) * ((L).nx * (L).ny) + (i) * (L).ny + (j))

@@ -731,6 +731,8 @@ __device__ __forceinline__ AxisMap pick_map(const AxisMap (&m)[3], int type)
 // continuity rows into partial[block]; the last block to finish (ticket
 // counter, reset by that block) sums the partials in block order and writes
 // sums[0] = sum of vol * b_P and sums[1] = vol_total (fixed per level).
+constexpr int kRestrictList = 5;  // longest inverse list of one axis (host-checked)
+
 template <typename T>
 __global__ void k_restrict_compat(LevelView<T> F, Vec4<T> rf, LevelView<T> Cl, Vec4<T> bc, Vec4<T> xc,
                                   TransferView tv, int scale_p, double vol_total, double *partial,
@@ -755,21 +757,37 @@ __global__ void k_restrict_compat(LevelView<T> F, Vec4<T> rf, LevelView<T> Cl, V
                           mz = pick_map(tv.m[2], ax_type(c, 2));
             T acc = 0, ws = 0;
             const T etac = c == 0 ? (T)Cl.ec[v] : (T)1;
-            const int x0 = mx.ptr[I], x1 = mx.ptr[I + 1], y0 = my.ptr[J], y1 = my.ptr[J + 1];
+            const int x0 = mx.ptr[I], nxq = mx.ptr[I + 1] - x0, y0 = my.ptr[J], nyq = my.ptr[J + 1] - y0;
             const T *rfc = comp(rf);
+            // the x and y lists (at most kRestrictList entries each, checked on
+            // the host) in registers, the x and y loops unrolled with fixed trip
+            // counts: the fine-node loads of one z line are independent of each
+            // other, so they are issued together rather than one after another
+            int xi[kRestrictList], yi[kRestrictList];
+            T xw[kRestrictList], yw[kRestrictList];
+#pragma unroll
+            for (int a = 0; a < kRestrictList; a++) {
+                xi[a] = a < nxq ? mx.idx[x0 + a] : 0;
+                xw[a] = a < nxq ? (T)mx.w[x0 + a] : (T)0;
+                yi[a] = a < nyq ? my.idx[y0 + a] : 0;
+                yw[a] = a < nyq ? (T)my.w[y0 + a] : (T)0;
+            }
             for (int qz = mz.ptr[K]; qz < mz.ptr[K + 1]; qz++) {
                 const int fk = mz.idx[qz];
                 const T wz = (T)mz.w[qz];
-                for (int qx = x0; qx < x1; qx++) {
-                    const int fi = mx.idx[qx];
-                    const T wzx = wz * (T)mx.w[qx];
-                    const int base = fk * (F.nx * F.ny) + fi * F.ny;
-                    for (int qy = y0; qy < y1; qy++) {
-                        const int f = base + my.idx[qy];
-                        if (F.bcm[f] & (1 << c)) continue;
-                        const T w = wzx * (T)my.w[qy];
-                        T val = rfc[f];
-                        if (c == 0 && scale_p) val *= (T)F.ec[f] / etac;
+#pragma unroll
+                for (int ax = 0; ax < kRestrictList; ax++) {
+                    if (ax >= nxq) break;
+                    const T wzx = wz * xw[ax];
+                    const int base = fk * (F.nx * F.ny) + xi[ax] * F.ny;
+#pragma unroll
+                    for (int ay = 0; ay < kRestrictList; ay++) {
+                        if (ay >= nyq) break;
+                        const int f = base + yi[ay];
+                        if (__ldg(F.bcm + f) & (1 << c)) continue;
+                        const T w = wzx * yw[ay];
+                        T val = __ldg(rfc + f);
+                        if (c == 0 && scale_p) val *= (T)__ldg(F.ec + f) / etac;
                         acc += val * w;
                         ws += w;
                     }
@@ -977,28 +995,51 @@ __device__ __forceinline__ double block_sum(double v, double *sh)
 // One sweep over the nodes for all pairs: a vector shared by several pairs
 // (the new direction against every stored one) comes from DRAM once and is
 // re-read from L1.
+// ND, the number of pairs, is a template parameter: the accumulators stay in
+// registers whatever ND is, and the node loop is unrolled so that each thread
+// has several independent loads in flight (one load at a time per thread left
+// the sweep latency-bound at a fraction of the HBM bandwidth).
+template <int ND>
 __global__ void k_dots_partial(DotJobs jobs, int n, int skip_node, double *partial)
 {
     __shared__ double sh[32];
-    double s[kMaxDots];
+    double s[ND];
 #pragma unroll
-    for (int q = 0; q < kMaxDots; q++) s[q] = 0;
+    for (int q = 0; q < ND; q++) s[q] = 0;
+    const int stride = gridDim.x * blockDim.x;
 #pragma unroll
     for (int c = 0; c < 4; c++) {
-        for (int u = blockIdx.x * blockDim.x + threadIdx.x; u < n; u += gridDim.x * blockDim.x) {
+        const double *a[ND], *b[ND];
+#pragma unroll
+        for (int q = 0; q < ND; q++) { a[q] = jobs.j[q].a[c]; b[q] = jobs.j[q].b[c]; }
+#pragma unroll 4
+        for (int u = blockIdx.x * blockDim.x + threadIdx.x; u < n; u += stride) {
             if (c == 0 && u == skip_node) continue;
 #pragma unroll
-            for (int q = 0; q < kMaxDots; q++)
-                if (q < jobs.nd) s[q] += jobs.j[q].a[c][u] * jobs.j[q].b[c][u];
+            for (int q = 0; q < ND; q++) s[q] += __ldg(a[q] + u) * __ldg(b[q] + u);
         }
     }
 #pragma unroll
-    for (int q = 0; q < kMaxDots; q++) {
-        if (q < jobs.nd) {  // uniform over the block: the barriers in block_sum are safe
-            const double t = block_sum(s[q], sh);
-            if (threadIdx.x == 0) partial[q * gridDim.x + blockIdx.x] = t;
-        }
+    for (int q = 0; q < ND; q++) {
+        const double t = block_sum(s[q], sh);
+        if (threadIdx.x == 0) partial[q * gridDim.x + blockIdx.x] = t;
     }
+}
+
+// k_dots_partial<jobs.nd> on kRedBlocks blocks of kThreads threads
+inline cudaError_t launch_dots(cudaStream_t st, const DotJobs &jobs, int n, int skip_node, double *partial)
+{
+    switch (jobs.nd) {
+#define P2_DOTS_CASE(N) \
+    case N: k_dots_partial<N><<<kRedBlocks, kThreads, 0, st>>>(jobs, n, skip_node, partial); break;
+        P2_DOTS_CASE(1) P2_DOTS_CASE(2) P2_DOTS_CASE(3) P2_DOTS_CASE(4) P2_DOTS_CASE(5) P2_DOTS_CASE(6)
+        P2_DOTS_CASE(7) P2_DOTS_CASE(8) P2_DOTS_CASE(9) P2_DOTS_CASE(10) P2_DOTS_CASE(11) P2_DOTS_CASE(12)
+        P2_DOTS_CASE(13) P2_DOTS_CASE(14) P2_DOTS_CASE(15) P2_DOTS_CASE(16) P2_DOTS_CASE(17) P2_DOTS_CASE(18)
+        P2_DOTS_CASE(19) P2_DOTS_CASE(20)
+#undef P2_DOTS_CASE
+    default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
 }
 
 __global__ void k_dots_final(int nd, int nparts, const double *partial, double *out)

@@ -23,6 +23,7 @@
 #include "p2_kernels.cuh"
 #include "p2_solver.h"
 #include "p2_sweep.cuh"
+#include "p2_tiled.cuh"
 
 namespace p2 {
 
@@ -189,8 +190,12 @@ static V *upload(DeviceArena &A, const std::vector<V> &h)
     return d;
 }
 
-static AxisMap upload_axis(DeviceArena &A, const HostAxis &h)
+static AxisMap upload_axis(DeviceArena &A, const HostAxis &h, bool restriction = false)
 {
+    for (size_t I = 0; restriction && I + 1 < h.ptr.size(); I++)
+        if (h.ptr[I + 1] - h.ptr[I] > kRestrictList)
+            throw Error(P2_ERR_UNSUPPORTED, "restriction list longer than " + std::to_string(kRestrictList) +
+                                                " fine nodes (grid coarsening not by factors of about 2)");
     AxisMap m;
     m.lo = upload(A, h.lo);
     m.w0 = upload(A, h.w0);
@@ -369,7 +374,7 @@ void Solver::set_grid(long nx, long ny, long nz, const double *gx, const double 
             for (int t = 0; t < 3; t++) {
                 HostAxis h;
                 axis_table(F.g[q], Cl.g[q], t, h);
-                F.tv.m[q][t] = upload_axis(grid_arena, h);
+                F.tv.m[q][t] = upload_axis(grid_arena, h, true);
             }
             HostAxis hr;
             axis_table_ronu(F.g[q], Cl.g[q], hr);
@@ -899,6 +904,87 @@ Vec4<float> &r_of<float>(Level &Lv) { return Lv.r32; }
 template <>
 Vec4<double> &r_of<double>(Level &Lv) { return Lv.r64; }
 
+// Levels at least this large run the shared-memory-staged colour pass
+// (smoother 6); smaller ones are latency-bound either way.
+constexpr long kTileMinNodes = 1L << 20;
+
+template <typename T>
+static void tiled_kernel_setup()
+{
+    static bool done = false;  // per instantiation, per process (the attribute is per function)
+    if (!done) {
+        P2_CUDA_TRY(cudaFuncSetAttribute(k_vanka_tiled<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)tile_smem_bytes<T>()));
+        done = true;
+    }
+}
+
+// Residual / operator rows on a level (k_rows, or k_rows_tiled on levels of
+// at least kTileMinNodes nodes): out = b - A x (mode 0) or A x (mode 1).
+template <typename T, typename S>
+static void launch_rows(cudaStream_t st, bool pdl, const LevelView<T> &V, const Fields<T, S> &f, const Vec4<T> &b,
+                        Vec4<T> &out, const Vec4<float> &o32, int mode)
+{
+    if (V.n < kTileMinNodes) {
+        if (pdl) pdl_launch(st, nblk(V.n), kThreads, k_rows<T, S>, V, f, b, out, o32, mode);
+        else {
+            k_rows<T, S><<<nblk(V.n), kThreads, 0, st>>>(V, f, b, out, o32, mode);
+            P2_COUNT_LAUNCH();
+        }
+        return;
+    }
+    using RT = RowTile<S>;
+    static bool attr_done = false;  // per instantiation
+    if (!attr_done) {
+        P2_CUDA_TRY(cudaFuncSetAttribute(k_rows_tiled<T, S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)RT::smem));
+        attr_done = true;
+    }
+    dim3 grid((V.nx + RT::TX - 1) / RT::TX, (V.ny + RT::TY - 1) / RT::TY, (V.nz + RT::TZ - 1) / RT::TZ);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = dim3(kTileThreads);
+    cfg.dynamicSmemBytes = RT::smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = pdl ? 1 : 0;
+    P2_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_rows_tiled<T, S>, V, f, b, out, o32, mode));
+    P2_COUNT_LAUNCH();
+}
+
+// One colour pass with the brick staged in shared memory (k_vanka_tiled).
+template <typename T>
+void Solver::tiled_pass(int l, const LevelView<T> &V, T *P, Vec4<T> &vin, Vec4<T> &vout, Vec4<T> &b, int col)
+{
+    Level &Lv = L[l];
+    tiled_kernel_setup<T>();
+    constexpr int TX = TileShape<T>::TX, TY = TileShape<T>::TY, TZ = TileShape<T>::TZ;
+    dim3 grid((Lv.nx - 1 + TX - 1) / TX, (Lv.ny - 1 + TY - 1) / TY, (Lv.nz - 1 + TZ - 1) / TZ);
+    const factor_t<T> *blk = (const factor_t<T> *)Lv.blk + (size_t)col * kBlkEntries * Lv.blk_stride;
+    const T om = (T)prm.omega;
+#ifdef P2_NO_PDL
+    k_vanka_tiled<T><<<grid, kTileThreads, tile_smem_bytes<T>(), st>>>(V, P, vin, vout, b, om, col, blk,
+                                                                      Lv.blk_stride);
+    P2_COUNT_LAUNCH();
+#else
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = dim3(kTileThreads);
+    cfg.dynamicSmemBytes = tile_smem_bytes<T>();
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    P2_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_vanka_tiled<T>, V, P, vin, vout, b, om, col, blk, Lv.blk_stride));
+    P2_COUNT_LAUNCH();
+#endif
+}
+
 // One colour pass of the selected smoother on level l.
 template <typename T>
 void Solver::smoother_pass(int l, const LevelView<T> &V, T *P, Vec4<T> &vin, Vec4<T> &vout, Vec4<T> &b, int col)
@@ -907,6 +993,12 @@ void Solver::smoother_pass(int l, const LevelView<T> &V, T *P, Vec4<T> &vin, Vec
     const long cells = (long)(Lv.nx - 1) * (Lv.nz - 1) * (Lv.ny / 2);
     const T om = (T)prm.omega;
     switch (prm.smoother) {
+    case 6:
+        if (Lv.n >= kTileMinNodes) {
+            tiled_pass<T>(l, V, P, vin, vout, b, col);
+            break;
+        }
+        // fall through: small levels take the plain pass
     case 1:
     case 5: {
         const factor_t<T> *blk = (const factor_t<T> *)Lv.blk + (size_t)col * kBlkEntries * Lv.blk_stride;
@@ -939,7 +1031,7 @@ void Solver::factor_smoother()
 
 void Solver::factor_cells()
 {
-    if (prm.smoother != 1 && prm.smoother != 5) return;
+    if (prm.smoother != 1 && prm.smoother != 5 && prm.smoother != 6) return;
     if (prm.precision == 0) factor_smoother<float>();
     else factor_smoother<double>();
 }
@@ -1047,7 +1139,7 @@ void Solver::level_residual(int l)
     Vec4<T> &x = vx_of<T>(Lv, 0), &b = b_of<T>(Lv), &r = r_of<T>(Lv);
     Fields<T, T> f{x.c[0], x.c[1], x.c[2], x.c[3]};
     Vec4<float> none;
-    pdl_launch(st, nblk(Lv.n), kThreads, k_rows<T, T>, V, f, b, r, none, 0);
+    launch_rows<T, T>(st, true, V, f, b, r, none, 0);
     if (Lv.nbc)
         pdl_launch(st, nblk(Lv.nbc), kThreads, k_bc_rows<T, T>, Lv.nbc, (const int *)Lv.bu, (const int *)Lv.bt,
                    (const float *)Lv.bk, f, b, r, none, 0);
@@ -1116,7 +1208,7 @@ void Solver::upload_nodes(const float *nu, const float *ro, const float *nxx, co
 
 void Solver::dots_sync(const DotJobs &jobs)
 {
-    k_dots_partial<<<kRedBlocks, kThreads, 0, st>>>(jobs, L[0].n, L[0].pin, partial); P2_COUNT_LAUNCH();
+    P2_CUDA_TRY(launch_dots(st, jobs, L[0].n, L[0].pin, partial)); P2_COUNT_LAUNCH();
     k_dots_final<<<1, 1024, 0, st>>>(jobs.nd, kRedBlocks, partial, dots); P2_COUNT_LAUNCH();
     P2_CUDA_TRY(cudaMemcpyAsync(hdots.get(), dots, sizeof(double) * jobs.nd, cudaMemcpyDeviceToHost, st));
     P2_CUDA_TRY(cudaStreamSynchronize(st));
@@ -1136,7 +1228,7 @@ void Solver::rows0(const Vec4<double> &x, Vec4<double> &out, Vec4<float> *r32, i
     LevelView<double> V = view<double>(0, true);
     Fields<double, double> f{x.c[0], x.c[1], x.c[2], x.c[3]};
     Vec4<float> o32 = r32 ? *r32 : Vec4<float>();
-    k_rows<double, double><<<nblk(L0.n), kThreads, 0, st>>>(V, f, gb, out, o32, mode); P2_COUNT_LAUNCH();
+    launch_rows<double, double>(st, false, V, f, gb, out, o32, mode);
     if (L0.nbc)
         k_bc_rows<double, double><<<nblk(L0.nbc), kThreads, 0, st>>>(L0.nbc, L0.bu, L0.bt, L0.bk, f, gb, out, o32,
                                                                    mode); P2_COUNT_LAUNCH();
@@ -1509,7 +1601,7 @@ void Solver::debug_apply(int l, const double *x, double *y)
     LevelView<double> V = view<double>(l, l == 0);
     Fields<double, double> f{X.v.c[0], X.v.c[1], X.v.c[2], X.v.c[3]};
     Vec4<float> none;
-    k_rows<double, double><<<nblk(Lv.n), kThreads, 0, st>>>(V, f, B.v, Y.v, none, 1); P2_COUNT_LAUNCH();
+    launch_rows<double, double>(st, false, V, f, B.v, Y.v, none, 1);
     if (Lv.nbc)
         k_bc_rows<double, double><<<nblk(Lv.nbc), kThreads, 0, st>>>(Lv.nbc, Lv.bu, Lv.bt, Lv.bk, f, B.v, Y.v, none, 1); P2_COUNT_LAUNCH();
     P2_CUDA_TRY(cudaGetLastError());

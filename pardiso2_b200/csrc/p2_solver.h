@@ -206,6 +206,8 @@ class Solver {
     void smoother_pass(int l, const LevelView<T> &V, T *P, Vec4<T> &vin, Vec4<T> &vout, Vec4<T> &b, int col);
     bool use_fused(int l) const;
     template <typename T>
+    void tiled_pass(int l, const LevelView<T> &V, T *P, Vec4<T> &vin, Vec4<T> &vout, Vec4<T> &b, int col);
+    template <typename T>
     void sweep_fused(int l, const LevelView<T> &V, Vec4<T> &xin, Vec4<T> &xout, Vec4<T> &b);
     template <typename T>
     void factor_smoother();

@@ -60,7 +60,15 @@ struct SweepBC {
 
 __device__ __forceinline__ int sw_ring(int p) { return (p + 4 * kSwRing) % kSwRing; }
 
-// unknowns read from global memory, addressed from the cell's low corner F
+// per-stencil viscosity field f (0 ec, 1 exy, 2 exz, 3 eyz) of a level
+template <typename T>
+__device__ __forceinline__ const float *eta_field(const LevelView<T> &L, int f)
+{
+    return f == 0 ? L.ec : (f == 1 ? L.exy : (f == 2 ? L.exz : L.eyz));
+}
+
+// unknowns read from global memory, addressed from the cell's low corner F;
+// viscosities from global memory
 template <typename T>
 struct GlobalAcc {
     const T *c[4];
@@ -69,25 +77,36 @@ struct GlobalAcc {
     {
         return __ldg(c[comp] + F + dx * sy + dy + dz * sz);
     }
+    __device__ __forceinline__ T eta(const LevelView<T> &L, int f, int dx, int dy, int dz) const
+    {
+        return eta_at(L, eta_field(L, f), F + dx * sy + dy + dz * sz);
+    }
 };
 
-// unknowns read from the shared ring: F at region coordinates (fx, fy), plane fz
+// unknowns read from the shared ring: F at region coordinates (fx, fy), plane
+// fz (F itself is the node index of the cell's low corner); viscosities from
+// global memory
 template <typename T>
 struct RingAcc {
     const T *B;
     int fx, fy, fz;
+    int F, sy, sz;
     __device__ __forceinline__ T v(int comp, int dx, int dy, int dz) const
     {
         return B[((sw_ring(fz + dz) * 4 + comp) * kSwRX + fx + dx) * kSwRY + fy + dy];
     }
+    __device__ __forceinline__ T eta(const LevelView<T> &L, int f, int dx, int dy, int dz) const
+    {
+        return eta_at(L, eta_field(L, f), F + dx * sy + dy + dz * sz);
+    }
 };
 
-// cell_rows with the unknowns taken from an accessor (same terms and order)
+// cell_rows with the unknowns and the viscosities taken from an accessor
+// (same terms and order)
 template <typename T, typename Acc>
-__device__ __forceinline__ void cell_rows_acc(const LevelView<T> &L, const Acc &A, int i, int j, int k, int F,
-                                              T ax[6], T &div)
+__device__ __forceinline__ void cell_rows_acc(const LevelView<T> &L, const Acc &A, int i, int j, int k, T ax[6],
+                                              T &div)
 {
-    const int sy = L.ny, sz = L.nx * L.ny;
     const T vx0 = A.v(1, 0, 0, 0), vxX = A.v(1, 1, 0, 0), vxXX = A.v(1, 2, 0, 0), vxm = A.v(1, -1, 0, 0);
     const T vxY = A.v(1, 0, 1, 0), vxy_ = A.v(1, 0, -1, 0), vxXY = A.v(1, 1, 1, 0), vxXy = A.v(1, 1, -1, 0);
     const T vxZ = A.v(1, 0, 0, 1), vxz_ = A.v(1, 0, 0, -1), vxXZ = A.v(1, 1, 0, 1), vxXz = A.v(1, 1, 0, -1);
@@ -101,50 +120,49 @@ __device__ __forceinline__ void cell_rows_acc(const LevelView<T> &L, const Acc &
     const T hx0 = L.ax.ih[i - 1], hx1 = L.ax.ih[i], hx2 = L.ax.ih[i + 1];
     const T hy0 = L.ay.ih[j - 1], hy1 = L.ay.ih[j], hy2 = L.ay.ih[j + 1];
     const T hz0 = L.az.ih[k - 1], hz1 = L.az.ih[k], hz2 = L.az.ih[k + 1];
-    const int u = F + sz + sy + 1;
     const T exx = (vxX - vx0) * hx1, eyy = (vyY - vy0) * hy1, ezz = (vzZ - vz0) * hz1;
     div = exx + eyy + ezz;
-    const T E2 = two * eta_at(L, L.ec, u);
+    const T E2 = two * A.eta(L, 0, 1, 1, 1);
     const T s0 = E2 * (exx - div * third), s1 = E2 * (eyy - div * third), s2 = E2 * (ezz - div * third);
     T sL, sR, sF, sB, sD, sU;
     {
         const T a = (vx0 - vxm) * hx0, b = (vyxY - vyx_) * hy1, c = (vzxZ - vzx_) * hz1;
-        sL = two * eta_at(L, L.ec, u - sy) * (a - (a + b + c) * third);
+        sL = two * A.eta(L, 0, 0, 1, 1) * (a - (a + b + c) * third);
     }
     {
         const T a = (vxXX - vxX) * hx2, b = (vyXY - vyX) * hy1, c = (vzXZ - vzX) * hz1;
-        sR = two * eta_at(L, L.ec, u + sy) * (a - (a + b + c) * third);
+        sR = two * A.eta(L, 0, 2, 1, 1) * (a - (a + b + c) * third);
     }
     {
         const T a = (vxXy - vxy_) * hx1, b = (vy0 - vym) * hy0, c = (vzyZ - vzy_) * hz1;
-        sF = two * eta_at(L, L.ec, u - 1) * (b - (a + b + c) * third);
+        sF = two * A.eta(L, 0, 1, 0, 1) * (b - (a + b + c) * third);
     }
     {
         const T a = (vxXY - vxY) * hx1, b = (vyYY - vyY) * hy2, c = (vzYZ - vzY) * hz1;
-        sB = two * eta_at(L, L.ec, u + 1) * (b - (a + b + c) * third);
+        sB = two * A.eta(L, 0, 1, 2, 1) * (b - (a + b + c) * third);
     }
     {
         const T a = (vxXz - vxz_) * hx1, b = (vyYz - vyz_) * hy1, c = (vz0 - vzm) * hz0;
-        sD = two * eta_at(L, L.ec, u - sz) * (c - (a + b + c) * third);
+        sD = two * A.eta(L, 0, 1, 1, 0) * (c - (a + b + c) * third);
     }
     {
         const T a = (vxXZ - vxZ) * hx1, b = (vyYZ - vyZ) * hy1, c = (vzZZ - vzZ) * hz2;
-        sU = two * eta_at(L, L.ec, u + sz) * (c - (a + b + c) * third);
+        sU = two * A.eta(L, 0, 1, 1, 2) * (c - (a + b + c) * third);
     }
     const T ex0 = L.ax.ihe[i - 1], ex1 = L.ax.ihe[i], ey0 = L.ay.ihe[j - 1], ey1 = L.ay.ihe[j];
     const T ez0 = L.az.ihe[k - 1], ez1 = L.az.ihe[k];
-    const T xy00 = two * eta_at(L, L.exy, F) * ((vx0 - vxy_) * ey0 + (vy0 - vyx_) * ex0);
-    const T xy01 = two * eta_at(L, L.exy, F + 1) * ((vxY - vx0) * ey1 + (vyY - vyxY) * ex0);
-    const T xy10 = two * eta_at(L, L.exy, F + sy) * ((vxX - vxXy) * ey0 + (vyX - vy0) * ex1);
-    const T xy11 = two * eta_at(L, L.exy, F + sy + 1) * ((vxXY - vxX) * ey1 + (vyXY - vyY) * ex1);
-    const T xz00 = two * eta_at(L, L.exz, F) * ((vx0 - vxz_) * ez0 + (vz0 - vzx_) * ex0);
-    const T xz01 = two * eta_at(L, L.exz, F + sz) * ((vxZ - vx0) * ez1 + (vzZ - vzxZ) * ex0);
-    const T xz10 = two * eta_at(L, L.exz, F + sy) * ((vxX - vxXz) * ez0 + (vzX - vz0) * ex1);
-    const T xz11 = two * eta_at(L, L.exz, F + sy + sz) * ((vxXZ - vxX) * ez1 + (vzXZ - vzZ) * ex1);
-    const T yz00 = two * eta_at(L, L.eyz, F) * ((vy0 - vyz_) * ez0 + (vz0 - vzy_) * ey0);
-    const T yz01 = two * eta_at(L, L.eyz, F + sz) * ((vyZ - vy0) * ez1 + (vzZ - vzyZ) * ey0);
-    const T yz10 = two * eta_at(L, L.eyz, F + 1) * ((vyY - vyYz) * ez0 + (vzY - vz0) * ey1);
-    const T yz11 = two * eta_at(L, L.eyz, F + 1 + sz) * ((vyYZ - vyY) * ez1 + (vzYZ - vzZ) * ey1);
+    const T xy00 = two * A.eta(L, 1, 0, 0, 0) * ((vx0 - vxy_) * ey0 + (vy0 - vyx_) * ex0);
+    const T xy01 = two * A.eta(L, 1, 0, 1, 0) * ((vxY - vx0) * ey1 + (vyY - vyxY) * ex0);
+    const T xy10 = two * A.eta(L, 1, 1, 0, 0) * ((vxX - vxXy) * ey0 + (vyX - vy0) * ex1);
+    const T xy11 = two * A.eta(L, 1, 1, 1, 0) * ((vxXY - vxX) * ey1 + (vyXY - vyY) * ex1);
+    const T xz00 = two * A.eta(L, 2, 0, 0, 0) * ((vx0 - vxz_) * ez0 + (vz0 - vzx_) * ex0);
+    const T xz01 = two * A.eta(L, 2, 0, 0, 1) * ((vxZ - vx0) * ez1 + (vzZ - vzxZ) * ex0);
+    const T xz10 = two * A.eta(L, 2, 1, 0, 0) * ((vxX - vxXz) * ez0 + (vzX - vz0) * ex1);
+    const T xz11 = two * A.eta(L, 2, 1, 0, 1) * ((vxXZ - vxX) * ez1 + (vzXZ - vzZ) * ex1);
+    const T yz00 = two * A.eta(L, 3, 0, 0, 0) * ((vy0 - vyz_) * ez0 + (vz0 - vzy_) * ey0);
+    const T yz01 = two * A.eta(L, 3, 0, 0, 1) * ((vyZ - vy0) * ez1 + (vzZ - vzyZ) * ey0);
+    const T yz10 = two * A.eta(L, 3, 0, 1, 0) * ((vyY - vyYz) * ez0 + (vzY - vz0) * ey1);
+    const T yz11 = two * A.eta(L, 3, 0, 1, 1) * ((vyYZ - vyY) * ez1 + (vzYZ - vzZ) * ey1);
     const T p0 = A.v(0, 1, 1, 1), pL = A.v(0, 0, 1, 1), pR = A.v(0, 2, 1, 1), pF = A.v(0, 1, 0, 1);
     const T pB = A.v(0, 1, 2, 1), pD = A.v(0, 1, 1, 0), pU = A.v(0, 1, 1, 2);
     const T cx0 = L.ax.ihc[i - 1], cx1 = L.ax.ihc[i], cy0 = L.ay.ihc[j - 1], cy1 = L.ay.ihc[j];
@@ -171,7 +189,7 @@ __device__ __forceinline__ void vanka_update(const LevelView<T> &L, const Acc &A
     const int fc[6] = {1, 1, 2, 2, 3, 3};
     const int fi[6] = {F, F + sy, F, F + 1, F, F + sz};
     T ax[6], div;
-    cell_rows_acc(L, A, i, j, k, F, ax, div);
+    cell_rows_acc(L, A, i, j, k, ax, div);
     const T hx = L.ax.ih[i], hy = L.ay.ih[j], hz = L.az.ih[k];
     const T cc[6] = {-hx, hx, -hy, hy, -hz, hz};
     T v[6];
@@ -344,7 +362,7 @@ __global__ void __launch_bounds__(kSwThreads) k_vanka_sweep(LevelView<T> L, Vec4
                     const int xr = i - 1 - X0, yr = j - 1 - Y0;
                     const int F = (kb - 1) * sz + (i - 1) * sy + (j - 1);
                     if (black) {
-                        RingAcc<T> A{B, xr, yr, kb - 1};
+                        RingAcc<T> A{B, xr, yr, kb - 1, F, sy, sz};
                         const uint8_t fm[6] = {mask_at(i - 1, j - 1, kb - 1), mask_at(i, j - 1, kb - 1),
                                                mask_at(i - 1, j - 1, kb - 1), mask_at(i - 1, j, kb - 1),
                                                mask_at(i - 1, j - 1, kb - 1), mask_at(i - 1, j - 1, kb)};
