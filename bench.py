@@ -527,17 +527,27 @@ def fixture(cfg):
     return np.load(path) if os.path.exists(path) else None
 
 
+def velocity_rel_l2(sol, ref):
+    """Relative L2 error of the velocity as one vector field (vx, vy, vz)."""
+    d = sum(float(np.linalg.norm(np.asarray(sol[k], np.float64) - np.asarray(ref[k], np.float64))) ** 2
+            for k in SOL_KEYS[:3])
+    r = sum(float(np.linalg.norm(np.asarray(ref[k], np.float64))) ** 2 for k in SOL_KEYS[:3])
+    return float((d / r) ** 0.5) if r > 0 else float(d ** 0.5)
+
+
 def errors_vs_fixture(sol, m, fx):
-    """Relative L2 error per field on the fixture's sub-lattice (every
-    stride-th node per axis) and of the full-field norm, against the oracle
-    port's solution converged to 1e-10."""
+    """Relative L2 error per field and of the velocity vector on the
+    fixture's sub-lattice (every stride-th node per axis), and of the
+    full-field norms, against the oracle port's solution converged to 1e-10."""
     nx, ny, nz = m.shape
     st = int(fx["stride"])
     out = {}
+    sub = {}
     for k in SOL_KEYS:
-        a = np.asarray(sol[k], np.float64).reshape(nz, nx, ny)[::st, ::st, ::st].reshape(-1)
-        out[k] = rel_l2(a, fx["sub_" + k])
+        sub[k] = np.asarray(sol[k], np.float64).reshape(nz, nx, ny)[::st, ::st, ::st].reshape(-1)
+        out[k] = rel_l2(sub[k], fx["sub_" + k])
         out[k + "_norm"] = float(abs(np.linalg.norm(sol[k]) - float(fx["norm_" + k])) / float(fx["norm_" + k]))
+    out["velocity"] = velocity_rel_l2(sub, {k: fx["sub_" + k] for k in SOL_KEYS})
     return out
 
 
@@ -680,6 +690,7 @@ def main():
     sol64 = p64.ctx.solution(n)
     p64.close()
     err_vs_fp64 = {k: rel_l2(sol[k], sol64[k]) for k in SOL_KEYS}
+    err_vs_fp64["velocity"] = velocity_rel_l2(sol, sol64)
     del sol64
     # against the oracle: its converged solution (fixture) on the large grids,
     # a live oracle solve to 1e-11 on the small ones
@@ -698,6 +709,7 @@ def main():
         ref = so.solution()
         so.close()
         err_vs_oracle = {k: rel_l2(sol[k], ref[k]) for k in SOL_KEYS}
+        err_vs_oracle["velocity"] = velocity_rel_l2(sol, ref)
         err_vs_oracle["reference"] = "oracle port solved live to 1e-11, full fields"
 
     # one marker advection step (movemark, RK4) of the resident markers through

@@ -417,6 +417,19 @@ p2_status p2_debug_smooth(p2_ctx *ctx, int level, int sweeps, const double *b, d
  * (both colours with their boundary rows), `sweeps` sweeps timed together
  * after a 256 MB write that evicts L2, mean of 10 repetitions. */
 p2_status p2_debug_time_sweep(p2_ctx *ctx, int level, int sweeps, double *ms_per_sweep);
+/* Average device time of one stage of the solve on the state left by the
+ * last solve, each of `reps` repetitions timed alone after a 256 MB write
+ * that evicts L2: stage 0 the V-cycle residual of `level`, 1 the level-0
+ * FP64 true residual, 2 the restriction of `level` to level + 1, 3 the
+ * prolongation of level + 1 to `level`, 4 the level-0 FP64 operator.
+ * `variant` selects the kernel of the operator rows (0 by level size and
+ * precision, 1 one thread per node from global memory, 2 z-marching planes
+ * in shared memory). */
+p2_status p2_debug_time_stage(p2_ctx *ctx, int stage, int level, int variant, int reps, double *ms);
+/* Kernel of the operator rows for the following calls of this context
+ * (variant as for p2_debug_time_stage; 0, the default, chooses by level
+ * size).  Captured V-cycle graphs are dropped so that solves use it too. */
+p2_status p2_debug_rows_kernel(p2_ctx *ctx, int variant);
 
 #ifdef __cplusplus
 }

@@ -21,7 +21,7 @@ EXPORTED = ["p2_default_params", "p2_create", "p2_destroy", "p2_last_error", "p2
             "p2_set_nodes", "p2_stokes_solve", "p2_stokes_solve_resident", "p2_get_solution", "p2_ronurecalc",
             "p2_upload_markers", "p2_ronurecalc_resident", "p2_get_nodes", "p2_debug_apply", "p2_debug_restrict",
             "p2_debug_prolong", "p2_debug_level_fields", "p2_debug_time_smoother", "p2_debug_smooth",
-            "p2_debug_time_sweep", "p2_ronurecalc_noalloc", "p2_autotune",
+            "p2_debug_time_sweep", "p2_debug_time_stage", "p2_debug_rows_kernel", "p2_ronurecalc_noalloc", "p2_autotune",
             "p2_movemark", "p2_movemark_resident", "p2_get_markers", "p2_stress_strain",
             "p2_stokes_solve_batch", "p2_movemark_strain", "p2_ronurecalc_powerlaw", "p2_effbulk_visc",
             "p2_default_heat_params", "p2_heat_set_bc", "p2_titerate", "p2_prn_read_header", "p2_prn_read",
@@ -420,8 +420,11 @@ def _debug_sigs(L):
     L.p2_debug_time_smoother.argtypes = [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_double)]
     L.p2_debug_smooth.argtypes = [C.c_void_p, C.c_int, C.c_int, _dpp, _dpp]
     L.p2_debug_time_sweep.argtypes = [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_double)]
+    L.p2_debug_time_stage.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_double)]
+    L.p2_debug_rows_kernel.argtypes = [C.c_void_p, C.c_int]
     for f in ("p2_debug_apply", "p2_debug_restrict", "p2_debug_prolong", "p2_debug_level_fields",
-              "p2_debug_time_smoother", "p2_debug_smooth", "p2_debug_time_sweep"):
+              "p2_debug_time_smoother", "p2_debug_smooth", "p2_debug_time_sweep", "p2_debug_time_stage",
+              "p2_debug_rows_kernel"):
         getattr(L, f).restype = C.c_int
 
 
@@ -466,6 +469,19 @@ class DebugHooks:
         ms = C.c_double()
         self.ctx._check(self.ctx.L.p2_debug_time_sweep(self.ctx.h, level, sweeps, C.byref(ms)), "p2_debug_time_sweep")
         return ms.value
+
+    STAGES = {"residual": 0, "true_residual": 1, "restrict": 2, "prolong": 3, "operator": 4}
+
+    def time_stage(self, stage: str, level: int = 0, variant: int = 0, reps: int = 10) -> float:
+        """Mean device time (ms) of one solve stage (p2_debug_time_stage)."""
+        ms = C.c_double()
+        self.ctx._check(self.ctx.L.p2_debug_time_stage(self.ctx.h, self.STAGES[stage], level, variant, reps,
+                                                       C.byref(ms)), "p2_debug_time_stage")
+        return ms.value
+
+    def rows_kernel(self, variant: int):
+        """Kernel of the operator rows for later calls (p2_debug_rows_kernel)."""
+        self.ctx._check(self.ctx.L.p2_debug_rows_kernel(self.ctx.h, variant), "p2_debug_rows_kernel")
 
     def level_fields(self, total_nodes: int):
         nu = np.zeros(total_nodes, np.float32)

@@ -528,6 +528,24 @@ p2_status p2_debug_time_sweep(p2_ctx *ctx, int level, int sweeps, double *ms_per
     });
 }
 
+p2_status p2_debug_rows_kernel(p2_ctx *ctx, int variant)
+{
+    return guard(ctx, [&] {
+        if (variant < 0 || variant > 2) throw p2::Error(P2_ERR_ARG, "rows kernel variant must be 0..2");
+        ctx->s->dbg_rows_variant = variant;
+        ctx->s->drop_graphs_public();
+    });
+}
+
+p2_status p2_debug_time_stage(p2_ctx *ctx, int stage, int level, int variant, int reps, double *ms)
+{
+    return guard(ctx, [&] {
+        if (!ms) throw p2::Error(P2_ERR_ARG, "null argument");
+        P2_CUDA_TRY(cudaSetDevice(ctx->s->dev));
+        *ms = ctx->s->debug_time_stage(stage, level, variant, reps);
+    });
+}
+
 p2_status p2_debug_level_fields(p2_ctx *ctx, float *nu, float *ro)
 {
     return guard(ctx, [&] {

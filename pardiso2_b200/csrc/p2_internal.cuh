@@ -96,8 +96,7 @@ struct LevelView {
     int pin;                            // pinned pressure cell node, -1 if none
 };
 
-// Plain loads (not __ldg): the row functions below also run on level views
-// whose arrays are shared-memory copies of a brick (k_rows_tiled).
+// Plain loads (not __ldg), as everywhere in the stencils below.
 template <typename T>
 __device__ __forceinline__ T eta_at(const LevelView<T> &L, const float *a, int i)
 {
@@ -123,46 +122,134 @@ __device__ __forceinline__ T ld(const S *a, int i)
 
 #define P2IDX(L, i, j, k) ((k) * ((L).nx * (L).ny) + (i) * (L).ny + (j))
 
+// The stencils below read the unknowns and viscosities through an accessor
+// A with A.u(c, a, b, cc) (unknown c = 0 P, 1 Vx, 2 Vy, 3 Vz at node
+// (a, b, cc)) and A.e(f, a, b, cc) (viscosity field f = 0 ec, 1 exy, 2 exz,
+// 3 eyz, clamped as eta_at does), so the same expressions run on global
+// arrays (NodeAcc) and on planes staged in shared memory (k_rows_zm).  The
+// rows take their stresses from A.snn / A.sxy / A.sxz / A.syz: NodeAcc
+// computes them in place, k_rows_zm reads them from planes of stresses that
+// it computed once per cell and edge with the same expressions.
+template <typename T, typename A>
+__device__ __forceinline__ void cell_rates_a(const LevelView<T> &L, const A &X, int a, int b, int c, T &dxx, T &dyy,
+                                             T &dzz)
+{
+    dxx = (X.u(1, a, b - 1, c - 1) - X.u(1, a - 1, b - 1, c - 1)) * L.ax.ih[a];
+    dyy = (X.u(2, a - 1, b, c - 1) - X.u(2, a - 1, b - 1, c - 1)) * L.ay.ih[b];
+    dzz = (X.u(3, a - 1, b - 1, c) - X.u(3, a - 1, b - 1, c - 1)) * L.az.ih[c];
+}
+
+// Normal stress component d (0 xx, 1 yy, 2 zz) in cell (a,b,c).
+template <typename T, typename A>
+__device__ __forceinline__ T snn_a(const LevelView<T> &L, const A &X, int d, int a, int b, int c)
+{
+    T dxx, dyy, dzz;
+    cell_rates_a(L, X, a, b, c, dxx, dyy, dzz);
+    T div3 = (dxx + dyy + dzz) / (T)3.0;
+    T e = d == 0 ? dxx : (d == 1 ? dyy : dzz);
+    return (T)2.0 * X.e(0, a, b, c) * (e - div3);
+}
+
+template <typename T, typename A>
+__device__ __forceinline__ T sxy_a(const LevelView<T> &L, const A &X, int a, int b, int c)
+{
+    return (T)2.0 * X.e(1, a, b, c) *
+           ((X.u(1, a, b, c) - X.u(1, a, b - 1, c)) * L.ay.ihe[b] + (X.u(2, a, b, c) - X.u(2, a - 1, b, c)) * L.ax.ihe[a]);
+}
+template <typename T, typename A>
+__device__ __forceinline__ T sxz_a(const LevelView<T> &L, const A &X, int a, int b, int c)
+{
+    return (T)2.0 * X.e(2, a, b, c) *
+           ((X.u(1, a, b, c) - X.u(1, a, b, c - 1)) * L.az.ihe[c] + (X.u(3, a, b, c) - X.u(3, a - 1, b, c)) * L.ax.ihe[a]);
+}
+template <typename T, typename A>
+__device__ __forceinline__ T syz_a(const LevelView<T> &L, const A &X, int a, int b, int c)
+{
+    return (T)2.0 * X.e(3, a, b, c) *
+           ((X.u(2, a, b, c) - X.u(2, a, b, c - 1)) * L.az.ihe[c] + (X.u(3, a, b, c) - X.u(3, a, b - 1, c)) * L.ay.ihe[b]);
+}
+
+// Accessor on global arrays; its stresses are computed where they are used.
+template <typename T, typename S>
+struct NodeAcc {
+    const LevelView<T> &L;
+    const Fields<T, S> &x;
+    __device__ __forceinline__ T u(int c, int a, int b, int cc) const
+    {
+        const S *p = c == 0 ? x.p : (c == 1 ? x.vx : (c == 2 ? x.vy : x.vz));
+        return ld<T>(p, P2IDX(L, a, b, cc));
+    }
+    __device__ __forceinline__ T e(int f, int a, int b, int cc) const
+    {
+        const float *p = f == 0 ? L.ec : (f == 1 ? L.exy : (f == 2 ? L.exz : L.eyz));
+        return eta_at(L, p, P2IDX(L, a, b, cc));
+    }
+    __device__ __forceinline__ T snn(int d, int a, int b, int cc) const { return snn_a(L, *this, d, a, b, cc); }
+    __device__ __forceinline__ T sxy(int a, int b, int cc) const { return sxy_a(L, *this, a, b, cc); }
+    __device__ __forceinline__ T sxz(int a, int b, int cc) const { return sxz_a(L, *this, a, b, cc); }
+    __device__ __forceinline__ T syz(int a, int b, int cc) const { return syz_a(L, *this, a, b, cc); }
+};
+
+// The rows take the stresses from the accessor (X.snn .. X.syz) and the
+// pressures and velocities from X.u.
+template <typename T, typename A>
+__device__ __forceinline__ T row_vx_a(const LevelView<T> &L, const A &X, int i, int j, int k)
+{
+    return (X.snn(0, i + 1, j + 1, k + 1) - X.snn(0, i, j + 1, k + 1)) * L.ax.ihc[i] +
+           (X.sxy(i, j + 1, k) - X.sxy(i, j, k)) * L.ay.ihv[j] +
+           (X.sxz(i, j, k + 1) - X.sxz(i, j, k)) * L.az.ihv[k] -
+           (X.u(0, i + 1, j + 1, k + 1) - X.u(0, i, j + 1, k + 1)) * L.ax.ihc[i];
+}
+template <typename T, typename A>
+__device__ __forceinline__ T row_vy_a(const LevelView<T> &L, const A &X, int i, int j, int k)
+{
+    return (X.snn(1, i + 1, j + 1, k + 1) - X.snn(1, i + 1, j, k + 1)) * L.ay.ihc[j] +
+           (X.sxy(i + 1, j, k) - X.sxy(i, j, k)) * L.ax.ihv[i] +
+           (X.syz(i, j, k + 1) - X.syz(i, j, k)) * L.az.ihv[k] -
+           (X.u(0, i + 1, j + 1, k + 1) - X.u(0, i + 1, j, k + 1)) * L.ay.ihc[j];
+}
+template <typename T, typename A>
+__device__ __forceinline__ T row_vz_a(const LevelView<T> &L, const A &X, int i, int j, int k)
+{
+    return (X.snn(2, i + 1, j + 1, k + 1) - X.snn(2, i + 1, j + 1, k)) * L.az.ihc[k] +
+           (X.sxz(i + 1, j, k) - X.sxz(i, j, k)) * L.ax.ihv[i] +
+           (X.syz(i, j + 1, k) - X.syz(i, j, k)) * L.ay.ihv[j] -
+           (X.u(0, i + 1, j + 1, k + 1) - X.u(0, i + 1, j + 1, k)) * L.az.ihc[k];
+}
+template <typename T, typename A>
+__device__ __forceinline__ T row_p_a(const LevelView<T> &L, const A &X, int i, int j, int k)
+{
+    return (X.u(1, i, j - 1, k - 1) - X.u(1, i - 1, j - 1, k - 1)) * L.ax.ih[i] +
+           (X.u(2, i - 1, j, k - 1) - X.u(2, i - 1, j - 1, k - 1)) * L.ay.ih[j] +
+           (X.u(3, i - 1, j - 1, k) - X.u(3, i - 1, j - 1, k - 1)) * L.az.ih[k];
+}
+
+// The same on global arrays.
 template <typename T, typename S>
 __device__ __forceinline__ void cell_rates(const LevelView<T> &L, const Fields<T, S> &x, int a, int b, int c,
                                            T &dxx, T &dyy, T &dzz)
 {
-    dxx = (ld<T>(x.vx, P2IDX(L, a, b - 1, c - 1)) - ld<T>(x.vx, P2IDX(L, a - 1, b - 1, c - 1))) * L.ax.ih[a];
-    dyy = (ld<T>(x.vy, P2IDX(L, a - 1, b, c - 1)) - ld<T>(x.vy, P2IDX(L, a - 1, b - 1, c - 1))) * L.ay.ih[b];
-    dzz = (ld<T>(x.vz, P2IDX(L, a - 1, b - 1, c)) - ld<T>(x.vz, P2IDX(L, a - 1, b - 1, c - 1))) * L.az.ih[c];
+    cell_rates_a(L, NodeAcc<T, S>{L, x}, a, b, c, dxx, dyy, dzz);
 }
-
-// Normal stress component d (0 xx, 1 yy, 2 zz) in cell (a,b,c).
 template <typename T, typename S>
 __device__ __forceinline__ T snn(const LevelView<T> &L, const Fields<T, S> &x, int d, int a, int b, int c)
 {
-    T dxx, dyy, dzz;
-    cell_rates(L, x, a, b, c, dxx, dyy, dzz);
-    T div3 = (dxx + dyy + dzz) / (T)3.0;
-    T e = d == 0 ? dxx : (d == 1 ? dyy : dzz);
-    return (T)2.0 * eta_at(L, L.ec, P2IDX(L, a, b, c)) * (e - div3);
+    return snn_a(L, NodeAcc<T, S>{L, x}, d, a, b, c);
 }
-
 template <typename T, typename S>
 __device__ __forceinline__ T sxy(const LevelView<T> &L, const Fields<T, S> &x, int a, int b, int c)
 {
-    return (T)2.0 * eta_at(L, L.exy, P2IDX(L, a, b, c)) *
-           ((ld<T>(x.vx, P2IDX(L, a, b, c)) - ld<T>(x.vx, P2IDX(L, a, b - 1, c))) * L.ay.ihe[b] +
-            (ld<T>(x.vy, P2IDX(L, a, b, c)) - ld<T>(x.vy, P2IDX(L, a - 1, b, c))) * L.ax.ihe[a]);
+    return sxy_a(L, NodeAcc<T, S>{L, x}, a, b, c);
 }
 template <typename T, typename S>
 __device__ __forceinline__ T sxz(const LevelView<T> &L, const Fields<T, S> &x, int a, int b, int c)
 {
-    return (T)2.0 * eta_at(L, L.exz, P2IDX(L, a, b, c)) *
-           ((ld<T>(x.vx, P2IDX(L, a, b, c)) - ld<T>(x.vx, P2IDX(L, a, b, c - 1))) * L.az.ihe[c] +
-            (ld<T>(x.vz, P2IDX(L, a, b, c)) - ld<T>(x.vz, P2IDX(L, a - 1, b, c))) * L.ax.ihe[a]);
+    return sxz_a(L, NodeAcc<T, S>{L, x}, a, b, c);
 }
 template <typename T, typename S>
 __device__ __forceinline__ T syz(const LevelView<T> &L, const Fields<T, S> &x, int a, int b, int c)
 {
-    return (T)2.0 * eta_at(L, L.eyz, P2IDX(L, a, b, c)) *
-           ((ld<T>(x.vy, P2IDX(L, a, b, c)) - ld<T>(x.vy, P2IDX(L, a, b, c - 1))) * L.az.ihe[c] +
-            (ld<T>(x.vz, P2IDX(L, a, b, c)) - ld<T>(x.vz, P2IDX(L, a, b - 1, c))) * L.ay.ihe[b]);
+    return syz_a(L, NodeAcc<T, S>{L, x}, a, b, c);
 }
 
 // Diagonals of the x-, y-, z-Stokes rows at node (i,j,k).
@@ -209,39 +296,28 @@ __device__ __forceinline__ T diag_vz(const LevelView<T> &L, int i, int j, int k)
 template <typename T, typename S>
 __device__ __forceinline__ T row_vx(const LevelView<T> &L, const Fields<T, S> &x, int i, int j, int k, T *diag)
 {
-    T v = (snn(L, x, 0, i + 1, j + 1, k + 1) - snn(L, x, 0, i, j + 1, k + 1)) * L.ax.ihc[i] +
-          (sxy(L, x, i, j + 1, k) - sxy(L, x, i, j, k)) * L.ay.ihv[j] +
-          (sxz(L, x, i, j, k + 1) - sxz(L, x, i, j, k)) * L.az.ihv[k] -
-          (ld<T>(x.p, P2IDX(L, i + 1, j + 1, k + 1)) - ld<T>(x.p, P2IDX(L, i, j + 1, k + 1))) * L.ax.ihc[i];
+    T v = row_vx_a(L, NodeAcc<T, S>{L, x}, i, j, k);
     if (diag) *diag = diag_vx(L, i, j, k);
     return v;
 }
 template <typename T, typename S>
 __device__ __forceinline__ T row_vy(const LevelView<T> &L, const Fields<T, S> &x, int i, int j, int k, T *diag)
 {
-    T v = (snn(L, x, 1, i + 1, j + 1, k + 1) - snn(L, x, 1, i + 1, j, k + 1)) * L.ay.ihc[j] +
-          (sxy(L, x, i + 1, j, k) - sxy(L, x, i, j, k)) * L.ax.ihv[i] +
-          (syz(L, x, i, j, k + 1) - syz(L, x, i, j, k)) * L.az.ihv[k] -
-          (ld<T>(x.p, P2IDX(L, i + 1, j + 1, k + 1)) - ld<T>(x.p, P2IDX(L, i + 1, j, k + 1))) * L.ay.ihc[j];
+    T v = row_vy_a(L, NodeAcc<T, S>{L, x}, i, j, k);
     if (diag) *diag = diag_vy(L, i, j, k);
     return v;
 }
 template <typename T, typename S>
 __device__ __forceinline__ T row_vz(const LevelView<T> &L, const Fields<T, S> &x, int i, int j, int k, T *diag)
 {
-    T v = (snn(L, x, 2, i + 1, j + 1, k + 1) - snn(L, x, 2, i + 1, j + 1, k)) * L.az.ihc[k] +
-          (sxz(L, x, i + 1, j, k) - sxz(L, x, i, j, k)) * L.ax.ihv[i] +
-          (syz(L, x, i, j + 1, k) - syz(L, x, i, j, k)) * L.ay.ihv[j] -
-          (ld<T>(x.p, P2IDX(L, i + 1, j + 1, k + 1)) - ld<T>(x.p, P2IDX(L, i + 1, j + 1, k))) * L.az.ihc[k];
+    T v = row_vz_a(L, NodeAcc<T, S>{L, x}, i, j, k);
     if (diag) *diag = diag_vz(L, i, j, k);
     return v;
 }
 template <typename T, typename S>
 __device__ __forceinline__ T row_p(const LevelView<T> &L, const Fields<T, S> &x, int i, int j, int k)
 {
-    return (ld<T>(x.vx, P2IDX(L, i, j - 1, k - 1)) - ld<T>(x.vx, P2IDX(L, i - 1, j - 1, k - 1))) * L.ax.ih[i] +
-           (ld<T>(x.vy, P2IDX(L, i - 1, j, k - 1)) - ld<T>(x.vy, P2IDX(L, i - 1, j - 1, k - 1))) * L.ay.ih[j] +
-           (ld<T>(x.vz, P2IDX(L, i - 1, j - 1, k)) - ld<T>(x.vz, P2IDX(L, i - 1, j - 1, k - 1))) * L.az.ih[k];
+    return row_p_a(L, NodeAcc<T, S>{L, x}, i, j, k);
 }
 
 __host__ __device__ __forceinline__ bool valid_pos(int c, int i, int j, int k, int nx, int ny, int nz)

@@ -772,27 +772,36 @@ __global__ void k_restrict_compat(LevelView<T> F, Vec4<T> rf, LevelView<T> Cl, V
                 yi[a] = a < nyq ? my.idx[y0 + a] : 0;
                 yw[a] = a < nyq ? (T)my.w[y0 + a] : (T)0;
             }
+            // the value, mask and viscosity loads of a fine node do not depend
+            // on each other or on a branch: a boundary row contributes with
+            // weight 0 (its value times 0 adds nothing), so every load of a z
+            // line can be in flight at once
             for (int qz = mz.ptr[K]; qz < mz.ptr[K + 1]; qz++) {
                 const int fk = mz.idx[qz];
                 const T wz = (T)mz.w[qz];
 #pragma unroll
                 for (int ax = 0; ax < kRestrictList; ax++) {
-                    if (ax >= nxq) break;
-                    const T wzx = wz * xw[ax];
-                    const int base = fk * (F.nx * F.ny) + xi[ax] * F.ny;
+                    if (ax < nxq) {
+                        const T wzx = wz * xw[ax];
+                        const int base = fk * (F.nx * F.ny) + xi[ax] * F.ny;
 #pragma unroll
-                    for (int ay = 0; ay < kRestrictList; ay++) {
-                        if (ay >= nyq) break;
-                        const int f = base + yi[ay];
-                        if (__ldg(F.bcm + f) & (1 << c)) continue;
-                        const T w = wzx * yw[ay];
-                        T val = __ldg(rfc + f);
-                        if (c == 0 && scale_p) val *= (T)__ldg(F.ec + f) / etac;
-                        acc += val * w;
-                        ws += w;
+                        for (int ay = 0; ay < kRestrictList; ay++) {
+                            if (ay < nyq) {
+                                const int f = base + yi[ay];
+                                const bool bnd = __ldg(F.bcm + f) & (1 << c);
+                                T val = __ldg(rfc + f);
+                                if (c == 0 && scale_p) val *= (T)__ldg(F.ec + f);
+                                const T w = bnd ? (T)0 : wzx * yw[ay];
+                                acc += val * w;
+                                ws += w;
+                            }
+                        }
                     }
                 }
             }
+            // the pressure residuals' viscosity ratio eta_f / eta_c: eta_f per
+            // fine node above, the division by eta_c once here
+            if (c == 0 && scale_p) acc /= etac;
             out = ws != (T)0 ? acc / ws : (T)0;
             if (c == 0 && I > 0 && J > 0 && K > 0)
                 contrib = (double)out / ((double)Cl.ax.ih[I] * (double)Cl.ay.ih[J] * (double)Cl.az.ih[K]);

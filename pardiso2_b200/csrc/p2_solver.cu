@@ -23,7 +23,7 @@
 #include "p2_kernels.cuh"
 #include "p2_solver.h"
 #include "p2_sweep.cuh"
-#include "p2_tiled.cuh"
+#include "p2_zmarch.cuh"
 
 namespace p2 {
 
@@ -904,28 +904,21 @@ Vec4<float> &r_of<float>(Level &Lv) { return Lv.r32; }
 template <>
 Vec4<double> &r_of<double>(Level &Lv) { return Lv.r64; }
 
-// Levels at least this large run the shared-memory-staged colour pass
-// (smoother 6); smaller ones are latency-bound either way.
-constexpr long kTileMinNodes = 1L << 20;
+// Levels of at least this many nodes evaluate their rows with k_rows_zm.
+constexpr long kZmMinNodes = 1L << 17;
 
-template <typename T>
-static void tiled_kernel_setup()
-{
-    static bool done = false;  // per instantiation, per process (the attribute is per function)
-    if (!done) {
-        P2_CUDA_TRY(cudaFuncSetAttribute(k_vanka_tiled<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)tile_smem_bytes<T>()));
-        done = true;
-    }
-}
-
-// Residual / operator rows on a level (k_rows, or k_rows_tiled on levels of
-// at least kTileMinNodes nodes): out = b - A x (mode 0) or A x (mode 1).
+// Residual / operator rows on a level: out = b - A x (mode 0) or A x
+// (mode 1).  variant 0 picks k_rows_zm for FP32 rows on levels of at least
+// kZmMinNodes nodes and k_rows otherwise (measured at 257^3: k_rows_zm
+// 0.66 ms against k_rows 0.72 ms for the FP32 residual, but 1.33 against
+// 1.08 ms for the FP64 rows, where the double planes leave two blocks per
+// SM); 1 forces k_rows, 2 k_rows_zm (the timing hook compares them).
 template <typename T, typename S>
 static void launch_rows(cudaStream_t st, bool pdl, const LevelView<T> &V, const Fields<T, S> &f, const Vec4<T> &b,
-                        Vec4<T> &out, const Vec4<float> &o32, int mode)
+                        Vec4<T> &out, const Vec4<float> &o32, int mode, int variant = 0)
 {
-    if (V.n < kTileMinNodes) {
+    if (variant == 0) variant = (sizeof(S) == 4 && V.n >= kZmMinNodes) ? 2 : 1;
+    if (variant == 1) {
         if (pdl) pdl_launch(st, nblk(V.n), kThreads, k_rows<T, S>, V, f, b, out, o32, mode);
         else {
             k_rows<T, S><<<nblk(V.n), kThreads, 0, st>>>(V, f, b, out, o32, mode);
@@ -933,56 +926,28 @@ static void launch_rows(cudaStream_t st, bool pdl, const LevelView<T> &V, const 
         }
         return;
     }
-    using RT = RowTile<S>;
-    static bool attr_done = false;  // per instantiation
-    if (!attr_done) {
-        P2_CUDA_TRY(cudaFuncSetAttribute(k_rows_tiled<T, S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)RT::smem));
-        attr_done = true;
-    }
-    dim3 grid((V.nx + RT::TX - 1) / RT::TX, (V.ny + RT::TY - 1) / RT::TY, (V.nz + RT::TZ - 1) / RT::TZ);
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = grid;
-    cfg.blockDim = dim3(kTileThreads);
-    cfg.dynamicSmemBytes = RT::smem;
-    cfg.stream = st;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
     attr[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = attr;
     cfg.numAttrs = pdl ? 1 : 0;
-    P2_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_rows_tiled<T, S>, V, f, b, out, o32, mode));
-    P2_COUNT_LAUNCH();
-}
-
-// One colour pass with the brick staged in shared memory (k_vanka_tiled).
-template <typename T>
-void Solver::tiled_pass(int l, const LevelView<T> &V, T *P, Vec4<T> &vin, Vec4<T> &vout, Vec4<T> &b, int col)
-{
-    Level &Lv = L[l];
-    tiled_kernel_setup<T>();
-    constexpr int TX = TileShape<T>::TX, TY = TileShape<T>::TY, TZ = TileShape<T>::TZ;
-    dim3 grid((Lv.nx - 1 + TX - 1) / TX, (Lv.ny - 1 + TY - 1) / TY, (Lv.nz - 1 + TZ - 1) / TZ);
-    const factor_t<T> *blk = (const factor_t<T> *)Lv.blk + (size_t)col * kBlkEntries * Lv.blk_stride;
-    const T om = (T)prm.omega;
-#ifdef P2_NO_PDL
-    k_vanka_tiled<T><<<grid, kTileThreads, tile_smem_bytes<T>(), st>>>(V, P, vin, vout, b, om, col, blk,
-                                                                      Lv.blk_stride);
-    P2_COUNT_LAUNCH();
-#else
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = grid;
-    cfg.blockDim = dim3(kTileThreads);
-    cfg.dynamicSmemBytes = tile_smem_bytes<T>();
     cfg.stream = st;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    attr[0].val.programmaticStreamSerializationAllowed = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    P2_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_vanka_tiled<T>, V, P, vin, vout, b, om, col, blk, Lv.blk_stride));
-    P2_COUNT_LAUNCH();
-#endif
+    if (variant == 2) {
+        static bool attr_done = false;  // per instantiation (the attribute is per function)
+        if (!attr_done) {
+            P2_CUDA_TRY(cudaFuncSetAttribute(k_rows_zm<T, S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)zm_smem_bytes<T, S>()));
+            attr_done = true;
+        }
+        cfg.gridDim = dim3((V.nx + kZmTX - 1) / kZmTX, (V.ny + kZmTY - 1) / kZmTY, (V.nz + kZmKZ - 1) / kZmKZ);
+        cfg.blockDim = dim3(kZmThreads);
+        cfg.dynamicSmemBytes = zm_smem_bytes<T, S>();
+        P2_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_rows_zm<T, S>, V, f, b, out, o32, mode));
+        P2_COUNT_LAUNCH();
+        return;
+    }
+    throw Error(P2_ERR_ARG, "rows kernel variant must be 0, 1 or 2");
 }
 
 // One colour pass of the selected smoother on level l.
@@ -993,12 +958,6 @@ void Solver::smoother_pass(int l, const LevelView<T> &V, T *P, Vec4<T> &vin, Vec
     const long cells = (long)(Lv.nx - 1) * (Lv.nz - 1) * (Lv.ny / 2);
     const T om = (T)prm.omega;
     switch (prm.smoother) {
-    case 6:
-        if (Lv.n >= kTileMinNodes) {
-            tiled_pass<T>(l, V, P, vin, vout, b, col);
-            break;
-        }
-        // fall through: small levels take the plain pass
     case 1:
     case 5: {
         const factor_t<T> *blk = (const factor_t<T> *)Lv.blk + (size_t)col * kBlkEntries * Lv.blk_stride;
@@ -1031,7 +990,7 @@ void Solver::factor_smoother()
 
 void Solver::factor_cells()
 {
-    if (prm.smoother != 1 && prm.smoother != 5 && prm.smoother != 6) return;
+    if (prm.smoother != 1 && prm.smoother != 5) return;
     if (prm.precision == 0) factor_smoother<float>();
     else factor_smoother<double>();
 }
@@ -1139,7 +1098,7 @@ void Solver::level_residual(int l)
     Vec4<T> &x = vx_of<T>(Lv, 0), &b = b_of<T>(Lv), &r = r_of<T>(Lv);
     Fields<T, T> f{x.c[0], x.c[1], x.c[2], x.c[3]};
     Vec4<float> none;
-    launch_rows<T, T>(st, true, V, f, b, r, none, 0);
+    launch_rows<T, T>(st, true, V, f, b, r, none, 0, dbg_rows_variant);
     if (Lv.nbc)
         pdl_launch(st, nblk(Lv.nbc), kThreads, k_bc_rows<T, T>, Lv.nbc, (const int *)Lv.bu, (const int *)Lv.bt,
                    (const float *)Lv.bk, f, b, r, none, 0);
@@ -1228,7 +1187,7 @@ void Solver::rows0(const Vec4<double> &x, Vec4<double> &out, Vec4<float> *r32, i
     LevelView<double> V = view<double>(0, true);
     Fields<double, double> f{x.c[0], x.c[1], x.c[2], x.c[3]};
     Vec4<float> o32 = r32 ? *r32 : Vec4<float>();
-    launch_rows<double, double>(st, false, V, f, gb, out, o32, mode);
+    launch_rows<double, double>(st, false, V, f, gb, out, o32, mode, dbg_rows_variant);
     if (L0.nbc)
         k_bc_rows<double, double><<<nblk(L0.nbc), kThreads, 0, st>>>(L0.nbc, L0.bu, L0.bt, L0.bk, f, gb, out, o32,
                                                                    mode); P2_COUNT_LAUNCH();
@@ -1601,7 +1560,7 @@ void Solver::debug_apply(int l, const double *x, double *y)
     LevelView<double> V = view<double>(l, l == 0);
     Fields<double, double> f{X.v.c[0], X.v.c[1], X.v.c[2], X.v.c[3]};
     Vec4<float> none;
-    launch_rows<double, double>(st, false, V, f, B.v, Y.v, none, 1);
+    launch_rows<double, double>(st, false, V, f, B.v, Y.v, none, 1, dbg_rows_variant);
     if (Lv.nbc)
         k_bc_rows<double, double><<<nblk(Lv.nbc), kThreads, 0, st>>>(Lv.nbc, Lv.bu, Lv.bt, Lv.bk, f, B.v, Y.v, none, 1); P2_COUNT_LAUNCH();
     P2_CUDA_TRY(cudaGetLastError());
@@ -1708,6 +1667,72 @@ double Solver::debug_time_sweep(int l, int sweeps)
     }
     P2_CUDA_TRY(cudaGetLastError());
     return total / reps / sweeps;
+}
+
+// Average device time of one stage of the solve on the state left by the
+// last solve, each repetition timed alone after a 256 MB write that evicts
+// L2: 0 the V-cycle residual of `level` (its rows kernel chosen by variant:
+// 0 by level size, 1 k_rows, 2 k_rows_zm), 1 the level-0
+// FP64 true residual with its float copy (same variants), 2 the restriction
+// of `level` to level + 1, 3 the prolongation of level + 1 to `level`, 4 the
+// level-0 FP64 operator q = A z (rows variants).
+double Solver::debug_time_stage(int stage, int l, int variant, int reps)
+{
+    if (l < 0 || l >= (int)L.size() || reps < 1 || stage < 0 || stage > 4 || variant < 0 || variant > 2)
+        throw Error(P2_ERR_ARG, "bad stage, level, variant or repetition count");
+    if ((stage == 2 || stage == 3) && l + 1 >= (int)L.size()) throw Error(P2_ERR_ARG, "no coarser level");
+    if (!nodes_ready) throw Error(P2_ERR_STATE, "no node fields");
+    const size_t flush_bytes = (size_t)256 << 20;
+    void *flush = nullptr;
+    P2_CUDA_TRY(cudaMalloc(&flush, flush_bytes));
+    struct Free { void *p; ~Free() { if (p) cudaFree(p); } } hold{flush};
+    const int saved = dbg_rows_variant;
+    dbg_rows_variant = variant;
+    double total = 0;
+    try {
+        for (int r = 0; r < reps; r++) {
+            P2_CUDA_TRY(cudaMemsetAsync(flush, r & 0xff, flush_bytes, st));
+            P2_CUDA_TRY(cudaEventRecord(ev[5], st));
+            const bool f32 = prm.precision == 0;
+            if (stage == 0) {
+                if (f32) level_residual<float>(l);
+                else level_residual<double>(l);
+            } else if (stage == 1) {
+                rows0(gx, gr, f32 ? &L[0].r32 : nullptr, 0);
+            } else if (stage == 4) {
+                rows0(Z[0], Q[0], nullptr, 1);
+            } else if (stage == 2) {
+                Level &F = L[l], &Cl = L[l + 1];
+                if (f32)
+                    pdl_launch(st, nblk(4L * Cl.n), kThreads, k_restrict_compat<float>, view<float>(l, false), F.r32,
+                               view<float>(l + 1, false), Cl.b32, Cl.x32, F.tv, 1, Cl.compat_vol, rpartial, rticket,
+                               scal);
+                else
+                    pdl_launch(st, nblk(4L * Cl.n), kThreads, k_restrict_compat<double>, view<double>(l, false),
+                               F.r64, view<double>(l + 1, false), Cl.b64, Cl.x64, F.tv, 1, Cl.compat_vol, rpartial,
+                               rticket, scal);
+            } else {
+                Level &F = L[l], &Cl = L[l + 1];
+                if (f32)
+                    pdl_launch(st, nblk(F.n), kThreads, k_prolong<float>, view<float>(l, false), F.x32,
+                               view<float>(l + 1, false), Cl.x32, F.tv, (float)prm.p1koef, (float)prm.v1koef);
+                else
+                    pdl_launch(st, nblk(F.n), kThreads, k_prolong<double>, view<double>(l, false), F.x64,
+                               view<double>(l + 1, false), Cl.x64, F.tv, prm.p1koef, prm.v1koef);
+            }
+            P2_CUDA_TRY(cudaEventRecord(ev[6], st));
+            P2_CUDA_TRY(cudaEventSynchronize(ev[6]));
+            P2_CUDA_TRY(cudaGetLastError());
+            float ms = 0;
+            P2_CUDA_TRY(cudaEventElapsedTime(&ms, ev[5], ev[6]));
+            total += ms;
+        }
+    } catch (...) {
+        dbg_rows_variant = saved;
+        throw;
+    }
+    dbg_rows_variant = saved;
+    return total / reps;
 }
 
 // nu, ro of every level (after ronurestrict), concatenated like the reference's nu[] / ro[]

@@ -148,6 +148,9 @@ class Solver {
     void debug_level_fields(float *nu, float *ro);
     double debug_time_smoother(int level, int passes);
     double debug_time_sweep(int level, int sweeps);
+    double debug_time_stage(int stage, int level, int variant, int reps);
+    int dbg_rows_variant = 0;     // kernel of the operator rows (launch_rows), 0 = by level size
+    void drop_graphs_public() { drop_graphs(); }
     void debug_smooth(int level, int sweeps, const double *b, double *x);
     p2_tune_info autotune(int trial_iters);
     bool verbose = false;
@@ -205,8 +208,6 @@ class Solver {
     template <typename T>
     void smoother_pass(int l, const LevelView<T> &V, T *P, Vec4<T> &vin, Vec4<T> &vout, Vec4<T> &b, int col);
     bool use_fused(int l) const;
-    template <typename T>
-    void tiled_pass(int l, const LevelView<T> &V, T *P, Vec4<T> &vin, Vec4<T> &vout, Vec4<T> &b, int col);
     template <typename T>
     void sweep_fused(int l, const LevelView<T> &V, Vec4<T> &xin, Vec4<T> &xout, Vec4<T> &b);
     template <typename T>

@@ -82,53 +82,3 @@ def test_fused_and_split_solves_agree(spheres113):
     for k in ("vx", "vy", "vz", "pr"):
         d = np.linalg.norm(sols[0][k] - sols[1][k]) / np.linalg.norm(sols[1][k])
         assert d < 1e-6, (k, d)
-
-
-@pytest.fixture(scope="module")
-def spheres131():
-    """Level 0 above the tiled pass's size threshold (1 M nodes), with partial
-    bricks along every axis (130 x 100 x 98 cells)."""
-    m = M.random_spheres_model(131, 4, 12, (1e-2, 1e3), markers=(2, 2, 2), seed=11, name="spheres131",
-                               shape=(131, 101, 99))
-    prob = P.StokesProblem(m)
-    f = prob.ronurecalc()
-    prob.close()
-    return m, f
-
-
-@pytest.mark.parametrize("precision", [0, 1])
-@pytest.mark.parametrize("sweeps", [2, 3])
-def test_tiled_pass_matches_plain_pass(spheres131, precision, sweeps):
-    """Smoother 6 (colour passes with the brick staged in shared memory,
-    k_vanka_tiled) against smoother 1 (k_vanka_stored) on level 0."""
-    m, f = spheres131
-    shape = level_shape(m, 0)
-    n = shape[0] * shape[1] * shape[2]
-    rng = np.random.Generator(np.random.PCG64(200 + sweeps))
-    mask = unknown_mask(shape)
-    b = np.where(mask, rng.standard_normal(4 * n), 0.0)
-    x = np.where(mask, rng.standard_normal(4 * n) * 1e-2, 0.0)
-    tiled = smooth_with(m, f, 6, precision, 0, sweeps, b, x)
-    plain = smooth_with(m, f, 1, precision, 0, sweeps, b, x)
-    assert np.all(np.isfinite(tiled))
-    tol = 1e-5 if precision == 0 else 1e-12
-    for c in range(4):
-        d = np.linalg.norm(tiled[c::4] - plain[c::4]) / np.linalg.norm(plain[c::4] - x[c::4])
-        assert d < tol, (c, d)
-
-
-def test_tiled_and_plain_solves_agree(spheres131):
-    m, f = spheres131
-    sols, its = [], []
-    for smoother in (6, 1):
-        prob = P.StokesProblem(m, smoother=smoother, tol=1e-8, sweep_growth=2)
-        prob.set_nodes(f)
-        sol, info = prob.solve_fp64()
-        prob.close()
-        assert info.status == 0, info.as_dict()
-        sols.append(sol)
-        its.append(info.iterations)
-    assert abs(its[0] - its[1]) <= 1, its
-    for k in ("vx", "vy", "vz", "pr"):
-        d = np.linalg.norm(sols[0][k] - sols[1][k]) / np.linalg.norm(sols[1][k])
-        assert d < 1e-6, (k, d)
