@@ -430,6 +430,10 @@ p2_status p2_debug_time_stage(p2_ctx *ctx, int stage, int level, int variant, in
  * (variant as for p2_debug_time_stage; 0, the default, chooses by level
  * size).  Captured V-cycle graphs are dropped so that solves use it too. */
 p2_status p2_debug_rows_kernel(p2_ctx *ctx, int variant);
+/* x = one preconditioning V-cycle (the solver's precision, exact coarsest
+ * solve) applied from zero to the level-0 right-hand side b, both
+ * interleaved [P, Vx, Vy, Vz] per node of level 0. */
+p2_status p2_debug_vcycle(p2_ctx *ctx, const double *b, double *x);
 
 #ifdef __cplusplus
 }

@@ -13,7 +13,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libp2cuda.so")
 SOURCES = ["p2_solver.cu", "p2_lu.cu", "p2_markers.cu", "p2_post.cu", "p2_heat.cu", "p2_capi.cu", "p2_prn.cu"]
-HEADERS = ["p2_internal.cuh", "p2_kernels.cuh", "p2_interp.cuh", "p2_solver.h", "p2_sweep.cuh", "p2_zmarch.cuh"]
+HEADERS = ["p2_internal.cuh", "p2_kernels.cuh", "p2_interp.cuh", "p2_solver.h", "p2_sweep.cuh", "p2_zmarch.cuh", "p2_coarse.cuh"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
               "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall", "--expt-relaxed-constexpr"]
 

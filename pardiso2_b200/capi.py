@@ -21,7 +21,7 @@ EXPORTED = ["p2_default_params", "p2_create", "p2_destroy", "p2_last_error", "p2
             "p2_set_nodes", "p2_stokes_solve", "p2_stokes_solve_resident", "p2_get_solution", "p2_ronurecalc",
             "p2_upload_markers", "p2_ronurecalc_resident", "p2_get_nodes", "p2_debug_apply", "p2_debug_restrict",
             "p2_debug_prolong", "p2_debug_level_fields", "p2_debug_time_smoother", "p2_debug_smooth",
-            "p2_debug_time_sweep", "p2_debug_time_stage", "p2_debug_rows_kernel", "p2_ronurecalc_noalloc", "p2_autotune",
+            "p2_debug_time_sweep", "p2_debug_time_stage", "p2_debug_rows_kernel", "p2_debug_vcycle", "p2_ronurecalc_noalloc", "p2_autotune",
             "p2_movemark", "p2_movemark_resident", "p2_get_markers", "p2_stress_strain",
             "p2_stokes_solve_batch", "p2_movemark_strain", "p2_ronurecalc_powerlaw", "p2_effbulk_visc",
             "p2_default_heat_params", "p2_heat_set_bc", "p2_titerate", "p2_prn_read_header", "p2_prn_read",
@@ -422,9 +422,10 @@ def _debug_sigs(L):
     L.p2_debug_time_sweep.argtypes = [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_double)]
     L.p2_debug_time_stage.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_double)]
     L.p2_debug_rows_kernel.argtypes = [C.c_void_p, C.c_int]
+    L.p2_debug_vcycle.argtypes = [C.c_void_p, _dpp, _dpp]
     for f in ("p2_debug_apply", "p2_debug_restrict", "p2_debug_prolong", "p2_debug_level_fields",
               "p2_debug_time_smoother", "p2_debug_smooth", "p2_debug_time_sweep", "p2_debug_time_stage",
-              "p2_debug_rows_kernel"):
+              "p2_debug_rows_kernel", "p2_debug_vcycle"):
         getattr(L, f).restype = C.c_int
 
 
@@ -482,6 +483,13 @@ class DebugHooks:
     def rows_kernel(self, variant: int):
         """Kernel of the operator rows for later calls (p2_debug_rows_kernel)."""
         self.ctx._check(self.ctx.L.p2_debug_rows_kernel(self.ctx.h, variant), "p2_debug_rows_kernel")
+
+    def vcycle(self, b: np.ndarray) -> np.ndarray:
+        """One preconditioning V-cycle from zero for the level-0 rhs b (p2_debug_vcycle)."""
+        x = np.zeros(b.size, np.float64)
+        self.ctx._check(self.ctx.L.p2_debug_vcycle(self.ctx.h, np.ascontiguousarray(b, np.float64), x),
+                        "p2_debug_vcycle")
+        return x
 
     def level_fields(self, total_nodes: int):
         nu = np.zeros(total_nodes, np.float32)

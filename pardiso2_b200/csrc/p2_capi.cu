@@ -537,6 +537,15 @@ p2_status p2_debug_rows_kernel(p2_ctx *ctx, int variant)
     });
 }
 
+p2_status p2_debug_vcycle(p2_ctx *ctx, const double *b, double *x)
+{
+    return guard(ctx, [&] {
+        if (!b || !x) throw p2::Error(P2_ERR_ARG, "null argument");
+        P2_CUDA_TRY(cudaSetDevice(ctx->s->dev));
+        ctx->s->debug_vcycle(b, x);
+    });
+}
+
 p2_status p2_debug_time_stage(p2_ctx *ctx, int stage, int level, int variant, int reps, double *ms)
 {
     return guard(ctx, [&] {

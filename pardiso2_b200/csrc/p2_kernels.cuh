@@ -25,10 +25,9 @@ constexpr int kThreads = 256;
 // written by k_bc_rows).  Optionally also writes a float copy (the FP32
 // right-hand side of the mixed-precision V-cycle).
 template <typename T, typename S>
-__global__ void k_rows(LevelView<T> L, Fields<T, S> x, Vec4<T> b, Vec4<T> out, Vec4<float> out32, int mode)
+__device__ __forceinline__ void rows_item(const LevelView<T> &L, const Fields<T, S> &x, const Vec4<T> &b,
+                                          const Vec4<T> &out, const Vec4<float> &out32, int mode, int u)
 {
-    pdl_enter();
-    int u = blockIdx.x * blockDim.x + threadIdx.x;
     if (u >= L.n) return;
     int j = u % L.ny, i = (u / L.ny) % L.nx, k = u / (L.nx * L.ny);
     uint8_t m = L.bcm[u];
@@ -47,15 +46,20 @@ __global__ void k_rows(LevelView<T> L, Fields<T, S> x, Vec4<T> b, Vec4<T> out, V
         if (out32.c[0]) out32.c[c][u] = (float)v;
     }
 }
+template <typename T, typename S>
+__global__ void k_rows(LevelView<T> L, Fields<T, S> x, Vec4<T> b, Vec4<T> out, Vec4<float> out32, int mode)
+{
+    pdl_enter();
+    rows_item(L, x, b, out, out32, mode, blockIdx.x * blockDim.x + threadIdx.x);
+}
 
 // Boundary rows x_u = b_u + koef * x_t: residual (mode 0) b_u + koef x_t - x_u,
 // or operator (mode 1) x_u - koef x_t.
 template <typename T, typename S>
-__global__ void k_bc_rows(int nbc, const int *bu, const int *bt, const float *bk, Fields<T, S> x, Vec4<T> b,
-                          Vec4<T> out, Vec4<float> out32, int mode)
+__device__ __forceinline__ void bc_rows_item(int nbc, const int *bu, const int *bt, const float *bk,
+                                             const Fields<T, S> &x, const Vec4<T> &b, const Vec4<T> &out,
+                                             const Vec4<float> &out32, int mode, int q)
 {
-    pdl_enter();
-    int q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= nbc) return;
     int uc = bu[q], c = uc & 3, u = uc >> 2, t = bt[q];
     const S *xs[4] = {x.p, x.vx, x.vy, x.vz};
@@ -63,6 +67,13 @@ __global__ void k_bc_rows(int nbc, const int *bu, const int *bt, const float *bk
     T v = mode == 0 ? b.c[c][u] + xt - (T)xs[c][u] : (T)xs[c][u] - xt;
     out.c[c][u] = v;
     if (out32.c[0]) out32.c[c][u] = (float)v;
+}
+template <typename T, typename S>
+__global__ void k_bc_rows(int nbc, const int *bu, const int *bt, const float *bk, Fields<T, S> x, Vec4<T> b,
+                          Vec4<T> out, Vec4<float> out32, int mode)
+{
+    pdl_enter();
+    bc_rows_item(nbc, bu, bt, bk, x, b, out, out32, mode, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 // All boundary rows in one launch: each row walks its copy chain (the rows
@@ -73,11 +84,9 @@ __global__ void k_bc_rows(int nbc, const int *bu, const int *bt, const float *bk
 constexpr int kMaxBcChain = 8;
 
 template <typename T>
-__global__ void k_bc_set_chain(int nbc, const int *bu, const int *bt, const float *bk, const int *bnext, Vec4<T> x,
-                               Vec4<T> b)
+__device__ __forceinline__ void bc_set_chain_item(int nbc, const int *bu, const int *bt, const float *bk,
+                                                  const int *bnext, const Vec4<T> &x, const Vec4<T> &b, int q)
 {
-    pdl_enter();
-    int q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= nbc) return;
     int chain[kMaxBcChain];
     int m = 0, r = q;
@@ -98,6 +107,13 @@ __global__ void k_bc_set_chain(int nbc, const int *bu, const int *bt, const floa
     uc = bu[q];
     x.c[uc & 3][uc >> 2] = v;
 }
+template <typename T>
+__global__ void k_bc_set_chain(int nbc, const int *bu, const int *bt, const float *bk, const int *bnext, Vec4<T> x,
+                               Vec4<T> b)
+{
+    pdl_enter();
+    bc_set_chain_item(nbc, bu, bt, bk, bnext, x, b, blockIdx.x * blockDim.x + threadIdx.x);
+}
 
 // ---------------------------------------------------------------------------
 // One colour pass of the cell-block smoother (diagonal Vanka / SCGS) over the
@@ -109,11 +125,10 @@ __global__ void k_bc_set_chain(int nbc, const int *bu, const int *bt, const floa
 // cell of each colour), the pressure is updated in place (a cell's pressure is
 // read only by its own face rows among the cells of one colour).
 template <typename T>
-__global__ void k_vanka(LevelView<T> L, T *P, Vec4<T> vin, Vec4<T> vout, Vec4<T> b, T omega, int col)
+__device__ __forceinline__ void vanka_item(const LevelView<T> &L, T *P, const Vec4<T> &vin, const Vec4<T> &vout,
+                                           const Vec4<T> &b, T omega, int col, long t)
 {
-    pdl_enter();
     int half = (L.ny) / 2;  // >= number of cells of one colour on a y-line
-    long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
     long lines = (long)(L.nx - 1) * (L.nz - 1);
     if (t >= lines * half) return;
     int jj = (int)(t % half);
@@ -159,6 +174,12 @@ __global__ void k_vanka(LevelView<T> L, T *P, Vec4<T> vin, Vec4<T> vout, Vec4<T>
     for (int q = 0; q < 6; q++) {
         if (d[q] != (T)0) vout.c[fc[q]][fi[q]] = vin.c[fc[q]][fi[q]] + omega * (r[q] - g[q] * dp) / d[q];
     }
+}
+template <typename T>
+__global__ void k_vanka(LevelView<T> L, T *P, Vec4<T> vin, Vec4<T> vout, Vec4<T> b, T omega, int col)
+{
+    pdl_enter();
+    vanka_item(L, P, vin, vout, b, omega, col, (long)blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -402,7 +423,8 @@ __device__ __forceinline__ void cell_rows(const LevelView<T> &L, const Fields<T,
     const T yz10 = two * eta_at(L, L.eyz, F + 1) * ((vyY - vyYz) * ez0 + (vzY - vz0) * ey1);
     const T yz11 = two * eta_at(L, L.eyz, F + 1 + sz) * ((vyYZ - vyY) * ez1 + (vzYZ - vzZ) * ey1);
     const T *pp = x.p + u;
-    const T p0 = __ldg(pp), pL = __ldg(pp - sy), pR = __ldg(pp + sy), pF = __ldg(pp - 1), pB = __ldg(pp + 1);
+    const T p0 = __ldg(pp), pL = __ldg(pp - sy), pR = __ldg(pp + sy), pF = __ldg(pp - 1),
+            pB = __ldg(pp + 1);
     const T pD = __ldg(pp - sz), pU = __ldg(pp + sz);
     const T cx0 = L.ax.ihc[i - 1], cx1 = L.ax.ihc[i], cy0 = L.ay.ihc[j - 1], cy1 = L.ay.ihc[j];
     const T cz0 = L.az.ihc[k - 1], cz1 = L.az.ihc[k];
@@ -649,12 +671,10 @@ __global__ void __launch_bounds__(128) k_vanka_factor(LevelView<T> L, int col, S
 }
 
 template <typename T>
-__global__ void __launch_bounds__(128, sizeof(T) == 4 ? P2_STORED_MIN_BLOCKS : 3) k_vanka_stored(
-    LevelView<T> L, T *P, Vec4<T> vin, Vec4<T> vout, Vec4<T> b, T omega, int col,
-    const factor_t<T> *__restrict__ blk, long stride)
+__device__ __forceinline__ void vanka_stored_item(const LevelView<T> &L, T *P, const Vec4<T> &vin,
+                                                  const Vec4<T> &vout, const Vec4<T> &b, T omega, int col,
+                                                  const factor_t<T> *__restrict__ blk, long stride, long t)
 {
-    pdl_enter();
-    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
     int i, j, k;
     if (!colour_cell(L, col, t, i, j, k)) return;
     Fields<T, T> x{P, vin.c[1], vin.c[2], vin.c[3]};
@@ -702,6 +722,14 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? P2_STORED_MIN_BLOCKS : 3
     for (int q = 0; q < 6; q++)
         if (act[q]) vout.c[fc[q]][fi[q]] = vin.c[fc[q]][fi[q]] + omega * (y1[q] - dp * y2[q]);
 }
+template <typename T>
+__global__ void __launch_bounds__(128, sizeof(T) == 4 ? P2_STORED_MIN_BLOCKS : 3) k_vanka_stored(
+    LevelView<T> L, T *P, Vec4<T> vin, Vec4<T> vout, Vec4<T> b, T omega, int col,
+    const factor_t<T> *__restrict__ blk, long stride)
+{
+    pdl_enter();
+    vanka_stored_item(L, P, vin, vout, b, omega, col, blk, stride, (long)blockIdx.x * blockDim.x + threadIdx.x);
+}
 
 // ---------------------------------------------------------------------------
 // Transfers.  Per-axis tables (host-built from the reference's index rules,
@@ -734,14 +762,10 @@ __device__ __forceinline__ AxisMap pick_map(const AxisMap (&m)[3], int type)
 constexpr int kRestrictList = 5;  // longest inverse list of one axis (host-checked)
 
 template <typename T>
-__global__ void k_restrict_compat(LevelView<T> F, Vec4<T> rf, LevelView<T> Cl, Vec4<T> bc, Vec4<T> xc,
-                                  TransferView tv, int scale_p, double vol_total, double *partial,
-                                  unsigned *ticket, double *sums)
+__device__ __forceinline__ double restrict_item(const LevelView<T> &F, const Vec4<T> &rf, const LevelView<T> &Cl,
+                                               const Vec4<T> &bc, const Vec4<T> &xc, const TransferView &tv,
+                                               int scale_p, long t)
 {
-    pdl_enter();
-    __shared__ double sh[32];
-    __shared__ bool last;
-    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
     const int n = Cl.n;
     double contrib = 0;
     if (t < 4L * n) {
@@ -808,6 +832,18 @@ __global__ void k_restrict_compat(LevelView<T> F, Vec4<T> rf, LevelView<T> Cl, V
         }
         bcc[v] = out;
     }
+    return contrib;
+}
+template <typename T>
+__global__ void k_restrict_compat(LevelView<T> F, Vec4<T> rf, LevelView<T> Cl, Vec4<T> bc, Vec4<T> xc,
+                                  TransferView tv, int scale_p, double vol_total, double *partial,
+                                  unsigned *ticket, double *sums)
+{
+    pdl_enter();
+    __shared__ double sh[32];
+    __shared__ bool last;
+    const double contrib =
+        restrict_item(F, rf, Cl, bc, xc, tv, scale_p, (long)blockIdx.x * blockDim.x + threadIdx.x);
     const double bsum = block_sum(contrib, sh);
     if (threadIdx.x == 0) {
         partial[blockIdx.x] = bsum;
@@ -830,10 +866,9 @@ __global__ void k_restrict_compat(LevelView<T> F, Vec4<T> rf, LevelView<T> Cl, V
 
 // x_f += sum_c w x_c * (p1koef | v1koef) over every fine unknown position.
 template <typename T>
-__global__ void k_prolong(LevelView<T> F, Vec4<T> xf, LevelView<T> Cl, Vec4<T> xc, TransferView tv, T p1, T v1)
+__device__ __forceinline__ void prolong_item(const LevelView<T> &F, const Vec4<T> &xf, const LevelView<T> &Cl,
+                                             const Vec4<T> &xc, const TransferView &tv, T p1, T v1, int u)
 {
-    pdl_enter();
-    int u = blockIdx.x * blockDim.x + threadIdx.x;
     if (u >= F.n) return;
     int j = u % F.ny, i = (u / F.ny) % F.nx, k = u / (F.nx * F.ny);
     for (int c = 0; c < 4; c++) {
@@ -854,6 +889,12 @@ __global__ void k_prolong(LevelView<T> F, Vec4<T> xf, LevelView<T> Cl, Vec4<T> x
                 }
         xf.c[c][u] += s * (c == 0 ? p1 : v1);
     }
+}
+template <typename T>
+__global__ void k_prolong(LevelView<T> F, Vec4<T> xf, LevelView<T> Cl, Vec4<T> xc, TransferView tv, T p1, T v1)
+{
+    pdl_enter();
+    prolong_item(F, xf, Cl, xc, tv, p1, v1, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 // ronurestrict (move3mgNew.c:3386-3527): coarse nu, ro as weighted averages
@@ -1064,14 +1105,18 @@ __global__ void k_dots_final(int nd, int nparts, const double *partial, double *
 
 // Sum of volume * b_P over continuity rows and of the volumes (compatibility).
 template <typename T>
+__device__ __forceinline__ void compat_apply_item(const LevelView<T> &L, T *bp, double s0, double s1, int u)
+{
+    if (u >= L.n || s1 <= 0) return;
+    int j = u % L.ny, i = (u / L.ny) % L.nx, k = u / (L.nx * L.ny);
+    if (i == 0 || j == 0 || k == 0 || (L.bcm[u] & BC_P)) return;
+    bp[u] -= (T)(s0 / s1);
+}
+template <typename T>
 __global__ void k_compat_apply(LevelView<T> L, T *bp, const double *sums)
 {
     pdl_enter();
-    int u = blockIdx.x * blockDim.x + threadIdx.x;
-    if (u >= L.n || sums[1] <= 0) return;
-    int j = u % L.ny, i = (u / L.ny) % L.nx, k = u / (L.nx * L.ny);
-    if (i == 0 || j == 0 || k == 0 || (L.bcm[u] & BC_P)) return;
-    bp[u] -= (T)(sums[0] / sums[1]);
+    compat_apply_item(L, bp, sums[0], sums[1], blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -1099,6 +1144,89 @@ __global__ void k_cgs_update(int n, const double *coef, Vec4<double> y, VecList 
         y.c[c][u] = sy;
         z.c[c][u] = sz;
     }
+}
+
+// GCR scalars kept on the device (no host round trip inside an iteration):
+// coef[j] = (q, Q_j) / (Q_j, Q_j) for the k stored directions.
+__global__ void k_gcr_coef(int k, const double *dots, const double *qq, double *coef)
+{
+    const int j = threadIdx.x;
+    if (j < k) coef[j] = dots[j] / qq[j];
+}
+// qq_k = (q', q') and alpha = (r, q') / qq_k from dots[0], dots[1]; a
+// direction without a positive norm sets flag[0] = 1 and alpha = 0.
+__global__ void k_gcr_alpha(const double *dots, double *qqk, double *alpha, double *flag)
+{
+    if (threadIdx.x != 0) return;
+    const double qq = dots[0];
+    qqk[0] = qq;
+    if (qq > 0) {
+        alpha[0] = dots[1] / qq;
+    } else {
+        alpha[0] = 0;
+        flag[0] = 1;
+    }
+}
+
+// Classical Gram-Schmidt update of the new direction with its dot products:
+//   q' = q - sum_j coef_j Q_j (in place), z' = z - sum_j coef_j Z_j (z read
+//   from zs, stored as S; z' written to zo, which may be zs),
+// and per block the partial sums of (q', q') and (r, q'), in the node loop
+// of k_dots_partial (kRedBlocks blocks of kThreads threads, components outer,
+// nodes strided, the pinned pressure cell skipped), so the sums are the ones
+// a separate dot-product pass over q' would give.  NV, the number of stored
+// directions, is a template parameter: the coefficients stay in registers and
+// the loads of all directions of a node are issued together.
+template <int NV, typename S>
+__global__ void k_cgs_update_dots(int n, const double *coef, Vec4<double> q, VecList X, Vec4<S> zs,
+                                  Vec4<double> zo, VecList Z, Vec4<double> r, int skip_node, double *partial)
+{
+    __shared__ double sh[32];
+    double cf[NV > 0 ? NV : 1];
+#pragma unroll
+    for (int j = 0; j < NV; j++) cf[j] = coef[j];
+    double sqq = 0, srq = 0;
+    const int stride = gridDim.x * blockDim.x;
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+        for (int u = blockIdx.x * blockDim.x + threadIdx.x; u < n; u += stride) {
+            double sy = q.c[c][u], sz = (double)zs.c[c][u];
+#pragma unroll
+            for (int j = 0; j < NV; j++) {
+                sy -= cf[j] * X.v[j][c][u];
+                sz -= cf[j] * Z.v[j][c][u];
+            }
+            q.c[c][u] = sy;
+            zo.c[c][u] = sz;
+            if (c == 0 && u == skip_node) continue;
+            sqq += sy * sy;
+            srq += r.c[c][u] * sy;
+        }
+    }
+    const double t0 = block_sum(sqq, sh);
+    if (threadIdx.x == 0) partial[blockIdx.x] = t0;
+    const double t1 = block_sum(srq, sh);
+    if (threadIdx.x == 0) partial[gridDim.x + blockIdx.x] = t1;
+}
+
+// k_cgs_update_dots<nv, S> on kRedBlocks blocks of kThreads threads
+template <typename S>
+inline cudaError_t launch_cgs_update_dots(cudaStream_t st, int nv, int n, const double *coef, const Vec4<double> &q,
+                                          const VecList &X, const Vec4<S> &zs, const Vec4<double> &zo,
+                                          const VecList &Z, const Vec4<double> &r, int skip_node, double *partial)
+{
+    switch (nv) {
+#define P2_CGS_CASE(N)                                                                                          \
+    case N:                                                                                                     \
+        k_cgs_update_dots<N, S><<<kRedBlocks, kThreads, 0, st>>>(n, coef, q, X, zs, zo, Z, r, skip_node, partial); \
+        break;
+        P2_CGS_CASE(0) P2_CGS_CASE(1) P2_CGS_CASE(2) P2_CGS_CASE(3) P2_CGS_CASE(4) P2_CGS_CASE(5) P2_CGS_CASE(6)
+        P2_CGS_CASE(7) P2_CGS_CASE(8) P2_CGS_CASE(9) P2_CGS_CASE(10) P2_CGS_CASE(11) P2_CGS_CASE(12)
+        P2_CGS_CASE(13) P2_CGS_CASE(14) P2_CGS_CASE(15) P2_CGS_CASE(16) P2_CGS_CASE(17)
+#undef P2_CGS_CASE
+    default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
 }
 
 __global__ void k_f32_to_f64(int n, Vec4<float> a, Vec4<double> b)

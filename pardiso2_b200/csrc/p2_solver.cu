@@ -24,6 +24,7 @@
 #include "p2_solver.h"
 #include "p2_sweep.cuh"
 #include "p2_zmarch.cuh"
+#include "p2_coarse.cuh"
 
 namespace p2 {
 
@@ -237,6 +238,7 @@ Solver::~Solver()
     heat_mk_arena.release();
     heat = HeatState{};
     for (int i = 0; i < 8; i++) cudaEventDestroy(ev[i]);
+    for (auto e : vc_ev) cudaEventDestroy(e);
     if (ev_lu) cudaEventDestroy(ev_lu);
     if (st_lu) cudaStreamDestroy(st_lu);
     if (st) cudaStreamDestroy(st);
@@ -578,7 +580,10 @@ void Solver::allocate_work()
             const size_t tsz = prm.precision == 0 ? sizeof(factor_t<float>) : sizeof(factor_t<double>);
             Lv.blk = arena.alloc(tsz * 2 * kBlkEntries * (size_t)Lv.blk_stride);
         }
-        if (prm.precision == 1 || l == 0) { v64(Lv.x64); v64(Lv.y64); v64(Lv.b64); v64(Lv.r64); }
+        if (prm.precision == 1 || l == 0) {
+            v64(Lv.x64); v64(Lv.y64); v64(Lv.r64);
+            if (!(prm.precision == 1 && l == 0)) v64(Lv.b64);  // FP64 level 0: gr, set below
+        }
         if (prm.precision == 1 && l > 0) {}
     }
     // level-0 raw fields
@@ -598,6 +603,8 @@ void Solver::allocate_work()
         v.n = (int)n0;
     };
     v64n(gx); v64n(gb); v64n(gr);
+    if (prm.precision == 1) L[0].b64 = gr;  // the FP64 cycle's level-0 right-hand side is the residual
+    qq_dev = (double *)arena.alloc(sizeof(double) * m);
     Z.assign(m, Vec4<double>());
     Q.assign(m, Vec4<double>());
     for (int q = 0; q < m; q++) { v64n(Z[q]); v64n(Q[q]); }
@@ -745,46 +752,6 @@ __global__ void k_probe_rows(LevelView<double> Lc, const double *probes, const i
     }
 }
 
-// b_F = b on the free unknowns
-template <typename T>
-__global__ void k_coarse_gather(int nF, const int *fre, Vec4<T> b, T *bF)
-{
-    pdl_enter();
-    int q = blockIdx.x * blockDim.x + threadIdx.x;
-    if (q >= nF) return;
-    int uc = fre[q];
-    bF[q] = b.c[uc & 3][uc >> 2];
-}
-template <typename T>
-__global__ void k_coarse_scatter(int nF, const int *fre, const T *xF, Vec4<T> x)
-{
-    pdl_enter();
-    int q = blockIdx.x * blockDim.x + threadIdx.x;
-    if (q >= nF) return;
-    int uc = fre[q];
-    x.c[uc & 3][uc >> 2] = xF[q];
-}
-// y = Ainv b  (column-major nF x nF), one warp per 32 rows slice of columns.
-template <typename T>
-__global__ void k_gemv(int n, const T *A, const T *b, T *y)
-{
-    pdl_enter();
-    // block: 256 threads = 8 warps; rows r0..r0+31 per block, warps split the columns
-    __shared__ T part[8][33];
-    int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    int r = blockIdx.x * 32 + lane;
-    T s = 0;
-    if (r < n)
-        for (int c = w; c < n; c += 8) s += A[(size_t)c * n + r] * __ldg(b + c);
-    part[w][lane] = s;
-    __syncthreads();
-    if (w == 0 && r < n) {
-        T t = 0;
-        for (int q = 0; q < 8; q++) t += part[q][lane];
-        y[r] = t;
-    }
-}
-
 void Solver::coarse_setup()
 {
     // an LU left running by a solve that ended in an error still reads A_c
@@ -917,7 +884,7 @@ template <typename T, typename S>
 static void launch_rows(cudaStream_t st, bool pdl, const LevelView<T> &V, const Fields<T, S> &f, const Vec4<T> &b,
                         Vec4<T> &out, const Vec4<float> &o32, int mode, int variant = 0)
 {
-    if (variant == 0) variant = (sizeof(S) == 4 && V.n >= kZmMinNodes) ? 2 : 1;
+    if (variant == 0) variant = (sizeof(T) == 4 && V.n >= kZmMinNodes) ? 2 : 1;
     if (variant == 1) {
         if (pdl) pdl_launch(st, nblk(V.n), kThreads, k_rows<T, S>, V, f, b, out, o32, mode);
         else {
@@ -1180,38 +1147,36 @@ static DotJob job(const Vec4<double> &a, const Vec4<double> &b)
     return j;
 }
 
-// out = b - A x (mode 0) or A x (mode 1) on level 0 in FP64; r32 optional.
-void Solver::rows0(const Vec4<double> &x, Vec4<double> &out, Vec4<float> *r32, int mode)
+// out = b - A x (mode 0) or A x (mode 1) on level 0 in FP64 (x stored as
+// S); r32 optional.
+template <typename S>
+void Solver::rows0(const Vec4<S> &x, Vec4<double> &out, Vec4<float> *r32, int mode)
 {
     Level &L0 = L[0];
     LevelView<double> V = view<double>(0, true);
-    Fields<double, double> f{x.c[0], x.c[1], x.c[2], x.c[3]};
+    Fields<double, S> f{x.c[0], x.c[1], x.c[2], x.c[3]};
     Vec4<float> o32 = r32 ? *r32 : Vec4<float>();
-    launch_rows<double, double>(st, false, V, f, gb, out, o32, mode, dbg_rows_variant);
-    if (L0.nbc)
-        k_bc_rows<double, double><<<nblk(L0.nbc), kThreads, 0, st>>>(L0.nbc, L0.bu, L0.bt, L0.bk, f, gb, out, o32,
-                                                                   mode); P2_COUNT_LAUNCH();
+    launch_rows<double, S>(st, false, V, f, gb, out, o32, mode, dbg_rows_variant);
+    if (L0.nbc) {
+        k_bc_rows<double, S><<<nblk(L0.nbc), kThreads, 0, st>>>(L0.nbc, L0.bu, L0.bt, L0.bk, f, gb, out, o32, mode);
+        P2_COUNT_LAUNCH();
+    }
 }
 
-// z = V(r): one preconditioning V-cycle for the level-0 right-hand side r.
-void Solver::precondition(Vec4<double> &z)
+// One preconditioning V-cycle from zero for the level-0 right-hand side r:
+// the mixed cycle reads float(r), which the true residual wrote into b32;
+// the FP64 cycle's level-0 right-hand side is r itself (b64 of level 0 is
+// gr).  The correction stays in x32 / x64; the Gram-Schmidt update reads it
+// from there.
+void Solver::precondition()
 {
     Level &L0 = L[0];
     if (prm.precision == 0) {
-        // r32 already holds float(r); run the FP32 cycle on b32 := r32
-        for (int c = 0; c < 4; c++)
-            P2_CUDA_TRY(cudaMemcpyAsync(L0.b32.c[c], L0.r32.c[c], sizeof(float) * L0.n, cudaMemcpyDeviceToDevice, st));
         for (int c = 0; c < 4; c++) P2_CUDA_TRY(cudaMemsetAsync(L0.x32.c[c], 0, sizeof(float) * L0.n, st));
         run_vcycle_graph<float>();
-        k_f32_to_f64<<<nblk(L0.n), kThreads, 0, st>>>(L0.n, L0.x32, z); P2_COUNT_LAUNCH();
     } else {
-        for (int c = 0; c < 4; c++) {
-            P2_CUDA_TRY(cudaMemcpyAsync(L0.b64.c[c], gr.c[c], sizeof(double) * L0.n, cudaMemcpyDeviceToDevice, st));
-            P2_CUDA_TRY(cudaMemsetAsync(L0.x64.c[c], 0, sizeof(double) * L0.n, st));
-        }
+        for (int c = 0; c < 4; c++) P2_CUDA_TRY(cudaMemsetAsync(L0.x64.c[c], 0, sizeof(double) * L0.n, st));
         run_vcycle_graph<double>();
-        for (int c = 0; c < 4; c++)
-            P2_CUDA_TRY(cudaMemcpyAsync(z.c[c], L0.x64.c[c], sizeof(double) * L0.n, cudaMemcpyDeviceToDevice, st));
     }
 }
 
@@ -1280,58 +1245,78 @@ p2_solve_info Solver::solve()
     double bnorm = std::sqrt(bnorm2);
     if (!(bnorm > 0)) bnorm = 1.0;
     int m = restart, k = 0, it = 0;
-    std::vector<double> qq(m, 1.0);
     float vc_ms = 0;
     double rel = 0;
+    if ((int)vc_ev.size() < 2) {
+        vc_ev.resize(2);
+        for (auto &e : vc_ev) P2_CUDA_TRY(cudaEventCreate(&e));
+    }
+    std::vector<std::pair<int, int>> vc_marks;  // event pairs around each V-cycle
+    P2_CUDA_TRY(cudaMemsetAsync(scal + 4, 0, sizeof(double), st));  // non-positive direction norm flag
     for (;;) {
-        // true FP64 residual (and its float copy for the mixed-precision cycle)
-        rows0(gx, gr, prm.precision == 0 ? &L0.r32 : nullptr, 0);
+        // true FP64 residual (its float copy is the mixed cycle's right-hand side)
+        rows0(gx, gr, prm.precision == 0 ? &L0.b32 : nullptr, 0);
+        // the one host synchronisation of an iteration: the residual norm and
+        // the flag of the previous iteration's direction
         J.nd = 1;
         J.j[0] = job(gr, gr);
-        dots_sync(J);
+        P2_CUDA_TRY(launch_dots(st, J, L0.n, L0.pin, partial)); P2_COUNT_LAUNCH();
+        k_dots_final<<<1, 1024, 0, st>>>(1, kRedBlocks, partial, dots); P2_COUNT_LAUNCH();
+        P2_CUDA_TRY(cudaMemcpyAsync(hdots.get(), dots, sizeof(double), cudaMemcpyDeviceToHost, st));
+        P2_CUDA_TRY(cudaMemcpyAsync(hdots.get() + 1, scal + 4, sizeof(double), cudaMemcpyDeviceToHost, st));
+        P2_CUDA_TRY(cudaStreamSynchronize(st));
         double rr = hdots.get()[0];
         rel = std::sqrt(rr) / bnorm;
         if (it == 0) info.rel_residual0 = rel;
         if (verbose) std::fprintf(stderr, "p2cuda: iteration %d rel residual %.3e\n", it, rel);
-        if (!std::isfinite(rel)) { info.status = P2_ERR_NAN; break; }
+        if (hdots.get()[1] != 0.0 || !std::isfinite(rel)) { info.status = P2_ERR_NAN; break; }
         if (rel <= prm.tol) { info.status = P2_OK; break; }
         if (it >= prm.max_iter) { info.status = P2_ERR_NOT_CONVERGED; break; }
         Vec4<double> &z = Z[k], &q = Q[k];
         if (it >= lu_overlap_iters) lu_finish();
         coarse_mode = lu_pending ? 1 : 0;
-        P2_CUDA_TRY(cudaEventRecord(ev[2], st));
-        precondition(z);
-        P2_CUDA_TRY(cudaEventRecord(ev[3], st));
-        rows0(z, q, nullptr, 1);
-        // classical Gram-Schmidt against the stored directions, plus (r,q)
-        J.nd = 0;
-        for (int j = 0; j < k; j++) J.j[J.nd++] = job(q, Q[j]);
-        if (k > 0) {
-            dots_sync(J);
-            std::vector<double> coef(k);
-            for (int j = 0; j < k; j++) coef[j] = hdots.get()[j] / qq[j];
-            P2_CUDA_TRY(cudaMemcpyAsync(scal + 8, coef.data(), sizeof(double) * k, cudaMemcpyHostToDevice, st));
-            VecList X{}, Zl{};
-            for (int j = 0; j < k; j++)
-                for (int c = 0; c < 4; c++) { X.v[j][c] = Q[j].c[c]; Zl.v[j][c] = Z[j].c[c]; }
-            X.nv = Zl.nv = k;
-            k_cgs_update<<<nblk(n), kThreads, 0, st>>>((int)n, scal + 8, q, X, z, Zl); P2_COUNT_LAUNCH();
+        const int e0 = 2 * (int)vc_marks.size();
+        if ((int)vc_ev.size() < e0 + 2) {
+            const size_t old = vc_ev.size();
+            vc_ev.resize(e0 + 2);
+            for (size_t e = old; e < vc_ev.size(); e++) P2_CUDA_TRY(cudaEventCreate(&vc_ev[e]));
         }
-        J.nd = 2;
-        J.j[0] = job(q, q);
-        J.j[1] = job(gr, q);
-        dots_sync(J);
-        qq[k] = hdots.get()[0];
-        if (!(qq[k] > 0)) { info.status = P2_ERR_NAN; break; }
-        double alpha = hdots.get()[1] / qq[k];
-        P2_CUDA_TRY(cudaMemcpyAsync(scal + 2, &alpha, sizeof(double), cudaMemcpyHostToDevice, st));
+        P2_CUDA_TRY(cudaEventRecord(vc_ev[e0], st));
+        precondition();
+        P2_CUDA_TRY(cudaEventRecord(vc_ev[e0 + 1], st));
+        vc_marks.push_back({e0, e0 + 1});
+        // q = A c for the correction c (x32 or x64 of level 0)
+        if (prm.precision == 0) rows0(L0.x32, q, nullptr, 1);
+        else rows0(L0.x64, q, nullptr, 1);
+        // classical Gram-Schmidt against the stored directions: coefficients
+        // on the device, then one pass that updates q and z and sums (q', q')
+        // and (r, q'), then alpha on the device and the solution update
+        if (k > 0) {
+            J.nd = 0;
+            for (int j = 0; j < k; j++) J.j[J.nd++] = job(q, Q[j]);
+            P2_CUDA_TRY(launch_dots(st, J, L0.n, L0.pin, partial)); P2_COUNT_LAUNCH();
+            k_dots_final<<<1, 1024, 0, st>>>(k, kRedBlocks, partial, dots); P2_COUNT_LAUNCH();
+            k_gcr_coef<<<1, 32, 0, st>>>(k, dots, qq_dev, scal + 8); P2_COUNT_LAUNCH();
+        }
+        VecList X{}, Zl{};
+        for (int j = 0; j < k; j++)
+            for (int c = 0; c < 4; c++) { X.v[j][c] = Q[j].c[c]; Zl.v[j][c] = Z[j].c[c]; }
+        X.nv = Zl.nv = k;
+        if (prm.precision == 0)
+            P2_CUDA_TRY(launch_cgs_update_dots<float>(st, k, (int)n, scal + 8, q, X, L0.x32, z, Zl, gr, L0.pin, partial));
+        else
+            P2_CUDA_TRY(launch_cgs_update_dots<double>(st, k, (int)n, scal + 8, q, X, L0.x64, z, Zl, gr, L0.pin, partial));
+        P2_COUNT_LAUNCH();
+        k_dots_final<<<1, 1024, 0, st>>>(2, kRedBlocks, partial, dots); P2_COUNT_LAUNCH();
+        k_gcr_alpha<<<1, 32, 0, st>>>(dots, qq_dev + k, scal + 2, scal + 4); P2_COUNT_LAUNCH();
         k_axpy4<<<nblk(n), kThreads, 0, st>>>((int)n, scal + 2, 1.0, gx, z); P2_COUNT_LAUNCH();
-        float t = 0;
-        P2_CUDA_TRY(cudaEventSynchronize(ev[3]));
-        P2_CUDA_TRY(cudaEventElapsedTime(&t, ev[2], ev[3]));
-        vc_ms += t;
         k = (k + 1) % m;
         it++;
+    }
+    for (const auto &mk : vc_marks) {
+        float t = 0;
+        P2_CUDA_TRY(cudaEventElapsedTime(&t, vc_ev[mk.first], vc_ev[mk.second]));
+        vc_ms += t;
     }
     // the overlapped LU has to be finished (and its pivots checked) before
     // the solve returns; the graphs after it use the exact coarsest solve
@@ -1637,6 +1622,38 @@ void Solver::debug_smooth(int l, int sweeps, const double *b, double *x)
     }
     P2_CUDA_TRY(cudaGetLastError());
     from_vec4(st, X.v, Lv.n, x);
+}
+
+// One preconditioning V-cycle (in the solver's precision, with the exact
+// coarsest solve) from x = 0 for the level-0 right-hand side b.
+void Solver::debug_vcycle(const double *b, double *x)
+{
+    debug_prepare();
+    factor_cells();
+    coarse_setup();
+    lu_finish();
+    coarse_mode = 0;
+    Level &L0 = L[0];
+    TmpVec B(L0.n), X(L0.n);
+    to_vec4(st, b, L0.n, B.v);
+    if (prm.precision == 0) {
+        for (int c = 0; c < 4; c++) {
+            d2f(st, (size_t)L0.n, B.v.c[c], L0.b32.c[c]);
+            P2_CUDA_TRY(cudaMemsetAsync(L0.x32.c[c], 0, sizeof(float) * L0.n, st));
+        }
+        run_vcycle_graph<float>();
+        k_f32_to_f64<<<nblk(L0.n), kThreads, 0, st>>>(L0.n, L0.x32, X.v); P2_COUNT_LAUNCH();
+    } else {
+        for (int c = 0; c < 4; c++) {
+            P2_CUDA_TRY(cudaMemcpyAsync(L0.b64.c[c], B.v.c[c], sizeof(double) * L0.n, cudaMemcpyDeviceToDevice, st));
+            P2_CUDA_TRY(cudaMemsetAsync(L0.x64.c[c], 0, sizeof(double) * L0.n, st));
+        }
+        run_vcycle_graph<double>();
+        for (int c = 0; c < 4; c++)
+            P2_CUDA_TRY(cudaMemcpyAsync(X.v.c[c], L0.x64.c[c], sizeof(double) * L0.n, cudaMemcpyDeviceToDevice, st));
+    }
+    P2_CUDA_TRY(cudaGetLastError());
+    from_vec4(st, X.v, L0.n, x);
 }
 
 // Average device time of one smoother sweep on level l as the V-cycle runs

@@ -152,6 +152,7 @@ class Solver {
     int dbg_rows_variant = 0;     // kernel of the operator rows (launch_rows), 0 = by level size
     void drop_graphs_public() { drop_graphs(); }
     void debug_smooth(int level, int sweeps, const double *b, double *x);
+    void debug_vcycle(const double *b, double *x);
     p2_tune_info autotune(int trial_iters);
     bool verbose = false;
 
@@ -215,6 +216,7 @@ class Solver {
     void factor_cells();
     template <typename T>
     void level_residual(int l);
+
     template <typename T>
     void vcycle();
     template <typename T>
@@ -223,8 +225,11 @@ class Solver {
     void capture_vcycle_graph();
     void set_nodes_device();
     void dots_sync(const DotJobs &jobs);
-    void rows0(const Vec4<double> &x, Vec4<double> &out, Vec4<float> *r32, int mode);
-    void precondition(Vec4<double> &z);
+    template <typename S>
+    void rows0(const Vec4<S> &x, Vec4<double> &out, Vec4<float> *r32, int mode);
+    void precondition();
+    std::vector<cudaEvent_t> vc_ev;  // V-cycle timing events of a solve (reused)
+    double *qq_dev = nullptr;        // (Q_j, Q_j) of the stored directions
     void debug_prepare();
     Grid3 grid3() const;
     void ensure_move_buffers(long nmark);
