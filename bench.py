@@ -625,7 +625,7 @@ def main():
     else:
         from pardiso2_b200.capi import TuneInfo
         tune = TuneInfo(smoother=args.smoother, sweep_growth=args.sweep_growth, est_ms=float("nan"),
-                        rate=float("nan"), candidates=0, trial_iters=0, sweep_max=64)
+                        rate=float("nan"), candidates=0, trial_iters=0, sweep_max=64, restart=args.restart)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
     def one(p):
@@ -678,7 +678,7 @@ def main():
 
     # the plain FP64 solve (FP64 GCR, FP64 V-cycle) for comparison; fewer
     # steps on the large grids (each is about a second there)
-    p64 = P.StokesProblem(m, device=local, precision=1, tol=1e-8, restart=args.restart, smoother=tune.smoother,
+    p64 = P.StokesProblem(m, device=local, precision=1, tol=1e-8, restart=tune.restart, smoother=tune.smoother,
                           sweep_growth=tune.sweep_growth, sweep_max=tune.sweep_max)
     p64.ctx.upload_markers(m.markx, m.marky, m.markz, m.markt, m.rocks.n0, m.rocks.n1, m.rocks.ro)
     p64.ctx.ronurecalc_resident()
@@ -761,8 +761,8 @@ def main():
         "solver": {"smoother": ("full" if tune.smoother else "diagonal") + " cell-block Vanka, autotuned",
                    "sweeps": "4 pre + 4 post on level 0, x%d per coarser level, at most %d" % (tune.sweep_growth,
                                                                                                 tune.sweep_max),
-                   "mixed": "FP64 GCR(%d) (true residual and update in FP64), FP32 V-cycle" % args.restart,
-                   "fp64": "FP64 GCR(%d), FP64 V-cycle" % args.restart},
+                   "mixed": "FP64 GCR(%d) (true residual and update in FP64), FP32 V-cycle" % tune.restart,
+                   "fp64": "FP64 GCR(%d), FP64 V-cycle" % tune.restart},
         "converged": all(i.status == 0 for i in infos), "iterations": last.iterations,
         "rel_residual": last.rel_residual,
         "fp64_ms_per_solve": fp64_ms, "fp64_steps": k64, "iterations_fp64": i64[-1].iterations,

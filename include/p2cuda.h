@@ -103,6 +103,8 @@ typedef struct {
     int trial_iters;     /* outer iterations per trial */
     int sweep_max;       /* most sweeps on any level: sweeps on level l =
                             min(sweep_max, npre[0] * sweep_growth^l) */
+    int restart;         /* chosen GCR restart length (12 or the configured one, whichever
+                            full solve of the chosen schedule was faster) */
 } p2_tune_info;
 
 /* Fill p with the reference's defaults (mode.t3c) and this library's. */

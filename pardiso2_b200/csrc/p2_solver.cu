@@ -871,20 +871,23 @@ Vec4<float> &r_of<float>(Level &Lv) { return Lv.r32; }
 template <>
 Vec4<double> &r_of<double>(Level &Lv) { return Lv.r64; }
 
-// Levels of at least this many nodes evaluate their rows with k_rows_zm.
-constexpr long kZmMinNodes = 1L << 17;
+// FP32 rows run k_rows_zm when its grid has at least this many blocks (8
+// per SM): with fewer, a block's column of planes is a long serial march and
+// the device is not filled (measured at 129^3: 145 against 93 us for k_rows on
+// level 0, 425 blocks; 128 us for 14 MB on level 1, 81 blocks), while at 257^3
+// (2673 blocks) it beats k_rows (0.66 against 0.72 ms).
+constexpr long kZmMinBlocks = 8L * 148;
 
-// Residual / operator rows on a level: out = b - A x (mode 0) or A x
-// (mode 1).  variant 0 picks k_rows_zm for FP32 rows on levels of at least
-// kZmMinNodes nodes and k_rows otherwise (measured at 257^3: k_rows_zm
-// 0.66 ms against k_rows 0.72 ms for the FP32 residual, but 1.33 against
-// 1.08 ms for the FP64 rows, where the double planes leave two blocks per
-// SM); 1 forces k_rows, 2 k_rows_zm (the timing hook compares them).
+static long zm_blocks(int nx, int ny, int nz)
+{
+    return (long)((nx + kZmTX - 1) / kZmTX) * ((ny + kZmTY - 1) / kZmTY) * ((nz + kZmKZ - 1) / kZmKZ);
+}
+
 template <typename T, typename S>
 static void launch_rows(cudaStream_t st, bool pdl, const LevelView<T> &V, const Fields<T, S> &f, const Vec4<T> &b,
                         Vec4<T> &out, const Vec4<float> &o32, int mode, int variant = 0)
 {
-    if (variant == 0) variant = (sizeof(T) == 4 && V.n >= kZmMinNodes) ? 2 : 1;
+    if (variant == 0) variant = (sizeof(T) == 4 && zm_blocks(V.nx, V.ny, V.nz) >= kZmMinBlocks) ? 2 : 1;
     if (variant == 1) {
         if (pdl) pdl_launch(st, nblk(V.n), kThreads, k_rows<T, S>, V, f, b, out, o32, mode);
         else {
@@ -1413,6 +1416,30 @@ p2_tune_info Solver::autotune(int trial_iters)
             prm.npre[l] = (int)std::min<long>(best.sweep_max, base_pre * f);
             prm.npost[l] = (int)std::min<long>(best.sweep_max, base_post * f);
         }
+    }
+    // GCR restart length: full solves of the chosen schedule with the
+    // configured length and with 12 (the directions stay allocated for the
+    // longer one); the trials above stop before a restart shows its effect
+    best.restart = restart;
+    if (std::isfinite(best.est_ms) && restart > 12) {
+        const int configured = restart;
+        double t_best = INFINITY;
+        for (int m : {configured, 12}) {
+            restart = m;
+            drop_graphs();
+            set_initial(nullptr, nullptr, nullptr, nullptr);
+            if (prm.precision == 0) capture_vcycle_graph<float>();
+            else capture_vcycle_graph<double>();
+            p2_solve_info in = solve();
+            const double t = in.status == P2_OK ? in.ms_total - in.ms_setup : INFINITY;
+            if (verbose)
+                std::fprintf(stderr, "p2cuda: autotune restart %d: %d its, %.1f ms\n", m, in.iterations, t);
+            if (t < t_best) {
+                t_best = t;
+                best.restart = m;
+            }
+        }
+        restart = best.restart;
     }
     drop_graphs();
     set_initial(nullptr, nullptr, nullptr, nullptr);

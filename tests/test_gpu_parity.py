@@ -131,6 +131,7 @@ def test_autotune_choice_reaches_the_reference_solution(gcase):
     tune = prob.autotune(6)
     assert tune.candidates == 6 and tune.smoother in (0, 1) and tune.sweep_growth in (1, 2)
     assert tune.sweep_max in (16, 64)
+    assert tune.restart in (12, 16)
     assert np.isfinite(tune.est_ms) and 0 < tune.rate < 1
     sol, info = prob.solve_fp64()
     prob.close()
