@@ -625,7 +625,8 @@ def main():
     else:
         from pardiso2_b200.capi import TuneInfo
         tune = TuneInfo(smoother=args.smoother, sweep_growth=args.sweep_growth, est_ms=float("nan"),
-                        rate=float("nan"), candidates=0, trial_iters=0, sweep_max=64, restart=args.restart)
+                        rate=float("nan"), candidates=0, trial_iters=0, sweep_max=64, restart=args.restart,
+                        sweeps0=4)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
     def one(p):
@@ -678,10 +679,13 @@ def main():
 
     # the plain FP64 solve (FP64 GCR, FP64 V-cycle) for comparison; fewer
     # steps on the large grids (each is about a second there)
-    p64 = P.StokesProblem(m, device=local, precision=1, tol=1e-8, restart=tune.restart, smoother=tune.smoother,
-                          sweep_growth=tune.sweep_growth, sweep_max=tune.sweep_max)
+    # the FP64 solve gets its own autotuned schedule (the same candidates),
+    # so each precision runs its best configuration
+    p64 = P.StokesProblem(m, device=local, precision=1, tol=1e-8, restart=args.restart, smoother=args.smoother,
+                          sweep_growth=args.sweep_growth)
     p64.ctx.upload_markers(m.markx, m.marky, m.markz, m.markt, m.rocks.n0, m.rocks.n1, m.rocks.ro)
     p64.ctx.ronurecalc_resident()
+    tune64 = p64.autotune(args.tune_iters) if args.tune_iters > 0 else tune
     k64 = min(args.steps, 3) if big else args.steps
     for _ in range(max(1, min(args.warmup, 1 if big else args.warmup))):
         one(p64)
@@ -759,10 +763,13 @@ def main():
         "vs_baseline": None, "dtype": "f32 V-cycle / f64 outer GCR", "data": "synthetic",
         "config": config_dict(args.config, m, world),
         "solver": {"smoother": ("full" if tune.smoother else "diagonal") + " cell-block Vanka, autotuned",
-                   "sweeps": "4 pre + 4 post on level 0, x%d per coarser level, at most %d" % (tune.sweep_growth,
-                                                                                                tune.sweep_max),
+                   "sweeps": "%d pre + %d post on level 0; 4 x %d^l on level l >= 1, at most %d"
+                             % (tune.sweeps0, tune.sweeps0, tune.sweep_growth, tune.sweep_max),
                    "mixed": "FP64 GCR(%d) (true residual and update in FP64), FP32 V-cycle" % tune.restart,
-                   "fp64": "FP64 GCR(%d), FP64 V-cycle" % tune.restart},
+                   "fp64": "FP64 GCR(%d), FP64 V-cycle, %s cell block, %d + %d sweeps on level 0, 4 x %d^l on level "
+                           "l >= 1 at most %d (autotuned on its own)"
+                           % (tune64.restart, "full" if tune64.smoother else "diagonal", tune64.sweeps0,
+                              tune64.sweeps0, tune64.sweep_growth, tune64.sweep_max)},
         "converged": all(i.status == 0 for i in infos), "iterations": last.iterations,
         "rel_residual": last.rel_residual,
         "fp64_ms_per_solve": fp64_ms, "fp64_steps": k64, "iterations_fp64": i64[-1].iterations,
@@ -789,6 +796,7 @@ def main():
                         "launches": 2}
     line["heat"] = heat_leg(prob, m, args, rank == 0 and world == 1 and not args.no_cpu_baseline and args.config <= 2)
     line["autotune"] = tune.as_dict()
+    line["autotune_fp64"] = tune64.as_dict()
     prob.close()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1

@@ -101,10 +101,11 @@ typedef struct {
     double rate;         /* measured residual reduction per outer iteration */
     int candidates;      /* configurations tried */
     int trial_iters;     /* outer iterations per trial */
-    int sweep_max;       /* most sweeps on any level: sweeps on level l =
-                            min(sweep_max, npre[0] * sweep_growth^l) */
+    int sweep_max;       /* most sweeps on any level: sweeps on level l >= 1 =
+                            min(sweep_max, npre[0] * sweep_growth^l) with the configured npre[0] */
     int restart;         /* chosen GCR restart length (12 or the configured one, whichever
                             full solve of the chosen schedule was faster) */
+    int sweeps0;         /* pre- (and post-) sweeps on level 0: npre[0], or half of it */
 } p2_tune_info;
 
 /* Fill p with the reference's defaults (mode.t3c) and this library's. */
@@ -154,10 +155,12 @@ p2_status p2_get_solution(p2_ctx *ctx, double *vx, double *vy, double *vz, doubl
 /* Smoother autotuner (no counterpart in the reference, whose sweep counts
  * come from mode.t3c multinnn): on the resident node fields, runs
  * trial_iters outer iterations from a zero guess with each candidate (full
- * or diagonal cell block, constant or doubling sweeps per coarser level),
- * estimates each candidate's time to p2_params.tol from its measured rate
- * and time per iteration, and keeps the cheapest in this context's
- * parameters.  Call it once per model before the time loop. */
+ * or diagonal cell block, constant or doubling sweeps per coarser level, the
+ * configured or half the sweeps on level 0), estimates each candidate's time
+ * to p2_params.tol from its measured rate and time per iteration, keeps the
+ * cheapest in this context's parameters, then picks the GCR restart length
+ * (12 or the configured one) by two full solves.  Call it once per model
+ * before the time loop. */
 p2_status p2_autotune(p2_ctx *ctx, int trial_iters, p2_tune_info *info);
 
 /* ronurecalc(): marker -> node viscosity/density interpolation.  Rock

@@ -41,7 +41,7 @@ class Params(C.Structure):
 class TuneInfo(C.Structure):
     _fields_ = [("smoother", C.c_int), ("sweep_growth", C.c_int), ("est_ms", C.c_double), ("rate", C.c_double),
                 ("candidates", C.c_int), ("trial_iters", C.c_int), ("sweep_max", C.c_int),
-                ("restart", C.c_int)]
+                ("restart", C.c_int), ("sweeps0", C.c_int)]
 
     def as_dict(self) -> Dict:
         return {k: getattr(self, k) for k, _ in self._fields_}

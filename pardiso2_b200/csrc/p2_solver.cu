@@ -1356,10 +1356,15 @@ p2_tune_info Solver::autotune(int trial_iters)
     best.est_ms = INFINITY;
     best.trial_iters = trial_iters;
     double setup_ms = INFINITY;
-    // candidates: smoother x (sweep growth per coarser level, most sweeps per level)
-    struct Cand { int smoother, growth, cap; };
-    const Cand cands[6] = {{1, 1, 64}, {1, 2, 64}, {1, 2, 16}, {0, 1, 64}, {0, 2, 64}, {0, 2, 16}};
-    for (const Cand &cd : cands) {
+    // candidates: smoother x (sweep growth per coarser level, most sweeps per
+    // level) x (sweeps on level 0: the configured ones or half of them; the
+    // coarser levels keep theirs)
+    struct Cand { int smoother, growth, cap, half0; };
+    const Cand cands[12] = {{1, 1, 64, 0}, {1, 2, 64, 0}, {1, 2, 16, 0}, {0, 1, 64, 0}, {0, 2, 64, 0}, {0, 2, 16, 0},
+                            {1, 1, 64, 1}, {1, 2, 64, 1}, {1, 2, 16, 1}, {0, 1, 64, 1}, {0, 2, 64, 1}, {0, 2, 16, 1}};
+    const int ncand = (base_pre >= 2 && base_post >= 2) ? 12 : 6;
+    for (int ci = 0; ci < ncand; ci++) {
+        const Cand &cd = cands[ci];
         {
             prm = saved;
             prm.smoother = cd.smoother;
@@ -1369,6 +1374,10 @@ p2_tune_info Solver::autotune(int trial_iters)
                 for (int q = 0; q < l; q++) f *= cd.growth;
                 prm.npre[l] = (int)std::min<long>(cd.cap, base_pre * f);
                 prm.npost[l] = (int)std::min<long>(cd.cap, base_post * f);
+            }
+            if (cd.half0) {
+                prm.npre[0] = base_pre / 2;
+                prm.npost[0] = base_post / 2;
             }
             drop_graphs();
             set_initial(nullptr, nullptr, nullptr, nullptr);
@@ -1389,14 +1398,15 @@ p2_tune_info Solver::autotune(int trial_iters)
             }
             setup_ms = std::min(setup_ms, (double)in.ms_setup);
             if (verbose)
-                std::fprintf(stderr, "p2cuda: autotune smoother %d growth %d cap %d: %d its, rate %.3f, est %.1f ms\n",
-                             prm.smoother, cd.growth, cd.cap, in.iterations, rate, est);
+                std::fprintf(stderr, "p2cuda: autotune smoother %d growth %d cap %d level-0 sweeps %d: %d its, rate %.3f, "
+                             "est %.1f ms\n", prm.smoother, cd.growth, cd.cap, prm.npre[0], in.iterations, rate, est);
             best.candidates++;
             if (est < best.est_ms) {
                 best.est_ms = est;
                 best.smoother = prm.smoother;
                 best.sweep_growth = cd.growth;
                 best.sweep_max = cd.cap;
+                best.sweeps0 = prm.npre[0];
                 best.rate = rate;
             }
         }
@@ -1408,6 +1418,7 @@ p2_tune_info Solver::autotune(int trial_iters)
         best.smoother = saved.smoother;
         best.sweep_growth = 1;
         best.sweep_max = 64;
+        best.sweeps0 = saved.npre[0];
     } else {
         prm.smoother = best.smoother;
         for (int l = 0; l < nl; l++) {
@@ -1415,6 +1426,10 @@ p2_tune_info Solver::autotune(int trial_iters)
             for (int q = 0; q < l; q++) f *= best.sweep_growth;
             prm.npre[l] = (int)std::min<long>(best.sweep_max, base_pre * f);
             prm.npost[l] = (int)std::min<long>(best.sweep_max, base_post * f);
+        }
+        if (best.sweeps0 != base_pre) {
+            prm.npre[0] = base_pre / 2;
+            prm.npost[0] = base_post / 2;
         }
     }
     // GCR restart length: full solves of the chosen schedule with the

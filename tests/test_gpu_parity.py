@@ -129,7 +129,8 @@ def test_autotune_choice_reaches_the_reference_solution(gcase):
     prob = P.StokesProblem(m, tol=1e-8)
     prob.set_nodes({k: g["node_" + k] for k in FIELDS})
     tune = prob.autotune(6)
-    assert tune.candidates == 6 and tune.smoother in (0, 1) and tune.sweep_growth in (1, 2)
+    assert tune.candidates == 12 and tune.smoother in (0, 1) and tune.sweep_growth in (1, 2)
+    assert tune.sweeps0 in (prob.params.npre[0], prob.params.npre[0] // 2)
     assert tune.sweep_max in (16, 64)
     assert tune.restart in (12, 16)
     assert np.isfinite(tune.est_ms) and 0 < tune.rate < 1
