@@ -1130,22 +1130,6 @@ __global__ void k_axpy4(int n, const double *alpha, double sign, Vec4<double> y,
     for (int c = 0; c < 4; c++) y.c[c][u] += a * x.c[c][u];
 }
 
-// y -= sum_q coef[q] * X_q  and  z -= sum_q coef[q] * Z_q  (classical Gram-Schmidt)
-__global__ void k_cgs_update(int n, const double *coef, Vec4<double> y, VecList X, Vec4<double> z, VecList Z)
-{
-    int u = blockIdx.x * blockDim.x + threadIdx.x;
-    if (u >= n) return;
-    for (int c = 0; c < 4; c++) {
-        double sy = y.c[c][u], sz = z.c[c][u];
-        for (int q = 0; q < X.nv; q++) {
-            sy -= coef[q] * X.v[q][c][u];
-            sz -= coef[q] * Z.v[q][c][u];
-        }
-        y.c[c][u] = sy;
-        z.c[c][u] = sz;
-    }
-}
-
 // GCR scalars kept on the device (no host round trip inside an iteration):
 // coef[j] = (q, Q_j) / (Q_j, Q_j) for the k stored directions.
 __global__ void k_gcr_coef(int k, const double *dots, const double *qq, double *coef)
