@@ -427,13 +427,14 @@ p2_status p2_debug_time_sweep(p2_ctx *ctx, int level, int sweeps, double *ms_per
  * that evicts L2: stage 0 the V-cycle residual of `level`, 1 the level-0
  * FP64 true residual, 2 the restriction of `level` to level + 1, 3 the
  * prolongation of level + 1 to `level`, 4 the level-0 FP64 operator.
- * `variant` selects the kernel of the operator rows (0 by level size and
- * precision, 1 one thread per node from global memory, 2 z-marching planes
- * in shared memory). */
+ * `variant` selects the kernel of the operator rows (0 by the level's grid
+ * size and the precision, 1 one thread per node from global memory, 2
+ * z-marching planes in shared memory). */
 p2_status p2_debug_time_stage(p2_ctx *ctx, int stage, int level, int variant, int reps, double *ms);
 /* Kernel of the operator rows for the following calls of this context
- * (variant as for p2_debug_time_stage; 0, the default, chooses by level
- * size).  Captured V-cycle graphs are dropped so that solves use it too. */
+ * (variant as for p2_debug_time_stage; 0, the default, chooses by the
+ * level's grid size and the precision).  Captured V-cycle graphs are dropped
+ * so that solves use it too. */
 p2_status p2_debug_rows_kernel(p2_ctx *ctx, int variant);
 /* x = one preconditioning V-cycle (the solver's precision, exact coarsest
  * solve) applied from zero to the level-0 right-hand side b, both

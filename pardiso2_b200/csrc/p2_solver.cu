@@ -1731,7 +1731,7 @@ double Solver::debug_time_sweep(int l, int sweeps)
 // Average device time of one stage of the solve on the state left by the
 // last solve, each repetition timed alone after a 256 MB write that evicts
 // L2: 0 the V-cycle residual of `level` (its rows kernel chosen by variant:
-// 0 by level size, 1 k_rows, 2 k_rows_zm), 1 the level-0
+// 0 by grid size and precision, 1 k_rows, 2 k_rows_zm), 1 the level-0
 // FP64 true residual with its float copy (same variants), 2 the restriction
 // of `level` to level + 1, 3 the prolongation of level + 1 to `level`, 4 the
 // level-0 FP64 operator q = A z (rows variants).

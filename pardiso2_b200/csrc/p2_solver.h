@@ -149,7 +149,7 @@ class Solver {
     double debug_time_smoother(int level, int passes);
     double debug_time_sweep(int level, int sweeps);
     double debug_time_stage(int stage, int level, int variant, int reps);
-    int dbg_rows_variant = 0;     // kernel of the operator rows (launch_rows), 0 = by level size
+    int dbg_rows_variant = 0;     // kernel of the operator rows (launch_rows), 0 = by grid size and precision
     void drop_graphs_public() { drop_graphs(); }
     void debug_smooth(int level, int sweeps, const double *b, double *x);
     void debug_vcycle(const double *b, double *x);
